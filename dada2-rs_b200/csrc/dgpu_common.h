@@ -1,0 +1,141 @@
+// Plain-data structures shared by the CUDA kernels and the C++ host driver.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace dgpu {
+
+// Alignment / screen parameters (AlignParams, src/nwalign.rs:63-90) plus the
+// compare-loop switches the kernels read.
+struct KParams {
+  int32_t match, mismatch, gap, homo_gap;
+  int32_t use_kmers, kmer_size, band, vectorized, gapless;
+  int32_t use_quals, greedy;
+  int32_t ncol;  // error-matrix columns
+};
+
+// Device view of a pool of uniques (one or more samples, concatenated).
+struct PoolDev {
+  const uint8_t* seq;     // 1..4 codes; raw g starts at off[g]
+  const uint8_t* qual;    // rounded mean Phred, same offsets (nullptr: none)
+  const uint32_t* off;
+  const uint32_t* len;
+  const uint8_t* kmer8;   // nraw x 4^k saturating u8 counts
+  const uint32_t* reads;
+  const uint8_t* lock;
+  double* e_minmax;
+  const double* err;      // 16 x ncol
+  // per-raw results of the latest compare launch
+  double* res_lambda;
+  uint32_t* res_ham;
+  uint8_t* res_status;
+  uint32_t nraw;
+  uint32_t maxlen;
+};
+
+// One compare task: a new center against every raw of one sample.
+struct TaskDev {
+  uint32_t base;          // first global raw of the sample
+  uint32_t n;             // raws in the sample
+  uint32_t center;        // global raw index of the center
+  uint32_t center_reads;
+  double total_reads;     // B.reads of the sample
+  double cutoff;          // kdist_cutoff for this call
+  uint32_t out_off;       // first slot of this task's comp output
+  uint32_t cluster;       // cluster index i (for the store's update_raw rule)
+};
+
+// res_status layout: low 2 bits = outcome, next 3 bits = aligner.
+enum : uint8_t { ST_ALIGNED = 0, ST_SKIPPED = 1, ST_SHROUDED = 2 };
+enum : uint8_t { AM_NONE = 0, AM_GAPLESS = 1, AM_VECTORIZED = 2, AM_HOMO = 3, AM_ENDSFREE = 4 };
+
+// Per-task counters written by the store kernel.
+enum { TC_SCREENED = 0, TC_ALIGNED, TC_SHROUD, TC_STORED, TC_GAPLESS, TC_VECTORIZED, TC_HOMO,
+       TC_ENDSFREE, TC_NCOUNTERS };
+
+// Device error bits (OR-ed into the status word; the host turns them into codes).
+enum : uint32_t {
+  DERR_TRACEBACK = 1u << 0,   // invalid pointer reached (the reference panics here)
+  DERR_GEOMETRY = 1u << 1,    // a pair exceeded the scratch bounds it was sized for
+  DERR_BAND_RANGE = 1u << 2,  // vectorized band bookkeeping left the compressed matrix
+  DERR_UNSUPPORTED = 1u << 3, // band wider than the row-major kernel supports
+  DERR_LAMBDA = 1u << 4,      // a non-ACGT code reached the lambda product
+};
+
+// Scratch geometry for the NW kernels, sized by the host for a pool.
+struct NwGeom {
+  int32_t lmax;        // longest sequence
+  int32_t vec_ncol;    // bound on the vectorized compressed width
+  int32_t vec_nrow;    // 2*lmax+1
+  int32_t rm_pairs;    // bound on offset pairs of the row-major band (ceil(W/2))
+  int32_t nwarps;      // resident warps of the persistent NW kernels
+  size_t vec_scratch;  // bytes per warp (pointer matrix)
+  size_t rm_scratch;   // bytes per warp (pointer bit planes)
+};
+
+// ---- shared-memory carving, used by kernels and by the host sizing code ----
+constexpr int kScreenWarps = 8;   // warps per screen CTA
+constexpr int kNwWarps = 4;       // warps per NW CTA
+constexpr int kStageBytes = 4096; // traceback staging per warp
+
+__host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
+__host__ __device__ inline size_t err_smem_bytes(int ncol) { return align16(size_t(16) * size_t(ncol) * 8); }
+__host__ __device__ inline size_t screen_smem_per_warp(uint32_t maxlen) {
+  return align16(size_t(maxlen) * 2) + align16(maxlen);
+}
+__host__ __device__ inline int rm_kbound(int rm_pairs) {
+  int k = (rm_pairs + 31) / 32, b = 1;
+  while (b < k) b <<= 1;
+  return b;
+}
+__host__ __device__ inline size_t nw_smem_per_warp_vec(const NwGeom& g) {
+  return align16(g.lmax) * 2 + align16(size_t(3) * g.vec_ncol * 2) + align16(size_t(g.vec_ncol) * 2) +
+         align16(g.vec_ncol) + align16(kStageBytes) + align16(g.lmax) + align16(size_t(g.lmax) * 2);
+}
+__host__ __device__ inline size_t nw_smem_per_warp_rm(const NwGeom& g) {
+  return align16(g.lmax) * 4 + align16(size_t(32) * 2 * rm_kbound(g.rm_pairs) * 4) + align16(g.lmax) +
+         align16(size_t(g.lmax) * 2);
+}
+
+// ---- launchers (dgpu_kernels.cu) ----
+void launch_profiles(const uint8_t* seq, const uint32_t* off, const uint32_t* len, uint32_t nraw,
+                     int k, uint8_t* kmer8, cudaStream_t st);
+// Runs screen/gapless/lambda, both NW kernels and the ordered store for `ntask`
+// tasks; `task_prefix` holds ntask+1 running raw counts.
+struct CompareLaunch {
+  PoolDev pool;
+  KParams kp;
+  const TaskDev* tasks;
+  const uint32_t* task_prefix;
+  uint32_t ntask;
+  uint32_t total_items;
+  uint32_t* queue_vec;      // nraw capacity
+  uint32_t* queue_rm;
+  uint32_t* queue_counts;   // [2]
+  uint8_t* nw_scratch;      // nwarps * max(vec_scratch, rm_scratch)
+  NwGeom geom;
+  uint32_t* err_word;
+  // store outputs
+  uint32_t* comp_index;
+  double* comp_lambda;
+  uint32_t* comp_ham;
+  uint32_t* task_counters;  // ntask * TC_NCOUNTERS
+  uint32_t* task_nstored;   // ntask
+  double* task_self;        // ntask
+  int do_store;
+};
+// ev (optional): 5 events recorded before the screen and after screen, vectorized NW,
+// row-major NW and store, for per-kernel device times.
+void launch_compare(const CompareLaunch& L, cudaStream_t st, cudaEvent_t* ev = nullptr);
+
+// Alignment-only entry used by the parity tests: emits al0/al1 strings.
+void launch_align_debug(int which, const uint8_t* s1cat, const uint32_t* off1, const uint32_t* len1,
+                        const uint8_t* s2cat, const uint32_t* off2, const uint32_t* len2, uint32_t npairs,
+                        KParams kp, int end_gap, const NwGeom& geom, uint8_t* scratch, uint8_t* al0,
+                        uint8_t* al1, const uint32_t* aloff, uint32_t* alen, uint32_t* err_word,
+                        cudaStream_t st);
+
+}  // namespace dgpu

@@ -1,0 +1,1608 @@
+// Host side of the B200 compare step: device pools, the clustering loop that
+// drives the compare kernels, and the C ABI declared in include/dada2_b200.h.
+//
+// The loop restates run_dada (src/dada.rs:749-1110): compare cluster 0 with the
+// screen off, then bud -> compare -> shuffle -> p-update until nothing buds. The
+// compare (screen, alignment, lambda, store) runs on the GPU; the serial phases
+// (shuffle, p-update, bud) run here, one host thread per sample in batch mode.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <functional>
+#include <limits>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "dada2_b200.h"
+#include "dgpu_common.h"
+
+namespace dgpu {
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CUDA_TRY(x)                                                                     \
+  do {                                                                                  \
+    cudaError_t e_ = (x);                                                               \
+    if (e_ != cudaSuccess) return fail(DGPU_E_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define TRY(x)            \
+  do {                    \
+    int r_ = (x);         \
+    if (r_ != 0) return r_; \
+  } while (0)
+
+using Clock = std::chrono::steady_clock;
+static double secs(Clock::time_point a, Clock::time_point b) { return std::chrono::duration<double>(b - a).count(); }
+
+// Process-wide kernel accounting behind dgpu_stats_*.
+struct GlobalStats {
+  std::mutex mu;
+  dgpu_kernel_stats s{};
+  std::atomic<bool> timing{false};
+  std::vector<double> round_ms;  // latency of each compare call (launch to results on the host)
+};
+static GlobalStats g_stats;
+
+// ---------------------------------------------------------------------------
+// Buffers
+// ---------------------------------------------------------------------------
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  int alloc(size_t count) {
+    release();
+    if (count == 0) count = 1;
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(DGPU_E_NOMEM, "cudaMalloc(" + std::to_string(count * sizeof(T)) + " bytes): " + cudaGetErrorString(e));
+    }
+    p = static_cast<T*>(q);
+    n = count;
+    return 0;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+};
+
+// Pinned host memory mapped into the device address space: the store kernel
+// writes its small per-call outputs straight into it.
+template <class T>
+struct HBuf {
+  T* h = nullptr;
+  T* d = nullptr;
+  size_t n = 0;
+  int alloc(size_t count) {
+    release();
+    if (count == 0) count = 1;
+    void* q = nullptr;
+    cudaError_t e = cudaHostAlloc(&q, count * sizeof(T), cudaHostAllocMapped);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(DGPU_E_NOMEM, std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
+    }
+    void* dq = nullptr;
+    e = cudaHostGetDevicePointer(&dq, q, 0);
+    if (e != cudaSuccess) {
+      cudaFreeHost(q);
+      cudaGetLastError();
+      return fail(DGPU_E_CUDA, std::string("cudaHostGetDevicePointer: ") + cudaGetErrorString(e));
+    }
+    h = static_cast<T*>(q);
+    d = static_cast<T*>(dq);
+    n = count;
+    return 0;
+  }
+  void release() {
+    if (h) cudaFreeHost(h);
+    h = d = nullptr;
+    n = 0;
+  }
+  HBuf() = default;
+  HBuf(const HBuf&) = delete;
+  HBuf& operator=(const HBuf&) = delete;
+  ~HBuf() { release(); }
+};
+
+// ---------------------------------------------------------------------------
+// Device pool: the resident uniques of one or more samples
+// ---------------------------------------------------------------------------
+struct Pool {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  uint32_t nraw = 0, lmax = 0, lmin = 0;
+  KParams kp{};
+  NwGeom geom{};
+  int sms = 148;
+  DBuf<uint8_t> seq, qual, kmer8, lock, status;
+  DBuf<uint32_t> off, len, reads, ham, queue_vec, queue_rm, queue_counts, err_word;
+  DBuf<double> e_minmax, err, lambda;
+  DBuf<uint8_t> scratch;
+  DBuf<TaskDev> tasks;
+  DBuf<uint32_t> task_prefix;
+  HBuf<uint32_t> comp_index, comp_ham, task_counters, task_nstored;
+  HBuf<double> comp_lambda, task_self;
+  HBuf<TaskDev> task_stage;
+  HBuf<uint32_t> prefix_stage;
+  HBuf<uint8_t> lock_host;  // pinned host copy of every lock flag
+  bool has_qual = false;
+  uint32_t ntask_cap = 0;
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+
+  ~Pool() {
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    if (st) cudaStreamDestroy(st);
+  }
+
+  int init(int dev) {
+    device = dev;
+    CUDA_TRY(cudaSetDevice(dev));
+    CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
+    return 0;
+  }
+
+  // seqs: codes 1..4 concatenated; quals_u8 may be null.
+  int upload(uint32_t n, const uint8_t* seqs, const uint32_t* offs, const uint32_t* lens, const uint8_t* quals_u8,
+             const uint32_t* rd, const KParams& params, const double* errm) {
+    kp = params;
+    nraw = n;
+    lmax = 0;
+    lmin = 0xffffffffu;
+    uint64_t total = 0;
+    for (uint32_t t = 0; t < n; ++t) {
+      lmax = std::max(lmax, lens[t]);
+      lmin = std::min(lmin, lens[t]);
+      total += lens[t];
+    }
+    if (total >= 0xffffffffull) return fail(DGPU_E_UNSUPPORTED, "more than 4 GiB of sequence in one pool");
+    std::vector<uint32_t> o(n);
+    std::vector<uint8_t> packed(total ? total : 1);
+    std::vector<uint8_t> qpacked;
+    has_qual = quals_u8 != nullptr;
+    if (has_qual) qpacked.resize(total ? total : 1);
+    uint64_t w = 0;
+    for (uint32_t t = 0; t < n; ++t) {
+      o[t] = uint32_t(w);
+      std::memcpy(packed.data() + w, seqs + offs[t], lens[t]);
+      if (has_qual) std::memcpy(qpacked.data() + w, quals_u8 + offs[t], lens[t]);
+      w += lens[t];
+    }
+    const size_t nk = size_t(1) << (2 * kp.kmer_size);
+    TRY(seq.alloc(packed.size()));
+    TRY(off.alloc(n));
+    TRY(len.alloc(n));
+    TRY(reads.alloc(n));
+    TRY(lock.alloc(n));
+    TRY(status.alloc(n));
+    TRY(ham.alloc(n));
+    TRY(lambda.alloc(n));
+    TRY(e_minmax.alloc(n));
+    TRY(queue_vec.alloc(n));
+    TRY(queue_rm.alloc(n));
+    TRY(queue_counts.alloc(4));
+    TRY(err_word.alloc(1));
+    TRY(err.alloc(size_t(16) * kp.ncol));
+    TRY(kmer8.alloc(kp.use_kmers ? size_t(n) * nk : 1));
+    TRY(comp_index.alloc(n));
+    TRY(comp_ham.alloc(n));
+    TRY(comp_lambda.alloc(n));
+    TRY(lock_host.alloc(n));
+    std::memset(lock_host.h, 0, n);
+    if (has_qual) {
+      TRY(qual.alloc(qpacked.size()));
+      CUDA_TRY(cudaMemcpyAsync(qual.p, qpacked.data(), qpacked.size(), cudaMemcpyHostToDevice, st));
+    }
+    CUDA_TRY(cudaMemcpyAsync(seq.p, packed.data(), packed.size(), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(off.p, o.data(), size_t(n) * 4, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(len.p, lens, size_t(n) * 4, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(reads.p, rd, size_t(n) * 4, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(err.p, errm, size_t(16) * kp.ncol * 8, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemsetAsync(lock.p, 0, n, st));
+    CUDA_TRY(cudaMemsetAsync(err_word.p, 0, 4, st));
+    TRY(reset_e_minmax());
+    if (kp.use_kmers) {
+      launch_profiles(seq.p, off.p, len.p, n, kp.kmer_size, kmer8.p, st);
+      std::lock_guard<std::mutex> g(g_stats.mu);
+      g_stats.s.launches[0] += 1;
+    }
+    CUDA_TRY(cudaGetLastError());
+    TRY(size_nw());
+    CUDA_TRY(cudaStreamSynchronize(st));  // the staging vectors go out of scope
+    return 0;
+  }
+
+  int reset_e_minmax() {
+    std::vector<double> v(nraw ? nraw : 1, -999.0);  // B::new (src/containers.rs:342)
+    CUDA_TRY(cudaMemcpyAsync(e_minmax.p, v.data(), size_t(nraw) * 8, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return 0;
+  }
+
+  int size_nw() {
+    const bool use_homo = kp.homo_gap != kp.gap && kp.homo_gap <= 0;
+    const bool vec_possible = kp.vectorized && !use_homo && lmin <= 3500;
+    const bool rm_possible = use_homo || !kp.vectorized || lmax > 3500;
+    geom.lmax = int32_t(lmax);
+    const int64_t bb = kp.band < 0 ? int64_t(lmax) : int64_t(kp.band);
+    const int64_t diff = int64_t(lmax) - int64_t(lmin);
+    geom.vec_ncol = int32_t(4 + (std::min<int64_t>(bb, lmax) + 1) / 2 + std::min<int64_t>(bb + diff, lmax) / 2);
+    geom.vec_nrow = int32_t(2 * lmax + 1);
+    int64_t W = kp.band < 0 ? int64_t(2 * lmax + 1) : std::min<int64_t>(2 * bb + diff + 1, 2 * int64_t(lmax) + 1);
+    geom.rm_pairs = int32_t(std::min<int64_t>((W + 1) / 2, 512));
+    const int kb = rm_kbound(geom.rm_pairs);
+    geom.vec_scratch = vec_possible ? align16(size_t(geom.vec_nrow) * size_t(geom.vec_ncol)) : 0;
+    geom.rm_scratch = rm_possible ? align16(size_t(2 * lmax + 1) * 2 * kb * 4) : 0;
+    geom.nwarps = sms * 2 * kNwWarps;
+    const size_t per = std::max<size_t>(std::max(geom.vec_scratch, geom.rm_scratch), 16);
+    TRY(scratch.alloc(per * size_t(geom.nwarps)));
+    return 0;
+  }
+
+  PoolDev view() const {
+    PoolDev v;
+    v.seq = seq.p;
+    v.qual = has_qual ? qual.p : nullptr;
+    v.off = off.p;
+    v.len = len.p;
+    v.kmer8 = kmer8.p;
+    v.reads = reads.p;
+    v.lock = lock.p;
+    v.e_minmax = e_minmax.p;
+    v.err = err.p;
+    v.res_lambda = lambda.p;
+    v.res_ham = ham.p;
+    v.res_status = status.p;
+    v.nraw = nraw;
+    v.maxlen = lmax;
+    return v;
+  }
+
+  int ensure_tasks(uint32_t ntask) {
+    if (ntask <= ntask_cap) return 0;
+    uint32_t cap = std::max<uint32_t>(ntask, 64);
+    TRY(tasks.alloc(cap));
+    TRY(task_prefix.alloc(cap + 1));
+    TRY(task_counters.alloc(size_t(cap) * TC_NCOUNTERS));
+    TRY(task_nstored.alloc(cap));
+    TRY(task_self.alloc(cap));
+    TRY(task_stage.alloc(cap));
+    TRY(prefix_stage.alloc(cap + 1));
+    ntask_cap = cap;
+    return 0;
+  }
+
+  // Launches one compare over `ntask` tasks already in task_stage; waits for it.
+  int run_compare(uint32_t ntask, bool do_store, double* wait_s) {
+    const auto t_call = Clock::now();
+    TRY(ensure_tasks(ntask));
+    uint32_t total = 0;
+    for (uint32_t t = 0; t < ntask; ++t) {
+      prefix_stage.h[t] = total;
+      task_stage.h[t].out_off = total;
+      total += task_stage.h[t].n;
+    }
+    prefix_stage.h[ntask] = total;
+    CUDA_TRY(cudaMemcpyAsync(tasks.p, task_stage.h, sizeof(TaskDev) * ntask, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(task_prefix.p, prefix_stage.h, 4 * (ntask + 1), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemsetAsync(queue_counts.p, 0, 16, st));
+    CompareLaunch L{};
+    L.pool = view();
+    L.kp = kp;
+    L.tasks = tasks.p;
+    L.task_prefix = task_prefix.p;
+    L.ntask = ntask;
+    L.total_items = total;
+    L.queue_vec = queue_vec.p;
+    L.queue_rm = queue_rm.p;
+    L.queue_counts = queue_counts.p;
+    L.nw_scratch = scratch.p;
+    L.geom = geom;
+    L.err_word = err_word.p;
+    L.comp_index = comp_index.d;
+    L.comp_lambda = comp_lambda.d;
+    L.comp_ham = comp_ham.d;
+    L.task_counters = task_counters.d;
+    L.task_nstored = task_nstored.d;
+    L.task_self = task_self.d;
+    L.do_store = do_store ? 1 : 0;
+    const bool timing = g_stats.timing.load();
+    launch_compare(L, st, timing ? ev : nullptr);
+    CUDA_TRY(cudaGetLastError());
+    auto t0 = Clock::now();
+    CUDA_TRY(cudaStreamSynchronize(st));
+    const auto t1 = Clock::now();
+    if (wait_s) *wait_s += secs(t0, t1);
+    {
+      float ms[4] = {0, 0, 0, 0};
+      if (timing)
+        for (int k = 0; k < 4; ++k) CUDA_TRY(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));
+      uint64_t screened = 0;
+      if (do_store)
+        for (uint32_t t = 0; t < ntask; ++t) screened += task_counters.h[size_t(t) * TC_NCOUNTERS + TC_SCREENED];
+      std::lock_guard<std::mutex> g(g_stats.mu);
+      dgpu_kernel_stats& S = g_stats.s;
+      S.launches[1] += 1;
+      S.launches[2] += 1;
+      S.launches[3] += 1;
+      if (do_store) S.launches[4] += 1;
+      for (int k = 0; k < 4; ++k) S.ms[k + 1] += ms[k];
+      S.rounds += 1;
+      S.compares += total;
+      S.screened += screened;
+      S.screen_bytes += screened * (uint64_t(1) << (2 * kp.kmer_size)) + uint64_t(total) * 16u;
+      if (g_stats.round_ms.size() < (size_t(1) << 20)) g_stats.round_ms.push_back(1e3 * secs(t_call, t1));
+    }
+    uint32_t ew = 0;
+    CUDA_TRY(cudaMemcpy(&ew, err_word.p, 4, cudaMemcpyDeviceToHost));
+    if (ew) {
+      cudaMemsetAsync(err_word.p, 0, 4, st);
+      std::string what;
+      if (ew & DERR_TRACEBACK) what += " invalid traceback pointer;";
+      if (ew & DERR_GEOMETRY) what += " alignment exceeded its scratch bounds;";
+      if (ew & DERR_BAND_RANGE) what += " vectorized band left the compressed matrix;";
+      if (ew & DERR_UNSUPPORTED) what += " band wider than 1024 offsets on the row-major aligner;";
+      if (ew & DERR_LAMBDA) what += " non-ACGT code or quality beyond the error matrix in lambda;";
+      return fail(ew & DERR_UNSUPPORTED ? DGPU_E_UNSUPPORTED : DGPU_E_DEVICE, "device error:" + what);
+    }
+    return 0;
+  }
+
+  int push_locks(uint32_t base, uint32_t n) {
+    CUDA_TRY(cudaMemcpyAsync(lock.p + base, lock_host.h + base, n, cudaMemcpyHostToDevice, st));
+    return 0;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Clustering state of one sample (containers.rs B/Bi/Raw, SoA)
+// ---------------------------------------------------------------------------
+struct Comp {
+  uint32_t i = 0, index = 0;
+  double lambda = 0.0;
+  uint32_t hamming = 0;
+};
+struct BudCand {
+  double p;
+  uint32_t reads;
+  uint32_t r;
+  uint32_t raw;
+};
+struct Cand {
+  uint32_t ci;
+  double lambda;
+  uint32_t hamming;
+};
+struct Cluster {
+  int64_t center = -1;
+  std::vector<uint32_t> raws;
+  uint32_t reads = 0;
+  bool update_e = true, check_locks = true;
+  double self_ = 0.0;
+  int32_t birth_type = 0;
+  uint32_t birth_from = 0;
+  double birth_pval = 0.0, birth_fold = 1.0, birth_e = 0.0;
+  Comp birth_comp;
+  std::vector<Comp> comp;
+  bool has_bm = false, has_bmp = false;
+  BudCand bm{}, bmp{};
+};
+
+struct RunStats {
+  uint64_t compare_calls = 0, cmp_scanned = 0, screened = 0, aligned = 0, stored = 0;
+  uint64_t gapless = 0, vectorized = 0, homo = 0, endsfree = 0, shuffle_calls = 0, shuffle_moves = 0;
+  double t_compare = 0, t_total = 0, t_host = 0, t_wait = 0;
+};
+
+struct DadaConf {
+  double omega_a, omega_p, omega_c, min_fold, kdist_cutoff;
+  bool detect_singletons, greedy;
+  uint32_t min_hamming, min_abund;
+  size_t max_clust;
+};
+
+struct SampleState {
+  uint32_t n = 0, base = 0;
+  uint32_t total_reads = 0;
+  const uint32_t* reads = nullptr;  // n entries
+  const uint8_t* prior = nullptr;   // n entries
+  uint8_t* lock = nullptr;          // n entries, pinned (Pool::lock_host + base)
+  std::vector<Comp> rcomp;
+  std::vector<double> p;
+  std::vector<uint32_t> raw_cluster;
+  std::vector<Cluster> clusters;
+  std::vector<std::vector<Cand>> cand;
+  uint64_t nalign = 0, nshroud = 0;
+  RunStats stats;
+  bool lock_dirty = false, done = false;
+  int64_t pending = -1;  // cluster whose compare is queued
+  // shuffle carry (src/cluster.rs:848-866)
+  std::vector<Comp> compmax;
+  std::vector<double> emax;
+  std::vector<uint32_t> reads_used, dirty_list, reads_fell_list;
+  std::vector<uint8_t> in_affected, dirty_cluster, reads_fell;
+  std::vector<uint32_t> affected;
+  bool built = false;
+  const DadaConf* conf = nullptr;
+
+  void init(uint32_t n_, uint32_t base_, const uint32_t* rd, const uint8_t* pr, uint8_t* lk, const DadaConf* c) {
+    n = n_;
+    base = base_;
+    reads = rd;
+    prior = pr;
+    lock = lk;
+    conf = c;
+    total_reads = 0;
+    for (uint32_t t = 0; t < n; ++t) total_reads += reads[t];
+    rcomp.assign(n, Comp());
+    p.assign(n, 0.0);
+    raw_cluster.assign(n, 0);
+    cand.assign(n, {});
+    clusters.clear();
+    Cluster c0;
+    c0.birth_e = double(total_reads);
+    c0.raws.resize(n);
+    for (uint32_t t = 0; t < n; ++t) c0.raws[t] = t;
+    c0.reads = total_reads;
+    clusters.push_back(std::move(c0));
+    assign_center(0);
+  }
+
+  void assign_center(size_t i) {  // src/containers.rs:450-463 (last maximum wins)
+    Cluster& c = clusters[i];
+    if (c.raws.empty()) return;
+    uint32_t best = c.raws[0];
+    for (uint32_t r : c.raws)
+      if (reads[r] >= reads[best]) best = r;
+    c.center = best;
+  }
+
+  void add_raw(size_t ci, uint32_t raw) {  // src/containers.rs:403-415
+    raw_cluster[raw] = uint32_t(ci);
+    clusters[ci].raws.push_back(raw);
+    clusters[ci].reads += reads[raw];
+    clusters[ci].update_e = true;
+  }
+
+  uint32_t pop_raw(size_t ci, size_t r) {  // src/containers.rs:424-435 (swap_remove)
+    std::vector<uint32_t>& v = clusters[ci].raws;
+    uint32_t raw = v[r];
+    v[r] = v.back();
+    v.pop_back();
+    clusters[ci].reads -= reads[raw];
+    clusters[ci].update_e = true;
+    return raw;
+  }
+
+  TaskDev task_for(size_t ci, double cutoff) const {
+    TaskDev T{};
+    T.base = base;
+    T.n = n;
+    T.center = base + uint32_t(clusters[ci].center);
+    T.center_reads = reads[clusters[ci].center];
+    T.total_reads = double(total_reads);
+    T.cutoff = cutoff;
+    T.cluster = uint32_t(ci);
+    return T;
+  }
+
+  // The store's host half: comps from the device into cluster ci (src/cluster.rs:351-397).
+  void absorb(size_t ci, const Pool& P, uint32_t t) {
+    const uint32_t* ctr = P.task_counters.h + size_t(t) * TC_NCOUNTERS;
+    const uint32_t ns = P.task_nstored.h[t];
+    const uint32_t o = P.task_stage.h[t].out_off;
+    nalign += ctr[TC_SCREENED];
+    nshroud += ctr[TC_SHROUD];
+    stats.compare_calls++;
+    stats.cmp_scanned += n;
+    stats.screened += ctr[TC_SCREENED];
+    stats.aligned += ctr[TC_ALIGNED];
+    stats.stored += ns;
+    stats.gapless += ctr[TC_GAPLESS];
+    stats.vectorized += ctr[TC_VECTORIZED];
+    stats.homo += ctr[TC_HOMO];
+    stats.endsfree += ctr[TC_ENDSFREE];
+    Cluster& c = clusters[ci];
+    c.self_ = P.task_self.h[t];
+    c.comp.resize(ns);
+    const uint32_t center = uint32_t(c.center);
+    for (uint32_t k = 0; k < ns; ++k) {
+      Comp cp{uint32_t(ci), P.comp_index.h[o + k], P.comp_lambda.h[o + k], P.comp_ham.h[o + k]};
+      c.comp[k] = cp;
+      if (ci == 0 || cp.index == center) rcomp[cp.index] = cp;
+    }
+    for (const Comp& cp : c.comp) cand[cp.index].push_back(Cand{uint32_t(ci), cp.lambda, cp.hamming});  // index_add_cluster
+  }
+
+  // ---- pval.rs ----
+  void p_update() {  // src/pval.rs:45-130
+    const DadaConf& C = *conf;
+    for (size_t i = 0; i < clusters.size(); ++i) {
+      Cluster& bi = clusters[i];
+      if (bi.update_e) {
+        const uint32_t bi_reads = bi.reads;
+        bool have = false, havep = false;
+        BudCand bm{}, bmp{};
+        for (size_t r = 0; r < bi.raws.size(); ++r) {
+          const uint32_t raw = bi.raws[r];
+          const double pv = get_pA(reads[raw], prior[raw] != 0, rcomp[raw].lambda, rcomp[raw].hamming, bi_reads);
+          p[raw] = pv;
+          if (r == 0) continue;
+          if (reads[raw] < C.min_abund || rcomp[raw].hamming < C.min_hamming) continue;
+          const bool fold_ok = C.min_fold <= 1.0 || double(reads[raw]) >= C.min_fold * rcomp[raw].lambda * double(bi_reads);
+          if (!fold_ok) continue;
+          const BudCand cd{pv, reads[raw], uint32_t(r), raw};
+          if (!have || pv < bm.p || (pv == bm.p && cd.reads > bm.reads)) {
+            bm = cd;
+            have = true;
+          }
+          if (prior[raw] && (!havep || pv < bmp.p || (pv == bmp.p && cd.reads > bmp.reads))) {
+            bmp = cd;
+            havep = true;
+          }
+        }
+        bi.has_bm = have;
+        bi.bm = bm;
+        bi.has_bmp = havep;
+        bi.bmp = bmp;
+        bi.update_e = false;
+      }
+      if (C.greedy && bi.check_locks) {
+        const int64_t center = bi.center;
+        const uint32_t cr = center >= 0 ? reads[center] : 0;
+        for (uint32_t raw : bi.raws) {
+          const bool l = double(cr) * rcomp[raw].lambda > double(reads[raw]) || int64_t(raw) == center;
+          if (l && !lock[raw]) {
+            lock[raw] = 1;
+            lock_dirty = true;
+          }
+        }
+        bi.check_locks = false;
+      }
+    }
+  }
+
+  double get_pA(uint32_t rd, bool pr, double lambda, uint32_t hamming, uint32_t bi_reads) const {  // src/pval.rs:376-398
+    if (rd == 1 && !pr && !conf->detect_singletons) return 1.0;
+    if (hamming == 0) return 1.0;
+    if (lambda == 0.0) return 0.0;
+    return calc_pA(rd, lambda * double(bi_reads), pr || conf->detect_singletons);
+  }
+
+  // Regularised lower incomplete gamma, statrs 0.18.0's Poisson::sf kernel,
+  // following the published Cephes igam/igamc method (series when x <= 1 or
+  // x <= a, Legendre continued fraction otherwise).
+  static double gamma_lr(double a, double x) {
+    const double eps = 1e-15, big = 4503599627370496.0, big_inv = 2.22044604925031308085e-16;
+    if (std::isnan(a) || std::isnan(x)) return std::numeric_limits<double>::quiet_NaN();
+    const double ax = a * std::log(x) - x - std::lgamma(a);
+    if (ax < -709.78271289338399) return a < x ? 1.0 : 0.0;
+    if (x <= 1.0 || x <= a) {
+      double r = a, c = 1.0, ans = 1.0;
+      for (;;) {
+        r += 1.0;
+        c *= x / r;
+        ans += c;
+        if (c / ans <= eps) break;
+      }
+      return std::exp(ax) * ans / a;
+    }
+    double y = 1.0 - a, z = x + y + 1.0, c = 0.0;
+    double p3 = 1.0, q3 = x, p2 = x + 1.0, q2 = z * x, ans = p2 / q2;
+    for (;;) {
+      y += 1.0;
+      z += 2.0;
+      c += 1.0;
+      const double yc = y * c;
+      const double pn = p2 * z - p3 * yc, qn = q2 * z - q3 * yc;
+      p3 = p2;
+      p2 = pn;
+      q3 = q2;
+      q2 = qn;
+      if (std::fabs(pn) > big) {
+        p3 *= big_inv;
+        p2 *= big_inv;
+        q3 *= big_inv;
+        q2 *= big_inv;
+      }
+      if (qn != 0.0) {
+        const double nx = pn / qn, er = std::fabs((ans - nx) / nx);
+        ans = nx;
+        if (er <= eps) break;
+      }
+    }
+    return 1.0 - std::exp(ax) * ans;
+  }
+
+  static double upper_tail_direct(uint32_t rd, double lambda) {  // src/pval.rs:329-353
+    const double k = double(rd);
+    double log_kfact = 0.0;
+    for (uint32_t t = 1; t <= rd; ++t) log_kfact += std::log(double(t));
+    const double log_leading = -lambda + k * std::log(lambda) - log_kfact;
+    double sum = 1.0, term = 1.0;
+    for (uint32_t j = 1; j < 10000u; ++j) {
+      term *= lambda / (k + double(j));
+      if (!std::isfinite(term) || term <= 0.0) break;
+      const double ns = sum + term;
+      if (ns == sum) break;
+      sum = ns;
+    }
+    return std::exp(log_leading + std::log(sum));
+  }
+
+  static double calc_pA(uint32_t rd, double e, bool pr) {  // src/pval.rs:208-241
+    if (!(e > 0.0)) return 1.0;
+    double pv = gamma_lr(double(rd - 1) + 1.0, e);
+    if (pv == 0.0 && e > 0.0) pv = upper_tail_direct(rd, e);
+    if (pr) return pv;
+    double norm = 1.0 - std::exp(-e);
+    if (norm < 1e-7) norm = e - 0.5 * e * e;
+    return pv / norm;
+  }
+
+  // ---- cluster.rs: bud ----
+  int64_t bud() {  // src/cluster.rs:1501-1640
+    const DadaConf& C = *conf;
+    const uint32_t ic = uint32_t(clusters[0].center);
+    bool have = false, havep = false;
+    BudCand m{}, mp{};
+    size_t mci = 0, mpci = 0;
+    double min_p = p[ic], min_pp = p[ic];
+    uint32_t min_r = reads[ic], min_rp = reads[ic];
+    for (size_t ci = 0; ci < clusters.size(); ++ci) {
+      const Cluster& c = clusters[ci];
+      if (c.has_bm && (c.bm.p < min_p || (c.bm.p == min_p && c.bm.reads > min_r))) {
+        have = true;
+        m = c.bm;
+        mci = ci;
+        min_p = c.bm.p;
+        min_r = c.bm.reads;
+      }
+      if (c.has_bmp && (c.bmp.p < min_pp || (c.bmp.p == min_pp && c.bmp.reads > min_rp))) {
+        havep = true;
+        mp = c.bmp;
+        mpci = ci;
+        min_pp = c.bmp.p;
+        min_rp = c.bmp.reads;
+      }
+    }
+    const double p_a = min_p * double(n);
+    if (p_a < C.omega_a && have) return bud_tail(mci, m.r, m.raw, p_a, 1);
+    if (min_pp < C.omega_p && havep) return bud_tail(mpci, mp.r, mp.raw, min_pp, 2);
+    return -1;
+  }
+
+  int64_t bud_tail(size_t ci, uint32_t r, uint32_t raw, double pval, int32_t type) {
+    const double expected = rcomp[raw].lambda * double(clusters[ci].reads);
+    const Comp bc = rcomp[raw];
+    const double fold = double(reads[raw]) / std::max(expected, std::numeric_limits<double>::min());
+    pop_raw(ci, r);
+    Cluster nb;
+    nb.birth_type = type;
+    if (type == 1) nb.birth_from = uint32_t(ci);
+    nb.birth_pval = pval;
+    nb.birth_fold = fold;
+    nb.birth_e = expected;
+    nb.birth_comp = bc;
+    clusters.push_back(std::move(nb));
+    const size_t nci = clusters.size() - 1;
+    add_raw(nci, raw);
+    assign_center(nci);
+    return int64_t(nci);
+  }
+
+  // ---- cluster.rs: shuffle ----
+  size_t move_pass(size_t ci) {  // src/cluster.rs:748-767
+    size_t moves = 0;
+    size_t r = clusters[ci].raws.size();
+    while (r > 0) {
+      --r;
+      const uint32_t raw = clusters[ci].raws[r];
+      const uint32_t best = compmax[raw].i;
+      if (best != ci) {
+        if (clusters[ci].center == int64_t(raw)) continue;
+        pop_raw(ci, r);
+        add_raw(best, raw);
+        rcomp[raw] = compmax[raw];
+        ++moves;
+      }
+    }
+    return moves;
+  }
+
+  void record_change(uint32_t raw, uint32_t new_ci) {  // src/cluster.rs:792-810
+    if (new_ci == compmax[raw].i) return;
+    const uint32_t cur = raw_cluster[raw];
+    if (!dirty_cluster[cur]) {
+      dirty_cluster[cur] = 1;
+      dirty_list.push_back(cur);
+    }
+  }
+
+  void grow_to(size_t nc) {
+    reads_used.resize(nc, 0);
+    dirty_cluster.resize(nc, 0);
+    reads_fell.resize(nc, 0);
+  }
+
+  // src/cluster.rs:908-1320 with the default arms (carry, prune, incremental reconcile).
+  void shuffle_converge(size_t max_shuffle) {
+    const bool carried = built;
+    if (!carried) {
+      compmax.assign(n, Comp());
+      emax.assign(n, -std::numeric_limits<double>::infinity());
+      reads_used.clear();
+      dirty_cluster.clear();
+      reads_fell.clear();
+      grow_to(clusters.size());
+      for (const Cluster& bi : clusters) {
+        const double cr = double(bi.reads);
+        for (const Comp& cp : bi.comp) {
+          const double e = cp.lambda * cr;
+          if (e > emax[cp.index]) {
+            emax[cp.index] = e;
+            compmax[cp.index] = cp;
+          }
+        }
+      }
+      for (size_t ci = 0; ci < clusters.size(); ++ci) reads_used[ci] = clusters[ci].reads;
+      built = true;
+    } else {
+      grow_to(clusters.size());
+    }
+    in_affected.resize(n, 0);
+    bool after_reconcile = false, skip_move = carried;
+    size_t nshuffle = 0;
+    for (;;) {
+      if (skip_move) {
+        skip_move = false;
+        ++nshuffle;
+      } else {
+        size_t moves = 0;
+        if (after_reconcile) {
+          std::sort(dirty_list.begin(), dirty_list.end());
+          for (size_t k = 0; k < dirty_list.size(); ++k) moves += move_pass(dirty_list[k]);
+        } else {
+          for (size_t ci = 0; ci < clusters.size(); ++ci) moves += move_pass(ci);
+        }
+        for (uint32_t ci : dirty_list) dirty_cluster[ci] = 0;
+        dirty_list.clear();
+        dirty_cluster.resize(clusters.size(), 0);
+        stats.shuffle_moves += moves;
+        ++nshuffle;
+        if (moves == 0 || nshuffle >= max_shuffle) break;
+      }
+      reads_fell.resize(clusters.size(), 0);
+      for (size_t ci = 0; ci < reads_used.size(); ++ci) {
+        if (clusters[ci].reads < reads_used[ci] && !reads_fell[ci]) {
+          reads_fell[ci] = 1;
+          reads_fell_list.push_back(uint32_t(ci));
+        }
+      }
+      for (uint32_t ci : reads_fell_list) {
+        for (const Comp& cp : clusters[ci].comp) {
+          if (compmax[cp.index].i == ci && !in_affected[cp.index]) {
+            in_affected[cp.index] = 1;
+            affected.push_back(cp.index);
+          }
+        }
+      }
+      for (size_t ci = 0; ci < clusters.size(); ++ci) {
+        const uint32_t nr = clusters[ci].reads;
+        if (nr == reads_used[ci]) continue;
+        const double rf = double(nr);
+        for (const Comp& cp : clusters[ci].comp) {
+          const uint32_t raw = cp.index;
+          if (in_affected[raw]) continue;
+          const double e = cp.lambda * rf;
+          if (compmax[raw].i == uint32_t(ci)) {
+            emax[raw] = e;
+          } else if (e > emax[raw] || (e == emax[raw] && uint32_t(ci) < compmax[raw].i)) {
+            emax[raw] = e;
+            record_change(raw, uint32_t(ci));
+            compmax[raw] = cp;
+          }
+        }
+        reads_used[ci] = nr;
+      }
+      for (uint32_t raw : affected) {
+        double be = -std::numeric_limits<double>::infinity();
+        Comp best;
+        for (const Cand& c : cand[raw]) {
+          const double e = c.lambda * double(clusters[c.ci].reads);
+          if (e > be) {
+            be = e;
+            best = Comp{c.ci, raw, c.lambda, c.hamming};
+          }
+        }
+        if (best.i != compmax[raw].i) record_change(raw, best.i);
+        compmax[raw] = best;
+        emax[raw] = be;
+        in_affected[raw] = 0;
+      }
+      affected.clear();
+      for (uint32_t ci : reads_fell_list) reads_fell[ci] = 0;
+      reads_fell_list.clear();
+      after_reconcile = true;
+    }
+    stats.shuffle_calls += nshuffle;
+  }
+
+  // After the compare of cluster ci has been absorbed: the serial tail of one
+  // loop iteration, then the next bud. Returns the next cluster to compare or -1.
+  int64_t advance(size_t ci) {
+    if (ci > 0) shuffle_converge(10);  // MAX_SHUFFLE, src/dada.rs:39
+    p_update();
+    if (clusters.size() >= conf->max_clust) return -1;
+    return bud();
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Simple persistent worker pool for the per-sample host phases
+// ---------------------------------------------------------------------------
+class Workers {
+ public:
+  explicit Workers(int n) {
+    for (int t = 0; t < n; ++t) th_.emplace_back([this] { loop(); });
+  }
+  ~Workers() {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : th_) t.join();
+  }
+  void run(size_t n, const std::function<void(size_t)>& fn) {
+    if (th_.empty() || n <= 1) {
+      for (size_t t = 0; t < n; ++t) fn(t);
+      return;
+    }
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      fn_ = &fn;
+      n_ = n;
+      next_.store(0);
+      pending_ = th_.size();
+      ++gen_;
+    }
+    cv_.notify_all();
+    for (;;) {  // the caller works too
+      size_t t = next_.fetch_add(1);
+      if (t >= n) break;
+      fn(t);
+    }
+    std::unique_lock<std::mutex> g(mu_);
+    done_.wait(g, [this] { return pending_ == 0; });
+  }
+
+ private:
+  void loop() {
+    uint64_t seen = 0;
+    for (;;) {
+      std::unique_lock<std::mutex> g(mu_);
+      cv_.wait(g, [&] { return stop_ || gen_ != seen; });
+      if (stop_) return;
+      seen = gen_;
+      const std::function<void(size_t)>* fn = fn_;
+      const size_t n = n_;
+      g.unlock();
+      for (;;) {
+        size_t t = next_.fetch_add(1);
+        if (t >= n) break;
+        (*fn)(t);
+      }
+      g.lock();
+      if (--pending_ == 0) done_.notify_all();
+    }
+  }
+  std::vector<std::thread> th_;
+  std::mutex mu_;
+  std::condition_variable cv_, done_;
+  const std::function<void(size_t)>* fn_ = nullptr;
+  size_t n_ = 0, pending_ = 0;
+  std::atomic<size_t> next_{0};
+  uint64_t gen_ = 0;
+  bool stop_ = false;
+};
+
+// ---------------------------------------------------------------------------
+// Inputs: validation and encoding (src/dada.rs:248-418)
+// ---------------------------------------------------------------------------
+struct SampleInput {
+  uint32_t n = 0;
+  std::vector<uint8_t> seq;    // codes, concatenated
+  std::vector<uint32_t> off, len, reads;
+  std::vector<uint8_t> prior, qual;
+  bool has_qual = false;
+  uint32_t qmax = 0;
+};
+
+static int encode_sample(uint32_t s, uint32_t lo, uint32_t hi, const char* seqs, const uint32_t* offs,
+                         const uint32_t* lens, const uint32_t* abund, const uint8_t* prior, const uint32_t* qsums,
+                         int k, SampleInput& out) {
+  const std::string tag = "sample " + std::to_string(s) + ": ";
+  const uint32_t n = hi - lo;
+  if (n == 0) return fail(DGPU_E_INVALID, tag + "Zero input sequences.");
+  uint32_t maxlen = 0, minlen = 0xffffffffu;
+  for (uint32_t t = lo; t < hi; ++t) {
+    maxlen = std::max(maxlen, lens[t]);
+    minlen = std::min(minlen, lens[t]);
+  }
+  if (maxlen >= 9999) return fail(DGPU_E_INVALID, tag + "Input sequences exceed the maximum allowed length (9999).");
+  if (k < 3 || k > 8) return fail(DGPU_E_INVALID, tag + "kmer_size out of supported range (3..=8).");
+  if (k > 7) return fail(DGPU_E_UNSUPPORTED, "kmer_size 8 (sparse screen) is not supported on the GPU path");
+  if (minlen <= uint32_t(k)) return fail(DGPU_E_INVALID, tag + "All input sequences must be longer than the k-mer size.");
+  out.n = n;
+  out.off.resize(n);
+  out.len.resize(n);
+  out.reads.resize(n);
+  out.prior.assign(n, 0);
+  out.has_qual = qsums != nullptr;
+  uint64_t total = 0;
+  for (uint32_t t = lo; t < hi; ++t) total += lens[t];
+  out.seq.resize(total);
+  if (out.has_qual) out.qual.resize(total);
+  uint64_t w = 0;
+  out.qmax = 0;
+  for (uint32_t t = lo; t < hi; ++t) {
+    const uint32_t r = t - lo;
+    out.off[r] = uint32_t(w);
+    out.len[r] = lens[t];
+    out.reads[r] = abund[t];
+    out.prior[r] = prior ? prior[t] : 0;
+    const char* sq = seqs + offs[t];
+    for (uint32_t p = 0; p < lens[t]; ++p) {
+      uint8_t code;
+      switch (sq[p]) {
+        case 'A': case 'a': code = 1; break;
+        case 'C': case 'c': code = 2; break;
+        case 'G': case 'g': code = 3; break;
+        case 'T': case 't': case 'U': case 'u': code = 4; break;
+        default:
+          return fail(DGPU_E_INVALID, tag + "Sequence " + std::to_string(r) + " contains a non-ACGT base at position " +
+                                          std::to_string(p) + ".");
+      }
+      out.seq[w + p] = code;
+    }
+    if (out.has_qual) {  // src/containers.rs:128-137 and the qmax of src/dada.rs:337-346
+      const double c = double(abund[t]);
+      const double cq = double(std::max<uint32_t>(abund[t], 1));
+      for (uint32_t p = 0; p < lens[t]; ++p) {
+        const double q = std::round(double(qsums[offs[t] + p]) / c);
+        out.qual[w + p] = q >= 255.0 ? 255 : (q > 0.0 ? uint8_t(q) : 0);
+        const double qm = std::round(double(qsums[offs[t] + p]) / cq);
+        out.qmax = std::max<uint32_t>(out.qmax, qm > 0 ? uint32_t(qm) : 0);
+      }
+    }
+    w += lens[t];
+  }
+  return 0;
+}
+
+// Repeat the last learned column up to qmax (src/dada.rs:337-384).
+static std::vector<double> extend_err(const double* errm, int ncol, uint32_t qmax, int& new_ncol) {
+  new_ncol = ncol;
+  if (int64_t(qmax) < ncol) return std::vector<double>(errm, errm + 16 * size_t(ncol));
+  new_ncol = int(qmax) + 1;
+  std::vector<double> ext(16 * size_t(new_ncol));
+  for (int t = 0; t < 16; ++t) {
+    for (int q = 0; q < ncol; ++q) ext[size_t(t) * new_ncol + q] = errm[size_t(t) * ncol + q];
+    for (int q = ncol; q < new_ncol; ++q) ext[size_t(t) * new_ncol + q] = errm[size_t(t) * ncol + ncol - 1];
+  }
+  return ext;
+}
+
+static KParams to_kparams(const dgpu_align_params& a, int use_quals, int greedy, int ncol) {
+  KParams k{};
+  k.match = a.match_score;
+  k.mismatch = a.mismatch;
+  k.gap = a.gap_p;
+  k.homo_gap = a.homo_gap_p;
+  k.use_kmers = a.use_kmers ? 1 : 0;
+  k.kmer_size = a.kmer_size;
+  k.band = a.band;
+  k.vectorized = a.vectorized ? 1 : 0;
+  k.gapless = a.gapless ? 1 : 0;
+  k.use_quals = use_quals ? 1 : 0;
+  k.greedy = greedy ? 1 : 0;
+  k.ncol = ncol;
+  return k;
+}
+
+}  // namespace dgpu
+
+// ---------------------------------------------------------------------------
+// Results
+// ---------------------------------------------------------------------------
+struct dgpu_result {
+  uint32_t nraw = 0;
+  std::vector<uint32_t> cl_reads, cl_birth_from, cl_birth_hamming, cl_seq_off, cl_mem_off, mem_raw, mem_hamming;
+  std::vector<int32_t> cl_birth_type, map;
+  std::vector<double> cl_birth_pval, cl_birth_fold, cl_birth_e, mem_lambda, mem_pval, pvals;
+  std::vector<uint8_t> cl_seq;
+  uint64_t counters[16] = {0};
+  double times[4] = {0};
+};
+
+namespace dgpu {
+
+// Final p-values, the map and the cluster summaries (src/dada.rs:502-564).
+static dgpu_result* finish(SampleState& S, const SampleInput& in) {
+  dgpu_result* R = new dgpu_result();
+  const uint32_t n = S.n;
+  R->nraw = n;
+  R->pvals.assign(n, 0.0);
+  R->map.assign(n, -1);
+  std::vector<uint8_t> correct(n, 0);
+  for (size_t ci = 0; ci < S.clusters.size(); ++ci) {
+    const Cluster& c = S.clusters[ci];
+    for (uint32_t raw : c.raws) {
+      double pv;
+      bool ok;
+      if (int64_t(raw) == c.center) {
+        pv = 1.0;
+        ok = true;
+      } else {
+        pv = SampleState::calc_pA(S.reads[raw], S.rcomp[raw].lambda * double(c.reads), true);
+        ok = pv >= S.conf->omega_c;
+      }
+      S.p[raw] = pv;
+      correct[raw] = ok;
+      R->pvals[raw] = pv;
+    }
+  }
+  for (size_t ci = 0; ci < S.clusters.size(); ++ci)
+    for (uint32_t raw : S.clusters[ci].raws)
+      if (correct[raw]) R->map[raw] = int32_t(ci);
+  uint32_t so = 0, mo = 0;
+  for (const Cluster& c : S.clusters) {
+    R->cl_reads.push_back(c.reads);
+    R->cl_birth_type.push_back(c.birth_type);
+    R->cl_birth_from.push_back(c.birth_from);
+    R->cl_birth_pval.push_back(c.birth_pval);
+    R->cl_birth_fold.push_back(c.birth_fold);
+    R->cl_birth_e.push_back(c.birth_e);
+    R->cl_birth_hamming.push_back(c.birth_comp.hamming);
+    R->cl_seq_off.push_back(so);
+    if (c.center >= 0) {
+      const uint32_t ce = uint32_t(c.center);
+      R->cl_seq.insert(R->cl_seq.end(), in.seq.begin() + in.off[ce], in.seq.begin() + in.off[ce] + in.len[ce]);
+      so += in.len[ce];
+    }
+    R->cl_mem_off.push_back(mo);
+    for (uint32_t raw : c.raws) {
+      R->mem_raw.push_back(raw);
+      R->mem_hamming.push_back(S.rcomp[raw].hamming);
+      R->mem_lambda.push_back(S.rcomp[raw].lambda);
+      R->mem_pval.push_back(S.p[raw]);
+    }
+    mo += uint32_t(c.raws.size());
+  }
+  R->cl_seq_off.push_back(so);
+  R->cl_mem_off.push_back(mo);
+  const RunStats& st = S.stats;
+  const uint64_t c[16] = {S.nalign, st.compare_calls, st.cmp_scanned, st.screened, st.aligned, st.stored,
+                          st.gapless, st.vectorized, st.homo, st.endsfree, st.shuffle_calls, st.shuffle_moves,
+                          S.nshroud, 0, 0, 0};
+  std::copy(c, c + 16, R->counters);
+  R->times[0] = st.t_compare;
+  R->times[1] = st.t_total;
+  R->times[2] = st.t_host;
+  R->times[3] = st.t_wait;
+  return R;
+}
+
+// The clustering loop over any number of samples resident in one pool. Every
+// round launches one compare covering each still-active sample's newest
+// cluster; the host phases then run per sample on the worker pool.
+static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_params& ap, int host_threads) {
+  const size_t ns = S.size();
+  Workers W(host_threads > 1 ? host_threads - 1 : 0);
+  std::vector<int64_t> next(ns, 0);
+  std::vector<size_t> active;
+  double wait = 0.0, host = 0.0;
+  auto t_start = Clock::now();
+  for (size_t s = 0; s < ns; ++s) S[s].pending = 0;  // round 0: cluster 0 with the screen off
+  for (;;) {
+    active.clear();
+    for (size_t s = 0; s < ns; ++s)
+      if (S[s].pending >= 0) active.push_back(s);
+    if (active.empty()) break;
+    TRY(P.ensure_tasks(uint32_t(active.size())));
+    for (size_t a = 0; a < active.size(); ++a) {
+      SampleState& ss = S[active[a]];
+      const size_t ci = size_t(ss.pending);
+      P.task_stage.h[a] = ss.task_for(ci, ci == 0 ? 1.0 : ap.kdist_cutoff);  // init_params, src/dada.rs:835-838
+      if (ss.lock_dirty) {
+        TRY(P.push_locks(ss.base, ss.n));
+        ss.lock_dirty = false;
+      }
+    }
+    auto tc = Clock::now();
+    TRY(P.run_compare(uint32_t(active.size()), true, &wait));
+    const double tcmp = secs(tc, Clock::now());
+    auto th = Clock::now();
+    W.run(active.size(), [&](size_t a) {
+      SampleState& ss = S[active[a]];
+      const size_t ci = size_t(ss.pending);
+      ss.absorb(ci, P, uint32_t(a));
+      ss.stats.t_compare += tcmp;
+      ss.pending = ss.advance(ci);
+    });
+    host += secs(th, Clock::now());
+  }
+  const double total = secs(t_start, Clock::now());
+  for (auto& ss : S) {
+    ss.stats.t_total = total;
+    ss.stats.t_host = host;
+    ss.stats.t_wait = wait;
+  }
+  return 0;
+}
+
+// A prepared batch: encoded samples resident on one device.
+struct Batch {
+  Pool pool;
+  std::vector<SampleInput> in;
+  std::vector<uint32_t> bases, reads;
+  std::vector<uint8_t> priors;
+  DadaConf conf{};
+  std::vector<DadaConf> confs;
+  dgpu_align_params align{};
+  int host_threads = 1;
+};
+
+static int batch_prepare(Batch& B, int device, const dgpu_dada_params* prm, int nsamples, const uint32_t* sample_start,
+                         const char* seqs, const uint32_t* offs, const uint32_t* lens, const uint32_t* abund,
+                         const uint8_t* prior, const uint32_t* qsums, const double* errm, int ncol) {
+  if (!prm || !seqs || !offs || !lens || !abund || !errm || nsamples <= 0 || !sample_start)
+    return fail(DGPU_E_INVALID, "null argument or no samples");
+  if (ncol <= 0) return fail(DGPU_E_INVALID, "Error matrix length does not match 16 x ncol.");
+  const int k = prm->align.kmer_size;
+  B.in.assign(static_cast<size_t>(nsamples), SampleInput());
+  uint32_t qmax = 0;
+  bool any_q = false;
+  for (int s = 0; s < nsamples; ++s) {
+    if (sample_start[s + 1] < sample_start[s]) return fail(DGPU_E_INVALID, "sample_start must be non-decreasing");
+    TRY(encode_sample(uint32_t(s), sample_start[s], sample_start[s + 1], seqs, offs, lens, abund, prior, qsums, k,
+                      B.in[size_t(s)]));
+    if (B.in[size_t(s)].has_qual) {
+      any_q = true;
+      qmax = std::max(qmax, B.in[size_t(s)].qmax);
+    }
+  }
+  int ncol2 = ncol;
+  std::vector<double> err = any_q ? extend_err(errm, ncol, qmax, ncol2)
+                                  : std::vector<double>(errm, errm + 16 * size_t(ncol));
+  std::vector<uint8_t> seqcat, qualcat;
+  std::vector<uint32_t> off, len;
+  for (const SampleInput& si : B.in) {
+    B.bases.push_back(uint32_t(off.size()));
+    const uint32_t sb = uint32_t(seqcat.size());
+    seqcat.insert(seqcat.end(), si.seq.begin(), si.seq.end());
+    if (any_q) {
+      if (si.has_qual) qualcat.insert(qualcat.end(), si.qual.begin(), si.qual.end());
+      else qualcat.insert(qualcat.end(), si.seq.size(), 0);
+    }
+    for (uint32_t r = 0; r < si.n; ++r) {
+      off.push_back(sb + si.off[r]);
+      len.push_back(si.len[r]);
+      B.reads.push_back(si.reads[r]);
+      B.priors.push_back(si.prior[r]);
+    }
+  }
+  TRY(B.pool.init(device));
+  const KParams kp = to_kparams(prm->align, prm->use_quals, prm->greedy, ncol2);
+  TRY(B.pool.upload(uint32_t(off.size()), seqcat.data(), off.data(), len.data(), any_q ? qualcat.data() : nullptr,
+                    B.reads.data(), kp, err.data()));
+  B.conf.omega_a = prm->omega_a;
+  B.conf.omega_p = prm->omega_p;
+  B.conf.omega_c = prm->omega_c;
+  B.conf.min_fold = prm->min_fold;
+  B.conf.kdist_cutoff = prm->align.kdist_cutoff;
+  B.conf.detect_singletons = prm->detect_singletons != 0;
+  B.conf.greedy = prm->greedy != 0;
+  B.conf.min_hamming = prm->min_hamming;
+  B.conf.min_abund = prm->min_abund;
+  B.confs.assign(static_cast<size_t>(nsamples), B.conf);
+  for (int s = 0; s < nsamples; ++s)
+    B.confs[size_t(s)].max_clust = prm->max_clust == 0 ? B.in[size_t(s)].n : size_t(prm->max_clust);
+  B.align = prm->align;
+  int threads = prm->host_threads;
+  if (threads <= 0) threads = int(std::max(1u, std::thread::hardware_concurrency()));
+  B.host_threads = std::min(threads, nsamples);
+  return 0;
+}
+
+static int batch_run(Batch& B, dgpu_result** out) {
+  const size_t ns = B.in.size();
+  Pool& P = B.pool;
+  CUDA_TRY(cudaSetDevice(P.device));
+  TRY(P.reset_e_minmax());
+  std::memset(P.lock_host.h, 0, P.nraw);
+  CUDA_TRY(cudaMemsetAsync(P.lock.p, 0, P.nraw, P.st));
+  std::vector<SampleState> S(ns);
+  for (size_t s = 0; s < ns; ++s)
+    S[s].init(B.in[s].n, B.bases[s], B.reads.data() + B.bases[s], B.priors.data() + B.bases[s],
+              P.lock_host.h + B.bases[s], &B.confs[s]);
+  TRY(run_samples(P, S, B.align, B.host_threads));
+  for (size_t s = 0; s < ns; ++s) out[s] = finish(S[s], B.in[s]);
+  return 0;
+}
+
+}  // namespace dgpu
+
+// ---------------------------------------------------------------------------
+// Compare-level context
+// ---------------------------------------------------------------------------
+struct dgpu_batch {
+  dgpu::Batch b;
+};
+
+struct dgpu_ctx {
+  dgpu::Pool pool;
+  dgpu::KParams kp{};
+  std::vector<double> err;
+  std::vector<uint32_t> reads;
+  bool uploaded = false;
+};
+
+using namespace dgpu;
+
+extern "C" {
+
+const char* dgpu_last_error(void) { return g_err.c_str(); }
+
+int dgpu_device_count(int* count) {
+  if (!count) return fail(DGPU_E_INVALID, "null count");
+  int c = 0;
+  cudaError_t e = cudaGetDeviceCount(&c);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *count = 0;
+    return fail(DGPU_E_CUDA, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+  }
+  *count = c;
+  return 0;
+}
+
+int dgpu_ctx_create(int device, const dgpu_align_params* params, const double* err_mat, int ncol, int use_quals,
+                    dgpu_ctx** out) {
+  if (!params || !err_mat || !out || ncol <= 0) return fail(DGPU_E_INVALID, "null argument or ncol <= 0");
+  if (params->kmer_size < 3 || params->kmer_size > 8)
+    return fail(DGPU_E_INVALID, "kmer_size out of supported range (3..=8).");
+  if (params->kmer_size > 7) return fail(DGPU_E_UNSUPPORTED, "kmer_size 8 (sparse screen) is not supported on the GPU path");
+  dgpu_ctx* c = new dgpu_ctx();
+  int rc = c->pool.init(device);
+  if (rc) {
+    delete c;
+    return rc;
+  }
+  c->kp = to_kparams(*params, use_quals, 1, ncol);
+  c->err.assign(err_mat, err_mat + 16 * size_t(ncol));
+  *out = c;
+  return 0;
+}
+
+void dgpu_ctx_destroy(dgpu_ctx* ctx) { delete ctx; }
+
+int dgpu_upload_raws(dgpu_ctx* ctx, int nraw, const uint8_t* seqs, const uint32_t* offs, const uint32_t* lens,
+                     const uint8_t* quals, const uint32_t* reads) {
+  if (!ctx || nraw <= 0 || !seqs || !offs || !lens || !reads) return fail(DGPU_E_INVALID, "null argument or nraw <= 0");
+  for (int t = 0; t < nraw; ++t) {
+    if (lens[t] <= uint32_t(ctx->kp.kmer_size)) return fail(DGPU_E_INVALID, "sequence not longer than the k-mer size");
+    if (lens[t] >= 9999) return fail(DGPU_E_INVALID, "sequence length >= 9999");
+    for (uint32_t p = 0; p < lens[t]; ++p)
+      if (seqs[offs[t] + p] < 1 || seqs[offs[t] + p] > 4) return fail(DGPU_E_INVALID, "non-ACGT code in sequence");
+    if (quals)
+      for (uint32_t p = 0; p < lens[t]; ++p)
+        if (quals[offs[t] + p] >= ctx->kp.ncol) return fail(DGPU_E_INVALID, "quality beyond the error matrix");
+  }
+  ctx->reads.assign(reads, reads + nraw);
+  TRY(ctx->pool.upload(uint32_t(nraw), seqs, offs, lens, quals, reads, ctx->kp, ctx->err.data()));
+  ctx->uploaded = true;
+  return 0;
+}
+
+int dgpu_set_locks(dgpu_ctx* ctx, const uint8_t* lock) {
+  if (!ctx || !ctx->uploaded || !lock) return fail(DGPU_E_INVALID, "no raws uploaded or null lock");
+  std::memcpy(ctx->pool.lock_host.h, lock, ctx->pool.nraw);
+  TRY(ctx->pool.push_locks(0, ctx->pool.nraw));
+  CUDA_TRY(cudaStreamSynchronize(ctx->pool.st));
+  return 0;
+}
+
+int dgpu_reset_e_minmax(dgpu_ctx* ctx) {
+  if (!ctx || !ctx->uploaded) return fail(DGPU_E_INVALID, "no raws uploaded");
+  return ctx->pool.reset_e_minmax();
+}
+
+int dgpu_get_e_minmax(dgpu_ctx* ctx, double* out) {
+  if (!ctx || !ctx->uploaded || !out) return fail(DGPU_E_INVALID, "no raws uploaded or null output");
+  CUDA_TRY(cudaMemcpy(out, ctx->pool.e_minmax.p, size_t(ctx->pool.nraw) * 8, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+static int ctx_task(dgpu_ctx* ctx, int center, int cluster_i, double cutoff, int greedy) {
+  if (!ctx || !ctx->uploaded) return fail(DGPU_E_INVALID, "no raws uploaded");
+  if (center < 0 || uint32_t(center) >= ctx->pool.nraw) return fail(DGPU_E_INVALID, "center out of range");
+  ctx->pool.kp.greedy = greedy ? 1 : 0;
+  TRY(ctx->pool.ensure_tasks(1));
+  TaskDev T{};
+  T.base = 0;
+  T.n = ctx->pool.nraw;
+  T.center = uint32_t(center);
+  T.center_reads = ctx->reads[size_t(center)];
+  uint64_t tot = 0;
+  for (uint32_t r : ctx->reads) tot += r;
+  T.total_reads = double(uint32_t(tot));
+  T.cutoff = cutoff;
+  T.cluster = uint32_t(cluster_i);
+  ctx->pool.task_stage.h[0] = T;
+  return 0;
+}
+
+static void fill_counters(const uint32_t* c, uint32_t stored, dgpu_counters* cnt) {
+  if (!cnt) return;
+  cnt->screened = c[TC_SCREENED];
+  cnt->aligned = c[TC_ALIGNED];
+  cnt->shrouded = c[TC_SHROUD];
+  cnt->stored = stored;
+  cnt->gapless = c[TC_GAPLESS];
+  cnt->vectorized = c[TC_VECTORIZED];
+  cnt->homo = c[TC_HOMO];
+  cnt->endsfree = c[TC_ENDSFREE];
+}
+
+int dgpu_compare(dgpu_ctx* ctx, int center, double kdist_cutoff, int greedy, double* lambda_out,
+                 uint32_t* hamming_out, uint8_t* skipped_out, dgpu_counters* cnt) {
+  TRY(ctx_task(ctx, center, 0, kdist_cutoff, greedy));
+  Pool& P = ctx->pool;
+  TRY(P.run_compare(1, false, nullptr));
+  const uint32_t n = P.nraw;
+  std::vector<uint8_t> st(n);
+  if (lambda_out) CUDA_TRY(cudaMemcpy(lambda_out, P.lambda.p, size_t(n) * 8, cudaMemcpyDeviceToHost));
+  if (hamming_out) CUDA_TRY(cudaMemcpy(hamming_out, P.ham.p, size_t(n) * 4, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(st.data(), P.status.p, n, cudaMemcpyDeviceToHost));
+  if (skipped_out)
+    for (uint32_t t = 0; t < n; ++t) skipped_out[t] = (st[t] & 3u) == ST_SKIPPED;
+  if (cnt) {
+    uint32_t c[TC_NCOUNTERS] = {0};
+    for (uint32_t t = 0; t < n; ++t) {
+      const uint8_t o = st[t] & 3u, m = st[t] >> 2;
+      c[TC_SCREENED] += o != ST_SKIPPED;
+      c[TC_ALIGNED] += o == ST_ALIGNED;
+      c[TC_SHROUD] += o == ST_SHROUDED;
+      c[TC_GAPLESS] += m == AM_GAPLESS;
+      c[TC_VECTORIZED] += m == AM_VECTORIZED;
+      c[TC_HOMO] += m == AM_HOMO;
+      c[TC_ENDSFREE] += m == AM_ENDSFREE;
+    }
+    fill_counters(c, 0, cnt);
+  }
+  return 0;
+}
+
+int dgpu_compare_store(dgpu_ctx* ctx, int center, int cluster_i, double kdist_cutoff, int greedy,
+                       uint32_t* comp_index, double* comp_lambda, uint32_t* comp_hamming, int* nstored,
+                       double* self_out, dgpu_counters* cnt) {
+  TRY(ctx_task(ctx, center, cluster_i, kdist_cutoff, greedy));
+  Pool& P = ctx->pool;
+  TRY(P.run_compare(1, true, nullptr));
+  const uint32_t ns = P.task_nstored.h[0];
+  if (comp_index) std::memcpy(comp_index, P.comp_index.h, size_t(ns) * 4);
+  if (comp_lambda) std::memcpy(comp_lambda, P.comp_lambda.h, size_t(ns) * 8);
+  if (comp_hamming) std::memcpy(comp_hamming, P.comp_ham.h, size_t(ns) * 4);
+  if (nstored) *nstored = int(ns);
+  if (self_out) *self_out = P.task_self.h[0];
+  fill_counters(P.task_counters.h, ns, cnt);
+  return 0;
+}
+
+int dgpu_batch_prepare(int device, const dgpu_dada_params* params, int nsamples, const uint32_t* sample_start,
+                       const char* seqs, const uint32_t* offs, const uint32_t* lens, const uint32_t* abund,
+                       const uint8_t* prior, const uint32_t* qual_sums, const double* err_mat, int ncol,
+                       dgpu_batch** out) {
+  if (!out) return fail(DGPU_E_INVALID, "null output");
+  dgpu_batch* b = new dgpu_batch();
+  int rc = batch_prepare(b->b, device, params, nsamples, sample_start, seqs, offs, lens, abund, prior, qual_sums,
+                         err_mat, ncol);
+  if (rc) {
+    delete b;
+    return rc;
+  }
+  *out = b;
+  return 0;
+}
+
+int dgpu_batch_run(dgpu_batch* batch, dgpu_result** out) {
+  if (!batch || !out) return fail(DGPU_E_INVALID, "null argument");
+  return batch_run(batch->b, out);
+}
+
+void dgpu_batch_free(dgpu_batch* batch) { delete batch; }
+
+int dgpu_dada(int device, const dgpu_dada_params* params, int nraw, const char* seqs, const uint32_t* offs,
+              const uint32_t* lens, const uint32_t* abund, const uint8_t* prior, const uint32_t* qual_sums,
+              const double* err_mat, int ncol, dgpu_result** out) {
+  if (nraw <= 0) return fail(DGPU_E_INVALID, "Zero input sequences.");
+  if (!params) return fail(DGPU_E_INVALID, "null params");
+  const uint32_t ss[2] = {0, uint32_t(nraw)};
+  dgpu_dada_params p1 = *params;
+  p1.host_threads = 1;
+  return dgpu_dada_batch(device, &p1, 1, ss, seqs, offs, lens, abund, prior, qual_sums, err_mat, ncol, out);
+}
+
+int dgpu_dada_batch(int device, const dgpu_dada_params* params, int nsamples, const uint32_t* sample_start,
+                    const char* seqs, const uint32_t* offs, const uint32_t* lens, const uint32_t* abund,
+                    const uint8_t* prior, const uint32_t* qual_sums, const double* err_mat, int ncol,
+                    dgpu_result** out) {
+  if (!out) return fail(DGPU_E_INVALID, "null output");
+  dgpu_batch b;
+  TRY(batch_prepare(b.b, device, params, nsamples, sample_start, seqs, offs, lens, abund, prior, qual_sums, err_mat,
+                    ncol));
+  return batch_run(b.b, out);
+}
+
+int dgpu_stats_reset(void) {
+  std::lock_guard<std::mutex> g(g_stats.mu);
+  g_stats.s = dgpu_kernel_stats{};
+  g_stats.round_ms.clear();
+  return 0;
+}
+
+int dgpu_stats_latencies(double* out, int cap) {
+  std::lock_guard<std::mutex> g(g_stats.mu);
+  const int n = int(std::min<size_t>(g_stats.round_ms.size(), size_t(cap > 0 ? cap : 0)));
+  if (out && n > 0) std::memcpy(out, g_stats.round_ms.data(), size_t(n) * 8);
+  return int(g_stats.round_ms.size());
+}
+
+int dgpu_stats_timing(int enable) {
+  g_stats.timing.store(enable != 0);
+  return 0;
+}
+
+int dgpu_stats_read(dgpu_kernel_stats* out) {
+  if (!out) return fail(DGPU_E_INVALID, "null output");
+  std::lock_guard<std::mutex> g(g_stats.mu);
+  *out = g_stats.s;
+  return 0;
+}
+
+int dgpu_result_sizes(const dgpu_result* r, int64_t* sizes) {
+  if (!r || !sizes) return fail(DGPU_E_INVALID, "null argument");
+  sizes[0] = int64_t(r->cl_reads.size());
+  sizes[1] = int64_t(r->nraw);
+  sizes[2] = int64_t(r->mem_raw.size());
+  sizes[3] = int64_t(r->cl_seq.size());
+  return 0;
+}
+
+int dgpu_result_fill(const dgpu_result* r, const dgpu_dada_out* o) {
+  if (!r || !o) return fail(DGPU_E_INVALID, "null argument");
+  auto cp = [](auto* dst, const auto& v) {
+    if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+  };
+  cp(o->cl_reads, r->cl_reads);
+  cp(o->cl_birth_type, r->cl_birth_type);
+  cp(o->cl_birth_from, r->cl_birth_from);
+  cp(o->cl_birth_pval, r->cl_birth_pval);
+  cp(o->cl_birth_fold, r->cl_birth_fold);
+  cp(o->cl_birth_e, r->cl_birth_e);
+  cp(o->cl_birth_hamming, r->cl_birth_hamming);
+  cp(o->cl_seq_off, r->cl_seq_off);
+  cp(o->cl_seq, r->cl_seq);
+  cp(o->cl_mem_off, r->cl_mem_off);
+  cp(o->mem_raw, r->mem_raw);
+  cp(o->mem_hamming, r->mem_hamming);
+  cp(o->mem_lambda, r->mem_lambda);
+  cp(o->mem_pval, r->mem_pval);
+  cp(o->map, r->map);
+  cp(o->pvals, r->pvals);
+  if (o->counters) std::memcpy(o->counters, r->counters, sizeof(r->counters));
+  if (o->times) std::memcpy(o->times, r->times, sizeof(r->times));
+  return 0;
+}
+
+void dgpu_result_free(dgpu_result* r) { delete r; }
+
+int dgpu_align_debug(int device, int which, int npairs, const uint8_t* s1cat, const uint32_t* off1,
+                     const uint32_t* len1, const uint8_t* s2cat, const uint32_t* off2, const uint32_t* len2,
+                     const dgpu_align_params* params, int end_gap, uint8_t* al0, uint8_t* al1, const uint32_t* al_off,
+                     uint32_t* al_len) {
+  if (npairs <= 0 || !params || !s1cat || !s2cat || which < 0 || which > 2) return fail(DGPU_E_INVALID, "bad argument");
+  CUDA_TRY(cudaSetDevice(device));
+  uint32_t lmax = 0, lmin = 0xffffffffu;
+  size_t b1 = 0, b2 = 0, bal = 0;
+  for (int t = 0; t < npairs; ++t) {
+    lmax = std::max({lmax, len1[t], len2[t]});
+    lmin = std::min({lmin, len1[t], len2[t]});
+    b1 = std::max<size_t>(b1, size_t(off1[t]) + len1[t]);
+    b2 = std::max<size_t>(b2, size_t(off2[t]) + len2[t]);
+    bal = std::max<size_t>(bal, size_t(al_off[t]) + len1[t] + len2[t]);
+    if (which == 0 && (len1[t] > 3500 || len2[t] > 3500)) return fail(DGPU_E_INVALID, "vectorized aligner needs len <= 3500");
+  }
+  KParams kp = to_kparams(*params, 0, 0, 1);
+  kp.gap = params->gap_p;
+  NwGeom g{};
+  g.lmax = int32_t(lmax);
+  const int64_t bb = kp.band < 0 ? int64_t(lmax) : int64_t(kp.band);
+  const int64_t diff = int64_t(lmax) - int64_t(lmin);
+  g.vec_ncol = int32_t(4 + (std::min<int64_t>(bb, lmax) + 1) / 2 + std::min<int64_t>(bb + diff, lmax) / 2);
+  g.vec_nrow = int32_t(2 * lmax + 1);
+  int64_t W = kp.band < 0 ? int64_t(2 * lmax + 1) : std::min<int64_t>(2 * bb + diff + 1, 2 * int64_t(lmax) + 1);
+  g.rm_pairs = int32_t(std::min<int64_t>((W + 1) / 2, 512));
+  g.vec_scratch = align16(size_t(g.vec_nrow) * g.vec_ncol);
+  g.rm_scratch = align16(size_t(2 * lmax + 1) * 2 * rm_kbound(g.rm_pairs) * 4);
+  g.nwarps = npairs;
+  const size_t per = which == 0 ? g.vec_scratch : g.rm_scratch;
+  DBuf<uint8_t> d1, d2, scr, a0, a1;
+  DBuf<uint32_t> o1, l1, o2, l2, ao, al, ew;
+  TRY(d1.alloc(b1));
+  TRY(d2.alloc(b2));
+  TRY(scr.alloc(per * size_t(npairs)));
+  TRY(a0.alloc(bal));
+  TRY(a1.alloc(bal));
+  TRY(o1.alloc(npairs));
+  TRY(l1.alloc(npairs));
+  TRY(o2.alloc(npairs));
+  TRY(l2.alloc(npairs));
+  TRY(ao.alloc(npairs));
+  TRY(al.alloc(npairs));
+  TRY(ew.alloc(1));
+  CUDA_TRY(cudaMemcpy(d1.p, s1cat, b1, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(d2.p, s2cat, b2, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(o1.p, off1, 4 * size_t(npairs), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(l1.p, len1, 4 * size_t(npairs), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(o2.p, off2, 4 * size_t(npairs), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(l2.p, len2, 4 * size_t(npairs), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(ao.p, al_off, 4 * size_t(npairs), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemset(al.p, 0, 4 * size_t(npairs)));
+  CUDA_TRY(cudaMemset(ew.p, 0, 4));
+  launch_align_debug(which, d1.p, o1.p, l1.p, d2.p, o2.p, l2.p, uint32_t(npairs), kp, end_gap, g, scr.p, a0.p, a1.p,
+                     ao.p, al.p, ew.p, nullptr);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaDeviceSynchronize());
+  uint32_t e = 0;
+  CUDA_TRY(cudaMemcpy(&e, ew.p, 4, cudaMemcpyDeviceToHost));
+  std::vector<uint8_t> h0(bal), h1(bal);
+  CUDA_TRY(cudaMemcpy(h0.data(), a0.p, bal, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(h1.data(), a1.p, bal, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(al_len, al.p, 4 * size_t(npairs), cudaMemcpyDeviceToHost));
+  for (int t = 0; t < npairs; ++t) {  // traceback order -> left to right
+    const uint32_t o = al_off[t], n = al_len[t];
+    for (uint32_t q = 0; q < n; ++q) {
+      al0[o + q] = h0[o + n - 1 - q];
+      al1[o + q] = h1[o + n - 1 - q];
+    }
+  }
+  if (e) return fail(e & DERR_UNSUPPORTED ? DGPU_E_UNSUPPORTED : DGPU_E_DEVICE, "device error flag " + std::to_string(e));
+  return 0;
+}
+
+}  // extern "C"

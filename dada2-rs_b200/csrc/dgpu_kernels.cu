@@ -1,0 +1,1050 @@
+// CUDA kernels of the dada compare step (sm_100a).
+//
+//   k_profiles  -- K1: dense saturating u8 k-mer counts per unique (src/kmers.rs:79-101)
+//   k_screen    -- K2/K3/K6: greedy skip, k-mer screen, ordered-k-mer distance, gapless
+//                  alignment and the FP64 lambda product, one warp per (center, raw)
+//                  (src/cluster.rs:279-330, src/nwalign.rs:1244-1327, src/pval.rs:253-320)
+//   k_nw_vec    -- K4: replica of the rolling i16 anti-diagonal aligner + traceback
+//                  (src/nwalign.rs:665-1140), one warp per pair, persistent
+//   k_nw_rm     -- K5: the row-major i32 ends-free / homopolymer aligner
+//                  (src/nwalign.rs:336-528) evaluated as an anti-diagonal wavefront,
+//                  one warp per pair, persistent
+//   k_store     -- K7: ordered store + e_minmax update + counters (src/cluster.rs:351-397)
+//
+// Built with --fmad=false: the FP64 product and the k-mer distances must round
+// exactly like the reference's separately-rounded operations.
+#include <cfloat>
+#include <cstdio>
+
+#include "dgpu_common.h"
+
+namespace dgpu {
+
+#define FULL 0xffffffffu
+static constexpr int kNegSentinel = -9999;  // BAND_SENTINEL, src/nwalign.rs:30
+
+__device__ __forceinline__ int16_t sadd16(int16_t a, int16_t b) {
+  int s = int(a) + int(b);
+  s = s > 32767 ? 32767 : (s < -32768 ? -32768 : s);
+  return int16_t(s);
+}
+
+__device__ __forceinline__ uint32_t find_task(const uint32_t* prefix, uint32_t ntask, uint32_t item) {
+  uint32_t lo = 0, hi = ntask;  // largest t with prefix[t] <= item
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (prefix[mid] <= item) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// ---------------------------------------------------------------------------
+// K1: k-mer profiles
+// ---------------------------------------------------------------------------
+__global__ void k_profiles(const uint8_t* __restrict__ seq, const uint32_t* __restrict__ off,
+                           const uint32_t* __restrict__ len, uint32_t nraw, int k,
+                           uint8_t* __restrict__ kmer8) {
+  extern __shared__ uint32_t cnt[];
+  const int nk = 1 << (2 * k);
+  for (uint32_t g = blockIdx.x; g < nraw; g += gridDim.x) {
+    for (int t = threadIdx.x; t < nk; t += blockDim.x) cnt[t] = 0;
+    __syncthreads();
+    const uint8_t* s = seq + off[g];
+    const int L = int(len[g]);
+    for (int p = threadIdx.x; p + k <= L; p += blockDim.x) {
+      int idx = 0;
+      bool ok = true;
+      for (int q = 0; q < k; ++q) {
+        unsigned nt = s[p + q];
+        if (nt < 1u || nt > 4u) {
+          ok = false;
+          break;
+        }
+        idx = idx * 4 + int(nt - 1u);
+      }
+      if (ok) atomicAdd(&cnt[idx], 1u);
+    }
+    __syncthreads();
+    uint32_t* out = reinterpret_cast<uint32_t*>(kmer8 + size_t(g) * size_t(nk));
+    for (int t = threadIdx.x; t < nk / 4; t += blockDim.x) {
+      uint32_t w = 0;
+      for (int b = 0; b < 4; ++b) w |= min(cnt[4 * t + b], 255u) << (8 * b);
+      out[t] = w;
+    }
+    __syncthreads();
+  }
+}
+
+void launch_profiles(const uint8_t* seq, const uint32_t* off, const uint32_t* len, uint32_t nraw, int k,
+                     uint8_t* kmer8, cudaStream_t st) {
+  if (nraw == 0) return;
+  size_t smem = size_t(4) << (2 * k);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_profiles, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  int grid = int(nraw < 148u * 16u ? nraw : 148u * 16u);
+  k_profiles<<<grid, 256, smem, st>>>(seq, off, len, nraw, k, kmer8);
+}
+
+// ---------------------------------------------------------------------------
+// Shared helpers for the lambda product
+// ---------------------------------------------------------------------------
+// fidx[p] = err row * ncol + quality column for raw position p; lane 0 then forms
+// the left-to-right product (src/pval.rs:311-313). Returns the product on all lanes.
+__device__ double lambda_chain(int lane, const uint16_t* fidx, int L, const double* err_s) {
+  double lam = 1.0;
+  if (lane == 0) {
+    int p = 0;
+    for (; p + 4 <= L; p += 4) {
+      double f0 = err_s[fidx[p]], f1 = err_s[fidx[p + 1]], f2 = err_s[fidx[p + 2]], f3 = err_s[fidx[p + 3]];
+      lam = __dmul_rn(lam, f0);
+      lam = __dmul_rn(lam, f1);
+      lam = __dmul_rn(lam, f2);
+      lam = __dmul_rn(lam, f3);
+    }
+    for (; p < L; ++p) lam = __dmul_rn(lam, err_s[fidx[p]]);
+  }
+  return __shfl_sync(FULL, lam, 0);
+}
+
+// tcode[p] (row of the error matrix for raw position p) + quality -> fidx.
+__device__ bool build_fidx(int lane, const uint8_t* tcode, const uint8_t* qual_g, int L, int ncol, int use_quals,
+                           uint16_t* fidx) {
+  bool bad = false;
+  for (int p = lane; p < L; p += 32) {
+    unsigned t = tcode[p];
+    bad |= t > 15u;
+    unsigned q = (use_quals && qual_g) ? qual_g[p] : 0u;
+    bad |= q >= unsigned(ncol);
+    fidx[p] = uint16_t(t * unsigned(ncol) + q);
+  }
+  return __any_sync(FULL, bad);
+}
+
+// ---------------------------------------------------------------------------
+// K2/K3/K6: screen, gapless alignment, lambda
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t mismatch_word(const uint8_t* a, const uint8_t* b, int base, int n, int lane) {
+  int p = base + lane;
+  bool mm = p < n && a[p] != b[p];
+  return __ballot_sync(FULL, mm);
+}
+
+__global__ void __launch_bounds__(kScreenWarps * 32) k_screen(CompareLaunch L) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const KParams& kp = L.kp;
+  double* err_s = reinterpret_cast<double*>(smem_raw);
+  const int nerr = 16 * kp.ncol;
+  for (int t = threadIdx.x; t < nerr; t += blockDim.x) err_s[t] = L.pool.err[t];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const size_t err_bytes = err_smem_bytes(kp.ncol);
+  unsigned char* wbase = smem_raw + err_bytes + size_t(wib) * screen_smem_per_warp(L.pool.maxlen);
+  uint16_t* fidx = reinterpret_cast<uint16_t*>(wbase);
+  uint8_t* tcode = wbase + align16(size_t(L.pool.maxlen) * 2);
+  __syncthreads();
+
+  const int k = kp.kmer_size;
+  const int nk16 = (1 << (2 * k)) / 16;
+  const uint32_t warps_total = gridDim.x * kScreenWarps;
+  for (uint32_t item = blockIdx.x * kScreenWarps + wib; item < L.total_items; item += warps_total) {
+    const uint32_t t = find_task(L.task_prefix, L.ntask, item);
+    const TaskDev T = L.tasks[t];
+    const uint32_t g = T.base + (item - L.task_prefix[t]);
+    const uint32_t c = T.center;
+    const int lc = int(L.pool.len[c]), lg = int(L.pool.len[g]);
+    const uint8_t* sc = L.pool.seq + L.pool.off[c];
+    const uint8_t* sg = L.pool.seq + L.pool.off[g];
+
+    if (kp.greedy && (L.pool.reads[g] > T.center_reads || L.pool.lock[g])) {
+      if (lane == 0) {
+        L.pool.res_lambda[g] = 0.0;
+        L.pool.res_ham[g] = 0xffffffffu;
+        L.pool.res_status[g] = ST_SKIPPED;
+      }
+      continue;
+    }
+    double kdist = 0.0, kodist = -1.0;
+    if (kp.use_kmers) {
+      const uint4* pc = reinterpret_cast<const uint4*>(L.pool.kmer8 + size_t(c) * size_t(nk16) * 16);
+      const uint4* pg = reinterpret_cast<const uint4*>(L.pool.kmer8 + size_t(g) * size_t(nk16) * 16);
+      uint32_t dot = 0, ovf = 0;
+      for (int v = lane; v < nk16; v += 32) {
+        uint4 a = __ldg(pc + v);
+        uint4 b = __ldcs(pg + v);
+        uint32_t m0 = __vminu4(a.x, b.x), m1 = __vminu4(a.y, b.y), m2 = __vminu4(a.z, b.z), m3 = __vminu4(a.w, b.w);
+        dot = __dp4a(m0, 0x01010101u, dot);
+        dot = __dp4a(m1, 0x01010101u, dot);
+        dot = __dp4a(m2, 0x01010101u, dot);
+        dot = __dp4a(m3, 0x01010101u, dot);
+        ovf |= __vcmpeq4(m0, 0xffffffffu) | __vcmpeq4(m1, 0xffffffffu) | __vcmpeq4(m2, 0xffffffffu) |
+               __vcmpeq4(m3, 0xffffffffu);
+      }
+      dot = __reduce_add_sync(FULL, dot);
+      ovf = __reduce_or_sync(FULL, ovf);
+      if (ovf) {
+        // A k-mer saturated in both profiles: recompute the exact u16 dot
+        // (src/nwalign.rs:1270-1277). Each window of the raw contributes 1 when its
+        // rank among equal windows of the raw is below the center's count.
+        uint32_t exact = 0;
+        for (int p = lane; p + k <= lg; p += 32) {
+          int x = 0;
+          for (int q = 0; q < k; ++q) x = x * 4 + int(sg[p + q]) - 1;
+          uint32_t rank = 0, cnt = 0;
+          for (int p2 = 0; p2 < p; ++p2) {
+            int y = 0;
+            for (int q = 0; q < k; ++q) y = y * 4 + int(sg[p2 + q]) - 1;
+            rank += (y == x);
+          }
+          for (int p2 = 0; p2 + k <= lc; ++p2) {
+            int y = 0;
+            for (int q = 0; q < k; ++q) y = y * 4 + int(sc[p2 + q]) - 1;
+            cnt += (y == x);
+          }
+          exact += rank < cnt ? 1u : 0u;
+        }
+        dot = __reduce_add_sync(FULL, exact);
+      }
+      const int minl = lc < lg ? lc : lg;
+      kdist = 1.0 - double(dot) / double(minl - k + 1);
+    }
+    const bool shroud = kp.use_kmers && kdist > T.cutoff;
+    if (shroud) {
+      if (lane == 0) {
+        L.pool.res_lambda[g] = 0.0;
+        L.pool.res_ham[g] = 0xffffffffu;
+        L.pool.res_status[g] = ST_SHROUDED;
+      }
+      continue;
+    }
+    // Positional mismatch scan: ordered-k-mer distance (src/kmers.rs:314-328, equal
+    // windows <=> equal k-mer codes for ACGT input) and the gapless Hamming count.
+    const int minl = lc < lg ? lc : lg;
+    const bool want_kod = kp.use_kmers && kp.gapless && lc == lg;
+    uint32_t ham = 0;
+    if (want_kod || kp.band == 0) {
+      const int klen = lc - (k - 1);
+      const uint32_t kmask = (k >= 32) ? 0xffffffffu : ((1u << k) - 1u);
+      uint32_t eq = 0;
+      uint32_t cur = mismatch_word(sc, sg, 0, minl, lane);
+      for (int b = 0; b < minl; b += 32) {
+        uint32_t nxt = mismatch_word(sc, sg, b + 32, minl, lane);
+        ham += __popc(cur);
+        if (want_kod) {
+          unsigned long long both = (static_cast<unsigned long long>(nxt) << 32) | cur;
+          int j = b + lane;
+          bool ok = j < klen && ((uint32_t(both >> lane) & kmask) == 0u);
+          eq += __popc(__ballot_sync(FULL, ok));
+        }
+        cur = nxt;
+      }
+      if (want_kod && klen > 0) kodist = 1.0 - double(eq) / double(klen);
+    }
+    const bool gapless = kp.band == 0 || (kp.gapless && fabs(kodist - kdist) < DBL_EPSILON);
+    if (!gapless) {
+      const bool use_homo = kp.homo_gap != kp.gap && kp.homo_gap <= 0;
+      const bool vec = kp.vectorized && lc <= 3500 && lg <= 3500 && !use_homo;
+      if (lane == 0) {
+        if (vec) {
+          uint32_t slot = atomicAdd(&L.queue_counts[0], 1u);
+          L.queue_vec[slot] = item;
+        } else {
+          uint32_t slot = atomicAdd(&L.queue_counts[1], 1u);
+          L.queue_rm[slot] = item;
+        }
+      }
+      continue;
+    }
+    // Gapless: raw position p aligns to center position p while p < len(center).
+    for (int p = lane; p < lg; p += 32) {
+      unsigned r = sg[p];
+      unsigned code = (p < lc) ? (unsigned(sc[p]) - 1u) * 4u + (r - 1u) : (r - 1u) * 5u;
+      const bool valid = r >= 1u && r <= 4u && (p >= lc || (sc[p] >= 1 && sc[p] <= 4));
+      tcode[p] = uint8_t(valid ? code : 255u);
+    }
+    __syncwarp();
+    const uint8_t* qg = L.pool.qual ? L.pool.qual + L.pool.off[g] : nullptr;
+    bool bad = build_fidx(lane, tcode, qg, lg, kp.ncol, kp.use_quals, fidx);
+    __syncwarp();
+    double lam = bad ? 0.0 : lambda_chain(lane, fidx, lg, err_s);
+    if (lane == 0) {
+      if (bad) atomicOr(L.err_word, DERR_LAMBDA);
+      L.pool.res_lambda[g] = lam;
+      L.pool.res_ham[g] = ham;
+      L.pool.res_status[g] = uint8_t(ST_ALIGNED | (AM_GAPLESS << 2));
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K4: vectorized (compressed anti-diagonal) aligner
+// ---------------------------------------------------------------------------
+struct VecSmem {
+  uint8_t* s1;
+  uint8_t* s2;
+  int16_t* rows;  // 3 x ncol rolling slots
+  int16_t* diag;
+  uint8_t* prow;
+  uint8_t* stage;
+  uint8_t* tcode;
+  uint16_t* fidx;
+};
+
+__device__ __forceinline__ int sat_sub1(int v) { return v == 0 ? 0 : v - 1; }
+
+// Aligns s1_in (center) against s2_in (raw). On success fills tcode[] for the
+// raw positions and returns the substitution count in *ham. With dbg0/dbg1 the
+// alignment rows are written in traceback (reversed) order for the tests.
+__device__ bool vec_align_warp(int lane, const uint8_t* g1, int l1, const uint8_t* g2, int l2, int16_t match,
+                               int16_t mismatch, int16_t gap, int16_t egp, int band_in, const VecSmem& S,
+                               uint8_t* pmat, int ncol_bound, int nrow_bound, uint32_t* ham_out,
+                               uint32_t* err_word, uint8_t* dbg0, uint8_t* dbg1, uint32_t* dbg_len) {
+  const bool swap = l1 > l2;
+  const int len1 = swap ? l2 : l1, len2 = swap ? l1 : l2;
+  {
+    const uint8_t* a = swap ? g2 : g1;
+    const uint8_t* b = swap ? g1 : g2;
+    for (int p = lane; p < len1; p += 32) S.s1[p] = a[p];
+    for (int p = lane; p < len2; p += 32) S.s2[p] = b[p];
+  }
+  const int band = band_in < 0 ? len2 : band_in;
+  const int start_col = 1 + (min(band, len1) + 1) / 2;
+  const int ncol = 2 + start_col + min(band + len2 - len1, len2) / 2;
+  const int nrow = len1 + len2 + 1;
+  if (ncol > ncol_bound || nrow > nrow_bound || ncol < 4) {
+    if (lane == 0) atomicOr(err_word, DERR_GEOMETRY);
+    return false;
+  }
+  int16_t min_score = min(min(min(mismatch, gap), match), int16_t(0));
+  const int16_t fill = int16_t(uint16_t(uint16_t(0x8000u) - uint16_t(min_score)));
+  const int lfl = 1 + min(band, len1);
+  const int tfl = 1 + min(band + len2 - len1, len2);
+  for (int c = lane; c < 3 * ncol; c += 32) S.rows[c] = 0;
+  for (int c = lane; c < ncol; c += 32) S.diag[c] = 0;
+  for (int c = lane; c < 2 * ncol; c += 32) pmat[c] = 0;
+  __syncwarp();
+  auto left_col = [&](int row) { int a = start_col - 1, b = (row - 1) / 2; return a > b ? a - b : 0; };
+  auto top_col = [&](int row) { return start_col + row / 2; };
+  if (lane == 0) {
+    for (int row = 0; row < 2; ++row) {
+      int16_t* slot = S.rows + row * ncol;
+      slot[0] = fill;
+      slot[1] = fill;
+      slot[ncol - 2] = fill;
+      slot[ncol - 1] = fill;
+      if (row == 0) {
+        slot[start_col] = 0;
+      } else {
+        if (row < lfl) {
+          slot[left_col(row)] = egp;
+          pmat[row * ncol + left_col(row)] = 3;
+        }
+        if (row < tfl) {
+          slot[top_col(row)] = egp;
+          pmat[row * ncol + top_col(row)] = 2;
+        }
+      }
+    }
+    pmat[start_col] = 0;
+  }
+  __syncwarp();
+  int16_t row_free = egp;
+  int sl0 = 0, sl1 = 1, sl2 = 2;
+  int col_min = start_col, col_max = start_col, i_max = 0, j_min = 0;
+  bool even = true, recalc_left = false, recalc_right = false;
+  const int band_mod2 = band % 2;
+  const int top_limit = min(band + len2 - len1, len2);
+  const int full_band = band + len2 - len1;
+  for (int row = 2; row <= len1 + len2; ++row) {
+    if (!(col_max >= col_min && col_max < ncol)) {
+      if (lane == 0) atomicOr(err_word, DERR_BAND_RANGE);
+      return false;
+    }
+    const int n = col_max - col_min + 1;
+    row_free = sadd16(row_free, egp);
+    int16_t* cur = S.rows + sl2 * ncol;
+    const int16_t* prev = S.rows + sl1 * ncol;
+    const int16_t* prev2 = S.rows + sl0 * ncol;
+    for (int c = lane; c < ncol; c += 32) S.prow[c] = 0;
+    __syncwarp();
+    if (lane == 0) {
+      cur[0] = fill;
+      cur[1] = fill;
+      cur[ncol - 2] = fill;
+      cur[ncol - 1] = fill;
+      if (row < lfl) {
+        cur[left_col(row)] = row_free;
+        S.prow[left_col(row)] = 3;
+      }
+      if (row < tfl) {
+        cur[top_col(row)] = row_free;
+        S.prow[top_col(row)] = 2;
+      }
+    }
+    __syncwarp();
+    {
+      int k_lo = i_max - len1 + 1;
+      k_lo = k_lo < 0 ? 0 : (k_lo > n ? n : k_lo);
+      int k_hi = min(i_max + 1, len2 - j_min);
+      k_hi = k_hi < 0 ? 0 : (k_hi > n ? n : k_hi);
+      k_hi = max(k_hi, k_lo);
+      for (int k = lane; k < n; k += 32) {
+        const int c = col_min + k;
+        int16_t v;
+        if (k < k_lo || k >= k_hi) v = fill;
+        else v = (S.s1[i_max - k] == S.s2[j_min + k]) ? match : mismatch;
+        S.diag[c] = sadd16(prev2[c], v);
+      }
+    }
+    __syncwarp();
+    const int eo = even ? 1 : 0;
+    const int left_off = col_min - eo, up_off = col_min + 1 - eo;
+    if (left_off < 0 || up_off + n > ncol) {
+      if (lane == 0) atomicOr(err_word, DERR_BAND_RANGE);
+      return false;
+    }
+    for (int k = lane; k < n; k += 32) {
+      int16_t l = sadd16(prev[left_off + k], gap);
+      int16_t u = sadd16(prev[up_off + k], gap);
+      int16_t dg = S.diag[col_min + k];
+      int16_t e;
+      uint8_t pe;
+      if (swap) {
+        if (l >= u) { e = l; pe = 2; } else { e = u; pe = 3; }
+      } else {
+        if (u >= l) { e = u; pe = 3; } else { e = l; pe = 2; }
+      }
+      if (dg > e) { e = dg; pe = 1; }
+      cur[col_min + k] = e;
+      S.prow[col_min + k] = pe;
+    }
+    __syncwarp();
+    if (row == min(band, len1)) {
+      col_min = sat_sub1(col_min);
+      i_max += 1;
+      j_min -= 1;
+    }
+    if (row == min(band + len2 - len1, len2)) col_max += 1;
+    if (egp > gap) {
+      if (recalc_left && lane == 0) {
+        int16_t d_free = sadd16(prev[left_off], egp);
+        int16_t cv = cur[col_min];
+        uint8_t pc = S.prow[col_min];
+        if (d_free > cv) {
+          cur[col_min] = d_free;
+          S.prow[col_min] = 2;
+        } else if (!(d_free != cv || (!swap && pc != 1) || (swap && pc == 2))) {
+          S.prow[col_min] = 2;
+        }
+      }
+      if (i_max == len1 - 1) recalc_left = true;
+      if (recalc_right) {
+        const int idx = up_off + col_max - col_min;
+        if (idx < 0 || idx >= ncol || col_max >= ncol) {
+          if (lane == 0) atomicOr(err_word, DERR_BAND_RANGE);
+          return false;
+        }
+        if (lane == 0) {
+          int16_t d_free = sadd16(prev[idx], egp);
+          int16_t cv = cur[col_max];
+          uint8_t pc = S.prow[col_max];
+          if (d_free > cv) {
+            cur[col_max] = d_free;
+            S.prow[col_max] = 3;
+          } else if (!(d_free != cv || (!swap && pc == 3) || (swap && pc != 1))) {
+            S.prow[col_max] = 3;
+          }
+        }
+      }
+      if ((row + 1) / 2 + col_max - start_col == len2) recalc_right = true;
+    }
+    __syncwarp();
+    for (int c = lane; c < ncol; c += 32) pmat[size_t(row) * ncol + c] = S.prow[c];
+    if (row < band && row < len1) {
+      if (even) col_min = sat_sub1(col_min);
+      i_max += 1;
+    } else if (i_max < len1 - 1) {
+      if (band_mod2 == 0) {
+        if (even) j_min += 1;
+        else i_max += 1;
+      } else if (even) {
+        col_min = sat_sub1(col_min);
+        i_max += 1;
+      } else {
+        col_min += 1;
+        j_min += 1;
+      }
+    } else {
+      if (!even) col_min += 1;
+      j_min += 1;
+    }
+    if (row < top_limit) {
+      if (!even) col_max += 1;
+    } else if ((row + 1) / 2 + col_max - start_col < len2) {
+      if (full_band % 2 == 0) {
+        if (even) col_max = sat_sub1(col_max);
+        else col_max += 1;
+      }
+    } else if (even) {
+      col_max = sat_sub1(col_max);
+    }
+    const int t = sl0;
+    sl0 = sl1;
+    sl1 = sl2;
+    sl2 = t;
+    even = !even;
+  }
+  __syncwarp();
+  // Traceback (src/nwalign.rs:1090-1139), staged through shared memory in row chunks.
+  const uint8_t* raw = swap ? S.s1 : S.s2;
+  const int lraw = swap ? len1 : len2;
+  for (int p = lane; p < lraw; p += 32) S.tcode[p] = uint8_t((unsigned(raw[p]) - 1u) * 5u);
+  const int rps = kStageBytes / ncol;
+  int slo = 0x7fffffff;
+  int i = len1, j = len2;
+  uint32_t ham = 0, alen = 0;
+  bool ok = true;
+  __syncwarp();
+  while (i > 0 || j > 0) {
+    const int cs = 2 * start_col + j - i;
+    if (cs < 0) { ok = false; break; }
+    const int col = cs / 2;
+    const int r = i + j;
+    if (r < slo) {
+      const int nlo = max(0, r - rps + 1);
+      __syncwarp();
+      const int nb = (r - nlo + 1) * ncol;
+      const uint8_t* src = pmat + size_t(nlo) * ncol;
+      for (int x = lane; x < nb; x += 32) S.stage[x] = src[x];
+      __syncwarp();
+      slo = nlo;
+    }
+    const uint8_t v = S.stage[(r - slo) * ncol + col];
+    if (v == 1 && i > 0 && j > 0) {
+      const uint8_t a = S.s1[i - 1], b = S.s2[j - 1];
+      const int rp = swap ? i - 1 : j - 1;
+      const uint8_t cn = swap ? b : a, rn = swap ? a : b;
+      if (lane == 0) S.tcode[rp] = uint8_t((unsigned(cn) - 1u) * 4u + (unsigned(rn) - 1u));
+      ham += (a != b) ? 1u : 0u;
+      if (dbg0 && lane == 0) {
+        dbg0[alen] = swap ? b : a;
+        dbg1[alen] = swap ? a : b;
+      }
+      --i;
+      --j;
+    } else if (v == 2 && j > 0) {
+      if (dbg0 && lane == 0) {
+        dbg0[alen] = swap ? S.s2[j - 1] : uint8_t('-');
+        dbg1[alen] = swap ? uint8_t('-') : S.s2[j - 1];
+      }
+      --j;
+    } else if (v == 3 && i > 0) {
+      if (dbg0 && lane == 0) {
+        dbg0[alen] = swap ? uint8_t('-') : S.s1[i - 1];
+        dbg1[alen] = swap ? S.s1[i - 1] : uint8_t('-');
+      }
+      --i;
+    } else {
+      ok = false;
+      break;
+    }
+    ++alen;
+  }
+  __syncwarp();
+  if (!ok) {
+    if (lane == 0) atomicOr(err_word, DERR_TRACEBACK);
+    return false;
+  }
+  if (dbg_len && lane == 0) *dbg_len = alen;
+  *ham_out = ham;
+  return true;
+}
+
+__device__ VecSmem carve_vec(unsigned char* base, int lmax, int ncol_bound) {
+  VecSmem S;
+  size_t o = 0;
+  auto take = [&](size_t bytes) { unsigned char* p = base + o; o += (bytes + 15) & ~size_t(15); return p; };
+  S.s1 = take(lmax);
+  S.s2 = take(lmax);
+  S.rows = reinterpret_cast<int16_t*>(take(size_t(3) * ncol_bound * 2));
+  S.diag = reinterpret_cast<int16_t*>(take(size_t(ncol_bound) * 2));
+  S.prow = take(ncol_bound);
+  S.stage = take(kStageBytes);
+  S.tcode = take(lmax);
+  S.fidx = reinterpret_cast<uint16_t*>(take(size_t(lmax) * 2));
+  return S;
+}
+
+
+// ---------------------------------------------------------------------------
+// K5: row-major ends-free / homopolymer aligner as an anti-diagonal wavefront
+// ---------------------------------------------------------------------------
+struct RmSmem {
+  uint8_t* s1;
+  uint8_t* s2;
+  uint8_t* h1;
+  uint8_t* h2;
+  uint32_t* stage;  // 32 diagonals x 2K words
+  uint8_t* tcode;
+  uint16_t* fidx;
+};
+
+__device__ void homo_mask_warp(int lane, const uint8_t* s, int n, uint8_t* m) {
+  // p lies in a run of >= 3 equal bases (src/nwalign.rs:211-227)
+  for (int p = lane; p < n; p += 32) {
+    bool in = false;
+    if (p >= 2 && s[p - 2] == s[p] && s[p - 1] == s[p]) in = true;
+    if (p >= 1 && p + 1 < n && s[p - 1] == s[p] && s[p + 1] == s[p]) in = true;
+    if (p + 2 < n && s[p + 1] == s[p] && s[p + 2] == s[p]) in = true;
+    m[p] = in ? 1 : 0;
+  }
+}
+
+template <int K>
+__device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8_t* g2, int len2, int match,
+                              int mismatch, int gap, int homo_gap, int band, bool homo, const RmSmem& S,
+                              uint32_t* pscr, uint32_t* ham_out, uint32_t* err_word, uint8_t* dbg0, uint8_t* dbg1,
+                              uint32_t* dbg_len) {
+  for (int p = lane; p < len1; p += 32) S.s1[p] = g1[p];
+  for (int p = lane; p < len2; p += 32) S.s2[p] = g2[p];
+  __syncwarp();
+  if (homo) {
+    homo_mask_warp(lane, S.s1, len1, S.h1);
+    homo_mask_warp(lane, S.s2, len2, S.h2);
+  }
+  int lband, rband, o_lo, o_hi;
+  if (band >= 0) {
+    if (len2 > len1) { lband = band; rband = band + (len2 - len1); }
+    else if (len1 > len2) { lband = band + (len1 - len2); rband = band; }
+    else { lband = band; rband = band; }
+    o_lo = max(-lband, -len1);
+    o_hi = min(rband, len2);
+  } else {
+    lband = len1;
+    rband = len2;
+    o_lo = -len1;
+    o_hi = len2;
+  }
+  const int W = o_hi - o_lo + 1;
+  const int P = (W + 1) / 2;
+  if (P > 32 * K) {
+    if (lane == 0) atomicOr(err_word, DERR_UNSUPPORTED);
+    return false;
+  }
+  __syncwarp();
+  int ve[K], vo[K];
+#pragma unroll
+  for (int m = 0; m < K; ++m) { ve[m] = kNegSentinel; vo[m] = kNegSentinel; }
+  uint32_t pw[2 * K];
+#pragma unroll
+  for (int m = 0; m < 2 * K; ++m) pw[m] = 0;
+  const int tmax = len1 + len2;
+  for (int t = 0; t <= tmax; ++t) {
+    const int par = (t - o_lo) & 1;
+#pragma unroll
+    for (int m = 0; m < K; ++m) {
+      const int q = lane + 32 * m;
+      const int o = o_lo + 2 * q + par;
+      int own = par ? vo[m] : ve[m];
+      int left_nb, up_nb;
+      if (par == 0) {
+        int a = __shfl_up_sync(FULL, vo[m], 1);
+        int a31 = (m > 0) ? __shfl_sync(FULL, vo[m > 0 ? m - 1 : 0], 31) : kNegSentinel;
+        left_nb = (lane == 0) ? a31 : a;
+        if (q == 0) left_nb = kNegSentinel;
+        up_nb = vo[m];
+      } else {
+        int b = __shfl_down_sync(FULL, ve[m], 1);
+        int b0 = (m + 1 < K) ? __shfl_sync(FULL, ve[m + 1 < K ? m + 1 : m], 0) : kNegSentinel;
+        up_nb = (lane == 31) ? b0 : b;
+        if (q + 1 >= P) up_nb = kNegSentinel;
+        left_nb = ve[m];
+      }
+      const int i = (t - o) >> 1, j = (t + o) >> 1;
+      int val, code = 0;
+      if (q >= P || o > o_hi) {
+        val = kNegSentinel;
+      } else if (i >= 1 && i <= len1 && j >= 1 && j <= len2) {
+        const int up = up_nb + ((j == len2) ? 0 : ((homo && S.h1[i - 1]) ? homo_gap : gap));
+        const int left = left_nb + ((i == len1) ? 0 : ((homo && S.h2[j - 1]) ? homo_gap : gap));
+        const int dg = own + (S.s1[i - 1] == S.s2[j - 1] ? match : mismatch);
+        if (up >= dg && up >= left) { val = up; code = 3; }
+        else if (left >= dg) { val = left; code = 2; }
+        else { val = dg; code = 1; }
+      } else if (i >= 0 && j >= 0 && i <= len1 && j <= len2) {
+        val = 0;  // row 0 / column 0 inside the band
+      } else {
+        val = kNegSentinel;
+      }
+      if (par) vo[m] = val;
+      else ve[m] = val;
+      const uint32_t b0w = __ballot_sync(FULL, code & 1);
+      const uint32_t b1w = __ballot_sync(FULL, (code >> 1) & 1);
+      if (lane == (t & 31)) {
+        pw[2 * m] = b0w;
+        pw[2 * m + 1] = b1w;
+      }
+    }
+    if ((t & 31) == 31 || t == tmax) {
+      const int base = t & ~31;
+      if (base + lane <= t) {
+        uint32_t* dst = pscr + size_t(base + lane) * (2 * K);
+#pragma unroll
+        for (int m = 0; m < 2 * K; ++m) dst[m] = pw[m];
+      }
+    }
+  }
+  __syncwarp();
+  // Traceback (src/nwalign.rs:234-273): row 0 moves left, column 0 moves up.
+  for (int p = lane; p < len2; p += 32) S.tcode[p] = uint8_t((unsigned(S.s2[p]) - 1u) * 5u);
+  int i = len1, j = len2, slo = 0x7fffffff;
+  uint32_t ham = 0, alen = 0;
+  bool ok = true;
+  __syncwarp();
+  while (i > 0 || j > 0) {
+    int v;
+    if (i == 0) v = 2;
+    else if (j == 0) v = 3;
+    else {
+      const int o = j - i, t = i + j;
+      if (o < o_lo || o > o_hi) { ok = false; break; }
+      if (t < slo) {
+        const int nlo = max(0, t - 31);
+        __syncwarp();
+        const int nw = (t - nlo + 1) * 2 * K;
+        const uint32_t* src = pscr + size_t(nlo) * (2 * K);
+        for (int x = lane; x < nw; x += 32) S.stage[x] = src[x];
+        __syncwarp();
+        slo = nlo;
+      }
+      const int q = (o - o_lo) >> 1, L = q & 31, m = q >> 5;
+      const uint32_t* w = S.stage + (t - slo) * (2 * K) + 2 * m;
+      v = int((w[0] >> L) & 1u) | (int((w[1] >> L) & 1u) << 1);
+    }
+    if (v == 1) {
+      const uint8_t a = S.s1[i - 1], b = S.s2[j - 1];
+      if (lane == 0) S.tcode[j - 1] = uint8_t((unsigned(a) - 1u) * 4u + (unsigned(b) - 1u));
+      ham += (a != b) ? 1u : 0u;
+      if (dbg0 && lane == 0) { dbg0[alen] = a; dbg1[alen] = b; }
+      --i;
+      --j;
+    } else if (v == 2) {
+      if (dbg0 && lane == 0) { dbg0[alen] = '-'; dbg1[alen] = S.s2[j - 1]; }
+      --j;
+    } else if (v == 3) {
+      if (dbg0 && lane == 0) { dbg0[alen] = S.s1[i - 1]; dbg1[alen] = '-'; }
+      --i;
+    } else {
+      ok = false;
+      break;
+    }
+    ++alen;
+  }
+  __syncwarp();
+  if (!ok) {
+    if (lane == 0) atomicOr(err_word, DERR_TRACEBACK);
+    return false;
+  }
+  if (dbg_len && lane == 0) *dbg_len = alen;
+  *ham_out = ham;
+  return true;
+}
+
+__device__ RmSmem carve_rm(unsigned char* base, int lmax, int kbound) {
+  RmSmem S;
+  size_t o = 0;
+  auto take = [&](size_t bytes) { unsigned char* p = base + o; o += (bytes + 15) & ~size_t(15); return p; };
+  S.s1 = take(lmax);
+  S.s2 = take(lmax);
+  S.h1 = take(lmax);
+  S.h2 = take(lmax);
+  S.stage = reinterpret_cast<uint32_t*>(take(size_t(32) * 2 * kbound * 4));
+  S.tcode = take(lmax);
+  S.fidx = reinterpret_cast<uint16_t*>(take(size_t(lmax) * 2));
+  return S;
+}
+
+
+__device__ bool rm_dispatch(int lane, const uint8_t* g1, int len1, const uint8_t* g2, int len2, const KParams& kp,
+                            bool homo, int kbound, const RmSmem& S, uint32_t* pscr, uint32_t* ham, uint32_t* err_word,
+                            uint8_t* d0, uint8_t* d1, uint32_t* dl) {
+  int lband, rband, o_lo, o_hi;
+  if (kp.band >= 0) {
+    lband = kp.band + (len1 > len2 ? len1 - len2 : 0);
+    rband = kp.band + (len2 > len1 ? len2 - len1 : 0);
+    o_lo = max(-lband, -len1);
+    o_hi = min(rband, len2);
+  } else {
+    o_lo = -len1;
+    o_hi = len2;
+  }
+  const int P = (o_hi - o_lo + 2) / 2;
+  const int need = (P + 31) / 32;
+  if (need > kbound) {
+    if (lane == 0) atomicOr(err_word, DERR_UNSUPPORTED);
+    return false;
+  }
+#define RM_CASE(KK)                                                                                                  \
+  if (need <= KK)                                                                                                    \
+    return rm_align_warp<KK>(lane, g1, len1, g2, len2, kp.match, kp.mismatch, kp.gap, kp.homo_gap, kp.band, homo, S, \
+                             pscr, ham, err_word, d0, d1, dl);
+  RM_CASE(1)
+  RM_CASE(2)
+  RM_CASE(4)
+  RM_CASE(8)
+  RM_CASE(16)
+#undef RM_CASE
+  if (lane == 0) atomicOr(err_word, DERR_UNSUPPORTED);
+  return false;
+}
+
+// ---------------------------------------------------------------------------
+// Persistent NW kernels over the queues filled by k_screen
+// ---------------------------------------------------------------------------
+template <bool VEC>
+__global__ void __launch_bounds__(kNwWarps * 32) k_nw(CompareLaunch L) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const KParams& kp = L.kp;
+  double* err_s = reinterpret_cast<double*>(smem_raw);
+  const int nerr = 16 * kp.ncol;
+  for (int t = threadIdx.x; t < nerr; t += blockDim.x) err_s[t] = L.pool.err[t];
+  const size_t err_bytes = err_smem_bytes(kp.ncol);
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int gw = blockIdx.x * kNwWarps + wib;
+  const int kb = rm_kbound(L.geom.rm_pairs);
+  __syncthreads();
+  VecSmem VS;
+  RmSmem RS;
+  if (VEC) {
+    VS = carve_vec(smem_raw + err_bytes + size_t(wib) * nw_smem_per_warp_vec(L.geom), L.geom.lmax, L.geom.vec_ncol);
+  } else {
+    RS = carve_rm(smem_raw + err_bytes + size_t(wib) * nw_smem_per_warp_rm(L.geom), L.geom.lmax, kb);
+  }
+  const size_t scr_bytes = VEC ? L.geom.vec_scratch : L.geom.rm_scratch;
+  uint8_t* scratch = L.nw_scratch + size_t(gw) * scr_bytes;
+  const uint32_t* queue = VEC ? L.queue_vec : L.queue_rm;
+  uint32_t* taken = &L.queue_counts[VEC ? 2 : 3];
+  const uint32_t count = *(volatile uint32_t*)&L.queue_counts[VEC ? 0 : 1];
+  for (;;) {
+    uint32_t slot = 0;
+    if (lane == 0) slot = atomicAdd(taken, 1u);
+    slot = __shfl_sync(FULL, slot, 0);
+    if (slot >= count) break;
+    const uint32_t item = queue[slot];
+    const uint32_t t = find_task(L.task_prefix, L.ntask, item);
+    const TaskDev T = L.tasks[t];
+    const uint32_t g = T.base + (item - L.task_prefix[t]);
+    const uint32_t c = T.center;
+    const int lc = int(L.pool.len[c]), lg = int(L.pool.len[g]);
+    const uint8_t* sc = L.pool.seq + L.pool.off[c];
+    const uint8_t* sg = L.pool.seq + L.pool.off[g];
+    uint32_t ham = 0;
+    bool ok;
+    uint8_t* tcode;
+    uint16_t* fidx;
+    uint8_t method;
+    if (VEC) {
+      ok = vec_align_warp(lane, sc, lc, sg, lg, int16_t(kp.match), int16_t(kp.mismatch), int16_t(kp.gap), 0, kp.band,
+                          VS, scratch, L.geom.vec_ncol, L.geom.vec_nrow, &ham, L.err_word, nullptr, nullptr, nullptr);
+      tcode = VS.tcode;
+      fidx = VS.fidx;
+      method = AM_VECTORIZED;
+    } else {
+      const bool homo = kp.homo_gap != kp.gap && kp.homo_gap <= 0;
+      ok = rm_dispatch(lane, sc, lc, sg, lg, kp, homo, kb, RS, reinterpret_cast<uint32_t*>(scratch), &ham, L.err_word,
+                       nullptr, nullptr, nullptr);
+      tcode = RS.tcode;
+      fidx = RS.fidx;
+      method = homo ? AM_HOMO : AM_ENDSFREE;
+    }
+    double lam = 0.0;
+    if (ok) {
+      const uint8_t* qg = L.pool.qual ? L.pool.qual + L.pool.off[g] : nullptr;
+      bool bad = build_fidx(lane, tcode, qg, lg, kp.ncol, kp.use_quals, fidx);
+      __syncwarp();
+      if (bad) {
+        if (lane == 0) atomicOr(L.err_word, DERR_LAMBDA);
+      } else {
+        lam = lambda_chain(lane, fidx, lg, err_s);
+      }
+    }
+    if (lane == 0) {
+      L.pool.res_lambda[g] = lam;
+      L.pool.res_ham[g] = ok ? ham : 0xffffffffu;
+      L.pool.res_status[g] = uint8_t(ST_ALIGNED | (method << 2));
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K7: ordered store (one CTA per task)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_store(CompareLaunch L) {
+  __shared__ uint32_t warp_cnt[32];
+  __shared__ uint32_t ctr[TC_NCOUNTERS];
+  const uint32_t t = blockIdx.x;
+  const TaskDev T = L.tasks[t];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (threadIdx.x < TC_NCOUNTERS) ctr[threadIdx.x] = 0;
+  __syncthreads();
+  uint32_t c_scr = 0, c_al = 0, c_sh = 0, c_gl = 0, c_ve = 0, c_ho = 0, c_ef = 0;
+  uint32_t running = 0;
+  for (uint32_t b = 0; b < T.n; b += blockDim.x) {
+    const uint32_t r = b + threadIdx.x;
+    const bool valid = r < T.n;
+    bool store = false;
+    double lam = 0.0;
+    uint32_t ham = 0;
+    if (valid) {
+      const uint32_t g = T.base + r;
+      const uint8_t st = L.pool.res_status[g];
+      lam = L.pool.res_lambda[g];
+      ham = L.pool.res_ham[g];
+      const uint8_t outcome = st & 3u, meth = st >> 2;
+      c_scr += outcome != ST_SKIPPED;
+      c_al += outcome == ST_ALIGNED;
+      c_sh += outcome == ST_SHROUDED;
+      c_gl += meth == AM_GAPLESS;
+      c_ve += meth == AM_VECTORIZED;
+      c_ho += meth == AM_HOMO;
+      c_ef += meth == AM_ENDSFREE;
+      const double e = L.pool.e_minmax[g];
+      if (__dmul_rn(lam, T.total_reads) > e) {
+        store = true;
+        const double ne = __dmul_rn(lam, double(T.center_reads));
+        if (ne > e) L.pool.e_minmax[g] = ne;
+      }
+      if (g == T.center) L.task_self[t] = lam;
+    }
+    const uint32_t bal = __ballot_sync(FULL, store);
+    if (lane == 0) warp_cnt[w] = __popc(bal);
+    __syncthreads();
+    if (w == 0) {
+      uint32_t v = lane < nw ? warp_cnt[lane] : 0u;
+      uint32_t incl = v;
+      for (int d = 1; d < 32; d <<= 1) {
+        uint32_t y = __shfl_up_sync(FULL, incl, d);
+        if (lane >= d) incl += y;
+      }
+      if (lane < nw) warp_cnt[lane] = incl - v;
+      const uint32_t tot = __shfl_sync(FULL, incl, 31);
+      if (lane == 0) ctr[TC_STORED] = tot;  // this chunk's total, read below
+    }
+    __syncthreads();
+    if (store) {
+      const uint32_t pos = running + warp_cnt[w] + __popc(bal & ((1u << lane) - 1u));
+      const uint32_t o = T.out_off + pos;
+      L.comp_index[o] = r;
+      L.comp_lambda[o] = lam;
+      L.comp_ham[o] = (ham == 0xffffffffu) ? 0u : ham;
+    }
+    running += ctr[TC_STORED];
+    __syncthreads();
+  }
+  c_scr = __reduce_add_sync(FULL, c_scr);
+  c_al = __reduce_add_sync(FULL, c_al);
+  c_sh = __reduce_add_sync(FULL, c_sh);
+  c_gl = __reduce_add_sync(FULL, c_gl);
+  c_ve = __reduce_add_sync(FULL, c_ve);
+  c_ho = __reduce_add_sync(FULL, c_ho);
+  c_ef = __reduce_add_sync(FULL, c_ef);
+  if (lane == 0) {
+    atomicAdd(&ctr[TC_SCREENED], c_scr);
+    atomicAdd(&ctr[TC_ALIGNED], c_al);
+    atomicAdd(&ctr[TC_SHROUD], c_sh);
+    atomicAdd(&ctr[TC_GAPLESS], c_gl);
+    atomicAdd(&ctr[TC_VECTORIZED], c_ve);
+    atomicAdd(&ctr[TC_HOMO], c_ho);
+    atomicAdd(&ctr[TC_ENDSFREE], c_ef);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ctr[TC_STORED] = running;
+    L.task_nstored[t] = running;
+  }
+  __syncthreads();
+  if (threadIdx.x < TC_NCOUNTERS) L.task_counters[size_t(t) * TC_NCOUNTERS + threadIdx.x] = ctr[threadIdx.x];
+}
+
+static int g_sm_count = 0;
+static int sm_count() {
+  if (g_sm_count == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sm_count <= 0) g_sm_count = 148;
+  }
+  return g_sm_count;
+}
+
+void launch_compare(const CompareLaunch& L, cudaStream_t st, cudaEvent_t* ev) {
+  if (L.total_items == 0) return;
+  const size_t err_bytes = err_smem_bytes(L.kp.ncol);
+  const size_t screen_smem = err_bytes + size_t(kScreenWarps) * screen_smem_per_warp(L.pool.maxlen);
+  if (screen_smem > 48 * 1024)
+    cudaFuncSetAttribute(k_screen, cudaFuncAttributeMaxDynamicSharedMemorySize, int(screen_smem));
+  const int sms = sm_count();
+  uint32_t blocks = (L.total_items + kScreenWarps - 1) / kScreenWarps;
+  const uint32_t cap = uint32_t(sms) * 8u;
+  if (blocks > cap) blocks = cap;
+  if (ev) cudaEventRecord(ev[0], st);
+  k_screen<<<blocks, kScreenWarps * 32, screen_smem, st>>>(L);
+  if (ev) cudaEventRecord(ev[1], st);
+  const int nw_blocks = L.geom.nwarps / kNwWarps;
+  const size_t vsm = err_bytes + size_t(kNwWarps) * nw_smem_per_warp_vec(L.geom);
+  if (vsm > 48 * 1024) cudaFuncSetAttribute(k_nw<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(vsm));
+  k_nw<true><<<nw_blocks, kNwWarps * 32, vsm, st>>>(L);
+  if (ev) cudaEventRecord(ev[2], st);
+  const size_t rsm = err_bytes + size_t(kNwWarps) * nw_smem_per_warp_rm(L.geom);
+  if (rsm > 48 * 1024) cudaFuncSetAttribute(k_nw<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(rsm));
+  k_nw<false><<<nw_blocks, kNwWarps * 32, rsm, st>>>(L);
+  if (ev) cudaEventRecord(ev[3], st);
+  if (L.do_store) k_store<<<L.ntask, 1024, 0, st>>>(L);
+  if (ev) cudaEventRecord(ev[4], st);
+}
+
+// ---------------------------------------------------------------------------
+// Alignment-only debug kernel (parity tests): one warp per pair.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kNwWarps * 32) k_align_debug(int which, const uint8_t* s1cat, const uint32_t* off1,
+                                                              const uint32_t* len1, const uint8_t* s2cat,
+                                                              const uint32_t* off2, const uint32_t* len2,
+                                                              uint32_t npairs, KParams kp, int end_gap, NwGeom geom,
+                                                              uint8_t* scratch, uint8_t* al0, uint8_t* al1,
+                                                              const uint32_t* aloff, uint32_t* alen, uint32_t* err_word) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t pair = blockIdx.x * kNwWarps + wib;
+  if (pair >= npairs) return;
+  const size_t scr = which == 0 ? geom.vec_scratch : geom.rm_scratch;
+  uint8_t* my_scr = scratch + size_t(pair) * scr;
+  uint32_t ham = 0;
+  const uint8_t* a = s1cat + off1[pair];
+  const uint8_t* b = s2cat + off2[pair];
+  if (which == 0) {
+    VecSmem S = carve_vec(smem_raw + size_t(wib) * nw_smem_per_warp_vec(geom), geom.lmax, geom.vec_ncol);
+    vec_align_warp(lane, a, int(len1[pair]), b, int(len2[pair]), int16_t(kp.match), int16_t(kp.mismatch),
+                   int16_t(kp.gap), int16_t(end_gap), kp.band, S, my_scr, geom.vec_ncol, geom.vec_nrow, &ham, err_word,
+                   al0 + aloff[pair], al1 + aloff[pair], alen + pair);
+  } else {
+    const int kb = rm_kbound(geom.rm_pairs);
+    RmSmem S = carve_rm(smem_raw + size_t(wib) * nw_smem_per_warp_rm(geom), geom.lmax, kb);
+    rm_dispatch(lane, a, int(len1[pair]), b, int(len2[pair]), kp, which == 1, kb, S, reinterpret_cast<uint32_t*>(my_scr),
+                &ham, err_word, al0 + aloff[pair], al1 + aloff[pair], alen + pair);
+  }
+}
+
+void launch_align_debug(int which, const uint8_t* s1cat, const uint32_t* off1, const uint32_t* len1,
+                        const uint8_t* s2cat, const uint32_t* off2, const uint32_t* len2, uint32_t npairs, KParams kp,
+                        int end_gap, const NwGeom& geom, uint8_t* scratch, uint8_t* al0, uint8_t* al1,
+                        const uint32_t* aloff, uint32_t* alen, uint32_t* err_word, cudaStream_t st) {
+  if (npairs == 0) return;
+  const size_t per = which == 0 ? nw_smem_per_warp_vec(geom) : nw_smem_per_warp_rm(geom);
+  const size_t smem = per * kNwWarps;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_align_debug, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  const uint32_t blocks = (npairs + kNwWarps - 1) / kNwWarps;
+  k_align_debug<<<blocks, kNwWarps * 32, smem, st>>>(which, s1cat, off1, len1, s2cat, off2, len2, npairs, kp, end_gap,
+                                                     geom, scratch, al0, al1, aloff, alen, err_word);
+}
+
+}  // namespace dgpu

@@ -1,0 +1,382 @@
+"""B200 (sm_100a) implementation of the compare step of dada2-rs `dada`.
+
+The compare kernels and the clustering loop live in libdada2_b200.so (C ABI:
+include/dada2_b200.h). This module is a thin Python mirror of the reference's
+interface for the path:
+
+* :class:`CompareContext` -- uniques resident on one GPU; ``compare`` is the map
+  of ``b_compare_parallel`` (src/cluster.rs:279-330) and ``b_compare_parallel``
+  is map + store (src/cluster.rs:239-423).
+* :func:`dada_uniques` -- one sample end to end (src/dada.rs:225-592).
+* :func:`dada_uniques_batch` -- many independent samples in one pass.
+
+Sequences are ASCII (A/C/G/T/U, either case); qualities are per-position Phred
+SUMS over the reads of each unique, as the reference's derep produces them.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from ._lib import (AlignParamsC, CountersC, DadaOutC, DadaParamsC, DgpuError, InvalidInput, KernelStatsC,
+                   check, device_count, lib, ptr)
+
+__all__ = ["AlignParams", "DadaParams", "CompareContext", "dada_uniques", "dada_uniques_batch",
+           "ResidentBatch", "PackedBatch", "align_pairs", "stats_reset", "stats_timing", "stats_read",
+           "DgpuError", "InvalidInput", "device_count", "METHOD_NAMES", "KERNEL_NAMES"]
+
+KERNEL_NAMES = ["profiles", "screen", "nw_vectorized", "nw_rowmajor", "store"]
+
+METHOD_NAMES = {0: "none", 1: "gapless", 2: "vectorized", 3: "homo", 4: "endsfree"}
+COUNTER_KEYS = ["nalign", "compare_calls", "cmp_scanned", "screened", "aligned", "stored",
+                "gapless", "vectorized", "homo", "endsfree", "shuffle_calls", "shuffle_moves",
+                "nshroud"]
+
+
+@dataclass
+class AlignParams:
+    """AlignParams (src/nwalign.rs:63-90); defaults from src/main.rs:4393-4433."""
+    match_score: int = 5
+    mismatch: int = -4
+    gap_p: int = -8
+    homo_gap_p: int = -8
+    use_kmers: bool = True
+    kdist_cutoff: float = 0.42
+    kmer_size: int = 5
+    band: int = 16
+    vectorized: bool = True
+    gapless: bool = True
+
+    def c(self) -> AlignParamsC:
+        return AlignParamsC(int(self.match_score), int(self.mismatch), int(self.gap_p),
+                            int(self.homo_gap_p), int(bool(self.use_kmers)), float(self.kdist_cutoff),
+                            int(self.kmer_size), int(self.band), int(bool(self.vectorized)),
+                            int(bool(self.gapless)))
+
+
+@dataclass
+class DadaParams:
+    """The DadaParams fields the clustering loop reads (src/dada.rs:54-101)."""
+    align: AlignParams = field(default_factory=AlignParams)
+    omega_a: float = 1e-40
+    omega_p: float = 1e-4
+    omega_c: float = 1e-40
+    detect_singletons: bool = False
+    max_clust: int = 0
+    min_fold: float = 1.0
+    min_hamming: int = 1
+    min_abund: int = 1
+    use_quals: bool = True
+    greedy: bool = True
+    host_threads: int = 0
+
+    def c(self) -> DadaParamsC:
+        return DadaParamsC(self.align.c(), float(self.omega_a), float(self.omega_p), float(self.omega_c),
+                           int(bool(self.detect_singletons)), int(self.max_clust), float(self.min_fold),
+                           int(self.min_hamming), int(self.min_abund), int(bool(self.use_quals)),
+                           int(bool(self.greedy)), int(self.host_threads))
+
+
+def _counters(c: CountersC) -> dict:
+    return {n: int(getattr(c, n)) for n, _ in CountersC._fields_}
+
+
+class CompareContext:
+    """Uniques resident on one device; the drop-in for b_compare_parallel.
+
+    ``seqs`` are arrays of codes 1..4; ``quals`` rounded mean Phred (u8) or None.
+    """
+
+    def __init__(self, params: AlignParams, err: np.ndarray, ncol: int, use_quals: bool = True,
+                 device: int = 0):
+        self.h = C.c_void_p()
+        self._err = np.ascontiguousarray(err, np.float64)
+        pc = params.c()
+        check(lib().dgpu_ctx_create(device, C.byref(pc), ptr(self._err), int(ncol), int(bool(use_quals)),
+                                    C.byref(self.h)))
+        self.n = 0
+
+    def upload(self, seqs, reads, quals=None):
+        seqs = [np.ascontiguousarray(s, np.uint8) for s in seqs]
+        lens = np.array([len(s) for s in seqs], np.uint32)
+        offs = np.concatenate([[0], np.cumsum(lens)[:-1]]).astype(np.uint32)
+        cat = np.concatenate(seqs).astype(np.uint8)
+        qcat = None if quals is None else np.concatenate(
+            [np.ascontiguousarray(q, np.uint8) for q in quals]).astype(np.uint8)
+        rd = np.ascontiguousarray(reads, np.uint32)
+        check(lib().dgpu_upload_raws(self.h, len(seqs), ptr(cat), ptr(offs), ptr(lens), ptr(qcat), ptr(rd)))
+        self.n = len(seqs)
+
+    def set_locks(self, lock):
+        lk = np.ascontiguousarray(lock, np.uint8)
+        check(lib().dgpu_set_locks(self.h, ptr(lk)))
+
+    def reset_e_minmax(self):
+        check(lib().dgpu_reset_e_minmax(self.h))
+
+    def e_minmax(self) -> np.ndarray:
+        out = np.zeros(self.n, np.float64)
+        check(lib().dgpu_get_e_minmax(self.h, ptr(out)))
+        return out
+
+    def compare(self, center: int, kdist_cutoff: float, greedy: bool = True):
+        """The map: per-raw (lambda, hamming or UINT32_MAX, skipped)."""
+        lam = np.zeros(self.n, np.float64)
+        ham = np.zeros(self.n, np.uint32)
+        skp = np.zeros(self.n, np.uint8)
+        cnt = CountersC()
+        check(lib().dgpu_compare(self.h, int(center), float(kdist_cutoff), int(bool(greedy)), ptr(lam), ptr(ham),
+                                 ptr(skp), C.byref(cnt)))
+        return lam, ham, skp.astype(bool), _counters(cnt)
+
+    def b_compare_parallel(self, center: int, cluster_i: int, kdist_cutoff: float, greedy: bool = True):
+        """Map + store: the stored comparisons in ascending raw order."""
+        idx = np.zeros(self.n, np.uint32)
+        lam = np.zeros(self.n, np.float64)
+        ham = np.zeros(self.n, np.uint32)
+        ns = C.c_int(0)
+        self_ = C.c_double(0.0)
+        cnt = CountersC()
+        check(lib().dgpu_compare_store(self.h, int(center), int(cluster_i), float(kdist_cutoff), int(bool(greedy)),
+                                       ptr(idx), ptr(lam), ptr(ham), C.byref(ns), C.byref(self_), C.byref(cnt)))
+        k = ns.value
+        return {"index": idx[:k].copy(), "lambda": lam[:k].copy(), "hamming": ham[:k].copy(),
+                "self": self_.value, "counters": _counters(cnt)}
+
+    def close(self):
+        if self.h:
+            lib().dgpu_ctx_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _pack(seqs, abund, quals=None, prior=None):
+    enc = [s.encode("ascii") if isinstance(s, str) else bytes(s) for s in seqs]
+    lens = np.array([len(s) for s in enc], np.uint32)
+    offs = np.concatenate([[0], np.cumsum(lens)[:-1]]).astype(np.uint32)
+    cat = np.frombuffer(b"".join(enc), np.uint8).copy()
+    ab = np.ascontiguousarray(abund, np.uint32)
+    qcat = None
+    if quals is not None:
+        qcat = np.concatenate([np.ascontiguousarray(q, np.uint32) for q in quals]).astype(np.uint32)
+    pr = None if prior is None else np.ascontiguousarray(prior, np.uint8)
+    return cat, offs, lens, ab, qcat, pr
+
+
+def _read_result(h) -> dict:
+    sizes = np.zeros(4, np.int64)
+    check(lib().dgpu_result_sizes(h, ptr(sizes)))
+    ncl, nraw, nmem, nseq = (int(x) for x in sizes)
+    a = {
+        "cl_reads": np.zeros(ncl, np.uint32), "cl_birth_type": np.zeros(ncl, np.int32),
+        "cl_birth_from": np.zeros(ncl, np.uint32), "cl_birth_pval": np.zeros(ncl, np.float64),
+        "cl_birth_fold": np.zeros(ncl, np.float64), "cl_birth_e": np.zeros(ncl, np.float64),
+        "cl_birth_hamming": np.zeros(ncl, np.uint32), "cl_seq_off": np.zeros(ncl + 1, np.uint32),
+        "cl_seq": np.zeros(max(nseq, 1), np.uint8), "cl_mem_off": np.zeros(ncl + 1, np.uint32),
+        "mem_raw": np.zeros(max(nmem, 1), np.uint32), "mem_hamming": np.zeros(max(nmem, 1), np.uint32),
+        "mem_lambda": np.zeros(max(nmem, 1), np.float64), "mem_pval": np.zeros(max(nmem, 1), np.float64),
+        "map": np.zeros(max(nraw, 1), np.int32), "pvals": np.zeros(max(nraw, 1), np.float64),
+        "counters": np.zeros(16, np.uint64), "times": np.zeros(4, np.float64),
+    }
+    o = DadaOutC(*[ptr(a[n]) for n, _ in DadaOutC._fields_])
+    check(lib().dgpu_result_fill(h, C.byref(o)))
+    res = {"nclust": ncl, "nraw": nraw, **a}
+    res["map"] = a["map"][:nraw]
+    res["pvals"] = a["pvals"][:nraw]
+    res["counters"] = {k: int(v) for k, v in zip(COUNTER_KEYS, a["counters"])}
+    res["clusters"] = []
+    for ci in range(ncl):
+        s0, s1 = a["cl_seq_off"][ci], a["cl_seq_off"][ci + 1]
+        m0, m1 = a["cl_mem_off"][ci], a["cl_mem_off"][ci + 1]
+        res["clusters"].append({
+            "sequence": a["cl_seq"][s0:s1].copy(), "reads": int(a["cl_reads"][ci]),
+            "members": a["mem_raw"][m0:m1].copy(), "hammings": a["mem_hamming"][m0:m1].copy(),
+            "lambdas": a["mem_lambda"][m0:m1].copy(), "pvals": a["mem_pval"][m0:m1].copy(),
+            "birth_type": int(a["cl_birth_type"][ci]), "birth_from": int(a["cl_birth_from"][ci]),
+            "birth_pval": float(a["cl_birth_pval"][ci]), "birth_fold": float(a["cl_birth_fold"][ci]),
+            "birth_e": float(a["cl_birth_e"][ci]), "birth_hamming": int(a["cl_birth_hamming"][ci]),
+        })
+    return res
+
+
+def dada_uniques(seqs, abund, err, ncol, params: DadaParams | None = None, quals=None, prior=None,
+                 device: int = 0) -> dict:
+    """Denoise one sample on the GPU (src/dada.rs:225-592)."""
+    params = params or DadaParams()
+    cat, offs, lens, ab, qcat, pr = _pack(seqs, abund, quals, prior)
+    err = np.ascontiguousarray(err, np.float64)
+    pc = params.c()
+    h = C.c_void_p()
+    check(lib().dgpu_dada(device, C.byref(pc), len(lens), ptr(cat), ptr(offs), ptr(lens), ptr(ab), ptr(pr),
+                          ptr(qcat), ptr(err), int(ncol), C.byref(h)))
+    try:
+        return _read_result(h)
+    finally:
+        lib().dgpu_result_free(h)
+
+
+class PackedBatch:
+    """Host buffers of a batch, packed once so repeated runs time only the call."""
+
+    def __init__(self, samples, with_quals=True):
+        seqs, ab, qs = [], [], []
+        starts = [0]
+        for s in samples:
+            seqs.extend(s.seqs)
+            ab.append(np.asarray(s.abund, np.uint32))
+            if with_quals:
+                qs.extend(s.quals)
+            starts.append(starts[-1] + len(s.seqs))
+        self.cat, self.offs, self.lens, self.ab, self.qcat, self.pr = _pack(
+            seqs, np.concatenate(ab), qs if with_quals else None, None)
+        self.starts = np.array(starts, np.uint32)
+        self.nsamples = len(samples)
+        self.h2d_bytes = int(self.cat.nbytes + self.offs.nbytes + self.lens.nbytes + self.ab.nbytes +
+                             (self.qcat.nbytes if self.qcat is not None else 0) + self.starts.nbytes)
+
+
+def dada_uniques_batch(samples, err, ncol, params: DadaParams | None = None, device: int = 0,
+                       packed: PackedBatch | None = None, read_results: bool = True):
+    """Denoise many independent samples in one pass. ``samples`` are objects
+    with ``seqs``, ``abund`` and ``quals`` (sums) attributes."""
+    params = params or DadaParams()
+    pb = packed or PackedBatch(samples)
+    err = np.ascontiguousarray(err, np.float64)
+    pc = params.c()
+    hs = (C.c_void_p * pb.nsamples)()
+    check(lib().dgpu_dada_batch(device, C.byref(pc), pb.nsamples, ptr(pb.starts), ptr(pb.cat), ptr(pb.offs),
+                                ptr(pb.lens), ptr(pb.ab), ptr(pb.pr), ptr(pb.qcat), ptr(err), int(ncol),
+                                C.cast(hs, C.c_void_p)))
+    out = []
+    try:
+        for i in range(pb.nsamples):
+            out.append(_read_result(hs[i]) if read_results else None)
+    finally:
+        for i in range(pb.nsamples):
+            if hs[i]:
+                lib().dgpu_result_free(hs[i])
+    return out
+
+
+class ResidentBatch:
+    """Samples validated, encoded and uploaded once (inputs resident in HBM);
+    ``run`` executes the whole clustering loop and may be repeated."""
+
+    def __init__(self, samples, err, ncol, params: DadaParams | None = None, device: int = 0,
+                 packed: PackedBatch | None = None):
+        self.params = params or DadaParams()
+        self.pb = packed or PackedBatch(samples)
+        self._err = np.ascontiguousarray(err, np.float64)
+        pc = self.params.c()
+        self.h = C.c_void_p()
+        pb = self.pb
+        check(lib().dgpu_batch_prepare(device, C.byref(pc), pb.nsamples, ptr(pb.starts), ptr(pb.cat), ptr(pb.offs),
+                                       ptr(pb.lens), ptr(pb.ab), ptr(pb.pr), ptr(pb.qcat), ptr(self._err), int(ncol),
+                                       C.byref(self.h)))
+
+    def run(self, read_results: bool = True):
+        n = self.pb.nsamples
+        hs = (C.c_void_p * n)()
+        rc = lib().dgpu_batch_run(self.h, C.cast(hs, C.c_void_p))
+        out = []
+        try:
+            check(rc)
+            for i in range(n):
+                out.append(_read_result(hs[i]) if read_results else _read_counters(hs[i]))
+        finally:
+            for i in range(n):
+                if hs[i]:
+                    lib().dgpu_result_free(hs[i])
+        return out
+
+    def close(self):
+        if self.h:
+            lib().dgpu_batch_free(self.h)
+            self.h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _read_counters(h) -> dict:
+    cnt = np.zeros(16, np.uint64)
+    tm = np.zeros(4, np.float64)
+    o = DadaOutC(*[None] * len(DadaOutC._fields_))
+    o.counters = ptr(cnt)
+    o.times = ptr(tm)
+    check(lib().dgpu_result_fill(h, C.byref(o)))
+    sizes = np.zeros(4, np.int64)
+    check(lib().dgpu_result_sizes(h, ptr(sizes)))
+    return {"nclust": int(sizes[0]), "nraw": int(sizes[1]),
+            "counters": {k: int(v) for k, v in zip(COUNTER_KEYS, cnt)}, "times": tm}
+
+
+def stats_reset():
+    check(lib().dgpu_stats_reset())
+
+
+def stats_timing(enable: bool):
+    check(lib().dgpu_stats_timing(int(bool(enable))))
+
+
+def stats_latencies() -> np.ndarray:
+    """Per compare call latency (ms) since the last reset."""
+    n = lib().dgpu_stats_latencies(None, 0)
+    out = np.zeros(max(n, 1), np.float64)
+    n = lib().dgpu_stats_latencies(ptr(out), len(out))
+    return out[:n]
+
+
+def stats_read() -> dict:
+    s = KernelStatsC()
+    check(lib().dgpu_stats_read(C.byref(s)))
+    return {"launches": {k: int(s.launches[i]) for i, k in enumerate(KERNEL_NAMES)},
+            "ms": {k: float(s.ms[i]) for i, k in enumerate(KERNEL_NAMES)},
+            "rounds": int(s.rounds), "compares": int(s.compares), "screened": int(s.screened),
+            "screen_bytes": int(s.screen_bytes)}
+
+
+ALIGN_VECTORIZED, ALIGN_HOMO, ALIGN_ENDSFREE = 0, 1, 2
+
+
+def align_pairs(which: int, pairs, params: AlignParams | None = None, end_gap: int = 0, device: int = 0):
+    """Run one of the GPU aligners on (s1, s2) code arrays; returns (al0, al1) rows."""
+    params = params or AlignParams()
+    s1 = [np.ascontiguousarray(a, np.uint8) for a, _ in pairs]
+    s2 = [np.ascontiguousarray(b, np.uint8) for _, b in pairs]
+    l1 = np.array([len(s) for s in s1], np.uint32)
+    l2 = np.array([len(s) for s in s2], np.uint32)
+    o1 = np.concatenate([[0], np.cumsum(l1)[:-1]]).astype(np.uint32)
+    o2 = np.concatenate([[0], np.cumsum(l2)[:-1]]).astype(np.uint32)
+    cap = l1.astype(np.int64) + l2
+    ao = np.concatenate([[0], np.cumsum(cap)[:-1]]).astype(np.uint32)
+    a0 = np.zeros(int(cap.sum()) + 1, np.uint8)
+    a1 = np.zeros(int(cap.sum()) + 1, np.uint8)
+    alen = np.zeros(len(pairs), np.uint32)
+    c1, c2 = np.concatenate(s1), np.concatenate(s2)
+    pc = params.c()
+    check(lib().dgpu_align_debug(device, which, len(pairs), ptr(c1), ptr(o1), ptr(l1), ptr(c2), ptr(o2), ptr(l2),
+                                 C.byref(pc), int(end_gap), ptr(a0), ptr(a1), ptr(ao), ptr(alen)))
+    return [(a0[o:o + n].copy(), a1[o:o + n].copy()) for o, n in zip(ao, alen)]

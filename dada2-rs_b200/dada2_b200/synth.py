@@ -1,0 +1,252 @@
+"""Seeded synthetic amplicon samples with the shapes of the benchmark configs.
+
+No public dataset is named for these workloads and the reference's real
+datasets are not available, so every input is generated here, deterministically
+from ``seed = 1000 + config``:
+
+* true variants are uniform-random ACGT;
+* reads are drawn from the variants with the stated abundance law;
+* substitutions follow a 16 x nq transition-by-quality error matrix whose rows
+  are ``ref*4 + query`` (A=0..T=3) and whose columns are Phred Q, the layout the
+  compare step reads (error rate 10^(-Q/10), transitions twice as likely as
+  transversions, off-diagonals clamped to [1e-7, 0.25], diagonal = 1 - sum);
+* reads are dereplicated the way the reference's derep does it
+  (src/derep.rs:179-185): uniques by abundance descending, ties by sequence
+  ascending, with per-position integer Phred SUMS (u32).
+
+The same matrix is handed to the denoiser as its error model.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+NT = np.frombuffer(b"ACGT", np.uint8)
+# transitions A<->G and C<->T weigh 2, transversions 1 (per reference base)
+_W = np.array([[0, 1, 2, 1], [1, 0, 1, 2], [2, 1, 0, 1], [1, 2, 1, 0]], np.float64)
+
+
+@dataclass
+class Sample:
+    """One dereplicated sample: ASCII uniques, abundances and Phred sums."""
+    seqs: list
+    abund: np.ndarray
+    quals: list
+    nreads: int = 0
+    name: str = ""
+
+
+@dataclass
+class Workload:
+    config: int
+    name: str
+    samples: list
+    err: np.ndarray   # flat 16 x ncol, row-major
+    ncol: int
+    band: int = 16
+    homo_gap_p: int = -8
+    kmer_size: int = 5
+    notes: dict = field(default_factory=dict)
+
+
+def error_matrix(nq: int, floor: float = 0.0) -> np.ndarray:
+    """16 x nq matrix: err[(ref*4+qry), Q]."""
+    q = np.arange(nq, dtype=np.float64)
+    e = np.maximum(10.0 ** (-q / 10.0), floor)
+    m = np.zeros((16, nq))
+    for a in range(4):
+        off = np.clip(np.outer(_W[a] / 4.0, e), 1e-7, 0.25)
+        off[a] = 0.0
+        for b in range(4):
+            m[a * 4 + b] = off[b]
+        m[a * 4 + a] = 1.0 - off.sum(axis=0)
+    return m.reshape(-1)
+
+
+def _random_variants(rng, n, lengths):
+    return [rng.integers(0, 4, size=int(L)).astype(np.uint8) for L in lengths[:n]]
+
+
+def _apply_subs(rng, reads_codes, quals, errm, ncol):
+    """Substitute per position with probability 1 - err[diag, Q]; draw the
+    replacement base proportionally to the off-diagonal rates."""
+    n, L = reads_codes.shape
+    e = errm.reshape(16, ncol)
+    diag_rows = reads_codes.astype(np.int64) * 5  # row a*4+a
+    p_err = 1.0 - e[diag_rows, quals]
+    hit = rng.random((n, L)) < p_err
+    if not hit.any():
+        return reads_codes
+    ri, ci = np.nonzero(hit)
+    ref = reads_codes[ri, ci].astype(np.int64)
+    qv = quals[ri, ci]
+    w = np.stack([e[ref * 4 + b, qv] for b in range(4)], axis=1)
+    w[np.arange(len(ref)), ref] = 0.0
+    w /= w.sum(axis=1, keepdims=True)
+    u = rng.random(len(ref))[:, None]
+    newb = (u > np.cumsum(w, axis=1)).sum(axis=1)
+    out = reads_codes.copy()
+    out[ri, ci] = np.minimum(newb, 3).astype(np.uint8)
+    return out
+
+
+def _derep(seq_rows, qual_rows):
+    """Group identical reads: returns ASCII uniques sorted by (-count, seq)."""
+    keys = {}
+    counts = []
+    qsums = []
+    order = []
+    for s, q in zip(seq_rows, qual_rows):
+        k = s.tobytes()
+        j = keys.get(k)
+        if j is None:
+            keys[k] = len(counts)
+            counts.append(1)
+            qsums.append(q.astype(np.uint32).copy())
+            order.append(k)
+        else:
+            counts[j] += 1
+            qsums[j] += q
+    ascii_seqs = [NT[np.frombuffer(k, np.uint8)].tobytes().decode() for k in order]
+    idx = sorted(range(len(order)), key=lambda t: (-counts[t], ascii_seqs[t]))
+    return ([ascii_seqs[t] for t in idx], np.array([counts[t] for t in idx], np.uint32),
+            [qsums[t] for t in idx])
+
+
+def illumina_sample(rng, nvariants, nreads, L, errm, ncol, abund_exp=1.5, qhi=38, qlo=25,
+                    qsd=2.0, qmin=2, qmax=41, chunk=20000):
+    variants = _random_variants(rng, nvariants, [L] * nvariants)
+    w = np.arange(1, nvariants + 1, dtype=np.float64) ** (-abund_exp)
+    w /= w.sum()
+    vidx = rng.choice(nvariants, size=nreads, p=w)
+    prof = np.linspace(qhi, qlo, L)
+    vmat = np.stack(variants)
+    # reads may carry Q above the model's last column (the denoiser then extends
+    # the model by repeating that column, src/dada.rs:337-384); draw their
+    # errors from the un-truncated rate law
+    gen = error_matrix(qmax + 1) if qmax + 1 > ncol else errm
+    gcol = max(qmax + 1, ncol)
+    seq_rows, qual_rows = [], []
+    for lo in range(0, nreads, chunk):
+        hi = min(nreads, lo + chunk)
+        n = hi - lo
+        q = np.clip(np.rint(prof[None, :] + rng.normal(0.0, qsd, size=(n, L))), qmin, qmax).astype(np.int64)
+        codes = _apply_subs(rng, vmat[vidx[lo:hi]], q, gen, gcol)
+        seq_rows.extend(codes)
+        qual_rows.extend(q.astype(np.uint32))
+    seqs, abund, quals = _derep(seq_rows, qual_rows)
+    return Sample(seqs, abund, quals, nreads)
+
+
+def _homopolymer_mask(codes):
+    n = len(codes)
+    m = np.zeros(n, bool)
+    s = 0
+    while s < n:
+        e = s + 1
+        while e < n and codes[e] == codes[s]:
+            e += 1
+        if e - s >= 3:
+            m[s:e] = True
+        s = e
+    return m
+
+
+def pacbio_sample(rng, nvariants, nuniques, lmin, lmax, errm, ncol, sub_rate=2e-3, indel_rate=5e-3,
+                  qbins=(40, 50, 60, 70, 80, 93)):
+    lengths = rng.integers(lmin, lmax + 1, size=nvariants)
+    variants = _random_variants(rng, nvariants, lengths)
+    masks = [_homopolymer_mask(v) for v in variants]
+    w = np.arange(1, nvariants + 1, dtype=np.float64) ** (-1.0)
+    w /= w.sum()
+    qb = np.array(qbins)
+    seq_rows, qual_rows = {}, {}
+    uniques = set()
+    nreads = 0
+    while len(uniques) < nuniques:
+        v = int(rng.choice(nvariants, p=w))
+        base = variants[v]
+        L = len(base)
+        # homopolymer indels: inside runs of >= 3, a base is dropped or doubled
+        hit = (rng.random(L) < indel_rate) & masks[v]
+        ins = rng.random(L) < 0.5
+        codes = []
+        for t in range(L):
+            if not hit[t]:
+                codes.append(base[t])
+            elif ins[t]:
+                codes.extend((base[t], base[t]))  # run extended by one
+        codes = np.array(codes, np.uint8)
+        sub = rng.random(len(codes)) < sub_rate
+        if sub.any():
+            codes[sub] = (codes[sub] + rng.integers(1, 4, size=int(sub.sum()))) % 4
+        q = qb[rng.integers(0, len(qb), size=len(codes))].astype(np.uint32)
+        k = codes.tobytes()
+        nreads += 1
+        if k in seq_rows:
+            seq_rows[k][1] += 1
+            qual_rows[k] += q
+        else:
+            seq_rows[k] = [codes, 1]
+            qual_rows[k] = q.copy()
+            uniques.add(k)
+    keys = list(seq_rows.keys())
+    ascii_seqs = {k: NT[np.frombuffer(k, np.uint8)].tobytes().decode() for k in keys}
+    keys.sort(key=lambda k: (-seq_rows[k][1], ascii_seqs[k]))
+    return Sample([ascii_seqs[k] for k in keys], np.array([seq_rows[k][1] for k in keys], np.uint32),
+                  [qual_rows[k] for k in keys], nreads)
+
+
+def config0(seed: int = 1000) -> Workload:
+    """Plain single-sample Illumina: 20 variants x 250 nt, 20,000 reads, Zipf 1.5."""
+    rng = np.random.default_rng(seed)
+    ncol = 41
+    errm = error_matrix(ncol)
+    s = illumina_sample(rng, 20, 20000, 250, errm, ncol)
+    s.name = "config0"
+    return Workload(0, "plain single-sample Illumina (20 variants x 250 nt, 20k reads)", [s], errm, ncol)
+
+
+def config1(seed: int = 1001, nsamples: int = 40, umin: int = 500, umax: int = 30000) -> Workload:
+    """40 samples, uniques log-uniform in [500, 30000], 250/220 nt alternating,
+    50-400 variants each."""
+    rng = np.random.default_rng(seed)
+    ncol = 41
+    errm = error_matrix(ncol)
+    samples = []
+    for si in range(nsamples):
+        target = int(np.exp(rng.uniform(np.log(umin), np.log(umax))))
+        nvar = int(rng.integers(50, 401))
+        L = 250 if si % 2 == 0 else 220
+        # ~16% of reads carry an error at this quality profile and nearly all of
+        # those are unique, so size the read count to land near the target
+        nreads = max(int((target - nvar) / 0.155), 2 * nvar)
+        s = illumina_sample(rng, nvar, nreads, L, errm, ncol)
+        s.name = f"config1.s{si}"
+        samples.append(s)
+    return Workload(1, "batched 40-sample Illumina (250/220 nt, 500-30k uniques)", samples, errm, ncol)
+
+
+def config2(seed: int = 1002, nuniques: int = 5000) -> Workload:
+    """PacBio full-length 16S: 60 variants of 1400-1550 nt, indel-heavy."""
+    rng = np.random.default_rng(seed)
+    ncol = 94
+    errm = error_matrix(ncol, floor=1e-3)
+    s = pacbio_sample(rng, 60, nuniques, 1400, 1550, errm, ncol)
+    s.name = "config2"
+    return Workload(2, "PacBio full-length 16S (1400-1550 nt, band 32, homopolymer gap -1)", [s], errm,
+                    ncol, band=32, homo_gap_p=-1)
+
+
+def small_illumina(seed: int, nvariants=8, nreads=3000, L=150) -> Workload:
+    """A seconds-scale Illumina sample for parity tests."""
+    rng = np.random.default_rng(seed)
+    ncol = 41
+    errm = error_matrix(ncol)
+    s = illumina_sample(rng, nvariants, nreads, L, errm, ncol)
+    s.name = f"small{seed}"
+    return Workload(-1, "small Illumina parity case", [s], errm, ncol)
+
+
+CONFIGS = {0: config0, 1: config1, 2: config2}

@@ -1,0 +1,189 @@
+/*
+ * dada2_b200.h -- C ABI of the B200 (sm_100a) implementation of the compare step
+ * inside dada2-rs `dada` divisive clustering.
+ *
+ * Everything here is plain C: pointers, sizes and POD structs. Host buffers are
+ * owned by the caller; device memory is owned by a context or by the call that
+ * allocated it. Every function returns 0 on success or a negative DGPU_E_* code;
+ * dgpu_last_error() then describes the failure (per calling thread). No call
+ * traps or aborts on bad input; a device-side failure (for example an invalid
+ * traceback pointer, where the reference panics) is reported as DGPU_E_DEVICE.
+ *
+ * Reference interfaces replaced (paths are within HPCBio/dada2-rs 0.2.0):
+ *   dgpu_ctx_create      AlignParams + error matrix setup   src/nwalign.rs:63-90, src/dada.rs:54-101
+ *   dgpu_upload_raws     Raw::from_qual_sums + raw_assign_kmers
+ *                                                           src/containers.rs:128-137, src/kmers.rs:213-221
+ *   dgpu_compare         the per-raw map of b_compare_parallel
+ *                                                           src/cluster.rs:279-330
+ *   dgpu_compare_store   map + serial store of b_compare_parallel
+ *                                                           src/cluster.rs:239-423
+ *   dgpu_dada            dada_uniques (plain: one sample)   src/dada.rs:225-592
+ *   dgpu_dada_batch      many independent samples at once (the per-sample fan-out of
+ *                        for_each_sample_concurrent)        src/main.rs:4648-4697
+ *   dgpu_align_debug     the aligners alone (test entry)    src/nwalign.rs:336-1140
+ *
+ * Threading: a context is used by one host thread at a time. Calls that take no
+ * context are reentrant.
+ */
+#ifndef DADA2_B200_H
+#define DADA2_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DGPU_OK 0
+#define DGPU_E_INVALID (-1)     /* rejected input (same checks as dada_uniques_cached) */
+#define DGPU_E_CUDA (-2)        /* a CUDA runtime call failed */
+#define DGPU_E_DEVICE (-3)      /* a kernel reported an error flag */
+#define DGPU_E_UNSUPPORTED (-4) /* a parameter combination this build does not cover */
+#define DGPU_E_NOMEM (-5)
+
+/* AlignParams (src/nwalign.rs:63-90); booleans are 0/1. */
+typedef struct {
+  int32_t match_score, mismatch, gap_p, homo_gap_p;
+  int32_t use_kmers;
+  double kdist_cutoff;
+  int32_t kmer_size, band, vectorized, gapless;
+} dgpu_align_params;
+
+/* The DadaParams fields the clustering loop reads (src/dada.rs:54-101). */
+typedef struct {
+  dgpu_align_params align;
+  double omega_a, omega_p, omega_c;
+  int32_t detect_singletons, max_clust;
+  double min_fold;
+  uint32_t min_hamming, min_abund;
+  int32_t use_quals, greedy;
+  int32_t host_threads; /* threads for the host phases of dgpu_dada_batch; 0 = all cores */
+} dgpu_dada_params;
+
+/* Counters of one compare call (CompareTiming's denominators, src/cluster.rs:190-231). */
+typedef struct {
+  uint64_t screened, aligned, shrouded, stored;
+  uint64_t gapless, vectorized, homo, endsfree;
+} dgpu_counters;
+
+/* Output layout of dgpu_dada / dgpu_dada_batch results (all caller-allocated;
+ * sizes from dgpu_result_sizes). Cluster c's center sequence is
+ * cl_seq[cl_seq_off[c] .. cl_seq_off[c+1]) (codes 1..4); its members are
+ * mem_*[cl_mem_off[c] .. cl_mem_off[c+1]). map[r] = -1 when raw r was not
+ * corrected to any cluster (src/dada.rs:525-533). counters (16 slots):
+ * nalign, compare_calls, cmp_scanned (sum of nraw over compare calls),
+ * screened, aligned, stored, gapless, vectorized, homo, endsfree,
+ * shuffle_calls, shuffle_moves, nshroud. times (4 slots, seconds): compare,
+ * total, host phases, device wait. */
+typedef struct {
+  uint32_t* cl_reads;
+  int32_t* cl_birth_type;
+  uint32_t* cl_birth_from;
+  double* cl_birth_pval;
+  double* cl_birth_fold;
+  double* cl_birth_e;
+  uint32_t* cl_birth_hamming;
+  uint32_t* cl_seq_off;
+  uint8_t* cl_seq;
+  uint32_t* cl_mem_off;
+  uint32_t* mem_raw;
+  uint32_t* mem_hamming;
+  double* mem_lambda;
+  double* mem_pval;
+  int32_t* map;
+  double* pvals;
+  uint64_t* counters;
+  double* times;
+} dgpu_dada_out;
+
+typedef struct dgpu_ctx dgpu_ctx;
+typedef struct dgpu_result dgpu_result;
+typedef struct dgpu_batch dgpu_batch;
+
+/* Process-wide kernel accounting (for benchmarks). Index k: 0 profiles,
+ * 1 screen, 2 vectorized NW, 3 row-major NW, 4 store. ms[] is filled only
+ * while timing is enabled (CUDA events around each kernel on its stream).
+ * screen_bytes = algorithmic bytes of the screen: 4^k profile bytes per
+ * non-skipped compare plus 16 bytes of per-raw metadata per compare. */
+typedef struct {
+  uint64_t launches[5];
+  double ms[5];
+  uint64_t rounds, compares, screened, screen_bytes;
+} dgpu_kernel_stats;
+
+const char* dgpu_last_error(void);
+int dgpu_device_count(int* count);
+
+/* ---- compare-level drop-in (one pool of uniques resident on one device) ---- */
+int dgpu_ctx_create(int device, const dgpu_align_params* params, const double* err_mat, int ncol,
+                    int use_quals, dgpu_ctx** out);
+void dgpu_ctx_destroy(dgpu_ctx* ctx);
+/* seqs: concatenated codes 1..4 (A,C,G,T); quals: rounded mean Phred per
+ * position, same offsets, or NULL. Builds the k-mer profiles on the device. */
+int dgpu_upload_raws(dgpu_ctx* ctx, int nraw, const uint8_t* seqs, const uint32_t* offs,
+                     const uint32_t* lens, const uint8_t* quals, const uint32_t* reads);
+int dgpu_set_locks(dgpu_ctx* ctx, const uint8_t* lock);
+/* Reset every raw's running max expected abundance to -999 (B::new). */
+int dgpu_reset_e_minmax(dgpu_ctx* ctx);
+int dgpu_get_e_minmax(dgpu_ctx* ctx, double* out);
+/* The map: per raw lambda, hamming (UINT32_MAX = shrouded or skipped), skipped flag. */
+int dgpu_compare(dgpu_ctx* ctx, int center, double kdist_cutoff, int greedy, double* lambda_out,
+                 uint32_t* hamming_out, uint8_t* skipped_out, dgpu_counters* cnt);
+/* Map + store: comps with lambda*total_reads > e_minmax, ascending raw index,
+ * e_minmax updated on the device; self_out = the center's own lambda. */
+int dgpu_compare_store(dgpu_ctx* ctx, int center, int cluster_i, double kdist_cutoff, int greedy,
+                       uint32_t* comp_index, double* comp_lambda, uint32_t* comp_hamming,
+                       int* nstored, double* self_out, dgpu_counters* cnt);
+
+/* ---- full denoising ---- */
+/* One sample (ASCII uniques, per-position Phred SUMS or NULL). */
+int dgpu_dada(int device, const dgpu_dada_params* params, int nraw, const char* seqs,
+              const uint32_t* offs, const uint32_t* lens, const uint32_t* abund, const uint8_t* prior,
+              const uint32_t* qual_sums, const double* err_mat, int ncol, dgpu_result** out);
+/* Many independent samples in one pass: sample s owns uniques
+ * [sample_start[s], sample_start[s+1]) of the concatenated inputs. out[s]
+ * receives one result per sample. */
+int dgpu_dada_batch(int device, const dgpu_dada_params* params, int nsamples,
+                    const uint32_t* sample_start, const char* seqs, const uint32_t* offs,
+                    const uint32_t* lens, const uint32_t* abund, const uint8_t* prior,
+                    const uint32_t* qual_sums, const double* err_mat, int ncol, dgpu_result** out);
+/* The same work split in two: prepare validates, encodes and uploads the
+ * samples and builds their k-mer profiles (the inputs become resident in HBM);
+ * run executes the whole clustering loop on the resident inputs and may be
+ * called repeatedly (each run starts from a fresh partition). out needs
+ * nsamples slots. */
+int dgpu_batch_prepare(int device, const dgpu_dada_params* params, int nsamples,
+                       const uint32_t* sample_start, const char* seqs, const uint32_t* offs,
+                       const uint32_t* lens, const uint32_t* abund, const uint8_t* prior,
+                       const uint32_t* qual_sums, const double* err_mat, int ncol, dgpu_batch** out);
+int dgpu_batch_run(dgpu_batch* batch, dgpu_result** out);
+void dgpu_batch_free(dgpu_batch* batch);
+
+int dgpu_stats_reset(void);
+int dgpu_stats_timing(int enable);
+int dgpu_stats_read(dgpu_kernel_stats* out);
+/* Latency (ms) of each compare call since the last reset, from launch to the
+ * results being on the host; copies up to cap values, returns how many exist. */
+int dgpu_stats_latencies(double* out, int cap);
+
+/* sizes: [nclust, nraw, total members, total center-sequence bytes] */
+int dgpu_result_sizes(const dgpu_result* res, int64_t* sizes);
+int dgpu_result_fill(const dgpu_result* res, const dgpu_dada_out* out);
+void dgpu_result_free(dgpu_result* res);
+
+/* ---- aligners alone (test entry) ----
+ * which: 0 vectorized (compressed anti-diagonal i16, end_gap as given),
+ *        1 ends-free with homopolymer gaps, 2 ends-free i32.
+ * al0/al1 receive each pair's rows at al_off[p] (capacity len1+len2) in
+ * left-to-right order; al_len[p] their length. */
+int dgpu_align_debug(int device, int which, int npairs, const uint8_t* s1cat, const uint32_t* off1,
+                     const uint32_t* len1, const uint8_t* s2cat, const uint32_t* off2,
+                     const uint32_t* len2, const dgpu_align_params* params, int end_gap,
+                     uint8_t* al0, uint8_t* al1, const uint32_t* al_off, uint32_t* al_len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DADA2_B200_H */

@@ -1,0 +1,61 @@
+"""The C ABI library builds, loads without a GPU and exports every declared entry point."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "dada2_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER, encoding="utf-8").read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(dgpu_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_header_declares_the_boundary():
+    names = declared_symbols()
+    for required in ("dgpu_ctx_create", "dgpu_upload_raws", "dgpu_compare", "dgpu_compare_store",
+                     "dgpu_dada", "dgpu_dada_batch", "dgpu_ctx_destroy", "dgpu_last_error"):
+        assert required in names
+
+
+def test_library_exports_every_declared_symbol():
+    from dada2_b200 import _lib
+
+    if not os.path.exists(_lib.LIB_PATH):
+        import importlib.util
+
+        spec = importlib.util.spec_from_file_location("dgpu_build", os.path.join(ROOT, "dada2-rs_b200", "build.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        mod.build()
+    L = ctypes.CDLL(_lib.LIB_PATH)
+    missing = [n for n in declared_symbols() if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_errors_are_reported_without_a_device():
+    from dada2_b200 import _lib
+
+    L = _lib.lib()
+    n = ctypes.c_int(-1)
+    rc = L.dgpu_device_count(ctypes.byref(n))
+    assert rc in (0, _lib.DGPU_E_CUDA)
+    # a null argument is rejected before any CUDA call
+    rc = L.dgpu_result_sizes(None, None)
+    assert rc == _lib.DGPU_E_INVALID
+    assert b"null" in L.dgpu_last_error()
+
+
+def test_gpu_entry_points_fail_loudly_without_a_device():
+    import numpy as np
+
+    import dada2_b200 as D
+
+    if D.device_count() > 0:
+        pytest.skip("a GPU is present; covered by the gpu tests")
+    with pytest.raises(D.DgpuError):
+        D.dada_uniques(["ACGTACGTAC"], [3], np.full(16, 0.01), 1)

@@ -1,0 +1,271 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle.
+
+Integer outputs (alignments, hamming, membership, counters) must be identical;
+FP64 outputs (lambda, p-values, birth statistics) must be bit-identical -- the
+kernels restate the reference's ordered, separately-rounded arithmetic.
+"""
+import numpy as np
+import pytest
+
+import dada2_b200 as D
+from dada2_b200 import synth
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+MASK64 = (1 << 64) - 1
+
+
+def xorshift(x):
+    x ^= (x << 13) & MASK64
+    x ^= x >> 7
+    x ^= (x << 17) & MASK64
+    return x & MASK64
+
+
+def fuzz_pairs(fz):
+    """The reference's rolling-vs-full fuzz inputs (src/nwalign.rs:2873-2952)."""
+    state = fz["seed"]
+    out = []
+    for l1, l2 in fz["length_pairs"]:
+        for band in fz["bands"]:
+            for trial in range(fz["trials"]):
+                s1 = []
+                for _ in range(l1):
+                    state = xorshift(state)
+                    s1.append(1 + state % 4)
+                if trial == 0 and l1 == l2:
+                    s2 = list(s1)
+                else:
+                    v = list(s1[:min(l2, l1)]) if l2 <= l1 else list(s1)
+                    v = (v + [1] * l2)[:l2]
+                    for t in range(len(v)):
+                        state = xorshift(state)
+                        if state % 16 < trial:
+                            state = xorshift(state)
+                            v[t] = 1 + state % 4
+                    s2 = v
+                out.append((band, np.array(s1, np.uint8), np.array(s2, np.uint8)))
+    return out
+
+
+def test_vectorized_aligner_matches_oracle_on_reference_fuzz(refvec):
+    pairs = fuzz_pairs(refvec["rolling_fuzz"])
+    for egp in refvec["rolling_fuzz"]["end_gap_ps"]:
+        by_band = {}
+        for band, a, b in pairs:
+            by_band.setdefault(band, []).append((a, b))
+        n = 0
+        for band, ps in by_band.items():
+            got = D.align_pairs(D.ALIGN_VECTORIZED, ps, D.AlignParams(band=band), end_gap=egp)
+            for (a, b), (g0, g1) in zip(ps, got):
+                w0, w1 = O.align(O.ALIGN_VECTORIZED, a, b, end_gap=egp, band=band)
+                assert np.array_equal(g0, w0) and np.array_equal(g1, w1), (len(a), len(b), band, egp)
+                n += 1
+        assert n == len(pairs)
+
+
+def random_pairs(seed, n, lmin, lmax, indel=True):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        L = int(rng.integers(lmin, lmax + 1))
+        a = rng.integers(1, 5, size=L).astype(np.uint8)
+        b = list(a)
+        for _ in range(int(rng.integers(0, 6))):
+            p = int(rng.integers(0, len(b)))
+            op = int(rng.integers(0, 3 if indel else 1))
+            if op == 0:
+                b[p] = int(rng.integers(1, 5))
+            elif op == 1:
+                b.insert(p, b[p])  # homopolymer-style insertion
+            elif len(b) > 8:
+                b.pop(p)
+        out.append((a, np.array(b, np.uint8)))
+    return out
+
+
+@pytest.mark.parametrize("band", [-1, 0, 3, 16, 32])
+def test_rowmajor_aligners_match_oracle(band):
+    pairs = random_pairs(100 + band, 120, 20, 180)
+    for which, owhich, hg in ((D.ALIGN_HOMO, O.ALIGN_HOMO, -1), (D.ALIGN_ENDSFREE, O.ALIGN_ENDSFREE, -8)):
+        p = D.AlignParams(band=band, homo_gap_p=hg)
+        got = D.align_pairs(which, pairs, p)
+        for (a, b), (g0, g1) in zip(pairs, got):
+            w0, w1 = O.align(owhich, a, b, homo_gap=hg, band=band)
+            assert np.array_equal(g0, w0) and np.array_equal(g1, w1), (which, band, len(a), len(b))
+
+
+def test_homopolymer_dispatch_pair_on_gpu(refvec):
+    hd = refvec["homo_dispatch"]
+    s1, s2 = O.encode(hd["s1"]), O.encode(hd["s2"])
+    (g0, g1), = D.align_pairs(D.ALIGN_HOMO, [(s1, s2)], D.AlignParams(homo_gap_p=hd["homo_gap_p"]))
+    w0, w1 = O.align(O.ALIGN_HOMO, s1, s2, homo_gap=hd["homo_gap_p"], band=16)
+    assert np.array_equal(g0, w0) and np.array_equal(g1, w1)
+
+
+def pool(refvec):
+    pl = refvec["compare_pool"]
+    nxt = {"A": "C", "C": "G", "G": "T"}
+    seqs, reads = [], []
+    for n, r in pl["n_reads"]:
+        s = list(pl["base"])
+        for p in range(n):
+            idx = (p * pl["mut_mul"] + pl["mut_add"]) % len(s)
+            s[idx] = nxt.get(s[idx], "A")
+        seqs.append(O.encode("".join(s)))
+        reads.append(r)
+    return pl, seqs, reads
+
+
+def test_compare_pool_matches_oracle(refvec):
+    pl, seqs, reads = pool(refvec)
+    err = np.full(16 * pl["ncol"], pl["err_flat"])
+    for greedy in (False, True):
+        op = O.AlignParams(homo_gap_p=pl["homo_gap_p"], kdist_cutoff=pl["kdist_cutoff"], kmer_size=pl["k"],
+                           band=pl["band"])
+        sess = O.Session(seqs, reads, k=pl["k"], use_quals=False)
+        sess.set_center(0, pl["center"])
+        wl, wh, ws, _ = sess.compare_map(0, err, pl["ncol"], op, greedy=greedy)
+        want = sess.compare(0, err, pl["ncol"], op, greedy=greedy)
+        gp = D.AlignParams(homo_gap_p=pl["homo_gap_p"], kdist_cutoff=pl["kdist_cutoff"], kmer_size=pl["k"],
+                           band=pl["band"])
+        with D.CompareContext(gp, err, pl["ncol"], use_quals=False) as ctx:
+            ctx.upload(seqs, reads)
+            gl, gh, gs, gc = ctx.compare(pl["center"], pl["kdist_cutoff"], greedy=greedy)
+            assert gl.tobytes() == wl.tobytes()
+            assert np.array_equal(gh, wh) and np.array_equal(gs, ws)
+            got = ctx.b_compare_parallel(pl["center"], 0, pl["kdist_cutoff"], greedy=greedy)
+            assert np.array_equal(got["index"], want["index"])
+            assert got["lambda"].tobytes() == want["lambda"].tobytes()
+            assert np.array_equal(got["hamming"], want["hamming"])
+            assert got["self"] == want["self"]
+            c, w = got["counters"], want["counters"]
+            assert (c["screened"], c["aligned"], c["shrouded"], c["stored"]) == (
+                w["screened"], w["aligned"], w["nshroud"], w["stored"])
+            assert np.array_equal(ctx.e_minmax(), want["e_minmax"])
+
+
+def _rounded_quals(sample):
+    return [np.floor(np.asarray(q, np.float64) / a + 0.5).astype(np.uint8) for q, a in zip(sample.quals, sample.abund)]
+
+
+def _extend(err, ncol, quals):
+    """Repeat the last column up to the largest quality (src/dada.rs:337-384)."""
+    qmax = max(int(q.max()) for q in quals)
+    if qmax < ncol:
+        return err, ncol
+    m = np.asarray(err).reshape(16, ncol)
+    ext = np.concatenate([m, np.repeat(m[:, -1:], qmax + 1 - ncol, axis=1)], axis=1)
+    return ext.reshape(-1).copy(), qmax + 1
+
+
+@pytest.mark.parametrize("seed", [11, 12])
+def test_compare_many_centers_matches_oracle(seed):
+    w = synth.small_illumina(seed, nvariants=6, nreads=1500, L=120)
+    s = w.samples[0]
+    seqs = [O.encode(x) for x in s.seqs]
+    quals = _rounded_quals(s)
+    err, ncol = _extend(w.err, w.ncol, quals)
+    sess = O.Session(seqs, s.abund, quals=quals, k=5, use_quals=True)
+    with D.CompareContext(D.AlignParams(), err, ncol) as ctx:
+        ctx.upload(seqs, s.abund, quals=quals)
+        for center in (0, 1, 2, 5, len(seqs) // 2, len(seqs) - 1):
+            ci = sess.add_center(center)
+            for cutoff in (0.42, 1.0):
+                pa = O.AlignParams(kdist_cutoff=cutoff)
+                wl, wh, ws, wm = sess.compare_map(ci, err, ncol, pa, greedy=True)
+                gl, gh, gs, _ = ctx.compare(center, cutoff, greedy=True)
+                assert gl.tobytes() == wl.tobytes(), (center, cutoff)
+                assert np.array_equal(gh, wh) and np.array_equal(gs, ws)
+
+
+def assert_same_dada(got, want):
+    assert got["nclust"] == want["nclust"]
+    assert np.array_equal(got["map"], want["map"])
+    assert got["pvals"].tobytes() == want["pvals"].tobytes()
+    for k in ("nalign", "nshroud", "compare_calls", "cmp_scanned", "screened", "aligned", "stored",
+              "gapless", "vectorized", "homo", "endsfree", "shuffle_calls", "shuffle_moves"):
+        assert got["counters"][k] == want["counters"][k], k
+    for g, w in zip(got["clusters"], want["clusters"]):
+        assert np.array_equal(g["sequence"], w["sequence"])
+        assert g["reads"] == w["reads"]
+        assert np.array_equal(g["members"], w["members"])
+        assert np.array_equal(g["hammings"], w["hammings"])
+        assert g["lambdas"].tobytes() == w["lambdas"].tobytes()
+        assert g["pvals"].tobytes() == w["pvals"].tobytes()
+        for k in ("birth_type", "birth_from", "birth_hamming"):
+            assert g[k] == w[k]
+        for k in ("birth_pval", "birth_fold", "birth_e"):
+            assert np.float64(g[k]).tobytes() == np.float64(w[k]).tobytes(), k
+
+
+@pytest.mark.parametrize("seed", [21, 22, 23])
+def test_dada_small_matches_oracle(seed):
+    w = synth.small_illumina(seed)
+    s = w.samples[0]
+    want = O.dada(s.seqs, s.abund, w.err, w.ncol, O.DadaParams(nthreads=4), quals=s.quals)
+    got = D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, D.DadaParams(), quals=s.quals)
+    assert want["nclust"] > 3
+    assert_same_dada(got, want)
+
+
+def test_dada_config0_matches_oracle():
+    w = synth.config0()
+    s = w.samples[0]
+    want = O.dada(s.seqs, s.abund, w.err, w.ncol, O.DadaParams(nthreads=8), quals=s.quals)
+    got = D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, D.DadaParams(), quals=s.quals)
+    assert_same_dada(got, want)
+
+
+def test_dada_batch_matches_per_sample_oracle():
+    ws = [synth.small_illumina(30 + i, nvariants=4 + i, nreads=800 + 300 * i, L=100 + 20 * (i % 3)) for i in range(5)]
+    err, ncol = ws[0].err, ws[0].ncol
+    samples = [w.samples[0] for w in ws]
+    got = D.dada_uniques_batch(samples, err, ncol, D.DadaParams(host_threads=3))
+    for s, g in zip(samples, got):
+        want = O.dada(s.seqs, s.abund, err, ncol, O.DadaParams(nthreads=4), quals=s.quals)
+        assert_same_dada(g, want)
+
+
+def test_dada_homopolymer_long_reads_matches_oracle():
+    w = synth.config2(seed=77, nuniques=120)
+    s = w.samples[0]
+    op = O.DadaParams(align=O.AlignParams(band=32, homo_gap_p=-1), nthreads=8)
+    dp = D.DadaParams(align=D.AlignParams(band=32, homo_gap_p=-1))
+    want = O.dada(s.seqs, s.abund, w.err, w.ncol, op, quals=s.quals)
+    got = D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, dp, quals=s.quals)
+    assert want["counters"]["homo"] > 0
+    assert_same_dada(got, want)
+
+
+@pytest.mark.parametrize("variant", ["band0", "no_kmers", "no_quals", "no_greedy", "unbanded"])
+def test_dada_parameter_variants_match_oracle(variant):
+    w = synth.small_illumina(41, nvariants=5, nreads=1200, L=90)
+    s = w.samples[0]
+    oa, da = O.AlignParams(), D.AlignParams()
+    okw, dkw = {}, {}
+    quals = s.quals
+    if variant == "band0":
+        oa.band = da.band = 0
+    elif variant == "no_kmers":
+        oa.use_kmers = da.use_kmers = False
+    elif variant == "no_quals":
+        quals = None
+    elif variant == "no_greedy":
+        okw["greedy"] = dkw["greedy"] = False
+    elif variant == "unbanded":
+        oa.band = da.band = -1
+    want = O.dada(s.seqs, s.abund, w.err, w.ncol, O.DadaParams(align=oa, nthreads=4, **okw), quals=quals)
+    got = D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, D.DadaParams(align=da, **dkw), quals=quals)
+    assert_same_dada(got, want)
+
+
+def test_invalid_inputs_are_rejected_like_the_reference():
+    err = np.full(16 * 41, 0.01)
+    with pytest.raises(D.InvalidInput, match="non-ACGT"):
+        D.dada_uniques(["ACGTNACGTA", "ACGTACGTAA"], [3, 2], err, 41)
+    with pytest.raises(D.InvalidInput, match="longer than the k-mer"):
+        D.dada_uniques(["ACGT", "ACGTACGTAA"], [3, 2], err, 41)
+    with pytest.raises(D.InvalidInput):
+        D.dada_uniques([], [], err, 41)
