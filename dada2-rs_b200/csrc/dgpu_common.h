@@ -80,6 +80,7 @@ struct NwGeom {
 constexpr int kScreenWarps = 8;   // warps per screen CTA
 constexpr int kNwWarps = 4;       // warps per NW CTA
 constexpr int kStageBytes = 4096; // traceback staging per warp
+constexpr int kStoreSpan = 8192;  // raws per store CTA (its own output segment)
 
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
 __host__ __device__ inline size_t err_smem_bytes(int ncol) { return align16(size_t(16) * size_t(ncol) * 8); }
@@ -99,6 +100,11 @@ __host__ __device__ inline size_t nw_smem_per_warp_rm(const NwGeom& g) {
   return align16(g.lmax) * 4 + align16(size_t(32) * 2 * rm_kbound(g.rm_pairs) * 4) + align16(g.lmax) +
          align16(size_t(g.lmax) * 2);
 }
+// The align kernel carves either layout from the same per-warp region.
+__host__ __device__ inline size_t align_smem_per_warp(const NwGeom& g) {
+  const size_t a = nw_smem_per_warp_vec(g), b = nw_smem_per_warp_rm(g);
+  return a > b ? a : b;
+}
 
 // ---- launchers (dgpu_kernels.cu) ----
 void launch_profiles(const uint8_t* seq, const uint32_t* off, const uint32_t* len, uint32_t nraw,
@@ -112,9 +118,10 @@ struct CompareLaunch {
   const uint32_t* task_prefix;
   uint32_t ntask;
   uint32_t total_items;
-  uint32_t* queue_vec;      // nraw capacity
+  uint32_t* queue_vec;      // nraw capacity each
   uint32_t* queue_rm;
-  uint32_t* queue_counts;   // [2]
+  uint32_t* queue_pass;
+  uint32_t* queue_counts;   // [pushed vec, pushed rm, taken vec, taken rm, pushed pass]
   uint8_t* nw_scratch;      // nwarps * max(vec_scratch, rm_scratch)
   NwGeom geom;
   uint32_t* err_word;
@@ -122,13 +129,17 @@ struct CompareLaunch {
   uint32_t* comp_index;
   double* comp_lambda;
   uint32_t* comp_ham;
-  uint32_t* task_counters;  // ntask * TC_NCOUNTERS
-  uint32_t* task_nstored;   // ntask
   double* task_self;        // ntask
+  // store CTAs: CTA b covers raws [store_chunk[b]*kStoreSpan, +kStoreSpan) of
+  // task store_task[b]; blk_counters[b] = its counters, TC_STORED its count
+  const uint32_t* store_task;
+  const uint32_t* store_chunk;
+  uint32_t* blk_counters;
+  uint32_t nstore_blocks;
   int do_store;
 };
-// ev (optional): 5 events recorded before the screen and after screen, vectorized NW,
-// row-major NW and store, for per-kernel device times.
+// ev (optional): 4 events recorded before the screen and after screen, align
+// and store, for per-kernel device times.
 void launch_compare(const CompareLaunch& L, cudaStream_t st, cudaEvent_t* ev = nullptr);
 
 // Alignment-only entry used by the parity tests: emits al0/al1 strings.

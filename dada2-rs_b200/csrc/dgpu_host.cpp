@@ -11,6 +11,7 @@
 #include <cmath>
 #include <condition_variable>
 #include <cstring>
+#include <deque>
 #include <functional>
 #include <limits>
 #include <mutex>
@@ -135,19 +136,22 @@ struct Pool {
   NwGeom geom{};
   int sms = 148;
   DBuf<uint8_t> seq, qual, kmer8, lock, status;
-  DBuf<uint32_t> off, len, reads, ham, queue_vec, queue_rm, queue_counts, err_word;
+  DBuf<uint32_t> off, len, reads, ham, queue_vec, queue_rm, queue_pass, queue_counts, err_word;
   DBuf<double> e_minmax, err, lambda;
   DBuf<uint8_t> scratch;
   DBuf<TaskDev> tasks;
   DBuf<uint32_t> task_prefix;
-  HBuf<uint32_t> comp_index, comp_ham, task_counters, task_nstored;
+  HBuf<uint32_t> comp_index, comp_ham, blk_counters;
   HBuf<double> comp_lambda, task_self;
   HBuf<TaskDev> task_stage;
-  HBuf<uint32_t> prefix_stage;
+  HBuf<uint32_t> prefix_stage, store_stage;  // prefix; then (task, chunk) per store CTA
+  DBuf<uint32_t> store_map;
+  std::vector<uint32_t> task_blk0;  // first store CTA of each task in the latest launch
+  uint32_t nblk_cap = 0;
   HBuf<uint8_t> lock_host;  // pinned host copy of every lock flag
   bool has_qual = false;
   uint32_t ntask_cap = 0;
-  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
   ~Pool() {
     for (auto& e : ev)
@@ -202,7 +206,8 @@ struct Pool {
     TRY(e_minmax.alloc(n));
     TRY(queue_vec.alloc(n));
     TRY(queue_rm.alloc(n));
-    TRY(queue_counts.alloc(4));
+    TRY(queue_pass.alloc(n));
+    TRY(queue_counts.alloc(8));
     TRY(err_word.alloc(1));
     TRY(err.alloc(size_t(16) * kp.ncol));
     TRY(kmer8.alloc(kp.use_kmers ? size_t(n) * nk : 1));
@@ -253,9 +258,11 @@ struct Pool {
     int64_t W = kp.band < 0 ? int64_t(2 * lmax + 1) : std::min<int64_t>(2 * bb + diff + 1, 2 * int64_t(lmax) + 1);
     geom.rm_pairs = int32_t(std::min<int64_t>((W + 1) / 2, 512));
     const int kb = rm_kbound(geom.rm_pairs);
-    geom.vec_scratch = vec_possible ? align16(size_t(geom.vec_nrow) * size_t(geom.vec_ncol)) : 0;
+    // byte matrix for the shared-memory form, two u32 bit-planes per 32 columns
+    // (at most 4 groups) for the register form
+    geom.vec_scratch = vec_possible ? align16(size_t(geom.vec_nrow) * std::max<size_t>(size_t(geom.vec_ncol), 32)) : 0;
     geom.rm_scratch = rm_possible ? align16(size_t(2 * lmax + 1) * 2 * kb * 4) : 0;
-    geom.nwarps = sms * 2 * kNwWarps;
+    geom.nwarps = sms * 4 * kNwWarps;
     const size_t per = std::max<size_t>(std::max(geom.vec_scratch, geom.rm_scratch), 16);
     TRY(scratch.alloc(per * size_t(geom.nwarps)));
     return 0;
@@ -285,8 +292,6 @@ struct Pool {
     uint32_t cap = std::max<uint32_t>(ntask, 64);
     TRY(tasks.alloc(cap));
     TRY(task_prefix.alloc(cap + 1));
-    TRY(task_counters.alloc(size_t(cap) * TC_NCOUNTERS));
-    TRY(task_nstored.alloc(cap));
     TRY(task_self.alloc(cap));
     TRY(task_stage.alloc(cap));
     TRY(prefix_stage.alloc(cap + 1));
@@ -294,20 +299,62 @@ struct Pool {
     return 0;
   }
 
+  int ensure_blocks(uint32_t nblk) {
+    if (nblk <= nblk_cap) return 0;
+    const uint32_t cap = std::max<uint32_t>(nblk, 256);
+    TRY(store_stage.alloc(size_t(2) * cap));
+    TRY(store_map.alloc(size_t(2) * cap));
+    TRY(blk_counters.alloc(size_t(cap) * TC_NCOUNTERS));
+    nblk_cap = cap;
+    return 0;
+  }
+
+  // Stored comps of task t (latest launch), in ascending raw order.
+  template <class F>
+  void for_each_stored(uint32_t t, F&& f) const {
+    const TaskDev& T = task_stage.h[t];
+    const uint32_t nb = (T.n + kStoreSpan - 1) / kStoreSpan;
+    for (uint32_t b = 0; b < nb; ++b) {
+      const uint32_t cnt = blk_counters.h[size_t(task_blk0[t] + b) * TC_NCOUNTERS + TC_STORED];
+      const uint32_t o = T.out_off + b * uint32_t(kStoreSpan);
+      for (uint32_t k = 0; k < cnt; ++k) f(comp_index.h[o + k], comp_lambda.h[o + k], comp_ham.h[o + k]);
+    }
+  }
+
+  // Counters of task t summed over its store CTAs.
+  void task_counters(uint32_t t, uint32_t* out) const {
+    for (int k = 0; k < TC_NCOUNTERS; ++k) out[k] = 0;
+    const uint32_t nb = (task_stage.h[t].n + kStoreSpan - 1) / kStoreSpan;
+    for (uint32_t b = 0; b < nb; ++b)
+      for (int k = 0; k < TC_NCOUNTERS; ++k) out[k] += blk_counters.h[size_t(task_blk0[t] + b) * TC_NCOUNTERS + k];
+  }
+
   // Launches one compare over `ntask` tasks already in task_stage; waits for it.
   int run_compare(uint32_t ntask, bool do_store, double* wait_s) {
     const auto t_call = Clock::now();
     TRY(ensure_tasks(ntask));
-    uint32_t total = 0;
+    uint32_t total = 0, nblk = 0;
+    task_blk0.assign(ntask, 0);
     for (uint32_t t = 0; t < ntask; ++t) {
       prefix_stage.h[t] = total;
       task_stage.h[t].out_off = total;
       total += task_stage.h[t].n;
+      task_blk0[t] = nblk;
+      nblk += (task_stage.h[t].n + kStoreSpan - 1) / kStoreSpan;
     }
     prefix_stage.h[ntask] = total;
+    TRY(ensure_blocks(nblk));
+    for (uint32_t t = 0; t < ntask; ++t) {
+      const uint32_t nb = (task_stage.h[t].n + kStoreSpan - 1) / kStoreSpan;
+      for (uint32_t b = 0; b < nb; ++b) {
+        store_stage.h[task_blk0[t] + b] = t;
+        store_stage.h[nblk + task_blk0[t] + b] = b;
+      }
+    }
     CUDA_TRY(cudaMemcpyAsync(tasks.p, task_stage.h, sizeof(TaskDev) * ntask, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(task_prefix.p, prefix_stage.h, 4 * (ntask + 1), cudaMemcpyHostToDevice, st));
-    CUDA_TRY(cudaMemsetAsync(queue_counts.p, 0, 16, st));
+    CUDA_TRY(cudaMemcpyAsync(store_map.p, store_stage.h, size_t(8) * nblk, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemsetAsync(queue_counts.p, 0, 32, st));
     CompareLaunch L{};
     L.pool = view();
     L.kp = kp;
@@ -317,6 +364,7 @@ struct Pool {
     L.total_items = total;
     L.queue_vec = queue_vec.p;
     L.queue_rm = queue_rm.p;
+    L.queue_pass = queue_pass.p;
     L.queue_counts = queue_counts.p;
     L.nw_scratch = scratch.p;
     L.geom = geom;
@@ -324,9 +372,11 @@ struct Pool {
     L.comp_index = comp_index.d;
     L.comp_lambda = comp_lambda.d;
     L.comp_ham = comp_ham.d;
-    L.task_counters = task_counters.d;
-    L.task_nstored = task_nstored.d;
     L.task_self = task_self.d;
+    L.store_task = store_map.p;
+    L.store_chunk = store_map.p + nblk;
+    L.blk_counters = blk_counters.d;
+    L.nstore_blocks = nblk;
     L.do_store = do_store ? 1 : 0;
     const bool timing = g_stats.timing.load();
     launch_compare(L, st, timing ? ev : nullptr);
@@ -336,19 +386,18 @@ struct Pool {
     const auto t1 = Clock::now();
     if (wait_s) *wait_s += secs(t0, t1);
     {
-      float ms[4] = {0, 0, 0, 0};
+      float ms[3] = {0, 0, 0};
       if (timing)
-        for (int k = 0; k < 4; ++k) CUDA_TRY(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));
+        for (int k = 0; k < 3; ++k) CUDA_TRY(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));
       uint64_t screened = 0;
       if (do_store)
-        for (uint32_t t = 0; t < ntask; ++t) screened += task_counters.h[size_t(t) * TC_NCOUNTERS + TC_SCREENED];
+        for (uint32_t b = 0; b < nblk; ++b) screened += blk_counters.h[size_t(b) * TC_NCOUNTERS + TC_SCREENED];
       std::lock_guard<std::mutex> g(g_stats.mu);
       dgpu_kernel_stats& S = g_stats.s;
       S.launches[1] += 1;
       S.launches[2] += 1;
-      S.launches[3] += 1;
-      if (do_store) S.launches[4] += 1;
-      for (int k = 0; k < 4; ++k) S.ms[k + 1] += ms[k];
+      if (do_store) S.launches[3] += 1;
+      for (int k = 0; k < 3; ++k) S.ms[k + 1] += ms[k];
       S.rounds += 1;
       S.compares += total;
       S.screened += screened;
@@ -510,9 +559,9 @@ struct SampleState {
 
   // The store's host half: comps from the device into cluster ci (src/cluster.rs:351-397).
   void absorb(size_t ci, const Pool& P, uint32_t t) {
-    const uint32_t* ctr = P.task_counters.h + size_t(t) * TC_NCOUNTERS;
-    const uint32_t ns = P.task_nstored.h[t];
-    const uint32_t o = P.task_stage.h[t].out_off;
+    uint32_t ctr[TC_NCOUNTERS];
+    P.task_counters(t, ctr);
+    const uint32_t ns = ctr[TC_STORED];
     nalign += ctr[TC_SCREENED];
     nshroud += ctr[TC_SHROUD];
     stats.compare_calls++;
@@ -526,13 +575,14 @@ struct SampleState {
     stats.endsfree += ctr[TC_ENDSFREE];
     Cluster& c = clusters[ci];
     c.self_ = P.task_self.h[t];
-    c.comp.resize(ns);
+    c.comp.clear();
+    c.comp.reserve(ns);
     const uint32_t center = uint32_t(c.center);
-    for (uint32_t k = 0; k < ns; ++k) {
-      Comp cp{uint32_t(ci), P.comp_index.h[o + k], P.comp_lambda.h[o + k], P.comp_ham.h[o + k]};
-      c.comp[k] = cp;
+    P.for_each_stored(t, [&](uint32_t idx, double lam, uint32_t ham) {
+      const Comp cp{uint32_t(ci), idx, lam, ham};
+      c.comp.push_back(cp);
       if (ci == 0 || cp.index == center) rcomp[cp.index] = cp;
-    }
+    });
     for (const Comp& cp : c.comp) cand[cp.index].push_back(Cand{uint32_t(ci), cp.lambda, cp.hamming});  // index_add_cluster
   }
 
@@ -929,6 +979,55 @@ class Workers {
   bool stop_ = false;
 };
 
+// Asynchronous job queue: the host phases of a sample run here while the GPU
+// works on other samples' compares.
+class JobQueue {
+ public:
+  explicit JobQueue(int n) {
+    for (int t = 0; t < n; ++t) th_.emplace_back([this] { loop(); });
+  }
+  ~JobQueue() {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : th_) t.join();
+  }
+  bool inline_mode() const { return th_.empty(); }
+  void submit(std::function<void()> fn) {
+    if (th_.empty()) {
+      fn();
+      return;
+    }
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      q_.push_back(std::move(fn));
+    }
+    cv_.notify_one();
+  }
+
+ private:
+  void loop() {
+    for (;;) {
+      std::function<void()> fn;
+      {
+        std::unique_lock<std::mutex> g(mu_);
+        cv_.wait(g, [&] { return stop_ || !q_.empty(); });
+        if (q_.empty()) return;
+        fn = std::move(q_.front());
+        q_.pop_front();
+      }
+      fn();
+    }
+  }
+  std::vector<std::thread> th_;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::deque<std::function<void()>> q_;
+  bool stop_ = false;
+};
+
 // ---------------------------------------------------------------------------
 // Inputs: validation and encoding (src/dada.rs:248-418)
 // ---------------------------------------------------------------------------
@@ -1116,52 +1215,85 @@ static dgpu_result* finish(SampleState& S, const SampleInput& in) {
   return R;
 }
 
-// The clustering loop over any number of samples resident in one pool. Every
-// round launches one compare covering each still-active sample's newest
-// cluster; the host phases then run per sample on the worker pool.
+// The clustering loop over any number of samples resident in one pool.
+// Samples advance independently: whenever the GPU is free, one compare launch
+// covers every sample whose next cluster is ready; each sample's host phases
+// (shuffle, p-update, bud) then run on the job queue while the GPU serves the
+// others. A sample's own sequence of steps is exactly run_dada's.
 static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_params& ap, int host_threads) {
   const size_t ns = S.size();
-  Workers W(host_threads > 1 ? host_threads - 1 : 0);
-  std::vector<int64_t> next(ns, 0);
-  std::vector<size_t> active;
-  double wait = 0.0, host = 0.0;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::vector<size_t> ready;
+  size_t finished = 0;
+  for (size_t s = 0; s < ns; ++s) {
+    S[s].pending = 0;  // cluster 0 first, with the screen off
+    ready.push_back(s);
+  }
+  double wait = 0.0;
+  std::atomic<int64_t> host_ns{0};
   auto t_start = Clock::now();
-  for (size_t s = 0; s < ns; ++s) S[s].pending = 0;  // round 0: cluster 0 with the screen off
-  for (;;) {
-    active.clear();
-    for (size_t s = 0; s < ns; ++s)
-      if (S[s].pending >= 0) active.push_back(s);
-    if (active.empty()) break;
-    TRY(P.ensure_tasks(uint32_t(active.size())));
-    for (size_t a = 0; a < active.size(); ++a) {
-      SampleState& ss = S[active[a]];
-      const size_t ci = size_t(ss.pending);
-      P.task_stage.h[a] = ss.task_for(ci, ci == 0 ? 1.0 : ap.kdist_cutoff);  // init_params, src/dada.rs:835-838
-      if (ss.lock_dirty) {
-        TRY(P.push_locks(ss.base, ss.n));
-        ss.lock_dirty = false;
+  int rc = 0;
+  {
+    JobQueue jobs(host_threads > 1 ? host_threads : 0);
+    std::vector<size_t> batch;
+    for (;;) {
+      batch.clear();
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return !ready.empty() || finished == ns; });
+        if (ready.empty()) break;
+        batch.swap(ready);
+      }
+      std::sort(batch.begin(), batch.end());
+      rc = P.ensure_tasks(uint32_t(batch.size()));
+      if (rc) break;
+      for (size_t a = 0; a < batch.size(); ++a) {
+        SampleState& ss = S[batch[a]];
+        const size_t ci = size_t(ss.pending);
+        P.task_stage.h[a] = ss.task_for(ci, ci == 0 ? 1.0 : ap.kdist_cutoff);  // init_params, src/dada.rs:835-838
+        if (ss.lock_dirty) {
+          rc = P.push_locks(ss.base, ss.n);
+          if (rc) break;
+          ss.lock_dirty = false;
+        }
+      }
+      if (rc) break;
+      auto tc = Clock::now();
+      rc = P.run_compare(uint32_t(batch.size()), true, &wait);
+      if (rc) break;
+      const double tcmp = secs(tc, Clock::now());
+      for (size_t a = 0; a < batch.size(); ++a) {
+        SampleState& ss = S[batch[a]];
+        ss.absorb(size_t(ss.pending), P, uint32_t(a));
+        ss.stats.t_compare += tcmp;
+      }
+      for (size_t a = 0; a < batch.size(); ++a) {
+        const size_t sidx = batch[a];
+        jobs.submit([&, sidx] {
+          SampleState& ss = S[sidx];
+          auto th = Clock::now();
+          ss.pending = ss.advance(size_t(ss.pending));
+          host_ns += int64_t(1e9 * secs(th, Clock::now()));
+          std::lock_guard<std::mutex> g(mu);
+          if (ss.pending >= 0) ready.push_back(sidx);
+          else ++finished;
+          cv.notify_one();
+        });
       }
     }
-    auto tc = Clock::now();
-    TRY(P.run_compare(uint32_t(active.size()), true, &wait));
-    const double tcmp = secs(tc, Clock::now());
-    auto th = Clock::now();
-    W.run(active.size(), [&](size_t a) {
-      SampleState& ss = S[active[a]];
-      const size_t ci = size_t(ss.pending);
-      ss.absorb(ci, P, uint32_t(a));
-      ss.stats.t_compare += tcmp;
-      ss.pending = ss.advance(ci);
-    });
-    host += secs(th, Clock::now());
+    if (rc) {  // let queued host phases drain before the queue is torn down
+      std::unique_lock<std::mutex> lk(mu);
+      lk.unlock();
+    }
   }
   const double total = secs(t_start, Clock::now());
   for (auto& ss : S) {
     ss.stats.t_total = total;
-    ss.stats.t_host = host;
+    ss.stats.t_host = double(host_ns.load()) * 1e-9;
     ss.stats.t_wait = wait;
   }
-  return 0;
+  return rc;
 }
 
 // A prepared batch: encoded samples resident on one device.
@@ -1186,10 +1318,31 @@ static int batch_prepare(Batch& B, int device, const dgpu_dada_params* prm, int 
   B.in.assign(static_cast<size_t>(nsamples), SampleInput());
   uint32_t qmax = 0;
   bool any_q = false;
-  for (int s = 0; s < nsamples; ++s) {
+  for (int s = 0; s < nsamples; ++s)
     if (sample_start[s + 1] < sample_start[s]) return fail(DGPU_E_INVALID, "sample_start must be non-decreasing");
-    TRY(encode_sample(uint32_t(s), sample_start[s], sample_start[s + 1], seqs, offs, lens, abund, prior, qsums, k,
-                      B.in[size_t(s)]));
+  {
+    // encode samples in parallel; the first failing sample (by index) reports
+    std::vector<int> rcs(static_cast<size_t>(nsamples), 0);
+    std::vector<std::string> msgs(static_cast<size_t>(nsamples));
+    const int nt = std::max(1, std::min(nsamples, int(std::thread::hardware_concurrency())));
+    std::atomic<int> next{0};
+    auto work = [&] {
+      for (;;) {
+        const int s = next.fetch_add(1);
+        if (s >= nsamples) break;
+        rcs[size_t(s)] = encode_sample(uint32_t(s), sample_start[s], sample_start[s + 1], seqs, offs, lens, abund,
+                                       prior, qsums, k, B.in[size_t(s)]);
+        if (rcs[size_t(s)]) msgs[size_t(s)] = g_err;
+      }
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; ++t) th.emplace_back(work);
+    work();
+    for (auto& t : th) t.join();
+    for (int s = 0; s < nsamples; ++s)
+      if (rcs[size_t(s)]) return fail(rcs[size_t(s)], msgs[size_t(s)]);
+  }
+  for (int s = 0; s < nsamples; ++s) {
     if (B.in[size_t(s)].has_qual) {
       any_q = true;
       qmax = std::max(qmax, B.in[size_t(s)].qmax);
@@ -1413,13 +1566,18 @@ int dgpu_compare_store(dgpu_ctx* ctx, int center, int cluster_i, double kdist_cu
   TRY(ctx_task(ctx, center, cluster_i, kdist_cutoff, greedy));
   Pool& P = ctx->pool;
   TRY(P.run_compare(1, true, nullptr));
-  const uint32_t ns = P.task_nstored.h[0];
-  if (comp_index) std::memcpy(comp_index, P.comp_index.h, size_t(ns) * 4);
-  if (comp_lambda) std::memcpy(comp_lambda, P.comp_lambda.h, size_t(ns) * 8);
-  if (comp_hamming) std::memcpy(comp_hamming, P.comp_ham.h, size_t(ns) * 4);
-  if (nstored) *nstored = int(ns);
+  uint32_t ctr[TC_NCOUNTERS];
+  P.task_counters(0, ctr);
+  uint32_t k = 0;
+  P.for_each_stored(0, [&](uint32_t idx, double lam, uint32_t ham) {
+    if (comp_index) comp_index[k] = idx;
+    if (comp_lambda) comp_lambda[k] = lam;
+    if (comp_hamming) comp_hamming[k] = ham;
+    ++k;
+  });
+  if (nstored) *nstored = int(k);
   if (self_out) *self_out = P.task_self.h[0];
-  fill_counters(P.task_counters.h, ns, cnt);
+  fill_counters(ctr, k, cnt);
   return 0;
 }
 
@@ -1557,7 +1715,7 @@ int dgpu_align_debug(int device, int which, int npairs, const uint8_t* s1cat, co
   g.vec_nrow = int32_t(2 * lmax + 1);
   int64_t W = kp.band < 0 ? int64_t(2 * lmax + 1) : std::min<int64_t>(2 * bb + diff + 1, 2 * int64_t(lmax) + 1);
   g.rm_pairs = int32_t(std::min<int64_t>((W + 1) / 2, 512));
-  g.vec_scratch = align16(size_t(g.vec_nrow) * g.vec_ncol);
+  g.vec_scratch = align16(size_t(g.vec_nrow) * std::max<size_t>(size_t(g.vec_ncol), 32));
   g.rm_scratch = align16(size_t(2 * lmax + 1) * 2 * rm_kbound(g.rm_pairs) * 4);
   g.nwarps = npairs;
   const size_t per = which == 0 ? g.vec_scratch : g.rm_scratch;

@@ -129,149 +129,172 @@ __device__ __forceinline__ uint32_t mismatch_word(const uint8_t* a, const uint8_
   return __ballot_sync(FULL, mm);
 }
 
-__global__ void __launch_bounds__(kScreenWarps * 32) k_screen(CompareLaunch L) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+// Lean streaming screen: greedy skip, profile dot product, strict cutoff
+// (src/cluster.rs:295-298, src/kmers.rs:254-269, src/nwalign.rs:1299).
+// A warp takes 32 consecutive items: lane l resolves item l's task and raw
+// metadata, then the warp streams the raw profiles four at a time against the
+// center profile held in registers. Survivors go to the align queue with their
+// kdist parked in res_lambda.
+template <int K>
+__global__ void __launch_bounds__(kScreenWarps * 32, 4) k_screen(CompareLaunch L) {
+  constexpr int NK16 = (1 << (2 * K)) / 16;            // 16-byte vectors per profile
+  constexpr int VPL = NK16 >= 32 ? NK16 / 32 : 1;      // vectors per lane
+  constexpr bool CENTER_REGS = VPL <= 2;               // k <= 5: center stays in registers
+  constexpr int NB = VPL == 1 ? 4 : (VPL == 2 ? 3 : 1); // raw profiles in flight per warp
   const KParams& kp = L.kp;
-  double* err_s = reinterpret_cast<double*>(smem_raw);
-  const int nerr = 16 * kp.ncol;
-  for (int t = threadIdx.x; t < nerr; t += blockDim.x) err_s[t] = L.pool.err[t];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const size_t err_bytes = err_smem_bytes(kp.ncol);
-  unsigned char* wbase = smem_raw + err_bytes + size_t(wib) * screen_smem_per_warp(L.pool.maxlen);
-  uint16_t* fidx = reinterpret_cast<uint16_t*>(wbase);
-  uint8_t* tcode = wbase + align16(size_t(L.pool.maxlen) * 2);
-  __syncthreads();
-
-  const int k = kp.kmer_size;
-  const int nk16 = (1 << (2 * k)) / 16;
   const uint32_t warps_total = gridDim.x * kScreenWarps;
-  for (uint32_t item = blockIdx.x * kScreenWarps + wib; item < L.total_items; item += warps_total) {
-    const uint32_t t = find_task(L.task_prefix, L.ntask, item);
-    const TaskDev T = L.tasks[t];
-    const uint32_t g = T.base + (item - L.task_prefix[t]);
-    const uint32_t c = T.center;
-    const int lc = int(L.pool.len[c]), lg = int(L.pool.len[g]);
-    const uint8_t* sc = L.pool.seq + L.pool.off[c];
-    const uint8_t* sg = L.pool.seq + L.pool.off[g];
-
-    if (kp.greedy && (L.pool.reads[g] > T.center_reads || L.pool.lock[g])) {
-      if (lane == 0) {
+  const uint8_t* kmer8 = L.pool.kmer8;
+  for (uint32_t chunk = (blockIdx.x * kScreenWarps + wib) * 32u; chunk < L.total_items; chunk += warps_total * 32u) {
+    const uint32_t item = chunk + lane;
+    const bool valid = item < L.total_items;
+    uint32_t t = 0, g = 0, c = 0;
+    bool skip = false;
+    if (valid) {
+      t = find_task(L.task_prefix, L.ntask, item);
+      g = L.tasks[t].base + (item - L.task_prefix[t]);
+      c = L.tasks[t].center;
+      skip = kp.greedy && (L.pool.reads[g] > L.tasks[t].center_reads || L.pool.lock[g]);
+    }
+    const bool need = valid && !skip && kp.use_kmers;
+    uint32_t mydot = 0, myovf = 0;
+    uint32_t todo = __ballot_sync(FULL, need);
+    // center profile of the chunk's first needing item, kept in registers
+    uint32_t cur_c = 0xffffffffu;
+    uint4 cv[CENTER_REGS ? VPL : 1];
+    (void)cur_c;
+    while (todo) {
+      int js[NB];
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        js[q] = -1;
+        if (todo) {
+          js[q] = __ffs(todo) - 1;
+          todo &= todo - 1;
+        }
+      }
+      uint32_t gq[NB], cq[NB];
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        const int src = js[q] < 0 ? 0 : js[q];
+        gq[q] = __shfl_sync(FULL, g, src);
+        cq[q] = __shfl_sync(FULL, c, src);
+      }
+      constexpr int RV = CENTER_REGS ? VPL : 1;
+      uint4 rv[NB][RV];
+      if (CENTER_REGS) {
+#pragma unroll
+        for (int q = 0; q < NB; ++q) {
+          if (js[q] >= 0) {
+            const uint4* pg = reinterpret_cast<const uint4*>(kmer8 + size_t(gq[q]) * size_t(NK16) * 16);
+#pragma unroll
+            for (int v = 0; v < RV; ++v) {
+              const int idx = lane + 32 * v;
+              rv[q][v] = idx < NK16 ? __ldcs(pg + idx) : make_uint4(0, 0, 0, 0);
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        if (js[q] < 0) continue;
+        const uint4* pc = reinterpret_cast<const uint4*>(kmer8 + size_t(cq[q]) * size_t(NK16) * 16);
+        const uint4* pg = reinterpret_cast<const uint4*>(kmer8 + size_t(gq[q]) * size_t(NK16) * 16);
+        if (CENTER_REGS && cq[q] != cur_c) {
+#pragma unroll
+          for (int v = 0; v < VPL; ++v) {
+            const int idx = lane + 32 * v;
+            cv[CENTER_REGS ? v : 0] = idx < NK16 ? __ldg(pc + idx) : make_uint4(0, 0, 0, 0);
+          }
+          cur_c = cq[q];
+        }
+        uint32_t dot = 0, ovf = 0;
+#pragma unroll 4
+        for (int v = 0; v < VPL; ++v) {
+          const int idx = lane + 32 * v;
+          const uint4 a = CENTER_REGS ? cv[CENTER_REGS ? v : 0] : (idx < NK16 ? __ldg(pc + idx) : make_uint4(0, 0, 0, 0));
+          const uint4 b2 = CENTER_REGS ? rv[q][CENTER_REGS ? v : 0] : (idx < NK16 ? __ldcs(pg + idx) : make_uint4(0, 0, 0, 0));
+          const uint32_t m0 = __vminu4(a.x, b2.x), m1 = __vminu4(a.y, b2.y), m2 = __vminu4(a.z, b2.z),
+                         m3 = __vminu4(a.w, b2.w);
+          dot = __dp4a(m0, 0x01010101u, dot);
+          dot = __dp4a(m1, 0x01010101u, dot);
+          dot = __dp4a(m2, 0x01010101u, dot);
+          dot = __dp4a(m3, 0x01010101u, dot);
+          ovf |= __vcmpeq4(m0, 0xffffffffu) | __vcmpeq4(m1, 0xffffffffu) | __vcmpeq4(m2, 0xffffffffu) |
+                 __vcmpeq4(m3, 0xffffffffu);
+        }
+        dot = __reduce_add_sync(FULL, dot);
+        ovf = __reduce_or_sync(FULL, ovf);
+        if (lane == js[q]) {
+          mydot = dot;
+          myovf = ovf;
+        }
+      }
+    }
+    // Saturated k-mers (min == 255 somewhere): the exact u16 dot
+    // (src/nwalign.rs:1270-1277), one item at a time by the whole warp. Each
+    // window of the raw contributes 1 when its rank among equal windows of the
+    // raw is below the center's count of that k-mer.
+    uint32_t ovf_mask = __ballot_sync(FULL, need && myovf != 0);
+    while (ovf_mask) {
+      const int j = __ffs(ovf_mask) - 1;
+      ovf_mask &= ovf_mask - 1;
+      const uint32_t gj = __shfl_sync(FULL, g, j), cj = __shfl_sync(FULL, c, j);
+      const int lc = int(L.pool.len[cj]), lg = int(L.pool.len[gj]);
+      const uint8_t* sc = L.pool.seq + L.pool.off[cj];
+      const uint8_t* sg = L.pool.seq + L.pool.off[gj];
+      uint32_t exact = 0;
+      for (int p = lane; p + K <= lg; p += 32) {
+        int x = 0;
+        for (int q = 0; q < K; ++q) x = x * 4 + int(sg[p + q]) - 1;
+        uint32_t rank = 0, cnt = 0;
+        for (int p2 = 0; p2 < p; ++p2) {
+          int y = 0;
+          for (int q = 0; q < K; ++q) y = y * 4 + int(sg[p2 + q]) - 1;
+          rank += (y == x);
+        }
+        for (int p2 = 0; p2 + K <= lc; ++p2) {
+          int y = 0;
+          for (int q = 0; q < K; ++q) y = y * 4 + int(sc[p2 + q]) - 1;
+          cnt += (y == x);
+        }
+        exact += rank < cnt ? 1u : 0u;
+      }
+      exact = __reduce_add_sync(FULL, exact);
+      if (lane == j) mydot = exact;
+    }
+    bool pass = false;
+    if (valid) {
+      if (skip) {
         L.pool.res_lambda[g] = 0.0;
         L.pool.res_ham[g] = 0xffffffffu;
         L.pool.res_status[g] = ST_SKIPPED;
-      }
-      continue;
-    }
-    double kdist = 0.0, kodist = -1.0;
-    if (kp.use_kmers) {
-      const uint4* pc = reinterpret_cast<const uint4*>(L.pool.kmer8 + size_t(c) * size_t(nk16) * 16);
-      const uint4* pg = reinterpret_cast<const uint4*>(L.pool.kmer8 + size_t(g) * size_t(nk16) * 16);
-      uint32_t dot = 0, ovf = 0;
-      for (int v = lane; v < nk16; v += 32) {
-        uint4 a = __ldg(pc + v);
-        uint4 b = __ldcs(pg + v);
-        uint32_t m0 = __vminu4(a.x, b.x), m1 = __vminu4(a.y, b.y), m2 = __vminu4(a.z, b.z), m3 = __vminu4(a.w, b.w);
-        dot = __dp4a(m0, 0x01010101u, dot);
-        dot = __dp4a(m1, 0x01010101u, dot);
-        dot = __dp4a(m2, 0x01010101u, dot);
-        dot = __dp4a(m3, 0x01010101u, dot);
-        ovf |= __vcmpeq4(m0, 0xffffffffu) | __vcmpeq4(m1, 0xffffffffu) | __vcmpeq4(m2, 0xffffffffu) |
-               __vcmpeq4(m3, 0xffffffffu);
-      }
-      dot = __reduce_add_sync(FULL, dot);
-      ovf = __reduce_or_sync(FULL, ovf);
-      if (ovf) {
-        // A k-mer saturated in both profiles: recompute the exact u16 dot
-        // (src/nwalign.rs:1270-1277). Each window of the raw contributes 1 when its
-        // rank among equal windows of the raw is below the center's count.
-        uint32_t exact = 0;
-        for (int p = lane; p + k <= lg; p += 32) {
-          int x = 0;
-          for (int q = 0; q < k; ++q) x = x * 4 + int(sg[p + q]) - 1;
-          uint32_t rank = 0, cnt = 0;
-          for (int p2 = 0; p2 < p; ++p2) {
-            int y = 0;
-            for (int q = 0; q < k; ++q) y = y * 4 + int(sg[p2 + q]) - 1;
-            rank += (y == x);
-          }
-          for (int p2 = 0; p2 + k <= lc; ++p2) {
-            int y = 0;
-            for (int q = 0; q < k; ++q) y = y * 4 + int(sc[p2 + q]) - 1;
-            cnt += (y == x);
-          }
-          exact += rank < cnt ? 1u : 0u;
+      } else {
+        double kdist = 0.0;
+        bool shroud = false;
+        if (kp.use_kmers) {
+          const int lc = int(L.pool.len[c]), lg = int(L.pool.len[g]);
+          const int minl = lc < lg ? lc : lg;
+          kdist = 1.0 - double(mydot) / double(minl - K + 1);
+          shroud = kdist > L.tasks[t].cutoff;
         }
-        dot = __reduce_add_sync(FULL, exact);
-      }
-      const int minl = lc < lg ? lc : lg;
-      kdist = 1.0 - double(dot) / double(minl - k + 1);
-    }
-    const bool shroud = kp.use_kmers && kdist > T.cutoff;
-    if (shroud) {
-      if (lane == 0) {
-        L.pool.res_lambda[g] = 0.0;
-        L.pool.res_ham[g] = 0xffffffffu;
-        L.pool.res_status[g] = ST_SHROUDED;
-      }
-      continue;
-    }
-    // Positional mismatch scan: ordered-k-mer distance (src/kmers.rs:314-328, equal
-    // windows <=> equal k-mer codes for ACGT input) and the gapless Hamming count.
-    const int minl = lc < lg ? lc : lg;
-    const bool want_kod = kp.use_kmers && kp.gapless && lc == lg;
-    uint32_t ham = 0;
-    if (want_kod || kp.band == 0) {
-      const int klen = lc - (k - 1);
-      const uint32_t kmask = (k >= 32) ? 0xffffffffu : ((1u << k) - 1u);
-      uint32_t eq = 0;
-      uint32_t cur = mismatch_word(sc, sg, 0, minl, lane);
-      for (int b = 0; b < minl; b += 32) {
-        uint32_t nxt = mismatch_word(sc, sg, b + 32, minl, lane);
-        ham += __popc(cur);
-        if (want_kod) {
-          unsigned long long both = (static_cast<unsigned long long>(nxt) << 32) | cur;
-          int j = b + lane;
-          bool ok = j < klen && ((uint32_t(both >> lane) & kmask) == 0u);
-          eq += __popc(__ballot_sync(FULL, ok));
-        }
-        cur = nxt;
-      }
-      if (want_kod && klen > 0) kodist = 1.0 - double(eq) / double(klen);
-    }
-    const bool gapless = kp.band == 0 || (kp.gapless && fabs(kodist - kdist) < DBL_EPSILON);
-    if (!gapless) {
-      const bool use_homo = kp.homo_gap != kp.gap && kp.homo_gap <= 0;
-      const bool vec = kp.vectorized && lc <= 3500 && lg <= 3500 && !use_homo;
-      if (lane == 0) {
-        if (vec) {
-          uint32_t slot = atomicAdd(&L.queue_counts[0], 1u);
-          L.queue_vec[slot] = item;
+        if (shroud) {
+          L.pool.res_lambda[g] = 0.0;
+          L.pool.res_ham[g] = 0xffffffffu;
+          L.pool.res_status[g] = ST_SHROUDED;
         } else {
-          uint32_t slot = atomicAdd(&L.queue_counts[1], 1u);
-          L.queue_rm[slot] = item;
+          L.pool.res_lambda[g] = kdist;
+          pass = true;
         }
       }
-      continue;
     }
-    // Gapless: raw position p aligns to center position p while p < len(center).
-    for (int p = lane; p < lg; p += 32) {
-      unsigned r = sg[p];
-      unsigned code = (p < lc) ? (unsigned(sc[p]) - 1u) * 4u + (r - 1u) : (r - 1u) * 5u;
-      const bool valid = r >= 1u && r <= 4u && (p >= lc || (sc[p] >= 1 && sc[p] <= 4));
-      tcode[p] = uint8_t(valid ? code : 255u);
+    const uint32_t pm = __ballot_sync(FULL, pass);
+    if (pm) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(&L.queue_counts[4], uint32_t(__popc(pm)));
+      base = __shfl_sync(FULL, base, 0);
+      if (pass) L.queue_pass[base + __popc(pm & ((1u << lane) - 1u))] = item;
     }
-    __syncwarp();
-    const uint8_t* qg = L.pool.qual ? L.pool.qual + L.pool.off[g] : nullptr;
-    bool bad = build_fidx(lane, tcode, qg, lg, kp.ncol, kp.use_quals, fidx);
-    __syncwarp();
-    double lam = bad ? 0.0 : lambda_chain(lane, fidx, lg, err_s);
-    if (lane == 0) {
-      if (bad) atomicOr(L.err_word, DERR_LAMBDA);
-      L.pool.res_lambda[g] = lam;
-      L.pool.res_ham[g] = ham;
-      L.pool.res_status[g] = uint8_t(ST_ALIGNED | (AM_GAPLESS << 2));
-    }
-    __syncwarp();
   }
 }
 
@@ -575,6 +598,329 @@ __device__ VecSmem carve_vec(unsigned char* base, int lmax, int ncol_bound) {
 }
 
 
+// Register form of the same aligner for compressed widths up to 32*M columns:
+// lane l owns columns l + 32m; the three rolling rows live in registers
+// (r3 = the slot being overwritten, still holding row-3 values, as in the
+// reference's rotating buffer), left/up neighbours come from warp shuffles and
+// each row's 2-bit pointers are two ballot bit-planes per 32 columns, buffered
+// 32 rows per flush to the per-warp scratch.
+template <int M>
+__device__ bool vec_align_reg(int lane, const uint8_t* g1, int l1, const uint8_t* g2, int l2, int16_t match,
+                              int16_t mismatch, int16_t gap, int16_t egp, int band_in, const VecSmem& S,
+                              uint32_t* pscr, int nrow_bound, uint32_t* ham_out, uint32_t* err_word, uint8_t* dbg0,
+                              uint8_t* dbg1, uint32_t* dbg_len) {
+  const bool swap = l1 > l2;
+  const int len1 = swap ? l2 : l1, len2 = swap ? l1 : l2;
+  {
+    const uint8_t* a = swap ? g2 : g1;
+    const uint8_t* b = swap ? g1 : g2;
+    for (int p = lane; p < len1; p += 32) S.s1[p] = a[p];
+    for (int p = lane; p < len2; p += 32) S.s2[p] = b[p];
+  }
+  const int band = band_in < 0 ? len2 : band_in;
+  const int start_col = 1 + (min(band, len1) + 1) / 2;
+  const int ncol = 2 + start_col + min(band + len2 - len1, len2) / 2;
+  const int nrow = len1 + len2 + 1;
+  if (ncol > 32 * M || nrow > nrow_bound || ncol < 4) {
+    if (lane == 0) atomicOr(err_word, DERR_GEOMETRY);
+    return false;
+  }
+  const int16_t min_score = min(min(min(mismatch, gap), match), int16_t(0));
+  const int16_t fill = int16_t(uint16_t(uint16_t(0x8000u) - uint16_t(min_score)));
+  const int lfl = 1 + min(band, len1);
+  const int tfl = 1 + min(band + len2 - len1, len2);
+  auto left_col = [&](int row) { int a = start_col - 1, b = (row - 1) / 2; return a > b ? a - b : 0; };
+  auto top_col = [&](int row) { return start_col + row / 2; };
+  int16_t r3[M], r2[M], r1[M];
+  uint32_t pbuf[2 * M];
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const int c = lane + 32 * m;
+    const bool sent = c == 0 || c == 1 || c == ncol - 2 || c == ncol - 1;
+    int16_t v0 = sent ? fill : int16_t(0);
+    if (c == start_col) v0 = 0;
+    int16_t v1 = sent ? fill : int16_t(0);
+    uint8_t c1 = 0;
+    if (1 < lfl && c == left_col(1)) { v1 = egp; c1 = 3; }
+    if (1 < tfl && c == top_col(1)) { v1 = egp; c1 = 2; }
+    r3[m] = 0;
+    r2[m] = v0;
+    r1[m] = v1;
+    const uint32_t w0 = __ballot_sync(FULL, c1 & 1), w1 = __ballot_sync(FULL, (c1 >> 1) & 1);
+    pbuf[2 * m] = lane == 0 ? 0u : (lane == 1 ? w0 : 0u);
+    pbuf[2 * m + 1] = lane == 0 ? 0u : (lane == 1 ? w1 : 0u);
+  }
+  __syncwarp();
+  int16_t row_free = egp;
+  int col_min = start_col, col_max = start_col, i_max = 0, j_min = 0;
+  bool even = true, recalc_left = false, recalc_right = false;
+  const int band_mod2 = band % 2;
+  const int top_limit = min(band + len2 - len1, len2);
+  const int full_band = band + len2 - len1;
+  const int last = len1 + len2;
+  bool ok = true;
+  const int bt_row1 = min(band, len1);
+  const int bt_row2 = min(band + len2 - len1, len2);
+  const bool fb_even = full_band % 2 == 0;
+  for (int row = 2; row <= last; ++row) {
+    const int n = col_max - col_min + 1;
+    const int eo = even ? 1 : 0;
+    const int left_off = col_min - eo, up_off = col_min + 1 - eo;
+    if ((col_max < col_min) | (col_max >= ncol) | (left_off < 0) | (up_off + n > ncol)) { ok = false; break; }
+    row_free = sadd16(row_free, egp);
+    int k_lo = i_max - len1 + 1;
+    k_lo = k_lo < 0 ? 0 : (k_lo > n ? n : k_lo);
+    int k_hi = min(i_max + 1, len2 - j_min);
+    k_hi = k_hi < 0 ? 0 : (k_hi > n ? n : k_hi);
+    k_hi = max(k_hi, k_lo);
+    const int lcol = row < lfl ? left_col(row) : -1;
+    const int tcol = row < tfl ? top_col(row) : -1;
+    int16_t cur[M];
+    uint8_t cc[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const int16_t a = int16_t(__shfl_up_sync(FULL, int(r1[m]), 1));
+      const int16_t a31 = m > 0 ? int16_t(__shfl_sync(FULL, int(r1[m > 0 ? m - 1 : 0]), 31)) : int16_t(0);
+      const int16_t b = int16_t(__shfl_down_sync(FULL, int(r1[m]), 1));
+      const int16_t b0 = (m + 1 < M) ? int16_t(__shfl_sync(FULL, int(r1[m + 1 < M ? m + 1 : m]), 0)) : int16_t(0);
+      const int16_t lm1 = lane == 0 ? a31 : a;   // row-1 value at column c-1
+      const int16_t rp1 = lane == 31 ? b0 : b;   // row-1 value at column c+1
+      const int c = lane + 32 * m;
+      int16_t v = r3[m];
+      uint8_t code = 0;
+      if (c == 0 || c == 1 || c == ncol - 2 || c == ncol - 1) v = fill;
+      if (c == lcol) { v = row_free; code = 3; }
+      if (c == tcol) { v = row_free; code = 2; }
+      if (c >= col_min && c <= col_max) {
+        const int k = c - col_min;
+        int16_t sc;
+        if (k < k_lo || k >= k_hi) sc = fill;
+        else sc = (S.s1[i_max - k] == S.s2[j_min + k]) ? match : mismatch;
+        const int16_t dg = sadd16(r2[m], sc);
+        const int16_t l = sadd16(eo ? lm1 : r1[m], gap);
+        const int16_t u = sadd16(eo ? r1[m] : rp1, gap);
+        int16_t e;
+        uint8_t pe;
+        if (swap) {
+          if (l >= u) { e = l; pe = 2; } else { e = u; pe = 3; }
+        } else {
+          if (u >= l) { e = u; pe = 3; } else { e = l; pe = 2; }
+        }
+        if (dg > e) { e = dg; pe = 1; }
+        v = e;
+        code = pe;
+      }
+      cur[m] = v;
+      cc[m] = code;
+    }
+    {  // band transition at the wedge boundaries (src/nwalign.rs:980-987), branch-free
+      const bool t1 = row == bt_row1;
+      col_min = t1 ? sat_sub1(col_min) : col_min;
+      i_max += t1 ? 1 : 0;
+      j_min -= t1 ? 1 : 0;
+      col_max += (row == bt_row2) ? 1 : 0;
+    }
+    if (egp > gap) {
+      if (recalc_left) {
+        int16_t pv = r1[0];
+#pragma unroll
+        for (int m = 1; m < M; ++m)
+          if ((left_off >> 5) == m) pv = r1[m];
+        pv = int16_t(__shfl_sync(FULL, int(pv), left_off & 31));
+        const int16_t d_free = sadd16(pv, egp);
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+          if (lane + 32 * m == col_min) {
+            const int16_t cv = cur[m];
+            const uint8_t pc = cc[m];
+            if (d_free > cv) {
+              cur[m] = d_free;
+              cc[m] = 2;
+            } else if (!(d_free != cv || (!swap && pc != 1) || (swap && pc == 2))) {
+              cc[m] = 2;
+            }
+          }
+        }
+      }
+      if (i_max == len1 - 1) recalc_left = true;
+      if (recalc_right) {
+        const int idx = up_off + col_max - col_min;
+        if (idx < 0 || idx >= ncol || col_max >= ncol) { ok = false; break; }
+        int16_t pv = r1[0];
+#pragma unroll
+        for (int m = 1; m < M; ++m)
+          if ((idx >> 5) == m) pv = r1[m];
+        pv = int16_t(__shfl_sync(FULL, int(pv), idx & 31));
+        const int16_t d_free = sadd16(pv, egp);
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+          if (lane + 32 * m == col_max) {
+            const int16_t cv = cur[m];
+            const uint8_t pc = cc[m];
+            if (d_free > cv) {
+              cur[m] = d_free;
+              cc[m] = 3;
+            } else if (!(d_free != cv || (!swap && pc == 3) || (swap && pc != 1))) {
+              cc[m] = 3;
+            }
+          }
+        }
+      }
+      if ((row + 1) / 2 + col_max - start_col == len2) recalc_right = true;
+    }
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const uint32_t w0 = __ballot_sync(FULL, cc[m] & 1), w1 = __ballot_sync(FULL, (cc[m] >> 1) & 1);
+      if (lane == (row & 31)) {
+        pbuf[2 * m] = w0;
+        pbuf[2 * m + 1] = w1;
+      }
+    }
+    if ((row & 31) == 31 || row == last) {
+      const int base = row & ~31;
+      if (base + lane <= row) {
+        uint32_t* dst = pscr + size_t(base + lane) * (2 * M);
+#pragma unroll
+        for (int w = 0; w < 2 * M; ++w) dst[w] = pbuf[w];
+      }
+    }
+    {  // advance the band for the next anti-diagonal (src/nwalign.rs:1028-1079), branch-free
+      const bool e = even;
+      const bool regA = row < band && row < len1;
+      const bool regB = !regA && i_max < len1 - 1;
+      const int cm = col_min, im = i_max, jm = j_min;
+      const int cmA = e ? sat_sub1(cm) : cm, imA = im + 1, jmA = jm;
+      int cmB, imB, jmB;
+      if (band_mod2 == 0) {
+        cmB = cm;
+        imB = e ? im : im + 1;
+        jmB = e ? jm + 1 : jm;
+      } else {
+        cmB = e ? sat_sub1(cm) : cm + 1;
+        imB = e ? im + 1 : im;
+        jmB = e ? jm : jm + 1;
+      }
+      const int cmC = e ? cm : cm + 1, imC = im, jmC = jm + 1;
+      col_min = regA ? cmA : (regB ? cmB : cmC);
+      i_max = regA ? imA : (regB ? imB : imC);
+      j_min = regA ? jmA : (regB ? jmB : jmC);
+      const int cx = col_max;
+      const bool rt = row < top_limit;
+      const bool mid = !rt && ((row + 1) / 2 + cx - start_col < len2);
+      const int cxA = e ? cx : cx + 1;
+      const int cxB = fb_even ? (e ? sat_sub1(cx) : cx + 1) : cx;
+      const int cxC = e ? sat_sub1(cx) : cx;
+      col_max = rt ? cxA : (mid ? cxB : cxC);
+    }
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      r3[m] = r2[m];
+      r2[m] = r1[m];
+      r1[m] = cur[m];
+    }
+    even = !even;
+  }
+  if (!ok) {
+    if (lane == 0) atomicOr(err_word, DERR_BAND_RANGE);
+    return false;
+  }
+  if (last < 2) {  // rows 0/1 only: flush the buffered words
+    if (lane <= last) {
+      uint32_t* dst = pscr + size_t(lane) * (2 * M);
+#pragma unroll
+      for (int w = 0; w < 2 * M; ++w) dst[w] = pbuf[w];
+    }
+  }
+  __syncwarp();
+  // Traceback through the bit-planes, 32 rows staged in shared memory at a time.
+  const uint8_t* raw = swap ? S.s1 : S.s2;
+  const int lraw = swap ? len1 : len2;
+  for (int p = lane; p < lraw; p += 32) S.tcode[p] = uint8_t((unsigned(raw[p]) - 1u) * 5u);
+  uint32_t* stage = reinterpret_cast<uint32_t*>(S.stage);
+  int slo = 0x7fffffff;
+  int i = len1, j = len2;
+  uint32_t ham = 0, alen = 0;
+  __syncwarp();
+  while (i > 0 || j > 0) {
+    const int cs = 2 * start_col + j - i;
+    if (cs < 0) { ok = false; break; }
+    const int col = cs / 2;
+    const int r = i + j;
+    if (r < slo) {
+      const int nlo = max(0, r - 31);
+      __syncwarp();
+      const int nw = (r - nlo + 1) * 2 * M;
+      const uint32_t* src = pscr + size_t(nlo) * (2 * M);
+      for (int x = lane; x < nw; x += 32) stage[x] = src[x];
+      __syncwarp();
+      slo = nlo;
+    }
+    const uint32_t* wrow = stage + (r - slo) * (2 * M) + 2 * (col >> 5);
+    const int bit = col & 31;
+    const int v = int((wrow[0] >> bit) & 1u) | (int((wrow[1] >> bit) & 1u) << 1);
+    if (v == 1 && i > 0 && j > 0) {
+      const uint8_t a = S.s1[i - 1], b = S.s2[j - 1];
+      const int rp = swap ? i - 1 : j - 1;
+      const uint8_t cn = swap ? b : a, rn = swap ? a : b;
+      if (lane == 0) S.tcode[rp] = uint8_t((unsigned(cn) - 1u) * 4u + (unsigned(rn) - 1u));
+      ham += (a != b) ? 1u : 0u;
+      if (dbg0 && lane == 0) {
+        dbg0[alen] = swap ? b : a;
+        dbg1[alen] = swap ? a : b;
+      }
+      --i;
+      --j;
+    } else if (v == 2 && j > 0) {
+      if (dbg0 && lane == 0) {
+        dbg0[alen] = swap ? S.s2[j - 1] : uint8_t('-');
+        dbg1[alen] = swap ? uint8_t('-') : S.s2[j - 1];
+      }
+      --j;
+    } else if (v == 3 && i > 0) {
+      if (dbg0 && lane == 0) {
+        dbg0[alen] = swap ? uint8_t('-') : S.s1[i - 1];
+        dbg1[alen] = swap ? S.s1[i - 1] : uint8_t('-');
+      }
+      --i;
+    } else {
+      ok = false;
+      break;
+    }
+    ++alen;
+  }
+  __syncwarp();
+  if (!ok) {
+    if (lane == 0) atomicOr(err_word, DERR_TRACEBACK);
+    return false;
+  }
+  if (dbg_len && lane == 0) *dbg_len = alen;
+  *ham_out = ham;
+  return true;
+}
+
+// Picks the register form when the pair's compressed width fits 128 columns.
+__device__ bool vec_align_any(int lane, const uint8_t* g1, int l1, const uint8_t* g2, int l2, int16_t match,
+                              int16_t mismatch, int16_t gap, int16_t egp, int band_in, const VecSmem& S,
+                              uint8_t* scratch, int ncol_bound, int nrow_bound, uint32_t* ham_out, uint32_t* err_word,
+                              uint8_t* dbg0, uint8_t* dbg1, uint32_t* dbg_len) {
+  const int len1 = min(l1, l2), len2 = max(l1, l2);
+  const int band = band_in < 0 ? len2 : band_in;
+  const int start_col = 1 + (min(band, len1) + 1) / 2;
+  const int ncol = 2 + start_col + min(band + len2 - len1, len2) / 2;
+  uint32_t* w = reinterpret_cast<uint32_t*>(scratch);
+  if (ncol <= 32)
+    return vec_align_reg<1>(lane, g1, l1, g2, l2, match, mismatch, gap, egp, band_in, S, w, nrow_bound, ham_out,
+                            err_word, dbg0, dbg1, dbg_len);
+  if (ncol <= 64)
+    return vec_align_reg<2>(lane, g1, l1, g2, l2, match, mismatch, gap, egp, band_in, S, w, nrow_bound, ham_out,
+                            err_word, dbg0, dbg1, dbg_len);
+  if (ncol <= 128)
+    return vec_align_reg<4>(lane, g1, l1, g2, l2, match, mismatch, gap, egp, band_in, S, w, nrow_bound, ham_out,
+                            err_word, dbg0, dbg1, dbg_len);
+  return vec_align_warp(lane, g1, l1, g2, l2, match, mismatch, gap, egp, band_in, S, scratch, ncol_bound, nrow_bound,
+                        ham_out, err_word, dbg0, dbg1, dbg_len);
+}
+
 // ---------------------------------------------------------------------------
 // K5: row-major ends-free / homopolymer aligner as an anti-diagonal wavefront
 // ---------------------------------------------------------------------------
@@ -798,11 +1144,15 @@ __device__ bool rm_dispatch(int lane, const uint8_t* g1, int len1, const uint8_t
 }
 
 // ---------------------------------------------------------------------------
-// Persistent NW kernels over the queues filled by k_screen
+// Pairs that passed the screen (one warp per pair, grid-stride over the queue):
+// ordered-k-mer distance (src/kmers.rs:314-328; equal windows <=> equal k-mer
+// codes for ACGT input), method choice (src/nwalign.rs:1324-1403), then the
+// gapless alignment or the vectorized / row-major aligner, then lambda.
 // ---------------------------------------------------------------------------
-template <bool VEC>
-__global__ void __launch_bounds__(kNwWarps * 32) k_nw(CompareLaunch L) {
+__global__ void __launch_bounds__(kNwWarps * 32) k_align(CompareLaunch L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const uint32_t count = *(volatile uint32_t*)&L.queue_counts[4];
+  if (blockIdx.x * kNwWarps >= count) return;  // nothing queued for this block
   const KParams& kp = L.kp;
   double* err_s = reinterpret_cast<double*>(smem_raw);
   const int nerr = 16 * kp.ncol;
@@ -811,25 +1161,16 @@ __global__ void __launch_bounds__(kNwWarps * 32) k_nw(CompareLaunch L) {
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int gw = blockIdx.x * kNwWarps + wib;
   const int kb = rm_kbound(L.geom.rm_pairs);
+  unsigned char* wbase = smem_raw + err_bytes + size_t(wib) * align_smem_per_warp(L.geom);
+  const VecSmem VS = carve_vec(wbase, L.geom.lmax, L.geom.vec_ncol);
+  const RmSmem RS = carve_rm(wbase, L.geom.lmax, kb);
+  const size_t scr_stride = L.geom.vec_scratch > L.geom.rm_scratch ? L.geom.vec_scratch : L.geom.rm_scratch;
+  uint8_t* scratch = L.nw_scratch + size_t(gw) * scr_stride;
   __syncthreads();
-  VecSmem VS;
-  RmSmem RS;
-  if (VEC) {
-    VS = carve_vec(smem_raw + err_bytes + size_t(wib) * nw_smem_per_warp_vec(L.geom), L.geom.lmax, L.geom.vec_ncol);
-  } else {
-    RS = carve_rm(smem_raw + err_bytes + size_t(wib) * nw_smem_per_warp_rm(L.geom), L.geom.lmax, kb);
-  }
-  const size_t scr_bytes = VEC ? L.geom.vec_scratch : L.geom.rm_scratch;
-  uint8_t* scratch = L.nw_scratch + size_t(gw) * scr_bytes;
-  const uint32_t* queue = VEC ? L.queue_vec : L.queue_rm;
-  uint32_t* taken = &L.queue_counts[VEC ? 2 : 3];
-  const uint32_t count = *(volatile uint32_t*)&L.queue_counts[VEC ? 0 : 1];
-  for (;;) {
-    uint32_t slot = 0;
-    if (lane == 0) slot = atomicAdd(taken, 1u);
-    slot = __shfl_sync(FULL, slot, 0);
-    if (slot >= count) break;
-    const uint32_t item = queue[slot];
+  const int k = kp.kmer_size;
+  const uint32_t warps_total = gridDim.x * kNwWarps;
+  for (uint32_t slot = uint32_t(gw); slot < count; slot += warps_total) {
+    const uint32_t item = L.queue_pass[slot];
     const uint32_t t = find_task(L.task_prefix, L.ntask, item);
     const TaskDev T = L.tasks[t];
     const uint32_t g = T.base + (item - L.task_prefix[t]);
@@ -837,29 +1178,64 @@ __global__ void __launch_bounds__(kNwWarps * 32) k_nw(CompareLaunch L) {
     const int lc = int(L.pool.len[c]), lg = int(L.pool.len[g]);
     const uint8_t* sc = L.pool.seq + L.pool.off[c];
     const uint8_t* sg = L.pool.seq + L.pool.off[g];
+    const double kdist = L.pool.res_lambda[g];
+    double kodist = -1.0;
+    const int minl = lc < lg ? lc : lg;
+    const bool want_kod = kp.use_kmers && kp.gapless && lc == lg;
     uint32_t ham = 0;
-    bool ok;
-    uint8_t* tcode;
-    uint16_t* fidx;
-    uint8_t method;
-    if (VEC) {
-      ok = vec_align_warp(lane, sc, lc, sg, lg, int16_t(kp.match), int16_t(kp.mismatch), int16_t(kp.gap), 0, kp.band,
-                          VS, scratch, L.geom.vec_ncol, L.geom.vec_nrow, &ham, L.err_word, nullptr, nullptr, nullptr);
-      tcode = VS.tcode;
-      fidx = VS.fidx;
-      method = AM_VECTORIZED;
-    } else {
-      const bool homo = kp.homo_gap != kp.gap && kp.homo_gap <= 0;
-      ok = rm_dispatch(lane, sc, lc, sg, lg, kp, homo, kb, RS, reinterpret_cast<uint32_t*>(scratch), &ham, L.err_word,
-                       nullptr, nullptr, nullptr);
-      tcode = RS.tcode;
-      fidx = RS.fidx;
-      method = homo ? AM_HOMO : AM_ENDSFREE;
+    if (want_kod || kp.band == 0) {
+      const int klen = lc - (k - 1);
+      const uint32_t kmask = (k >= 32) ? 0xffffffffu : ((1u << k) - 1u);
+      uint32_t eq = 0;
+      uint32_t cur = mismatch_word(sc, sg, 0, minl, lane);
+      for (int b = 0; b < minl; b += 32) {
+        const uint32_t nxt = mismatch_word(sc, sg, b + 32, minl, lane);
+        ham += __popc(cur);
+        if (want_kod) {
+          const unsigned long long both = (static_cast<unsigned long long>(nxt) << 32) | cur;
+          const int j = b + lane;
+          const bool ok = j < klen && ((uint32_t(both >> lane) & kmask) == 0u);
+          eq += __popc(__ballot_sync(FULL, ok));
+        }
+        cur = nxt;
+      }
+      if (want_kod && klen > 0) kodist = 1.0 - double(eq) / double(klen);
     }
+    const bool gapless = kp.band == 0 || (kp.gapless && fabs(kodist - kdist) < DBL_EPSILON);
+    bool ok = true;
+    uint8_t method;
+    uint8_t* tcode = VS.tcode;
+    uint16_t* fidx = VS.fidx;
+    if (gapless) {
+      // raw position p aligns to center position p while p < len(center)
+      for (int p = lane; p < lg; p += 32) {
+        const unsigned r = sg[p];
+        const unsigned code = (p < lc) ? (unsigned(sc[p]) - 1u) * 4u + (r - 1u) : (r - 1u) * 5u;
+        const bool valid = r >= 1u && r <= 4u && (p >= lc || (sc[p] >= 1 && sc[p] <= 4));
+        tcode[p] = uint8_t(valid ? code : 255u);
+      }
+      method = AM_GAPLESS;
+    } else {
+      const bool use_homo = kp.homo_gap != kp.gap && kp.homo_gap <= 0;
+      const bool vec = kp.vectorized && lc <= 3500 && lg <= 3500 && !use_homo;
+      if (vec) {
+        ok = vec_align_any(lane, sc, lc, sg, lg, int16_t(kp.match), int16_t(kp.mismatch), int16_t(kp.gap), 0,
+                           kp.band, VS, scratch, L.geom.vec_ncol, L.geom.vec_nrow, &ham, L.err_word, nullptr,
+                           nullptr, nullptr);
+        method = AM_VECTORIZED;
+      } else {
+        ok = rm_dispatch(lane, sc, lc, sg, lg, kp, use_homo, kb, RS, reinterpret_cast<uint32_t*>(scratch), &ham,
+                         L.err_word, nullptr, nullptr, nullptr);
+        tcode = RS.tcode;
+        fidx = RS.fidx;
+        method = use_homo ? AM_HOMO : AM_ENDSFREE;
+      }
+    }
+    __syncwarp();
     double lam = 0.0;
     if (ok) {
       const uint8_t* qg = L.pool.qual ? L.pool.qual + L.pool.off[g] : nullptr;
-      bool bad = build_fidx(lane, tcode, qg, lg, kp.ncol, kp.use_quals, fidx);
+      const bool bad = build_fidx(lane, tcode, qg, lg, kp.ncol, kp.use_quals, fidx);
       __syncwarp();
       if (bad) {
         if (lane == 0) atomicOr(L.err_word, DERR_LAMBDA);
@@ -879,27 +1255,33 @@ __global__ void __launch_bounds__(kNwWarps * 32) k_nw(CompareLaunch L) {
 // ---------------------------------------------------------------------------
 // K7: ordered store (one CTA per task)
 // ---------------------------------------------------------------------------
+// Each CTA owns kStoreSpan consecutive raws of one task; its stored comps go
+// to that span's own segment of the task's output (so concatenating segments
+// in order gives ascending raw order) with a per-CTA count and counters.
 __global__ void __launch_bounds__(1024) k_store(CompareLaunch L) {
-  __shared__ uint32_t warp_cnt[32];
+  constexpr int IPT = kStoreSpan / 1024;
+  __shared__ uint32_t warp_off[32];
   __shared__ uint32_t ctr[TC_NCOUNTERS];
-  const uint32_t t = blockIdx.x;
+  const uint32_t blk = blockIdx.x;
+  const uint32_t t = L.store_task[blk];
+  const uint32_t span0 = L.store_chunk[blk] * uint32_t(kStoreSpan);
   const TaskDev T = L.tasks[t];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if (threadIdx.x < TC_NCOUNTERS) ctr[threadIdx.x] = 0;
   __syncthreads();
   uint32_t c_scr = 0, c_al = 0, c_sh = 0, c_gl = 0, c_ve = 0, c_ho = 0, c_ef = 0;
-  uint32_t running = 0;
-  for (uint32_t b = 0; b < T.n; b += blockDim.x) {
-    const uint32_t r = b + threadIdx.x;
-    const bool valid = r < T.n;
-    bool store = false;
-    double lam = 0.0;
-    uint32_t ham = 0;
-    if (valid) {
+  const uint32_t r0 = span0 + threadIdx.x * IPT;
+  uint32_t flags = 0;
+  double lam[IPT];
+  uint32_t ham[IPT];
+#pragma unroll
+  for (int q = 0; q < IPT; ++q) {
+    lam[q] = 0.0;
+    ham[q] = 0;
+    const uint32_t r = r0 + q;
+    if (r < T.n) {
       const uint32_t g = T.base + r;
       const uint8_t st = L.pool.res_status[g];
-      lam = L.pool.res_lambda[g];
-      ham = L.pool.res_ham[g];
       const uint8_t outcome = st & 3u, meth = st >> 2;
       c_scr += outcome != ST_SKIPPED;
       c_al += outcome == ST_ALIGNED;
@@ -908,38 +1290,47 @@ __global__ void __launch_bounds__(1024) k_store(CompareLaunch L) {
       c_ve += meth == AM_VECTORIZED;
       c_ho += meth == AM_HOMO;
       c_ef += meth == AM_ENDSFREE;
+      lam[q] = L.pool.res_lambda[g];
+      ham[q] = L.pool.res_ham[g];
       const double e = L.pool.e_minmax[g];
-      if (__dmul_rn(lam, T.total_reads) > e) {
-        store = true;
-        const double ne = __dmul_rn(lam, double(T.center_reads));
+      if (__dmul_rn(lam[q], T.total_reads) > e) {
+        flags |= 1u << q;
+        const double ne = __dmul_rn(lam[q], double(T.center_reads));
         if (ne > e) L.pool.e_minmax[g] = ne;
       }
-      if (g == T.center) L.task_self[t] = lam;
+      if (g == T.center) L.task_self[t] = lam[q];
     }
-    const uint32_t bal = __ballot_sync(FULL, store);
-    if (lane == 0) warp_cnt[w] = __popc(bal);
-    __syncthreads();
-    if (w == 0) {
-      uint32_t v = lane < nw ? warp_cnt[lane] : 0u;
-      uint32_t incl = v;
-      for (int d = 1; d < 32; d <<= 1) {
-        uint32_t y = __shfl_up_sync(FULL, incl, d);
-        if (lane >= d) incl += y;
-      }
-      if (lane < nw) warp_cnt[lane] = incl - v;
-      const uint32_t tot = __shfl_sync(FULL, incl, 31);
-      if (lane == 0) ctr[TC_STORED] = tot;  // this chunk's total, read below
+  }
+  const uint32_t cnt = __popc(flags);
+  uint32_t incl = cnt;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t y = __shfl_up_sync(FULL, incl, d);
+    if (lane >= d) incl += y;
+  }
+  if (lane == 31) warp_off[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    const uint32_t v = lane < nw ? warp_off[lane] : 0u;
+    uint32_t wi = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t y = __shfl_up_sync(FULL, wi, d);
+      if (lane >= d) wi += y;
     }
-    __syncthreads();
-    if (store) {
-      const uint32_t pos = running + warp_cnt[w] + __popc(bal & ((1u << lane) - 1u));
-      const uint32_t o = T.out_off + pos;
-      L.comp_index[o] = r;
-      L.comp_lambda[o] = lam;
-      L.comp_ham[o] = (ham == 0xffffffffu) ? 0u : ham;
+    if (lane < nw) warp_off[lane] = wi - v;
+    if (lane == 31) ctr[TC_STORED] = wi;
+  }
+  __syncthreads();
+  uint32_t pos = warp_off[w] + (incl - cnt);
+#pragma unroll
+  for (int q = 0; q < IPT; ++q) {
+    if (flags & (1u << q)) {
+      const uint32_t o = T.out_off + span0 + pos++;
+      L.comp_index[o] = r0 + q;
+      L.comp_lambda[o] = lam[q];
+      L.comp_ham[o] = (ham[q] == 0xffffffffu) ? 0u : ham[q];
     }
-    running += ctr[TC_STORED];
-    __syncthreads();
   }
   c_scr = __reduce_add_sync(FULL, c_scr);
   c_al = __reduce_add_sync(FULL, c_al);
@@ -958,12 +1349,7 @@ __global__ void __launch_bounds__(1024) k_store(CompareLaunch L) {
     atomicAdd(&ctr[TC_ENDSFREE], c_ef);
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    ctr[TC_STORED] = running;
-    L.task_nstored[t] = running;
-  }
-  __syncthreads();
-  if (threadIdx.x < TC_NCOUNTERS) L.task_counters[size_t(t) * TC_NCOUNTERS + threadIdx.x] = ctr[threadIdx.x];
+  if (threadIdx.x < TC_NCOUNTERS) L.blk_counters[size_t(blk) * TC_NCOUNTERS + threadIdx.x] = ctr[threadIdx.x];
 }
 
 static int g_sm_count = 0;
@@ -979,28 +1365,25 @@ static int sm_count() {
 
 void launch_compare(const CompareLaunch& L, cudaStream_t st, cudaEvent_t* ev) {
   if (L.total_items == 0) return;
-  const size_t err_bytes = err_smem_bytes(L.kp.ncol);
-  const size_t screen_smem = err_bytes + size_t(kScreenWarps) * screen_smem_per_warp(L.pool.maxlen);
-  if (screen_smem > 48 * 1024)
-    cudaFuncSetAttribute(k_screen, cudaFuncAttributeMaxDynamicSharedMemorySize, int(screen_smem));
   const int sms = sm_count();
-  uint32_t blocks = (L.total_items + kScreenWarps - 1) / kScreenWarps;
+  uint32_t blocks = (L.total_items + kScreenWarps * 32 - 1) / (kScreenWarps * 32);
   const uint32_t cap = uint32_t(sms) * 8u;
   if (blocks > cap) blocks = cap;
   if (ev) cudaEventRecord(ev[0], st);
-  k_screen<<<blocks, kScreenWarps * 32, screen_smem, st>>>(L);
+  switch (L.kp.kmer_size) {
+    case 3: k_screen<3><<<blocks, kScreenWarps * 32, 0, st>>>(L); break;
+    case 4: k_screen<4><<<blocks, kScreenWarps * 32, 0, st>>>(L); break;
+    case 5: k_screen<5><<<blocks, kScreenWarps * 32, 0, st>>>(L); break;
+    case 6: k_screen<6><<<blocks, kScreenWarps * 32, 0, st>>>(L); break;
+    default: k_screen<7><<<blocks, kScreenWarps * 32, 0, st>>>(L); break;
+  }
   if (ev) cudaEventRecord(ev[1], st);
-  const int nw_blocks = L.geom.nwarps / kNwWarps;
-  const size_t vsm = err_bytes + size_t(kNwWarps) * nw_smem_per_warp_vec(L.geom);
-  if (vsm > 48 * 1024) cudaFuncSetAttribute(k_nw<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(vsm));
-  k_nw<true><<<nw_blocks, kNwWarps * 32, vsm, st>>>(L);
+  const size_t asm_ = err_smem_bytes(L.kp.ncol) + size_t(kNwWarps) * align_smem_per_warp(L.geom);
+  if (asm_ > 48 * 1024) cudaFuncSetAttribute(k_align, cudaFuncAttributeMaxDynamicSharedMemorySize, int(asm_));
+  k_align<<<L.geom.nwarps / kNwWarps, kNwWarps * 32, asm_, st>>>(L);
   if (ev) cudaEventRecord(ev[2], st);
-  const size_t rsm = err_bytes + size_t(kNwWarps) * nw_smem_per_warp_rm(L.geom);
-  if (rsm > 48 * 1024) cudaFuncSetAttribute(k_nw<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(rsm));
-  k_nw<false><<<nw_blocks, kNwWarps * 32, rsm, st>>>(L);
+  if (L.do_store) k_store<<<L.nstore_blocks, 1024, 0, st>>>(L);
   if (ev) cudaEventRecord(ev[3], st);
-  if (L.do_store) k_store<<<L.ntask, 1024, 0, st>>>(L);
-  if (ev) cudaEventRecord(ev[4], st);
 }
 
 // ---------------------------------------------------------------------------
@@ -1023,9 +1406,9 @@ __global__ void __launch_bounds__(kNwWarps * 32) k_align_debug(int which, const 
   const uint8_t* b = s2cat + off2[pair];
   if (which == 0) {
     VecSmem S = carve_vec(smem_raw + size_t(wib) * nw_smem_per_warp_vec(geom), geom.lmax, geom.vec_ncol);
-    vec_align_warp(lane, a, int(len1[pair]), b, int(len2[pair]), int16_t(kp.match), int16_t(kp.mismatch),
-                   int16_t(kp.gap), int16_t(end_gap), kp.band, S, my_scr, geom.vec_ncol, geom.vec_nrow, &ham, err_word,
-                   al0 + aloff[pair], al1 + aloff[pair], alen + pair);
+    vec_align_any(lane, a, int(len1[pair]), b, int(len2[pair]), int16_t(kp.match), int16_t(kp.mismatch),
+                  int16_t(kp.gap), int16_t(end_gap), kp.band, S, my_scr, geom.vec_ncol, geom.vec_nrow, &ham, err_word,
+                  al0 + aloff[pair], al1 + aloff[pair], alen + pair);
   } else {
     const int kb = rm_kbound(geom.rm_pairs);
     RmSmem S = carve_rm(smem_raw + size_t(wib) * nw_smem_per_warp_rm(geom), geom.lmax, kb);

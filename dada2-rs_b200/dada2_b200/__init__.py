@@ -27,7 +27,7 @@ __all__ = ["AlignParams", "DadaParams", "CompareContext", "dada_uniques", "dada_
            "ResidentBatch", "PackedBatch", "align_pairs", "stats_reset", "stats_timing", "stats_read",
            "DgpuError", "InvalidInput", "device_count", "METHOD_NAMES", "KERNEL_NAMES"]
 
-KERNEL_NAMES = ["profiles", "screen", "nw_vectorized", "nw_rowmajor", "store"]
+KERNEL_NAMES = ["profiles", "screen", "align", "store"]
 
 METHOD_NAMES = {0: "none", 1: "gapless", 2: "vectorized", 3: "homo", 4: "endsfree"}
 COUNTER_KEYS = ["nalign", "compare_calls", "cmp_scanned", "screened", "aligned", "stored",

@@ -48,7 +48,7 @@ class DadaParamsC(C.Structure):
 
 
 class KernelStatsC(C.Structure):
-    _fields_ = [("launches", C.c_uint64 * 5), ("ms", C.c_double * 5), ("rounds", C.c_uint64),
+    _fields_ = [("launches", C.c_uint64 * 4), ("ms", C.c_double * 4), ("rounds", C.c_uint64),
                 ("compares", C.c_uint64), ("screened", C.c_uint64), ("screen_bytes", C.c_uint64)]
 
 

@@ -102,13 +102,14 @@ typedef struct dgpu_result dgpu_result;
 typedef struct dgpu_batch dgpu_batch;
 
 /* Process-wide kernel accounting (for benchmarks). Index k: 0 profiles,
- * 1 screen, 2 vectorized NW, 3 row-major NW, 4 store. ms[] is filled only
+ * 1 screen, 2 align (ordered-k-mer distance, gapless or NW alignment and
+ * lambda for the pairs that passed the screen), 3 store. ms[] is filled only
  * while timing is enabled (CUDA events around each kernel on its stream).
  * screen_bytes = algorithmic bytes of the screen: 4^k profile bytes per
  * non-skipped compare plus 16 bytes of per-raw metadata per compare. */
 typedef struct {
-  uint64_t launches[5];
-  double ms[5];
+  uint64_t launches[4];
+  double ms[4];
   uint64_t rounds, compares, screened, screen_bytes;
 } dgpu_kernel_stats;
 

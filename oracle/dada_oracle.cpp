@@ -1371,19 +1371,28 @@ static void run_dada(B& bb, std::vector<Raw>&& raws, const DadaParams& params, c
              params.min_abund);
   size_t max_clust = params.max_clust == 0 ? bb.raws.size() : params.max_clust;
   ShuffleCarry carry;
+  auto since = [](std::chrono::steady_clock::time_point a) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - a).count();
+  };
   while (bb.clusters.size() < max_clust) {
+    t0 = std::chrono::steady_clock::now();
     int64_t newi = b_bud_incremental(bb, params.min_fold, params.min_hamming, params.min_abund);
+    rs.t_bud += since(t0);
     if (newi < 0) break;
     t0 = std::chrono::steady_clock::now();
     st = b_compare_parallel(bb, size_t(newi), err, ncol, params.align, params.greedy, params.nthreads);
     accumulate(rs, st, bb.raws.size());
-    rs.t_compare += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    rs.t_compare += since(t0);
+    t0 = std::chrono::steady_clock::now();
     index_add_cluster(cand, bb, size_t(newi));
     ShuffleResult sr = b_shuffle_converge(bb, cand, 10, carry);
     rs.shuffle_calls += sr.calls;
     rs.shuffle_moves += sr.moves;
+    rs.t_shuffle += since(t0);
+    t0 = std::chrono::steady_clock::now();
     b_p_update(bb, params.greedy, params.detect_singletons, params.min_fold, params.min_hamming,
                params.min_abund);
+    rs.t_pupdate += since(t0);
   }
 }
 

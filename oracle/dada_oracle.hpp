@@ -280,6 +280,7 @@ struct DadaRunStats {
   uint64_t gapless = 0, vectorized = 0, homo = 0, endsfree = 0;
   uint64_t shuffle_calls = 0, shuffle_moves = 0;
   double t_compare = 0.0, t_total = 0.0;  // seconds
+  double t_shuffle = 0.0, t_pupdate = 0.0, t_bud = 0.0;
 };
 struct DadaResult {
   std::vector<ClusterSummary> clusters;

@@ -377,8 +377,8 @@ void orc_c_dada_fill(void* h, const orc_dada_out* o) {
   std::copy(c, c + 16, o->counters);
   o->times[0] = s.t_compare;
   o->times[1] = s.t_total;
-  o->times[2] = 0.0;
-  o->times[3] = 0.0;
+  o->times[2] = s.t_shuffle + s.t_pupdate + s.t_bud;
+  o->times[3] = s.t_pupdate;
 }
 
 }  // extern "C"

@@ -269,3 +269,31 @@ def test_invalid_inputs_are_rejected_like_the_reference():
         D.dada_uniques(["ACGT", "ACGTACGTAA"], [3, 2], err, 41)
     with pytest.raises(D.InvalidInput):
         D.dada_uniques([], [], err, 41)
+
+
+def test_resident_batch_runs_repeat_identically():
+    ws = [synth.small_illumina(60 + i, nvariants=5, nreads=900 + 400 * i, L=110) for i in range(3)]
+    err, ncol = ws[0].err, ws[0].ncol
+    samples = [w.samples[0] for w in ws]
+    with D.ResidentBatch(samples, err, ncol, D.DadaParams(host_threads=4)) as rb:
+        first = rb.run()
+        second = rb.run()
+    for s, a, b in zip(samples, first, second):
+        assert_same_dada(a, b)
+        want = O.dada(s.seqs, s.abund, err, ncol, O.DadaParams(nthreads=4), quals=s.quals)
+        assert_same_dada(a, want)
+
+
+def test_kernel_stats_count_launches():
+    w = synth.small_illumina(71, nvariants=4, nreads=800, L=100)
+    s = w.samples[0]
+    D.stats_reset()
+    D.stats_timing(True)
+    r = D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, D.DadaParams(), quals=s.quals)
+    D.stats_timing(False)
+    st = D.stats_read()
+    assert st["rounds"] == r["counters"]["compare_calls"]
+    assert st["launches"]["screen"] == st["rounds"] and st["launches"]["profiles"] == 1
+    assert st["compares"] == r["counters"]["cmp_scanned"]
+    assert st["ms"]["screen"] > 0.0
+    assert len(D.stats_latencies()) == st["rounds"]
