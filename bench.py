@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--config", type=int, default=1)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
+                    help="weak: every rank denoises its own 40-sample batch; strong: the 40 samples are sharded")
     return ap.parse_args()
 
 
@@ -228,8 +230,12 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     import dada2_b200 as D
+    from dada2_b200 import multi
 
-    w = load_workload(args.config, rank)
+    w = load_workload(args.config, 0 if args.scaling == "strong" else rank)
+    if args.scaling == "strong" and world > 1:
+        mine = multi.shard_samples([len(s.seqs) for s in w.samples], rank, world)
+        w.samples = [w.samples[i] for i in mine]
     params = dada_params(w)
     pb = D.PackedBatch(w.samples)
     batch = D.ResidentBatch(w.samples, w.err, w.ncol, params, device=local, packed=pb)
@@ -262,15 +268,7 @@ def main():
     lat = D.stats_latencies()
     dt = ev0.elapsed_time(ev1) / 1e3
     nclust = [r["nclust"] for r in res]
-    t_max = dt
-    comps_all = comps
-    if world > 1:
-        t = torch.tensor([dt], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        t_max = float(t.item())
-        c = torch.tensor([float(comps)], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(c)
-        comps_all = int(c.item())
+    t_max, comps_all = multi.reduce_run(dt, comps, device="cuda")
     value = comps_all / t_max
 
     # ---- timed: end to end through the C ABI with host buffers ----
@@ -287,12 +285,8 @@ def main():
     e1.record()
     torch.cuda.synchronize()
     barrier()
-    e2e_dt = e0.elapsed_time(e1) / 1e3
-    if world > 1:
-        t = torch.tensor([e2e_dt], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_dt = float(t.item())
-    e2e = e2e_comps * world / e2e_dt
+    e2e_dt, e2e_comps_all = multi.reduce_run(e0.elapsed_time(e1) / 1e3, e2e_comps, device="cuda")
+    e2e = e2e_comps_all / e2e_dt
 
     # ---- plain single-sample path (rank 0 only; one pass) ----
     plain = None
@@ -330,7 +324,7 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "scaling": args.scaling, "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": w.name, "samples": len(w.samples), "uniques": int(sum(len(s.seqs) for s in w.samples)),
                    "clusters": int(sum(nclust)), "compares_per_step": comps // max(args.steps, 1),
                    "parallelism": f"samples sharded over {world} GPU(s), no collective",
@@ -345,6 +339,9 @@ def main():
         "latency_ms": {"p50": float(np.percentile(lat, 50)) if len(lat) else None,
                        "p99": float(np.percentile(lat, 99)) if len(lat) else None,
                        "unit": "per batched compare call"},
+        "host_phases_s_per_step": {"critical_sample": float(max(r["times"][2] for r in res)),
+                                   "all_samples": float(sum(r["times"][2] for r in res)),
+                                   "note": "shuffle + p-update + bud on the host, last timed step"},
         "gpu_launches": launches,
         "clocks": clk,
         "plain": plain,

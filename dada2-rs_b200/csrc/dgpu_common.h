@@ -24,6 +24,7 @@ struct PoolDev {
   const uint32_t* off;
   const uint32_t* len;
   const uint8_t* kmer8;   // nraw x 4^k saturating u8 counts
+  const uint8_t* sat;     // per raw: some k-mer count reached 255
   const uint32_t* reads;
   const uint8_t* lock;
   double* e_minmax;
@@ -108,7 +109,7 @@ __host__ __device__ inline size_t align_smem_per_warp(const NwGeom& g) {
 
 // ---- launchers (dgpu_kernels.cu) ----
 void launch_profiles(const uint8_t* seq, const uint32_t* off, const uint32_t* len, uint32_t nraw,
-                     int k, uint8_t* kmer8, cudaStream_t st);
+                     int k, uint8_t* kmer8, uint8_t* sat, cudaStream_t st);
 // Runs screen/gapless/lambda, both NW kernels and the ordered store for `ntask`
 // tasks; `task_prefix` holds ntask+1 running raw counts.
 struct CompareLaunch {

@@ -14,6 +14,7 @@
 #include <deque>
 #include <functional>
 #include <limits>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -135,7 +136,7 @@ struct Pool {
   KParams kp{};
   NwGeom geom{};
   int sms = 148;
-  DBuf<uint8_t> seq, qual, kmer8, lock, status;
+  DBuf<uint8_t> seq, qual, kmer8, sat, lock, status;
   DBuf<uint32_t> off, len, reads, ham, queue_vec, queue_rm, queue_pass, queue_counts, err_word;
   DBuf<double> e_minmax, err, lambda;
   DBuf<uint8_t> scratch;
@@ -211,6 +212,7 @@ struct Pool {
     TRY(err_word.alloc(1));
     TRY(err.alloc(size_t(16) * kp.ncol));
     TRY(kmer8.alloc(kp.use_kmers ? size_t(n) * nk : 1));
+    TRY(sat.alloc(n));
     TRY(comp_index.alloc(n));
     TRY(comp_ham.alloc(n));
     TRY(comp_lambda.alloc(n));
@@ -229,7 +231,7 @@ struct Pool {
     CUDA_TRY(cudaMemsetAsync(err_word.p, 0, 4, st));
     TRY(reset_e_minmax());
     if (kp.use_kmers) {
-      launch_profiles(seq.p, off.p, len.p, n, kp.kmer_size, kmer8.p, st);
+      launch_profiles(seq.p, off.p, len.p, n, kp.kmer_size, kmer8.p, sat.p, st);
       std::lock_guard<std::mutex> g(g_stats.mu);
       g_stats.s.launches[0] += 1;
     }
@@ -275,6 +277,7 @@ struct Pool {
     v.off = off.p;
     v.len = len.p;
     v.kmer8 = kmer8.p;
+    v.sat = sat.p;
     v.reads = reads.p;
     v.lock = lock.p;
     v.e_minmax = e_minmax.p;
@@ -424,6 +427,89 @@ struct Pool {
     return 0;
   }
 };
+
+// ---------------------------------------------------------------------------
+// Fork-join helpers for the large loops inside one sample's host phases. The
+// calling thread always works on its own loop, so a busy pool only means less
+// help, never a wait on unstarted work.
+// ---------------------------------------------------------------------------
+class Helpers {
+ public:
+  static Helpers& get() {
+    static Helpers h(std::max(1, int(std::thread::hardware_concurrency()) / 2));
+    return h;
+  }
+  // fn(chunk_index, lo, hi) over [0, n) in chunks of `grain`.
+  void parallel_for(size_t n, size_t grain, const std::function<void(size_t, size_t, size_t)>& fn) {
+    const size_t nch = (n + grain - 1) / grain;
+    if (nch <= 1 || th_.empty()) {
+      for (size_t c = 0; c < nch; ++c) fn(c, c * grain, std::min(n, (c + 1) * grain));
+      return;
+    }
+    auto task = std::make_shared<Task>();
+    task->fn = &fn;
+    task->n = n;
+    task->grain = grain;
+    task->nch = nch;
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      q_.push_back(task);
+    }
+    cv_.notify_all();
+    run(*task);
+    while (task->done.load(std::memory_order_acquire) < nch) std::this_thread::yield();
+  }
+  ~Helpers() {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : th_) t.join();
+  }
+
+ private:
+  struct Task {
+    const std::function<void(size_t, size_t, size_t)>* fn = nullptr;
+    size_t n = 0, grain = 1, nch = 0;
+    std::atomic<size_t> next{0}, done{0};
+  };
+  explicit Helpers(int n) {
+    for (int t = 0; t < n; ++t) th_.emplace_back([this] { loop(); });
+  }
+  static void run(Task& t) {
+    for (;;) {
+      const size_t c = t.next.fetch_add(1);
+      if (c >= t.nch) break;
+      (*t.fn)(c, c * t.grain, std::min(t.n, (c + 1) * t.grain));
+      t.done.fetch_add(1, std::memory_order_release);
+    }
+  }
+  void loop() {
+    for (;;) {
+      std::shared_ptr<Task> t;
+      {
+        std::unique_lock<std::mutex> g(mu_);
+        cv_.wait(g, [&] { return stop_ || !q_.empty(); });
+        if (stop_) return;
+        t = q_.front();
+        if (t->next.load() >= t->nch) {
+          q_.pop_front();
+          continue;
+        }
+      }
+      run(*t);
+    }
+  }
+  std::vector<std::thread> th_;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::deque<std::shared_ptr<Task>> q_;
+  bool stop_ = false;
+};
+
+static constexpr size_t kParMin = 8192;   // loops shorter than this stay serial
+static constexpr size_t kParGrain = 2048;
 
 // ---------------------------------------------------------------------------
 // Clustering state of one sample (containers.rs B/Bi/Raw, SoA)
@@ -587,36 +673,72 @@ struct SampleState {
   }
 
   // ---- pval.rs ----
+  // Bud candidate comparison of the cache scan: smaller p, then more reads;
+  // a scan in ascending position keeps the first of equals.
+  static bool better(const BudCand& c, const BudCand& m) {
+    return c.p < m.p || (c.p == m.p && c.reads > m.reads);
+  }
+
+  struct BudAcc {
+    bool have = false, havep = false;
+    BudCand bm{}, bmp{};
+  };
+
+  // Members [lo, hi) of cluster bi: reprice and fold into a local cache.
+  void reprice_range(const Cluster& bi, size_t lo, size_t hi, BudAcc& acc) {
+    const DadaConf& C = *conf;
+    const uint32_t bi_reads = bi.reads;
+    for (size_t r = lo; r < hi; ++r) {
+      const uint32_t raw = bi.raws[r];
+      const double pv = get_pA(reads[raw], prior[raw] != 0, rcomp[raw].lambda, rcomp[raw].hamming, bi_reads);
+      p[raw] = pv;
+      if (r == 0) continue;
+      if (reads[raw] < C.min_abund || rcomp[raw].hamming < C.min_hamming) continue;
+      const bool fold_ok = C.min_fold <= 1.0 || double(reads[raw]) >= C.min_fold * rcomp[raw].lambda * double(bi_reads);
+      if (!fold_ok) continue;
+      const BudCand cd{pv, reads[raw], uint32_t(r), raw};
+      if (!acc.have || better(cd, acc.bm)) {
+        acc.bm = cd;
+        acc.have = true;
+      }
+      if (prior[raw] && (!acc.havep || better(cd, acc.bmp))) {
+        acc.bmp = cd;
+        acc.havep = true;
+      }
+    }
+  }
+
   void p_update() {  // src/pval.rs:45-130
     const DadaConf& C = *conf;
     for (size_t i = 0; i < clusters.size(); ++i) {
       Cluster& bi = clusters[i];
       if (bi.update_e) {
-        const uint32_t bi_reads = bi.reads;
-        bool have = false, havep = false;
-        BudCand bm{}, bmp{};
-        for (size_t r = 0; r < bi.raws.size(); ++r) {
-          const uint32_t raw = bi.raws[r];
-          const double pv = get_pA(reads[raw], prior[raw] != 0, rcomp[raw].lambda, rcomp[raw].hamming, bi_reads);
-          p[raw] = pv;
-          if (r == 0) continue;
-          if (reads[raw] < C.min_abund || rcomp[raw].hamming < C.min_hamming) continue;
-          const bool fold_ok = C.min_fold <= 1.0 || double(reads[raw]) >= C.min_fold * rcomp[raw].lambda * double(bi_reads);
-          if (!fold_ok) continue;
-          const BudCand cd{pv, reads[raw], uint32_t(r), raw};
-          if (!have || pv < bm.p || (pv == bm.p && cd.reads > bm.reads)) {
-            bm = cd;
-            have = true;
-          }
-          if (prior[raw] && (!havep || pv < bmp.p || (pv == bmp.p && cd.reads > bmp.reads))) {
-            bmp = cd;
-            havep = true;
+        const size_t nm = bi.raws.size();
+        BudAcc acc;
+        if (nm < kParMin) {
+          reprice_range(bi, 0, nm, acc);
+        } else {
+          // chunk-local caches folded in chunk order: the same first-of-equals
+          // winner as one ascending scan
+          std::vector<BudAcc> part((nm + kParGrain - 1) / kParGrain);
+          Helpers::get().parallel_for(nm, kParGrain, [&](size_t c, size_t lo, size_t hi) {
+            reprice_range(bi, lo, hi, part[c]);
+          });
+          for (const BudAcc& a : part) {
+            if (a.have && (!acc.have || better(a.bm, acc.bm))) {
+              acc.bm = a.bm;
+              acc.have = true;
+            }
+            if (a.havep && (!acc.havep || better(a.bmp, acc.bmp))) {
+              acc.bmp = a.bmp;
+              acc.havep = true;
+            }
           }
         }
-        bi.has_bm = have;
-        bi.bm = bm;
-        bi.has_bmp = havep;
-        bi.bmp = bmp;
+        bi.has_bm = acc.have;
+        bi.bm = acc.bm;
+        bi.has_bmp = acc.havep;
+        bi.bmp = acc.bmp;
         bi.update_e = false;
       }
       if (C.greedy && bi.check_locks) {
@@ -647,7 +769,8 @@ struct SampleState {
   static double gamma_lr(double a, double x) {
     const double eps = 1e-15, big = 4503599627370496.0, big_inv = 2.22044604925031308085e-16;
     if (std::isnan(a) || std::isnan(x)) return std::numeric_limits<double>::quiet_NaN();
-    const double ax = a * std::log(x) - x - std::lgamma(a);
+    int sign_unused = 0;
+    const double ax = a * std::log(x) - x - lgamma_r(a, &sign_unused);
     if (ax < -709.78271289338399) return a < x ? 1.0 : 0.0;
     if (x <= 1.0 || x <= a) {
       double r = a, c = 1.0, ans = 1.0;
@@ -782,13 +905,64 @@ struct SampleState {
     return moves;
   }
 
-  void record_change(uint32_t raw, uint32_t new_ci) {  // src/cluster.rs:792-810
+  // src/cluster.rs:792-810. The dirty mark is an atomic test-and-set so the
+  // parallel passes below can share it; `out` receives clusters newly marked.
+  void record_change_to(uint32_t raw, uint32_t new_ci, std::vector<uint32_t>& out) {
     if (new_ci == compmax[raw].i) return;
     const uint32_t cur = raw_cluster[raw];
-    if (!dirty_cluster[cur]) {
-      dirty_cluster[cur] = 1;
-      dirty_list.push_back(cur);
+    if (!__atomic_exchange_n(&dirty_cluster[cur], uint8_t(1), __ATOMIC_RELAXED)) out.push_back(cur);
+  }
+  void record_change(uint32_t raw, uint32_t new_ci) { record_change_to(raw, new_ci, dirty_list); }
+
+  // Pass A2 over one changed cluster's comps [lo, hi) (src/cluster.rs:1177-1224).
+  void reconcile_a2(uint32_t ci, double rf, size_t lo, size_t hi, std::vector<uint32_t>& dirty_out) {
+    const std::vector<Comp>& cv = clusters[ci].comp;
+    for (size_t k = lo; k < hi; ++k) {
+      const Comp& cp = cv[k];
+      const uint32_t raw = cp.index;
+      if (in_affected[raw]) continue;
+      const double e = cp.lambda * rf;
+      if (compmax[raw].i == ci) {
+        emax[raw] = e;
+      } else if (e > emax[raw] || (e == emax[raw] && ci < compmax[raw].i)) {
+        emax[raw] = e;
+        record_change_to(raw, ci, dirty_out);
+        compmax[raw] = cp;
+      }
     }
+  }
+
+  // Pass B for affected raws [lo, hi): full candidate rescan (src/cluster.rs:1230-1247).
+  void reconcile_b(size_t lo, size_t hi, std::vector<uint32_t>& dirty_out) {
+    for (size_t k = lo; k < hi; ++k) {
+      const uint32_t raw = affected[k];
+      double be = -std::numeric_limits<double>::infinity();
+      Comp best;
+      for (const Cand& c : cand[raw]) {
+        const double e = c.lambda * double(clusters[c.ci].reads);
+        if (e > be) {
+          be = e;
+          best = Comp{c.ci, raw, c.lambda, c.hamming};
+        }
+      }
+      if (best.i != compmax[raw].i) record_change_to(raw, best.i, dirty_out);
+      compmax[raw] = best;
+      emax[raw] = be;
+      in_affected[raw] = 0;
+    }
+  }
+
+  // Runs fn over [0, n) serially or, for long loops, in parallel chunks whose
+  // newly dirtied clusters are appended in chunk order.
+  template <class F>
+  void par_dirty(size_t n, F&& fn) {
+    if (n < kParMin) {
+      fn(size_t(0), n, dirty_list);
+      return;
+    }
+    std::vector<std::vector<uint32_t>> loc((n + kParGrain - 1) / kParGrain);
+    Helpers::get().parallel_for(n, kParGrain, [&](size_t c, size_t lo, size_t hi) { fn(lo, hi, loc[c]); });
+    for (auto& v : loc) dirty_list.insert(dirty_list.end(), v.begin(), v.end());
   }
 
   void grow_to(size_t nc) {
@@ -851,47 +1025,40 @@ struct SampleState {
           reads_fell_list.push_back(uint32_t(ci));
         }
       }
+      // Pass A1: raws whose best cluster lost reads are queued for a rescan.
+      // Within one cluster's comps every raw is distinct, so long lists are
+      // split across threads; chunk results keep their order.
       for (uint32_t ci : reads_fell_list) {
-        for (const Comp& cp : clusters[ci].comp) {
-          if (compmax[cp.index].i == ci && !in_affected[cp.index]) {
-            in_affected[cp.index] = 1;
-            affected.push_back(cp.index);
+        const std::vector<Comp>& cv = clusters[ci].comp;
+        auto a1 = [&](size_t lo, size_t hi, std::vector<uint32_t>& out) {
+          for (size_t k = lo; k < hi; ++k) {
+            const uint32_t raw = cv[k].index;
+            if (compmax[raw].i == ci && !in_affected[raw]) {
+              in_affected[raw] = 1;
+              out.push_back(raw);
+            }
           }
+        };
+        if (cv.size() < kParMin) {
+          a1(0, cv.size(), affected);
+        } else {
+          std::vector<std::vector<uint32_t>> loc((cv.size() + kParGrain - 1) / kParGrain);
+          Helpers::get().parallel_for(cv.size(), kParGrain, [&](size_t c, size_t lo, size_t hi) { a1(lo, hi, loc[c]); });
+          for (auto& v : loc) affected.insert(affected.end(), v.begin(), v.end());
         }
       }
+      // Pass A2: changed clusters in ascending order.
       for (size_t ci = 0; ci < clusters.size(); ++ci) {
         const uint32_t nr = clusters[ci].reads;
         if (nr == reads_used[ci]) continue;
         const double rf = double(nr);
-        for (const Comp& cp : clusters[ci].comp) {
-          const uint32_t raw = cp.index;
-          if (in_affected[raw]) continue;
-          const double e = cp.lambda * rf;
-          if (compmax[raw].i == uint32_t(ci)) {
-            emax[raw] = e;
-          } else if (e > emax[raw] || (e == emax[raw] && uint32_t(ci) < compmax[raw].i)) {
-            emax[raw] = e;
-            record_change(raw, uint32_t(ci));
-            compmax[raw] = cp;
-          }
-        }
+        par_dirty(clusters[ci].comp.size(), [&](size_t lo, size_t hi, std::vector<uint32_t>& out) {
+          reconcile_a2(uint32_t(ci), rf, lo, hi, out);
+        });
         reads_used[ci] = nr;
       }
-      for (uint32_t raw : affected) {
-        double be = -std::numeric_limits<double>::infinity();
-        Comp best;
-        for (const Cand& c : cand[raw]) {
-          const double e = c.lambda * double(clusters[c.ci].reads);
-          if (e > be) {
-            be = e;
-            best = Comp{c.ci, raw, c.lambda, c.hamming};
-          }
-        }
-        if (best.i != compmax[raw].i) record_change(raw, best.i);
-        compmax[raw] = best;
-        emax[raw] = be;
-        in_affected[raw] = 0;
-      }
+      // Pass B: full rescans of the queued raws.
+      par_dirty(affected.size(), [&](size_t lo, size_t hi, std::vector<uint32_t>& out) { reconcile_b(lo, hi, out); });
       affected.clear();
       for (uint32_t ci : reads_fell_list) reads_fell[ci] = 0;
       reads_fell_list.clear();
@@ -1274,7 +1441,9 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
           SampleState& ss = S[sidx];
           auto th = Clock::now();
           ss.pending = ss.advance(size_t(ss.pending));
-          host_ns += int64_t(1e9 * secs(th, Clock::now()));
+          const double dh = secs(th, Clock::now());
+          ss.stats.t_host += dh;
+          host_ns += int64_t(1e9 * dh);
           std::lock_guard<std::mutex> g(mu);
           if (ss.pending >= 0) ready.push_back(sidx);
           else ++finished;
@@ -1290,7 +1459,6 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
   const double total = secs(t_start, Clock::now());
   for (auto& ss : S) {
     ss.stats.t_total = total;
-    ss.stats.t_host = double(host_ns.load()) * 1e-9;
     ss.stats.t_wait = wait;
   }
   return rc;

@@ -44,10 +44,12 @@ __device__ __forceinline__ uint32_t find_task(const uint32_t* prefix, uint32_t n
 // ---------------------------------------------------------------------------
 __global__ void k_profiles(const uint8_t* __restrict__ seq, const uint32_t* __restrict__ off,
                            const uint32_t* __restrict__ len, uint32_t nraw, int k,
-                           uint8_t* __restrict__ kmer8) {
+                           uint8_t* __restrict__ kmer8, uint8_t* __restrict__ sat) {
   extern __shared__ uint32_t cnt[];
+  __shared__ int any_sat;
   const int nk = 1 << (2 * k);
   for (uint32_t g = blockIdx.x; g < nraw; g += gridDim.x) {
+    if (threadIdx.x == 0) any_sat = 0;
     for (int t = threadIdx.x; t < nk; t += blockDim.x) cnt[t] = 0;
     __syncthreads();
     const uint8_t* s = seq + off[g];
@@ -67,22 +69,29 @@ __global__ void k_profiles(const uint8_t* __restrict__ seq, const uint32_t* __re
     }
     __syncthreads();
     uint32_t* out = reinterpret_cast<uint32_t*>(kmer8 + size_t(g) * size_t(nk));
+    int my_sat = 0;
     for (int t = threadIdx.x; t < nk / 4; t += blockDim.x) {
       uint32_t w = 0;
-      for (int b = 0; b < 4; ++b) w |= min(cnt[4 * t + b], 255u) << (8 * b);
+      for (int b = 0; b < 4; ++b) {
+        w |= min(cnt[4 * t + b], 255u) << (8 * b);
+        my_sat |= cnt[4 * t + b] >= 255u;
+      }
       out[t] = w;
     }
+    if (my_sat) any_sat = 1;
+    __syncthreads();
+    if (threadIdx.x == 0) sat[g] = uint8_t(any_sat);
     __syncthreads();
   }
 }
 
 void launch_profiles(const uint8_t* seq, const uint32_t* off, const uint32_t* len, uint32_t nraw, int k,
-                     uint8_t* kmer8, cudaStream_t st) {
+                     uint8_t* kmer8, uint8_t* sat, cudaStream_t st) {
   if (nraw == 0) return;
   size_t smem = size_t(4) << (2 * k);
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_profiles, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   int grid = int(nraw < 148u * 16u ? nraw : 148u * 16u);
-  k_profiles<<<grid, 256, smem, st>>>(seq, off, len, nraw, k, kmer8);
+  k_profiles<<<grid, 256, smem, st>>>(seq, off, len, nraw, k, kmer8, sat);
 }
 
 // ---------------------------------------------------------------------------
@@ -208,7 +217,7 @@ __global__ void __launch_bounds__(kScreenWarps * 32, 4) k_screen(CompareLaunch L
           }
           cur_c = cq[q];
         }
-        uint32_t dot = 0, ovf = 0;
+        uint32_t dot = 0;
 #pragma unroll 4
         for (int v = 0; v < VPL; ++v) {
           const int idx = lane + 32 * v;
@@ -220,22 +229,21 @@ __global__ void __launch_bounds__(kScreenWarps * 32, 4) k_screen(CompareLaunch L
           dot = __dp4a(m1, 0x01010101u, dot);
           dot = __dp4a(m2, 0x01010101u, dot);
           dot = __dp4a(m3, 0x01010101u, dot);
-          ovf |= __vcmpeq4(m0, 0xffffffffu) | __vcmpeq4(m1, 0xffffffffu) | __vcmpeq4(m2, 0xffffffffu) |
-                 __vcmpeq4(m3, 0xffffffffu);
         }
         dot = __reduce_add_sync(FULL, dot);
-        ovf = __reduce_or_sync(FULL, ovf);
-        if (lane == js[q]) {
-          mydot = dot;
-          myovf = ovf;
-        }
+        if (lane == js[q]) mydot = dot;
       }
     }
-    // Saturated k-mers (min == 255 somewhere): the exact u16 dot
-    // (src/nwalign.rs:1270-1277), one item at a time by the whole warp. Each
-    // window of the raw contributes 1 when its rank among equal windows of the
-    // raw is below the center's count of that k-mer.
-    uint32_t ovf_mask = __ballot_sync(FULL, need && myovf != 0);
+    // kmer_dist8 returns -1 (and the reference falls back to the exact u16
+    // distance, src/nwalign.rs:1270-1277) when some k-mer's min count is 255,
+    // which needs a saturated count in both profiles. Whenever both have one,
+    // the exact dot is taken instead: it equals the u8 dot when no min
+    // saturates, so the result is the reference's in every case. One item at a
+    // time by the whole warp: each window of the raw contributes 1 when its rank
+    // among equal windows of the raw is below the center's count of that k-mer.
+    const bool maybe_ovf = need && L.pool.sat[g] && L.pool.sat[c];
+    (void)myovf;
+    uint32_t ovf_mask = __ballot_sync(FULL, maybe_ovf);
     while (ovf_mask) {
       const int j = __ffs(ovf_mask) - 1;
       ovf_mask &= ovf_mask - 1;
@@ -1149,7 +1157,7 @@ __device__ bool rm_dispatch(int lane, const uint8_t* g1, int len1, const uint8_t
 // codes for ACGT input), method choice (src/nwalign.rs:1324-1403), then the
 // gapless alignment or the vectorized / row-major aligner, then lambda.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kNwWarps * 32) k_align(CompareLaunch L) {
+__global__ void __launch_bounds__(kNwWarps * 32, 4) k_align(CompareLaunch L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const uint32_t count = *(volatile uint32_t*)&L.queue_counts[4];
   if (blockIdx.x * kNwWarps >= count) return;  // nothing queued for this block

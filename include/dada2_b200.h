@@ -74,8 +74,9 @@ typedef struct {
  * corrected to any cluster (src/dada.rs:525-533). counters (16 slots):
  * nalign, compare_calls, cmp_scanned (sum of nraw over compare calls),
  * screened, aligned, stored, gapless, vectorized, homo, endsfree,
- * shuffle_calls, shuffle_moves, nshroud. times (4 slots, seconds): compare,
- * total, host phases, device wait. */
+ * shuffle_calls, shuffle_moves, nshroud. times (4 slots, seconds): this
+ * sample's compare calls (launch to results), the whole call, this sample's
+ * host phases (shuffle, p-update, bud), time the host waited on the device. */
 typedef struct {
   uint32_t* cl_reads;
   int32_t* cl_birth_type;

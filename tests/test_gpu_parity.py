@@ -297,3 +297,28 @@ def test_kernel_stats_count_launches():
     assert st["compares"] == r["counters"]["cmp_scanned"]
     assert st["ms"]["screen"] > 0.0
     assert len(D.stats_latencies()) == st["rounds"]
+
+
+def test_saturated_kmers_take_the_exact_distance():
+    """Profiles with a k-mer counted >= 255 in both sequences (src/nwalign.rs:1270-1277)."""
+    rng = np.random.default_rng(5)
+    seqs, reads = [], []
+    for t in range(12):
+        run = 262 + int(rng.integers(0, 40))  # the all-A 5-mer occurs run-4 >= 258 times
+        tail = rng.integers(1, 5, size=40 + int(rng.integers(0, 30))).astype(np.uint8)
+        s = np.concatenate([np.full(run, 1, np.uint8), tail])
+        if t % 3 == 1:
+            s[run + 5] = 1 + (s[run + 5] % 4)
+        seqs.append(s)
+        reads.append(50 - 3 * t)
+    err = np.full(16 * 41, 0.01)
+    op = O.AlignParams(kdist_cutoff=0.42)
+    sess = O.Session(seqs, reads, k=5, use_quals=False)
+    with D.CompareContext(D.AlignParams(), err, 41, use_quals=False) as ctx:
+        ctx.upload(seqs, reads)
+        for center in (0, 3, 7):
+            ci = sess.add_center(center)
+            wl, wh, ws, _ = sess.compare_map(ci, err, 41, op, greedy=False)
+            gl, gh, gs, _ = ctx.compare(center, 0.42, greedy=False)
+            assert gl.tobytes() == wl.tobytes()
+            assert np.array_equal(gh, wh) and np.array_equal(gs, ws)

@@ -1,0 +1,67 @@
+"""The N>1 path on CPU: world-size-2 gloo ranks, sharding and the timing reduction."""
+import os
+import socket
+
+import pytest
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, sizes, out):
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, os.path.join(root, "dada2-rs_b200"))
+    import datetime
+
+    import torch.distributed as dist
+
+    from dada2_b200 import multi
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    mine = multi.shard_samples(sizes, rank, world)
+    secs, comps = multi.reduce_run(1.0 + rank, 100 * (rank + 1))
+    out.put((rank, mine, secs, comps))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_shard_and_reduce():
+    torch = pytest.importorskip("torch")
+    import torch.multiprocessing as mp
+
+    sizes = [5637, 1975, 10356, 924, 477, 6232, 1996, 12127, 8685, 1738, 5994]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, sizes, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(2)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    res.sort()
+    owned = res[0][1] + res[1][1]
+    assert sorted(owned) == list(range(len(sizes)))  # complete and disjoint
+    loads = [sum(sizes[i] for i in r[1]) for r in res]
+    assert max(loads) - min(loads) <= max(sizes)
+    for _, _, secs, comps in res:
+        assert secs == 2.0 and comps == 300
+    _ = torch
+
+
+def test_single_process_reduce_is_identity():
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, os.path.join(root, "dada2-rs_b200"))
+    from dada2_b200 import multi
+
+    assert multi.reduce_run(3.5, 7) == (3.5, 7)
+    assert multi.shard_samples([3, 1, 2], 0, 1) == [0, 1, 2]
