@@ -150,4 +150,7 @@ void launch_align_debug(int which, const uint8_t* s1cat, const uint32_t* off1, c
                         uint8_t* al1, const uint32_t* aloff, uint32_t* alen, uint32_t* err_word,
                         cudaStream_t st);
 
+// Records the message dgpu_last_error() returns on this thread.
+void set_last_error(const char* msg);
+
 }  // namespace dgpu

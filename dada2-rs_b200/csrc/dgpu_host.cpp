@@ -32,6 +32,8 @@ static int fail(int code, const std::string& msg) {
   return code;
 }
 
+void set_last_error(const char* msg) { g_err = msg; }
+
 #define CUDA_TRY(x)                                                                     \
   do {                                                                                  \
     cudaError_t e_ = (x);                                                               \

@@ -13,9 +13,12 @@
 //
 // Built with --fmad=false: the FP64 product and the k-mer distances must round
 // exactly like the reference's separately-rounded operations.
+#include <algorithm>
 #include <cfloat>
 #include <cstdio>
+#include <mutex>
 
+#include "dada2_b200.h"
 #include "dgpu_common.h"
 
 namespace dgpu {
@@ -1438,4 +1441,152 @@ void launch_align_debug(int which, const uint8_t* s1cat, const uint32_t* off1, c
                                                      geom, scratch, al0, al1, aloff, alen, err_word);
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free alignment entry point (dgpu_align_pairs_noalloc).
+//
+// For callers that must not allocate device memory -- code running inside
+// CUDA stream capture, or hosts whose device memory is owned by another
+// allocator -- the pointer-matrix scratch the aligners need lives in this
+// file-scope array instead of a cudaMalloc'd buffer. Every GPU that loads the
+// library holds it until the process exits. Calls share it: two calls whose
+// kernels overlap on one device race on it.
+// ---------------------------------------------------------------------------
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;  // 16 MiB per device
+constexpr size_t kNoAllocHeader = 256;                     // error word, cleared per call
+static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
+
+// One warp per pair, persistent: warp w reuses scratch slot w for every pair
+// it takes, so any number of pairs fits as long as one slot does.
+__global__ void __launch_bounds__(kNwWarps * 32) k_align_noalloc(int which, const uint8_t* s1cat, const uint32_t* off1,
+                                                                const uint32_t* len1, const uint8_t* s2cat,
+                                                                const uint32_t* off2, const uint32_t* len2,
+                                                                uint32_t npairs, KParams kp, int end_gap, NwGeom geom,
+                                                                uint8_t* scratch, size_t slot_bytes, uint8_t* al0,
+                                                                uint8_t* al1, const uint32_t* aloff, uint32_t* alen,
+                                                                uint32_t* err_word) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t gw = blockIdx.x * kNwWarps + wib;
+  const uint32_t nw = gridDim.x * kNwWarps;
+  uint8_t* my_scr = scratch + size_t(gw) * slot_bytes;
+  const int kb = rm_kbound(geom.rm_pairs);
+  for (uint32_t pair = gw; pair < npairs; pair += nw) {
+    uint32_t ham = 0;
+    const uint8_t* a = s1cat + off1[pair];
+    const uint8_t* b = s2cat + off2[pair];
+    uint8_t* o0 = al0 + aloff[pair];
+    uint8_t* o1 = al1 + aloff[pair];
+    bool ok;
+    if (which == 0) {
+      VecSmem S = carve_vec(smem_raw + size_t(wib) * nw_smem_per_warp_vec(geom), geom.lmax, geom.vec_ncol);
+      ok = vec_align_any(lane, a, int(len1[pair]), b, int(len2[pair]), int16_t(kp.match), int16_t(kp.mismatch),
+                         int16_t(kp.gap), int16_t(end_gap), kp.band, S, my_scr, geom.vec_ncol, geom.vec_nrow, &ham,
+                         err_word, o0, o1, alen + pair);
+    } else {
+      RmSmem S = carve_rm(smem_raw + size_t(wib) * nw_smem_per_warp_rm(geom), geom.lmax, kb);
+      ok = rm_dispatch(lane, a, int(len1[pair]), b, int(len2[pair]), kp, which == 1, kb, S,
+                       reinterpret_cast<uint32_t*>(my_scr), &ham, err_word, o0, o1, alen + pair);
+    }
+    __syncwarp();
+    if (!ok) continue;
+    // the traceback wrote the rows end first; put them left to right
+    const uint32_t n = alen[pair];
+    for (uint32_t q = lane; q < n / 2; q += 32) {
+      const uint8_t x0 = o0[q], x1 = o1[q];
+      o0[q] = o0[n - 1 - q];
+      o1[q] = o1[n - 1 - q];
+      o0[n - 1 - q] = x0;
+      o1[n - 1 - q] = x1;
+    }
+    __syncwarp();
+  }
+}
+
+// Device address of g_noalloc_scratch, resolved once per device with that
+// device current (cudaGetSymbolAddress); host code must never hand the
+// symbol itself to a kernel.
+static std::mutex g_noalloc_mu;
+static uint8_t* g_noalloc_ptr[64] = {nullptr};
+
+static cudaError_t noalloc_scratch(int device, uint8_t** out) {
+  if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> g(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_ptr[device] = static_cast<uint8_t*>(p);
+  }
+  *out = g_noalloc_ptr[device];
+  return cudaSuccess;
+}
+
 }  // namespace dgpu
+
+extern "C" int dgpu_align_pairs_noalloc(int which, int npairs, int max_len, const uint8_t* s1cat,
+                                        const uint32_t* off1, const uint32_t* len1, const uint8_t* s2cat,
+                                        const uint32_t* off2, const uint32_t* len2, const dgpu_align_params* params,
+                                        int end_gap, uint8_t* al0, uint8_t* al1, const uint32_t* al_off,
+                                        uint32_t* al_len, void* stream) {
+  using namespace dgpu;
+  auto bad = [](int code, const char* msg) {
+    set_last_error(msg);  // reported by dgpu_last_error()
+    return code;
+  };
+  if (which < 0 || which > 2 || npairs <= 0 || !params || !s1cat || !off1 || !len1 || !s2cat || !off2 || !len2 ||
+      !al0 || !al1 || !al_off || !al_len)
+    return bad(DGPU_E_INVALID, "bad argument");
+  if (max_len <= 0 || max_len > 9998) return bad(DGPU_E_INVALID, "max_len must be in 1..9998");
+  if (which == 0 && max_len > 3500) return bad(DGPU_E_INVALID, "the vectorized aligner takes lengths <= 3500");
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return bad(DGPU_E_CUDA, cudaGetErrorString(e));
+  uint8_t* base = nullptr;
+  e = noalloc_scratch(device, &base);
+  if (e != cudaSuccess) return bad(DGPU_E_CUDA, cudaGetErrorString(e));
+  KParams kp{};
+  kp.match = params->match_score;
+  kp.mismatch = params->mismatch;
+  kp.gap = params->gap_p;
+  kp.homo_gap = params->homo_gap_p;
+  kp.band = params->band;
+  kp.ncol = 1;
+  // geometry bounds for any pair of lengths in [1, max_len]
+  NwGeom g{};
+  g.lmax = max_len;
+  const int64_t bb = kp.band < 0 ? int64_t(max_len) : int64_t(kp.band);
+  g.vec_ncol = int32_t(4 + (std::min<int64_t>(bb, max_len) + 1) / 2 + std::min<int64_t>(bb + max_len - 1, max_len) / 2);
+  g.vec_nrow = 2 * max_len + 1;
+  const int64_t W = kp.band < 0 ? int64_t(2 * max_len + 1) : std::min<int64_t>(2 * bb + max_len, 2 * int64_t(max_len) + 1);
+  g.rm_pairs = int32_t(std::min<int64_t>((W + 1) / 2, 512));
+  g.vec_scratch = align16(size_t(g.vec_nrow) * std::max<size_t>(size_t(g.vec_ncol), 32));
+  g.rm_scratch = align16(size_t(2 * max_len + 1) * 2 * rm_kbound(g.rm_pairs) * 4);
+  const size_t slot = which == 0 ? g.vec_scratch : g.rm_scratch;
+  const size_t avail = kNoAllocScratchBytes - kNoAllocHeader;
+  const size_t max_warps = avail / slot;
+  if (slot > avail || max_warps < size_t(kNwWarps))
+    return bad(DGPU_E_INVALID, "max_len too long: four alignments' scratch exceeds the 16 MiB static area");
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  size_t warps = std::min<size_t>(max_warps, size_t(std::max(sms, 1)) * 4 * kNwWarps);
+  warps = std::min<size_t>(warps, (size_t(npairs) + kNwWarps - 1) / kNwWarps * kNwWarps);
+  warps = std::max<size_t>(kNwWarps, warps / kNwWarps * kNwWarps);  // multiple of 4, <= max_warps
+  g.nwarps = int32_t(warps);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  uint32_t* err_word = reinterpret_cast<uint32_t*>(base);
+  e = cudaMemsetAsync(err_word, 0, 4, st);
+  if (e != cudaSuccess) return bad(DGPU_E_CUDA, cudaGetErrorString(e));
+  const size_t smem = (which == 0 ? nw_smem_per_warp_vec(g) : nw_smem_per_warp_rm(g)) * kNwWarps;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_align_noalloc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  k_align_noalloc<<<uint32_t(warps / kNwWarps), kNwWarps * 32, smem, st>>>(which, s1cat, off1, len1, s2cat, off2, len2,
+                                                                uint32_t(npairs), kp, end_gap, g, base + kNoAllocHeader,
+                                                                slot, al0, al1, al_off, al_len, err_word);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return bad(DGPU_E_CUDA, cudaGetErrorString(e));
+  uint32_t flag = 0;
+  e = cudaMemcpyAsync(&flag, err_word, 4, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return bad(DGPU_E_CUDA, cudaGetErrorString(e));
+  if (flag) return bad(flag & DERR_UNSUPPORTED ? DGPU_E_UNSUPPORTED : DGPU_E_DEVICE, "device error flag set");
+  return 0;
+}

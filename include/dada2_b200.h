@@ -184,6 +184,26 @@ int dgpu_align_debug(int device, int which, int npairs, const uint8_t* s1cat, co
                      const uint32_t* len2, const dgpu_align_params* params, int end_gap,
                      uint8_t* al0, uint8_t* al1, const uint32_t* al_off, uint32_t* al_len);
 
+/* ---- aligners without device allocation ----
+ * No counterpart in the reference. Same alignments as dgpu_align_debug, for
+ * callers that cannot allocate device memory (code running under CUDA stream
+ * capture, or hosts whose device memory belongs to another allocator): all
+ * pointers are caller-owned and must be readable/writable by the current
+ * device (device or managed memory), and the aligners' scratch is a 16 MiB
+ * static device array that every GPU loading this library holds until exit.
+ * max_len bounds every sequence length (at most 3500 for which = 0); lengths
+ * whose scratch for four concurrent alignments exceeds the array are rejected
+ * with DGPU_E_INVALID. The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress), so make it before any stream capture. Calls share
+ * the array: calls whose kernels overlap on one device race. Runs on `stream`
+ * (a cudaStream_t; NULL = legacy default stream) and returns after it finishes. */
+int dgpu_align_pairs_noalloc(int which, int npairs, int max_len, const uint8_t* s1cat,
+                             const uint32_t* off1, const uint32_t* len1, const uint8_t* s2cat,
+                             const uint32_t* off2, const uint32_t* len2,
+                             const dgpu_align_params* params, int end_gap, uint8_t* al0,
+                             uint8_t* al1, const uint32_t* al_off, uint32_t* al_len,
+                             void* stream);
+
 #ifdef __cplusplus
 }
 #endif
