@@ -80,6 +80,7 @@ struct NwGeom {
 // ---- shared-memory carving, used by kernels and by the host sizing code ----
 constexpr int kScreenWarps = 8;   // warps per screen CTA
 constexpr int kNwWarps = 4;       // warps per NW CTA
+constexpr int kAlignCtasPerSm = 5; // resident align CTAs per SM (96 registers per thread)
 constexpr int kStageBytes = 4096; // traceback staging per warp
 constexpr int kStoreSpan = 8192;  // raws per store CTA (its own output segment)
 
@@ -119,10 +120,8 @@ struct CompareLaunch {
   const uint32_t* task_prefix;
   uint32_t ntask;
   uint32_t total_items;
-  uint32_t* queue_vec;      // nraw capacity each
-  uint32_t* queue_rm;
-  uint32_t* queue_pass;
-  uint32_t* queue_counts;   // [pushed vec, pushed rm, taken vec, taken rm, pushed pass]
+  uint32_t* queue_pass;     // nraw capacity: items that passed the screen
+  uint32_t* queue_counts;   // 8 words; [4] = items pushed to queue_pass
   uint8_t* nw_scratch;      // nwarps * max(vec_scratch, rm_scratch)
   NwGeom geom;
   uint32_t* err_word;

@@ -10,10 +10,12 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <functional>
 #include <limits>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -59,29 +61,161 @@ struct GlobalStats {
 static GlobalStats g_stats;
 
 // ---------------------------------------------------------------------------
-// Buffers
+// Block cache. A finished pool gives its device and mapped-host blocks back
+// here (after synchronizing its stream, so every block in the cache is idle)
+// and the next pool takes blocks of about the size it asks for, so repeated
+// calls on similar batches do not pay for cudaMalloc / cudaHostAlloc / free
+// again. A block serves requests from half its size up to its size. The cache
+// holds at most kCacheCap bytes per device and kind; dgpu_cache_release empties
+// it, and a failed cudaMalloc empties it for that device and retries.
+// ---------------------------------------------------------------------------
+constexpr int kCacheDevs = 64;
+constexpr size_t kCacheCap = size_t(32) << 30;
+
+struct HostBlock {
+  void* h;
+  void* d;
+};
+
+struct BlockCache {
+  std::mutex mu;
+  std::multimap<size_t, void*> dev[kCacheDevs];
+  std::multimap<size_t, HostBlock> host[kCacheDevs];
+  size_t dev_bytes[kCacheDevs] = {};
+  size_t host_bytes[kCacheDevs] = {};
+};
+
+static BlockCache& block_cache() {
+  static BlockCache* c = new BlockCache;  // never destroyed: no CUDA calls at process exit
+  return *c;
+}
+
+static size_t block_round(size_t b) {
+  const size_t g = b >= (size_t(2) << 20) ? (size_t(2) << 20) : size_t(4096);
+  return (b + g - 1) / g * g;
+}
+
+static int current_device() {
+  int d = 0;
+  cudaGetDevice(&d);
+  return d;
+}
+
+static void* cache_take_dev(int dev, size_t bytes, size_t* got) {
+  if (dev < 0 || dev >= kCacheDevs) return nullptr;
+  BlockCache& c = block_cache();
+  std::lock_guard<std::mutex> g(c.mu);
+  auto it = c.dev[dev].lower_bound(bytes);
+  if (it == c.dev[dev].end() || it->first > 2 * bytes) return nullptr;
+  void* p = it->second;
+  *got = it->first;
+  c.dev_bytes[dev] -= it->first;
+  c.dev[dev].erase(it);
+  return p;
+}
+
+static bool cache_put_dev(int dev, size_t bytes, void* p) {
+  if (dev < 0 || dev >= kCacheDevs) return false;
+  BlockCache& c = block_cache();
+  std::lock_guard<std::mutex> g(c.mu);
+  if (c.dev_bytes[dev] + bytes > kCacheCap) return false;
+  c.dev[dev].emplace(bytes, p);
+  c.dev_bytes[dev] += bytes;
+  return true;
+}
+
+static bool cache_take_host(int dev, size_t bytes, size_t* got, HostBlock* out) {
+  if (dev < 0 || dev >= kCacheDevs) return false;
+  BlockCache& c = block_cache();
+  std::lock_guard<std::mutex> g(c.mu);
+  auto it = c.host[dev].lower_bound(bytes);
+  if (it == c.host[dev].end() || it->first > 2 * bytes) return false;
+  *out = it->second;
+  *got = it->first;
+  c.host_bytes[dev] -= it->first;
+  c.host[dev].erase(it);
+  return true;
+}
+
+static bool cache_put_host(int dev, size_t bytes, HostBlock b) {
+  if (dev < 0 || dev >= kCacheDevs) return false;
+  BlockCache& c = block_cache();
+  std::lock_guard<std::mutex> g(c.mu);
+  if (c.host_bytes[dev] + bytes > kCacheCap) return false;
+  c.host[dev].emplace(bytes, b);
+  c.host_bytes[dev] += bytes;
+  return true;
+}
+
+// Frees every cached block of `dev` (all devices when dev < 0); returns the
+// number of bytes released.
+static size_t cache_release(int dev) {
+  BlockCache& c = block_cache();
+  std::lock_guard<std::mutex> g(c.mu);
+  size_t freed = 0;
+  int prev = current_device();
+  for (int d = 0; d < kCacheDevs; ++d) {
+    if (dev >= 0 && d != dev) continue;
+    if (c.dev[d].empty() && c.host[d].empty()) continue;
+    cudaSetDevice(d);
+    for (auto& kv : c.dev[d]) cudaFree(kv.second);
+    for (auto& kv : c.host[d]) cudaFreeHost(kv.second.h);
+    freed += c.dev_bytes[d] + c.host_bytes[d];
+    c.dev[d].clear();
+    c.host[d].clear();
+    c.dev_bytes[d] = c.host_bytes[d] = 0;
+  }
+  cudaSetDevice(prev);
+  return freed;
+}
+
+// ---------------------------------------------------------------------------
+// Buffers. release() frees at once (cudaFree waits for the device, so a block
+// still read by queued work is safe); recycle() hands an idle block to the
+// cache and is only called once the owner's stream has drained.
 // ---------------------------------------------------------------------------
 template <class T>
 struct DBuf {
   T* p = nullptr;
   size_t n = 0;
+  size_t bytes = 0;
+  int dev = -1;
   int alloc(size_t count) {
     release();
     if (count == 0) count = 1;
-    void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, count * sizeof(T));
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      return fail(DGPU_E_NOMEM, "cudaMalloc(" + std::to_string(count * sizeof(T)) + " bytes): " + cudaGetErrorString(e));
+    const size_t want = block_round(count * sizeof(T));
+    const int d = current_device();
+    size_t got = 0;
+    void* q = cache_take_dev(d, want, &got);
+    if (!q) {
+      cudaError_t e = cudaMalloc(&q, want);
+      if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        cache_release(d);
+        e = cudaMalloc(&q, want);
+      }
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DGPU_E_NOMEM, "cudaMalloc(" + std::to_string(count * sizeof(T)) + " bytes): " +
+                                      cudaGetErrorString(e));
+      }
+      got = want;
     }
     p = static_cast<T*>(q);
     n = count;
+    bytes = got;
+    dev = d;
     return 0;
   }
   void release() {
     if (p) cudaFree(p);
     p = nullptr;
-    n = 0;
+    n = bytes = 0;
+  }
+  void recycle() {
+    if (p && !cache_put_dev(dev, bytes, p)) cudaFree(p);
+    p = nullptr;
+    n = bytes = 0;
   }
   DBuf() = default;
   DBuf(const DBuf&) = delete;
@@ -96,31 +230,45 @@ struct HBuf {
   T* h = nullptr;
   T* d = nullptr;
   size_t n = 0;
+  size_t bytes = 0;
+  int dev = -1;
   int alloc(size_t count) {
     release();
     if (count == 0) count = 1;
-    void* q = nullptr;
-    cudaError_t e = cudaHostAlloc(&q, count * sizeof(T), cudaHostAllocMapped);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      return fail(DGPU_E_NOMEM, std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
+    const size_t want = block_round(count * sizeof(T));
+    const int dv = current_device();
+    size_t got = 0;
+    HostBlock b{nullptr, nullptr};
+    if (!cache_take_host(dv, want, &got, &b)) {
+      cudaError_t e = cudaHostAlloc(&b.h, want, cudaHostAllocMapped);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DGPU_E_NOMEM, std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
+      }
+      e = cudaHostGetDevicePointer(&b.d, b.h, 0);
+      if (e != cudaSuccess) {
+        cudaFreeHost(b.h);
+        cudaGetLastError();
+        return fail(DGPU_E_CUDA, std::string("cudaHostGetDevicePointer: ") + cudaGetErrorString(e));
+      }
+      got = want;
     }
-    void* dq = nullptr;
-    e = cudaHostGetDevicePointer(&dq, q, 0);
-    if (e != cudaSuccess) {
-      cudaFreeHost(q);
-      cudaGetLastError();
-      return fail(DGPU_E_CUDA, std::string("cudaHostGetDevicePointer: ") + cudaGetErrorString(e));
-    }
-    h = static_cast<T*>(q);
-    d = static_cast<T*>(dq);
+    h = static_cast<T*>(b.h);
+    d = static_cast<T*>(b.d);
     n = count;
+    bytes = got;
+    dev = dv;
     return 0;
   }
   void release() {
     if (h) cudaFreeHost(h);
     h = d = nullptr;
-    n = 0;
+    n = bytes = 0;
+  }
+  void recycle() {
+    if (h && !cache_put_host(dev, bytes, HostBlock{h, d})) cudaFreeHost(h);
+    h = d = nullptr;
+    n = bytes = 0;
   }
   HBuf() = default;
   HBuf(const HBuf&) = delete;
@@ -128,49 +276,116 @@ struct HBuf {
   ~HBuf() { release(); }
 };
 
+template <class... B>
+static void recycle_all(B&... b) {
+  (b.recycle(), ...);
+}
+
 // ---------------------------------------------------------------------------
 // Device pool: the resident uniques of one or more samples
 // ---------------------------------------------------------------------------
-struct Pool {
-  int device = 0;
+struct Pool;
+
+// One launch context: its own stream, queue, NW scratch, task tables and store
+// bookkeeping, so that compares of different samples can be in flight at once.
+// Results land in the pool's raw-indexed arrays, which concurrent launches
+// never share: a sample has at most one compare pending.
+struct Slot {
+  Pool* P = nullptr;
   cudaStream_t st = nullptr;
-  uint32_t nraw = 0, lmax = 0, lmin = 0;
-  KParams kp{};
-  NwGeom geom{};
-  int sms = 148;
-  DBuf<uint8_t> seq, qual, kmer8, sat, lock, status;
-  DBuf<uint32_t> off, len, reads, ham, queue_vec, queue_rm, queue_pass, queue_counts, err_word;
-  DBuf<double> e_minmax, err, lambda;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  DBuf<uint32_t> queue_pass, queue_counts;
   DBuf<uint8_t> scratch;
   DBuf<TaskDev> tasks;
-  DBuf<uint32_t> task_prefix;
-  HBuf<uint32_t> comp_index, comp_ham, blk_counters;
-  HBuf<double> comp_lambda, task_self;
+  DBuf<uint32_t> task_prefix, store_map;
+  HBuf<uint32_t> blk_counters, prefix_stage, store_stage;  // prefix; then (task, chunk) per store CTA
+  HBuf<double> task_self;
   HBuf<TaskDev> task_stage;
-  HBuf<uint32_t> prefix_stage, store_stage;  // prefix; then (task, chunk) per store CTA
-  DBuf<uint32_t> store_map;
   std::vector<uint32_t> task_blk0;  // first store CTA of each task in the latest launch
-  uint32_t nblk_cap = 0;
-  HBuf<uint8_t> lock_host;  // pinned host copy of every lock flag
-  bool has_qual = false;
-  uint32_t ntask_cap = 0;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  uint32_t ntask_cap = 0, nblk_cap = 0;
 
-  ~Pool() {
+  ~Slot() {
+    if (st && cudaStreamSynchronize(st) == cudaSuccess)  // every block is idle now
+      recycle_all(queue_pass, queue_counts, scratch, tasks, task_prefix, store_map, blk_counters, prefix_stage,
+                  store_stage, task_self, task_stage);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
   }
 
-  int init(int dev) {
-    device = dev;
-    CUDA_TRY(cudaSetDevice(dev));
+  int init(Pool* pool) {
+    P = pool;
     CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
     return 0;
   }
 
+  int ensure_tasks(uint32_t ntask) {
+    if (ntask <= ntask_cap) return 0;
+    uint32_t cap = std::max<uint32_t>(ntask, 64);
+    TRY(tasks.alloc(cap));
+    TRY(task_prefix.alloc(cap + 1));
+    TRY(task_self.alloc(cap));
+    TRY(task_stage.alloc(cap));
+    TRY(prefix_stage.alloc(cap + 1));
+    ntask_cap = cap;
+    return 0;
+  }
+
+  int ensure_blocks(uint32_t nblk) {
+    if (nblk <= nblk_cap) return 0;
+    const uint32_t cap = std::max<uint32_t>(nblk, 256);
+    TRY(store_stage.alloc(size_t(2) * cap));
+    TRY(store_map.alloc(size_t(2) * cap));
+    TRY(blk_counters.alloc(size_t(cap) * TC_NCOUNTERS));
+    nblk_cap = cap;
+    return 0;
+  }
+
+  template <class F>
+  void for_each_stored(uint32_t t, F&& f) const;
+  void task_counters(uint32_t t, uint32_t* out) const;
+  int run_compare(uint32_t ntask, bool do_store, double* wait_s);
+};
+
+// Device pool: the resident uniques of one or more samples.
+struct Pool {
+  int device = 0;
+  cudaStream_t st = nullptr;  // uploads and resets
+  uint32_t nraw = 0, lmax = 0, lmin = 0;
+  KParams kp{};
+  NwGeom geom{};
+  int sms = 148;
+  int nslots = 1;
+  DBuf<uint8_t> seq, qual, kmer8, sat, lock, status;
+  DBuf<uint32_t> off, len, reads, ham, err_word;
+  DBuf<double> e_minmax, err, lambda;
+  // stored comps of each task, at the task's first raw (its sample's base)
+  HBuf<uint32_t> comp_index, comp_ham;
+  HBuf<double> comp_lambda;
+  HBuf<uint8_t> lock_host;  // pinned host copy of every lock flag
+  bool has_qual = false;
+  std::vector<std::unique_ptr<Slot>> slots;
+
+  ~Pool() {
+    slots.clear();  // each slot drains its own stream first
+    if (st && cudaStreamSynchronize(st) == cudaSuccess)
+      recycle_all(seq, qual, kmer8, sat, lock, status, off, len, reads, ham, err_word, e_minmax, err, lambda,
+                  comp_index, comp_ham, comp_lambda, lock_host);
+    if (st) cudaStreamDestroy(st);
+  }
+
+  // nslot launch contexts are made once the pool's geometry is known.
+  int init(int dev, int nslot = 1) {
+    device = dev;
+    nslots = std::max(1, nslot);
+    CUDA_TRY(cudaSetDevice(dev));
+    CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    return 0;
+  }
+
+  Slot& slot0() { return *slots[0]; }
   // seqs: codes 1..4 concatenated; quals_u8 may be null.
   int upload(uint32_t n, const uint8_t* seqs, const uint32_t* offs, const uint32_t* lens, const uint8_t* quals_u8,
              const uint32_t* rd, const KParams& params, const double* errm) {
@@ -185,20 +400,40 @@ struct Pool {
       total += lens[t];
     }
     if (total >= 0xffffffffull) return fail(DGPU_E_UNSUPPORTED, "more than 4 GiB of sequence in one pool");
-    std::vector<uint32_t> o(n);
-    std::vector<uint8_t> packed(total ? total : 1);
-    std::vector<uint8_t> qpacked;
     has_qual = quals_u8 != nullptr;
-    if (has_qual) qpacked.resize(total ? total : 1);
-    uint64_t w = 0;
-    for (uint32_t t = 0; t < n; ++t) {
-      o[t] = uint32_t(w);
-      std::memcpy(packed.data() + w, seqs + offs[t], lens[t]);
-      if (has_qual) std::memcpy(qpacked.data() + w, quals_u8 + offs[t], lens[t]);
-      w += lens[t];
+    // Sequences already packed back to back (offs[t] = running length) go up
+    // as they are; anything else is packed first.
+    bool contiguous = true;
+    {
+      uint64_t w = 0;
+      for (uint32_t t = 0; t < n && contiguous; ++t) {
+        contiguous = offs[t] == w;
+        w += lens[t];
+      }
     }
+    std::vector<uint32_t> o;
+    std::vector<uint8_t> packed, qpacked;
+    const uint8_t* seq_src = seqs;
+    const uint8_t* qual_src = quals_u8;
+    const uint32_t* off_src = offs;
+    if (!contiguous) {
+      o.resize(n);
+      packed.resize(total ? total : 1);
+      if (has_qual) qpacked.resize(total ? total : 1);
+      uint64_t w = 0;
+      for (uint32_t t = 0; t < n; ++t) {
+        o[t] = uint32_t(w);
+        std::memcpy(packed.data() + w, seqs + offs[t], lens[t]);
+        if (has_qual) std::memcpy(qpacked.data() + w, quals_u8 + offs[t], lens[t]);
+        w += lens[t];
+      }
+      seq_src = packed.data();
+      qual_src = has_qual ? qpacked.data() : nullptr;
+      off_src = o.data();
+    }
+    const size_t seq_bytes = total ? size_t(total) : 1;
     const size_t nk = size_t(1) << (2 * kp.kmer_size);
-    TRY(seq.alloc(packed.size()));
+    TRY(seq.alloc(seq_bytes));
     TRY(off.alloc(n));
     TRY(len.alloc(n));
     TRY(reads.alloc(n));
@@ -207,10 +442,6 @@ struct Pool {
     TRY(ham.alloc(n));
     TRY(lambda.alloc(n));
     TRY(e_minmax.alloc(n));
-    TRY(queue_vec.alloc(n));
-    TRY(queue_rm.alloc(n));
-    TRY(queue_pass.alloc(n));
-    TRY(queue_counts.alloc(8));
     TRY(err_word.alloc(1));
     TRY(err.alloc(size_t(16) * kp.ncol));
     TRY(kmer8.alloc(kp.use_kmers ? size_t(n) * nk : 1));
@@ -221,11 +452,11 @@ struct Pool {
     TRY(lock_host.alloc(n));
     std::memset(lock_host.h, 0, n);
     if (has_qual) {
-      TRY(qual.alloc(qpacked.size()));
-      CUDA_TRY(cudaMemcpyAsync(qual.p, qpacked.data(), qpacked.size(), cudaMemcpyHostToDevice, st));
+      TRY(qual.alloc(seq_bytes));
+      if (total) CUDA_TRY(cudaMemcpyAsync(qual.p, qual_src, size_t(total), cudaMemcpyHostToDevice, st));
     }
-    CUDA_TRY(cudaMemcpyAsync(seq.p, packed.data(), packed.size(), cudaMemcpyHostToDevice, st));
-    CUDA_TRY(cudaMemcpyAsync(off.p, o.data(), size_t(n) * 4, cudaMemcpyHostToDevice, st));
+    if (total) CUDA_TRY(cudaMemcpyAsync(seq.p, seq_src, size_t(total), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(off.p, off_src, size_t(n) * 4, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(len.p, lens, size_t(n) * 4, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(reads.p, rd, size_t(n) * 4, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(err.p, errm, size_t(16) * kp.ncol * 8, cudaMemcpyHostToDevice, st));
@@ -266,9 +497,17 @@ struct Pool {
     // (at most 4 groups) for the register form
     geom.vec_scratch = vec_possible ? align16(size_t(geom.vec_nrow) * std::max<size_t>(size_t(geom.vec_ncol), 32)) : 0;
     geom.rm_scratch = rm_possible ? align16(size_t(2 * lmax + 1) * 2 * kb * 4) : 0;
-    geom.nwarps = sms * 4 * kNwWarps;
+    geom.nwarps = sms * kAlignCtasPerSm * kNwWarps;
     const size_t per = std::max<size_t>(std::max(geom.vec_scratch, geom.rm_scratch), 16);
-    TRY(scratch.alloc(per * size_t(geom.nwarps)));
+    slots.clear();
+    for (int k = 0; k < nslots; ++k) {
+      slots.emplace_back(new Slot);
+      Slot& L = *slots.back();
+      TRY(L.init(this));
+      TRY(L.scratch.alloc(per * size_t(geom.nwarps)));
+      TRY(L.queue_pass.alloc(nraw));
+      TRY(L.queue_counts.alloc(8));
+    }
     return 0;
   }
 
@@ -292,143 +531,122 @@ struct Pool {
     return v;
   }
 
-  int ensure_tasks(uint32_t ntask) {
-    if (ntask <= ntask_cap) return 0;
-    uint32_t cap = std::max<uint32_t>(ntask, 64);
-    TRY(tasks.alloc(cap));
-    TRY(task_prefix.alloc(cap + 1));
-    TRY(task_self.alloc(cap));
-    TRY(task_stage.alloc(cap));
-    TRY(prefix_stage.alloc(cap + 1));
-    ntask_cap = cap;
-    return 0;
-  }
-
-  int ensure_blocks(uint32_t nblk) {
-    if (nblk <= nblk_cap) return 0;
-    const uint32_t cap = std::max<uint32_t>(nblk, 256);
-    TRY(store_stage.alloc(size_t(2) * cap));
-    TRY(store_map.alloc(size_t(2) * cap));
-    TRY(blk_counters.alloc(size_t(cap) * TC_NCOUNTERS));
-    nblk_cap = cap;
-    return 0;
-  }
-
-  // Stored comps of task t (latest launch), in ascending raw order.
-  template <class F>
-  void for_each_stored(uint32_t t, F&& f) const {
-    const TaskDev& T = task_stage.h[t];
-    const uint32_t nb = (T.n + kStoreSpan - 1) / kStoreSpan;
-    for (uint32_t b = 0; b < nb; ++b) {
-      const uint32_t cnt = blk_counters.h[size_t(task_blk0[t] + b) * TC_NCOUNTERS + TC_STORED];
-      const uint32_t o = T.out_off + b * uint32_t(kStoreSpan);
-      for (uint32_t k = 0; k < cnt; ++k) f(comp_index.h[o + k], comp_lambda.h[o + k], comp_ham.h[o + k]);
-    }
-  }
-
-  // Counters of task t summed over its store CTAs.
-  void task_counters(uint32_t t, uint32_t* out) const {
-    for (int k = 0; k < TC_NCOUNTERS; ++k) out[k] = 0;
-    const uint32_t nb = (task_stage.h[t].n + kStoreSpan - 1) / kStoreSpan;
-    for (uint32_t b = 0; b < nb; ++b)
-      for (int k = 0; k < TC_NCOUNTERS; ++k) out[k] += blk_counters.h[size_t(task_blk0[t] + b) * TC_NCOUNTERS + k];
-  }
-
-  // Launches one compare over `ntask` tasks already in task_stage; waits for it.
-  int run_compare(uint32_t ntask, bool do_store, double* wait_s) {
-    const auto t_call = Clock::now();
-    TRY(ensure_tasks(ntask));
-    uint32_t total = 0, nblk = 0;
-    task_blk0.assign(ntask, 0);
-    for (uint32_t t = 0; t < ntask; ++t) {
-      prefix_stage.h[t] = total;
-      task_stage.h[t].out_off = total;
-      total += task_stage.h[t].n;
-      task_blk0[t] = nblk;
-      nblk += (task_stage.h[t].n + kStoreSpan - 1) / kStoreSpan;
-    }
-    prefix_stage.h[ntask] = total;
-    TRY(ensure_blocks(nblk));
-    for (uint32_t t = 0; t < ntask; ++t) {
-      const uint32_t nb = (task_stage.h[t].n + kStoreSpan - 1) / kStoreSpan;
-      for (uint32_t b = 0; b < nb; ++b) {
-        store_stage.h[task_blk0[t] + b] = t;
-        store_stage.h[nblk + task_blk0[t] + b] = b;
-      }
-    }
-    CUDA_TRY(cudaMemcpyAsync(tasks.p, task_stage.h, sizeof(TaskDev) * ntask, cudaMemcpyHostToDevice, st));
-    CUDA_TRY(cudaMemcpyAsync(task_prefix.p, prefix_stage.h, 4 * (ntask + 1), cudaMemcpyHostToDevice, st));
-    CUDA_TRY(cudaMemcpyAsync(store_map.p, store_stage.h, size_t(8) * nblk, cudaMemcpyHostToDevice, st));
-    CUDA_TRY(cudaMemsetAsync(queue_counts.p, 0, 32, st));
-    CompareLaunch L{};
-    L.pool = view();
-    L.kp = kp;
-    L.tasks = tasks.p;
-    L.task_prefix = task_prefix.p;
-    L.ntask = ntask;
-    L.total_items = total;
-    L.queue_vec = queue_vec.p;
-    L.queue_rm = queue_rm.p;
-    L.queue_pass = queue_pass.p;
-    L.queue_counts = queue_counts.p;
-    L.nw_scratch = scratch.p;
-    L.geom = geom;
-    L.err_word = err_word.p;
-    L.comp_index = comp_index.d;
-    L.comp_lambda = comp_lambda.d;
-    L.comp_ham = comp_ham.d;
-    L.task_self = task_self.d;
-    L.store_task = store_map.p;
-    L.store_chunk = store_map.p + nblk;
-    L.blk_counters = blk_counters.d;
-    L.nstore_blocks = nblk;
-    L.do_store = do_store ? 1 : 0;
-    const bool timing = g_stats.timing.load();
-    launch_compare(L, st, timing ? ev : nullptr);
-    CUDA_TRY(cudaGetLastError());
-    auto t0 = Clock::now();
-    CUDA_TRY(cudaStreamSynchronize(st));
-    const auto t1 = Clock::now();
-    if (wait_s) *wait_s += secs(t0, t1);
-    {
-      float ms[3] = {0, 0, 0};
-      if (timing)
-        for (int k = 0; k < 3; ++k) CUDA_TRY(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));
-      uint64_t screened = 0;
-      if (do_store)
-        for (uint32_t b = 0; b < nblk; ++b) screened += blk_counters.h[size_t(b) * TC_NCOUNTERS + TC_SCREENED];
-      std::lock_guard<std::mutex> g(g_stats.mu);
-      dgpu_kernel_stats& S = g_stats.s;
-      S.launches[1] += 1;
-      S.launches[2] += 1;
-      if (do_store) S.launches[3] += 1;
-      for (int k = 0; k < 3; ++k) S.ms[k + 1] += ms[k];
-      S.rounds += 1;
-      S.compares += total;
-      S.screened += screened;
-      S.screen_bytes += screened * (uint64_t(1) << (2 * kp.kmer_size)) + uint64_t(total) * 16u;
-      if (g_stats.round_ms.size() < (size_t(1) << 20)) g_stats.round_ms.push_back(1e3 * secs(t_call, t1));
-    }
-    uint32_t ew = 0;
-    CUDA_TRY(cudaMemcpy(&ew, err_word.p, 4, cudaMemcpyDeviceToHost));
-    if (ew) {
-      cudaMemsetAsync(err_word.p, 0, 4, st);
-      std::string what;
-      if (ew & DERR_TRACEBACK) what += " invalid traceback pointer;";
-      if (ew & DERR_GEOMETRY) what += " alignment exceeded its scratch bounds;";
-      if (ew & DERR_BAND_RANGE) what += " vectorized band left the compressed matrix;";
-      if (ew & DERR_UNSUPPORTED) what += " band wider than 1024 offsets on the row-major aligner;";
-      if (ew & DERR_LAMBDA) what += " non-ACGT code or quality beyond the error matrix in lambda;";
-      return fail(ew & DERR_UNSUPPORTED ? DGPU_E_UNSUPPORTED : DGPU_E_DEVICE, "device error:" + what);
-    }
-    return 0;
-  }
-
-  int push_locks(uint32_t base, uint32_t n) {
-    CUDA_TRY(cudaMemcpyAsync(lock.p + base, lock_host.h + base, n, cudaMemcpyHostToDevice, st));
+  int push_locks(uint32_t base, uint32_t n, cudaStream_t s) {
+    CUDA_TRY(cudaMemcpyAsync(lock.p + base, lock_host.h + base, n, cudaMemcpyHostToDevice, s));
     return 0;
   }
 };
+
+// Stored comps of task t (latest launch), in ascending raw order.
+template <class F>
+void Slot::for_each_stored(uint32_t t, F&& f) const {
+  const TaskDev& T = task_stage.h[t];
+  const uint32_t nb = (T.n + kStoreSpan - 1) / kStoreSpan;
+  for (uint32_t b = 0; b < nb; ++b) {
+    const uint32_t cnt = blk_counters.h[size_t(task_blk0[t] + b) * TC_NCOUNTERS + TC_STORED];
+    const uint32_t o = T.out_off + b * uint32_t(kStoreSpan);
+    for (uint32_t k = 0; k < cnt; ++k) f(P->comp_index.h[o + k], P->comp_lambda.h[o + k], P->comp_ham.h[o + k]);
+  }
+}
+
+// Counters of task t summed over its store CTAs.
+void Slot::task_counters(uint32_t t, uint32_t* out) const {
+  for (int k = 0; k < TC_NCOUNTERS; ++k) out[k] = 0;
+  const uint32_t nb = (task_stage.h[t].n + kStoreSpan - 1) / kStoreSpan;
+  for (uint32_t b = 0; b < nb; ++b)
+    for (int k = 0; k < TC_NCOUNTERS; ++k) out[k] += blk_counters.h[size_t(task_blk0[t] + b) * TC_NCOUNTERS + k];
+}
+
+// Launches one compare over `ntask` tasks already in task_stage; waits for it.
+int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
+  const auto t_call = Clock::now();
+  TRY(ensure_tasks(ntask));
+  const Pool& Q = *P;
+  uint32_t total = 0, nblk = 0;
+  task_blk0.assign(ntask, 0);
+  for (uint32_t t = 0; t < ntask; ++t) {
+    prefix_stage.h[t] = total;
+    task_stage.h[t].out_off = task_stage.h[t].base;
+    total += task_stage.h[t].n;
+    task_blk0[t] = nblk;
+    nblk += (task_stage.h[t].n + kStoreSpan - 1) / kStoreSpan;
+  }
+  prefix_stage.h[ntask] = total;
+  TRY(ensure_blocks(nblk));
+  for (uint32_t t = 0; t < ntask; ++t) {
+    const uint32_t nb = (task_stage.h[t].n + kStoreSpan - 1) / kStoreSpan;
+    for (uint32_t b = 0; b < nb; ++b) {
+      store_stage.h[task_blk0[t] + b] = t;
+      store_stage.h[nblk + task_blk0[t] + b] = b;
+    }
+  }
+  CUDA_TRY(cudaMemcpyAsync(tasks.p, task_stage.h, sizeof(TaskDev) * ntask, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(task_prefix.p, prefix_stage.h, 4 * (ntask + 1), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(store_map.p, store_stage.h, size_t(8) * nblk, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemsetAsync(queue_counts.p, 0, 32, st));
+  CompareLaunch L{};
+  L.pool = Q.view();
+  L.kp = Q.kp;
+  L.tasks = tasks.p;
+  L.task_prefix = task_prefix.p;
+  L.ntask = ntask;
+  L.total_items = total;
+  L.queue_pass = queue_pass.p;
+  L.queue_counts = queue_counts.p;
+  L.nw_scratch = scratch.p;
+  L.geom = Q.geom;
+  L.err_word = Q.err_word.p;
+  L.comp_index = Q.comp_index.d;
+  L.comp_lambda = Q.comp_lambda.d;
+  L.comp_ham = Q.comp_ham.d;
+  L.task_self = task_self.d;
+  L.store_task = store_map.p;
+  L.store_chunk = store_map.p + nblk;
+  L.blk_counters = blk_counters.d;
+  L.nstore_blocks = nblk;
+  L.do_store = do_store ? 1 : 0;
+  const bool timing = g_stats.timing.load();
+  launch_compare(L, st, timing ? ev : nullptr);
+  CUDA_TRY(cudaGetLastError());
+  auto t0 = Clock::now();
+  CUDA_TRY(cudaStreamSynchronize(st));
+  const auto t1 = Clock::now();
+  if (wait_s) *wait_s += secs(t0, t1);
+  {
+    float ms[3] = {0, 0, 0};
+    if (timing)
+      for (int k = 0; k < 3; ++k) CUDA_TRY(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));
+    uint64_t screened = 0;
+    if (do_store)
+      for (uint32_t b = 0; b < nblk; ++b) screened += blk_counters.h[size_t(b) * TC_NCOUNTERS + TC_SCREENED];
+    std::lock_guard<std::mutex> g(g_stats.mu);
+    dgpu_kernel_stats& S = g_stats.s;
+    S.launches[1] += 1;
+    S.launches[2] += 1;
+    if (do_store) S.launches[3] += 1;
+    for (int k = 0; k < 3; ++k) S.ms[k + 1] += ms[k];
+    S.rounds += 1;
+    S.compares += total;
+    S.screened += screened;
+    S.screen_bytes += screened * (uint64_t(1) << (2 * Q.kp.kmer_size)) + uint64_t(total) * 16u;
+    if (g_stats.round_ms.size() < (size_t(1) << 20)) g_stats.round_ms.push_back(1e3 * secs(t_call, t1));
+  }
+  uint32_t ew = 0;
+  CUDA_TRY(cudaMemcpyAsync(&ew, Q.err_word.p, 4, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  if (ew) {
+    std::string what;
+    if (ew & DERR_TRACEBACK) what += " invalid traceback pointer;";
+    if (ew & DERR_GEOMETRY) what += " alignment exceeded its scratch bounds;";
+    if (ew & DERR_BAND_RANGE) what += " vectorized band left the compressed matrix;";
+    if (ew & DERR_UNSUPPORTED) what += " band wider than 1024 offsets on the row-major aligner;";
+    if (ew & DERR_LAMBDA) what += " non-ACGT code or quality beyond the error matrix in lambda;";
+    CUDA_TRY(cudaMemsetAsync(Q.err_word.p, 0, 4, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return fail(ew & DERR_UNSUPPORTED ? DGPU_E_UNSUPPORTED : DGPU_E_DEVICE, "device error:" + what);
+  }
+  return 0;
+}
 
 // ---------------------------------------------------------------------------
 // Fork-join helpers for the large loops inside one sample's host phases. The
@@ -551,6 +769,8 @@ struct RunStats {
   uint64_t compare_calls = 0, cmp_scanned = 0, screened = 0, aligned = 0, stored = 0;
   uint64_t gapless = 0, vectorized = 0, homo = 0, endsfree = 0, shuffle_calls = 0, shuffle_moves = 0;
   double t_compare = 0, t_total = 0, t_host = 0, t_wait = 0;
+  double t_done = -1;  // from the start of the loop until this sample finished
+  uint64_t ns_shuffle = 0, ns_pupdate = 0, ns_bud = 0;  // host phases, nanoseconds
 };
 
 struct DadaConf {
@@ -646,7 +866,7 @@ struct SampleState {
   }
 
   // The store's host half: comps from the device into cluster ci (src/cluster.rs:351-397).
-  void absorb(size_t ci, const Pool& P, uint32_t t) {
+  void absorb(size_t ci, const Slot& P, uint32_t t) {
     uint32_t ctr[TC_NCOUNTERS];
     P.task_counters(t, ctr);
     const uint32_t ns = ctr[TC_STORED];
@@ -1028,31 +1248,52 @@ struct SampleState {
         }
       }
       // Pass A1: raws whose best cluster lost reads are queued for a rescan.
-      // Within one cluster's comps every raw is distinct, so long lists are
-      // split across threads; chunk results keep their order.
+      // Every pass here follows a move pass (or the carried state, which ended
+      // with one), after which each raw sits in its best cluster unless it is
+      // a center; so the raws whose best is ci are ci's members plus centers
+      // of other clusters, the same set as ci's comps with best ci. Pass B
+      // rescans each queued raw on its own and the dirty list is sorted before
+      // use, so the queue order does not matter. Long member lists are split
+      // across threads.
       for (uint32_t ci : reads_fell_list) {
-        const std::vector<Comp>& cv = clusters[ci].comp;
+        const std::vector<uint32_t>& mem = clusters[ci].raws;
         auto a1 = [&](size_t lo, size_t hi, std::vector<uint32_t>& out) {
           for (size_t k = lo; k < hi; ++k) {
-            const uint32_t raw = cv[k].index;
+            const uint32_t raw = mem[k];
             if (compmax[raw].i == ci && !in_affected[raw]) {
               in_affected[raw] = 1;
               out.push_back(raw);
             }
           }
         };
-        if (cv.size() < kParMin) {
-          a1(0, cv.size(), affected);
+        if (mem.size() < kParMin) {
+          a1(0, mem.size(), affected);
         } else {
-          std::vector<std::vector<uint32_t>> loc((cv.size() + kParGrain - 1) / kParGrain);
-          Helpers::get().parallel_for(cv.size(), kParGrain, [&](size_t c, size_t lo, size_t hi) { a1(lo, hi, loc[c]); });
+          std::vector<std::vector<uint32_t>> loc((mem.size() + kParGrain - 1) / kParGrain);
+          Helpers::get().parallel_for(mem.size(), kParGrain, [&](size_t c, size_t lo, size_t hi) { a1(lo, hi, loc[c]); });
           for (auto& v : loc) affected.insert(affected.end(), v.begin(), v.end());
         }
+        for (size_t cj = 0; cj < clusters.size(); ++cj) {
+          if (cj == ci || clusters[cj].center < 0) continue;
+          const uint32_t raw = uint32_t(clusters[cj].center);
+          if (compmax[raw].i == ci && !in_affected[raw]) {
+            in_affected[raw] = 1;
+            affected.push_back(raw);
+          }
+        }
       }
-      // Pass A2: changed clusters in ascending order.
+      // Pass A2: changed clusters in ascending order. A cluster whose reads
+      // fell changes nothing here: every raw whose best it is was queued by A1
+      // and is skipped, and for any other raw e = lambda * reads only dropped
+      // below an emax that already held it (ties already went to the smaller
+      // index), so its scan is left out.
       for (size_t ci = 0; ci < clusters.size(); ++ci) {
         const uint32_t nr = clusters[ci].reads;
         if (nr == reads_used[ci]) continue;
+        if (nr < reads_used[ci]) {
+          reads_used[ci] = nr;
+          continue;
+        }
         const double rf = double(nr);
         par_dirty(clusters[ci].comp.size(), [&](size_t lo, size_t hi, std::vector<uint32_t>& out) {
           reconcile_a2(uint32_t(ci), rf, lo, hi, out);
@@ -1072,10 +1313,17 @@ struct SampleState {
   // After the compare of cluster ci has been absorbed: the serial tail of one
   // loop iteration, then the next bud. Returns the next cluster to compare or -1.
   int64_t advance(size_t ci) {
+    const auto t0 = Clock::now();
     if (ci > 0) shuffle_converge(10);  // MAX_SHUFFLE, src/dada.rs:39
+    const auto t1 = Clock::now();
     p_update();
+    const auto t2 = Clock::now();
+    stats.ns_shuffle += uint64_t(std::chrono::duration_cast<std::chrono::nanoseconds>(t1 - t0).count());
+    stats.ns_pupdate += uint64_t(std::chrono::duration_cast<std::chrono::nanoseconds>(t2 - t1).count());
     if (clusters.size() >= conf->max_clust) return -1;
-    return bud();
+    const int64_t next = bud();
+    stats.ns_bud += uint64_t(std::chrono::duration_cast<std::chrono::nanoseconds>(Clock::now() - t2).count());
+    return next;
   }
 };
 
@@ -1150,6 +1398,7 @@ class Workers {
 
 // Asynchronous job queue: the host phases of a sample run here while the GPU
 // works on other samples' compares.
+// Host-phase jobs, highest priority first (first come first among equals).
 class JobQueue {
  public:
   explicit JobQueue(int n) {
@@ -1164,14 +1413,14 @@ class JobQueue {
     for (auto& t : th_) t.join();
   }
   bool inline_mode() const { return th_.empty(); }
-  void submit(std::function<void()> fn) {
+  void submit(std::function<void()> fn, int64_t priority = 0) {
     if (th_.empty()) {
       fn();
       return;
     }
     {
       std::lock_guard<std::mutex> g(mu_);
-      q_.push_back(std::move(fn));
+      q_.emplace(-priority, std::move(fn));
     }
     cv_.notify_one();
   }
@@ -1184,8 +1433,8 @@ class JobQueue {
         std::unique_lock<std::mutex> g(mu_);
         cv_.wait(g, [&] { return stop_ || !q_.empty(); });
         if (q_.empty()) return;
-        fn = std::move(q_.front());
-        q_.pop_front();
+        fn = std::move(q_.begin()->second);
+        q_.erase(q_.begin());
       }
       fn();
     }
@@ -1193,7 +1442,7 @@ class JobQueue {
   std::vector<std::thread> th_;
   std::mutex mu_;
   std::condition_variable cv_;
-  std::deque<std::function<void()>> q_;
+  std::multimap<int64_t, std::function<void()>> q_;
   bool stop_ = false;
 };
 
@@ -1375,7 +1624,7 @@ static dgpu_result* finish(SampleState& S, const SampleInput& in) {
   const RunStats& st = S.stats;
   const uint64_t c[16] = {S.nalign, st.compare_calls, st.cmp_scanned, st.screened, st.aligned, st.stored,
                           st.gapless, st.vectorized, st.homo, st.endsfree, st.shuffle_calls, st.shuffle_moves,
-                          S.nshroud, 0, 0, 0};
+                          S.nshroud, st.ns_shuffle, st.ns_pupdate, st.ns_bud};
   std::copy(c, c + 16, R->counters);
   R->times[0] = st.t_compare;
   R->times[1] = st.t_total;
@@ -1385,10 +1634,12 @@ static dgpu_result* finish(SampleState& S, const SampleInput& in) {
 }
 
 // The clustering loop over any number of samples resident in one pool.
-// Samples advance independently: whenever the GPU is free, one compare launch
-// covers every sample whose next cluster is ready; each sample's host phases
-// (shuffle, p-update, bud) then run on the job queue while the GPU serves the
-// others. A sample's own sequence of steps is exactly run_dada's.
+// Samples advance independently. Each launch slot has a worker that takes
+// every sample whose next cluster is ready, runs one compare launch over them
+// and hands each sample's host phases (shuffle, p-update, bud) to the job
+// queue; with several slots a sample that becomes ready while a launch is in
+// flight goes out at once on another slot. A sample's own sequence of steps is
+// exactly run_dada's.
 static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_params& ap, int host_threads) {
   const size_t ns = S.size();
   std::mutex mu;
@@ -1400,70 +1651,107 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
     ready.push_back(s);
   }
   double wait = 0.0;
+  int rc = 0;
+  std::string err_msg;
   std::atomic<int64_t> host_ns{0};
   auto t_start = Clock::now();
-  int rc = 0;
   {
     JobQueue jobs(host_threads > 1 ? host_threads : 0);
-    std::vector<size_t> batch;
-    for (;;) {
-      batch.clear();
-      {
-        std::unique_lock<std::mutex> lk(mu);
-        cv.wait(lk, [&] { return !ready.empty() || finished == ns; });
-        if (ready.empty()) break;
-        batch.swap(ready);
+    auto worker = [&](Slot& L) {
+      if (cudaSetDevice(P.device) != cudaSuccess) {
+        std::lock_guard<std::mutex> g(mu);
+        if (!rc) {
+          rc = DGPU_E_CUDA;
+          err_msg = "cudaSetDevice failed in a launch worker";
+        }
+        cv.notify_all();
+        return;
       }
-      std::sort(batch.begin(), batch.end());
-      rc = P.ensure_tasks(uint32_t(batch.size()));
-      if (rc) break;
-      for (size_t a = 0; a < batch.size(); ++a) {
-        SampleState& ss = S[batch[a]];
-        const size_t ci = size_t(ss.pending);
-        P.task_stage.h[a] = ss.task_for(ci, ci == 0 ? 1.0 : ap.kdist_cutoff);  // init_params, src/dada.rs:835-838
-        if (ss.lock_dirty) {
-          rc = P.push_locks(ss.base, ss.n);
-          if (rc) break;
-          ss.lock_dirty = false;
+      std::vector<size_t> batch;
+      double my_wait = 0.0;
+      for (;;) {
+        batch.clear();
+        {
+          std::unique_lock<std::mutex> lk(mu);
+          cv.wait(lk, [&] { return !ready.empty() || finished == ns || rc != 0; });
+          if (ready.empty() || rc != 0) break;
+          batch.swap(ready);
+        }
+        std::sort(batch.begin(), batch.end());
+        int r = L.ensure_tasks(uint32_t(batch.size()));
+        for (size_t a = 0; a < batch.size() && !r; ++a) {
+          SampleState& ss = S[batch[a]];
+          const size_t ci = size_t(ss.pending);
+          L.task_stage.h[a] = ss.task_for(ci, ci == 0 ? 1.0 : ap.kdist_cutoff);  // init_params, src/dada.rs:835-838
+          if (ss.lock_dirty) {
+            r = P.push_locks(ss.base, ss.n, L.st);
+            ss.lock_dirty = false;
+          }
+        }
+        const auto tc = Clock::now();
+        if (!r) r = L.run_compare(uint32_t(batch.size()), true, &my_wait);
+        if (r) {
+          std::lock_guard<std::mutex> g(mu);
+          if (!rc) {
+            rc = r;
+            err_msg = g_err;
+          }
+          cv.notify_all();
+          break;
+        }
+        const double tcmp = secs(tc, Clock::now());
+        for (size_t a = 0; a < batch.size(); ++a) {
+          SampleState& ss = S[batch[a]];
+          ss.absorb(size_t(ss.pending), L, uint32_t(a));
+          ss.stats.t_compare += tcmp;
+        }
+        for (size_t a = 0; a < batch.size(); ++a) {
+          const size_t sidx = batch[a];
+          jobs.submit([&, sidx] {
+            SampleState& ss = S[sidx];
+            auto th = Clock::now();
+            ss.pending = ss.advance(size_t(ss.pending));
+            const double dh = secs(th, Clock::now());
+            ss.stats.t_host += dh;
+            host_ns += int64_t(1e9 * dh);
+            std::lock_guard<std::mutex> g(mu);
+            if (ss.pending >= 0) {
+              ready.push_back(sidx);
+            } else {
+              ++finished;
+              ss.stats.t_done = secs(t_start, Clock::now());
+            }
+            cv.notify_all();
+          }, int64_t(S[sidx].n));  // larger samples have the longer chains: serve them first
         }
       }
-      if (rc) break;
-      auto tc = Clock::now();
-      rc = P.run_compare(uint32_t(batch.size()), true, &wait);
-      if (rc) break;
-      const double tcmp = secs(tc, Clock::now());
-      for (size_t a = 0; a < batch.size(); ++a) {
-        SampleState& ss = S[batch[a]];
-        ss.absorb(size_t(ss.pending), P, uint32_t(a));
-        ss.stats.t_compare += tcmp;
-      }
-      for (size_t a = 0; a < batch.size(); ++a) {
-        const size_t sidx = batch[a];
-        jobs.submit([&, sidx] {
-          SampleState& ss = S[sidx];
-          auto th = Clock::now();
-          ss.pending = ss.advance(size_t(ss.pending));
-          const double dh = secs(th, Clock::now());
-          ss.stats.t_host += dh;
-          host_ns += int64_t(1e9 * dh);
-          std::lock_guard<std::mutex> g(mu);
-          if (ss.pending >= 0) ready.push_back(sidx);
-          else ++finished;
-          cv.notify_one();
-        });
-      }
-    }
-    if (rc) {  // let queued host phases drain before the queue is torn down
-      std::unique_lock<std::mutex> lk(mu);
-      lk.unlock();
-    }
-  }
+      std::lock_guard<std::mutex> g(mu);
+      wait += my_wait;
+    };
+    const size_t nw = std::min(P.slots.size(), ns);
+    std::vector<std::thread> th;
+    for (size_t k = 1; k < nw; ++k) th.emplace_back(worker, std::ref(*P.slots[k]));
+    worker(*P.slots[0]);
+    for (auto& t : th) t.join();
+  }  // the job queue drains its queued host phases here
   const double total = secs(t_start, Clock::now());
   for (auto& ss : S) {
-    ss.stats.t_total = total;
+    ss.stats.t_total = ss.stats.t_done >= 0 ? ss.stats.t_done : total;
     ss.stats.t_wait = wait;
   }
-  return rc;
+  if (rc) return fail(rc, err_msg);
+  return 0;
+}
+
+// Launch slots for a batch of nsamples: DGPU_LAUNCH_SLOTS (1..8) if set, else
+// 2; never more than there are samples.
+static int launch_slots(int nsamples) {
+  int k = 2;
+  if (const char* e = std::getenv("DGPU_LAUNCH_SLOTS")) {
+    const int v = std::atoi(e);
+    if (v >= 1 && v <= 8) k = v;
+  }
+  return std::max(1, std::min(k, nsamples));
 }
 
 // A prepared batch: encoded samples resident on one device.
@@ -1538,7 +1826,7 @@ static int batch_prepare(Batch& B, int device, const dgpu_dada_params* prm, int 
       B.priors.push_back(si.prior[r]);
     }
   }
-  TRY(B.pool.init(device));
+  TRY(B.pool.init(device, launch_slots(nsamples)));
   const KParams kp = to_kparams(prm->align, prm->use_quals, prm->greedy, ncol2);
   TRY(B.pool.upload(uint32_t(off.size()), seqcat.data(), off.data(), len.data(), any_q ? qualcat.data() : nullptr,
                     B.reads.data(), kp, err.data()));
@@ -1568,6 +1856,7 @@ static int batch_run(Batch& B, dgpu_result** out) {
   TRY(P.reset_e_minmax());
   std::memset(P.lock_host.h, 0, P.nraw);
   CUDA_TRY(cudaMemsetAsync(P.lock.p, 0, P.nraw, P.st));
+  CUDA_TRY(cudaStreamSynchronize(P.st));  // the launch slots run on their own streams
   std::vector<SampleState> S(ns);
   for (size_t s = 0; s < ns; ++s)
     S[s].init(B.in[s].n, B.bases[s], B.reads.data() + B.bases[s], B.priors.data() + B.bases[s],
@@ -1654,7 +1943,7 @@ int dgpu_upload_raws(dgpu_ctx* ctx, int nraw, const uint8_t* seqs, const uint32_
 int dgpu_set_locks(dgpu_ctx* ctx, const uint8_t* lock) {
   if (!ctx || !ctx->uploaded || !lock) return fail(DGPU_E_INVALID, "no raws uploaded or null lock");
   std::memcpy(ctx->pool.lock_host.h, lock, ctx->pool.nraw);
-  TRY(ctx->pool.push_locks(0, ctx->pool.nraw));
+  TRY(ctx->pool.push_locks(0, ctx->pool.nraw, ctx->pool.st));
   CUDA_TRY(cudaStreamSynchronize(ctx->pool.st));
   return 0;
 }
@@ -1674,7 +1963,7 @@ static int ctx_task(dgpu_ctx* ctx, int center, int cluster_i, double cutoff, int
   if (!ctx || !ctx->uploaded) return fail(DGPU_E_INVALID, "no raws uploaded");
   if (center < 0 || uint32_t(center) >= ctx->pool.nraw) return fail(DGPU_E_INVALID, "center out of range");
   ctx->pool.kp.greedy = greedy ? 1 : 0;
-  TRY(ctx->pool.ensure_tasks(1));
+  TRY(ctx->pool.slot0().ensure_tasks(1));
   TaskDev T{};
   T.base = 0;
   T.n = ctx->pool.nraw;
@@ -1685,7 +1974,7 @@ static int ctx_task(dgpu_ctx* ctx, int center, int cluster_i, double cutoff, int
   T.total_reads = double(uint32_t(tot));
   T.cutoff = cutoff;
   T.cluster = uint32_t(cluster_i);
-  ctx->pool.task_stage.h[0] = T;
+  ctx->pool.slot0().task_stage.h[0] = T;
   return 0;
 }
 
@@ -1705,7 +1994,7 @@ int dgpu_compare(dgpu_ctx* ctx, int center, double kdist_cutoff, int greedy, dou
                  uint32_t* hamming_out, uint8_t* skipped_out, dgpu_counters* cnt) {
   TRY(ctx_task(ctx, center, 0, kdist_cutoff, greedy));
   Pool& P = ctx->pool;
-  TRY(P.run_compare(1, false, nullptr));
+  TRY(P.slot0().run_compare(1, false, nullptr));
   const uint32_t n = P.nraw;
   std::vector<uint8_t> st(n);
   if (lambda_out) CUDA_TRY(cudaMemcpy(lambda_out, P.lambda.p, size_t(n) * 8, cudaMemcpyDeviceToHost));
@@ -1734,7 +2023,7 @@ int dgpu_compare_store(dgpu_ctx* ctx, int center, int cluster_i, double kdist_cu
                        uint32_t* comp_index, double* comp_lambda, uint32_t* comp_hamming, int* nstored,
                        double* self_out, dgpu_counters* cnt) {
   TRY(ctx_task(ctx, center, cluster_i, kdist_cutoff, greedy));
-  Pool& P = ctx->pool;
+  Slot& P = ctx->pool.slot0();
   TRY(P.run_compare(1, true, nullptr));
   uint32_t ctr[TC_NCOUNTERS];
   P.task_counters(0, ctr);
@@ -1794,6 +2083,12 @@ int dgpu_dada_batch(int device, const dgpu_dada_params* params, int nsamples, co
   TRY(batch_prepare(b.b, device, params, nsamples, sample_start, seqs, offs, lens, abund, prior, qual_sums, err_mat,
                     ncol));
   return batch_run(b.b, out);
+}
+
+int dgpu_cache_release(int device, uint64_t* freed) {
+  const size_t n = cache_release(device);
+  if (freed) *freed = uint64_t(n);
+  return 0;
 }
 
 int dgpu_stats_reset(void) {

@@ -13,6 +13,7 @@
 //
 // Built with --fmad=false: the FP64 product and the k-mer distances must round
 // exactly like the reference's separately-rounded operations.
+#include <atomic>
 #include <algorithm>
 #include <cfloat>
 #include <cstdio>
@@ -616,8 +617,8 @@ __device__ VecSmem carve_vec(unsigned char* base, int lmax, int ncol_bound) {
 // each row's 2-bit pointers are two ballot bit-planes per 32 columns, buffered
 // 32 rows per flush to the per-warp scratch.
 template <int M>
-__device__ bool vec_align_reg(int lane, const uint8_t* g1, int l1, const uint8_t* g2, int l2, int16_t match,
-                              int16_t mismatch, int16_t gap, int16_t egp, int band_in, const VecSmem& S,
+__device__ bool vec_align_reg(int lane, const uint8_t* g1, int l1, const uint8_t* g2, int l2, int16_t match16,
+                              int16_t mismatch16, int16_t gap16, int16_t egp16, int band_in, const VecSmem& S,
                               uint32_t* pscr, int nrow_bound, uint32_t* ham_out, uint32_t* err_word, uint8_t* dbg0,
                               uint8_t* dbg1, uint32_t* dbg_len) {
   const bool swap = l1 > l2;
@@ -636,201 +637,225 @@ __device__ bool vec_align_reg(int lane, const uint8_t* g1, int l1, const uint8_t
     if (lane == 0) atomicOr(err_word, DERR_GEOMETRY);
     return false;
   }
-  const int16_t min_score = min(min(min(mismatch, gap), match), int16_t(0));
-  const int16_t fill = int16_t(uint16_t(uint16_t(0x8000u) - uint16_t(min_score)));
+  // i16 scores held in int lanes; every add saturates to the i16 range exactly
+  // as i16::saturating_add does.
+  const int match = match16, mismatch = mismatch16, gap = gap16, egp = egp16;
+  const int min_score = min(min(min(mismatch, gap), match), 0);
+  const int fill = int(int16_t(uint16_t(uint16_t(0x8000u) - uint16_t(min_score))));
+  auto sat = [](int v) { return max(-32768, min(32767, v)); };
   const int lfl = 1 + min(band, len1);
   const int tfl = 1 + min(band + len2 - len1, len2);
+  const int edge_rows = max(lfl, tfl);
   auto left_col = [&](int row) { int a = start_col - 1, b = (row - 1) / 2; return a > b ? a - b : 0; };
   auto top_col = [&](int row) { return start_col + row / 2; };
-  int16_t r3[M], r2[M], r1[M];
+  int r3[M], r2[M], r1[M];
+  bool sentinel[M];
   uint32_t pbuf[2 * M];
 #pragma unroll
   for (int m = 0; m < M; ++m) {
     const int c = lane + 32 * m;
-    const bool sent = c == 0 || c == 1 || c == ncol - 2 || c == ncol - 1;
-    int16_t v0 = sent ? fill : int16_t(0);
+    sentinel[m] = c == 0 || c == 1 || c == ncol - 2 || c == ncol - 1;
+    int v0 = sentinel[m] ? fill : 0;
     if (c == start_col) v0 = 0;
-    int16_t v1 = sent ? fill : int16_t(0);
-    uint8_t c1 = 0;
+    int v1 = sentinel[m] ? fill : 0;
+    uint32_t c1 = 0;
     if (1 < lfl && c == left_col(1)) { v1 = egp; c1 = 3; }
     if (1 < tfl && c == top_col(1)) { v1 = egp; c1 = 2; }
     r3[m] = 0;
     r2[m] = v0;
     r1[m] = v1;
     const uint32_t w0 = __ballot_sync(FULL, c1 & 1), w1 = __ballot_sync(FULL, (c1 >> 1) & 1);
-    pbuf[2 * m] = lane == 0 ? 0u : (lane == 1 ? w0 : 0u);
-    pbuf[2 * m + 1] = lane == 0 ? 0u : (lane == 1 ? w1 : 0u);
+    pbuf[2 * m] = lane == 1 ? w0 : 0u;
+    pbuf[2 * m + 1] = lane == 1 ? w1 : 0u;
   }
   __syncwarp();
-  int16_t row_free = egp;
+  int row_free = egp;
   int col_min = start_col, col_max = start_col, i_max = 0, j_min = 0;
-  bool even = true, recalc_left = false, recalc_right = false;
+  bool recalc_left = false, recalc_right = false;
   const int band_mod2 = band % 2;
   const int top_limit = min(band + len2 - len1, len2);
   const int full_band = band + len2 - len1;
   const int last = len1 + len2;
-  bool ok = true;
   const int bt_row1 = min(band, len1);
   const int bt_row2 = min(band + len2 - len1, len2);
   const bool fb_even = full_band % 2 == 0;
-  for (int row = 2; row <= last; ++row) {
-    const int n = col_max - col_min + 1;
-    const int eo = even ? 1 : 0;
-    const int left_off = col_min - eo, up_off = col_min + 1 - eo;
-    if ((col_max < col_min) | (col_max >= ncol) | (left_off < 0) | (up_off + n > ncol)) { ok = false; break; }
-    row_free = sadd16(row_free, egp);
-    int k_lo = i_max - len1 + 1;
-    k_lo = k_lo < 0 ? 0 : (k_lo > n ? n : k_lo);
-    int k_hi = min(i_max + 1, len2 - j_min);
-    k_hi = k_hi < 0 ? 0 : (k_hi > n ? n : k_hi);
-    k_hi = max(k_hi, k_lo);
-    const int lcol = row < lfl ? left_col(row) : -1;
-    const int tcol = row < tfl ? top_col(row) : -1;
-    int16_t cur[M];
-    uint8_t cc[M];
+  const bool do_recalc = egp > gap;
+  bool bad = false;
+  // Rows go in even/odd pairs so that the anti-diagonal parity is known at
+  // compile time: an even row reads its left neighbour from column c-1 and its
+  // up neighbour from column c of the previous row, an odd row from c and c+1.
+  // A corrupted band state cannot address memory out of bounds (sequence reads
+  // are range-tested, lane indexes are masked), so it is checked once per pair.
+  for (int row0 = 2; row0 <= last; row0 += 2) {
 #pragma unroll
-    for (int m = 0; m < M; ++m) {
-      const int16_t a = int16_t(__shfl_up_sync(FULL, int(r1[m]), 1));
-      const int16_t a31 = m > 0 ? int16_t(__shfl_sync(FULL, int(r1[m > 0 ? m - 1 : 0]), 31)) : int16_t(0);
-      const int16_t b = int16_t(__shfl_down_sync(FULL, int(r1[m]), 1));
-      const int16_t b0 = (m + 1 < M) ? int16_t(__shfl_sync(FULL, int(r1[m + 1 < M ? m + 1 : m]), 0)) : int16_t(0);
-      const int16_t lm1 = lane == 0 ? a31 : a;   // row-1 value at column c-1
-      const int16_t rp1 = lane == 31 ? b0 : b;   // row-1 value at column c+1
-      const int c = lane + 32 * m;
-      int16_t v = r3[m];
-      uint8_t code = 0;
-      if (c == 0 || c == 1 || c == ncol - 2 || c == ncol - 1) v = fill;
-      if (c == lcol) { v = row_free; code = 3; }
-      if (c == tcol) { v = row_free; code = 2; }
-      if (c >= col_min && c <= col_max) {
-        const int k = c - col_min;
-        int16_t sc;
-        if (k < k_lo || k >= k_hi) sc = fill;
-        else sc = (S.s1[i_max - k] == S.s2[j_min + k]) ? match : mismatch;
-        const int16_t dg = sadd16(r2[m], sc);
-        const int16_t l = sadd16(eo ? lm1 : r1[m], gap);
-        const int16_t u = sadd16(eo ? r1[m] : rp1, gap);
-        int16_t e;
-        uint8_t pe;
-        if (swap) {
-          if (l >= u) { e = l; pe = 2; } else { e = u; pe = 3; }
+    for (int ph = 0; ph < 2; ++ph) {
+      const int row = row0 + ph;
+      if (ph == 1 && row > last) break;
+      const bool E = ph == 0;
+      const int n = col_max - col_min + 1;
+      const int eo = E ? 1 : 0;
+      const int left_off = col_min - eo, up_off = col_min + 1 - eo;
+      bad |= (col_max < col_min) | (col_max >= ncol) | (left_off < 0) | (up_off + n > ncol);
+      row_free = sat(row_free + egp);
+      int lcol = -1, tcol = -1;
+      if (row < edge_rows) {  // ends-free edge cells exist only near the start
+        lcol = row < lfl ? left_col(row) : -1;
+        tcol = row < tfl ? top_col(row) : -1;
+      }
+      int cur[M];
+      uint32_t cc[M];
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        int nb;  // the previous row's value in the column this parity reads besides c
+        if (E) {
+          const int a = __shfl_up_sync(FULL, r1[m], 1);
+          const int a31 = m > 0 ? __shfl_sync(FULL, r1[m > 0 ? m - 1 : 0], 31) : 0;
+          nb = lane == 0 ? a31 : a;  // column c-1
         } else {
-          if (u >= l) { e = u; pe = 3; } else { e = l; pe = 2; }
+          const int b = __shfl_down_sync(FULL, r1[m], 1);
+          const int b0 = (m + 1 < M) ? __shfl_sync(FULL, r1[m + 1 < M ? m + 1 : m], 0) : 0;
+          nb = lane == 31 ? b0 : b;  // column c+1
         }
-        if (dg > e) { e = dg; pe = 1; }
-        v = e;
-        code = pe;
+        const int c = lane + 32 * m;
+        int v = sentinel[m] ? fill : r3[m];
+        uint32_t code = 0;
+        if (c == lcol) { v = row_free; code = 3; }
+        if (c == tcol) { v = row_free; code = 2; }
+        const int k = c - col_min;
+        if ((unsigned)k < (unsigned)n) {
+          const int si = i_max - k, sj = j_min + k;
+          int sc = fill;
+          if ((unsigned)si < (unsigned)len1 && (unsigned)sj < (unsigned)len2)
+            sc = (S.s1[si] == S.s2[sj]) ? match : mismatch;
+          const int dg = sat(r2[m] + sc);
+          const int l = sat((E ? nb : r1[m]) + gap);
+          const int u = sat((E ? r1[m] : nb) + gap);
+          int e;
+          uint32_t pe;
+          if (swap) {
+            const bool lw = l >= u;
+            e = lw ? l : u;
+            pe = lw ? 2u : 3u;
+          } else {
+            const bool uw = u >= l;
+            e = uw ? u : l;
+            pe = uw ? 3u : 2u;
+          }
+          const bool dw = dg > e;
+          v = dw ? dg : e;
+          code = dw ? 1u : pe;
+        }
+        cur[m] = v;
+        cc[m] = code;
       }
-      cur[m] = v;
-      cc[m] = code;
-    }
-    {  // band transition at the wedge boundaries (src/nwalign.rs:980-987), branch-free
-      const bool t1 = row == bt_row1;
-      col_min = t1 ? sat_sub1(col_min) : col_min;
-      i_max += t1 ? 1 : 0;
-      j_min -= t1 ? 1 : 0;
-      col_max += (row == bt_row2) ? 1 : 0;
-    }
-    if (egp > gap) {
-      if (recalc_left) {
-        int16_t pv = r1[0];
+      {  // band transition at the wedge boundaries (src/nwalign.rs:980-987)
+        const bool t1 = row == bt_row1;
+        col_min = t1 ? sat_sub1(col_min) : col_min;
+        i_max += t1 ? 1 : 0;
+        j_min -= t1 ? 1 : 0;
+        col_max += (row == bt_row2) ? 1 : 0;
+      }
+      if (do_recalc) {
+        if (recalc_left) {
+          int pv = r1[0];
 #pragma unroll
-        for (int m = 1; m < M; ++m)
-          if ((left_off >> 5) == m) pv = r1[m];
-        pv = int16_t(__shfl_sync(FULL, int(pv), left_off & 31));
-        const int16_t d_free = sadd16(pv, egp);
+          for (int m = 1; m < M; ++m)
+            if ((left_off >> 5) == m) pv = r1[m];
+          pv = __shfl_sync(FULL, pv, left_off & 31);
+          const int d_free = sat(pv + egp);
 #pragma unroll
-        for (int m = 0; m < M; ++m) {
-          if (lane + 32 * m == col_min) {
-            const int16_t cv = cur[m];
-            const uint8_t pc = cc[m];
-            if (d_free > cv) {
-              cur[m] = d_free;
-              cc[m] = 2;
-            } else if (!(d_free != cv || (!swap && pc != 1) || (swap && pc == 2))) {
-              cc[m] = 2;
+          for (int m = 0; m < M; ++m) {
+            if (lane + 32 * m == col_min) {
+              const int cv = cur[m];
+              const uint32_t pc = cc[m];
+              if (d_free > cv) {
+                cur[m] = d_free;
+                cc[m] = 2;
+              } else if (!(d_free != cv || (!swap && pc != 1) || (swap && pc == 2))) {
+                cc[m] = 2;
+              }
             }
           }
         }
-      }
-      if (i_max == len1 - 1) recalc_left = true;
-      if (recalc_right) {
-        const int idx = up_off + col_max - col_min;
-        if (idx < 0 || idx >= ncol || col_max >= ncol) { ok = false; break; }
-        int16_t pv = r1[0];
+        if (i_max == len1 - 1) recalc_left = true;
+        if (recalc_right) {
+          const int idx = up_off + col_max - col_min;
+          bad |= idx < 0 || idx >= ncol || col_max >= ncol;
+          int pv = r1[0];
 #pragma unroll
-        for (int m = 1; m < M; ++m)
-          if ((idx >> 5) == m) pv = r1[m];
-        pv = int16_t(__shfl_sync(FULL, int(pv), idx & 31));
-        const int16_t d_free = sadd16(pv, egp);
+          for (int m = 1; m < M; ++m)
+            if ((idx >> 5) == m) pv = r1[m];
+          pv = __shfl_sync(FULL, pv, idx & 31);
+          const int d_free = sat(pv + egp);
 #pragma unroll
-        for (int m = 0; m < M; ++m) {
-          if (lane + 32 * m == col_max) {
-            const int16_t cv = cur[m];
-            const uint8_t pc = cc[m];
-            if (d_free > cv) {
-              cur[m] = d_free;
-              cc[m] = 3;
-            } else if (!(d_free != cv || (!swap && pc == 3) || (swap && pc != 1))) {
-              cc[m] = 3;
+          for (int m = 0; m < M; ++m) {
+            if (lane + 32 * m == col_max) {
+              const int cv = cur[m];
+              const uint32_t pc = cc[m];
+              if (d_free > cv) {
+                cur[m] = d_free;
+                cc[m] = 3;
+              } else if (!(d_free != cv || (!swap && pc == 3) || (swap && pc != 1))) {
+                cc[m] = 3;
+              }
             }
           }
         }
+        if ((row + 1) / 2 + col_max - start_col == len2) recalc_right = true;
       }
-      if ((row + 1) / 2 + col_max - start_col == len2) recalc_right = true;
-    }
 #pragma unroll
-    for (int m = 0; m < M; ++m) {
-      const uint32_t w0 = __ballot_sync(FULL, cc[m] & 1), w1 = __ballot_sync(FULL, (cc[m] >> 1) & 1);
-      if (lane == (row & 31)) {
-        pbuf[2 * m] = w0;
-        pbuf[2 * m + 1] = w1;
+      for (int m = 0; m < M; ++m) {
+        const uint32_t w0 = __ballot_sync(FULL, cc[m] & 1u), w1 = __ballot_sync(FULL, cc[m] & 2u);
+        if (lane == (row & 31)) {
+          pbuf[2 * m] = w0;
+          pbuf[2 * m + 1] = w1;
+        }
       }
-    }
-    if ((row & 31) == 31 || row == last) {
-      const int base = row & ~31;
-      if (base + lane <= row) {
-        uint32_t* dst = pscr + size_t(base + lane) * (2 * M);
+      if ((row & 31) == 31 || row == last) {
+        const int base = row & ~31;
+        if (base + lane <= row) {
+          uint32_t* dst = pscr + size_t(base + lane) * (2 * M);
 #pragma unroll
-        for (int w = 0; w < 2 * M; ++w) dst[w] = pbuf[w];
+          for (int w = 0; w < 2 * M; ++w) dst[w] = pbuf[w];
+        }
       }
-    }
-    {  // advance the band for the next anti-diagonal (src/nwalign.rs:1028-1079), branch-free
-      const bool e = even;
-      const bool regA = row < band && row < len1;
-      const bool regB = !regA && i_max < len1 - 1;
-      const int cm = col_min, im = i_max, jm = j_min;
-      const int cmA = e ? sat_sub1(cm) : cm, imA = im + 1, jmA = jm;
-      int cmB, imB, jmB;
-      if (band_mod2 == 0) {
-        cmB = cm;
-        imB = e ? im : im + 1;
-        jmB = e ? jm + 1 : jm;
-      } else {
-        cmB = e ? sat_sub1(cm) : cm + 1;
-        imB = e ? im + 1 : im;
-        jmB = e ? jm : jm + 1;
+      {  // advance the band for the next anti-diagonal (src/nwalign.rs:1028-1079)
+        const bool regA = row < band && row < len1;
+        const bool regB = !regA && i_max < len1 - 1;
+        const int cm = col_min, im = i_max, jm = j_min;
+        const int cmA = E ? sat_sub1(cm) : cm, imA = im + 1, jmA = jm;
+        int cmB, imB, jmB;
+        if (band_mod2 == 0) {
+          cmB = cm;
+          imB = E ? im : im + 1;
+          jmB = E ? jm + 1 : jm;
+        } else {
+          cmB = E ? sat_sub1(cm) : cm + 1;
+          imB = E ? im + 1 : im;
+          jmB = E ? jm : jm + 1;
+        }
+        const int cmC = E ? cm : cm + 1, imC = im, jmC = jm + 1;
+        col_min = regA ? cmA : (regB ? cmB : cmC);
+        i_max = regA ? imA : (regB ? imB : imC);
+        j_min = regA ? jmA : (regB ? jmB : jmC);
+        const int cx = col_max;
+        const bool rt = row < top_limit;
+        const bool mid = !rt && ((row + 1) / 2 + cx - start_col < len2);
+        const int cxA = E ? cx : cx + 1;
+        const int cxB = fb_even ? (E ? sat_sub1(cx) : cx + 1) : cx;
+        const int cxC = E ? sat_sub1(cx) : cx;
+        col_max = rt ? cxA : (mid ? cxB : cxC);
       }
-      const int cmC = e ? cm : cm + 1, imC = im, jmC = jm + 1;
-      col_min = regA ? cmA : (regB ? cmB : cmC);
-      i_max = regA ? imA : (regB ? imB : imC);
-      j_min = regA ? jmA : (regB ? jmB : jmC);
-      const int cx = col_max;
-      const bool rt = row < top_limit;
-      const bool mid = !rt && ((row + 1) / 2 + cx - start_col < len2);
-      const int cxA = e ? cx : cx + 1;
-      const int cxB = fb_even ? (e ? sat_sub1(cx) : cx + 1) : cx;
-      const int cxC = e ? sat_sub1(cx) : cx;
-      col_max = rt ? cxA : (mid ? cxB : cxC);
-    }
 #pragma unroll
-    for (int m = 0; m < M; ++m) {
-      r3[m] = r2[m];
-      r2[m] = r1[m];
-      r1[m] = cur[m];
+      for (int m = 0; m < M; ++m) {
+        r3[m] = r2[m];
+        r2[m] = r1[m];
+        r1[m] = cur[m];
+      }
     }
-    even = !even;
+    if (bad) break;
   }
+  bool ok = !bad;
   if (!ok) {
     if (lane == 0) atomicOr(err_word, DERR_BAND_RANGE);
     return false;
@@ -843,7 +868,10 @@ __device__ bool vec_align_reg(int lane, const uint8_t* g1, int l1, const uint8_t
     }
   }
   __syncwarp();
-  // Traceback through the bit-planes, 32 rows staged in shared memory at a time.
+  // Traceback through the bit-planes. A window of up to 64 rows is staged in
+  // shared memory; lane t tests whether the t-th next step is diagonal (cell
+  // (i-t, j-t): row r-2t, same compressed column), so a run of f diagonal steps
+  // is taken at once, each lane doing one. A gap step is taken singly.
   const uint8_t* raw = swap ? S.s1 : S.s2;
   const int lraw = swap ? len1 : len2;
   for (int p = lane; p < lraw; p += 32) S.tcode[p] = uint8_t((unsigned(raw[p]) - 1u) * 5u);
@@ -854,11 +882,11 @@ __device__ bool vec_align_reg(int lane, const uint8_t* g1, int l1, const uint8_t
   __syncwarp();
   while (i > 0 || j > 0) {
     const int cs = 2 * start_col + j - i;
-    if (cs < 0) { ok = false; break; }
+    if (cs < 0 || cs / 2 >= ncol) { ok = false; break; }
     const int col = cs / 2;
     const int r = i + j;
-    if (r < slo) {
-      const int nlo = max(0, r - 31);
+    if (r < slo || (r - slo < 16 && slo > 0)) {
+      const int nlo = max(0, r - 63);
       __syncwarp();
       const int nw = (r - nlo + 1) * 2 * M;
       const uint32_t* src = pscr + size_t(nlo) * (2 * M);
@@ -866,28 +894,44 @@ __device__ bool vec_align_reg(int lane, const uint8_t* g1, int l1, const uint8_t
       __syncwarp();
       slo = nlo;
     }
-    const uint32_t* wrow = stage + (r - slo) * (2 * M) + 2 * (col >> 5);
-    const int bit = col & 31;
-    const int v = int((wrow[0] >> bit) & 1u) | (int((wrow[1] >> bit) & 1u) << 1);
-    if (v == 1 && i > 0 && j > 0) {
-      const uint8_t a = S.s1[i - 1], b = S.s2[j - 1];
-      const int rp = swap ? i - 1 : j - 1;
-      const uint8_t cn = swap ? b : a, rn = swap ? a : b;
-      if (lane == 0) S.tcode[rp] = uint8_t((unsigned(cn) - 1u) * 4u + (unsigned(rn) - 1u));
-      ham += (a != b) ? 1u : 0u;
-      if (dbg0 && lane == 0) {
-        dbg0[alen] = swap ? b : a;
-        dbg1[alen] = swap ? a : b;
+    const int rr = r - 2 * lane;
+    const bool inwin = rr >= slo;
+    int v = 0;
+    if (inwin) {
+      const uint32_t* wrow = stage + (rr - slo) * (2 * M) + 2 * (col >> 5);
+      const int bit = col & 31;
+      v = int((wrow[0] >> bit) & 1u) | (int((wrow[1] >> bit) & 1u) << 1);
+    }
+    const bool diag = inwin && v == 1 && i - lane > 0 && j - lane > 0;
+    const uint32_t nd = __ballot_sync(FULL, !diag);
+    const int f = nd ? __ffs(nd) - 1 : 32;
+    if (f > 0) {
+      bool mm = false;
+      if (lane < f) {
+        const uint8_t a = S.s1[i - 1 - lane], b = S.s2[j - 1 - lane];
+        const int rp = (swap ? i : j) - 1 - lane;
+        const uint8_t cn = swap ? b : a, rn = swap ? a : b;
+        S.tcode[rp] = uint8_t((unsigned(cn) - 1u) * 4u + (unsigned(rn) - 1u));
+        mm = a != b;
+        if (dbg0) {
+          dbg0[alen + lane] = swap ? b : a;
+          dbg1[alen + lane] = swap ? a : b;
+        }
       }
-      --i;
-      --j;
-    } else if (v == 2 && j > 0) {
+      ham += __popc(__ballot_sync(FULL, mm));
+      i -= f;
+      j -= f;
+      alen += uint32_t(f);
+      continue;
+    }
+    const int v0 = __shfl_sync(FULL, v, 0);
+    if (v0 == 2 && j > 0) {
       if (dbg0 && lane == 0) {
         dbg0[alen] = swap ? S.s2[j - 1] : uint8_t('-');
         dbg1[alen] = swap ? uint8_t('-') : S.s2[j - 1];
       }
       --j;
-    } else if (v == 3 && i > 0) {
+    } else if (v0 == 3 && i > 0) {
       if (dbg0 && lane == 0) {
         dbg0[alen] = swap ? uint8_t('-') : S.s1[i - 1];
         dbg1[alen] = swap ? S.s1[i - 1] : uint8_t('-');
@@ -1160,7 +1204,7 @@ __device__ bool rm_dispatch(int lane, const uint8_t* g1, int len1, const uint8_t
 // codes for ACGT input), method choice (src/nwalign.rs:1324-1403), then the
 // gapless alignment or the vectorized / row-major aligner, then lambda.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kNwWarps * 32, 4) k_align(CompareLaunch L) {
+__global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_align(CompareLaunch L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const uint32_t count = *(volatile uint32_t*)&L.queue_counts[4];
   if (blockIdx.x * kNwWarps >= count) return;  // nothing queued for this block
@@ -1391,6 +1435,17 @@ void launch_compare(const CompareLaunch& L, cudaStream_t st, cudaEvent_t* ev) {
   if (ev) cudaEventRecord(ev[1], st);
   const size_t asm_ = err_smem_bytes(L.kp.ncol) + size_t(kNwWarps) * align_smem_per_warp(L.geom);
   if (asm_ > 48 * 1024) cudaFuncSetAttribute(k_align, cudaFuncAttributeMaxDynamicSharedMemorySize, int(asm_));
+  {  // ask for the largest shared-memory carveout once per device so that
+     // kAlignCtasPerSm CTAs fit beside each other
+    static std::atomic<uint64_t> carved{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t bit = uint64_t(1) << (dev & 63);
+    if (!(carved.load(std::memory_order_relaxed) & bit)) {
+      cudaFuncSetAttribute(k_align, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+      carved.fetch_or(bit);
+    }
+  }
   k_align<<<L.geom.nwarps / kNwWarps, kNwWarps * 32, asm_, st>>>(L);
   if (ev) cudaEventRecord(ev[2], st);
   if (L.do_store) k_store<<<L.nstore_blocks, 1024, 0, st>>>(L);

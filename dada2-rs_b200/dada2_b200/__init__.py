@@ -32,7 +32,7 @@ KERNEL_NAMES = ["profiles", "screen", "align", "store"]
 METHOD_NAMES = {0: "none", 1: "gapless", 2: "vectorized", 3: "homo", 4: "endsfree"}
 COUNTER_KEYS = ["nalign", "compare_calls", "cmp_scanned", "screened", "aligned", "stored",
                 "gapless", "vectorized", "homo", "endsfree", "shuffle_calls", "shuffle_moves",
-                "nshroud"]
+                "nshroud", "ns_shuffle", "ns_pupdate", "ns_bud"]
 
 
 @dataclass
@@ -331,6 +331,14 @@ def _read_counters(h) -> dict:
     check(lib().dgpu_result_sizes(h, ptr(sizes)))
     return {"nclust": int(sizes[0]), "nraw": int(sizes[1]),
             "counters": {k: int(v) for k, v in zip(COUNTER_KEYS, cnt)}, "times": tm}
+
+
+def cache_release(device: int = -1) -> int:
+    """Frees the device and pinned host blocks finished pools left for reuse
+    (all devices when ``device`` < 0); returns the bytes given back."""
+    n = C.c_uint64(0)
+    check(lib().dgpu_cache_release(int(device), C.byref(n)))
+    return int(n.value)
 
 
 def stats_reset():

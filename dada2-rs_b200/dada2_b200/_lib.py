@@ -100,6 +100,7 @@ def lib():
         L.dgpu_batch_free.restype = None
         L.dgpu_stats_reset.argtypes = []
         L.dgpu_stats_timing.argtypes = [C.c_int]
+        L.dgpu_cache_release.argtypes = [C.c_int, C.POINTER(C.c_uint64)]
         L.dgpu_stats_read.argtypes = [C.POINTER(KernelStatsC)]
         L.dgpu_stats_latencies.argtypes = [_P, C.c_int]
         L.dgpu_align_debug.argtypes = [C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P,

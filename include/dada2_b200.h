@@ -74,9 +74,11 @@ typedef struct {
  * corrected to any cluster (src/dada.rs:525-533). counters (16 slots):
  * nalign, compare_calls, cmp_scanned (sum of nraw over compare calls),
  * screened, aligned, stored, gapless, vectorized, homo, endsfree,
- * shuffle_calls, shuffle_moves, nshroud. times (4 slots, seconds): this
- * sample's compare calls (launch to results), the whole call, this sample's
- * host phases (shuffle, p-update, bud), time the host waited on the device. */
+ * shuffle_calls, shuffle_moves, nshroud, then the nanoseconds this sample's
+ * host spent in shuffle, p-update and bud. times (4 slots, seconds): this
+ * sample's compare calls (launch to results), the time from the start of the
+ * clustering loop until this sample finished, this sample's host phases
+ * (shuffle, p-update, bud), time the host waited on the device. */
 typedef struct {
   uint32_t* cl_reads;
   int32_t* cl_birth_type;
@@ -161,6 +163,14 @@ int dgpu_batch_prepare(int device, const dgpu_dada_params* params, int nsamples,
                        const uint32_t* qual_sums, const double* err_mat, int ncol, dgpu_batch** out);
 int dgpu_batch_run(dgpu_batch* batch, dgpu_result** out);
 void dgpu_batch_free(dgpu_batch* batch);
+
+/* Device memory reuse. No counterpart in the reference (its compare step holds
+ * no device memory). A finished pool (dgpu_dada, dgpu_dada_batch,
+ * dgpu_batch_free) keeps its device and pinned host blocks in a per-device
+ * cache, at most 32 GiB of each kind per device, that the next call reuses.
+ * This frees every cached block of `device` (all devices when device < 0) and
+ * writes the bytes given back to *freed (may be NULL). */
+int dgpu_cache_release(int device, uint64_t* freed);
 
 int dgpu_stats_reset(void);
 int dgpu_stats_timing(int enable);
