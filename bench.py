@@ -270,6 +270,15 @@ def main():
     nclust = [r["nclust"] for r in res]
     t_max, comps_all = multi.reduce_run(dt, comps, device="cuda")
     value = comps_all / t_max
+    # pair outcomes of the last timed step, and the vectorized aligner's cells
+    # (the reference's cell model: (len1 + len2 + 1) x (band + 1) per pair)
+    mix = {k: int(sum(r["counters"][k] for r in res))
+           for k in ("screened", "aligned", "nshroud", "gapless", "vectorized", "homo", "endsfree")}
+    nw_cells = 0
+    for s, r in zip(w.samples, res):
+        L = int(np.median([len(q) for q in s.seqs]))
+        nw_cells += (r["counters"]["vectorized"] + r["counters"]["homo"] + r["counters"]["endsfree"]) * \
+            (2 * L + 1) * (w.band + 1)
 
     # ---- timed: end to end through the C ABI with host buffers ----
     barrier()
@@ -336,6 +345,11 @@ def main():
                      "algorithmic_bytes": "4^k profile bytes per non-skipped compare + 16 B metadata per compare",
                      "screen_ms_per_step": screen_ms / args.steps},
         "kernel_ms_per_step": {k: v / args.steps for k, v in st["ms"].items()},
+        "pairs_per_step": mix,
+        "nw": {"cells_per_step": nw_cells,
+               "gcups": (nw_cells / (st["ms"]["align"] / args.steps / 1e3) / 1e9) if st["ms"]["align"] > 0 else None,
+               "note": "cells = (len1+len2+1) x (band+1) per NW pair; gcups over the align kernel's device time, "
+                       "which also covers the gapless pairs and lambda"},
         "latency_ms": {"p50": float(np.percentile(lat, 50)) if len(lat) else None,
                        "p99": float(np.percentile(lat, 99)) if len(lat) else None,
                        "unit": "per batched compare call"},

@@ -80,9 +80,10 @@ struct NwGeom {
 // ---- shared-memory carving, used by kernels and by the host sizing code ----
 constexpr int kScreenWarps = 8;   // warps per screen CTA
 constexpr int kNwWarps = 4;       // warps per NW CTA
-constexpr int kAlignCtasPerSm = 5; // resident align CTAs per SM (96 registers per thread)
+constexpr int kAlignCtasPerSm = 4; // resident align CTAs per SM (128 registers per thread)
 constexpr int kStageBytes = 4096; // traceback staging per warp
 constexpr int kStoreSpan = 8192;  // raws per store CTA (its own output segment)
+constexpr int kSeqPad = 160;      // guard bytes on each side of the aligners' shared-memory sequences
 
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
 __host__ __device__ inline size_t err_smem_bytes(int ncol) { return align16(size_t(16) * size_t(ncol) * 8); }
@@ -95,7 +96,7 @@ __host__ __device__ inline int rm_kbound(int rm_pairs) {
   return b;
 }
 __host__ __device__ inline size_t nw_smem_per_warp_vec(const NwGeom& g) {
-  return align16(g.lmax) * 2 + align16(size_t(3) * g.vec_ncol * 2) + align16(size_t(g.vec_ncol) * 2) +
+  return align16(g.lmax + 2 * kSeqPad) * 2 + align16(size_t(3) * g.vec_ncol * 2) + align16(size_t(g.vec_ncol) * 2) +
          align16(g.vec_ncol) + align16(kStageBytes) + align16(g.lmax) + align16(size_t(g.lmax) * 2);
 }
 __host__ __device__ inline size_t nw_smem_per_warp_rm(const NwGeom& g) {

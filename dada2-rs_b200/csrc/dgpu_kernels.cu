@@ -598,8 +598,8 @@ __device__ VecSmem carve_vec(unsigned char* base, int lmax, int ncol_bound) {
   VecSmem S;
   size_t o = 0;
   auto take = [&](size_t bytes) { unsigned char* p = base + o; o += (bytes + 15) & ~size_t(15); return p; };
-  S.s1 = take(lmax);
-  S.s2 = take(lmax);
+  S.s1 = take(lmax + 2 * kSeqPad) + kSeqPad;  // guard bytes before and after
+  S.s2 = take(lmax + 2 * kSeqPad) + kSeqPad;
   S.rows = reinterpret_cast<int16_t*>(take(size_t(3) * ncol_bound * 2));
   S.diag = reinterpret_cast<int16_t*>(take(size_t(ncol_bound) * 2));
   S.prow = take(ncol_bound);
@@ -609,6 +609,99 @@ __device__ VecSmem carve_vec(unsigned char* base, int lmax, int ncol_bound) {
   return S;
 }
 
+
+// Traceback through the pointer bit-planes of the register aligners
+// (src/nwalign.rs:1090-1139). With planes_smem the planes of every row are
+// already in S.stage; otherwise they are read from the per-warp scratch.
+template <int M>
+__device__ bool reg_traceback(int lane, bool swap, int len1, int len2, int start_col, int ncol, const VecSmem& S,
+                              const uint32_t* pscr, bool planes_smem, uint32_t* ham_out, uint32_t* err_word,
+                              uint8_t* dbg0, uint8_t* dbg1, uint32_t* dbg_len) {
+  bool ok = true;
+  // Traceback through the bit-planes. A window of up to 64 rows is staged in
+  // shared memory; lane t tests whether the t-th next step is diagonal (cell
+  // (i-t, j-t): row r-2t, same compressed column), so a run of f diagonal steps
+  // is taken at once, each lane doing one. A gap step is taken singly.
+  const uint8_t* raw = swap ? S.s1 : S.s2;
+  const int lraw = swap ? len1 : len2;
+  for (int p = lane; p < lraw; p += 32) S.tcode[p] = uint8_t((unsigned(raw[p]) - 1u) * 5u);
+  uint32_t* stage = reinterpret_cast<uint32_t*>(S.stage);
+  int slo = planes_smem ? 0 : 0x7fffffff;  // planes already in shared memory: no staging
+  int i = len1, j = len2;
+  uint32_t ham = 0, alen = 0;
+  __syncwarp();
+  while (i > 0 || j > 0) {
+    const int cs = 2 * start_col + j - i;
+    if (cs < 0 || cs / 2 >= ncol) { ok = false; break; }
+    const int col = cs / 2;
+    const int r = i + j;
+    if (!planes_smem && (r < slo || (r - slo < 16 && slo > 0))) {
+      const int nlo = max(0, r - 63);
+      __syncwarp();
+      const int nw = (r - nlo + 1) * 2 * M;
+      const uint32_t* src = pscr + size_t(nlo) * (2 * M);
+      for (int x = lane; x < nw; x += 32) stage[x] = src[x];
+      __syncwarp();
+      slo = nlo;
+    }
+    const int rr = r - 2 * lane;
+    const bool inwin = rr >= slo;
+    int v = 0;
+    if (inwin) {
+      const uint32_t* wrow = stage + (rr - slo) * (2 * M) + 2 * (col >> 5);
+      const int bit = col & 31;
+      v = int((wrow[0] >> bit) & 1u) | (int((wrow[1] >> bit) & 1u) << 1);
+    }
+    const bool diag = inwin && v == 1 && i - lane > 0 && j - lane > 0;
+    const uint32_t nd = __ballot_sync(FULL, !diag);
+    const int f = nd ? __ffs(nd) - 1 : 32;
+    if (f > 0) {
+      bool mm = false;
+      if (lane < f) {
+        const uint8_t a = S.s1[i - 1 - lane], b = S.s2[j - 1 - lane];
+        const int rp = (swap ? i : j) - 1 - lane;
+        const uint8_t cn = swap ? b : a, rn = swap ? a : b;
+        S.tcode[rp] = uint8_t((unsigned(cn) - 1u) * 4u + (unsigned(rn) - 1u));
+        mm = a != b;
+        if (dbg0) {
+          dbg0[alen + lane] = swap ? b : a;
+          dbg1[alen + lane] = swap ? a : b;
+        }
+      }
+      ham += __popc(__ballot_sync(FULL, mm));
+      i -= f;
+      j -= f;
+      alen += uint32_t(f);
+      continue;
+    }
+    const int v0 = __shfl_sync(FULL, v, 0);
+    if (v0 == 2 && j > 0) {
+      if (dbg0 && lane == 0) {
+        dbg0[alen] = swap ? S.s2[j - 1] : uint8_t('-');
+        dbg1[alen] = swap ? uint8_t('-') : S.s2[j - 1];
+      }
+      --j;
+    } else if (v0 == 3 && i > 0) {
+      if (dbg0 && lane == 0) {
+        dbg0[alen] = swap ? uint8_t('-') : S.s1[i - 1];
+        dbg1[alen] = swap ? S.s1[i - 1] : uint8_t('-');
+      }
+      --i;
+    } else {
+      ok = false;
+      break;
+    }
+    ++alen;
+  }
+  __syncwarp();
+  if (!ok) {
+    if (lane == 0) atomicOr(err_word, DERR_TRACEBACK);
+    return false;
+  }
+  if (dbg_len && lane == 0) *dbg_len = alen;
+  *ham_out = ham;
+  return true;
+}
 
 // Register form of the same aligner for compressed widths up to 32*M columns:
 // lane l owns columns l + 32m; the three rolling rows live in registers
@@ -868,89 +961,410 @@ __device__ bool vec_align_reg(int lane, const uint8_t* g1, int l1, const uint8_t
     }
   }
   __syncwarp();
-  // Traceback through the bit-planes. A window of up to 64 rows is staged in
-  // shared memory; lane t tests whether the t-th next step is diagonal (cell
-  // (i-t, j-t): row r-2t, same compressed column), so a run of f diagonal steps
-  // is taken at once, each lane doing one. A gap step is taken singly.
-  const uint8_t* raw = swap ? S.s1 : S.s2;
-  const int lraw = swap ? len1 : len2;
-  for (int p = lane; p < lraw; p += 32) S.tcode[p] = uint8_t((unsigned(raw[p]) - 1u) * 5u);
-  uint32_t* stage = reinterpret_cast<uint32_t*>(S.stage);
-  int slo = 0x7fffffff;
-  int i = len1, j = len2;
-  uint32_t ham = 0, alen = 0;
-  __syncwarp();
-  while (i > 0 || j > 0) {
-    const int cs = 2 * start_col + j - i;
-    if (cs < 0 || cs / 2 >= ncol) { ok = false; break; }
-    const int col = cs / 2;
-    const int r = i + j;
-    if (r < slo || (r - slo < 16 && slo > 0)) {
-      const int nlo = max(0, r - 63);
-      __syncwarp();
-      const int nw = (r - nlo + 1) * 2 * M;
-      const uint32_t* src = pscr + size_t(nlo) * (2 * M);
-      for (int x = lane; x < nw; x += 32) stage[x] = src[x];
-      __syncwarp();
-      slo = nlo;
+  return reg_traceback<M>(lane, swap, len1, len2, start_col, ncol, S, pscr, false, ham_out, err_word, dbg0, dbg1,
+                          dbg_len);
+}
+
+// Fast register form: the cells, pointers and band bookkeeping of
+// vec_align_reg, computed with fewer instructions and a shorter dependency
+// chain per anti-diagonal. Bit-identical results rest on three facts:
+//  * With gap <= 0, end gap <= 0 and P = max(match, mismatch, 0), a value on
+//    anti-diagonal r is at most P*floor(r/2) (each row adds at most P over the
+//    row two back, and nothing else increases a value), so when
+//    P*((len1+len2)/2 + 1) <= 32767 no sum can pass 32767 and i16::saturating_add
+//    reduces to max(a + b, -32768), one DPX add-max.
+//  * The swap tie rule is a template parameter.
+//  * The band state of anti-diagonal r+1 and its sequence bytes are formed
+//    before the cells of r, so bookkeeping and shared-memory loads overlap the
+//    shuffle -> add -> max chain that carries the recurrence.
+// The caller has copied the (swapped) sequences to S.s1/S.s2. The pointer
+// bit-planes go straight to S.stage when every row fits there (PS),
+// else to the per-warp global scratch in 32-row flushes.
+template <int M, bool SWAP, bool PS>
+__device__ bool vec_align_fast(int lane, int len1, int len2, int match, int mismatch, int gap, int egp, int band,
+                               const VecSmem& S, uint32_t* pscr, uint32_t* ham_out,
+                               uint32_t* err_word, uint8_t* dbg0, uint8_t* dbg1, uint32_t* dbg_len) {
+  constexpr int LO = -32768;
+  const int start_col = 1 + (min(band, len1) + 1) / 2;
+  const int ncol = 2 + start_col + min(band + len2 - len1, len2) / 2;
+  const int min_score = min(min(min(mismatch, gap), match), 0);
+  const int fill = int(int16_t(uint16_t(uint16_t(0x8000u) - uint16_t(min_score))));
+  const int lfl = 1 + min(band, len1);
+  const int tfl = 1 + min(band + len2 - len1, len2);
+  const int edge_rows = max(lfl, tfl);
+  auto left_col = [&](int row) { int a = start_col - 1, b = (row - 1) / 2; return a > b ? a - b : 0; };
+  auto top_col = [&](int row) { return start_col + row / 2; };
+  uint32_t* planes = reinterpret_cast<uint32_t*>(S.stage);
+  int r3[M], r2[M], r1[M];
+  bool sentinel[M];
+  uint32_t pbuf[2 * M];
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const int c = lane + 32 * m;
+    sentinel[m] = c == 0 || c == 1 || c == ncol - 2 || c == ncol - 1;
+    int v0 = sentinel[m] ? fill : 0;
+    if (c == start_col) v0 = 0;
+    int v1 = sentinel[m] ? fill : 0;
+    uint32_t c1 = 0;
+    if (1 < lfl && c == left_col(1)) { v1 = egp; c1 = 3; }
+    if (1 < tfl && c == top_col(1)) { v1 = egp; c1 = 2; }
+    r3[m] = 0;
+    r2[m] = v0;
+    r1[m] = v1;
+    const uint32_t w0 = __ballot_sync(FULL, c1 & 1), w1 = __ballot_sync(FULL, (c1 >> 1) & 1);
+    if (PS) {
+      if (lane == 0) {
+        planes[2 * m] = 0u;
+        planes[2 * m + 1] = 0u;
+        planes[2 * M + 2 * m] = w0;
+        planes[2 * M + 2 * m + 1] = w1;
+      }
+    } else {
+      pbuf[2 * m] = lane == 1 ? w0 : 0u;
+      pbuf[2 * m + 1] = lane == 1 ? w1 : 0u;
     }
-    const int rr = r - 2 * lane;
-    const bool inwin = rr >= slo;
-    int v = 0;
-    if (inwin) {
-      const uint32_t* wrow = stage + (rr - slo) * (2 * M) + 2 * (col >> 5);
-      const int bit = col & 31;
-      v = int((wrow[0] >> bit) & 1u) | (int((wrow[1] >> bit) & 1u) << 1);
+  }
+  int row_free = egp;
+  int col_min = start_col, col_max = start_col, i_max = 0, j_min = 0;
+  bool recalc_left = false, recalc_right = false;
+  const int band_mod2 = band % 2;
+  const int top_limit = min(band + len2 - len1, len2);
+  const int full_band = band + len2 - len1;
+  const int last = len1 + len2;
+  const int bt_row1 = min(band, len1);
+  const int bt_row2 = min(band + len2 - len1, len2);
+  const bool fb_even = full_band % 2 == 0;
+  const bool do_recalc = egp > gap;
+  bool bad = false;
+  // Diagonal scores. Lane c reads s1[A - c] and s2[B + c] with A = i_max +
+  // col_min and B = j_min - col_min; the guard bytes around each sequence
+  // (0x10 before/after s1, 0x20 around s2) make every out-of-range position
+  // score `fill`, and clamping the uniform A, B keeps every read inside the
+  // guards whatever the band state.
+  const uint8_t* p1[M];
+  const uint8_t* p2[M];
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    p1[m] = S.s1 - (lane + 32 * m);
+    p2[m] = S.s2 + (lane + 32 * m);
+  }
+  auto scores_at = [&](int A, int B, int* out) {
+    A = min(max(A, 32 * M - 1 - kSeqPad), len1 + kSeqPad - 1);
+    B = min(max(B, -kSeqPad), len2 + kSeqPad - 32 * M);
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const uint32_t a = p1[m][A], b = p2[m][B];
+      out[m] = a == b ? match : (((a | b) & 0x30u) ? fill : mismatch);
     }
-    const bool diag = inwin && v == 1 && i - lane > 0 && j - lane > 0;
-    const uint32_t nd = __ballot_sync(FULL, !diag);
-    const int f = nd ? __ffs(nd) - 1 : 32;
-    if (f > 0) {
-      bool mm = false;
-      if (lane < f) {
-        const uint8_t a = S.s1[i - 1 - lane], b = S.s2[j - 1 - lane];
-        const int rp = (swap ? i : j) - 1 - lane;
-        const uint8_t cn = swap ? b : a, rn = swap ? a : b;
-        S.tcode[rp] = uint8_t((unsigned(cn) - 1u) * 4u + (unsigned(rn) - 1u));
-        mm = a != b;
-        if (dbg0) {
-          dbg0[alen + lane] = swap ? b : a;
-          dbg1[alen + lane] = swap ? a : b;
+  };
+  int sc[M];
+  scores_at(i_max + col_min, j_min - col_min, sc);
+  // Middle rows: past the ends-free edge cells and both wedge transitions,
+  // inside regime B of the band advance with no recalc pending. There the
+  // advance is fixed by the row's parity -- an even row adds 1 to B, an odd row
+  // adds 1 to A, col_min moves by -1/+1 when the band is odd and col_max by
+  // -1/+1 when band + len2 - len1 is even -- so (col_min, col_max) repeat every
+  // two rows and the range checks of the first middle pair cover the rest.
+  const int mid_lo = max(edge_rows - 1, max(bt_row1, bt_row2));
+  const int dcm = band_mod2 ? -1 : 0;  // col_min change on an even row (undone on the odd row)
+  const int dcx = fb_even ? -1 : 0;    // col_max change on an even row (undone on the odd row)
+  bool mid_checked = false;
+  for (int row0 = 2; row0 <= last; row0 += 2) {
+    const bool mid_pair = row0 > mid_lo && row0 + 1 <= last && !recalc_left && !recalc_right &&
+                          i_max + band_mod2 < len1 - 1 && (row0 + 1) / 2 + col_max - start_col < len2 &&
+                          (row0 + 2) / 2 + col_max + dcx - start_col < len2;
+    if (mid_pair) {
+      if (!mid_checked) {  // the checks of the generic rows, for this pair's two rows
+        const int cm1 = col_min + dcm, cx1 = col_max + dcx;
+        bad |= (col_max < col_min) | (col_max >= ncol) | (col_min - 1 < 0) | (col_max + 1 > ncol);
+        bad |= (cx1 < cm1) | (cx1 >= ncol) | (cm1 < 0) | (cx1 + 2 > ncol);
+        mid_checked = true;
+        if (bad) break;
+      }
+      int A = i_max + col_min, B = j_min - col_min;
+#pragma unroll
+      for (int ph = 0; ph < 2; ++ph) {
+        const bool E = ph == 0;
+        const int row = row0 + ph;
+        const unsigned n = unsigned(col_max - col_min + 1);
+        int cur[M];
+        bool b0[M], b1[M];
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+          int nb;
+          if (E) {
+            const int a = __shfl_up_sync(FULL, r1[m], 1);
+            if (M > 1) {
+              const int a31 = m > 0 ? __shfl_sync(FULL, r1[m > 0 ? m - 1 : 0], 31) : 0;
+              nb = lane == 0 ? a31 : a;
+            } else {
+              nb = a;
+            }
+          } else {
+            const int b = __shfl_down_sync(FULL, r1[m], 1);
+            if (M > 1) {
+              const int b0 = (m + 1 < M) ? __shfl_sync(FULL, r1[m + 1 < M ? m + 1 : m], 0) : 0;
+              nb = lane == 31 ? b0 : b;
+            } else {
+              nb = b;
+            }
+          }
+          // The value needs only max(dg, left, up): the shuffled term joins last
+          // with one add-max (dg >= -32768 already, so the clamp is implied).
+          // The pointer (tie rules) is formed beside it from the same terms.
+          const int dg = max(r2[m] + sc[m], LO);
+          const int own = max(r1[m] + gap, LO);  // up on even rows, left on odd rows
+          const int shf = max(nb + gap, LO);     // left on even rows, up on odd rows
+          const int v = max(nb + gap, max(dg, own));
+          const int l = E ? shf : own, u = E ? own : shf;
+          const bool in = unsigned(lane + 32 * m - col_min) < n;
+          cur[m] = in ? v : (sentinel[m] ? fill : r3[m]);
+          const bool dw = dg > max(l, u);
+          // code 1 (diag), 3 (up) or 2 (left) as two bits: bit 0 = diag or up, bit 1 = not diag
+          const bool upw = SWAP ? !(l >= u) : (u >= l);
+          b0[m] = in && (dw || upw);
+          b1[m] = in && !dw;
+        }
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+          const uint32_t w0 = __ballot_sync(FULL, b0[m]), w1 = __ballot_sync(FULL, b1[m]);
+          if (PS) {
+            if (lane == 0) *reinterpret_cast<uint2*>(planes + size_t(row) * (2 * M) + 2 * m) = make_uint2(w0, w1);
+          } else if (lane == (row & 31)) {
+            pbuf[2 * m] = w0;
+            pbuf[2 * m + 1] = w1;
+          }
+        }
+        if (!PS && (row & 31) == 31) {
+          const int base = row & ~31;
+          uint32_t* dst = pscr + size_t(base + lane) * (2 * M);
+#pragma unroll
+          for (int w = 0; w < 2 * M; ++w) dst[w] = pbuf[w];
+        }
+        if (E) {
+          B += 1;
+          col_min += dcm;
+          col_max += dcx;
+        } else {
+          A += 1;
+          col_min -= dcm;
+          col_max -= dcx;
+        }
+        int scn[M];
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+          const uint32_t a = p1[m][A], b = p2[m][B];
+          scn[m] = a == b ? match : (((a | b) & 0x30u) ? fill : mismatch);
+        }
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+          r3[m] = r2[m];
+          r2[m] = r1[m];
+          r1[m] = cur[m];
+          sc[m] = scn[m];
         }
       }
-      ham += __popc(__ballot_sync(FULL, mm));
-      i -= f;
-      j -= f;
-      alen += uint32_t(f);
+      i_max = A - col_min;
+      j_min = B + col_min;
       continue;
     }
-    const int v0 = __shfl_sync(FULL, v, 0);
-    if (v0 == 2 && j > 0) {
-      if (dbg0 && lane == 0) {
-        dbg0[alen] = swap ? S.s2[j - 1] : uint8_t('-');
-        dbg1[alen] = swap ? uint8_t('-') : S.s2[j - 1];
+    mid_checked = false;
+#pragma unroll
+    for (int ph = 0; ph < 2; ++ph) {
+      const int row = row0 + ph;
+      if (ph == 1 && row > last) break;
+      const bool E = ph == 0;
+      // ---- uniform bookkeeping for this anti-diagonal and the next ----
+      const int n = col_max - col_min + 1;
+      const int eo = E ? 1 : 0;
+      const int left_off = col_min - eo, up_off = col_min + 1 - eo;
+      bad |= (col_max < col_min) | (col_max >= ncol) | (left_off < 0) | (up_off + n > ncol);
+      row_free = max(row_free + egp, LO);
+      int lcol = -1, tcol = -1;
+      if (row < edge_rows) {  // ends-free edge cells exist only near the start
+        lcol = row < lfl ? left_col(row) : -1;
+        tcol = row < tfl ? top_col(row) : -1;
       }
-      --j;
-    } else if (v0 == 3 && i > 0) {
-      if (dbg0 && lane == 0) {
-        dbg0[alen] = swap ? uint8_t('-') : S.s1[i - 1];
-        dbg1[alen] = swap ? S.s1[i - 1] : uint8_t('-');
+      // band transition at the wedge boundaries (src/nwalign.rs:980-987)
+      const bool t1 = row == bt_row1;
+      const int cmT = t1 ? sat_sub1(col_min) : col_min;
+      const int imT = i_max + (t1 ? 1 : 0);
+      const int jmT = j_min - (t1 ? 1 : 0);
+      const int cxT = col_max + ((row == bt_row2) ? 1 : 0);
+      // advance the band for the next anti-diagonal (src/nwalign.rs:1028-1079)
+      int ncm, nim, njm, ncx;
+      {
+        const bool regA = row < band && row < len1;
+        const bool regB = !regA && imT < len1 - 1;
+        const int cmA = E ? sat_sub1(cmT) : cmT, imA = imT + 1, jmA = jmT;
+        int cmB, imB, jmB;
+        if (band_mod2 == 0) {
+          cmB = cmT;
+          imB = E ? imT : imT + 1;
+          jmB = E ? jmT + 1 : jmT;
+        } else {
+          cmB = E ? sat_sub1(cmT) : cmT + 1;
+          imB = E ? imT + 1 : imT;
+          jmB = E ? jmT : jmT + 1;
+        }
+        const int cmC = E ? cmT : cmT + 1, imC = imT, jmC = jmT + 1;
+        ncm = regA ? cmA : (regB ? cmB : cmC);
+        nim = regA ? imA : (regB ? imB : imC);
+        njm = regA ? jmA : (regB ? jmB : jmC);
+        const bool rt = row < top_limit;
+        const bool mid = !rt && ((row + 1) / 2 + cxT - start_col < len2);
+        const int cxA = E ? cxT : cxT + 1;
+        const int cxB = fb_even ? (E ? sat_sub1(cxT) : cxT + 1) : cxT;
+        const int cxC = E ? sat_sub1(cxT) : cxT;
+        ncx = rt ? cxA : (mid ? cxB : cxC);
       }
-      --i;
-    } else {
-      ok = false;
-      break;
+      // next anti-diagonal's diagonal scores (loads issued now, used next row)
+      int scn[M];
+      scores_at(nim + ncm, njm - ncm, scn);
+      // ---- the cells of this anti-diagonal ----
+      int cur[M];
+      uint32_t cc[M];
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        int nb;  // the previous row's value in the column this parity reads besides c
+        if (E) {
+          const int a = __shfl_up_sync(FULL, r1[m], 1);
+          if (M > 1) {
+            const int a31 = m > 0 ? __shfl_sync(FULL, r1[m > 0 ? m - 1 : 0], 31) : 0;
+            nb = lane == 0 ? a31 : a;  // column c-1
+          } else {
+            nb = a;  // lane 0 is column 0, a sentinel: never in band
+          }
+        } else {
+          const int b = __shfl_down_sync(FULL, r1[m], 1);
+          if (M > 1) {
+            const int b0 = (m + 1 < M) ? __shfl_sync(FULL, r1[m + 1 < M ? m + 1 : m], 0) : 0;
+            nb = lane == 31 ? b0 : b;  // column c+1
+          } else {
+            nb = b;  // column 31 is past the last in-band column when ncol <= 32
+          }
+        }
+        const int c = lane + 32 * m;
+        int v = sentinel[m] ? fill : r3[m];
+        uint32_t code = 0;
+        if (c == lcol) { v = row_free; code = 3; }
+        if (c == tcol) { v = row_free; code = 2; }
+        const int dg = max(r2[m] + sc[m], LO);
+        const int l = max((E ? nb : r1[m]) + gap, LO);
+        const int u = max((E ? r1[m] : nb) + gap, LO);
+        int e;
+        uint32_t pe;
+        if (SWAP) {
+          const bool lw = l >= u;
+          e = lw ? l : u;
+          pe = lw ? 2u : 3u;
+        } else {
+          const bool uw = u >= l;
+          e = uw ? u : l;
+          pe = uw ? 3u : 2u;
+        }
+        const bool dw = dg > e;
+        if ((unsigned)(c - col_min) < (unsigned)n) {
+          v = dw ? dg : e;
+          code = dw ? 1u : pe;
+        }
+        cur[m] = v;
+        cc[m] = code;
+      }
+      if (do_recalc) {
+        if (recalc_left) {
+          int pv = r1[0];
+#pragma unroll
+          for (int m = 1; m < M; ++m)
+            if ((left_off >> 5) == m) pv = r1[m];
+          pv = __shfl_sync(FULL, pv, left_off & 31);
+          const int d_free = max(pv + egp, LO);
+#pragma unroll
+          for (int m = 0; m < M; ++m) {
+            if (lane + 32 * m == cmT) {
+              const int cv = cur[m];
+              const uint32_t pc = cc[m];
+              if (d_free > cv) {
+                cur[m] = d_free;
+                cc[m] = 2;
+              } else if (!(d_free != cv || (!SWAP && pc != 1) || (SWAP && pc == 2))) {
+                cc[m] = 2;
+              }
+            }
+          }
+        }
+        if (imT == len1 - 1) recalc_left = true;
+        if (recalc_right) {
+          const int idx = up_off + cxT - cmT;
+          bad |= idx < 0 || idx >= ncol || cxT >= ncol;
+          int pv = r1[0];
+#pragma unroll
+          for (int m = 1; m < M; ++m)
+            if ((idx >> 5) == m) pv = r1[m];
+          pv = __shfl_sync(FULL, pv, idx & 31);
+          const int d_free = max(pv + egp, LO);
+#pragma unroll
+          for (int m = 0; m < M; ++m) {
+            if (lane + 32 * m == cxT) {
+              const int cv = cur[m];
+              const uint32_t pc = cc[m];
+              if (d_free > cv) {
+                cur[m] = d_free;
+                cc[m] = 3;
+              } else if (!(d_free != cv || (!SWAP && pc == 3) || (SWAP && pc != 1))) {
+                cc[m] = 3;
+              }
+            }
+          }
+        }
+        if ((row + 1) / 2 + cxT - start_col == len2) recalc_right = true;
+      }
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        const uint32_t w0 = __ballot_sync(FULL, cc[m] & 1u), w1 = __ballot_sync(FULL, cc[m] & 2u);
+        if (PS) {
+          if (lane == 0) *reinterpret_cast<uint2*>(planes + size_t(row) * (2 * M) + 2 * m) = make_uint2(w0, w1);
+        } else if (lane == (row & 31)) {
+          pbuf[2 * m] = w0;
+          pbuf[2 * m + 1] = w1;
+        }
+      }
+      if (!PS && ((row & 31) == 31 || row == last)) {
+        const int base = row & ~31;
+        if (base + lane <= row) {
+          uint32_t* dst = pscr + size_t(base + lane) * (2 * M);
+#pragma unroll
+          for (int w = 0; w < 2 * M; ++w) dst[w] = pbuf[w];
+        }
+      }
+      col_min = ncm;
+      i_max = nim;
+      j_min = njm;
+      col_max = ncx;
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        r3[m] = r2[m];
+        r2[m] = r1[m];
+        r1[m] = cur[m];
+        sc[m] = scn[m];
+      }
     }
-    ++alen;
+    if (bad) break;
   }
-  __syncwarp();
-  if (!ok) {
-    if (lane == 0) atomicOr(err_word, DERR_TRACEBACK);
+  if (bad) {
+    if (lane == 0) atomicOr(err_word, DERR_BAND_RANGE);
     return false;
   }
-  if (dbg_len && lane == 0) *dbg_len = alen;
-  *ham_out = ham;
-  return true;
+  if (!PS && last < 2) {  // rows 0/1 only: flush the buffered words
+    if (lane <= last) {
+      uint32_t* dst = pscr + size_t(lane) * (2 * M);
+#pragma unroll
+      for (int w = 0; w < 2 * M; ++w) dst[w] = pbuf[w];
+    }
+  }
+  __syncwarp();
+  return reg_traceback<M>(lane, SWAP, len1, len2, start_col, ncol, S, pscr, PS, ham_out, err_word, dbg0,
+                          dbg1, dbg_len);
 }
 
 // Picks the register form when the pair's compressed width fits 128 columns.
@@ -963,6 +1377,44 @@ __device__ bool vec_align_any(int lane, const uint8_t* g1, int l1, const uint8_t
   const int start_col = 1 + (min(band, len1) + 1) / 2;
   const int ncol = 2 + start_col + min(band + len2 - len1, len2) / 2;
   uint32_t* w = reinterpret_cast<uint32_t*>(scratch);
+  const int nrow = len1 + len2 + 1;
+  const int pmax = max(max(int(match), int(mismatch)), 0);
+  const bool fast = ncol >= 4 && ncol <= 128 && len1 >= 1 && nrow <= nrow_bound && gap <= 0 && egp <= 0 &&
+                    pmax * ((len1 + len2) / 2 + 1) <= 32767;
+  if (fast) {
+    const bool swap = l1 > l2;
+    {
+      const uint8_t* a = swap ? g2 : g1;
+      const uint8_t* b = swap ? g1 : g2;
+      for (int p = lane; p < len1; p += 32) S.s1[p] = a[p];
+      for (int p = lane; p < len2; p += 32) S.s2[p] = b[p];
+      for (int p = lane; p < kSeqPad; p += 32) {  // guard bytes: out-of-range positions score `fill`
+        S.s1[-1 - p] = 0x10;
+        S.s1[len1 + p] = 0x10;
+        S.s2[-1 - p] = 0x20;
+        S.s2[len2 + p] = 0x20;
+      }
+    }
+    __syncwarp();
+    const int mw = ncol <= 32 ? 1 : (ncol <= 64 ? 2 : 4);
+    const bool psm = size_t(nrow) * size_t(2 * mw) * 4u <= size_t(kStageBytes);
+#define VEC_FAST(MM, SW)                                                                                     \
+  return psm ? vec_align_fast<MM, SW, true>(lane, len1, len2, match, mismatch, gap, egp, band, S, w, ham_out,     \
+                                            err_word, dbg0, dbg1, dbg_len)                                      \
+             : vec_align_fast<MM, SW, false>(lane, len1, len2, match, mismatch, gap, egp, band, S, w, ham_out,    \
+                                             err_word, dbg0, dbg1, dbg_len)
+    if (mw == 1) {
+      if (swap) VEC_FAST(1, true);
+      VEC_FAST(1, false);
+    }
+    if (mw == 2) {
+      if (swap) VEC_FAST(2, true);
+      VEC_FAST(2, false);
+    }
+    if (swap) VEC_FAST(4, true);
+    VEC_FAST(4, false);
+#undef VEC_FAST
+  }
   if (ncol <= 32)
     return vec_align_reg<1>(lane, g1, l1, g2, l2, match, mismatch, gap, egp, band_in, S, w, nrow_bound, ham_out,
                             err_word, dbg0, dbg1, dbg_len);

@@ -85,6 +85,30 @@ def random_pairs(seed, n, lmin, lmax, indel=True):
     return out
 
 
+@pytest.mark.parametrize("match,mismatch,gap,egp", [
+    (5, -4, -8, 0),      # default scores: the add-max register form
+    (5, -4, -8, -8),     # end gaps as costly as inner gaps (no ends-free recalc)
+    (200, -4, -8, 0),    # match * (L + 1) past 32767: the exact saturating form
+    (5, -4, -8, 3),      # positive end gap: the exact saturating form
+    (40, -30, -60, -9),  # large penalties, lower saturation reached in band corners
+])
+@pytest.mark.parametrize("band", [-1, 8, 16, 40, 100])
+def test_vectorized_register_forms_match_oracle(band, match, mismatch, gap, egp):
+    pairs = random_pairs(7 + band + match, 60, 20, 330)
+    p = D.AlignParams(band=band, match_score=match, mismatch=mismatch, gap_p=gap, homo_gap_p=gap)
+    got = D.align_pairs(D.ALIGN_VECTORIZED, pairs, p, end_gap=egp)
+    for (a, b), (g0, g1) in zip(pairs, got):
+        w0, w1 = O.align(O.ALIGN_VECTORIZED, a, b, match=match, mismatch=mismatch, gap=gap, homo_gap=gap,
+                         end_gap=egp, band=band)
+        assert np.array_equal(g0, w0) and np.array_equal(g1, w1), (len(a), len(b), band, match, egp)
+    # the swapped orientation (first sequence longer) takes the other tie rule
+    got_sw = D.align_pairs(D.ALIGN_VECTORIZED, [(b, a) for a, b in pairs], p, end_gap=egp)
+    for (a, b), (g0, g1) in zip(pairs, got_sw):
+        w0, w1 = O.align(O.ALIGN_VECTORIZED, b, a, match=match, mismatch=mismatch, gap=gap, homo_gap=gap,
+                         end_gap=egp, band=band)
+        assert np.array_equal(g0, w0) and np.array_equal(g1, w1), ("swapped", len(a), len(b), band, match, egp)
+
+
 @pytest.mark.parametrize("band", [-1, 0, 3, 16, 32])
 def test_rowmajor_aligners_match_oracle(band):
     pairs = random_pairs(100 + band, 120, 20, 180)
