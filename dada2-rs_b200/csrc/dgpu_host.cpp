@@ -730,6 +730,8 @@ class Helpers {
 
 static constexpr size_t kParMin = 8192;   // loops shorter than this stay serial
 static constexpr size_t kParGrain = 2048;
+static constexpr size_t kParMinRepriced = 32;  // p-values worth splitting a reprice for
+static constexpr size_t kRepriceGrain = 256;   // members per reprice chunk
 
 // ---------------------------------------------------------------------------
 // Clustering state of one sample (containers.rs B/Bi/Raw, SoA)
@@ -754,6 +756,7 @@ struct Cluster {
   int64_t center = -1;
   std::vector<uint32_t> raws;
   uint32_t reads = 0;
+  uint32_t nvar = 0;  // members whose p is repriced (not fixed at 1.0)
   bool update_e = true, check_locks = true;
   double self_ = 0.0;
   int32_t birth_type = 0;
@@ -791,6 +794,8 @@ struct SampleState {
   std::vector<uint32_t> raw_cluster;
   std::vector<Cluster> clusters;
   std::vector<std::vector<Cand>> cand;
+  std::vector<uint32_t> ncand;   // cand[raw].size(), kept flat for the shuffle scans
+  std::vector<uint8_t> fixed_p;  // get_pA answers 1.0 whatever the cluster (src/pval.rs:383)
   uint64_t nalign = 0, nshroud = 0;
   RunStats stats;
   bool lock_dirty = false, done = false;
@@ -815,14 +820,29 @@ struct SampleState {
     for (uint32_t t = 0; t < n; ++t) total_reads += reads[t];
     rcomp.assign(n, Comp());
     p.assign(n, 0.0);
+    // A singleton without a prior gets p = 1.0 from get_pA for any cluster
+    // (unless singletons are detected), so it is set once here and never
+    // repriced. Such a raw never buds: the bud scan starts from p = 1.0 (the
+    // p of cluster 0's center, whose own comparison has hamming 0) and the
+    // center's reads, and a candidate replaces that only with a smaller p or
+    // an equal p and more reads.
+    fixed_p.assign(n, 0);
+    if (!conf->detect_singletons)
+      for (uint32_t t = 0; t < n; ++t)
+        if (reads[t] == 1 && !prior[t]) {
+          fixed_p[t] = 1;
+          p[t] = 1.0;
+        }
     raw_cluster.assign(n, 0);
     cand.assign(n, {});
+    ncand.assign(n, 0);
     clusters.clear();
     Cluster c0;
     c0.birth_e = double(total_reads);
     c0.raws.resize(n);
     for (uint32_t t = 0; t < n; ++t) c0.raws[t] = t;
     c0.reads = total_reads;
+    for (uint32_t t = 0; t < n; ++t) c0.nvar += fixed_p[t] ? 0u : 1u;
     clusters.push_back(std::move(c0));
     assign_center(0);
   }
@@ -840,6 +860,7 @@ struct SampleState {
     raw_cluster[raw] = uint32_t(ci);
     clusters[ci].raws.push_back(raw);
     clusters[ci].reads += reads[raw];
+    clusters[ci].nvar += fixed_p[raw] ? 0u : 1u;
     clusters[ci].update_e = true;
   }
 
@@ -849,6 +870,7 @@ struct SampleState {
     v[r] = v.back();
     v.pop_back();
     clusters[ci].reads -= reads[raw];
+    clusters[ci].nvar -= fixed_p[raw] ? 0u : 1u;
     clusters[ci].update_e = true;
     return raw;
   }
@@ -891,7 +913,13 @@ struct SampleState {
       c.comp.push_back(cp);
       if (ci == 0 || cp.index == center) rcomp[cp.index] = cp;
     });
-    for (const Comp& cp : c.comp) cand[cp.index].push_back(Cand{uint32_t(ci), cp.lambda, cp.hamming});  // index_add_cluster
+    for (const Comp& cp : c.comp) {  // index_add_cluster
+      const uint32_t raw = cp.index;
+      cand[raw].push_back(Cand{uint32_t(ci), cp.lambda, cp.hamming});
+      // A raw with one candidate keeps its emax implicit (see shuffle_converge);
+      // on gaining a second it gets the value the eager updates would hold.
+      if (++ncand[raw] == 2 && built) emax[raw] = compmax[raw].lambda * double(reads_used[compmax[raw].i]);
+    }
   }
 
   // ---- pval.rs ----
@@ -912,6 +940,7 @@ struct SampleState {
     const uint32_t bi_reads = bi.reads;
     for (size_t r = lo; r < hi; ++r) {
       const uint32_t raw = bi.raws[r];
+      if (fixed_p[raw]) continue;
       const double pv = get_pA(reads[raw], prior[raw] != 0, rcomp[raw].lambda, rcomp[raw].hamming, bi_reads);
       p[raw] = pv;
       if (r == 0) continue;
@@ -937,13 +966,13 @@ struct SampleState {
       if (bi.update_e) {
         const size_t nm = bi.raws.size();
         BudAcc acc;
-        if (nm < kParMin) {
+        if (bi.nvar < kParMinRepriced || nm < 2 * kRepriceGrain) {
           reprice_range(bi, 0, nm, acc);
         } else {
           // chunk-local caches folded in chunk order: the same first-of-equals
           // winner as one ascending scan
-          std::vector<BudAcc> part((nm + kParGrain - 1) / kParGrain);
-          Helpers::get().parallel_for(nm, kParGrain, [&](size_t c, size_t lo, size_t hi) {
+          std::vector<BudAcc> part((nm + kRepriceGrain - 1) / kRepriceGrain);
+          Helpers::get().parallel_for(nm, kRepriceGrain, [&](size_t c, size_t lo, size_t hi) {
             reprice_range(bi, lo, hi, part[c]);
           });
           for (const BudAcc& a : part) {
@@ -988,11 +1017,24 @@ struct SampleState {
   // Regularised lower incomplete gamma, statrs 0.18.0's Poisson::sf kernel,
   // following the published Cephes igam/igamc method (series when x <= 1 or
   // x <= a, Legendre continued fraction otherwise).
+  // lnGamma of the integer read counts, filled once; the same lgamma_r call
+  // on the same argument, so every value is the one computed on demand.
+  static double lgamma_of(double a) {
+    static const std::vector<double> table = [] {
+      std::vector<double> t(size_t(1) << 16);
+      int sg = 0;
+      for (size_t k = 1; k < t.size(); ++k) t[k] = lgamma_r(double(k), &sg);
+      return t;
+    }();
+    if (a >= 1.0 && a < double(table.size()) && a == std::floor(a)) return table[size_t(a)];
+    int sg = 0;
+    return lgamma_r(a, &sg);
+  }
+
   static double gamma_lr(double a, double x) {
     const double eps = 1e-15, big = 4503599627370496.0, big_inv = 2.22044604925031308085e-16;
     if (std::isnan(a) || std::isnan(x)) return std::numeric_limits<double>::quiet_NaN();
-    int sign_unused = 0;
-    const double ax = a * std::log(x) - x - lgamma_r(a, &sign_unused);
+    const double ax = a * std::log(x) - x - lgamma_of(a);
     if (ax < -709.78271289338399) return a < x ? 1.0 : 0.0;
     if (x <= 1.0 || x <= a) {
       double r = a, c = 1.0, ans = 1.0;
@@ -1031,10 +1073,25 @@ struct SampleState {
     return 1.0 - std::exp(ax) * ans;
   }
 
+  // ln(k!) as the left-to-right sum log(1) + ... + log(k) of src/pval.rs:333;
+  // the table holds the running sums of that same loop.
+  static double log_factorial(uint32_t rd) {
+    static const std::vector<double> table = [] {
+      std::vector<double> t(size_t(1) << 16);
+      double acc = 0.0;
+      t[0] = 0.0;
+      for (size_t k = 1; k < t.size(); ++k) t[k] = acc += std::log(double(k));
+      return t;
+    }();
+    if (rd < table.size()) return table[rd];
+    double acc = table.back();
+    for (uint32_t t = uint32_t(table.size()); t <= rd; ++t) acc += std::log(double(t));
+    return acc;
+  }
+
   static double upper_tail_direct(uint32_t rd, double lambda) {  // src/pval.rs:329-353
     const double k = double(rd);
-    double log_kfact = 0.0;
-    for (uint32_t t = 1; t <= rd; ++t) log_kfact += std::log(double(t));
+    const double log_kfact = log_factorial(rd);
     const double log_leading = -lambda + k * std::log(lambda) - log_kfact;
     double sum = 1.0, term = 1.0;
     for (uint32_t j = 1; j < 10000u; ++j) {
@@ -1247,6 +1304,14 @@ struct SampleState {
           reads_fell_list.push_back(uint32_t(ci));
         }
       }
+      // A raw with a single candidate cannot change cluster, and its emax is
+      // read only once it has a second candidate (pass A2 reads it through
+      // another cluster's comps, which it then has). Its emax is therefore left
+      // implicit: the eager updates would hold lambda * reads_used[its cluster],
+      // the reads as of the last reconcile, and index_add_cluster writes that
+      // value when the second candidate arrives. So pass A1 queues only raws
+      // with two or more candidates, and pass B's rescan of a single-candidate
+      // raw (which would leave it in place) is skipped.
       // Pass A1: raws whose best cluster lost reads are queued for a rescan.
       // Every pass here follows a move pass (or the carried state, which ended
       // with one), after which each raw sits in its best cluster unless it is
@@ -1260,7 +1325,7 @@ struct SampleState {
         auto a1 = [&](size_t lo, size_t hi, std::vector<uint32_t>& out) {
           for (size_t k = lo; k < hi; ++k) {
             const uint32_t raw = mem[k];
-            if (compmax[raw].i == ci && !in_affected[raw]) {
+            if (compmax[raw].i == ci && !in_affected[raw] && ncand[raw] > 1) {
               in_affected[raw] = 1;
               out.push_back(raw);
             }
