@@ -1082,90 +1082,113 @@ __device__ bool vec_align_fast(int lane, int len1, int len2, int match, int mism
         if (bad) break;
       }
       int A = i_max + col_min, B = j_min - col_min;
+      // (col_min, col_max) on the even and odd rows of every middle pair
+      const int cmE = col_min, cxE = col_max, cmO = col_min + dcm, cxO = col_max + dcx;
+      bool inE[M], inO[M];
+      int sc1[M];  // the odd row's diagonal scores
 #pragma unroll
-      for (int ph = 0; ph < 2; ++ph) {
-        const bool E = ph == 0;
-        const int row = row0 + ph;
-        const unsigned n = unsigned(col_max - col_min + 1);
-        int cur[M];
-        bool b0[M], b1[M];
-#pragma unroll
-        for (int m = 0; m < M; ++m) {
-          int nb;
-          if (E) {
-            const int a = __shfl_up_sync(FULL, r1[m], 1);
-            if (M > 1) {
-              const int a31 = m > 0 ? __shfl_sync(FULL, r1[m > 0 ? m - 1 : 0], 31) : 0;
-              nb = lane == 0 ? a31 : a;
-            } else {
-              nb = a;
-            }
-          } else {
-            const int b = __shfl_down_sync(FULL, r1[m], 1);
-            if (M > 1) {
-              const int b0 = (m + 1 < M) ? __shfl_sync(FULL, r1[m + 1 < M ? m + 1 : m], 0) : 0;
-              nb = lane == 31 ? b0 : b;
-            } else {
-              nb = b;
-            }
-          }
-          // The value needs only max(dg, left, up): the shuffled term joins last
-          // with one add-max (dg >= -32768 already, so the clamp is implied).
-          // The pointer (tie rules) is formed beside it from the same terms.
-          const int dg = max(r2[m] + sc[m], LO);
-          const int own = max(r1[m] + gap, LO);  // up on even rows, left on odd rows
-          const int shf = max(nb + gap, LO);     // left on even rows, up on odd rows
-          const int v = max(nb + gap, max(dg, own));
-          const int l = E ? shf : own, u = E ? own : shf;
-          const bool in = unsigned(lane + 32 * m - col_min) < n;
-          cur[m] = in ? v : (sentinel[m] ? fill : r3[m]);
-          const bool dw = dg > max(l, u);
-          // code 1 (diag), 3 (up) or 2 (left) as two bits: bit 0 = diag or up, bit 1 = not diag
-          const bool upw = SWAP ? !(l >= u) : (u >= l);
-          b0[m] = in && (dw || upw);
-          b1[m] = in && !dw;
-        }
-#pragma unroll
-        for (int m = 0; m < M; ++m) {
-          const uint32_t w0 = __ballot_sync(FULL, b0[m]), w1 = __ballot_sync(FULL, b1[m]);
-          if (PS) {
-            if (lane == 0) *reinterpret_cast<uint2*>(planes + size_t(row) * (2 * M) + 2 * m) = make_uint2(w0, w1);
-          } else if (lane == (row & 31)) {
-            pbuf[2 * m] = w0;
-            pbuf[2 * m + 1] = w1;
-          }
-        }
-        if (!PS && (row & 31) == 31) {
-          const int base = row & ~31;
-          uint32_t* dst = pscr + size_t(base + lane) * (2 * M);
-#pragma unroll
-          for (int w = 0; w < 2 * M; ++w) dst[w] = pbuf[w];
-        }
-        if (E) {
-          B += 1;
-          col_min += dcm;
-          col_max += dcx;
-        } else {
-          A += 1;
-          col_min -= dcm;
-          col_max -= dcx;
-        }
-        int scn[M];
-#pragma unroll
-        for (int m = 0; m < M; ++m) {
-          const uint32_t a = p1[m][A], b = p2[m][B];
-          scn[m] = a == b ? match : (((a | b) & 0x30u) ? fill : mismatch);
-        }
-#pragma unroll
-        for (int m = 0; m < M; ++m) {
-          r3[m] = r2[m];
-          r2[m] = r1[m];
-          r1[m] = cur[m];
-          sc[m] = scn[m];
-        }
+      for (int m = 0; m < M; ++m) {
+        const int c = lane + 32 * m;
+        inE[m] = unsigned(c - cmE) < unsigned(cxE - cmE + 1);
+        inO[m] = unsigned(c - cmO) < unsigned(cxO - cmO + 1);
+        const uint32_t x = p1[m][A], y = p2[m][B + 1];
+        sc1[m] = x == y ? match : (((x | y) & 0x30u) ? fill : mismatch);
       }
-      i_max = A - col_min;
-      j_min = B + col_min;
+      int r0 = row0;
+      for (;;) {
+        // Scores two rows ahead: over a pair A and B each rise by one, so the
+        // loads for rows r0+2 / r0+3 go out while rows r0 / r0+1 are computed.
+        int sc2[M], sc3[M];
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+          const uint32_t x = p1[m][A + 1], y = p2[m][B + 1];
+          sc2[m] = x == y ? match : (((x | y) & 0x30u) ? fill : mismatch);
+          const uint32_t x3 = p1[m][A + 1], y3 = p2[m][B + 2];
+          sc3[m] = x3 == y3 ? match : (((x3 | y3) & 0x30u) ? fill : mismatch);
+        }
+#pragma unroll
+        for (int ph = 0; ph < 2; ++ph) {
+          const bool E = ph == 0;
+          const int row = r0 + ph;
+          int cur[M];
+          bool b0[M], b1[M];
+#pragma unroll
+          for (int m = 0; m < M; ++m) {
+            int nb;
+            if (E) {
+              const int a = __shfl_up_sync(FULL, r1[m], 1);
+              if (M > 1) {
+                const int a31 = m > 0 ? __shfl_sync(FULL, r1[m > 0 ? m - 1 : 0], 31) : 0;
+                nb = lane == 0 ? a31 : a;
+              } else {
+                nb = a;
+              }
+            } else {
+              const int b = __shfl_down_sync(FULL, r1[m], 1);
+              if (M > 1) {
+                const int b0 = (m + 1 < M) ? __shfl_sync(FULL, r1[m + 1 < M ? m + 1 : m], 0) : 0;
+                nb = lane == 31 ? b0 : b;
+              } else {
+                nb = b;
+              }
+            }
+            // The value needs only max(dg, left, up): the shuffled term joins
+            // last with one add-max (dg >= -32768 already, so the clamp is
+            // implied). The pointer (tie rules) is formed beside it.
+            const int dg = max(r2[m] + (E ? sc[m] : sc1[m]), LO);
+            const int own = max(r1[m] + gap, LO);  // up on even rows, left on odd rows
+            const int shf = max(nb + gap, LO);     // left on even rows, up on odd rows
+            const int v = max(nb + gap, max(dg, own));
+            const int l = E ? shf : own, u = E ? own : shf;
+            const bool in = E ? inE[m] : inO[m];
+            cur[m] = in ? v : (sentinel[m] ? fill : r3[m]);
+            const bool dw = dg > max(l, u);
+            // code 1 (diag), 3 (up) or 2 (left) as two bits: bit 0 = diag or up, bit 1 = not diag
+            const bool upw = SWAP ? !(l >= u) : (u >= l);
+            b0[m] = in && (dw || upw);
+            b1[m] = in && !dw;
+          }
+#pragma unroll
+          for (int m = 0; m < M; ++m) {
+            const uint32_t w0 = __ballot_sync(FULL, b0[m]), w1 = __ballot_sync(FULL, b1[m]);
+            if (PS) {
+              if (lane == 0) *reinterpret_cast<uint2*>(planes + size_t(row) * (2 * M) + 2 * m) = make_uint2(w0, w1);
+            } else if (lane == (row & 31)) {
+              pbuf[2 * m] = w0;
+              pbuf[2 * m + 1] = w1;
+            }
+          }
+          if (!PS && (row & 31) == 31) {
+            const int base = row & ~31;
+            uint32_t* dst = pscr + size_t(base + lane) * (2 * M);
+#pragma unroll
+            for (int w = 0; w < 2 * M; ++w) dst[w] = pbuf[w];
+          }
+#pragma unroll
+          for (int m = 0; m < M; ++m) {
+            r3[m] = r2[m];
+            r2[m] = r1[m];
+            r1[m] = cur[m];
+          }
+        }
+        A += 1;
+        B += 1;
+        r0 += 2;
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+          sc[m] = sc2[m];
+          sc1[m] = sc3[m];
+        }
+        // the next pair stays in the middle regime (same tests as above)
+        if (!(r0 + 1 <= last && A - cmE + band_mod2 < len1 - 1 && (r0 + 1) / 2 + cxE - start_col < len2 &&
+              (r0 + 2) / 2 + cxO - start_col < len2))
+          break;
+      }
+      col_min = cmE;
+      col_max = cxE;
+      i_max = A - cmE;
+      j_min = B + cmE;
+      row0 = r0 - 2;  // the outer loop resumes at row r0
       continue;
     }
     mid_checked = false;
