@@ -82,7 +82,8 @@ constexpr int kScreenWarps = 8;   // warps per screen CTA
 constexpr int kNwWarps = 4;       // warps per NW CTA
 constexpr int kAlignCtasPerSm = 4; // resident align CTAs per SM (128 registers per thread)
 constexpr int kStageBytes = 4096; // traceback staging per warp
-constexpr int kStoreSpan = 8192;  // raws per store CTA (its own output segment)
+constexpr int kStoreSpan = 2048;  // raws per store CTA (its own output segment)
+constexpr int kStoreThreads = 256; // threads per store CTA
 constexpr int kSeqPad = 160;      // guard bytes on each side of the aligners' shared-memory sequences
 
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
@@ -138,6 +139,9 @@ struct CompareLaunch {
   uint32_t* blk_counters;
   uint32_t nstore_blocks;
   int do_store;
+  // with do_store: the store's first CTA copies *err_word to err_host (mapped
+  // host memory) and clears queue_counts for the launch context's next call
+  uint32_t* err_host;
 };
 // ev (optional): 4 events recorded before the screen and after screen, align
 // and store, for per-kernel device times.

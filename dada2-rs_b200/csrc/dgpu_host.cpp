@@ -55,7 +55,8 @@ static double secs(Clock::time_point a, Clock::time_point b) { return std::chron
 struct GlobalStats {
   std::mutex mu;
   dgpu_kernel_stats s{};
-  std::atomic<bool> timing{false};
+  std::atomic<uint64_t> timing_every{0};  // time every N-th compare call (0: none)
+  std::atomic<uint64_t> call_seq{0};
   std::vector<double> round_ms;  // latency of each compare call (launch to results on the host)
 };
 static GlobalStats g_stats;
@@ -294,20 +295,21 @@ struct Slot {
   Pool* P = nullptr;
   cudaStream_t st = nullptr;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-  DBuf<uint32_t> queue_pass, queue_counts;
+  DBuf<uint32_t> queue_pass, queue_counts, err_dev;
   DBuf<uint8_t> scratch;
-  DBuf<TaskDev> tasks;
-  DBuf<uint32_t> task_prefix, store_map;
-  HBuf<uint32_t> blk_counters, prefix_stage, store_stage;  // prefix; then (task, chunk) per store CTA
+  DBuf<uint8_t> dpack;  // tasks | task prefix | store map of the current launch
+  HBuf<uint8_t> hpack;  // its pinned staging copy (one upload per launch)
+  HBuf<uint32_t> blk_counters, err_host;
   HBuf<double> task_self;
   HBuf<TaskDev> task_stage;
   std::vector<uint32_t> task_blk0;  // first store CTA of each task in the latest launch
   uint32_t ntask_cap = 0, nblk_cap = 0;
+  size_t pack_cap = 0;
 
   ~Slot() {
     if (st && cudaStreamSynchronize(st) == cudaSuccess)  // every block is idle now
-      recycle_all(queue_pass, queue_counts, scratch, tasks, task_prefix, store_map, blk_counters, prefix_stage,
-                  store_stage, task_self, task_stage);
+      recycle_all(queue_pass, queue_counts, err_dev, scratch, dpack, hpack, blk_counters, err_host, task_self,
+                  task_stage);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
@@ -317,17 +319,22 @@ struct Slot {
     P = pool;
     CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
+    TRY(queue_counts.alloc(8));
+    TRY(err_dev.alloc(1));
+    TRY(err_host.alloc(1));
+    err_host.h[0] = 0;
+    // both start at zero; every call leaves them at zero again
+    CUDA_TRY(cudaMemsetAsync(queue_counts.p, 0, 32, st));
+    CUDA_TRY(cudaMemsetAsync(err_dev.p, 0, 4, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
     return 0;
   }
 
   int ensure_tasks(uint32_t ntask) {
     if (ntask <= ntask_cap) return 0;
     uint32_t cap = std::max<uint32_t>(ntask, 64);
-    TRY(tasks.alloc(cap));
-    TRY(task_prefix.alloc(cap + 1));
     TRY(task_self.alloc(cap));
     TRY(task_stage.alloc(cap));
-    TRY(prefix_stage.alloc(cap + 1));
     ntask_cap = cap;
     return 0;
   }
@@ -335,10 +342,17 @@ struct Slot {
   int ensure_blocks(uint32_t nblk) {
     if (nblk <= nblk_cap) return 0;
     const uint32_t cap = std::max<uint32_t>(nblk, 256);
-    TRY(store_stage.alloc(size_t(2) * cap));
-    TRY(store_map.alloc(size_t(2) * cap));
     TRY(blk_counters.alloc(size_t(cap) * TC_NCOUNTERS));
     nblk_cap = cap;
+    return 0;
+  }
+
+  int ensure_pack(size_t bytes) {
+    if (bytes <= pack_cap) return 0;
+    const size_t cap = std::max<size_t>(bytes, 16384);
+    TRY(hpack.alloc(cap));
+    TRY(dpack.alloc(cap));
+    pack_cap = cap;
     return 0;
   }
 
@@ -358,7 +372,7 @@ struct Pool {
   int sms = 148;
   int nslots = 1;
   DBuf<uint8_t> seq, qual, kmer8, sat, lock, status;
-  DBuf<uint32_t> off, len, reads, ham, err_word;
+  DBuf<uint32_t> off, len, reads, ham;
   DBuf<double> e_minmax, err, lambda;
   // stored comps of each task, at the task's first raw (its sample's base)
   HBuf<uint32_t> comp_index, comp_ham;
@@ -370,7 +384,7 @@ struct Pool {
   ~Pool() {
     slots.clear();  // each slot drains its own stream first
     if (st && cudaStreamSynchronize(st) == cudaSuccess)
-      recycle_all(seq, qual, kmer8, sat, lock, status, off, len, reads, ham, err_word, e_minmax, err, lambda,
+      recycle_all(seq, qual, kmer8, sat, lock, status, off, len, reads, ham, e_minmax, err, lambda,
                   comp_index, comp_ham, comp_lambda, lock_host);
     if (st) cudaStreamDestroy(st);
   }
@@ -442,7 +456,6 @@ struct Pool {
     TRY(ham.alloc(n));
     TRY(lambda.alloc(n));
     TRY(e_minmax.alloc(n));
-    TRY(err_word.alloc(1));
     TRY(err.alloc(size_t(16) * kp.ncol));
     TRY(kmer8.alloc(kp.use_kmers ? size_t(n) * nk : 1));
     TRY(sat.alloc(n));
@@ -461,7 +474,6 @@ struct Pool {
     CUDA_TRY(cudaMemcpyAsync(reads.p, rd, size_t(n) * 4, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(err.p, errm, size_t(16) * kp.ncol * 8, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemsetAsync(lock.p, 0, n, st));
-    CUDA_TRY(cudaMemsetAsync(err_word.p, 0, 4, st));
     TRY(reset_e_minmax());
     if (kp.use_kmers) {
       launch_profiles(seq.p, off.p, len.p, n, kp.kmer_size, kmer8.p, sat.p, st);
@@ -506,7 +518,6 @@ struct Pool {
       TRY(L.init(this));
       TRY(L.scratch.alloc(per * size_t(geom.nwarps)));
       TRY(L.queue_pass.alloc(nraw));
-      TRY(L.queue_counts.alloc(8));
     }
     return 0;
   }
@@ -558,6 +569,8 @@ void Slot::task_counters(uint32_t t, uint32_t* out) const {
 }
 
 // Launches one compare over `ntask` tasks already in task_stage; waits for it.
+// The launch's tables go up in one copy; with the store, the error flags come
+// back through mapped memory and the queue counters are rearmed on the device.
 int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
   const auto t_call = Clock::now();
   TRY(ensure_tasks(ntask));
@@ -565,49 +578,59 @@ int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
   uint32_t total = 0, nblk = 0;
   task_blk0.assign(ntask, 0);
   for (uint32_t t = 0; t < ntask; ++t) {
-    prefix_stage.h[t] = total;
     task_stage.h[t].out_off = task_stage.h[t].base;
-    total += task_stage.h[t].n;
     task_blk0[t] = nblk;
     nblk += (task_stage.h[t].n + kStoreSpan - 1) / kStoreSpan;
   }
-  prefix_stage.h[ntask] = total;
   TRY(ensure_blocks(nblk));
+  const size_t o_pref = align16(sizeof(TaskDev) * ntask);
+  const size_t o_map = o_pref + align16(size_t(4) * (ntask + 1));
+  const size_t pack_bytes = o_map + align16(size_t(8) * std::max<uint32_t>(nblk, 1));
+  TRY(ensure_pack(pack_bytes));
+  std::memcpy(hpack.h, task_stage.h, sizeof(TaskDev) * ntask);
+  uint32_t* pref = reinterpret_cast<uint32_t*>(hpack.h + o_pref);
+  uint32_t* smap = reinterpret_cast<uint32_t*>(hpack.h + o_map);
   for (uint32_t t = 0; t < ntask; ++t) {
+    pref[t] = total;
+    total += task_stage.h[t].n;
     const uint32_t nb = (task_stage.h[t].n + kStoreSpan - 1) / kStoreSpan;
     for (uint32_t b = 0; b < nb; ++b) {
-      store_stage.h[task_blk0[t] + b] = t;
-      store_stage.h[nblk + task_blk0[t] + b] = b;
+      smap[task_blk0[t] + b] = t;
+      smap[nblk + task_blk0[t] + b] = b;
     }
   }
-  CUDA_TRY(cudaMemcpyAsync(tasks.p, task_stage.h, sizeof(TaskDev) * ntask, cudaMemcpyHostToDevice, st));
-  CUDA_TRY(cudaMemcpyAsync(task_prefix.p, prefix_stage.h, 4 * (ntask + 1), cudaMemcpyHostToDevice, st));
-  CUDA_TRY(cudaMemcpyAsync(store_map.p, store_stage.h, size_t(8) * nblk, cudaMemcpyHostToDevice, st));
-  CUDA_TRY(cudaMemsetAsync(queue_counts.p, 0, 32, st));
+  pref[ntask] = total;
+  CUDA_TRY(cudaMemcpyAsync(dpack.p, hpack.h, pack_bytes, cudaMemcpyHostToDevice, st));
   CompareLaunch L{};
   L.pool = Q.view();
   L.kp = Q.kp;
-  L.tasks = tasks.p;
-  L.task_prefix = task_prefix.p;
+  L.tasks = reinterpret_cast<const TaskDev*>(dpack.p);
+  L.task_prefix = reinterpret_cast<const uint32_t*>(dpack.p + o_pref);
   L.ntask = ntask;
   L.total_items = total;
   L.queue_pass = queue_pass.p;
   L.queue_counts = queue_counts.p;
   L.nw_scratch = scratch.p;
   L.geom = Q.geom;
-  L.err_word = Q.err_word.p;
+  L.err_word = err_dev.p;
   L.comp_index = Q.comp_index.d;
   L.comp_lambda = Q.comp_lambda.d;
   L.comp_ham = Q.comp_ham.d;
   L.task_self = task_self.d;
-  L.store_task = store_map.p;
-  L.store_chunk = store_map.p + nblk;
+  L.store_task = reinterpret_cast<const uint32_t*>(dpack.p + o_map);
+  L.store_chunk = L.store_task + nblk;
   L.blk_counters = blk_counters.d;
   L.nstore_blocks = nblk;
   L.do_store = do_store ? 1 : 0;
-  const bool timing = g_stats.timing.load();
+  L.err_host = err_host.d;
+  const uint64_t every = g_stats.timing_every.load();
+  const bool timing = every != 0 && g_stats.call_seq.fetch_add(1) % every == 0;
   launch_compare(L, st, timing ? ev : nullptr);
   CUDA_TRY(cudaGetLastError());
+  if (!do_store) {  // no store kernel to rearm the queue or report the flags
+    CUDA_TRY(cudaMemsetAsync(queue_counts.p, 0, 32, st));
+    CUDA_TRY(cudaMemcpyAsync(err_host.h, err_dev.p, 4, cudaMemcpyDeviceToHost, st));
+  }
   auto t0 = Clock::now();
   CUDA_TRY(cudaStreamSynchronize(st));
   const auto t1 = Clock::now();
@@ -628,12 +651,16 @@ int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
     S.rounds += 1;
     S.compares += total;
     S.screened += screened;
-    S.screen_bytes += screened * (uint64_t(1) << (2 * Q.kp.kmer_size)) + uint64_t(total) * 16u;
+    const uint64_t sb = screened * (uint64_t(1) << (2 * Q.kp.kmer_size)) + uint64_t(total) * 16u;
+    S.screen_bytes += sb;
+    if (timing) {
+      S.timed_rounds += 1;
+      S.timed_screen_bytes += sb;
+      S.timed_compares += total;
+    }
     if (g_stats.round_ms.size() < (size_t(1) << 20)) g_stats.round_ms.push_back(1e3 * secs(t_call, t1));
   }
-  uint32_t ew = 0;
-  CUDA_TRY(cudaMemcpyAsync(&ew, Q.err_word.p, 4, cudaMemcpyDeviceToHost, st));
-  CUDA_TRY(cudaStreamSynchronize(st));
+  const uint32_t ew = *reinterpret_cast<volatile uint32_t*>(err_host.h);
   if (ew) {
     std::string what;
     if (ew & DERR_TRACEBACK) what += " invalid traceback pointer;";
@@ -641,7 +668,8 @@ int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
     if (ew & DERR_BAND_RANGE) what += " vectorized band left the compressed matrix;";
     if (ew & DERR_UNSUPPORTED) what += " band wider than 1024 offsets on the row-major aligner;";
     if (ew & DERR_LAMBDA) what += " non-ACGT code or quality beyond the error matrix in lambda;";
-    CUDA_TRY(cudaMemsetAsync(Q.err_word.p, 0, 4, st));
+    err_host.h[0] = 0;
+    CUDA_TRY(cudaMemsetAsync(err_dev.p, 0, 4, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     return fail(ew & DERR_UNSUPPORTED ? DGPU_E_UNSUPPORTED : DGPU_E_DEVICE, "device error:" + what);
   }
@@ -1809,9 +1837,9 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
 }
 
 // Launch slots for a batch of nsamples: DGPU_LAUNCH_SLOTS (1..8) if set, else
-// 2; never more than there are samples.
+// 3; never more than there are samples.
 static int launch_slots(int nsamples) {
-  int k = 2;
+  int k = 3;
   if (const char* e = std::getenv("DGPU_LAUNCH_SLOTS")) {
     const int v = std::atoi(e);
     if (v >= 1 && v <= 8) k = v;
@@ -1908,8 +1936,11 @@ static int batch_prepare(Batch& B, int device, const dgpu_dada_params* prm, int 
   for (int s = 0; s < nsamples; ++s)
     B.confs[size_t(s)].max_clust = prm->max_clust == 0 ? B.in[size_t(s)].n : size_t(prm->max_clust);
   B.align = prm->align;
+  // Host phases of different samples share the cores with the intra-sample
+  // helpers (half the cores) and the launch workers, so by default they get
+  // the other half.
   int threads = prm->host_threads;
-  if (threads <= 0) threads = int(std::max(1u, std::thread::hardware_concurrency()));
+  if (threads <= 0) threads = int(std::max(1u, std::thread::hardware_concurrency() / 2));
   B.host_threads = std::min(threads, nsamples);
   return 0;
 }
@@ -2170,8 +2201,9 @@ int dgpu_stats_latencies(double* out, int cap) {
   return int(g_stats.round_ms.size());
 }
 
-int dgpu_stats_timing(int enable) {
-  g_stats.timing.store(enable != 0);
+int dgpu_stats_timing(int every) {
+  g_stats.timing_every.store(every > 0 ? uint64_t(every) : 0u);
+  g_stats.call_seq.store(0);
   return 0;
 }
 

@@ -1788,8 +1788,8 @@ __global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_align(Compar
 // Each CTA owns kStoreSpan consecutive raws of one task; its stored comps go
 // to that span's own segment of the task's output (so concatenating segments
 // in order gives ascending raw order) with a per-CTA count and counters.
-__global__ void __launch_bounds__(1024) k_store(CompareLaunch L) {
-  constexpr int IPT = kStoreSpan / 1024;
+__global__ void __launch_bounds__(kStoreThreads) k_store(CompareLaunch L) {
+  constexpr int IPT = kStoreSpan / kStoreThreads;
   __shared__ uint32_t warp_off[32];
   __shared__ uint32_t ctr[TC_NCOUNTERS];
   const uint32_t blk = blockIdx.x;
@@ -1880,6 +1880,12 @@ __global__ void __launch_bounds__(1024) k_store(CompareLaunch L) {
   }
   __syncthreads();
   if (threadIdx.x < TC_NCOUNTERS) L.blk_counters[size_t(blk) * TC_NCOUNTERS + threadIdx.x] = ctr[threadIdx.x];
+  if (blk == 0) {
+    // the screen and align kernels have finished: hand their error flags to
+    // the host through mapped memory and rearm the queue for the next call
+    if (threadIdx.x == 0) *reinterpret_cast<volatile uint32_t*>(L.err_host) = *L.err_word;
+    if (threadIdx.x < 8) L.queue_counts[threadIdx.x] = 0;
+  }
 }
 
 static int g_sm_count = 0;
@@ -1923,7 +1929,7 @@ void launch_compare(const CompareLaunch& L, cudaStream_t st, cudaEvent_t* ev) {
   }
   k_align<<<L.geom.nwarps / kNwWarps, kNwWarps * 32, asm_, st>>>(L);
   if (ev) cudaEventRecord(ev[2], st);
-  if (L.do_store) k_store<<<L.nstore_blocks, 1024, 0, st>>>(L);
+  if (L.do_store) k_store<<<L.nstore_blocks, kStoreThreads, 0, st>>>(L);
   if (ev) cudaEventRecord(ev[3], st);
 }
 

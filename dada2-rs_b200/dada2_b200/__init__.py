@@ -345,8 +345,10 @@ def stats_reset():
     check(lib().dgpu_stats_reset())
 
 
-def stats_timing(enable: bool):
-    check(lib().dgpu_stats_timing(int(bool(enable))))
+def stats_timing(every):
+    """Per-kernel device timing of every ``every``-th compare call (True = every
+    call, False/0 = off)."""
+    check(lib().dgpu_stats_timing(int(every)))
 
 
 def stats_latencies() -> np.ndarray:
@@ -363,7 +365,8 @@ def stats_read() -> dict:
     return {"launches": {k: int(s.launches[i]) for i, k in enumerate(KERNEL_NAMES)},
             "ms": {k: float(s.ms[i]) for i, k in enumerate(KERNEL_NAMES)},
             "rounds": int(s.rounds), "compares": int(s.compares), "screened": int(s.screened),
-            "screen_bytes": int(s.screen_bytes)}
+            "screen_bytes": int(s.screen_bytes), "timed_rounds": int(s.timed_rounds),
+            "timed_screen_bytes": int(s.timed_screen_bytes), "timed_compares": int(s.timed_compares)}
 
 
 ALIGN_VECTORIZED, ALIGN_HOMO, ALIGN_ENDSFREE = 0, 1, 2

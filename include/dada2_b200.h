@@ -58,7 +58,7 @@ typedef struct {
   double min_fold;
   uint32_t min_hamming, min_abund;
   int32_t use_quals, greedy;
-  int32_t host_threads; /* threads for the host phases of dgpu_dada_batch; 0 = all cores */
+  int32_t host_threads; /* threads for the host phases of dgpu_dada_batch; 0 = half the cores */
 } dgpu_dada_params;
 
 /* Counters of one compare call (CompareTiming's denominators, src/cluster.rs:190-231). */
@@ -106,14 +106,17 @@ typedef struct dgpu_batch dgpu_batch;
 
 /* Process-wide kernel accounting (for benchmarks). Index k: 0 profiles,
  * 1 screen, 2 align (ordered-k-mer distance, gapless or NW alignment and
- * lambda for the pairs that passed the screen), 3 store. ms[] is filled only
- * while timing is enabled (CUDA events around each kernel on its stream).
- * screen_bytes = algorithmic bytes of the screen: 4^k profile bytes per
- * non-skipped compare plus 16 bytes of per-raw metadata per compare. */
+ * lambda for the pairs that passed the screen), 3 store. screen_bytes =
+ * algorithmic bytes of the screen: 4^k profile bytes per non-skipped compare
+ * plus 16 bytes of per-raw metadata per compare. ms[] sums the device time
+ * (CUDA events around each kernel on its stream) of the timed compare calls
+ * only -- every N-th call while dgpu_stats_timing(N) is in force -- and the
+ * timed_* fields count those calls, their screen bytes and compares. */
 typedef struct {
   uint64_t launches[4];
   double ms[4];
   uint64_t rounds, compares, screened, screen_bytes;
+  uint64_t timed_rounds, timed_screen_bytes, timed_compares;
 } dgpu_kernel_stats;
 
 const char* dgpu_last_error(void);
@@ -173,7 +176,9 @@ void dgpu_batch_free(dgpu_batch* batch);
 int dgpu_cache_release(int device, uint64_t* freed);
 
 int dgpu_stats_reset(void);
-int dgpu_stats_timing(int enable);
+/* every = 0 stops the per-kernel timing; every = N >= 1 times every N-th
+ * compare call (events cost a few microseconds per call). */
+int dgpu_stats_timing(int every);
 int dgpu_stats_read(dgpu_kernel_stats* out);
 /* Latency (ms) of each compare call since the last reset, from launch to the
  * results being on the host; copies up to cap values, returns how many exist. */
