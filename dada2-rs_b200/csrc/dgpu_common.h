@@ -79,6 +79,7 @@ struct NwGeom {
 
 // ---- shared-memory carving, used by kernels and by the host sizing code ----
 constexpr int kScreenWarps = 8;   // warps per screen CTA
+constexpr int kScreenSmemTasks = 128; // tasks whose table the screen keeps in shared memory
 constexpr int kNwWarps = 4;       // warps per NW CTA
 constexpr int kAlignCtasPerSm = 4; // resident align CTAs per SM (128 registers per thread)
 constexpr int kStageBytes = 4096; // traceback staging per warp
@@ -98,7 +99,8 @@ __host__ __device__ inline int rm_kbound(int rm_pairs) {
 }
 __host__ __device__ inline size_t nw_smem_per_warp_vec(const NwGeom& g) {
   return align16(g.lmax + 2 * kSeqPad) * 2 + align16(size_t(3) * g.vec_ncol * 2) + align16(size_t(g.vec_ncol) * 2) +
-         align16(g.vec_ncol) + align16(kStageBytes) + align16(g.lmax) + align16(size_t(g.lmax) * 2);
+         align16(g.vec_ncol) + align16(kStageBytes) + align16(g.lmax) + align16(size_t(g.lmax) * 2) +
+         align16(g.lmax);
 }
 __host__ __device__ inline size_t nw_smem_per_warp_rm(const NwGeom& g) {
   return align16(g.lmax) * 4 + align16(size_t(32) * 2 * rm_kbound(g.rm_pairs) * 4) + align16(g.lmax) +

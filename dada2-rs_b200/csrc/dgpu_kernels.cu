@@ -158,16 +158,44 @@ __global__ void __launch_bounds__(kScreenWarps * 32, 4) k_screen(CompareLaunch L
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const uint32_t warps_total = gridDim.x * kScreenWarps;
   const uint8_t* kmer8 = L.pool.kmer8;
+  // The task table and its prefix go to shared memory when they fit, so the
+  // per-item task search costs no global round trips.
+  __shared__ uint32_t s_prefix[kScreenSmemTasks + 1];
+  __shared__ uint32_t s_base[kScreenSmemTasks], s_center[kScreenSmemTasks], s_creads[kScreenSmemTasks];
+  __shared__ double s_cutoff[kScreenSmemTasks];
+  const bool tasks_smem = L.ntask <= uint32_t(kScreenSmemTasks);
+  if (tasks_smem) {
+    for (uint32_t t = threadIdx.x; t <= L.ntask; t += blockDim.x) {
+      s_prefix[t] = L.task_prefix[t];
+      if (t < L.ntask) {
+        const TaskDev T = L.tasks[t];
+        s_base[t] = T.base;
+        s_center[t] = T.center;
+        s_creads[t] = T.center_reads;
+        s_cutoff[t] = T.cutoff;
+      }
+    }
+    __syncthreads();
+  }
   for (uint32_t chunk = (blockIdx.x * kScreenWarps + wib) * 32u; chunk < L.total_items; chunk += warps_total * 32u) {
     const uint32_t item = chunk + lane;
     const bool valid = item < L.total_items;
     uint32_t t = 0, g = 0, c = 0;
     bool skip = false;
     if (valid) {
-      t = find_task(L.task_prefix, L.ntask, item);
-      g = L.tasks[t].base + (item - L.task_prefix[t]);
-      c = L.tasks[t].center;
-      skip = kp.greedy && (L.pool.reads[g] > L.tasks[t].center_reads || L.pool.lock[g]);
+      uint32_t creads;
+      if (tasks_smem) {
+        t = find_task(s_prefix, L.ntask, item);
+        g = s_base[t] + (item - s_prefix[t]);
+        c = s_center[t];
+        creads = s_creads[t];
+      } else {
+        t = find_task(L.task_prefix, L.ntask, item);
+        g = L.tasks[t].base + (item - L.task_prefix[t]);
+        c = L.tasks[t].center;
+        creads = L.tasks[t].center_reads;
+      }
+      skip = kp.greedy && (L.pool.reads[g] > creads || L.pool.lock[g]);
     }
     const bool need = valid && !skip && kp.use_kmers;
     uint32_t mydot = 0, myovf = 0;
@@ -288,7 +316,7 @@ __global__ void __launch_bounds__(kScreenWarps * 32, 4) k_screen(CompareLaunch L
           const int lc = int(L.pool.len[c]), lg = int(L.pool.len[g]);
           const int minl = lc < lg ? lc : lg;
           kdist = 1.0 - double(mydot) / double(minl - K + 1);
-          shroud = kdist > L.tasks[t].cutoff;
+          shroud = kdist > (tasks_smem ? s_cutoff[t] : L.tasks[t].cutoff);
         }
         if (shroud) {
           L.pool.res_lambda[g] = 0.0;
@@ -321,7 +349,7 @@ struct VecSmem {
   uint8_t* prow;
   uint8_t* stage;
   uint8_t* tcode;
-  uint16_t* fidx;
+  uint16_t* fidx;  // followed by lmax bytes for the raw's staged qualities (vec_qual)
 };
 
 __device__ __forceinline__ int sat_sub1(int v) { return v == 0 ? 0 : v - 1; }
@@ -607,6 +635,37 @@ __device__ VecSmem carve_vec(unsigned char* base, int lmax, int ncol_bound) {
   S.tcode = take(lmax);
   S.fidx = reinterpret_cast<uint16_t*>(take(size_t(lmax) * 2));
   return S;
+}
+__device__ __forceinline__ uint8_t* vec_qual(const VecSmem& S, int lmax) {
+  return reinterpret_cast<uint8_t*>(S.fidx) + align16(size_t(lmax) * 2);
+}
+
+// Copies a (n bytes), b (m bytes) and, when q is given, q (m bytes) from
+// global to shared memory with every load of a 256-position block issued
+// before the first store, so a pair's inputs arrive in one round trip.
+__device__ __forceinline__ void stage3(int lane, const uint8_t* __restrict__ a, int n, uint8_t* da,
+                                       const uint8_t* __restrict__ b, int m, uint8_t* db,
+                                       const uint8_t* __restrict__ q, uint8_t* dq) {
+  const int top = n > m ? n : m;
+  for (int base = 0; base < top; base += 256) {
+    uint8_t va[8], vb[8], vq[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int p = base + lane + 32 * i;
+      va[i] = p < n ? __ldg(a + p) : uint8_t(0);
+      vb[i] = p < m ? __ldg(b + p) : uint8_t(0);
+      vq[i] = (q && p < m) ? __ldg(q + p) : uint8_t(0);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int p = base + lane + 32 * i;
+      if (p < n) da[p] = va[i];
+      if (p < m) {
+        db[p] = vb[i];
+        if (q) dq[p] = vq[i];
+      }
+    }
+  }
 }
 
 
@@ -1391,10 +1450,12 @@ __device__ bool vec_align_fast(int lane, int len1, int len2, int match, int mism
 }
 
 // Picks the register form when the pair's compressed width fits 128 columns.
+// With `staged` the caller has already put the shorter sequence (the first on
+// ties) in S.s1 and the other in S.s2, and g1/g2 point at those copies.
 __device__ bool vec_align_any(int lane, const uint8_t* g1, int l1, const uint8_t* g2, int l2, int16_t match,
                               int16_t mismatch, int16_t gap, int16_t egp, int band_in, const VecSmem& S,
                               uint8_t* scratch, int ncol_bound, int nrow_bound, uint32_t* ham_out, uint32_t* err_word,
-                              uint8_t* dbg0, uint8_t* dbg1, uint32_t* dbg_len) {
+                              uint8_t* dbg0, uint8_t* dbg1, uint32_t* dbg_len, bool staged = false) {
   const int len1 = min(l1, l2), len2 = max(l1, l2);
   const int band = band_in < 0 ? len2 : band_in;
   const int start_col = 1 + (min(band, len1) + 1) / 2;
@@ -1409,8 +1470,10 @@ __device__ bool vec_align_any(int lane, const uint8_t* g1, int l1, const uint8_t
     {
       const uint8_t* a = swap ? g2 : g1;
       const uint8_t* b = swap ? g1 : g2;
-      for (int p = lane; p < len1; p += 32) S.s1[p] = a[p];
-      for (int p = lane; p < len2; p += 32) S.s2[p] = b[p];
+      if (!staged) {
+        for (int p = lane; p < len1; p += 32) S.s1[p] = a[p];
+        for (int p = lane; p < len2; p += 32) S.s2[p] = b[p];
+      }
       for (int p = lane; p < kSeqPad; p += 32) {  // guard bytes: out-of-range positions score `fill`
         S.s1[-1 - p] = 0x10;
         S.s1[len1 + p] = 0x10;
@@ -1708,7 +1771,25 @@ __global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_align(Compar
     const int lc = int(L.pool.len[c]), lg = int(L.pool.len[g]);
     const uint8_t* sc = L.pool.seq + L.pool.off[c];
     const uint8_t* sg = L.pool.seq + L.pool.off[g];
+    const uint8_t* qg = L.pool.qual ? L.pool.qual + L.pool.off[g] : nullptr;
     const double kdist = L.pool.res_lambda[g];
+    const bool use_homo = kp.homo_gap != kp.gap && kp.homo_gap <= 0;
+    const bool rm = use_homo || !kp.vectorized || lc > 3500 || lg > 3500;
+    if (!rm) {
+      // both sequences (shorter first, as the vectorized aligner wants them)
+      // and the raw's qualities go to shared memory in one round trip; the
+      // steps below read them there
+      const bool swap = lc > lg;
+      uint8_t* dc = swap ? VS.s2 : VS.s1;
+      uint8_t* dg = swap ? VS.s1 : VS.s2;
+      uint8_t* dq = vec_qual(VS, L.geom.lmax);
+      const bool stage_q = kp.use_quals && qg != nullptr;
+      stage3(lane, sc, lc, dc, sg, lg, dg, stage_q ? qg : nullptr, dq);
+      __syncwarp();
+      sc = dc;
+      sg = dg;
+      if (stage_q) qg = dq;
+    }
     double kodist = -1.0;
     const int minl = lc < lg ? lc : lg;
     const bool want_kod = kp.use_kmers && kp.gapless && lc == lg;
@@ -1746,12 +1827,10 @@ __global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_align(Compar
       }
       method = AM_GAPLESS;
     } else {
-      const bool use_homo = kp.homo_gap != kp.gap && kp.homo_gap <= 0;
-      const bool vec = kp.vectorized && lc <= 3500 && lg <= 3500 && !use_homo;
-      if (vec) {
+      if (!rm) {
         ok = vec_align_any(lane, sc, lc, sg, lg, int16_t(kp.match), int16_t(kp.mismatch), int16_t(kp.gap), 0,
                            kp.band, VS, scratch, L.geom.vec_ncol, L.geom.vec_nrow, &ham, L.err_word, nullptr,
-                           nullptr, nullptr);
+                           nullptr, nullptr, true);
         method = AM_VECTORIZED;
       } else {
         ok = rm_dispatch(lane, sc, lc, sg, lg, kp, use_homo, kb, RS, reinterpret_cast<uint32_t*>(scratch), &ham,
@@ -1764,7 +1843,6 @@ __global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_align(Compar
     __syncwarp();
     double lam = 0.0;
     if (ok) {
-      const uint8_t* qg = L.pool.qual ? L.pool.qual + L.pool.off[g] : nullptr;
       const bool bad = build_fidx(lane, tcode, qg, lg, kp.ncol, kp.use_quals, fidx);
       __syncwarp();
       if (bad) {
