@@ -113,6 +113,7 @@ __host__ __device__ inline size_t align_smem_per_warp(const NwGeom& g) {
 }
 
 // ---- launchers (dgpu_kernels.cu) ----
+void launch_fill_f64(double* p, size_t n, double v, cudaStream_t st);
 void launch_profiles(const uint8_t* seq, const uint32_t* off, const uint32_t* len, uint32_t nraw,
                      int k, uint8_t* kmer8, uint8_t* sat, cudaStream_t st);
 // Runs screen/gapless/lambda, both NW kernels and the ordered store for `ntask`

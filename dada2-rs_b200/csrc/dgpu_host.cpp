@@ -61,6 +61,12 @@ struct GlobalStats {
 };
 static GlobalStats g_stats;
 
+// Host-to-device bytes the compare path copies (uploads, lock flags, task tables).
+static void count_h2d(uint64_t bytes) {
+  std::lock_guard<std::mutex> g(g_stats.mu);
+  g_stats.s.h2d_bytes += bytes;
+}
+
 // ---------------------------------------------------------------------------
 // Block cache. A finished pool gives its device and mapped-host blocks back
 // here (after synchronizing its stream, so every block in the cache is idle)
@@ -473,6 +479,7 @@ struct Pool {
     CUDA_TRY(cudaMemcpyAsync(len.p, lens, size_t(n) * 4, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(reads.p, rd, size_t(n) * 4, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(err.p, errm, size_t(16) * kp.ncol * 8, cudaMemcpyHostToDevice, st));
+    count_h2d(uint64_t(total) * (has_qual ? 2 : 1) + uint64_t(n) * 12 + uint64_t(16) * kp.ncol * 8);
     CUDA_TRY(cudaMemsetAsync(lock.p, 0, n, st));
     TRY(reset_e_minmax());
     if (kp.use_kmers) {
@@ -487,8 +494,8 @@ struct Pool {
   }
 
   int reset_e_minmax() {
-    std::vector<double> v(nraw ? nraw : 1, -999.0);  // B::new (src/containers.rs:342)
-    CUDA_TRY(cudaMemcpyAsync(e_minmax.p, v.data(), size_t(nraw) * 8, cudaMemcpyHostToDevice, st));
+    launch_fill_f64(e_minmax.p, nraw, -999.0, st);  // B::new (src/containers.rs:342)
+    CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(st));
     return 0;
   }
@@ -544,6 +551,7 @@ struct Pool {
 
   int push_locks(uint32_t base, uint32_t n, cudaStream_t s) {
     CUDA_TRY(cudaMemcpyAsync(lock.p + base, lock_host.h + base, n, cudaMemcpyHostToDevice, s));
+    count_h2d(n);
     return 0;
   }
 };
@@ -601,6 +609,7 @@ int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
   }
   pref[ntask] = total;
   CUDA_TRY(cudaMemcpyAsync(dpack.p, hpack.h, pack_bytes, cudaMemcpyHostToDevice, st));
+  count_h2d(pack_bytes);
   CompareLaunch L{};
   L.pool = Q.view();
   L.kp = Q.kp;
@@ -1542,75 +1551,149 @@ class JobQueue {
 // ---------------------------------------------------------------------------
 // Inputs: validation and encoding (src/dada.rs:248-418)
 // ---------------------------------------------------------------------------
-struct SampleInput {
-  uint32_t n = 0;
-  std::vector<uint8_t> seq;    // codes, concatenated
+// A batch of samples encoded for the pool: codes 1..4 and rounded mean
+// qualities of every unique back to back (sample after sample, input order),
+// with per-unique offsets, lengths, reads and priors. The byte buffers belong
+// to the caller (pinned host memory for an upload).
+struct EncodedView {
+  uint8_t* seq = nullptr;
+  uint8_t* qual = nullptr;  // null when the input has no qualities
   std::vector<uint32_t> off, len, reads;
-  std::vector<uint8_t> prior, qual;
-  bool has_qual = false;
+  std::vector<uint8_t> prior;
   uint32_t qmax = 0;
 };
 
-static int encode_sample(uint32_t s, uint32_t lo, uint32_t hi, const char* seqs, const uint32_t* offs,
-                         const uint32_t* lens, const uint32_t* abund, const uint8_t* prior, const uint32_t* qsums,
-                         int k, SampleInput& out) {
-  const std::string tag = "sample " + std::to_string(s) + ": ";
-  const uint32_t n = hi - lo;
-  if (n == 0) return fail(DGPU_E_INVALID, tag + "Zero input sequences.");
-  uint32_t maxlen = 0, minlen = 0xffffffffu;
-  for (uint32_t t = lo; t < hi; ++t) {
-    maxlen = std::max(maxlen, lens[t]);
-    minlen = std::min(minlen, lens[t]);
+// Structural checks of dada_uniques_cached (src/dada.rs:248-317) for each
+// sample, in the order the reference applies them; returns the index of the
+// first failing sample (nsamples if none) with its code and message. Also
+// returns the total sequence bytes.
+static int check_samples(int nsamples, const uint32_t* sample_start, const uint32_t* lens, int k, uint64_t* total,
+                         int* rc, std::string* msg) {
+  *total = 0;
+  for (int s = 0; s < nsamples; ++s) {
+    const uint32_t lo = sample_start[s], hi = sample_start[s + 1];
+    const std::string tag = "sample " + std::to_string(s) + ": ";
+    if (hi == lo) {
+      *rc = DGPU_E_INVALID;
+      *msg = tag + "Zero input sequences.";
+      return s;
+    }
+    uint32_t maxlen = 0, minlen = 0xffffffffu;
+    for (uint32_t t = lo; t < hi; ++t) {
+      maxlen = std::max(maxlen, lens[t]);
+      minlen = std::min(minlen, lens[t]);
+      *total += lens[t];
+    }
+    if (maxlen >= 9999) {
+      *rc = DGPU_E_INVALID;
+      *msg = tag + "Input sequences exceed the maximum allowed length (9999).";
+      return s;
+    }
+    if (k < 3 || k > 8) {
+      *rc = DGPU_E_INVALID;
+      *msg = tag + "kmer_size out of supported range (3..=8).";
+      return s;
+    }
+    if (k > 7) {
+      *rc = DGPU_E_UNSUPPORTED;
+      *msg = "kmer_size 8 (sparse screen) is not supported on the GPU path";
+      return s;
+    }
+    if (minlen <= uint32_t(k)) {
+      *rc = DGPU_E_INVALID;
+      *msg = tag + "All input sequences must be longer than the k-mer size.";
+      return s;
+    }
   }
-  if (maxlen >= 9999) return fail(DGPU_E_INVALID, tag + "Input sequences exceed the maximum allowed length (9999).");
-  if (k < 3 || k > 8) return fail(DGPU_E_INVALID, tag + "kmer_size out of supported range (3..=8).");
-  if (k > 7) return fail(DGPU_E_UNSUPPORTED, "kmer_size 8 (sparse screen) is not supported on the GPU path");
-  if (minlen <= uint32_t(k)) return fail(DGPU_E_INVALID, tag + "All input sequences must be longer than the k-mer size.");
-  out.n = n;
-  out.off.resize(n);
-  out.len.resize(n);
-  out.reads.resize(n);
-  out.prior.assign(n, 0);
-  out.has_qual = qsums != nullptr;
-  uint64_t total = 0;
-  for (uint32_t t = lo; t < hi; ++t) total += lens[t];
-  out.seq.resize(total);
-  if (out.has_qual) out.qual.resize(total);
+  return nsamples;
+}
+
+// Encodes uniques [sample_start[0], sample_start[nsamples]) into E (seq, qual
+// sized by the caller), in parallel chunks of uniques. Bases map A/C/G/T/U
+// (either case) to 1..4; qualities are round(sum / reads) saturated to u8
+// (src/containers.rs:128-137) and qmax the largest round(sum / max(reads, 1))
+// (src/dada.rs:337-346). On a non-ACGT base the first one in input order is
+// reported, as a sequential scan would: *bad_unique / *bad_pos (else
+// bad_unique = UINT32_MAX).
+static void encode_uniques(uint32_t t0, uint32_t t1, const char* seqs, const uint32_t* offs, const uint32_t* lens,
+                           const uint32_t* abund, const uint8_t* prior, const uint32_t* qsums, EncodedView& E,
+                           uint32_t* bad_unique, uint32_t* bad_pos) {
+  const uint32_t n = t1 - t0;
+  E.off.resize(n);
+  E.len.resize(n);
+  E.reads.resize(n);
+  E.prior.assign(n, 0);
   uint64_t w = 0;
-  out.qmax = 0;
-  for (uint32_t t = lo; t < hi; ++t) {
-    const uint32_t r = t - lo;
-    out.off[r] = uint32_t(w);
-    out.len[r] = lens[t];
-    out.reads[r] = abund[t];
-    out.prior[r] = prior ? prior[t] : 0;
-    const char* sq = seqs + offs[t];
-    for (uint32_t p = 0; p < lens[t]; ++p) {
-      uint8_t code;
-      switch (sq[p]) {
-        case 'A': case 'a': code = 1; break;
-        case 'C': case 'c': code = 2; break;
-        case 'G': case 'g': code = 3; break;
-        case 'T': case 't': case 'U': case 'u': code = 4; break;
-        default:
-          return fail(DGPU_E_INVALID, tag + "Sequence " + std::to_string(r) + " contains a non-ACGT base at position " +
-                                          std::to_string(p) + ".");
-      }
-      out.seq[w + p] = code;
-    }
-    if (out.has_qual) {  // src/containers.rs:128-137 and the qmax of src/dada.rs:337-346
-      const double c = double(abund[t]);
-      const double cq = double(std::max<uint32_t>(abund[t], 1));
-      for (uint32_t p = 0; p < lens[t]; ++p) {
-        const double q = std::round(double(qsums[offs[t] + p]) / c);
-        out.qual[w + p] = q >= 255.0 ? 255 : (q > 0.0 ? uint8_t(q) : 0);
-        const double qm = std::round(double(qsums[offs[t] + p]) / cq);
-        out.qmax = std::max<uint32_t>(out.qmax, qm > 0 ? uint32_t(qm) : 0);
-      }
-    }
-    w += lens[t];
+  for (uint32_t r = 0; r < n; ++r) {
+    E.off[r] = uint32_t(w);
+    E.len[r] = lens[t0 + r];
+    E.reads[r] = abund[t0 + r];
+    E.prior[r] = prior ? prior[t0 + r] : 0;
+    w += lens[t0 + r];
   }
-  return 0;
+  constexpr uint32_t kChunk = 512;
+  const uint32_t nch = (n + kChunk - 1) / kChunk;
+  std::vector<uint32_t> ch_bad(nch, 0xffffffffu), ch_pos(nch, 0), ch_qmax(nch, 0);
+  std::atomic<uint32_t> next{0};
+  auto work = [&] {
+    for (uint32_t c; (c = next.fetch_add(1)) < nch;) {
+      const uint32_t r0 = c * kChunk, r1 = std::min(n, r0 + kChunk);
+      uint32_t qm_max = 0;
+      for (uint32_t r = r0; r < r1; ++r) {
+        const uint32_t t = t0 + r;
+        const char* sq = seqs + offs[t];
+        uint8_t* out = E.seq + E.off[r];
+        bool bad = false;
+        for (uint32_t p = 0; p < lens[t]; ++p) {
+          uint8_t code;
+          switch (sq[p]) {
+            case 'A': case 'a': code = 1; break;
+            case 'C': case 'c': code = 2; break;
+            case 'G': case 'g': code = 3; break;
+            case 'T': case 't': case 'U': case 'u': code = 4; break;
+            default: code = 0; break;
+          }
+          if (!code) {
+            ch_bad[c] = r;
+            ch_pos[c] = p;
+            bad = true;
+            break;
+          }
+          out[p] = code;
+        }
+        if (bad) break;  // later uniques of this chunk cannot be the first failure
+        if (E.qual) {
+          const double cnt = double(abund[t]);
+          const double cq = double(std::max<uint32_t>(abund[t], 1));
+          const uint32_t* qs = qsums + offs[t];
+          uint8_t* qo = E.qual + E.off[r];
+          for (uint32_t p = 0; p < lens[t]; ++p) {
+            const double q = std::round(double(qs[p]) / cnt);
+            qo[p] = q >= 255.0 ? 255 : (q > 0.0 ? uint8_t(q) : 0);
+            const double qm = std::round(double(qs[p]) / cq);
+            qm_max = std::max<uint32_t>(qm_max, qm > 0 ? uint32_t(qm) : 0);
+          }
+        }
+      }
+      ch_qmax[c] = qm_max;
+    }
+  };
+  const uint32_t nt = std::max(1u, std::min(nch, std::thread::hardware_concurrency()));
+  std::vector<std::thread> th;
+  for (uint32_t t = 1; t < nt; ++t) th.emplace_back(work);
+  work();
+  for (auto& t : th) t.join();
+  *bad_unique = 0xffffffffu;
+  *bad_pos = 0;
+  E.qmax = 0;
+  for (uint32_t c = 0; c < nch; ++c) {
+    if (ch_bad[c] != 0xffffffffu) {
+      *bad_unique = ch_bad[c];
+      *bad_pos = ch_pos[c];
+      return;
+    }
+    E.qmax = std::max(E.qmax, ch_qmax[c]);
+  }
 }
 
 // Repeat the last learned column up to qmax (src/dada.rs:337-384).
@@ -1660,8 +1743,15 @@ struct dgpu_result {
 
 namespace dgpu {
 
+// The codes of one sample's uniques: raw r at seq + off[r], len[r] bytes.
+struct SampleSeqs {
+  const uint8_t* seq;
+  const uint32_t* off;
+  const uint32_t* len;
+};
+
 // Final p-values, the map and the cluster summaries (src/dada.rs:502-564).
-static dgpu_result* finish(SampleState& S, const SampleInput& in) {
+static dgpu_result* finish(SampleState& S, const SampleSeqs& in) {
   dgpu_result* R = new dgpu_result();
   const uint32_t n = S.n;
   R->nraw = n;
@@ -1700,7 +1790,7 @@ static dgpu_result* finish(SampleState& S, const SampleInput& in) {
     R->cl_seq_off.push_back(so);
     if (c.center >= 0) {
       const uint32_t ce = uint32_t(c.center);
-      R->cl_seq.insert(R->cl_seq.end(), in.seq.begin() + in.off[ce], in.seq.begin() + in.off[ce] + in.len[ce]);
+      R->cl_seq.insert(R->cl_seq.end(), in.seq + in.off[ce], in.seq + in.off[ce] + in.len[ce]);
       so += in.len[ce];
     }
     R->cl_mem_off.push_back(mo);
@@ -1850,13 +1940,17 @@ static int launch_slots(int nsamples) {
 // A prepared batch: encoded samples resident on one device.
 struct Batch {
   Pool pool;
-  std::vector<SampleInput> in;
-  std::vector<uint32_t> bases, reads;
-  std::vector<uint8_t> priors;
+  HBuf<uint8_t> seq_h, qual_h;  // pinned encoded codes / qualities of every unique
+  EncodedView E;
+  std::vector<uint32_t> bases, counts;  // first raw and number of raws of each sample
   DadaConf conf{};
   std::vector<DadaConf> confs;
   dgpu_align_params align{};
   int host_threads = 1;
+  ~Batch() {  // Pool::upload waited for its copies, so the staging blocks are idle
+    seq_h.recycle();
+    qual_h.recycle();
+  }
 };
 
 static int batch_prepare(Batch& B, int device, const dgpu_dada_params* prm, int nsamples, const uint32_t* sample_start,
@@ -1866,63 +1960,45 @@ static int batch_prepare(Batch& B, int device, const dgpu_dada_params* prm, int 
     return fail(DGPU_E_INVALID, "null argument or no samples");
   if (ncol <= 0) return fail(DGPU_E_INVALID, "Error matrix length does not match 16 x ncol.");
   const int k = prm->align.kmer_size;
-  B.in.assign(static_cast<size_t>(nsamples), SampleInput());
-  uint32_t qmax = 0;
-  bool any_q = false;
   for (int s = 0; s < nsamples; ++s)
     if (sample_start[s + 1] < sample_start[s]) return fail(DGPU_E_INVALID, "sample_start must be non-decreasing");
-  {
-    // encode samples in parallel; the first failing sample (by index) reports
-    std::vector<int> rcs(static_cast<size_t>(nsamples), 0);
-    std::vector<std::string> msgs(static_cast<size_t>(nsamples));
-    const int nt = std::max(1, std::min(nsamples, int(std::thread::hardware_concurrency())));
-    std::atomic<int> next{0};
-    auto work = [&] {
-      for (;;) {
-        const int s = next.fetch_add(1);
-        if (s >= nsamples) break;
-        rcs[size_t(s)] = encode_sample(uint32_t(s), sample_start[s], sample_start[s + 1], seqs, offs, lens, abund,
-                                       prior, qsums, k, B.in[size_t(s)]);
-        if (rcs[size_t(s)]) msgs[size_t(s)] = g_err;
-      }
-    };
-    std::vector<std::thread> th;
-    for (int t = 1; t < nt; ++t) th.emplace_back(work);
-    work();
-    for (auto& t : th) t.join();
-    for (int s = 0; s < nsamples; ++s)
-      if (rcs[size_t(s)]) return fail(rcs[size_t(s)], msgs[size_t(s)]);
+  // The reference validates sample after sample: the first sample that fails
+  // a structural check or holds a non-ACGT base reports.
+  uint64_t total = 0;
+  int src = 0;
+  std::string smsg;
+  const int first_bad = check_samples(nsamples, sample_start, lens, k, &total, &src, &smsg);
+  if (total >= 0xffffffffull) return fail(DGPU_E_UNSUPPORTED, "more than 4 GiB of sequence in one pool");
+  TRY(B.pool.init(device, launch_slots(nsamples)));
+  const int ns_ok = first_bad;  // samples [0, ns_ok) passed the structural checks
+  uint64_t ok_bytes = 0;
+  for (uint32_t t = sample_start[0]; t < sample_start[ns_ok]; ++t) ok_bytes += lens[t];
+  TRY(B.seq_h.alloc(size_t(ok_bytes ? ok_bytes : 1)));
+  if (qsums) TRY(B.qual_h.alloc(size_t(ok_bytes ? ok_bytes : 1)));
+  B.E.seq = B.seq_h.h;
+  B.E.qual = qsums ? B.qual_h.h : nullptr;
+  uint32_t bad_t = 0, bad_p = 0;
+  encode_uniques(sample_start[0], sample_start[ns_ok], seqs, offs, lens, abund, prior, qsums, B.E, &bad_t, &bad_p);
+  if (bad_t != 0xffffffffu) {
+    const uint32_t t = sample_start[0] + bad_t;
+    int s = 0;
+    while (sample_start[s + 1] <= t) ++s;
+    return fail(DGPU_E_INVALID, "sample " + std::to_string(s) + ": Sequence " + std::to_string(t - sample_start[s]) +
+                                    " contains a non-ACGT base at position " + std::to_string(bad_p) + ".");
   }
+  if (first_bad < nsamples) return fail(src, smsg);
+  B.bases.resize(size_t(nsamples));
+  B.counts.resize(size_t(nsamples));
   for (int s = 0; s < nsamples; ++s) {
-    if (B.in[size_t(s)].has_qual) {
-      any_q = true;
-      qmax = std::max(qmax, B.in[size_t(s)].qmax);
-    }
+    B.bases[size_t(s)] = sample_start[s] - sample_start[0];
+    B.counts[size_t(s)] = sample_start[s + 1] - sample_start[s];
   }
   int ncol2 = ncol;
-  std::vector<double> err = any_q ? extend_err(errm, ncol, qmax, ncol2)
+  std::vector<double> err = qsums ? extend_err(errm, ncol, B.E.qmax, ncol2)
                                   : std::vector<double>(errm, errm + 16 * size_t(ncol));
-  std::vector<uint8_t> seqcat, qualcat;
-  std::vector<uint32_t> off, len;
-  for (const SampleInput& si : B.in) {
-    B.bases.push_back(uint32_t(off.size()));
-    const uint32_t sb = uint32_t(seqcat.size());
-    seqcat.insert(seqcat.end(), si.seq.begin(), si.seq.end());
-    if (any_q) {
-      if (si.has_qual) qualcat.insert(qualcat.end(), si.qual.begin(), si.qual.end());
-      else qualcat.insert(qualcat.end(), si.seq.size(), 0);
-    }
-    for (uint32_t r = 0; r < si.n; ++r) {
-      off.push_back(sb + si.off[r]);
-      len.push_back(si.len[r]);
-      B.reads.push_back(si.reads[r]);
-      B.priors.push_back(si.prior[r]);
-    }
-  }
-  TRY(B.pool.init(device, launch_slots(nsamples)));
   const KParams kp = to_kparams(prm->align, prm->use_quals, prm->greedy, ncol2);
-  TRY(B.pool.upload(uint32_t(off.size()), seqcat.data(), off.data(), len.data(), any_q ? qualcat.data() : nullptr,
-                    B.reads.data(), kp, err.data()));
+  TRY(B.pool.upload(uint32_t(B.E.off.size()), B.E.seq, B.E.off.data(), B.E.len.data(), B.E.qual, B.E.reads.data(), kp,
+                    err.data()));
   B.conf.omega_a = prm->omega_a;
   B.conf.omega_p = prm->omega_p;
   B.conf.omega_c = prm->omega_c;
@@ -1934,7 +2010,7 @@ static int batch_prepare(Batch& B, int device, const dgpu_dada_params* prm, int 
   B.conf.min_abund = prm->min_abund;
   B.confs.assign(static_cast<size_t>(nsamples), B.conf);
   for (int s = 0; s < nsamples; ++s)
-    B.confs[size_t(s)].max_clust = prm->max_clust == 0 ? B.in[size_t(s)].n : size_t(prm->max_clust);
+    B.confs[size_t(s)].max_clust = prm->max_clust == 0 ? B.counts[size_t(s)] : size_t(prm->max_clust);
   B.align = prm->align;
   // Host phases of different samples share the cores with the intra-sample
   // helpers (half the cores) and the launch workers, so by default they get
@@ -1946,7 +2022,7 @@ static int batch_prepare(Batch& B, int device, const dgpu_dada_params* prm, int 
 }
 
 static int batch_run(Batch& B, dgpu_result** out) {
-  const size_t ns = B.in.size();
+  const size_t ns = B.counts.size();
   Pool& P = B.pool;
   CUDA_TRY(cudaSetDevice(P.device));
   TRY(P.reset_e_minmax());
@@ -1955,10 +2031,20 @@ static int batch_run(Batch& B, dgpu_result** out) {
   CUDA_TRY(cudaStreamSynchronize(P.st));  // the launch slots run on their own streams
   std::vector<SampleState> S(ns);
   for (size_t s = 0; s < ns; ++s)
-    S[s].init(B.in[s].n, B.bases[s], B.reads.data() + B.bases[s], B.priors.data() + B.bases[s],
+    S[s].init(B.counts[s], B.bases[s], B.E.reads.data() + B.bases[s], B.E.prior.data() + B.bases[s],
               P.lock_host.h + B.bases[s], &B.confs[s]);
   TRY(run_samples(P, S, B.align, B.host_threads));
-  for (size_t s = 0; s < ns; ++s) out[s] = finish(S[s], B.in[s]);
+  // final p-values and result tables, samples in parallel
+  std::atomic<size_t> next{0};
+  auto work = [&] {
+    for (size_t s; (s = next.fetch_add(1)) < ns;)
+      out[s] = finish(S[s], SampleSeqs{B.E.seq, B.E.off.data() + B.bases[s], B.E.len.data() + B.bases[s]});
+  };
+  const size_t nt = std::min<size_t>(ns, std::max(1u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> th;
+  for (size_t t = 1; t < nt; ++t) th.emplace_back(work);
+  work();
+  for (auto& t : th) t.join();
   return 0;
 }
 

@@ -98,6 +98,16 @@ void launch_profiles(const uint8_t* seq, const uint32_t* off, const uint32_t* le
   k_profiles<<<grid, 256, smem, st>>>(seq, off, len, nraw, k, kmer8, sat);
 }
 
+__global__ void k_fill_f64(double* __restrict__ p, size_t n, double v) {
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) p[i] = v;
+}
+
+void launch_fill_f64(double* p, size_t n, double v, cudaStream_t st) {
+  if (n == 0) return;
+  const size_t blocks = std::min<size_t>((n + 255) / 256, size_t(148) * 8);
+  k_fill_f64<<<unsigned(blocks), 256, 0, st>>>(p, n, v);
+}
+
 // ---------------------------------------------------------------------------
 // Shared helpers for the lambda product
 // ---------------------------------------------------------------------------

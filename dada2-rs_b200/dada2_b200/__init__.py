@@ -197,19 +197,46 @@ def _read_result(h) -> dict:
     res["map"] = a["map"][:nraw]
     res["pvals"] = a["pvals"][:nraw]
     res["counters"] = {k: int(v) for k, v in zip(COUNTER_KEYS, a["counters"])}
-    res["clusters"] = []
-    for ci in range(ncl):
+    res["clusters"] = ClusterList(a, ncl)
+    return res
+
+
+class ClusterList:
+    """Per-cluster views of a result's flat arrays (``cl_*``, ``mem_*``), built
+    on access: ``len``, indexing and iteration give one dict per cluster with
+    its center ``sequence`` (codes 1..4), ``reads``, ``members`` (raw indices in
+    membership order) with their ``hammings``, ``lambdas`` and ``pvals``, and
+    the ``birth_*`` statistics."""
+
+    def __init__(self, a: dict, n: int):
+        self._a = a
+        self._n = n
+
+    def __len__(self):
+        return self._n
+
+    def __getitem__(self, ci):
+        if isinstance(ci, slice):
+            return [self[k] for k in range(*ci.indices(self._n))]
+        if ci < 0:
+            ci += self._n
+        if not 0 <= ci < self._n:
+            raise IndexError(ci)
+        a = self._a
         s0, s1 = a["cl_seq_off"][ci], a["cl_seq_off"][ci + 1]
         m0, m1 = a["cl_mem_off"][ci], a["cl_mem_off"][ci + 1]
-        res["clusters"].append({
+        return {
             "sequence": a["cl_seq"][s0:s1].copy(), "reads": int(a["cl_reads"][ci]),
             "members": a["mem_raw"][m0:m1].copy(), "hammings": a["mem_hamming"][m0:m1].copy(),
             "lambdas": a["mem_lambda"][m0:m1].copy(), "pvals": a["mem_pval"][m0:m1].copy(),
             "birth_type": int(a["cl_birth_type"][ci]), "birth_from": int(a["cl_birth_from"][ci]),
             "birth_pval": float(a["cl_birth_pval"][ci]), "birth_fold": float(a["cl_birth_fold"][ci]),
             "birth_e": float(a["cl_birth_e"][ci]), "birth_hamming": int(a["cl_birth_hamming"][ci]),
-        })
-    return res
+        }
+
+    def __iter__(self):
+        for ci in range(self._n):
+            yield self[ci]
 
 
 def dada_uniques(seqs, abund, err, ncol, params: DadaParams | None = None, quals=None, prior=None,
@@ -366,7 +393,8 @@ def stats_read() -> dict:
             "ms": {k: float(s.ms[i]) for i, k in enumerate(KERNEL_NAMES)},
             "rounds": int(s.rounds), "compares": int(s.compares), "screened": int(s.screened),
             "screen_bytes": int(s.screen_bytes), "timed_rounds": int(s.timed_rounds),
-            "timed_screen_bytes": int(s.timed_screen_bytes), "timed_compares": int(s.timed_compares)}
+            "timed_screen_bytes": int(s.timed_screen_bytes), "timed_compares": int(s.timed_compares),
+            "h2d_bytes": int(s.h2d_bytes)}
 
 
 ALIGN_VECTORIZED, ALIGN_HOMO, ALIGN_ENDSFREE = 0, 1, 2

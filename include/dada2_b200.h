@@ -117,6 +117,7 @@ typedef struct {
   double ms[4];
   uint64_t rounds, compares, screened, screen_bytes;
   uint64_t timed_rounds, timed_screen_bytes, timed_compares;
+  uint64_t h2d_bytes;  /* host-to-device bytes copied: uploads, lock flags, per-call task tables */
 } dgpu_kernel_stats;
 
 const char* dgpu_last_error(void);

@@ -295,6 +295,29 @@ def test_invalid_inputs_are_rejected_like_the_reference():
         D.dada_uniques([], [], err, 41)
 
 
+class _S:
+    def __init__(self, seqs, abund):
+        self.seqs, self.abund = seqs, np.array(abund, np.uint32)
+        self.quals = [np.full(len(x), 30 * a, np.uint32) for x, a in zip(seqs, abund)]
+
+
+def test_batch_reports_the_first_failing_sample_in_input_order():
+    """Samples are validated in order (src/dada.rs:248-317): the first sample
+    with a structural error or a non-ACGT base reports, and within a sample
+    the length checks come before the base scan."""
+    err = np.full(16 * 41, 0.01)
+    good = _S(["ACGTACGTAA", "ACGTACGTAC"], [3, 2])
+    bad_base = _S(["ACGTACGTAA", "ACGTACNTAC", "ACGTXCGTAC"], [3, 2, 1])
+    too_short = _S(["ACGTACGTAA", "ACG"], [3, 2])
+    with pytest.raises(D.InvalidInput, match=r"sample 1: Sequence 1 contains a non-ACGT base at position 6"):
+        D.dada_uniques_batch([good, bad_base, too_short], err, 41)
+    with pytest.raises(D.InvalidInput, match=r"sample 1: All input sequences must be longer"):
+        D.dada_uniques_batch([good, too_short, bad_base], err, 41)
+    both = _S(["ACGTNCGTAA", "ACG"], [3, 2])  # structural failure wins inside one sample
+    with pytest.raises(D.InvalidInput, match=r"sample 0: All input sequences must be longer"):
+        D.dada_uniques_batch([both, good], err, 41)
+
+
 def test_resident_batch_runs_repeat_identically():
     ws = [synth.small_illumina(60 + i, nvariants=5, nreads=900 + 400 * i, L=110) for i in range(3)]
     err, ncol = ws[0].err, ws[0].ncol
