@@ -23,8 +23,13 @@ struct PoolDev {
   const uint8_t* qual;    // rounded mean Phred, same offsets (nullptr: none)
   const uint32_t* off;
   const uint32_t* len;
-  const uint8_t* kmer8;   // nraw x 4^k saturating u8 counts
+  const uint8_t* kmer8;   // nraw x 4^k saturating u8 counts (k <= 7)
   const uint8_t* sat;     // per raw: some k-mer count reached 255
+  // k = 8: each raw's present k-mers as ascending (index, saturating count)
+  // pairs, kidx/kcnt[off[g] .. off[g] + knum[g])
+  const uint16_t* kidx;
+  const uint8_t* kcnt;
+  const uint32_t* knum;
   const uint32_t* reads;
   const uint8_t* lock;
   double* e_minmax;
@@ -116,6 +121,10 @@ __host__ __device__ inline size_t align_smem_per_warp(const NwGeom& g) {
 void launch_fill_f64(double* p, size_t n, double v, cudaStream_t st);
 void launch_profiles(const uint8_t* seq, const uint32_t* off, const uint32_t* len, uint32_t nraw,
                      int k, uint8_t* kmer8, uint8_t* sat, cudaStream_t st);
+// k = 8: sparse profiles (see PoolDev::kidx); lmax bounds every length.
+void launch_profiles_sparse(const uint8_t* seq, const uint32_t* off, const uint32_t* len, uint32_t nraw,
+                            uint32_t lmax, uint16_t* kidx, uint8_t* kcnt, uint32_t* knum, uint8_t* sat,
+                            cudaStream_t st);
 // Runs screen/gapless/lambda, both NW kernels and the ordered store for `ntask`
 // tasks; `task_prefix` holds ntask+1 running raw counts.
 struct CompareLaunch {

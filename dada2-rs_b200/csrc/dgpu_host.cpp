@@ -378,7 +378,9 @@ struct Pool {
   int sms = 148;
   int nslots = 1;
   DBuf<uint8_t> seq, qual, kmer8, sat, lock, status;
-  DBuf<uint32_t> off, len, reads, ham;
+  DBuf<uint32_t> off, len, reads, ham, knum;
+  DBuf<uint16_t> kidx;
+  DBuf<uint8_t> kcnt;
   DBuf<double> e_minmax, err, lambda;
   // stored comps of each task, at the task's first raw (its sample's base)
   HBuf<uint32_t> comp_index, comp_ham;
@@ -390,7 +392,7 @@ struct Pool {
   ~Pool() {
     slots.clear();  // each slot drains its own stream first
     if (st && cudaStreamSynchronize(st) == cudaSuccess)
-      recycle_all(seq, qual, kmer8, sat, lock, status, off, len, reads, ham, e_minmax, err, lambda,
+      recycle_all(seq, qual, kmer8, sat, lock, status, off, len, reads, ham, knum, kidx, kcnt, e_minmax, err, lambda,
                   comp_index, comp_ham, comp_lambda, lock_host);
     if (st) cudaStreamDestroy(st);
   }
@@ -463,7 +465,11 @@ struct Pool {
     TRY(lambda.alloc(n));
     TRY(e_minmax.alloc(n));
     TRY(err.alloc(size_t(16) * kp.ncol));
-    TRY(kmer8.alloc(kp.use_kmers ? size_t(n) * nk : 1));
+    const bool sparse = kp.use_kmers && kp.kmer_size >= 8;  // src/kmers.rs:213-221
+    TRY(kmer8.alloc(kp.use_kmers && !sparse ? size_t(n) * nk : 1));
+    TRY(kidx.alloc(sparse ? seq_bytes : 1));
+    TRY(kcnt.alloc(sparse ? seq_bytes : 1));
+    TRY(knum.alloc(sparse ? n : 1));
     TRY(sat.alloc(n));
     TRY(comp_index.alloc(n));
     TRY(comp_ham.alloc(n));
@@ -483,7 +489,10 @@ struct Pool {
     CUDA_TRY(cudaMemsetAsync(lock.p, 0, n, st));
     TRY(reset_e_minmax());
     if (kp.use_kmers) {
-      launch_profiles(seq.p, off.p, len.p, n, kp.kmer_size, kmer8.p, sat.p, st);
+      if (sparse)
+        launch_profiles_sparse(seq.p, off.p, len.p, n, lmax, kidx.p, kcnt.p, knum.p, sat.p, st);
+      else
+        launch_profiles(seq.p, off.p, len.p, n, kp.kmer_size, kmer8.p, sat.p, st);
       std::lock_guard<std::mutex> g(g_stats.mu);
       g_stats.s.launches[0] += 1;
     }
@@ -537,6 +546,9 @@ struct Pool {
     v.len = len.p;
     v.kmer8 = kmer8.p;
     v.sat = sat.p;
+    v.kidx = kidx.p;
+    v.kcnt = kcnt.p;
+    v.knum = knum.p;
     v.reads = reads.p;
     v.lock = lock.p;
     v.e_minmax = e_minmax.p;
@@ -660,7 +672,11 @@ int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
     S.rounds += 1;
     S.compares += total;
     S.screened += screened;
-    const uint64_t sb = screened * (uint64_t(1) << (2 * Q.kp.kmer_size)) + uint64_t(total) * 16u;
+    // algorithmic screen bytes: the raw's 4^k profile, or for k = 8 its sparse
+    // list (3 bytes per present k-mer, at most L - k + 1), plus 16 B of metadata
+    const uint64_t prof = Q.kp.kmer_size >= 8 ? uint64_t(3) * (Q.lmax - uint32_t(Q.kp.kmer_size) + 1)
+                                              : (uint64_t(1) << (2 * Q.kp.kmer_size));
+    const uint64_t sb = screened * prof + uint64_t(total) * 16u;
     S.screen_bytes += sb;
     if (timing) {
       S.timed_rounds += 1;
@@ -1594,11 +1610,6 @@ static int check_samples(int nsamples, const uint32_t* sample_start, const uint3
       *msg = tag + "kmer_size out of supported range (3..=8).";
       return s;
     }
-    if (k > 7) {
-      *rc = DGPU_E_UNSUPPORTED;
-      *msg = "kmer_size 8 (sparse screen) is not supported on the GPU path";
-      return s;
-    }
     if (minlen <= uint32_t(k)) {
       *rc = DGPU_E_INVALID;
       *msg = tag + "All input sequences must be longer than the k-mer size.";
@@ -2089,7 +2100,6 @@ int dgpu_ctx_create(int device, const dgpu_align_params* params, const double* e
   if (!params || !err_mat || !out || ncol <= 0) return fail(DGPU_E_INVALID, "null argument or ncol <= 0");
   if (params->kmer_size < 3 || params->kmer_size > 8)
     return fail(DGPU_E_INVALID, "kmer_size out of supported range (3..=8).");
-  if (params->kmer_size > 7) return fail(DGPU_E_UNSUPPORTED, "kmer_size 8 (sparse screen) is not supported on the GPU path");
   dgpu_ctx* c = new dgpu_ctx();
   int rc = c->pool.init(device);
   if (rc) {

@@ -98,6 +98,96 @@ void launch_profiles(const uint8_t* seq, const uint32_t* off, const uint32_t* le
   k_profiles<<<grid, 256, smem, st>>>(seq, off, len, nraw, k, kmer8, sat);
 }
 
+// K1 for k = 8 (src/kmers.rs:113-120): one CTA per raw sorts its window codes
+// in shared memory (bitonic), then run-length encodes them into ascending
+// (index, count) pairs with counts saturating at 255 (the u16 count is exact up
+// to 9,991 windows, so `count >= 255` also gives the saturation flag).
+__global__ void __launch_bounds__(256) k_profiles_sparse(const uint8_t* __restrict__ seq,
+                                                         const uint32_t* __restrict__ off,
+                                                         const uint32_t* __restrict__ len, uint32_t nraw,
+                                                         uint16_t* __restrict__ kidx, uint8_t* __restrict__ kcnt,
+                                                         uint32_t* __restrict__ knum, uint8_t* __restrict__ sat) {
+  extern __shared__ uint32_t keys[];  // padded to a power of two >= the longest window count
+  __shared__ uint32_t warp_tot[8];
+  __shared__ int any_sat;
+  constexpr int K = 8;
+  for (uint32_t g = blockIdx.x; g < nraw; g += gridDim.x) {
+    const uint8_t* s = seq + off[g];
+    const int L = int(len[g]);
+    const int nwin = L >= K ? L - K + 1 : 0;
+    int np2 = 1;
+    while (np2 < nwin) np2 <<= 1;
+    for (int p = threadIdx.x; p < np2; p += blockDim.x) {
+      uint32_t x = 0xffffffffu;  // padding sorts last
+      if (p < nwin) {
+        x = 0;
+        for (int q = 0; q < K; ++q) x = x * 4u + (unsigned(s[p + q]) - 1u);  // codes are 1..4 (validated)
+      }
+      keys[p] = x;
+    }
+    if (threadIdx.x == 0) any_sat = 0;
+    __syncthreads();
+    for (int size = 2; size <= np2; size <<= 1) {
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        for (int i = threadIdx.x; i < np2; i += blockDim.x) {
+          const int j = i ^ stride;
+          if (j > i) {
+            const bool up = (i & size) == 0;
+            const uint32_t a = keys[i], b = keys[j];
+            if ((a > b) == up) {
+              keys[i] = b;
+              keys[j] = a;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    // run starts -> ascending distinct indices with their counts
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t written = 0;
+    for (int base = 0; base < nwin; base += blockDim.x) {
+      const int i = base + threadIdx.x;
+      const bool start = i < nwin && (i == 0 || keys[i] != keys[i - 1]);
+      const uint32_t bal = __ballot_sync(FULL, start);
+      if (lane == 0) warp_tot[w] = __popc(bal);
+      __syncthreads();
+      uint32_t before = written;
+      for (int q = 0; q < w; ++q) before += warp_tot[q];
+      uint32_t tot = 0;
+      for (int q = 0; q < int(blockDim.x >> 5); ++q) tot += warp_tot[q];
+      if (start) {
+        int e = i + 1;
+        while (e < nwin && keys[e] == keys[i]) ++e;
+        const int cnt = e - i;
+        const uint32_t slot = before + __popc(bal & ((1u << lane) - 1u));
+        kidx[off[g] + slot] = uint16_t(keys[i]);
+        kcnt[off[g] + slot] = uint8_t(cnt < 255 ? cnt : 255);
+        if (cnt >= 255) any_sat = 1;
+      }
+      written += tot;
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      knum[g] = written;
+      sat[g] = uint8_t(any_sat);
+    }
+    __syncthreads();
+  }
+}
+
+void launch_profiles_sparse(const uint8_t* seq, const uint32_t* off, const uint32_t* len, uint32_t nraw, uint32_t lmax,
+                            uint16_t* kidx, uint8_t* kcnt, uint32_t* knum, uint8_t* sat, cudaStream_t st) {
+  if (nraw == 0) return;
+  size_t np2 = 1;
+  while (np2 < lmax) np2 <<= 1;
+  const size_t smem = np2 * 4;
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(k_profiles_sparse, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  const int grid = int(nraw < 148u * 8u ? nraw : 148u * 8u);
+  k_profiles_sparse<<<grid, 256, smem, st>>>(seq, off, len, nraw, kidx, kcnt, knum, sat);
+}
+
 __global__ void k_fill_f64(double* __restrict__ p, size_t n, double v) {
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) p[i] = v;
 }
@@ -210,70 +300,99 @@ __global__ void __launch_bounds__(kScreenWarps * 32, 4) k_screen(CompareLaunch L
     const bool need = valid && !skip && kp.use_kmers;
     uint32_t mydot = 0, myovf = 0;
     uint32_t todo = __ballot_sync(FULL, need);
-    // center profile of the chunk's first needing item, kept in registers
-    uint32_t cur_c = 0xffffffffu;
-    uint4 cv[CENTER_REGS ? VPL : 1];
-    (void)cur_c;
-    while (todo) {
-      int js[NB];
-#pragma unroll
-      for (int q = 0; q < NB; ++q) {
-        js[q] = -1;
-        if (todo) {
-          js[q] = __ffs(todo) - 1;
-          todo &= todo - 1;
+    if constexpr (K >= 8) {
+      // Sparse screen (src/kmers.rs:280-308): only k-mers present in both
+      // sequences contribute min(count, count); one item at a time, each lane
+      // takes raw entries and finds their index in the center's ascending list.
+      while (todo) {
+        const int j = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const uint32_t gj = __shfl_sync(FULL, g, j), cj = __shfl_sync(FULL, c, j);
+        const uint32_t na = L.pool.knum[gj], nc = L.pool.knum[cj];
+        const uint16_t* ai = L.pool.kidx + L.pool.off[gj];
+        const uint8_t* ac = L.pool.kcnt + L.pool.off[gj];
+        const uint16_t* ci = L.pool.kidx + L.pool.off[cj];
+        const uint8_t* cc = L.pool.kcnt + L.pool.off[cj];
+        uint32_t dot = 0;
+        for (uint32_t e = lane; e < na; e += 32) {
+          const uint16_t x = ai[e];
+          uint32_t lo = 0, hi = nc;
+          while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (ci[mid] < x) lo = mid + 1;
+            else hi = mid;
+          }
+          if (lo < nc && ci[lo] == x) dot += min(unsigned(ac[e]), unsigned(cc[lo]));
         }
+        dot = __reduce_add_sync(FULL, dot);
+        if (lane == j) mydot = dot;
       }
-      uint32_t gq[NB], cq[NB];
-#pragma unroll
-      for (int q = 0; q < NB; ++q) {
-        const int src = js[q] < 0 ? 0 : js[q];
-        gq[q] = __shfl_sync(FULL, g, src);
-        cq[q] = __shfl_sync(FULL, c, src);
-      }
-      constexpr int RV = CENTER_REGS ? VPL : 1;
-      uint4 rv[NB][RV];
-      if (CENTER_REGS) {
-#pragma unroll
+    } else {
+      // center profile of the chunk's first needing item, kept in registers
+      uint32_t cur_c = 0xffffffffu;
+      uint4 cv[CENTER_REGS ? VPL : 1];
+      (void)cur_c;
+      while (todo) {
+        int js[NB];
+  #pragma unroll
         for (int q = 0; q < NB; ++q) {
-          if (js[q] >= 0) {
-            const uint4* pg = reinterpret_cast<const uint4*>(kmer8 + size_t(gq[q]) * size_t(NK16) * 16);
-#pragma unroll
-            for (int v = 0; v < RV; ++v) {
-              const int idx = lane + 32 * v;
-              rv[q][v] = idx < NK16 ? __ldcs(pg + idx) : make_uint4(0, 0, 0, 0);
+          js[q] = -1;
+          if (todo) {
+            js[q] = __ffs(todo) - 1;
+            todo &= todo - 1;
+          }
+        }
+        uint32_t gq[NB], cq[NB];
+  #pragma unroll
+        for (int q = 0; q < NB; ++q) {
+          const int src = js[q] < 0 ? 0 : js[q];
+          gq[q] = __shfl_sync(FULL, g, src);
+          cq[q] = __shfl_sync(FULL, c, src);
+        }
+        constexpr int RV = CENTER_REGS ? VPL : 1;
+        uint4 rv[NB][RV];
+        if (CENTER_REGS) {
+  #pragma unroll
+          for (int q = 0; q < NB; ++q) {
+            if (js[q] >= 0) {
+              const uint4* pg = reinterpret_cast<const uint4*>(kmer8 + size_t(gq[q]) * size_t(NK16) * 16);
+  #pragma unroll
+              for (int v = 0; v < RV; ++v) {
+                const int idx = lane + 32 * v;
+                rv[q][v] = idx < NK16 ? __ldcs(pg + idx) : make_uint4(0, 0, 0, 0);
+              }
             }
           }
         }
-      }
-#pragma unroll
-      for (int q = 0; q < NB; ++q) {
-        if (js[q] < 0) continue;
-        const uint4* pc = reinterpret_cast<const uint4*>(kmer8 + size_t(cq[q]) * size_t(NK16) * 16);
-        const uint4* pg = reinterpret_cast<const uint4*>(kmer8 + size_t(gq[q]) * size_t(NK16) * 16);
-        if (CENTER_REGS && cq[q] != cur_c) {
-#pragma unroll
+  #pragma unroll
+        for (int q = 0; q < NB; ++q) {
+          if (js[q] < 0) continue;
+          const uint4* pc = reinterpret_cast<const uint4*>(kmer8 + size_t(cq[q]) * size_t(NK16) * 16);
+          const uint4* pg = reinterpret_cast<const uint4*>(kmer8 + size_t(gq[q]) * size_t(NK16) * 16);
+          if (CENTER_REGS && cq[q] != cur_c) {
+  #pragma unroll
+            for (int v = 0; v < VPL; ++v) {
+              const int idx = lane + 32 * v;
+              cv[CENTER_REGS ? v : 0] = idx < NK16 ? __ldg(pc + idx) : make_uint4(0, 0, 0, 0);
+            }
+            cur_c = cq[q];
+          }
+          uint32_t dot = 0;
+  #pragma unroll 4
           for (int v = 0; v < VPL; ++v) {
             const int idx = lane + 32 * v;
-            cv[CENTER_REGS ? v : 0] = idx < NK16 ? __ldg(pc + idx) : make_uint4(0, 0, 0, 0);
+            const uint4 a = CENTER_REGS ? cv[CENTER_REGS ? v : 0] : (idx < NK16 ? __ldg(pc + idx) : make_uint4(0, 0, 0, 0));
+            const uint4 b2 = CENTER_REGS ? rv[q][CENTER_REGS ? v : 0] : (idx < NK16 ? __ldcs(pg + idx) : make_uint4(0, 0, 0, 0));
+            const uint32_t m0 = __vminu4(a.x, b2.x), m1 = __vminu4(a.y, b2.y), m2 = __vminu4(a.z, b2.z),
+                           m3 = __vminu4(a.w, b2.w);
+            dot = __dp4a(m0, 0x01010101u, dot);
+            dot = __dp4a(m1, 0x01010101u, dot);
+            dot = __dp4a(m2, 0x01010101u, dot);
+            dot = __dp4a(m3, 0x01010101u, dot);
           }
-          cur_c = cq[q];
+          dot = __reduce_add_sync(FULL, dot);
+          if (lane == js[q]) mydot = dot;
         }
-        uint32_t dot = 0;
-#pragma unroll 4
-        for (int v = 0; v < VPL; ++v) {
-          const int idx = lane + 32 * v;
-          const uint4 a = CENTER_REGS ? cv[CENTER_REGS ? v : 0] : (idx < NK16 ? __ldg(pc + idx) : make_uint4(0, 0, 0, 0));
-          const uint4 b2 = CENTER_REGS ? rv[q][CENTER_REGS ? v : 0] : (idx < NK16 ? __ldcs(pg + idx) : make_uint4(0, 0, 0, 0));
-          const uint32_t m0 = __vminu4(a.x, b2.x), m1 = __vminu4(a.y, b2.y), m2 = __vminu4(a.z, b2.z),
-                         m3 = __vminu4(a.w, b2.w);
-          dot = __dp4a(m0, 0x01010101u, dot);
-          dot = __dp4a(m1, 0x01010101u, dot);
-          dot = __dp4a(m2, 0x01010101u, dot);
-          dot = __dp4a(m3, 0x01010101u, dot);
-        }
-        dot = __reduce_add_sync(FULL, dot);
-        if (lane == js[q]) mydot = dot;
       }
     }
     // kmer_dist8 returns -1 (and the reference falls back to the exact u16
@@ -1999,7 +2118,8 @@ void launch_compare(const CompareLaunch& L, cudaStream_t st, cudaEvent_t* ev) {
     case 4: k_screen<4><<<blocks, kScreenWarps * 32, 0, st>>>(L); break;
     case 5: k_screen<5><<<blocks, kScreenWarps * 32, 0, st>>>(L); break;
     case 6: k_screen<6><<<blocks, kScreenWarps * 32, 0, st>>>(L); break;
-    default: k_screen<7><<<blocks, kScreenWarps * 32, 0, st>>>(L); break;
+    case 7: k_screen<7><<<blocks, kScreenWarps * 32, 0, st>>>(L); break;
+    default: k_screen<8><<<blocks, kScreenWarps * 32, 0, st>>>(L); break;
   }
   if (ev) cudaEventRecord(ev[1], st);
   const size_t asm_ = err_smem_bytes(L.kp.ncol) + size_t(kNwWarps) * align_smem_per_warp(L.geom);

@@ -185,19 +185,20 @@ def _extend(err, ncol, quals):
 
 
 @pytest.mark.parametrize("seed", [11, 12])
-def test_compare_many_centers_matches_oracle(seed):
+@pytest.mark.parametrize("k", [5, 8])  # k = 8: the sparse screen (src/kmers.rs:280-308)
+def test_compare_many_centers_matches_oracle(seed, k):
     w = synth.small_illumina(seed, nvariants=6, nreads=1500, L=120)
     s = w.samples[0]
     seqs = [O.encode(x) for x in s.seqs]
     quals = _rounded_quals(s)
     err, ncol = _extend(w.err, w.ncol, quals)
-    sess = O.Session(seqs, s.abund, quals=quals, k=5, use_quals=True)
-    with D.CompareContext(D.AlignParams(), err, ncol) as ctx:
+    sess = O.Session(seqs, s.abund, quals=quals, k=k, use_quals=True)
+    with D.CompareContext(D.AlignParams(kmer_size=k), err, ncol) as ctx:
         ctx.upload(seqs, s.abund, quals=quals)
         for center in (0, 1, 2, 5, len(seqs) // 2, len(seqs) - 1):
             ci = sess.add_center(center)
             for cutoff in (0.42, 1.0):
-                pa = O.AlignParams(kdist_cutoff=cutoff)
+                pa = O.AlignParams(kdist_cutoff=cutoff, kmer_size=k)
                 wl, wh, ws, wm = sess.compare_map(ci, err, ncol, pa, greedy=True)
                 gl, gh, gs, _ = ctx.compare(center, cutoff, greedy=True)
                 assert gl.tobytes() == wl.tobytes(), (center, cutoff)
@@ -263,7 +264,7 @@ def test_dada_homopolymer_long_reads_matches_oracle():
     assert_same_dada(got, want)
 
 
-@pytest.mark.parametrize("variant", ["band0", "no_kmers", "no_quals", "no_greedy", "unbanded"])
+@pytest.mark.parametrize("variant", ["band0", "no_kmers", "no_quals", "no_greedy", "unbanded", "kmer3", "kmer8"])
 def test_dada_parameter_variants_match_oracle(variant):
     w = synth.small_illumina(41, nvariants=5, nreads=1200, L=90)
     s = w.samples[0]
@@ -280,6 +281,10 @@ def test_dada_parameter_variants_match_oracle(variant):
         okw["greedy"] = dkw["greedy"] = False
     elif variant == "unbanded":
         oa.band = da.band = -1
+    elif variant == "kmer3":
+        oa.kmer_size = da.kmer_size = 3
+    elif variant == "kmer8":  # sparse screen (src/kmers.rs:213-221, 280-308)
+        oa.kmer_size = da.kmer_size = 8
     want = O.dada(s.seqs, s.abund, w.err, w.ncol, O.DadaParams(align=oa, nthreads=4, **okw), quals=quals)
     got = D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, D.DadaParams(align=da, **dkw), quals=quals)
     assert_same_dada(got, want)
@@ -346,7 +351,8 @@ def test_kernel_stats_count_launches():
     assert len(D.stats_latencies()) == st["rounds"]
 
 
-def test_saturated_kmers_take_the_exact_distance():
+@pytest.mark.parametrize("k", [5, 8])
+def test_saturated_kmers_take_the_exact_distance(k):
     """Profiles with a k-mer counted >= 255 in both sequences (src/nwalign.rs:1270-1277)."""
     rng = np.random.default_rng(5)
     seqs, reads = [], []
@@ -359,9 +365,9 @@ def test_saturated_kmers_take_the_exact_distance():
         seqs.append(s)
         reads.append(50 - 3 * t)
     err = np.full(16 * 41, 0.01)
-    op = O.AlignParams(kdist_cutoff=0.42)
-    sess = O.Session(seqs, reads, k=5, use_quals=False)
-    with D.CompareContext(D.AlignParams(), err, 41, use_quals=False) as ctx:
+    op = O.AlignParams(kdist_cutoff=0.42, kmer_size=k)
+    sess = O.Session(seqs, reads, k=k, use_quals=False)
+    with D.CompareContext(D.AlignParams(kmer_size=k), err, 41, use_quals=False) as ctx:
         ctx.upload(seqs, reads)
         for center in (0, 3, 7):
             ci = sess.add_center(center)
