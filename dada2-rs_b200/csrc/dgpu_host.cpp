@@ -826,6 +826,8 @@ struct RunStats {
   uint64_t gapless = 0, vectorized = 0, homo = 0, endsfree = 0, shuffle_calls = 0, shuffle_moves = 0;
   double t_compare = 0, t_total = 0, t_host = 0, t_wait = 0;
   double t_done = -1;  // from the start of the loop until this sample finished
+  double t_slot_wait = 0, t_job_wait = 0;  // ready -> launched; results -> host phase started
+  Clock::time_point t_mark{};              // when the sample last became ready / got its results
   uint64_t ns_shuffle = 0, ns_pupdate = 0, ns_bud = 0;  // host phases, nanoseconds
 };
 
@@ -1749,7 +1751,7 @@ struct dgpu_result {
   std::vector<double> cl_birth_pval, cl_birth_fold, cl_birth_e, mem_lambda, mem_pval, pvals;
   std::vector<uint8_t> cl_seq;
   uint64_t counters[16] = {0};
-  double times[4] = {0};
+  double times[6] = {0};
 };
 
 namespace dgpu {
@@ -1824,6 +1826,8 @@ static dgpu_result* finish(SampleState& S, const SampleSeqs& in) {
   R->times[1] = st.t_total;
   R->times[2] = st.t_host;
   R->times[3] = st.t_wait;
+  R->times[4] = st.t_slot_wait;
+  R->times[5] = st.t_job_wait;
   return R;
 }
 
@@ -1834,14 +1838,18 @@ static dgpu_result* finish(SampleState& S, const SampleSeqs& in) {
 // queue; with several slots a sample that becomes ready while a launch is in
 // flight goes out at once on another slot. A sample's own sequence of steps is
 // exactly run_dada's.
+static size_t batch_max_samples();
+
 static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_params& ap, int host_threads) {
   const size_t ns = S.size();
+  const size_t batch_max = batch_max_samples();
   std::mutex mu;
   std::condition_variable cv;
   std::vector<size_t> ready;
   size_t finished = 0;
   for (size_t s = 0; s < ns; ++s) {
     S[s].pending = 0;  // cluster 0 first, with the screen off
+    S[s].stats.t_mark = Clock::now();
     ready.push_back(s);
   }
   double wait = 0.0;
@@ -1869,9 +1877,21 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
           std::unique_lock<std::mutex> lk(mu);
           cv.wait(lk, [&] { return !ready.empty() || finished == ns || rc != 0; });
           if (ready.empty() || rc != 0) break;
-          batch.swap(ready);
+          if (ready.size() <= batch_max) {
+            batch.swap(ready);
+          } else {
+            // the largest samples (the longest chains) go first
+            std::stable_sort(ready.begin(), ready.end(), [&](size_t x, size_t y) { return S[x].n > S[y].n; });
+            batch.assign(ready.begin(), ready.begin() + batch_max);
+            ready.erase(ready.begin(), ready.begin() + batch_max);
+            if (!ready.empty()) cv.notify_one();
+          }
         }
         std::sort(batch.begin(), batch.end());
+        {
+          const auto now = Clock::now();
+          for (size_t sidx : batch) S[sidx].stats.t_slot_wait += secs(S[sidx].stats.t_mark, now);
+        }
         int r = L.ensure_tasks(uint32_t(batch.size()));
         for (size_t a = 0; a < batch.size() && !r; ++a) {
           SampleState& ss = S[batch[a]];
@@ -1894,22 +1914,28 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
           break;
         }
         const double tcmp = secs(tc, Clock::now());
-        for (size_t a = 0; a < batch.size(); ++a) {
-          SampleState& ss = S[batch[a]];
-          ss.absorb(size_t(ss.pending), L, uint32_t(a));
-          ss.stats.t_compare += tcmp;
-        }
-        for (size_t a = 0; a < batch.size(); ++a) {
+        // each sample's host phase is queued as soon as its own results are
+        // absorbed, the largest samples (the longest chains) first
+        std::vector<uint32_t> order(batch.size());
+        for (size_t a = 0; a < batch.size(); ++a) order[a] = uint32_t(a);
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return S[batch[x]].n > S[batch[y]].n; });
+        for (uint32_t a : order) {
           const size_t sidx = batch[a];
+          SampleState& sa = S[sidx];
+          sa.absorb(size_t(sa.pending), L, a);
+          sa.stats.t_compare += tcmp;
+          sa.stats.t_mark = Clock::now();
           jobs.submit([&, sidx] {
             SampleState& ss = S[sidx];
             auto th = Clock::now();
+            ss.stats.t_job_wait += secs(ss.stats.t_mark, th);
             ss.pending = ss.advance(size_t(ss.pending));
             const double dh = secs(th, Clock::now());
             ss.stats.t_host += dh;
             host_ns += int64_t(1e9 * dh);
             std::lock_guard<std::mutex> g(mu);
             if (ss.pending >= 0) {
+              ss.stats.t_mark = Clock::now();
               ready.push_back(sidx);
             } else {
               ++finished;
@@ -1935,6 +1961,17 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
   }
   if (rc) return fail(rc, err_msg);
   return 0;
+}
+
+// Most samples one compare launch covers: DGPU_BATCH_MAX (1..4096) if set,
+// else 4. Small launches finish sooner, and the largest ready samples (the
+// longest chains of dependent rounds) are served first.
+static size_t batch_max_samples() {
+  if (const char* e = std::getenv("DGPU_BATCH_MAX")) {
+    const long v = std::atol(e);
+    if (v >= 1 && v <= 4096) return size_t(v);
+  }
+  return 4;
 }
 
 // Launch slots for a batch of nsamples: DGPU_LAUNCH_SLOTS (1..8) if set, else

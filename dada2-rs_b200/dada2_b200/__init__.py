@@ -189,7 +189,7 @@ def _read_result(h) -> dict:
         "mem_raw": np.zeros(max(nmem, 1), np.uint32), "mem_hamming": np.zeros(max(nmem, 1), np.uint32),
         "mem_lambda": np.zeros(max(nmem, 1), np.float64), "mem_pval": np.zeros(max(nmem, 1), np.float64),
         "map": np.zeros(max(nraw, 1), np.int32), "pvals": np.zeros(max(nraw, 1), np.float64),
-        "counters": np.zeros(16, np.uint64), "times": np.zeros(4, np.float64),
+        "counters": np.zeros(16, np.uint64), "times": np.zeros(6, np.float64),
     }
     o = DadaOutC(*[ptr(a[n]) for n, _ in DadaOutC._fields_])
     check(lib().dgpu_result_fill(h, C.byref(o)))
@@ -349,7 +349,7 @@ class ResidentBatch:
 
 def _read_counters(h) -> dict:
     cnt = np.zeros(16, np.uint64)
-    tm = np.zeros(4, np.float64)
+    tm = np.zeros(6, np.float64)
     o = DadaOutC(*[None] * len(DadaOutC._fields_))
     o.counters = ptr(cnt)
     o.times = ptr(tm)

@@ -75,10 +75,12 @@ typedef struct {
  * nalign, compare_calls, cmp_scanned (sum of nraw over compare calls),
  * screened, aligned, stored, gapless, vectorized, homo, endsfree,
  * shuffle_calls, shuffle_moves, nshroud, then the nanoseconds this sample's
- * host spent in shuffle, p-update and bud. times (4 slots, seconds): this
+ * host spent in shuffle, p-update and bud. times (6 slots, seconds): this
  * sample's compare calls (launch to results), the time from the start of the
  * clustering loop until this sample finished, this sample's host phases
- * (shuffle, p-update, bud), time the host waited on the device. */
+ * (shuffle, p-update, bud), time the host waited on the device, time this
+ * sample waited for a launch slot (ready to launched) and for a host thread
+ * (results absorbed to host phase started). */
 typedef struct {
   uint32_t* cl_reads;
   int32_t* cl_birth_type;
