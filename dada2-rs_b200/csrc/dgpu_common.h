@@ -159,6 +159,25 @@ struct CompareLaunch {
 // and store, for per-kernel device times.
 void launch_compare(const CompareLaunch& L, cudaStream_t st, cudaEvent_t* ev = nullptr);
 
+// Final-subs pass (src/dada.rs:609-673) feeding the transition counts
+// (src/error.rs:194-249): item i realigns raw[i] against center[i]; counts go
+// to out + sample[i] * 16 * tncol. Items are ordered by sample.
+struct FinalSubsLaunch {
+  PoolDev pool;
+  KParams kp;  // the run's parameters with use_kmers = 0
+  NwGeom geom;
+  uint8_t* nw_scratch;
+  const uint32_t* raw;
+  const uint32_t* center;
+  const uint32_t* sample;
+  uint32_t nitems;
+  int tncol;      // columns counted (the error matrix's, or 1 without qualities)
+  int has_quals;  // count at the raw's quality (else column 0)
+  uint32_t* out;
+  uint32_t* err_word;
+};
+void launch_final_subs(const FinalSubsLaunch& F, cudaStream_t st);
+
 // Alignment-only entry used by the parity tests: emits al0/al1 strings.
 void launch_align_debug(int which, const uint8_t* s1cat, const uint32_t* off1, const uint32_t* len1,
                         const uint8_t* s2cat, const uint32_t* off2, const uint32_t* len2, uint32_t npairs,

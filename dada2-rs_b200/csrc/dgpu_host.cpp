@@ -1578,6 +1578,7 @@ struct EncodedView {
   uint8_t* qual = nullptr;  // null when the input has no qualities
   std::vector<uint32_t> off, len, reads;
   std::vector<uint8_t> prior;
+  std::vector<uint32_t> uqmax;  // per unique: its largest round(sum / max(reads, 1))
   uint32_t qmax = 0;
 };
 
@@ -1636,6 +1637,7 @@ static void encode_uniques(uint32_t t0, uint32_t t1, const char* seqs, const uin
   E.len.resize(n);
   E.reads.resize(n);
   E.prior.assign(n, 0);
+  E.uqmax.assign(n, 0);
   uint64_t w = 0;
   for (uint32_t r = 0; r < n; ++r) {
     E.off[r] = uint32_t(w);
@@ -1680,12 +1682,15 @@ static void encode_uniques(uint32_t t0, uint32_t t1, const char* seqs, const uin
           const double cq = double(std::max<uint32_t>(abund[t], 1));
           const uint32_t* qs = qsums + offs[t];
           uint8_t* qo = E.qual + E.off[r];
+          uint32_t qm_u = 0;
           for (uint32_t p = 0; p < lens[t]; ++p) {
             const double q = std::round(double(qs[p]) / cnt);
             qo[p] = q >= 255.0 ? 255 : (q > 0.0 ? uint8_t(q) : 0);
             const double qm = std::round(double(qs[p]) / cq);
-            qm_max = std::max<uint32_t>(qm_max, qm > 0 ? uint32_t(qm) : 0);
+            qm_u = std::max<uint32_t>(qm_u, qm > 0 ? uint32_t(qm) : 0);
           }
+          E.uqmax[r] = qm_u;
+          qm_max = std::max(qm_max, qm_u);
         }
       }
       ch_qmax[c] = qm_max;
@@ -1752,6 +1757,8 @@ struct dgpu_result {
   std::vector<uint8_t> cl_seq;
   uint64_t counters[16] = {0};
   double times[6] = {0};
+  std::vector<uint32_t> transitions;  // 16 x tncol when requested
+  int tncol = 0;
 };
 
 namespace dgpu {
@@ -1995,6 +2002,8 @@ struct Batch {
   std::vector<DadaConf> confs;
   dgpu_align_params align{};
   int host_threads = 1;
+  bool transitions = false;  // run the final-subs pass after the loop
+  int ncol_in = 0;           // the caller's error-matrix width (before extension)
   ~Batch() {  // Pool::upload waited for its copies, so the staging blocks are idle
     seq_h.recycle();
     qual_h.recycle();
@@ -2060,12 +2069,91 @@ static int batch_prepare(Batch& B, int device, const dgpu_dada_params* prm, int 
   for (int s = 0; s < nsamples; ++s)
     B.confs[size_t(s)].max_clust = prm->max_clust == 0 ? B.counts[size_t(s)] : size_t(prm->max_clust);
   B.align = prm->align;
+  B.transitions = prm->transitions != 0;
+  B.ncol_in = ncol;
   // Host phases of different samples share the cores with the intra-sample
   // helpers (half the cores) and the launch workers, so by default they get
   // the other half.
   int threads = prm->host_threads;
   if (threads <= 0) threads = int(std::max(1u, std::thread::hardware_concurrency() / 2));
   B.host_threads = std::min(threads, nsamples);
+  return 0;
+}
+
+// The final-subs pass and transition counts of every sample (DadaAux.transitions,
+// src/dada.rs:609-673, src/error.rs:194-249): each correct member (map != -1,
+// centers included) realigned against its cluster's center with the k-mer
+// screen off, on the device; counts land in each sample's result with the
+// sample's own error-matrix width (extended to its qmax + 1 when that is
+// larger), or one column without qualities.
+static int final_subs(Batch& B, std::vector<SampleState>& S, dgpu_result** out) {
+  Pool& P = B.pool;
+  const size_t ns = B.counts.size();
+  std::vector<uint32_t> raw, center, sample;
+  for (size_t s = 0; s < ns; ++s) {
+    const dgpu_result* R = out[s];
+    for (const Cluster& c : S[s].clusters) {
+      if (c.center < 0) continue;
+      for (uint32_t r : c.raws) {
+        if (R->map[r] < 0) continue;
+        raw.push_back(B.bases[s] + r);
+        center.push_back(B.bases[s] + uint32_t(c.center));
+        sample.push_back(uint32_t(s));
+      }
+    }
+  }
+  const bool has_q = B.E.qual != nullptr;
+  const int tncol = has_q ? P.kp.ncol : 1;
+  const size_t nbins = size_t(16) * size_t(tncol);
+  const uint32_t nitems = uint32_t(raw.size());
+  DBuf<uint32_t> items, counts, err;
+  TRY(items.alloc(size_t(3) * std::max<uint32_t>(nitems, 1)));
+  TRY(counts.alloc(ns * nbins));
+  TRY(err.alloc(1));
+  CUDA_TRY(cudaMemcpyAsync(items.p, raw.data(), size_t(4) * nitems, cudaMemcpyHostToDevice, P.st));
+  CUDA_TRY(cudaMemcpyAsync(items.p + nitems, center.data(), size_t(4) * nitems, cudaMemcpyHostToDevice, P.st));
+  CUDA_TRY(cudaMemcpyAsync(items.p + 2 * size_t(nitems), sample.data(), size_t(4) * nitems, cudaMemcpyHostToDevice,
+                           P.st));
+  count_h2d(uint64_t(12) * nitems);
+  CUDA_TRY(cudaMemsetAsync(counts.p, 0, ns * nbins * 4, P.st));
+  CUDA_TRY(cudaMemsetAsync(err.p, 0, 4, P.st));
+  FinalSubsLaunch F{};
+  F.pool = P.view();
+  F.kp = P.kp;
+  F.kp.use_kmers = 0;  // src/dada.rs:611-615: no k-mer screen, cutoff 1.0
+  F.geom = P.geom;
+  F.nw_scratch = P.slot0().scratch.p;
+  F.raw = items.p;
+  F.center = items.p + nitems;
+  F.sample = items.p + 2 * size_t(nitems);
+  F.nitems = nitems;
+  F.tncol = tncol;
+  F.has_quals = has_q ? 1 : 0;
+  F.out = counts.p;
+  F.err_word = err.p;
+  launch_final_subs(F, P.st);
+  CUDA_TRY(cudaGetLastError());
+  std::vector<uint32_t> host(ns * nbins);
+  uint32_t ew = 0;
+  CUDA_TRY(cudaMemcpyAsync(host.data(), counts.p, host.size() * 4, cudaMemcpyDeviceToHost, P.st));
+  CUDA_TRY(cudaMemcpyAsync(&ew, err.p, 4, cudaMemcpyDeviceToHost, P.st));
+  CUDA_TRY(cudaStreamSynchronize(P.st));
+  recycle_all(items, counts, err);
+  if (ew) return fail(ew & DERR_UNSUPPORTED ? DGPU_E_UNSUPPORTED : DGPU_E_DEVICE, "device error in the final-subs pass");
+  for (size_t s = 0; s < ns; ++s) {
+    int nc = 1;
+    if (has_q) {
+      uint32_t qm = 0;
+      for (uint32_t r = 0; r < B.counts[s]; ++r) qm = std::max(qm, B.E.uqmax[B.bases[s] + r]);
+      nc = int64_t(qm) >= B.ncol_in ? int(qm) + 1 : B.ncol_in;  // src/dada.rs:337-384, per sample
+    }
+    dgpu_result* R = out[s];
+    R->tncol = nc;
+    R->transitions.assign(size_t(16) * nc, 0u);
+    for (int t = 0; t < 16; ++t)
+      for (int q = 0; q < nc && q < tncol; ++q)
+        R->transitions[size_t(t) * nc + q] = host[s * nbins + size_t(t) * tncol + q];
+  }
   return 0;
 }
 
@@ -2093,6 +2181,7 @@ static int batch_run(Batch& B, dgpu_result** out) {
   for (size_t t = 1; t < nt; ++t) th.emplace_back(work);
   work();
   for (auto& t : th) t.join();
+  if (B.transitions) TRY(final_subs(B, S, out));
   return 0;
 }
 
@@ -2354,6 +2443,13 @@ int dgpu_result_sizes(const dgpu_result* r, int64_t* sizes) {
   sizes[2] = int64_t(r->mem_raw.size());
   sizes[3] = int64_t(r->cl_seq.size());
   return 0;
+}
+
+int dgpu_result_transitions(const dgpu_result* r, uint32_t* out) {
+  if (!r) return fail(DGPU_E_INVALID, "null argument");
+  if (out && !r->transitions.empty())
+    std::memcpy(out, r->transitions.data(), r->transitions.size() * sizeof(uint32_t));
+  return r->tncol;
 }
 
 int dgpu_result_fill(const dgpu_result* r, const dgpu_dada_out* o) {

@@ -201,6 +201,12 @@ void launch_fill_f64(double* p, size_t n, double v, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 // Shared helpers for the lambda product
 // ---------------------------------------------------------------------------
+// tcode[p]: the error-matrix row of raw position p -- 4 * (center nt) + raw nt
+// where the traceback aligned p to a center base, else kUnaligned | 5 * (raw nt)
+// (an insertion in the raw, weighed as a match by compute_lambda and left out
+// of the transition counts).
+constexpr unsigned kUnaligned = 0x80u;
+
 // fidx[p] = err row * ncol + quality column for raw position p; lane 0 then forms
 // the left-to-right product (src/pval.rs:311-313). Returns the product on all lanes.
 __device__ double lambda_chain(int lane, const uint16_t* fidx, int L, const double* err_s) {
@@ -224,7 +230,7 @@ __device__ bool build_fidx(int lane, const uint8_t* tcode, const uint8_t* qual_g
                            uint16_t* fidx) {
   bool bad = false;
   for (int p = lane; p < L; p += 32) {
-    unsigned t = tcode[p];
+    unsigned t = tcode[p] & 0x7fu;  // insertions in the raw weigh as matches (src/pval.rs:269-291)
     bad |= t > 15u;
     unsigned q = (use_quals && qual_g) ? qual_g[p] : 0u;
     bad |= q >= unsigned(ncol);
@@ -689,7 +695,7 @@ __device__ bool vec_align_warp(int lane, const uint8_t* g1, int l1, const uint8_
   // Traceback (src/nwalign.rs:1090-1139), staged through shared memory in row chunks.
   const uint8_t* raw = swap ? S.s1 : S.s2;
   const int lraw = swap ? len1 : len2;
-  for (int p = lane; p < lraw; p += 32) S.tcode[p] = uint8_t((unsigned(raw[p]) - 1u) * 5u);
+  for (int p = lane; p < lraw; p += 32) S.tcode[p] = uint8_t(kUnaligned | ((unsigned(raw[p]) - 1u) * 5u));
   const int rps = kStageBytes / ncol;
   int slo = 0x7fffffff;
   int i = len1, j = len2;
@@ -812,7 +818,7 @@ __device__ bool reg_traceback(int lane, bool swap, int len1, int len2, int start
   // is taken at once, each lane doing one. A gap step is taken singly.
   const uint8_t* raw = swap ? S.s1 : S.s2;
   const int lraw = swap ? len1 : len2;
-  for (int p = lane; p < lraw; p += 32) S.tcode[p] = uint8_t((unsigned(raw[p]) - 1u) * 5u);
+  for (int p = lane; p < lraw; p += 32) S.tcode[p] = uint8_t(kUnaligned | ((unsigned(raw[p]) - 1u) * 5u));
   uint32_t* stage = reinterpret_cast<uint32_t*>(S.stage);
   int slo = planes_smem ? 0 : 0x7fffffff;  // planes already in shared memory: no staging
   int i = len1, j = len2;
@@ -1763,7 +1769,7 @@ __device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8
   }
   __syncwarp();
   // Traceback (src/nwalign.rs:234-273): row 0 moves left, column 0 moves up.
-  for (int p = lane; p < len2; p += 32) S.tcode[p] = uint8_t((unsigned(S.s2[p]) - 1u) * 5u);
+  for (int p = lane; p < len2; p += 32) S.tcode[p] = uint8_t(kUnaligned | ((unsigned(S.s2[p]) - 1u) * 5u));
   int i = len1, j = len2, slo = 0x7fffffff;
   uint32_t ham = 0, alen = 0;
   bool ok = true;
@@ -1865,6 +1871,95 @@ __device__ bool rm_dispatch(int lane, const uint8_t* g1, int len1, const uint8_t
   return false;
 }
 
+// One pair (center c, raw g) through method selection (src/nwalign.rs:1315-1414)
+// and the chosen aligner. Both sequences (shorter first, as the vectorized
+// aligner wants them) and, with `want_qual`, the raw's qualities are staged in
+// the warp's shared memory in one round trip; the steps read them there. On
+// return tcode[p] holds each raw position's error-matrix row (see kUnaligned)
+// and qual the raw's qualities (staged copy, or the pool's, or null).
+struct PairResult {
+  bool ok;
+  uint8_t method;
+  uint32_t ham;
+  int lg;
+  const uint8_t* tcode;
+  uint16_t* fidx;
+  const uint8_t* qual;
+};
+
+__device__ __forceinline__ PairResult align_pair(int lane, const KParams& kp, const PoolDev& pool, const NwGeom& geom,
+                                                 uint32_t g, uint32_t c, double kdist, bool want_qual,
+                                                 const VecSmem& VS, const RmSmem& RS, int kb, uint8_t* scratch,
+                                                 uint32_t* err_word) {
+  const int k = kp.kmer_size;
+  const int lc = int(pool.len[c]), lg = int(pool.len[g]);
+  const uint8_t* sc = pool.seq + pool.off[c];
+  const uint8_t* sg = pool.seq + pool.off[g];
+  const uint8_t* qg = pool.qual ? pool.qual + pool.off[g] : nullptr;
+  const bool use_homo = kp.homo_gap != kp.gap && kp.homo_gap <= 0;
+  const bool rm = use_homo || !kp.vectorized || lc > 3500 || lg > 3500;
+  if (!rm) {
+    const bool swap = lc > lg;
+    uint8_t* dc = swap ? VS.s2 : VS.s1;
+    uint8_t* dg = swap ? VS.s1 : VS.s2;
+    uint8_t* dq = vec_qual(VS, geom.lmax);
+    const bool stage_q = want_qual && qg != nullptr;
+    stage3(lane, sc, lc, dc, sg, lg, dg, stage_q ? qg : nullptr, dq);
+    __syncwarp();
+    sc = dc;
+    sg = dg;
+    if (stage_q) qg = dq;
+  }
+  double kodist = -1.0;
+  const int minl = lc < lg ? lc : lg;
+  const bool want_kod = kp.use_kmers && kp.gapless && lc == lg;
+  PairResult R{true, AM_NONE, 0u, lg, VS.tcode, VS.fidx, qg};
+  uint32_t ham = 0;
+  if (want_kod || kp.band == 0) {
+    const int klen = lc - (k - 1);
+    const uint32_t kmask = (k >= 32) ? 0xffffffffu : ((1u << k) - 1u);
+    uint32_t eq = 0;
+    uint32_t cur = mismatch_word(sc, sg, 0, minl, lane);
+    for (int b = 0; b < minl; b += 32) {
+      const uint32_t nxt = mismatch_word(sc, sg, b + 32, minl, lane);
+      ham += __popc(cur);
+      if (want_kod) {
+        const unsigned long long both = (static_cast<unsigned long long>(nxt) << 32) | cur;
+        const int j = b + lane;
+        const bool ok = j < klen && ((uint32_t(both >> lane) & kmask) == 0u);
+        eq += __popc(__ballot_sync(FULL, ok));
+      }
+      cur = nxt;
+    }
+    if (want_kod && klen > 0) kodist = 1.0 - double(eq) / double(klen);
+  }
+  const bool gapless = kp.band == 0 || (kp.gapless && fabs(kodist - kdist) < DBL_EPSILON);
+  if (gapless) {
+    // raw position p aligns to center position p while p < len(center)
+    uint8_t* tcode = VS.tcode;
+    for (int p = lane; p < lg; p += 32) {
+      const unsigned r = sg[p];
+      const unsigned code = (p < lc) ? (unsigned(sc[p]) - 1u) * 4u + (r - 1u) : (kUnaligned | ((r - 1u) * 5u));
+      const bool valid = r >= 1u && r <= 4u && (p >= lc || (sc[p] >= 1 && sc[p] <= 4));
+      tcode[p] = uint8_t(valid ? code : 255u);
+    }
+    R.method = AM_GAPLESS;
+  } else if (!rm) {
+    R.ok = vec_align_any(lane, sc, lc, sg, lg, int16_t(kp.match), int16_t(kp.mismatch), int16_t(kp.gap), 0, kp.band,
+                         VS, scratch, geom.vec_ncol, geom.vec_nrow, &ham, err_word, nullptr, nullptr, nullptr, true);
+    R.method = AM_VECTORIZED;
+  } else {
+    R.ok = rm_dispatch(lane, sc, lc, sg, lg, kp, use_homo, kb, RS, reinterpret_cast<uint32_t*>(scratch), &ham,
+                       err_word, nullptr, nullptr, nullptr);
+    R.tcode = RS.tcode;
+    R.fidx = RS.fidx;
+    R.method = use_homo ? AM_HOMO : AM_ENDSFREE;
+  }
+  R.ham = ham;
+  __syncwarp();
+  return R;
+}
+
 // ---------------------------------------------------------------------------
 // Pairs that passed the screen (one warp per pair, grid-stride over the queue):
 // ordered-k-mer distance (src/kmers.rs:314-328; equal windows <=> equal k-mer
@@ -1889,104 +1984,100 @@ __global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_align(Compar
   const size_t scr_stride = L.geom.vec_scratch > L.geom.rm_scratch ? L.geom.vec_scratch : L.geom.rm_scratch;
   uint8_t* scratch = L.nw_scratch + size_t(gw) * scr_stride;
   __syncthreads();
-  const int k = kp.kmer_size;
   const uint32_t warps_total = gridDim.x * kNwWarps;
   for (uint32_t slot = uint32_t(gw); slot < count; slot += warps_total) {
     const uint32_t item = L.queue_pass[slot];
     const uint32_t t = find_task(L.task_prefix, L.ntask, item);
     const TaskDev T = L.tasks[t];
     const uint32_t g = T.base + (item - L.task_prefix[t]);
-    const uint32_t c = T.center;
-    const int lc = int(L.pool.len[c]), lg = int(L.pool.len[g]);
-    const uint8_t* sc = L.pool.seq + L.pool.off[c];
-    const uint8_t* sg = L.pool.seq + L.pool.off[g];
-    const uint8_t* qg = L.pool.qual ? L.pool.qual + L.pool.off[g] : nullptr;
-    const double kdist = L.pool.res_lambda[g];
-    const bool use_homo = kp.homo_gap != kp.gap && kp.homo_gap <= 0;
-    const bool rm = use_homo || !kp.vectorized || lc > 3500 || lg > 3500;
-    if (!rm) {
-      // both sequences (shorter first, as the vectorized aligner wants them)
-      // and the raw's qualities go to shared memory in one round trip; the
-      // steps below read them there
-      const bool swap = lc > lg;
-      uint8_t* dc = swap ? VS.s2 : VS.s1;
-      uint8_t* dg = swap ? VS.s1 : VS.s2;
-      uint8_t* dq = vec_qual(VS, L.geom.lmax);
-      const bool stage_q = kp.use_quals && qg != nullptr;
-      stage3(lane, sc, lc, dc, sg, lg, dg, stage_q ? qg : nullptr, dq);
-      __syncwarp();
-      sc = dc;
-      sg = dg;
-      if (stage_q) qg = dq;
-    }
-    double kodist = -1.0;
-    const int minl = lc < lg ? lc : lg;
-    const bool want_kod = kp.use_kmers && kp.gapless && lc == lg;
-    uint32_t ham = 0;
-    if (want_kod || kp.band == 0) {
-      const int klen = lc - (k - 1);
-      const uint32_t kmask = (k >= 32) ? 0xffffffffu : ((1u << k) - 1u);
-      uint32_t eq = 0;
-      uint32_t cur = mismatch_word(sc, sg, 0, minl, lane);
-      for (int b = 0; b < minl; b += 32) {
-        const uint32_t nxt = mismatch_word(sc, sg, b + 32, minl, lane);
-        ham += __popc(cur);
-        if (want_kod) {
-          const unsigned long long both = (static_cast<unsigned long long>(nxt) << 32) | cur;
-          const int j = b + lane;
-          const bool ok = j < klen && ((uint32_t(both >> lane) & kmask) == 0u);
-          eq += __popc(__ballot_sync(FULL, ok));
-        }
-        cur = nxt;
-      }
-      if (want_kod && klen > 0) kodist = 1.0 - double(eq) / double(klen);
-    }
-    const bool gapless = kp.band == 0 || (kp.gapless && fabs(kodist - kdist) < DBL_EPSILON);
-    bool ok = true;
-    uint8_t method;
-    uint8_t* tcode = VS.tcode;
-    uint16_t* fidx = VS.fidx;
-    if (gapless) {
-      // raw position p aligns to center position p while p < len(center)
-      for (int p = lane; p < lg; p += 32) {
-        const unsigned r = sg[p];
-        const unsigned code = (p < lc) ? (unsigned(sc[p]) - 1u) * 4u + (r - 1u) : (r - 1u) * 5u;
-        const bool valid = r >= 1u && r <= 4u && (p >= lc || (sc[p] >= 1 && sc[p] <= 4));
-        tcode[p] = uint8_t(valid ? code : 255u);
-      }
-      method = AM_GAPLESS;
-    } else {
-      if (!rm) {
-        ok = vec_align_any(lane, sc, lc, sg, lg, int16_t(kp.match), int16_t(kp.mismatch), int16_t(kp.gap), 0,
-                           kp.band, VS, scratch, L.geom.vec_ncol, L.geom.vec_nrow, &ham, L.err_word, nullptr,
-                           nullptr, nullptr, true);
-        method = AM_VECTORIZED;
-      } else {
-        ok = rm_dispatch(lane, sc, lc, sg, lg, kp, use_homo, kb, RS, reinterpret_cast<uint32_t*>(scratch), &ham,
-                         L.err_word, nullptr, nullptr, nullptr);
-        tcode = RS.tcode;
-        fidx = RS.fidx;
-        method = use_homo ? AM_HOMO : AM_ENDSFREE;
-      }
-    }
-    __syncwarp();
+    const PairResult R = align_pair(lane, kp, L.pool, L.geom, g, T.center, L.pool.res_lambda[g], kp.use_quals != 0, VS,
+                                    RS, kb, scratch, L.err_word);
     double lam = 0.0;
-    if (ok) {
-      const bool bad = build_fidx(lane, tcode, qg, lg, kp.ncol, kp.use_quals, fidx);
+    if (R.ok) {
+      const bool bad = build_fidx(lane, R.tcode, R.qual, R.lg, kp.ncol, kp.use_quals, R.fidx);
       __syncwarp();
       if (bad) {
         if (lane == 0) atomicOr(L.err_word, DERR_LAMBDA);
       } else {
-        lam = lambda_chain(lane, fidx, lg, err_s);
+        lam = lambda_chain(lane, R.fidx, R.lg, err_s);
       }
     }
     if (lane == 0) {
       L.pool.res_lambda[g] = lam;
-      L.pool.res_ham[g] = ok ? ham : 0xffffffffu;
-      L.pool.res_status[g] = uint8_t(ST_ALIGNED | (method << 2));
+      L.pool.res_ham[g] = R.ok ? R.ham : 0xffffffffu;
+      L.pool.res_status[g] = uint8_t(ST_ALIGNED | (R.method << 2));
     }
     __syncwarp();
   }
+}
+
+// ---------------------------------------------------------------------------
+// Final-subs pass and transition counts (src/dada.rs:609-673, src/error.rs:194-249)
+// ---------------------------------------------------------------------------
+// Every correct raw realigned against its cluster's center with the k-mer
+// screen off; each raw position the traceback aligned to a center base adds
+// the raw's reads at (4 * center nt + raw nt, the raw's quality there) of its
+// sample's 16 x tncol matrix. Warps take contiguous runs of items (ordered by
+// sample), count in a shared-memory histogram and flush it to the sample's
+// matrix when the sample changes and at the end.
+__global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_final_subs(FinalSubsLaunch F) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const KParams& kp = F.kp;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t gw = blockIdx.x * kNwWarps + wib;
+  const uint32_t nwarps = gridDim.x * kNwWarps;
+  const int kb = rm_kbound(F.geom.rm_pairs);
+  const size_t per_warp = align_smem_per_warp(F.geom) + align16(size_t(16) * F.tncol * 4);
+  unsigned char* wbase = smem_raw + size_t(wib) * per_warp;
+  const VecSmem VS = carve_vec(wbase, F.geom.lmax, F.geom.vec_ncol);
+  const RmSmem RS = carve_rm(wbase, F.geom.lmax, kb);
+  uint32_t* hist = reinterpret_cast<uint32_t*>(wbase + align_smem_per_warp(F.geom));
+  const int nbins = 16 * F.tncol;
+  const size_t scr_stride = F.geom.vec_scratch > F.geom.rm_scratch ? F.geom.vec_scratch : F.geom.rm_scratch;
+  uint8_t* scratch = F.nw_scratch + size_t(gw) * scr_stride;
+  for (int b = lane; b < nbins; b += 32) hist[b] = 0;
+  __syncwarp();
+  const uint32_t per = (F.nitems + nwarps - 1) / nwarps;
+  const uint32_t i0 = gw * per, i1 = min(F.nitems, i0 + per);
+  uint32_t cur_s = 0xffffffffu;
+  auto flush = [&]() {
+    __syncwarp();
+    if (cur_s != 0xffffffffu) {
+      uint32_t* dst = F.out + size_t(cur_s) * nbins;
+      for (int b = lane; b < nbins; b += 32) {
+        const uint32_t v = hist[b];
+        if (v) atomicAdd(dst + b, v);
+        hist[b] = 0;
+      }
+    }
+    __syncwarp();
+  };
+  for (uint32_t i = i0; i < i1; ++i) {
+    const uint32_t g = F.raw[i], c = F.center[i], smp = F.sample[i];
+    if (smp != cur_s) {
+      flush();
+      cur_s = smp;
+    }
+    const PairResult R = align_pair(lane, kp, F.pool, F.geom, g, c, 0.0, F.has_quals != 0, VS, RS, kb, scratch,
+                                    F.err_word);
+    if (!R.ok) continue;  // the error word reports it
+    const uint32_t reads = F.pool.reads[g];
+    for (int p = lane; p < R.lg; p += 32) {
+      const unsigned t = R.tcode[p];
+      if (t > 15u) continue;  // an insertion in the raw (or an invalid code)
+      const unsigned q = (F.has_quals && R.qual) ? R.qual[p] : 0u;
+      if (q < unsigned(F.tncol)) atomicAdd(&hist[t * F.tncol + q], reads);
+    }
+    __syncwarp();
+  }
+  flush();
+}
+
+void launch_final_subs(const FinalSubsLaunch& F, cudaStream_t st) {
+  if (F.nitems == 0) return;
+  const size_t smem = size_t(kNwWarps) * (align_smem_per_warp(F.geom) + align16(size_t(16) * F.tncol * 4));
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_final_subs, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  k_final_subs<<<F.geom.nwarps / kNwWarps, kNwWarps * 32, smem, st>>>(F);
 }
 
 // ---------------------------------------------------------------------------

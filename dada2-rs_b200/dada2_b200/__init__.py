@@ -71,12 +71,13 @@ class DadaParams:
     use_quals: bool = True
     greedy: bool = True
     host_threads: int = 0
+    transitions: bool = False  # also return DadaAux.transitions (src/error.rs:194-249)
 
     def c(self) -> DadaParamsC:
         return DadaParamsC(self.align.c(), float(self.omega_a), float(self.omega_p), float(self.omega_c),
                            int(bool(self.detect_singletons)), int(self.max_clust), float(self.min_fold),
                            int(self.min_hamming), int(self.min_abund), int(bool(self.use_quals)),
-                           int(bool(self.greedy)), int(self.host_threads))
+                           int(bool(self.greedy)), int(self.host_threads), int(bool(self.transitions)))
 
 
 def _counters(c: CountersC) -> dict:
@@ -198,6 +199,11 @@ def _read_result(h) -> dict:
     res["pvals"] = a["pvals"][:nraw]
     res["counters"] = {k: int(v) for k, v in zip(COUNTER_KEYS, a["counters"])}
     res["clusters"] = ClusterList(a, ncl)
+    tncol = lib().dgpu_result_transitions(h, None)
+    if tncol > 0:
+        tr = np.zeros(16 * tncol, np.uint32)
+        lib().dgpu_result_transitions(h, ptr(tr))
+        res["transitions"] = tr.reshape(16, tncol)
     return res
 
 

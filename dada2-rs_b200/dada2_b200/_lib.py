@@ -44,6 +44,7 @@ class DadaParamsC(C.Structure):
         ("omega_c", C.c_double), ("detect_singletons", C.c_int32), ("max_clust", C.c_int32),
         ("min_fold", C.c_double), ("min_hamming", C.c_uint32), ("min_abund", C.c_uint32),
         ("use_quals", C.c_int32), ("greedy", C.c_int32), ("host_threads", C.c_int32),
+        ("transitions", C.c_int32),
     ]
 
 
@@ -93,6 +94,8 @@ def lib():
                                       _P, _P, C.c_int, _P]
         L.dgpu_result_sizes.argtypes = [_P, _P]
         L.dgpu_result_fill.argtypes = [_P, C.POINTER(DadaOutC)]
+        L.dgpu_result_transitions.argtypes = [_P, _P]
+        L.dgpu_result_transitions.restype = C.c_int
         L.dgpu_result_free.argtypes = [_P]
         L.dgpu_result_free.restype = None
         L.dgpu_batch_prepare.argtypes = [C.c_int, C.POINTER(DadaParamsC), C.c_int, _P, _P, _P, _P, _P, _P,

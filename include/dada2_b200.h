@@ -59,6 +59,8 @@ typedef struct {
   uint32_t min_hamming, min_abund;
   int32_t use_quals, greedy;
   int32_t host_threads; /* threads for the host phases of dgpu_dada_batch; 0 = half the cores */
+  int32_t transitions;  /* 1: also count transitions by quality after the final-subs pass
+                           (DadaAux.transitions, src/dada.rs:609-673, src/error.rs:194-249) */
 } dgpu_dada_params;
 
 /* Counters of one compare call (CompareTiming's denominators, src/cluster.rs:190-231). */
@@ -190,6 +192,12 @@ int dgpu_stats_latencies(double* out, int cap);
 /* sizes: [nclust, nraw, total members, total center-sequence bytes] */
 int dgpu_result_sizes(const dgpu_result* res, int64_t* sizes);
 int dgpu_result_fill(const dgpu_result* res, const dgpu_dada_out* out);
+/* Transition counts of a run made with dgpu_dada_params.transitions = 1: the
+ * 16 x ncol matrix (row 4 * center nt + raw nt, column = quality; ncol is the
+ * sample's error-matrix width after extension, or 1 without qualities) is
+ * copied to out (when non-null) and ncol returned; 0 when not computed.
+ * Replaces transition_counts (src/error.rs:194-249). */
+int dgpu_result_transitions(const dgpu_result* res, uint32_t* out);
 void dgpu_result_free(dgpu_result* res);
 
 /* ---- aligners alone (test entry) ----

@@ -1511,6 +1511,39 @@ std::string dada_uniques(const std::vector<RawInput>& inputs, const DadaParams& 
     cs.birth_hamming = bi.birth_comp.hamming;
     out.clusters.push_back(std::move(cs));
   }
+  if (params.transitions) {
+    // src/dada.rs:609-617, 648-673: every raw realigned against its cluster's
+    // center with the k-mer screen off; then src/error.rs:194-249: for each
+    // correct member, every center position aligned to a raw base adds the
+    // raw's reads at (4*(center nt) + raw nt, the raw's quality there).
+    AlignParams fa = params.align;
+    fa.use_kmers = false;
+    fa.kdist_cutoff = 1.0;
+    const size_t tncol = has_quals ? ncol : 1;
+    out.transitions.assign(16 * tncol, 0u);
+    out.transitions_ncol = tncol;
+    AlignBuf buf;
+    for (const Bi& bi : bb.clusters) {
+      if (bi.center < 0) continue;
+      const Raw& cr = bb.raws[size_t(bi.center)];
+      for (size_t raw_idx : bi.raws) {
+        const Raw& raw = bb.raws[raw_idx];
+        if (!raw.correct) continue;
+        Sub sub;
+        int32_t method = 0;
+        if (!sub_new(cr, raw, fa, buf, sub, &method)) continue;
+        for (size_t pos0 = 0; pos0 < cr.seq.size(); ++pos0) {
+          if (sub.map[pos0] == GAP_GLYPH) continue;
+          const size_t pos1 = sub.map[pos0];
+          const size_t nti0 = cr.seq[pos0] ? cr.seq[pos0] - 1u : 0u;
+          const size_t nti1 = raw.seq[pos1] ? raw.seq[pos1] - 1u : 0u;
+          const size_t qual = has_quals ? (raw.has_qual ? raw.qual[pos1] : 0u) : 0u;
+          const size_t t = 4 * nti0 + nti1;
+          if (t < 16 && qual < tncol) out.transitions[t * tncol + qual] += raw.reads;
+        }
+      }
+    }
+  }
   out.nalign = bb.nalign;
   out.nshroud = bb.nshroud;
   out.nraw = uint32_t(nraw);

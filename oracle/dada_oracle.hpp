@@ -255,6 +255,7 @@ struct DadaParams {
   bool use_quals = true;
   bool greedy = true;
   int nthreads = 1;
+  bool transitions = false;  // also compute the DadaAux transition counts (src/dada.rs:609-640)
 };
 struct RawInput {
   std::string seq;  // ASCII
@@ -289,6 +290,9 @@ struct DadaResult {
   uint64_t nalign = 0, nshroud = 0;
   uint32_t nraw = 0;
   DadaRunStats stats;
+  // with DadaParams::transitions: 16 x transitions_ncol counts (src/error.rs:194-249)
+  std::vector<uint32_t> transitions;
+  size_t transitions_ncol = 0;
 };
 // Returns an empty string on success, else the validation error message.
 std::string dada_uniques(const std::vector<RawInput>& inputs, const DadaParams& params,

@@ -43,6 +43,7 @@ class DadaParamsC(C.Structure):
         ("omega_c", C.c_double), ("detect_singletons", C.c_int32), ("max_clust", C.c_int32),
         ("min_fold", C.c_double), ("min_hamming", C.c_uint32), ("min_abund", C.c_uint32),
         ("use_quals", C.c_int32), ("greedy", C.c_int32), ("nthreads", C.c_int32),
+        ("transitions", C.c_int32),
     ]
 
 
@@ -86,6 +87,7 @@ class DadaParams:
     use_quals: bool = True
     greedy: bool = True
     nthreads: int = 1
+    transitions: bool = False  # also return the DadaAux transition counts (src/error.rs:194-249)
 
 
 def lib():
@@ -123,6 +125,8 @@ def lib():
         _lib.orc_c_dada_free.argtypes = [C.c_void_p]
         _lib.orc_c_dada_sizes.argtypes = [C.c_void_p, _P]
         _lib.orc_c_dada_fill.argtypes = [C.c_void_p, C.POINTER(DadaOutC)]
+        _lib.orc_c_dada_transitions.argtypes = [C.c_void_p, _P]
+        _lib.orc_c_dada_transitions.restype = C.c_int
     return _lib
 
 
@@ -145,7 +149,8 @@ def dada_params_c(p) -> DadaParamsC:
     return DadaParamsC(align_params_c(p.align), float(p.omega_a), float(p.omega_p),
                        float(p.omega_c), int(bool(p.detect_singletons)), int(p.max_clust),
                        float(p.min_fold), int(p.min_hamming), int(p.min_abund),
-                       int(bool(p.use_quals)), int(bool(p.greedy)), int(p.nthreads))
+                       int(bool(p.use_quals)), int(bool(p.greedy)), int(p.nthreads),
+                       int(bool(getattr(p, "transitions", False))))
 
 
 # ---------------- kmers ----------------
@@ -447,7 +452,13 @@ def dada(seqs, abund, err, ncol, params: DadaParams, quals=None, prior=None):
             o = DadaOutC(*[_ptr(a[n]) for n, _ in DadaOutC._fields_])
             lib().orc_c_dada_fill(h, C.byref(o))
 
-        return unpack_result(sizes, fill)
+        res = unpack_result(sizes, fill)
+        tncol = lib().orc_c_dada_transitions(h, None)
+        if tncol:
+            tr = np.zeros(16 * tncol, np.uint32)
+            lib().orc_c_dada_transitions(h, _ptr(tr))
+            res["transitions"] = tr.reshape(16, tncol)
+        return res
     finally:
         lib().orc_c_dada_free(h)
 

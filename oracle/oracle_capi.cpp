@@ -26,6 +26,7 @@ typedef struct {
   double min_fold;
   uint32_t min_hamming, min_abund;
   int32_t use_quals, greedy, nthreads;
+  int32_t transitions;
 } orc_dada_params;
 
 typedef struct {
@@ -311,6 +312,7 @@ void* orc_c_dada(int nraw, const char* seqcat, const uint32_t* off, const uint32
   dp.use_quals = pp->use_quals != 0;
   dp.greedy = pp->greedy != 0;
   dp.nthreads = pp->nthreads;
+  dp.transitions = pp->transitions != 0;
   OrcDada* d = new OrcDada();
   std::string e = dada_uniques(in, dp, d->res);
   if (!e.empty()) {
@@ -325,6 +327,14 @@ void* orc_c_dada(int nraw, const char* seqcat, const uint32_t* off, const uint32
 }
 
 void orc_c_dada_free(void* h) { delete static_cast<OrcDada*>(h); }
+
+// Transition counts of a run made with transitions set: returns the column
+// count and copies 16 x ncol values to out (when non-null); 0 if none.
+int orc_c_dada_transitions(void* h, uint32_t* out) {
+  const DadaResult& r = static_cast<OrcDada*>(h)->res;
+  if (out) std::copy(r.transitions.begin(), r.transitions.end(), out);
+  return int(r.transitions_ncol);
+}
 
 // sizes: [nclust, nraw, total members, total center-sequence bytes]
 void orc_c_dada_sizes(void* h, int64_t* sizes) {

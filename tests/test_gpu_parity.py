@@ -375,3 +375,62 @@ def test_saturated_kmers_take_the_exact_distance(k):
             gl, gh, gs, _ = ctx.compare(center, 0.42, greedy=False)
             assert gl.tobytes() == wl.tobytes()
             assert np.array_equal(gh, wh) and np.array_equal(gs, ws)
+
+
+def _assert_same_transitions(got, want):
+    assert "transitions" in got and "transitions" in want
+    assert got["transitions"].shape == want["transitions"].shape
+    assert np.array_equal(got["transitions"], want["transitions"])
+
+
+@pytest.mark.parametrize("variant", ["default", "band0", "no_quals", "unbanded"])
+def test_transition_counts_match_oracle(variant):
+    """DadaAux.transitions: every correct raw realigned to its center with the
+    k-mer screen off (src/dada.rs:609-673), counted by transition and quality
+    (src/error.rs:194-249)."""
+    w = synth.small_illumina(52, nvariants=6, nreads=1500, L=120)
+    s = w.samples[0]
+    oa, da = O.AlignParams(), D.AlignParams()
+    quals = s.quals
+    if variant == "band0":
+        oa.band = da.band = 0
+    elif variant == "no_quals":
+        quals = None
+    elif variant == "unbanded":
+        oa.band = da.band = -1
+    want = O.dada(s.seqs, s.abund, w.err, w.ncol, O.DadaParams(align=oa, nthreads=4, transitions=True), quals=quals)
+    got = D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, D.DadaParams(align=da, transitions=True), quals=quals)
+    assert_same_dada(got, want)
+    _assert_same_transitions(got, want)
+    if quals is None:
+        assert got["transitions"].shape == (16, 1)
+    assert int(got["transitions"].sum()) > 0
+
+
+def test_transition_counts_homopolymer_path_match_oracle():
+    w = synth.config2(seed=78, nuniques=80)
+    s = w.samples[0]
+    op = O.DadaParams(align=O.AlignParams(band=32, homo_gap_p=-1), nthreads=8, transitions=True)
+    dp = D.DadaParams(align=D.AlignParams(band=32, homo_gap_p=-1), transitions=True)
+    want = O.dada(s.seqs, s.abund, w.err, w.ncol, op, quals=s.quals)
+    got = D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, dp, quals=s.quals)
+    _assert_same_transitions(got, want)
+
+
+def test_transition_counts_in_a_batch_use_each_samples_width():
+    """In a batch the error matrix is extended to the largest quality of any
+    sample, but each sample's counts keep the width its own run would have."""
+    ws = [synth.small_illumina(60 + i, nvariants=4, nreads=900, L=110) for i in range(3)]
+    err, ncol = ws[0].err, ws[0].ncol
+    samples = [w.samples[0] for w in ws]
+    # lift one sample's qualities past the error matrix so the widths differ
+    boosted = samples[1]
+    boosted.quals = [np.asarray(q, np.uint32) + np.uint32(8) * np.uint32(a) for q, a in zip(boosted.quals, boosted.abund)]
+    got = D.dada_uniques_batch(samples, err, ncol, D.DadaParams(host_threads=2, transitions=True))
+    widths = set()
+    for s, g in zip(samples, got):
+        want = O.dada(s.seqs, s.abund, err, ncol, O.DadaParams(nthreads=4, transitions=True), quals=s.quals)
+        assert_same_dada(g, want)
+        _assert_same_transitions(g, want)
+        widths.add(g["transitions"].shape[1])
+    assert len(widths) > 1
