@@ -300,6 +300,22 @@ def main():
     h2d = (D.stats_read()["h2d_bytes"] - h2d0) // max(args.steps, 1)
     e2e = e2e_comps_all / e2e_dt
 
+    # ---- the final-subs pass (transition counts), measured beside the step ----
+    final_subs = None
+    if rank == 0:
+        pt = D.DadaParams(align=params.align, greedy=params.greedy, transitions=True)
+        with D.ResidentBatch(w.samples, w.err, w.ncol, pt, device=local, packed=pb) as bt:
+            bt.run(read_results=False)
+            torch.cuda.synchronize()
+            f0 = time.perf_counter()
+            resf = bt.run(read_results=False)
+            f1 = time.perf_counter()
+        plain_step = dt / max(args.steps, 1)
+        members = int(sum(r["nraw"] for r in resf))
+        final_subs = {"ms_per_step_extra": 1e3 * ((f1 - f0) - plain_step), "step_ms_with": 1e3 * (f1 - f0),
+                      "raws": members, "note": "every correct raw realigned to its center (screen off) and counted by "
+                                                "transition and quality; wall clock of one run minus the timed step"}
+
     # ---- plain single-sample path (rank 0 only; one pass) ----
     plain = None
     if rank == 0 and not args.no_plain:
@@ -366,6 +382,7 @@ def main():
         "host_phases_s_per_step": {"critical_sample": float(max(r["times"][2] for r in res)),
                                    "all_samples": float(sum(r["times"][2] for r in res)),
                                    "note": "shuffle + p-update + bud on the host, last timed step"},
+        "final_subs": final_subs,
         "gpu_launches": launches,
         "clocks": clk,
         "plain": plain,
