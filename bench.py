@@ -153,6 +153,55 @@ def committed_traffic():
     return None
 
 
+def precision_report(w, params, device, omega_a=1e-40):
+    """The largest sample's first compare call (every unique against the
+    cluster-0 center, screen off) with ln(lambda) also formed as a compensated
+    FP32 sum: its largest errors against the FP64 product every decision uses,
+    and the share of pairs whose FP32 p-value falls within 1e3x of omega_a
+    (where the FP32 variant falls back to FP64)."""
+    import dada2_b200 as D
+
+    s = max(w.samples, key=lambda x: len(x.seqs))
+    lut = np.zeros(256, np.uint8)
+    for ch, c in zip("ACGT", (1, 2, 3, 4)):
+        lut[ord(ch)] = c
+    codes = [lut[np.frombuffer(x.encode(), np.uint8)] for x in s.seqs]
+    reads = np.asarray(s.abund, np.uint32)
+    quals = [np.floor(np.asarray(q, np.float64) / a + 0.5).astype(np.uint8) for q, a in zip(s.quals, reads)]
+    m = np.asarray(w.err, np.float64).reshape(16, w.ncol)
+    qmax = max(int(q.max()) for q in quals)
+    if qmax >= w.ncol:
+        m = np.concatenate([m, np.repeat(m[:, -1:], qmax + 1 - w.ncol, axis=1)], axis=1)
+    total = float(reads.sum())
+    with D.CompareContext(params.align, m.ravel().copy(), m.shape[1], device=device) as ctx:
+        ctx.upload(codes, reads, quals=quals)
+        ctx.set_lambda32(True)
+        center = int(np.flatnonzero(reads == reads.max())[-1])  # B::new's center (src/containers.rs:450-458)
+        lam, _, _, cnt = ctx.compare(center, 1.0, greedy=True)
+        ll32 = ctx.loglambda32().astype(np.float64)
+    al = np.isfinite(ll32)
+    normal = al & (lam > 1e-300)  # FP64 lambda is exact to its precision only while normal
+    rel = np.abs(np.exp(ll32[normal]) - lam[normal]) / lam[normal]
+    band = agree = disagree = 0
+    for r in np.nonzero(al)[0]:
+        p64 = D.calc_pA(int(reads[r]), float(lam[r]) * total)
+        p32 = D.calc_pA(int(reads[r]), float(np.exp(ll32[r])) * total)
+        if omega_a / 1e3 <= p32 <= omega_a * 1e3:
+            band += 1
+        elif normal[r]:
+            same = (p32 < omega_a) == (p64 < omega_a)
+            agree += same
+            disagree += not same
+    return {"pairs": int(al.sum()), "max_rel_err_lambda": float(rel.max()) if rel.size else None,
+            "max_abs_err_ln_lambda": float(np.max(np.abs(ll32[normal] - np.log(lam[normal])))) if normal.any() else None,
+            "fp64_fallback_rate": band / max(int(al.sum()), 1),
+            "decisions_outside_band": {"agree": agree, "differ": disagree},
+            "pairs_fp64_subnormal": int((al & ~normal).sum()),
+            "sample_uniques": len(s.seqs),
+            "note": "decisions always use FP64; FP32 is measured beside it. Where the FP64 product is subnormal "
+                    "(below 1e-300) it has lost its own relative precision, so those pairs are counted apart"}
+
+
 def cpu_subset(samples, target=12_000_000):
     """First samples (by index) whose expected compares add up to ~target."""
     out, tot = [], 0
@@ -316,6 +365,9 @@ def main():
                       "raws": members, "note": "every correct raw realigned to its center (screen off) and counted by "
                                                 "transition and quality; wall clock of one run minus the timed step"}
 
+    # ---- precision variant: FP32 compensated ln(lambda) beside the FP64 product ----
+    precision = precision_report(w, params, local) if rank == 0 else None
+
     # ---- plain single-sample path (rank 0 only; one pass) ----
     plain = None
     if rank == 0 and not args.no_plain:
@@ -383,6 +435,7 @@ def main():
                                    "all_samples": float(sum(r["times"][2] for r in res)),
                                    "note": "shuffle + p-update + bud on the host, last timed step"},
         "final_subs": final_subs,
+        "precision": precision,
         "gpu_launches": launches,
         "clocks": clk,
         "plain": plain,

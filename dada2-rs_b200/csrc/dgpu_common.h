@@ -15,6 +15,7 @@ struct KParams {
   int32_t use_kmers, kmer_size, band, vectorized, gapless;
   int32_t use_quals, greedy;
   int32_t ncol;  // error-matrix columns
+  int32_t lambda32;  // also form ln(lambda) as a compensated FP32 sum (precision report)
 };
 
 // Device view of a pool of uniques (one or more samples, concatenated).
@@ -38,6 +39,7 @@ struct PoolDev {
   double* res_lambda;
   uint32_t* res_ham;
   uint8_t* res_status;
+  float* res_loglam32;  // with KParams::lambda32: FP32 ln(lambda) of aligned pairs, -inf otherwise
   uint32_t nraw;
   uint32_t maxlen;
 };

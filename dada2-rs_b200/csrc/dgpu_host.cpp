@@ -382,6 +382,7 @@ struct Pool {
   DBuf<uint16_t> kidx;
   DBuf<uint8_t> kcnt;
   DBuf<double> e_minmax, err, lambda;
+  DBuf<float> loglam32;
   // stored comps of each task, at the task's first raw (its sample's base)
   HBuf<uint32_t> comp_index, comp_ham;
   HBuf<double> comp_lambda;
@@ -392,7 +393,7 @@ struct Pool {
   ~Pool() {
     slots.clear();  // each slot drains its own stream first
     if (st && cudaStreamSynchronize(st) == cudaSuccess)
-      recycle_all(seq, qual, kmer8, sat, lock, status, off, len, reads, ham, knum, kidx, kcnt, e_minmax, err, lambda,
+      recycle_all(seq, qual, kmer8, sat, lock, status, off, len, reads, ham, knum, kidx, kcnt, e_minmax, err, lambda, loglam32,
                   comp_index, comp_ham, comp_lambda, lock_host);
     if (st) cudaStreamDestroy(st);
   }
@@ -463,6 +464,7 @@ struct Pool {
     TRY(status.alloc(n));
     TRY(ham.alloc(n));
     TRY(lambda.alloc(n));
+    TRY(loglam32.alloc(n));
     TRY(e_minmax.alloc(n));
     TRY(err.alloc(size_t(16) * kp.ncol));
     const bool sparse = kp.use_kmers && kp.kmer_size >= 8;  // src/kmers.rs:213-221
@@ -556,6 +558,7 @@ struct Pool {
     v.res_lambda = lambda.p;
     v.res_ham = ham.p;
     v.res_status = status.p;
+    v.res_loglam32 = loglam32.p;
     v.nraw = nraw;
     v.maxlen = lmax;
     return v;
@@ -2306,6 +2309,24 @@ static void fill_counters(const uint32_t* c, uint32_t stored, dgpu_counters* cnt
   cnt->vectorized = c[TC_VECTORIZED];
   cnt->homo = c[TC_HOMO];
   cnt->endsfree = c[TC_ENDSFREE];
+}
+
+int dgpu_ctx_set_lambda32(dgpu_ctx* ctx, int enable) {
+  if (!ctx) return fail(DGPU_E_INVALID, "null context");
+  ctx->kp.lambda32 = enable ? 1 : 0;
+  ctx->pool.kp.lambda32 = ctx->kp.lambda32;
+  return 0;
+}
+
+int dgpu_get_loglambda32(dgpu_ctx* ctx, float* out) {
+  if (!ctx || !out) return fail(DGPU_E_INVALID, "null argument");
+  if (!ctx->uploaded) return fail(DGPU_E_INVALID, "no raws uploaded");
+  CUDA_TRY(cudaMemcpy(out, ctx->pool.loglam32.p, size_t(ctx->pool.nraw) * 4, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+double dgpu_calc_pA(uint32_t reads, double e_reads, int prior) {
+  return SampleState::calc_pA(reads, e_reads, prior != 0);
 }
 
 int dgpu_compare(dgpu_ctx* ctx, int center, double kdist_cutoff, int greedy, double* lambda_out,

@@ -225,6 +225,31 @@ __device__ double lambda_chain(int lane, const uint16_t* fidx, int L, const doub
   return __shfl_sync(FULL, lam, 0);
 }
 
+// ln(lambda) as a compensated FP32 sum of logf(err) over the raw's positions
+// (the precision variant of compute_lambda): each lane runs a Kahan sum over
+// its positions, then the lanes' (sum, correction) pairs are combined with an
+// error-free two-sum. Returns the result on all lanes.
+__device__ float loglambda32(int lane, const uint16_t* fidx, int L, const double* err_s) {
+  float s = 0.0f, c = 0.0f;
+  for (int p = lane; p < L; p += 32) {
+    const float y = logf(float(err_s[fidx[p]])) - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+  float e = -c;
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    const float so = __shfl_xor_sync(FULL, s, d), eo = __shfl_xor_sync(FULL, e, d);
+    const float sum = s + so;
+    const float bb = sum - s;
+    const float err = (s - (sum - bb)) + (so - bb);
+    s = sum;
+    e = e + eo + err;
+  }
+  return s + e;
+}
+
 // tcode[p] (row of the error matrix for raw position p) + quality -> fidx.
 __device__ bool build_fidx(int lane, const uint8_t* tcode, const uint8_t* qual_g, int L, int ncol, int use_quals,
                            uint16_t* fidx) {
@@ -440,6 +465,7 @@ __global__ void __launch_bounds__(kScreenWarps * 32, 4) k_screen(CompareLaunch L
     }
     bool pass = false;
     if (valid) {
+      if (kp.lambda32) L.pool.res_loglam32[g] = -INFINITY;
       if (skip) {
         L.pool.res_lambda[g] = 0.0;
         L.pool.res_ham[g] = 0xffffffffu;
@@ -1993,6 +2019,7 @@ __global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_align(Compar
     const PairResult R = align_pair(lane, kp, L.pool, L.geom, g, T.center, L.pool.res_lambda[g], kp.use_quals != 0, VS,
                                     RS, kb, scratch, L.err_word);
     double lam = 0.0;
+    float ll32 = -INFINITY;
     if (R.ok) {
       const bool bad = build_fidx(lane, R.tcode, R.qual, R.lg, kp.ncol, kp.use_quals, R.fidx);
       __syncwarp();
@@ -2000,9 +2027,11 @@ __global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_align(Compar
         if (lane == 0) atomicOr(L.err_word, DERR_LAMBDA);
       } else {
         lam = lambda_chain(lane, R.fidx, R.lg, err_s);
+        if (kp.lambda32) ll32 = loglambda32(lane, R.fidx, R.lg, err_s);
       }
     }
     if (lane == 0) {
+      if (kp.lambda32) L.pool.res_loglam32[g] = ll32;
       L.pool.res_lambda[g] = lam;
       L.pool.res_ham[g] = R.ok ? R.ham : 0xffffffffu;
       L.pool.res_status[g] = uint8_t(ST_ALIGNED | (R.method << 2));

@@ -146,6 +146,16 @@ class CompareContext:
         return {"index": idx[:k].copy(), "lambda": lam[:k].copy(), "hamming": ham[:k].copy(),
                 "self": self_.value, "counters": _counters(cnt)}
 
+    def set_lambda32(self, enable: bool = True):
+        """Also form ln(lambda) in compensated FP32 on later compares (precision report)."""
+        check(lib().dgpu_ctx_set_lambda32(self.h, int(bool(enable))))
+
+    def loglambda32(self) -> np.ndarray:
+        """FP32 ln(lambda) of the latest compare (-inf where the pair was not aligned)."""
+        out = np.zeros(self.n, np.float32)
+        check(lib().dgpu_get_loglambda32(self.h, ptr(out)))
+        return out
+
     def close(self):
         if self.h:
             lib().dgpu_ctx_destroy(self.h)
@@ -364,6 +374,11 @@ def _read_counters(h) -> dict:
     check(lib().dgpu_result_sizes(h, ptr(sizes)))
     return {"nclust": int(sizes[0]), "nraw": int(sizes[1]),
             "counters": {k: int(v) for k, v in zip(COUNTER_KEYS, cnt)}, "times": tm}
+
+
+def calc_pA(reads: int, e_reads: float, prior: bool = False) -> float:
+    """calc_pA (src/pval.rs:208-241), the library's FP64 p-value."""
+    return float(lib().dgpu_calc_pA(int(reads), float(e_reads), int(bool(prior))))
 
 
 def cache_release(device: int = -1) -> int:

@@ -95,6 +95,10 @@ def lib():
         L.dgpu_result_sizes.argtypes = [_P, _P]
         L.dgpu_result_fill.argtypes = [_P, C.POINTER(DadaOutC)]
         L.dgpu_result_transitions.argtypes = [_P, _P]
+        L.dgpu_ctx_set_lambda32.argtypes = [_P, C.c_int]
+        L.dgpu_get_loglambda32.argtypes = [_P, _P]
+        L.dgpu_calc_pA.argtypes = [C.c_uint32, C.c_double, C.c_int]
+        L.dgpu_calc_pA.restype = C.c_double
         L.dgpu_result_transitions.restype = C.c_int
         L.dgpu_result_free.argtypes = [_P]
         L.dgpu_result_free.restype = None

@@ -200,6 +200,19 @@ int dgpu_result_fill(const dgpu_result* res, const dgpu_dada_out* out);
 int dgpu_result_transitions(const dgpu_result* res, uint32_t* out);
 void dgpu_result_free(dgpu_result* res);
 
+/* Precision variant of compute_lambda (src/pval.rs:253-320): with enable = 1
+ * every later compare of the context also forms ln(lambda) of each aligned
+ * pair as a compensated FP32 sum of logf(err) beside the FP64 product (which
+ * stays the one every decision uses). dgpu_get_loglambda32 copies the latest
+ * compare's values (nraw floats; -inf for pairs not aligned). No counterpart
+ * in the reference, which computes FP64 only. */
+int dgpu_ctx_set_lambda32(dgpu_ctx* ctx, int enable);
+int dgpu_get_loglambda32(dgpu_ctx* ctx, float* out);
+/* calc_pA (src/pval.rs:208-241): the Poisson abundance p-value of a unique
+ * with `reads` reads against an expected e_reads, conditioned on being seen
+ * unless `prior`. */
+double dgpu_calc_pA(uint32_t reads, double e_reads, int prior);
+
 /* ---- aligners alone (test entry) ----
  * which: 0 vectorized (compressed anti-diagonal i16, end_gap as given),
  *        1 ends-free with homopolymer gaps, 2 ends-free i32.

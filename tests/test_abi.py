@@ -59,3 +59,20 @@ def test_gpu_entry_points_fail_loudly_without_a_device():
         pytest.skip("a GPU is present; covered by the gpu tests")
     with pytest.raises(D.DgpuError):
         D.dada_uniques(["ACGTACGTAC"], [3], np.full(16, 0.01), 1)
+
+
+def test_library_calc_pA_matches_the_oracle_bit_for_bit():
+    """The host p-value (calc_pA, src/pval.rs:208-241) the library exports is
+    the oracle's to the last bit, over both gamma branches, the log-space
+    fallback and the conditioning (no GPU needed)."""
+    import numpy as np
+
+    import dada2_b200 as D
+    from oracle import oracle as O
+
+    for k in (1, 2, 3, 5, 10, 40, 200, 3000):
+        for le in np.linspace(-14, 4, 61):
+            e = float(10.0 ** le)
+            for prior in (False, True):
+                a, b = D.calc_pA(k, e, prior), O.calc_pA(k, e, prior)
+                assert np.float64(a).tobytes() == np.float64(b).tobytes(), (k, e, prior, a, b)

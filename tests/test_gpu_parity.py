@@ -434,3 +434,45 @@ def test_transition_counts_in_a_batch_use_each_samples_width():
         _assert_same_transitions(g, want)
         widths.add(g["transitions"].shape[1])
     assert len(widths) > 1
+
+
+@pytest.mark.parametrize("L", [150, 250])
+def test_fp32_log_lambda_tracks_fp64(L):
+    """Precision variant: ln(lambda) as a compensated FP32 sum beside the FP64
+    product. Tolerances: |ln32 - ln64| <= 1e-5 * max(1, |ln64|); lambda's
+    relative error <= 1e-4 where FP64 lambda is normal; outside 1e3x of
+    omega_a the p-value decision p < omega_a agrees with FP64's."""
+    w = synth.small_illumina(70 + L, nvariants=8, nreads=2500, L=L)
+    s = w.samples[0]
+    seqs = [O.encode(x) for x in s.seqs]
+    quals = _rounded_quals(s)
+    err, ncol = _extend(w.err, w.ncol, quals)
+    reads = np.asarray(s.abund, np.uint32)
+    total = float(reads.sum())
+    omega_a = 1e-40
+    with D.CompareContext(D.AlignParams(), err, ncol) as ctx:
+        ctx.upload(seqs, reads, quals=quals)
+        ctx.set_lambda32(True)
+        n_band = n_all = 0
+        for center in (0, 3, len(seqs) // 2):
+            lam, ham, skp, cnt = ctx.compare(center, 1.0, greedy=False)
+            ll32 = ctx.loglambda32().astype(np.float64)
+            aligned = np.isfinite(ll32)
+            assert aligned.sum() == cnt["aligned"]
+            # FP64 lambda is only exact to its relative precision while it is a
+            # normal double; below that the product itself has underflowed
+            normal = aligned & (lam > 1e-300)
+            ll64 = np.log(lam[normal])
+            assert np.all(np.abs(ll32[normal] - ll64) <= 1e-5 * np.maximum(1.0, np.abs(ll64)))
+            rel = np.abs(np.exp(ll32[normal]) - lam[normal]) / lam[normal]
+            assert rel.max() <= 1e-4
+            assert np.all(ll32[aligned & ~normal] < np.log(1e-300) + 1e-3)
+            for r in np.nonzero(aligned)[0]:
+                p64 = D.calc_pA(int(reads[r]), float(lam[r]) * total)
+                p32 = D.calc_pA(int(reads[r]), float(np.exp(ll32[r])) * total)
+                n_all += 1
+                if omega_a / 1e3 <= p32 <= omega_a * 1e3:
+                    n_band += 1  # where the FP32 variant falls back to FP64
+                else:
+                    assert (p32 < omega_a) == (p64 < omega_a)
+        assert n_all > 0
