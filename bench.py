@@ -18,6 +18,8 @@ Multi-GPU (torchrun): samples are independent, so each rank denoises its own
 40-sample batch (seeded by rank) with no collective on the data path
 (weak scaling); timing is the max over ranks.
 
+--config 4 replays the denoising-service request trace (see service_bench).
+
 --impl reference times the CPU restatement of the reference (oracle/,
 multithreaded like the reference's per-sample fan-out) on a bounded subset of
 the same workload.
@@ -75,6 +77,8 @@ def load_workload(config: int, rank: int):
         return synth.config0(seed=1000 + 97 * rank)
     if config == 2:
         return synth.config2(seed=1002 + 97 * rank)
+    if config == 4:
+        return synth.config4(seed=1004 + 97 * rank)
     raise SystemExit(f"unknown config {config}")
 
 
@@ -264,10 +268,135 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+SERVICE_METRIC = "unique x center compares/s (denoising service, Poisson 20/s request trace)"
+
+
+def service_bench(args):
+    """The denoising-service workload: a Poisson trace of 48 requests replayed
+    in real time against DenoiseService (batched by length class, admitted by
+    device-memory footprint) and against one-request-at-a-time dgpu_dada;
+    then the same requests all at once (capacity). Latency is host wall time
+    from submit to result; compares/s is all requests' compares over the
+    replay's span. Rank 0 only."""
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    from dada2_b200 import synth
+
+    w = synth.config4(seed=1004)  # generated in a spawn pool before any GPU call
+    import torch
+
+    torch.cuda.set_device(local)
+    import dada2_b200 as D
+
+    params = D.DadaParams()
+    packs = [D.pack_sample(s.seqs, s.abund, s.quals) for s in w.samples]
+    arr = np.asarray(w.notes["arrivals"], np.float64)
+    for i in range(min(max(args.warmup, 1), len(packs))):
+        D.dada_uniques(None, None, w.err, w.ncol, params, packed=packs[i], read_result=False, device=local)
+
+    def replay_service(svc, arrivals):
+        t0 = time.perf_counter()
+        ts = []
+        for i, pk in enumerate(packs):
+            d = t0 + arrivals[i] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            ts.append(svc.submit(packed=pk))
+        out = [svc.wait(t, read_result=False) for t in ts]
+        span = time.perf_counter() - t0
+        return [lat for _, lat in out], sum(r["counters"]["cmp_scanned"] for r, _ in out), span
+
+    def replay_plain(arrivals):
+        t0 = time.perf_counter()
+        lats, comps = [], 0
+        for i, pk in enumerate(packs):
+            d = t0 + arrivals[i] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            r = D.dada_uniques(None, None, w.err, w.ncol, params, packed=pk, read_result=False, device=local)
+            lats.append(time.perf_counter() - (t0 + arrivals[i]))
+            comps += r["counters"]["cmp_scanned"]
+        return lats, comps, time.perf_counter() - t0
+
+    lens = np.tile(np.asarray(w.notes["lengths"]), max(args.steps, 1))
+
+    def summary(lats, comps, span):
+        lats = np.asarray(lats)
+        by_len = {}
+        for L in (150, 250, 1450):
+            m = lens[:len(lats)] == L
+            if m.any():
+                by_len[str(L)] = {"n": int(m.sum()), "p50_ms": 1e3 * float(np.percentile(lats[m], 50)),
+                                  "max_ms": 1e3 * float(lats[m].max())}
+        return {"p50_ms": 1e3 * float(np.percentile(lats, 50)), "p99_ms": 1e3 * float(np.percentile(lats, 99)),
+                "mean_ms": 1e3 * float(lats.mean()), "compares_per_s": comps / span, "span_s": span,
+                "compares": int(comps), "by_length": by_len}
+
+    D.stats_reset()
+    clocks = ClockSampler(local)
+    clocks.start()
+    svc_l, svc_c, svc_t, batches = [], 0, 0.0, 0
+    with D.DenoiseService(w.err, w.ncol, params, device=local) as svc:
+        for _ in range(args.steps):
+            lats, c, t = replay_service(svc, arr)
+            svc_l += lats
+            svc_c += c
+            svc_t += t
+        batches_trace = svc.stats()["batches"]
+        cap_svc = summary(*replay_service(svc, np.zeros_like(arr)))
+        batches = svc.stats()["batches"]
+    launches = int(sum(D.stats_read()["launches"].values()))
+    pl_l, pl_c, pl_t = [], 0, 0.0
+    for _ in range(args.steps):
+        lats, c, t = replay_plain(arr)
+        pl_l += lats
+        pl_c += c
+        pl_t += t
+    cap_plain = summary(*replay_plain(np.zeros_like(arr)))
+    clk = clocks.stop()
+    svc_sum, plain_sum = summary(svc_l, svc_c, svc_t), summary(pl_l, pl_c, pl_t)
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        sub = cpu_subset(w.samples, target=6_000_000)
+        c, t, cores = run_oracle(sub, w, os.cpu_count() or 1)
+        cpu = {"value": c / t, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"first {len(sub)} of {len(w.samples)} requests ({c} compares), C++ restatement of the "
+                         f"reference (oracle/), round(threads/4) samples at a time"}
+    u = [len(s.seqs) for s in w.samples]
+    line = {
+        "metric": SERVICE_METRIC, "value": svc_sum["compares_per_s"], "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * svc_t / max(args.steps, 1),
+        "higher_is_better": True, "scaling": "replicas only", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": w.name, "requests": len(u), "uniques_median": int(np.median(u)),
+                   "uniques_range": [int(min(u)), int(max(u))], "trace_s": float(arr[-1]),
+                   "note": "a step is one real-time replay of the trace; requests are generated Illumina-style "
+                           "samples (16 x 41 error model resident in the service)"},
+        "service": {**svc_sum, "batches": batches_trace,
+                    "workers": int(os.environ.get("DGPU_SERVICE_WORKERS", "3"))},
+        "host_cores": os.cpu_count(),
+        "one_at_a_time": plain_sum,
+        "capacity": {"service": {**cap_svc, "batches": batches - batches_trace}, "one_at_a_time": cap_plain,
+                     "note": "all requests submitted at t=0"},
+        "e2e": {"value": svc_sum["compares_per_s"], "unit": UNIT,
+                "h2d_bytes_per_step": int(sum(sum(x.nbytes for x in pk if x is not None) for pk in packs)),
+                "d2h_bytes_per_step": None, "note": "requests from host buffers through the service, results "
+                                                    "read back as sizes and counters"},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         reference_arm(args)
+        return
+    if args.config == 4:
+        service_bench(args)
         return
     rank, world, local = dist_env()
     import torch

@@ -1850,7 +1850,10 @@ static dgpu_result* finish(SampleState& S, const SampleSeqs& in) {
 // exactly run_dada's.
 static size_t batch_max_samples();
 
-static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_params& ap, int host_threads) {
+// on_finish (may be empty) is called for each sample as soon as its loop ends,
+// from the host thread that ran its last phase.
+static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_params& ap, int host_threads,
+                       const std::function<void(size_t)>& on_finish = {}) {
   const size_t ns = S.size();
   const size_t batch_max = batch_max_samples();
   std::mutex mu;
@@ -1943,13 +1946,18 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
             const double dh = secs(th, Clock::now());
             ss.stats.t_host += dh;
             host_ns += int64_t(1e9 * dh);
+            if (ss.pending < 0 && on_finish) {
+              ss.stats.t_done = secs(t_start, Clock::now());
+              ss.stats.t_total = ss.stats.t_done;
+              on_finish(sidx);
+            }
             std::lock_guard<std::mutex> g(mu);
             if (ss.pending >= 0) {
               ss.stats.t_mark = Clock::now();
               ready.push_back(sidx);
             } else {
               ++finished;
-              ss.stats.t_done = secs(t_start, Clock::now());
+              if (!on_finish) ss.stats.t_done = secs(t_start, Clock::now());
             }
             cv.notify_all();
           }, int64_t(S[sidx].n));  // larger samples have the longer chains: serve them first
@@ -2160,7 +2168,11 @@ static int final_subs(Batch& B, std::vector<SampleState>& S, dgpu_result** out) 
   return 0;
 }
 
-static int batch_run(Batch& B, dgpu_result** out) {
+// on_done (may be empty) receives each sample's result as soon as that sample
+// is finished, while others still run; the result then belongs to on_done's
+// owner and out[s] stays null. With transition counts requested every result
+// goes out at the end, after the final-subs pass.
+static int batch_run(Batch& B, dgpu_result** out, const std::function<void(size_t, dgpu_result*)>& on_done = {}) {
   const size_t ns = B.counts.size();
   Pool& P = B.pool;
   CUDA_TRY(cudaSetDevice(P.device));
@@ -2172,12 +2184,23 @@ static int batch_run(Batch& B, dgpu_result** out) {
   for (size_t s = 0; s < ns; ++s)
     S[s].init(B.counts[s], B.bases[s], B.E.reads.data() + B.bases[s], B.E.prior.data() + B.bases[s],
               P.lock_host.h + B.bases[s], &B.confs[s]);
-  TRY(run_samples(P, S, B.align, B.host_threads));
+  const bool early = on_done && !B.transitions;
+  std::vector<uint8_t> released(ns, 0);
+  std::function<void(size_t)> on_finish;
+  if (early)
+    on_finish = [&](size_t s) {
+      dgpu_result* R = finish(S[s], SampleSeqs{B.E.seq, B.E.off.data() + B.bases[s], B.E.len.data() + B.bases[s]});
+      R->times[3] = 0.0;  // the batch's slot wait is not known yet
+      released[s] = 1;
+      on_done(s, R);
+    };
+  TRY(run_samples(P, S, B.align, B.host_threads, on_finish));
   // final p-values and result tables, samples in parallel
   std::atomic<size_t> next{0};
   auto work = [&] {
     for (size_t s; (s = next.fetch_add(1)) < ns;)
-      out[s] = finish(S[s], SampleSeqs{B.E.seq, B.E.off.data() + B.bases[s], B.E.len.data() + B.bases[s]});
+      if (!released[s])
+        out[s] = finish(S[s], SampleSeqs{B.E.seq, B.E.off.data() + B.bases[s], B.E.len.data() + B.bases[s]});
   };
   const size_t nt = std::min<size_t>(ns, std::max(1u, std::thread::hardware_concurrency()));
   std::vector<std::thread> th;
@@ -2185,7 +2208,28 @@ static int batch_run(Batch& B, dgpu_result** out) {
   work();
   for (auto& t : th) t.join();
   if (B.transitions) TRY(final_subs(B, S, out));
+  if (on_done && !early)
+    for (size_t s = 0; s < ns; ++s) {
+      on_done(s, out[s]);
+      out[s] = nullptr;
+    }
   return 0;
+}
+
+// dgpu_dada_batch with each sample's result handed to on_done as soon as it
+// is ready (the denoising service's entry). Samples whose result was not
+// handed over when this fails have none.
+int dada_batch_each(int device, const dgpu_dada_params* params, int nsamples, const uint32_t* sample_start,
+                    const char* seqs, const uint32_t* offs, const uint32_t* lens, const uint32_t* abund,
+                    const uint8_t* prior, const uint32_t* qual_sums, const double* err_mat, int ncol,
+                    const std::function<void(size_t, dgpu_result*)>& on_done) {
+  Batch b;
+  TRY(batch_prepare(b, device, params, nsamples, sample_start, seqs, offs, lens, abund, prior, qual_sums, err_mat,
+                    ncol));
+  std::vector<dgpu_result*> out(size_t(nsamples), nullptr);
+  const int rc = batch_run(b, out.data(), on_done);
+  for (dgpu_result* r : out) delete r;
+  return rc;
 }
 
 }  // namespace dgpu

@@ -24,7 +24,7 @@ from ._lib import (AlignParamsC, CountersC, DadaOutC, DadaParamsC, DgpuError, In
                    check, device_count, lib, ptr)
 
 __all__ = ["AlignParams", "DadaParams", "CompareContext", "dada_uniques", "dada_uniques_batch",
-           "ResidentBatch", "PackedBatch", "align_pairs", "stats_reset", "stats_timing", "stats_read",
+           "ResidentBatch", "PackedBatch", "DenoiseService", "pack_sample", "align_pairs", "stats_reset", "stats_timing", "stats_read",
            "DgpuError", "InvalidInput", "device_count", "METHOD_NAMES", "KERNEL_NAMES"]
 
 KERNEL_NAMES = ["profiles", "screen", "align", "store"]
@@ -255,18 +255,25 @@ class ClusterList:
             yield self[ci]
 
 
+def pack_sample(seqs, abund, quals=None, prior=None):
+    """A sample's host buffers in the C ABI's layout, for repeated calls."""
+    return _pack(seqs, abund, quals, prior)
+
+
 def dada_uniques(seqs, abund, err, ncol, params: DadaParams | None = None, quals=None, prior=None,
-                 device: int = 0) -> dict:
-    """Denoise one sample on the GPU (src/dada.rs:225-592)."""
+                 device: int = 0, packed=None, read_result: bool = True) -> dict:
+    """Denoise one sample on the GPU (src/dada.rs:225-592). ``packed`` (from
+    ``pack_sample``) replaces seqs/abund/quals/prior; without ``read_result``
+    the result carries its sizes and counters only."""
     params = params or DadaParams()
-    cat, offs, lens, ab, qcat, pr = _pack(seqs, abund, quals, prior)
+    cat, offs, lens, ab, qcat, pr = packed if packed is not None else _pack(seqs, abund, quals, prior)
     err = np.ascontiguousarray(err, np.float64)
     pc = params.c()
     h = C.c_void_p()
     check(lib().dgpu_dada(device, C.byref(pc), len(lens), ptr(cat), ptr(offs), ptr(lens), ptr(ab), ptr(pr),
                           ptr(qcat), ptr(err), int(ncol), C.byref(h)))
     try:
-        return _read_result(h)
+        return _read_result(h) if read_result else _read_counters(h)
     finally:
         lib().dgpu_result_free(h)
 
@@ -374,6 +381,75 @@ def _read_counters(h) -> dict:
     check(lib().dgpu_result_sizes(h, ptr(sizes)))
     return {"nclust": int(sizes[0]), "nraw": int(sizes[1]),
             "counters": {k: int(v) for k, v in zip(COUNTER_KEYS, cnt)}, "times": tm}
+
+
+class DenoiseService:
+    """Requests (one sample each) submitted at any time and served on one
+    device: pending requests of one length class are batched in arrival order
+    within a device-memory budget and denoised together, so each result is
+    ``dada_uniques``' on that sample. ``wait`` returns (result, latency in s)."""
+
+    def __init__(self, err, ncol, params: DadaParams | None = None, device: int = 0, hbm_budget: int = 0):
+        self.params = params or DadaParams()
+        self._err = np.ascontiguousarray(err, np.float64)
+        pc = self.params.c()
+        self._live = {}
+        self.h = C.c_void_p()
+        check(lib().dgpu_service_create(device, C.byref(pc), ptr(self._err), int(ncol), int(hbm_budget),
+                                        C.byref(self.h)))
+
+    def submit(self, seqs=None, abund=None, quals=None, prior=None, packed=None) -> int:
+        """Queue one sample; ``packed`` (from ``pack_sample``) skips packing.
+        The packed buffers are held until the ticket's ``wait``."""
+        pk = packed if packed is not None else _pack(seqs, abund, quals, prior)
+        cat, offs, lens, ab, qcat, pr = pk
+        t = C.c_uint64(0)
+        check(lib().dgpu_service_submit(self.h, len(lens), ptr(cat), ptr(offs), ptr(lens), ptr(ab), ptr(pr),
+                                        ptr(qcat), C.byref(t)))
+        self._live[int(t.value)] = pk
+        return int(t.value)
+
+    def wait(self, ticket: int, read_result: bool = True):
+        """(result, latency from submit to completion in s); without
+        ``read_result`` the result carries its sizes and counters only."""
+        h = C.c_void_p()
+        lat = C.c_double(0.0)
+        rc = lib().dgpu_service_wait(self.h, int(ticket), C.byref(h), C.byref(lat))
+        self._live.pop(int(ticket), None)
+        try:
+            check(rc)
+            return (_read_result(h) if read_result else _read_counters(h)), float(lat.value)
+        finally:
+            if h:
+                lib().dgpu_result_free(h)
+
+    def hold(self, held: bool = True):
+        """While held no new batch starts; what is submitted meanwhile is
+        batched together on release (``hold(False)``)."""
+        check(lib().dgpu_service_hold(self.h, int(held)))
+
+    def stats(self) -> dict:
+        b, n = C.c_uint64(0), C.c_uint64(0)
+        check(lib().dgpu_service_stats(self.h, C.byref(b), C.byref(n)))
+        return {"batches": int(b.value), "served": int(n.value)}
+
+    def close(self):
+        if self.h:
+            lib().dgpu_service_destroy(self.h)  # serves what is pending before the buffers go
+            self.h = C.c_void_p()
+            self._live.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def calc_pA(reads: int, e_reads: float, prior: bool = False) -> float:

@@ -95,6 +95,13 @@ def lib():
         L.dgpu_result_sizes.argtypes = [_P, _P]
         L.dgpu_result_fill.argtypes = [_P, C.POINTER(DadaOutC)]
         L.dgpu_result_transitions.argtypes = [_P, _P]
+        L.dgpu_service_create.argtypes = [C.c_int, C.POINTER(DadaParamsC), _P, C.c_int, C.c_uint64, _P]
+        L.dgpu_service_submit.argtypes = [_P, C.c_int, _P, _P, _P, _P, _P, _P, _P]
+        L.dgpu_service_wait.argtypes = [_P, C.c_uint64, _P, _P]
+        L.dgpu_service_stats.argtypes = [_P, _P, _P]
+        L.dgpu_service_hold.argtypes = [_P, C.c_int]
+        L.dgpu_service_destroy.argtypes = [_P]
+        L.dgpu_service_destroy.restype = None
         L.dgpu_ctx_set_lambda32.argtypes = [_P, C.c_int]
         L.dgpu_get_loglambda32.argtypes = [_P, _P]
         L.dgpu_calc_pA.argtypes = [C.c_uint32, C.c_double, C.c_int]

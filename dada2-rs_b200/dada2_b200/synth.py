@@ -249,4 +249,50 @@ def small_illumina(seed: int, nvariants=8, nreads=3000, L=150) -> Workload:
     return Workload(-1, "small Illumina parity case", [s], errm, ncol)
 
 
-CONFIGS = {0: config0, 1: config1, 2: config2}
+# fraction of reads that end up unique at each length under the Q38->Q25
+# profile (measured on this generator), used to size a request's read count
+_UNIQUE_FRAC = {150: 0.076, 250: 0.145, 1450: 0.78}
+
+
+def service_request(seed: int, L: int, target: int, nvar: int) -> Sample:
+    """One request of the service trace: an Illumina-style sample of length L
+    with about ``target`` uniques from ``nvar`` variants (the error model is the
+    service's resident 16 x 41 matrix)."""
+    rng = np.random.default_rng(seed)
+    ncol = 41
+    errm = error_matrix(ncol)
+    nreads = max(int(target / _UNIQUE_FRAC[L]), 2 * nvar)
+    s = illumina_sample(rng, nvar, nreads, L, errm, ncol)
+    s.name = f"req{seed}"
+    return s
+
+
+def config4(seed: int = 1004, nrequests: int = 48, rate: float = 20.0, workers: int | None = None) -> Workload:
+    """Denoising-service trace: Poisson arrivals at ``rate``/s; uniques per
+    request log-normal with median 5,000 (sigma 1) clipped to [1,000, 50,000];
+    lengths 150 / 250 / 1,450 nt drawn 60 / 30 / 10 %; 50-200 variants each.
+    Requests are generated in a spawn-started process pool."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    import os
+
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=nrequests))
+    arrivals -= arrivals[0]
+    lengths = rng.choice([150, 250, 1450], size=nrequests, p=[0.6, 0.3, 0.1])
+    targets = np.clip(np.rint(np.exp(rng.normal(np.log(5000.0), 1.0, size=nrequests))), 1000, 50000).astype(int)
+    nvars = rng.integers(50, 201, size=nrequests)
+    seeds = [seed * 1000 + i for i in range(nrequests)]
+    nw = workers or max(1, min(nrequests, (os.cpu_count() or 2) // 2))
+    args = list(zip(seeds, lengths.tolist(), targets.tolist(), nvars.tolist()))
+    if nw > 1:
+        with cf.ProcessPoolExecutor(nw, mp_context=mp.get_context("spawn")) as ex:
+            samples = list(ex.map(service_request, *zip(*args)))
+    else:
+        samples = [service_request(*a) for a in args]
+    return Workload(4, f"denoising service ({nrequests} requests, Poisson {rate:g}/s, 150/250/1450 nt 60/30/10%)",
+                    samples, error_matrix(41), 41,
+                    notes={"arrivals": arrivals, "lengths": lengths, "targets": targets, "rate": rate})
+
+
+CONFIGS = {0: config0, 1: config1, 2: config2, 4: config4}

@@ -213,6 +213,34 @@ int dgpu_get_loglambda32(dgpu_ctx* ctx, float* out);
  * unless `prior`. */
 double dgpu_calc_pA(uint32_t reads, double e_reads, int prior);
 
+/* ---- denoising service ----
+ * Requests (one sample each, the inputs of dgpu_dada) are submitted at any
+ * time and served on `device` by a worker thread: pending requests of the
+ * oldest request's length class (longest unique <= 200, <= 600 or longer nt)
+ * are batched in arrival order while the estimated device-memory footprint of
+ * every batch in flight fits `hbm_budget` bytes (0: half the device's free
+ * memory) and denoised together like dgpu_dada_batch, so each result is
+ * dgpu_dada's on that sample; a request completes as soon as its own sample
+ * does. DGPU_SERVICE_WORKERS (default 3) batches run at once. The
+ * input buffers stay the caller's and must remain valid until the ticket's
+ * wait returns (they are read when the request is served; a batch packs
+ * copies of its requests' uniques). dgpu_service_wait blocks until the ticket is
+ * served and returns its result (free with dgpu_result_free) and its latency
+ * from submit to completion. Destroying the service serves what is pending.
+ * No counterpart in the reference, whose per-sample fan-out is
+ * for_each_sample_concurrent (src/main.rs:4648-4697). */
+typedef struct dgpu_service dgpu_service;
+int dgpu_service_create(int device, const dgpu_dada_params* params, const double* err_mat, int ncol,
+                        uint64_t hbm_budget, dgpu_service** out);
+int dgpu_service_submit(dgpu_service* svc, int nraw, const char* seqs, const uint32_t* offs, const uint32_t* lens,
+                        const uint32_t* abund, const uint8_t* prior, const uint32_t* qual_sums, uint64_t* ticket);
+int dgpu_service_wait(dgpu_service* svc, uint64_t ticket, dgpu_result** out, double* latency_s);
+/* While held (hold != 0) the service starts no new batch; requests submitted
+ * meanwhile are batched together when it is released. */
+int dgpu_service_hold(dgpu_service* svc, int hold);
+int dgpu_service_stats(dgpu_service* svc, uint64_t* batches, uint64_t* served);
+void dgpu_service_destroy(dgpu_service* svc);
+
 /* ---- aligners alone (test entry) ----
  * which: 0 vectorized (compressed anti-diagonal i16, end_gap as given),
  *        1 ends-free with homopolymer gaps, 2 ends-free i32.

@@ -61,6 +61,31 @@ def test_gpu_entry_points_fail_loudly_without_a_device():
         D.dada_uniques(["ACGTACGTAC"], [3], np.full(16, 0.01), 1)
 
 
+def test_service_lifecycle_without_a_device():
+    """Without a GPU the service's worker fails every request with a CUDA
+    error instead of hanging, and destroy returns."""
+    import numpy as np
+
+    import dada2_b200 as D
+
+    if D.device_count() > 0:
+        pytest.skip("a GPU is present; covered by the gpu tests")
+    with pytest.raises(D.DgpuError):  # a zero budget queries the device
+        D.DenoiseService(np.full(16, 0.01), 1)
+    svc = D.DenoiseService(np.full(16, 0.01), 1, hbm_budget=1 << 30)
+    try:
+        t = None
+        try:
+            t = svc.submit(["ACGTACGTAC"], [3])
+        except D.DgpuError:
+            pass  # the worker already stopped on the missing device
+        if t is not None:
+            with pytest.raises(D.DgpuError, match="cudaSetDevice"):
+                svc.wait(t)
+    finally:
+        svc.close()
+
+
 def test_library_calc_pA_matches_the_oracle_bit_for_bit():
     """The host p-value (calc_pA, src/pval.rs:208-241) the library exports is
     the oracle's to the last bit, over both gamma branches, the log-space

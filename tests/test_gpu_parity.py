@@ -476,3 +476,72 @@ def test_fp32_log_lambda_tracks_fp64(L):
                 else:
                     assert (p32 < omega_a) == (p64 < omega_a)
         assert n_all > 0
+
+
+def _service_reqs():
+    return [synth.small_illumina(80, nvariants=5, nreads=1500, L=150).samples[0],
+            synth.small_illumina(81, nvariants=6, nreads=3000, L=150).samples[0],
+            synth.small_illumina(84, nvariants=3, nreads=500, L=140).samples[0],
+            synth.small_illumina(82, nvariants=4, nreads=900, L=250).samples[0],
+            synth.small_illumina(83, nvariants=3, nreads=400, L=700).samples[0]]
+
+
+@pytest.mark.parametrize("transitions", [False, True])
+def test_service_results_match_single_sample_calls(transitions):
+    """Requests of three length classes, submitted together, come back as the
+    single-sample path's results on each sample and the oracle's: one batch per
+    class, each request released as soon as its own sample finishes (or, with
+    transition counts, after the batch's final-subs pass)."""
+    reqs = _service_reqs()
+    w = synth.small_illumina(80)
+    err, ncol = w.err, w.ncol
+    prm = D.DadaParams(host_threads=4, transitions=transitions)
+    with D.DenoiseService(err, ncol, prm) as svc:
+        svc.hold()
+        tickets = [svc.submit(s.seqs, s.abund, quals=s.quals) for s in reqs]
+        svc.hold(False)
+        got = [svc.wait(t) for t in tickets]
+        assert svc.stats() == {"batches": 3, "served": 5}
+    for s, (g, lat) in zip(reqs, got):
+        assert lat > 0.0
+        want = D.dada_uniques(s.seqs, s.abund, err, ncol, prm, quals=s.quals)
+        assert_same_dada(g, want)
+        if transitions:
+            assert np.array_equal(g["transitions"], want["transitions"])
+        else:
+            assert_same_dada(g, O.dada(s.seqs, s.abund, err, ncol, O.DadaParams(nthreads=4), quals=s.quals))
+
+
+def test_service_isolates_an_invalid_request():
+    """An invalid request in a batch gets its own error while its batch-mates
+    are served with their single-sample results."""
+    reqs = _service_reqs()[:2]
+    w = synth.small_illumina(80)
+    bad = _S(["ACGTACGTAA" * 15, "ACGTACNTAC" * 15], [3, 2])
+    with D.DenoiseService(w.err, w.ncol, D.DadaParams()) as svc:
+        svc.hold()
+        t0 = svc.submit(reqs[0].seqs, reqs[0].abund, quals=reqs[0].quals)
+        tbad = svc.submit(bad.seqs, bad.abund, quals=bad.quals)
+        t1 = svc.submit(reqs[1].seqs, reqs[1].abund, quals=reqs[1].quals)
+        svc.hold(False)
+        got = [svc.wait(t0)[0], svc.wait(t1)[0]]
+        with pytest.raises(D.InvalidInput, match="non-ACGT"):
+            svc.wait(tbad)
+        assert svc.stats() == {"batches": 1, "served": 3}
+    for s, g in zip(reqs, got):
+        assert_same_dada(g, D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, D.DadaParams(), quals=s.quals))
+
+
+def test_service_budget_splits_batches():
+    """A device-memory budget below two requests' footprint serves them one
+    batch each, with results unchanged."""
+    reqs = [synth.small_illumina(90 + i, nvariants=4, nreads=800, L=150).samples[0] for i in range(3)]
+    w = synth.small_illumina(90, nvariants=4, nreads=800, L=150)
+    with D.DenoiseService(w.err, w.ncol, D.DadaParams(), hbm_budget=1) as svc:
+        svc.hold()
+        ts = [svc.submit(s.seqs, s.abund, quals=s.quals) for s in reqs]
+        svc.hold(False)
+        got = [svc.wait(t)[0] for t in ts]
+        assert svc.stats() == {"batches": 3, "served": 3}
+    for s, g in zip(reqs, got):
+        assert_same_dada(g, D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, D.DadaParams(), quals=s.quals))
