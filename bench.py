@@ -18,6 +18,7 @@ Multi-GPU (torchrun): samples are independent, so each rank denoises its own
 40-sample batch (seeded by rank) with no collective on the data path
 (weak scaling); timing is the max over ranks.
 
+--config 3 denoises the pooled 400,000-unique sample (see pooled_bench);
 --config 4 replays the denoising-service request trace (see service_bench).
 
 --impl reference times the CPU restatement of the reference (oracle/,
@@ -77,6 +78,8 @@ def load_workload(config: int, rank: int):
         return synth.config0(seed=1000 + 97 * rank)
     if config == 2:
         return synth.config2(seed=1002 + 97 * rank)
+    if config == 3:
+        return synth.config3(seed=1003 + 97 * rank)
     if config == 4:
         return synth.config4(seed=1004 + 97 * rank)
     raise SystemExit(f"unknown config {config}")
@@ -268,6 +271,102 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+POOLED_METRIC = "unique x center compares/s (dada compare step, pooled 200-sample Illumina, one sample)"
+
+
+def _prefix_sample(s, n):
+    from dada2_b200 import synth
+
+    return synth.Sample(s.seqs[:n], np.asarray(s.abund[:n]), s.quals[:n], 0, name=f"{s.name}[:{n}]")
+
+
+def pooled_bench(args):
+    """Pooled mode: 200 samples pooled (first-seen order) into one sample of
+    about 400,000 uniques from 3,000 variants x 150 nt, denoised by the
+    single-sample path. value: inputs resident (ResidentBatch); e2e: dgpu_dada
+    from host buffers. Also the FP32 ln(lambda) report on its first compare
+    call and the oracle on a bounded prefix. Rank 0 only."""
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    from dada2_b200 import synth
+
+    w = synth.config3(seed=1003)  # generated in a spawn pool before any GPU call
+    import torch
+
+    torch.cuda.set_device(local)
+    import dada2_b200 as D
+
+    params = dada_params(w)
+    s = w.samples[0]
+    warm = _prefix_sample(s, 20000)
+    for _ in range(max(args.warmup, 1)):
+        D.dada_uniques(warm.seqs, warm.abund, w.err, w.ncol, params, quals=warm.quals, device=local,
+                       read_result=False)
+    pb = D.PackedBatch([s])
+    D.stats_reset()
+    D.stats_timing(TIMING_EVERY)
+    clocks = ClockSampler(local)
+    clocks.start()
+    with D.ResidentBatch([s], w.err, w.ncol, params, device=local, packed=pb) as rb:
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        comps = 0
+        for _ in range(args.steps):
+            res = rb.run(read_results=False)
+            comps += res[0]["counters"]["cmp_scanned"]
+        ev1.record()
+        torch.cuda.synchronize()
+    dt = ev0.elapsed_time(ev1) / 1e3
+    D.stats_timing(False)
+    st = D.stats_read()
+    lat = D.stats_latencies()
+    pk = D.pack_sample(s.seqs, s.abund, s.quals)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    e2e_comps = 0
+    for _ in range(args.steps):
+        r = D.dada_uniques(None, None, w.err, w.ncol, params, packed=pk, device=local, read_result=False)
+        e2e_comps += r["counters"]["cmp_scanned"]
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    e2e_dt = e0.elapsed_time(e1) / 1e3
+    precision = precision_report(w, params, local)
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        sub = _prefix_sample(s, 30000)
+        c, t, cores = run_oracle([sub], w, os.cpu_count() or 1)
+        cpu = {"value": c / t, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"the first 30,000 pooled uniques as one sample ({c} compares), C++ restatement of the "
+                         f"reference (oracle/)"}
+    r0 = res[0]
+    line = {
+        "metric": POOLED_METRIC, "value": comps / dt, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * dt / max(args.steps, 1), "higher_is_better": True,
+        "scaling": "replicas only", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w.name, "uniques": len(s.seqs), "clusters": int(r0["nclust"]),
+                   "compares_per_step": int(r0["counters"]["cmp_scanned"]),
+                   "note": "one pooled sample; a step is one full denoising; warm-up on its first 20,000 uniques"},
+        "e2e": {"value": e2e_comps / e2e_dt, "unit": UNIT, "h2d_bytes_per_step": int(pb.h2d_bytes),
+                "d2h_bytes_per_step": None},
+        "pairs_per_step": {k: int(r0["counters"][k]) for k in ("screened", "aligned", "nshroud", "gapless",
+                                                                "vectorized")},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)) if len(lat) else None,
+                       "p99": float(np.percentile(lat, 99)) if len(lat) else None, "unit": "per compare call"},
+        "host_phases_s_per_step": float(r0["times"][2]),
+        "kernel_ms_per_step": {k: v * (st["rounds"] / max(st["timed_rounds"], 1)) / max(args.steps, 1)
+                               for k, v in st["ms"].items()},
+        "precision": precision,
+        "gpu_launches": int(sum(st["launches"].values())),
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
 SERVICE_METRIC = "unique x center compares/s (denoising service, Poisson 20/s request trace)"
 
 
@@ -397,6 +496,9 @@ def main():
         return
     if args.config == 4:
         service_bench(args)
+        return
+    if args.config == 3:
+        pooled_bench(args)
         return
     rank, world, local = dist_env()
     import torch

@@ -808,9 +808,55 @@ struct Cand {
   double lambda;
   uint32_t hamming;
 };
+// One bit per member position: set where the member at that position has
+// the property. Updated with the member list, so scans can skip the rest.
+struct PosBits {
+  std::vector<uint64_t> w;
+  bool get(size_t r) const { return (r >> 6) < w.size() && ((w[r >> 6] >> (r & 63)) & 1u); }
+  void put(size_t r, bool v) {
+    const size_t k = r >> 6;
+    if (k >= w.size()) {
+      if (!v) return;
+      w.resize(k + 1, 0);
+    }
+    const uint64_t m = uint64_t(1) << (r & 63);
+    w[k] = v ? (w[k] | m) : (w[k] & ~m);
+  }
+  // f(r) for every set position in [lo, hi), ascending
+  template <class F>
+  void each(size_t lo, size_t hi, F&& f) const {
+    hi = std::min(hi, w.size() * 64);
+    for (size_t k = lo >> 6; k * 64 < hi; ++k) {
+      uint64_t x = w[k];
+      if (k * 64 < lo) x &= ~uint64_t(0) << (lo & 63);
+      while (x) {
+        const size_t r = k * 64 + size_t(__builtin_ctzll(x));
+        if (r >= hi) return;
+        f(r);
+        x &= x - 1;
+      }
+    }
+  }
+};
+
+// What a reprice reads of a member, kept beside the member list (position-
+// indexed) so the scans run through memory in order: the lambda and hamming of
+// the raw's comp to its cluster's center, its reads, and its prior in the top
+// bit of hp.
+struct MemberInfo {
+  double lambda;
+  uint32_t reads;
+  uint32_t hp;
+  uint32_t hamming() const { return hp & 0x7fffffffu; }
+  bool prior() const { return (hp >> 31) != 0; }
+};
+
 struct Cluster {
   int64_t center = -1;
   std::vector<uint32_t> raws;
+  std::vector<MemberInfo> info;  // info[r] describes raws[r]
+  PosBits var;    // members that are repriced (not fixed_p)
+  PosBits multi;  // members with two or more candidate clusters
   uint32_t reads = 0;
   uint32_t nvar = 0;  // members whose p is repriced (not fixed at 1.0)
   bool update_e = true, check_locks = true;
@@ -850,6 +896,7 @@ struct SampleState {
   std::vector<Comp> rcomp;
   std::vector<double> p;
   std::vector<uint32_t> raw_cluster;
+  std::vector<uint32_t> raw_pos;  // position of each raw in its cluster's member list
   std::vector<Cluster> clusters;
   std::vector<std::vector<Cand>> cand;
   std::vector<uint32_t> ncand;   // cand[raw].size(), kept flat for the shuffle scans
@@ -862,6 +909,8 @@ struct SampleState {
   std::vector<Comp> compmax;
   std::vector<double> emax;
   std::vector<uint32_t> reads_used, dirty_list, reads_fell_list;
+  std::vector<uint32_t> changed_raws;  // raws whose best cluster changed since the last move pass
+  std::vector<uint8_t> changed_mark;
   std::vector<uint8_t> in_affected, dirty_cluster, reads_fell;
   std::vector<uint32_t> affected;
   bool built = false;
@@ -892,13 +941,21 @@ struct SampleState {
           p[t] = 1.0;
         }
     raw_cluster.assign(n, 0);
+    raw_pos.resize(n);
     cand.assign(n, {});
     ncand.assign(n, 0);
+    changed_mark.assign(n, 0);
     clusters.clear();
     Cluster c0;
     c0.birth_e = double(total_reads);
     c0.raws.resize(n);
-    for (uint32_t t = 0; t < n; ++t) c0.raws[t] = t;
+    c0.info.resize(n);
+    for (uint32_t t = 0; t < n; ++t) {
+      c0.raws[t] = t;
+      raw_pos[t] = t;
+      c0.info[t] = member_info(t);
+      if (!fixed_p[t]) c0.var.put(t, true);
+    }
     c0.reads = total_reads;
     for (uint32_t t = 0; t < n; ++t) c0.nvar += fixed_p[t] ? 0u : 1u;
     clusters.push_back(std::move(c0));
@@ -914,8 +971,23 @@ struct SampleState {
     c.center = best;
   }
 
+  MemberInfo member_info(uint32_t raw) const {
+    return MemberInfo{rcomp[raw].lambda, reads[raw], (rcomp[raw].hamming & 0x7fffffffu) | (prior[raw] ? 0x80000000u : 0u)};
+  }
+  // rcomp[raw] = cp, and the copy beside the raw's place in its cluster
+  void set_rcomp(uint32_t raw, const Comp& cp) {
+    rcomp[raw] = cp;
+    clusters[raw_cluster[raw]].info[raw_pos[raw]] = member_info(raw);
+  }
+
   void add_raw(size_t ci, uint32_t raw) {  // src/containers.rs:403-415
     raw_cluster[raw] = uint32_t(ci);
+    Cluster& c = clusters[ci];
+    const size_t pos = c.raws.size();
+    c.info.push_back(member_info(raw));
+    raw_pos[raw] = uint32_t(pos);
+    c.var.put(pos, !fixed_p[raw]);
+    c.multi.put(pos, ncand[raw] > 1);
     clusters[ci].raws.push_back(raw);
     clusters[ci].reads += reads[raw];
     clusters[ci].nvar += fixed_p[raw] ? 0u : 1u;
@@ -924,9 +996,18 @@ struct SampleState {
 
   uint32_t pop_raw(size_t ci, size_t r) {  // src/containers.rs:424-435 (swap_remove)
     std::vector<uint32_t>& v = clusters[ci].raws;
+    Cluster& c = clusters[ci];
     uint32_t raw = v[r];
+    const size_t last = v.size() - 1;
     v[r] = v.back();
     v.pop_back();
+    c.info[r] = c.info.back();
+    c.info.pop_back();
+    raw_pos[v.size() > r ? v[r] : raw] = uint32_t(r);
+    c.var.put(r, c.var.get(last));
+    c.multi.put(r, c.multi.get(last));
+    c.var.put(last, false);
+    c.multi.put(last, false);
     clusters[ci].reads -= reads[raw];
     clusters[ci].nvar -= fixed_p[raw] ? 0u : 1u;
     clusters[ci].update_e = true;
@@ -969,14 +1050,17 @@ struct SampleState {
     P.for_each_stored(t, [&](uint32_t idx, double lam, uint32_t ham) {
       const Comp cp{uint32_t(ci), idx, lam, ham};
       c.comp.push_back(cp);
-      if (ci == 0 || cp.index == center) rcomp[cp.index] = cp;
+      if (ci == 0 || cp.index == center) set_rcomp(cp.index, cp);
     });
     for (const Comp& cp : c.comp) {  // index_add_cluster
       const uint32_t raw = cp.index;
       cand[raw].push_back(Cand{uint32_t(ci), cp.lambda, cp.hamming});
       // A raw with one candidate keeps its emax implicit (see shuffle_converge);
       // on gaining a second it gets the value the eager updates would hold.
-      if (++ncand[raw] == 2 && built) emax[raw] = compmax[raw].lambda * double(reads_used[compmax[raw].i]);
+      if (++ncand[raw] == 2) {
+        clusters[raw_cluster[raw]].multi.put(raw_pos[raw], true);
+        if (built) emax[raw] = compmax[raw].lambda * double(reads_used[compmax[raw].i]);
+      }
     }
   }
 
@@ -992,25 +1076,153 @@ struct SampleState {
     BudCand bm{}, bmp{};
   };
 
-  // Members [lo, hi) of cluster bi: reprice and fold into a local cache.
+  // get_pA, answering 0.0 at once where calc_pA's log-space tail
+  // (upper_tail_direct, reached when gamma_lr's exponent ax is below -709.78
+  // and k >= e) is sure to underflow: its log is ln P(X = k) plus the log of
+  // a sum below 1 / (1 - e / (k + 1)), and ln P(X = k) = ax - ln k to within
+  // rounding; a margin of 1 in the log keeps the test on the safe side.
+  double get_pA_quick(uint32_t rd, bool pr, double lambda, uint32_t hamming, uint32_t bi_reads) const {
+    if (!(rd == 1 && !pr && !conf->detect_singletons) && hamming != 0 && lambda != 0.0) {
+      const double e = lambda * double(bi_reads);
+      const double a = double(rd);
+      if (e > 0.0 && e < 0.5 * (a + 1.0)) {
+        const double ax = a * std::log(e) - e - lgamma_of(a);
+        if (ax < -709.78271289338399 && ax - std::log(a) - std::log1p(-e / (a + 1.0)) + 1.0 < -745.2) return 0.0;
+      }
+    }
+    return get_pA(rd, pr, lambda, hamming, bi_reads);
+  }
+
+  // A floor under get_pA's value that costs one log and one exp (0.0 when
+  // there is none). get_pA's shortcuts are answered exactly. Otherwise p is at
+  // least P(X = k) for X ~ Poisson(e), k = rd: the series form of gamma_lr
+  // returns exp(ax)/a times a sum of positive terms starting at 1, the
+  // continued fraction (e > 1 and e > k) returns at least P(X >= k) less an
+  // absolute rounding of about 1e-15, and the conditioning divides by a norm
+  // of at most 1. The floor is that P(X = k) = exp(ax)/a, from gamma_lr's own
+  // exponent, lowered by 1e-9 relative; it is kept only while it is normal,
+  // and in the continued-fraction range only while it is at least 1e-5, so it
+  // stays below the computed p whatever its rounding.
+  //
+  // *zero is set where get_pA is sure to answer exactly 0.0 (then the floor
+  // is that answer): get_pA's lambda == 0, or calc_pA's log-space tail
+  // underflowing (the test of get_pA_quick, loosened so it needs no log:
+  // ax <= k * ex * ln 2 - e - lnGamma(k) for e = m * 2^ex, m in [0.5, 1);
+  // -ln k <= 0; -ln(1 - r) <= 2r for r = e / (k + 1) < 1/2).
+  double pA_floor(uint32_t rd, bool pr, double lambda, uint32_t hamming, uint32_t bi_reads, bool* zero) const {
+    *zero = false;
+    if (rd == 1 && !pr && !conf->detect_singletons) return 1.0;
+    if (hamming == 0) return 1.0;
+    if (lambda == 0.0) {
+      *zero = true;
+      return 0.0;
+    }
+    const double e = lambda * double(bi_reads);
+    if (!(e > 0.0)) return 1.0;
+    const double a = double(rd);
+    // the Poisson median is at least e - ln 2, so P(X >= k) >= 1/2 for any
+    // k <= e - ln 2 (that range is the continued fraction's or gamma_lr's 1.0)
+    if (a <= e - 0.7) return 0.49;
+    uint64_t bits;
+    std::memcpy(&bits, &e, 8);
+    const int ex = int((bits >> 52) & 0x7ffu) - 1022;  // e < 2^ex (also for subnormal e)
+    const std::vector<double>& lgt = lgamma_table();
+    const double lg = rd < lgt.size() ? lgt[rd] : lgamma_of(a);
+    const double ax_hi = a * double(ex) * 0.6931471805599453 - e - lg;
+    if (ax_hi < -711.0) {  // below gamma_lr's underflow limit: no floor above 0
+      const double r = e / (a + 1.0);
+      *zero = r < 0.5 && ax_hi + 2.0 * r + 1.0 < -745.2;
+      return 0.0;
+    }
+    const double ax = a * std::log(e) - e - lgamma_of(a);
+    if (ax < -709.78271289338399) return a < e ? 1.0 : 0.0;  // gamma_lr answers 1.0, then p >= 1.0
+    const double lb = std::exp(ax) / a;
+    if (!(lb >= 1e-300)) return 0.0;
+    if (e > 1.0 && e > a && lb < 1e-5) return 0.0;
+    return lb * (1.0 - 1e-9);
+  }
+
+  // Members [lo, hi) of cluster bi: reprice and fold into a local cache. Only
+  // the bud candidates (src/pval.rs:91-123) and cluster 0's center (the bud
+  // scan's starting p) read these p-values; the final pass prices every member
+  // again. So a candidate whose floor lies above the exact p of the candidate
+  // with the lowest floor (above both, for a prior raw) can be neither cache
+  // entry and is not priced: the cache is the one a full scan builds.
   void reprice_range(const Cluster& bi, size_t lo, size_t hi, BudAcc& acc) {
     const DadaConf& C = *conf;
     const uint32_t bi_reads = bi.reads;
-    for (size_t r = lo; r < hi; ++r) {
+    const int64_t ic = clusters[0].center;
+    const MemberInfo* info = bi.info.data();
+    auto eligible = [&](size_t r) {
+      if (r == 0) return false;
+      const MemberInfo& m = info[r];
+      if (m.reads < C.min_abund || m.hamming() < C.min_hamming) return false;
+      return C.min_fold <= 1.0 || double(m.reads) >= C.min_fold * m.lambda * double(bi_reads);
+    };
+    auto price = [&](size_t r) {
+      const MemberInfo& m = info[r];
+      return get_pA_quick(m.reads, m.prior(), m.lambda, m.hamming(), bi_reads);
+    };
+    // pass 1: floors, and the exact p of the lowest-floor candidates
+    // (a candidate known to price at exactly 0.0 sets its threshold to 0.0)
+    thread_local std::vector<uint32_t> pos;
+    thread_local std::vector<double> floor_of;
+    thread_local std::vector<uint8_t> zero_of;
+    pos.clear();
+    bi.var.each(lo, hi, [&](size_t r) { pos.push_back(uint32_t(r)); });
+    floor_of.resize(pos.size());
+    zero_of.resize(pos.size());
+    double fmin = std::numeric_limits<double>::infinity(), fminp = fmin;
+    size_t amin = 0, aminp = 0;
+    bool any = false, anyp = false, zmin = false, zminp = false;
+    for (size_t i = 0; i < pos.size(); ++i) {
+      const size_t r = pos[i];
+      if (!eligible(r)) continue;
+      const MemberInfo& m = info[r];
+      bool z = false;
+      const double f = pA_floor(m.reads, m.prior(), m.lambda, m.hamming(), bi_reads, &z);
+      floor_of[i] = f;
+      zero_of[i] = z;
+      if (!zmin && (!any || f < fmin || z)) {
+        fmin = f;
+        amin = r;
+        any = true;
+        zmin = z;
+      }
+      if (m.prior() && !zminp && (!anyp || f < fminp || z)) {
+        fminp = f;
+        aminp = r;
+        anyp = true;
+        zminp = z;
+      }
+    }
+    const double t = zmin ? 0.0 : (any ? price(amin) : 0.0);
+    const double tp = zminp ? 0.0 : (anyp ? price(aminp) : 0.0);
+    // pass 2: exact p where it can decide, folded in ascending position
+    for (size_t i = 0; i < pos.size(); ++i) {
+      const size_t r = pos[i];
       const uint32_t raw = bi.raws[r];
-      if (fixed_p[raw]) continue;
-      const double pv = get_pA(reads[raw], prior[raw] != 0, rcomp[raw].lambda, rcomp[raw].hamming, bi_reads);
+      if (!eligible(r)) {
+        if (int64_t(raw) == ic) p[raw] = price(r);
+        continue;
+      }
+      const MemberInfo& m = info[r];
+      const double f = floor_of[i];
+      const bool pr = m.prior();
+      if (f > t && (!pr || f > tp)) continue;
+      // nor can it replace the entries this scan holds so far (p >= f)
+      auto held = [&](bool have, const BudCand& b) {
+        return have && (f > b.p || (f >= b.p && m.reads <= b.reads));
+      };
+      if (held(acc.have, acc.bm) && (!pr || held(acc.havep, acc.bmp))) continue;
+      const double pv = zero_of[i] ? 0.0 : price(r);
       p[raw] = pv;
-      if (r == 0) continue;
-      if (reads[raw] < C.min_abund || rcomp[raw].hamming < C.min_hamming) continue;
-      const bool fold_ok = C.min_fold <= 1.0 || double(reads[raw]) >= C.min_fold * rcomp[raw].lambda * double(bi_reads);
-      if (!fold_ok) continue;
-      const BudCand cd{pv, reads[raw], uint32_t(r), raw};
+      const BudCand cd{pv, m.reads, uint32_t(r), raw};
       if (!acc.have || better(cd, acc.bm)) {
         acc.bm = cd;
         acc.have = true;
       }
-      if (prior[raw] && (!acc.havep || better(cd, acc.bmp))) {
+      if (pr && (!acc.havep || better(cd, acc.bmp))) {
         acc.bmp = cd;
         acc.havep = true;
       }
@@ -1024,13 +1236,14 @@ struct SampleState {
       if (bi.update_e) {
         const size_t nm = bi.raws.size();
         BudAcc acc;
-        if (bi.nvar < kParMinRepriced || nm < 2 * kRepriceGrain) {
+        const size_t grain = kRepriceGrain;
+        if (bi.nvar < kParMinRepriced || nm < 2 * grain) {
           reprice_range(bi, 0, nm, acc);
         } else {
           // chunk-local caches folded in chunk order: the same first-of-equals
           // winner as one ascending scan
-          std::vector<BudAcc> part((nm + kRepriceGrain - 1) / kRepriceGrain);
-          Helpers::get().parallel_for(nm, kRepriceGrain, [&](size_t c, size_t lo, size_t hi) {
+          std::vector<BudAcc> part((nm + grain - 1) / grain);
+          Helpers::get().parallel_for(nm, grain, [&](size_t c, size_t lo, size_t hi) {
             reprice_range(bi, lo, hi, part[c]);
           });
           for (const BudAcc& a : part) {
@@ -1077,13 +1290,17 @@ struct SampleState {
   // x <= a, Legendre continued fraction otherwise).
   // lnGamma of the integer read counts, filled once; the same lgamma_r call
   // on the same argument, so every value is the one computed on demand.
-  static double lgamma_of(double a) {
+  static const std::vector<double>& lgamma_table() {
     static const std::vector<double> table = [] {
       std::vector<double> t(size_t(1) << 16);
       int sg = 0;
       for (size_t k = 1; k < t.size(); ++k) t[k] = lgamma_r(double(k), &sg);
       return t;
     }();
+    return table;
+  }
+  static double lgamma_of(double a) {
+    const std::vector<double>& table = lgamma_table();
     if (a >= 1.0 && a < double(table.size()) && a == std::floor(a)) return table[size_t(a)];
     int sg = 0;
     return lgamma_r(a, &sg);
@@ -1234,8 +1451,8 @@ struct SampleState {
       if (best != ci) {
         if (clusters[ci].center == int64_t(raw)) continue;
         pop_raw(ci, r);
-        add_raw(best, raw);
         rcomp[raw] = compmax[raw];
+        add_raw(best, raw);
         ++moves;
       }
     }
@@ -1244,15 +1461,20 @@ struct SampleState {
 
   // src/cluster.rs:792-810. The dirty mark is an atomic test-and-set so the
   // parallel passes below can share it; `out` receives clusters newly marked.
-  void record_change_to(uint32_t raw, uint32_t new_ci, std::vector<uint32_t>& out) {
+  // A reconcile's output: clusters that hold a raw whose best changed (each
+  // once) and those raws.
+  struct DirtyOut {
+    std::vector<uint32_t> clusters, raws;
+  };
+  void record_change_to(uint32_t raw, uint32_t new_ci, DirtyOut& out) {
     if (new_ci == compmax[raw].i) return;
     const uint32_t cur = raw_cluster[raw];
-    if (!__atomic_exchange_n(&dirty_cluster[cur], uint8_t(1), __ATOMIC_RELAXED)) out.push_back(cur);
+    out.raws.push_back(raw);
+    if (!__atomic_exchange_n(&dirty_cluster[cur], uint8_t(1), __ATOMIC_RELAXED)) out.clusters.push_back(cur);
   }
-  void record_change(uint32_t raw, uint32_t new_ci) { record_change_to(raw, new_ci, dirty_list); }
 
   // Pass A2 over one changed cluster's comps [lo, hi) (src/cluster.rs:1177-1224).
-  void reconcile_a2(uint32_t ci, double rf, size_t lo, size_t hi, std::vector<uint32_t>& dirty_out) {
+  void reconcile_a2(uint32_t ci, double rf, size_t lo, size_t hi, DirtyOut& dirty_out) {
     const std::vector<Comp>& cv = clusters[ci].comp;
     for (size_t k = lo; k < hi; ++k) {
       const Comp& cp = cv[k];
@@ -1270,7 +1492,7 @@ struct SampleState {
   }
 
   // Pass B for affected raws [lo, hi): full candidate rescan (src/cluster.rs:1230-1247).
-  void reconcile_b(size_t lo, size_t hi, std::vector<uint32_t>& dirty_out) {
+  void reconcile_b(size_t lo, size_t hi, DirtyOut& dirty_out) {
     for (size_t k = lo; k < hi; ++k) {
       const uint32_t raw = affected[k];
       double be = -std::numeric_limits<double>::infinity();
@@ -1293,13 +1515,47 @@ struct SampleState {
   // newly dirtied clusters are appended in chunk order.
   template <class F>
   void par_dirty(size_t n, F&& fn) {
+    auto merge = [&](const DirtyOut& d) {
+      dirty_list.insert(dirty_list.end(), d.clusters.begin(), d.clusters.end());
+      changed_raws.insert(changed_raws.end(), d.raws.begin(), d.raws.end());
+    };
     if (n < kParMin) {
-      fn(size_t(0), n, dirty_list);
+      DirtyOut d;
+      fn(size_t(0), n, d);
+      merge(d);
       return;
     }
-    std::vector<std::vector<uint32_t>> loc((n + kParGrain - 1) / kParGrain);
+    std::vector<DirtyOut> loc((n + kParGrain - 1) / kParGrain);
     Helpers::get().parallel_for(n, kParGrain, [&](size_t c, size_t lo, size_t hi) { fn(lo, hi, loc[c]); });
-    for (auto& v : loc) dirty_list.insert(dirty_list.end(), v.begin(), v.end());
+    for (const DirtyOut& d : loc) merge(d);
+  }
+
+  // The move passes of the dirty clusters in ascending order, visiting only
+  // the raws whose best cluster changed since the last move pass: after a move
+  // pass every raw but a center sits in its best cluster and the best changes
+  // only in a reconcile, so these are the only raws a full backward scan would
+  // move. Each cluster's movers go in descending position, the full scan's
+  // order; a swap_remove brings in the last member, which is never a pending
+  // mover, and appends to later clusters leave their positions alone, so the
+  // pops and appends are exactly the full passes'.
+  size_t move_changed() {
+    std::vector<std::pair<uint64_t, uint32_t>> mv;  // (cluster << 32 | ~position, raw)
+    for (uint32_t raw : changed_raws) {
+      if (changed_mark[raw]) continue;
+      changed_mark[raw] = 1;
+      const uint32_t ci = raw_cluster[raw];
+      if (compmax[raw].i != ci && clusters[ci].center != int64_t(raw))
+        mv.push_back({(uint64_t(ci) << 32) | uint64_t(0xffffffffu - raw_pos[raw]), raw});
+    }
+    for (uint32_t raw : changed_raws) changed_mark[raw] = 0;
+    std::sort(mv.begin(), mv.end());
+    for (const auto& m : mv) {
+      const uint32_t raw = m.second;
+      pop_raw(size_t(m.first >> 32), raw_pos[raw]);
+      rcomp[raw] = compmax[raw];
+      add_raw(compmax[raw].i, raw);
+    }
+    return mv.size();
   }
 
   void grow_to(size_t nc) {
@@ -1343,11 +1599,11 @@ struct SampleState {
       } else {
         size_t moves = 0;
         if (after_reconcile) {
-          std::sort(dirty_list.begin(), dirty_list.end());
-          for (size_t k = 0; k < dirty_list.size(); ++k) moves += move_pass(dirty_list[k]);
+          moves += move_changed();
         } else {
           for (size_t ci = 0; ci < clusters.size(); ++ci) moves += move_pass(ci);
         }
+        changed_raws.clear();
         for (uint32_t ci : dirty_list) dirty_cluster[ci] = 0;
         dirty_list.clear();
         dirty_cluster.resize(clusters.size(), 0);
@@ -1379,23 +1635,14 @@ struct SampleState {
       // use, so the queue order does not matter. Long member lists are split
       // across threads.
       for (uint32_t ci : reads_fell_list) {
-        const std::vector<uint32_t>& mem = clusters[ci].raws;
-        auto a1 = [&](size_t lo, size_t hi, std::vector<uint32_t>& out) {
-          for (size_t k = lo; k < hi; ++k) {
-            const uint32_t raw = mem[k];
-            if (compmax[raw].i == ci && !in_affected[raw] && ncand[raw] > 1) {
-              in_affected[raw] = 1;
-              out.push_back(raw);
-            }
+        const Cluster& cc = clusters[ci];
+        cc.multi.each(0, cc.raws.size(), [&](size_t k) {  // members with ncand > 1
+          const uint32_t raw = cc.raws[k];
+          if (compmax[raw].i == ci && !in_affected[raw]) {
+            in_affected[raw] = 1;
+            affected.push_back(raw);
           }
-        };
-        if (mem.size() < kParMin) {
-          a1(0, mem.size(), affected);
-        } else {
-          std::vector<std::vector<uint32_t>> loc((mem.size() + kParGrain - 1) / kParGrain);
-          Helpers::get().parallel_for(mem.size(), kParGrain, [&](size_t c, size_t lo, size_t hi) { a1(lo, hi, loc[c]); });
-          for (auto& v : loc) affected.insert(affected.end(), v.begin(), v.end());
-        }
+        });
         for (size_t cj = 0; cj < clusters.size(); ++cj) {
           if (cj == ci || clusters[cj].center < 0) continue;
           const uint32_t raw = uint32_t(clusters[cj].center);
@@ -1418,13 +1665,13 @@ struct SampleState {
           continue;
         }
         const double rf = double(nr);
-        par_dirty(clusters[ci].comp.size(), [&](size_t lo, size_t hi, std::vector<uint32_t>& out) {
+        par_dirty(clusters[ci].comp.size(), [&](size_t lo, size_t hi, DirtyOut& out) {
           reconcile_a2(uint32_t(ci), rf, lo, hi, out);
         });
         reads_used[ci] = nr;
       }
       // Pass B: full rescans of the queued raws.
-      par_dirty(affected.size(), [&](size_t lo, size_t hi, std::vector<uint32_t>& out) { reconcile_b(lo, hi, out); });
+      par_dirty(affected.size(), [&](size_t lo, size_t hi, DirtyOut& out) { reconcile_b(lo, hi, out); });
       affected.clear();
       for (uint32_t ci : reads_fell_list) reads_fell[ci] = 0;
       reads_fell_list.clear();

@@ -249,6 +249,70 @@ def small_illumina(seed: int, nvariants=8, nreads=3000, L=150) -> Workload:
     return Workload(-1, "small Illumina parity case", [s], errm, ncol)
 
 
+def _pooled_part(seed: int, vmat: np.ndarray, weights: np.ndarray, nreads: int, qhi=38, qlo=25, qsd=2.0,
+                 qmin=2, qmax=41, chunk=20000):
+    """One sample of the pooled workload, dereplicated (src/derep.rs:179-185)."""
+    rng = np.random.default_rng(seed)
+    nvar, L = vmat.shape
+    vidx = rng.choice(nvar, size=nreads, p=weights)
+    prof = np.linspace(qhi, qlo, L)
+    gen = error_matrix(qmax + 1)
+    seq_rows, qual_rows = [], []
+    for lo in range(0, nreads, chunk):
+        hi = min(nreads, lo + chunk)
+        q = np.clip(np.rint(prof[None, :] + rng.normal(0.0, qsd, size=(hi - lo, L))), qmin, qmax).astype(np.int64)
+        seq_rows.extend(_apply_subs(rng, vmat[vidx[lo:hi]], q, gen, qmax + 1))
+        qual_rows.extend(q.astype(np.uint32))
+    return _derep(seq_rows, qual_rows)
+
+
+def pool_samples(parts):
+    """Pooled uniques in first-seen order over the samples in input order, each
+    sample's uniques in its derep order; counts and per-position Phred sums add
+    up (src/main.rs:1355-1398)."""
+    index, seqs, counts, quals = {}, [], [], []
+    for s_seqs, s_counts, s_quals in parts:
+        for sq, c, q in zip(s_seqs, s_counts, s_quals):
+            j = index.get(sq)
+            if j is None:
+                index[sq] = len(seqs)
+                seqs.append(sq)
+                counts.append(int(c))
+                quals.append(np.array(q, np.uint32))
+            else:
+                counts[j] += int(c)
+                quals[j] += q
+    return seqs, np.array(counts, np.uint32), quals
+
+
+def config3(seed: int = 1003, nsamples: int = 200, nvariants: int = 3000, L: int = 150,
+            reads_per_sample: int = 38000, workers: int | None = None) -> Workload:
+    """Pooled mode: 3,000 variants x 150 nt with log-normal (sigma 2) abundances,
+    200 samples of Illumina-style reads (Q38->25 + N(0,2)) dereplicated and
+    pooled in first-seen order into about 400,000 uniques. Samples are
+    generated in a spawn-started process pool."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    import os
+
+    rng = np.random.default_rng(seed)
+    vmat = np.stack(_random_variants(rng, nvariants, [L] * nvariants))
+    w = np.exp(rng.normal(0.0, 2.0, size=nvariants))
+    w /= w.sum()
+    seeds = [seed * 1000 + i for i in range(nsamples)]
+    nw = workers or max(1, min(nsamples, (os.cpu_count() or 2) // 2))
+    if nw > 1:
+        with cf.ProcessPoolExecutor(nw, mp_context=mp.get_context("spawn")) as ex:
+            parts = list(ex.map(_pooled_part, seeds, [vmat] * nsamples, [w] * nsamples,
+                                [reads_per_sample] * nsamples, chunksize=4))
+    else:
+        parts = [_pooled_part(sd, vmat, w, reads_per_sample) for sd in seeds]
+    seqs, counts, quals = pool_samples(parts)
+    s = Sample(seqs, counts, quals, nsamples * reads_per_sample, name="config3.pooled")
+    return Workload(3, f"pooled {nsamples}-sample Illumina ({nvariants} variants x {L} nt, "
+                       f"{len(seqs)} pooled uniques)", [s], error_matrix(41), 41)
+
+
 # fraction of reads that end up unique at each length under the Q38->Q25
 # profile (measured on this generator), used to size a request's read count
 _UNIQUE_FRAC = {150: 0.076, 250: 0.145, 1450: 0.78}
@@ -295,4 +359,4 @@ def config4(seed: int = 1004, nrequests: int = 48, rate: float = 20.0, workers: 
                     notes={"arrivals": arrivals, "lengths": lengths, "targets": targets, "rate": rate})
 
 
-CONFIGS = {0: config0, 1: config1, 2: config2, 4: config4}
+CONFIGS = {0: config0, 1: config1, 2: config2, 3: config3, 4: config4}
