@@ -209,6 +209,28 @@ def precision_report(w, params, device, omega_a=1e-40):
                     "(below 1e-300) it has lost its own relative precision, so those pairs are counted apart"}
 
 
+def fp32_partition(samples, w, params, device):
+    """The samples denoised twice, with FP64 lambda (the drop-in) and with
+    decisions from the FP32 compensated log-sum lambda (FP64 within 1e3x of
+    the thresholds): whether the partitions agree, and the fallback rate."""
+    import dada2_b200 as D
+
+    p32 = D.DadaParams(align=params.align, greedy=params.greedy, lambda_fp32=True)
+    t0 = time.perf_counter()
+    a = D.dada_uniques_batch(samples, w.err, w.ncol, params, device=device)
+    t1 = time.perf_counter()
+    b = D.dada_uniques_batch(samples, w.err, w.ncol, p32, device=device)
+    t2 = time.perf_counter()
+    diff = sum(int(np.count_nonzero(x["map"] != y["map"])) for x, y in zip(a, b))
+    same_n = all(x["nclust"] == y["nclust"] for x, y in zip(a, b))
+    pv = sum(y["fp32"]["pvalues"] for y in b)
+    fb = sum(y["fp32"]["fallbacks"] for y in b)
+    return {"identical": bool(diff == 0 and same_n), "raws_mapped_differently": diff,
+            "clusters_fp64": int(sum(x["nclust"] for x in a)), "clusters_fp32": int(sum(y["nclust"] for y in b)),
+            "fp32_pvalues": int(pv), "fp64_fallbacks": int(fb), "fallback_rate": fb / max(pv, 1),
+            "s_fp64": t1 - t0, "s_fp32": t2 - t1}
+
+
 def cpu_subset(samples, target=12_000_000):
     """First samples (by index) whose expected compares add up to ~target."""
     out, tot = [], 0
@@ -335,6 +357,7 @@ def pooled_bench(args):
     clk = clocks.stop()
     e2e_dt = e0.elapsed_time(e1) / 1e3
     precision = precision_report(w, params, local)
+    precision["partition"] = fp32_partition([s], w, params, local)
     cpu = None
     if world == 1 and not args.no_cpu:
         sub = _prefix_sample(s, 30000)
@@ -598,6 +621,8 @@ def main():
 
     # ---- precision variant: FP32 compensated ln(lambda) beside the FP64 product ----
     precision = precision_report(w, params, local) if rank == 0 else None
+    if precision is not None:
+        precision["partition"] = fp32_partition(w.samples, w, params, local)
 
     # ---- plain single-sample path (rank 0 only; one pass) ----
     plain = None

@@ -145,6 +145,7 @@ struct CompareLaunch {
   uint32_t* comp_index;
   double* comp_lambda;
   uint32_t* comp_ham;
+  float* comp_ll32;         // with kp.lambda32: each stored comp's FP32 ln(lambda); else null
   double* task_self;        // ntask
   // store CTAs: CTA b covers raws [store_chunk[b]*kStoreSpan, +kStoreSpan) of
   // task store_task[b]; blk_counters[b] = its counters, TC_STORED its count

@@ -386,6 +386,7 @@ struct Pool {
   // stored comps of each task, at the task's first raw (its sample's base)
   HBuf<uint32_t> comp_index, comp_ham;
   HBuf<double> comp_lambda;
+  HBuf<float> comp_ll32;  // with kp.lambda32: FP32 ln(lambda) of each stored comp
   HBuf<uint8_t> lock_host;  // pinned host copy of every lock flag
   bool has_qual = false;
   std::vector<std::unique_ptr<Slot>> slots;
@@ -394,7 +395,7 @@ struct Pool {
     slots.clear();  // each slot drains its own stream first
     if (st && cudaStreamSynchronize(st) == cudaSuccess)
       recycle_all(seq, qual, kmer8, sat, lock, status, off, len, reads, ham, knum, kidx, kcnt, e_minmax, err, lambda, loglam32,
-                  comp_index, comp_ham, comp_lambda, lock_host);
+                  comp_index, comp_ham, comp_lambda, comp_ll32, lock_host);
     if (st) cudaStreamDestroy(st);
   }
 
@@ -476,6 +477,7 @@ struct Pool {
     TRY(comp_index.alloc(n));
     TRY(comp_ham.alloc(n));
     TRY(comp_lambda.alloc(n));
+    if (kp.lambda32) TRY(comp_ll32.alloc(n));
     TRY(lock_host.alloc(n));
     std::memset(lock_host.h, 0, n);
     if (has_qual) {
@@ -579,7 +581,10 @@ void Slot::for_each_stored(uint32_t t, F&& f) const {
   for (uint32_t b = 0; b < nb; ++b) {
     const uint32_t cnt = blk_counters.h[size_t(task_blk0[t] + b) * TC_NCOUNTERS + TC_STORED];
     const uint32_t o = T.out_off + b * uint32_t(kStoreSpan);
-    for (uint32_t k = 0; k < cnt; ++k) f(P->comp_index.h[o + k], P->comp_lambda.h[o + k], P->comp_ham.h[o + k]);
+    const float* ll = P->kp.lambda32 && P->comp_ll32.h ? P->comp_ll32.h + o : nullptr;
+    for (uint32_t k = 0; k < cnt; ++k)
+      f(P->comp_index.h[o + k], P->comp_lambda.h[o + k], P->comp_ham.h[o + k],
+        ll ? ll[k] : std::numeric_limits<float>::quiet_NaN());
   }
 }
 
@@ -640,6 +645,7 @@ int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
   L.comp_index = Q.comp_index.d;
   L.comp_lambda = Q.comp_lambda.d;
   L.comp_ham = Q.comp_ham.d;
+  L.comp_ll32 = Q.kp.lambda32 && Q.comp_ll32.h ? Q.comp_ll32.d : nullptr;
   L.task_self = task_self.d;
   L.store_task = reinterpret_cast<const uint32_t*>(dpack.p + o_map);
   L.store_chunk = L.store_task + nblk;
@@ -866,6 +872,7 @@ struct Cluster {
   double birth_pval = 0.0, birth_fold = 1.0, birth_e = 0.0;
   Comp birth_comp;
   std::vector<Comp> comp;
+  std::vector<double> comp64;  // with DadaConf::fp32: the FP64 lambda of each comp
   bool has_bm = false, has_bmp = false;
   BudCand bm{}, bmp{};
 };
@@ -885,6 +892,7 @@ struct DadaConf {
   bool detect_singletons, greedy;
   uint32_t min_hamming, min_abund;
   size_t max_clust;
+  bool fp32 = false;  // decisions from the FP32 lambda, FP64 near the thresholds
 };
 
 struct SampleState {
@@ -910,6 +918,8 @@ struct SampleState {
   std::vector<double> emax;
   std::vector<uint32_t> reads_used, dirty_list, reads_fell_list;
   std::vector<uint32_t> changed_raws;  // raws whose best cluster changed since the last move pass
+  std::vector<uint32_t> touched_list;  // clusters whose member list changed since the last pass A2
+  std::vector<uint8_t> touched;
   std::vector<uint8_t> changed_mark;
   std::vector<uint8_t> in_affected, dirty_cluster, reads_fell;
   std::vector<uint32_t> affected;
@@ -980,7 +990,16 @@ struct SampleState {
     clusters[raw_cluster[raw]].info[raw_pos[raw]] = member_info(raw);
   }
 
+  void touch(size_t ci) {
+    if (ci >= touched.size()) touched.resize(std::max(ci + 1, clusters.size()), 0);
+    if (!touched[ci]) {
+      touched[ci] = 1;
+      touched_list.push_back(uint32_t(ci));
+    }
+  }
+
   void add_raw(size_t ci, uint32_t raw) {  // src/containers.rs:403-415
+    touch(ci);
     raw_cluster[raw] = uint32_t(ci);
     Cluster& c = clusters[ci];
     const size_t pos = c.raws.size();
@@ -995,6 +1014,7 @@ struct SampleState {
   }
 
   uint32_t pop_raw(size_t ci, size_t r) {  // src/containers.rs:424-435 (swap_remove)
+    touch(ci);
     std::vector<uint32_t>& v = clusters[ci].raws;
     Cluster& c = clusters[ci];
     uint32_t raw = v[r];
@@ -1047,9 +1067,15 @@ struct SampleState {
     c.comp.clear();
     c.comp.reserve(ns);
     const uint32_t center = uint32_t(c.center);
-    P.for_each_stored(t, [&](uint32_t idx, double lam, uint32_t ham) {
-      const Comp cp{uint32_t(ci), idx, lam, ham};
+    c.comp64.clear();
+    const bool fp32 = conf->fp32;
+    P.for_each_stored(t, [&](uint32_t idx, double lam, uint32_t ham, float ll32) {
+      // with fp32 the decisions take exp of the FP32 log-sum; the FP64
+      // product is kept beside for the threshold fallback
+      const double ld = !fp32 || lam == 0.0 ? lam : std::exp(double(ll32));
+      const Comp cp{uint32_t(ci), idx, ld, ham};
       c.comp.push_back(cp);
+      if (fp32) c.comp64.push_back(lam);
       if (ci == 0 || cp.index == center) set_rcomp(cp.index, cp);
     });
     for (const Comp& cp : c.comp) {  // index_add_cluster
@@ -1148,7 +1174,61 @@ struct SampleState {
   // again. So a candidate whose floor lies above the exact p of the candidate
   // with the lowest floor (above both, for a prior raw) can be neither cache
   // entry and is not priced: the cache is the one a full scan builds.
+  // ---- FP32 lambda decisions (DadaConf::fp32) ----
+  std::atomic<uint64_t> fp32_evals{0}, fp32_fallbacks{0};
+  static bool near_threshold(double pv, double omega) { return pv >= omega * 1e-3 && pv <= omega * 1e3; }
+  // The FP64 lambda of raw's comp to its cluster's center: the comps of a
+  // cluster are in ascending raw order.
+  double lambda64_of(uint32_t raw) const {
+    const Comp& rc = rcomp[raw];
+    const Cluster& c = clusters[rc.i];
+    auto it = std::lower_bound(c.comp.begin(), c.comp.end(), raw,
+                               [](const Comp& x, uint32_t v) { return x.index < v; });
+    if (it == c.comp.end() || it->index != raw || c.comp64.empty()) return rc.lambda;
+    return c.comp64[size_t(it - c.comp.begin())];
+  }
+  // get_pA of a member with the FP32 lambda, repriced from the FP64 product
+  // where the bud would test it within 1e3x of omega_a (p times the raws) or,
+  // for a prior raw, of omega_p.
+  double price_fp32(uint32_t raw, uint32_t bi_reads) {
+    const DadaConf& C = *conf;
+    const bool pr = prior[raw] != 0;
+    double pv = get_pA(reads[raw], pr, rcomp[raw].lambda, rcomp[raw].hamming, bi_reads);
+    fp32_evals.fetch_add(1, std::memory_order_relaxed);
+    if (near_threshold(pv * double(n), C.omega_a) || (pr && near_threshold(pv, C.omega_p))) {
+      pv = get_pA(reads[raw], pr, lambda64_of(raw), rcomp[raw].hamming, bi_reads);
+      fp32_fallbacks.fetch_add(1, std::memory_order_relaxed);
+    }
+    return pv;
+  }
+  // The plain scan (every member priced), for the FP32 decisions.
+  void reprice_range_fp32(const Cluster& bi, size_t lo, size_t hi, BudAcc& acc) {
+    const DadaConf& C = *conf;
+    const uint32_t bi_reads = bi.reads;
+    bi.var.each(lo, hi, [&](size_t r) {
+      const uint32_t raw = bi.raws[r];
+      const double pv = price_fp32(raw, bi_reads);
+      p[raw] = pv;
+      if (r == 0) return;
+      if (reads[raw] < C.min_abund || rcomp[raw].hamming < C.min_hamming) return;
+      if (!(C.min_fold <= 1.0 || double(reads[raw]) >= C.min_fold * rcomp[raw].lambda * double(bi_reads))) return;
+      const BudCand cd{pv, reads[raw], uint32_t(r), raw};
+      if (!acc.have || better(cd, acc.bm)) {
+        acc.bm = cd;
+        acc.have = true;
+      }
+      if (prior[raw] && (!acc.havep || better(cd, acc.bmp))) {
+        acc.bmp = cd;
+        acc.havep = true;
+      }
+    });
+  }
+
   void reprice_range(const Cluster& bi, size_t lo, size_t hi, BudAcc& acc) {
+    if (conf->fp32) {
+      reprice_range_fp32(bi, lo, hi, acc);
+      return;
+    }
     const DadaConf& C = *conf;
     const uint32_t bi_reads = bi.reads;
     const int64_t ic = clusters[0].center;
@@ -1585,6 +1665,8 @@ struct SampleState {
         }
       }
       for (size_t ci = 0; ci < clusters.size(); ++ci) reads_used[ci] = clusters[ci].reads;
+      for (uint32_t ci : touched_list) touched[ci] = 0;
+      touched_list.clear();
       built = true;
     } else {
       grow_to(clusters.size());
@@ -1611,9 +1693,12 @@ struct SampleState {
         ++nshuffle;
         if (moves == 0 || nshuffle >= max_shuffle) break;
       }
+      // Only clusters whose member list changed since the last pass A2 can
+      // hold reads other than reads_used (A2 brings every other one level).
       reads_fell.resize(clusters.size(), 0);
-      for (size_t ci = 0; ci < reads_used.size(); ++ci) {
-        if (clusters[ci].reads < reads_used[ci] && !reads_fell[ci]) {
+      std::sort(touched_list.begin(), touched_list.end());
+      for (uint32_t ci : touched_list) {
+        if (ci < reads_used.size() && clusters[ci].reads < reads_used[ci] && !reads_fell[ci]) {
           reads_fell[ci] = 1;
           reads_fell_list.push_back(uint32_t(ci));
         }
@@ -1643,21 +1728,24 @@ struct SampleState {
             affected.push_back(raw);
           }
         });
+      }
+      // the centers of other clusters whose best is a cluster that lost reads
+      if (!reads_fell_list.empty())
         for (size_t cj = 0; cj < clusters.size(); ++cj) {
-          if (cj == ci || clusters[cj].center < 0) continue;
+          if (clusters[cj].center < 0) continue;
           const uint32_t raw = uint32_t(clusters[cj].center);
-          if (compmax[raw].i == ci && !in_affected[raw]) {
+          const uint32_t bi = compmax[raw].i;
+          if (bi != cj && reads_fell[bi] && !in_affected[raw]) {
             in_affected[raw] = 1;
             affected.push_back(raw);
           }
         }
-      }
       // Pass A2: changed clusters in ascending order. A cluster whose reads
       // fell changes nothing here: every raw whose best it is was queued by A1
       // and is skipped, and for any other raw e = lambda * reads only dropped
       // below an emax that already held it (ties already went to the smaller
       // index), so its scan is left out.
-      for (size_t ci = 0; ci < clusters.size(); ++ci) {
+      for (uint32_t ci : touched_list) {
         const uint32_t nr = clusters[ci].reads;
         if (nr == reads_used[ci]) continue;
         if (nr < reads_used[ci]) {
@@ -1670,6 +1758,8 @@ struct SampleState {
         });
         reads_used[ci] = nr;
       }
+      for (uint32_t ci : touched_list) touched[ci] = 0;
+      touched_list.clear();
       // Pass B: full rescans of the queued raws.
       par_dirty(affected.size(), [&](size_t lo, size_t hi, DirtyOut& out) { reconcile_b(lo, hi, out); });
       affected.clear();
@@ -2007,6 +2097,7 @@ struct dgpu_result {
   std::vector<uint8_t> cl_seq;
   uint64_t counters[16] = {0};
   double times[6] = {0};
+  uint64_t fp32[2] = {0, 0};          // FP32-lambda p-values, FP64 fallbacks among them
   std::vector<uint32_t> transitions;  // 16 x tncol when requested
   int tncol = 0;
 };
@@ -2038,6 +2129,13 @@ static dgpu_result* finish(SampleState& S, const SampleSeqs& in) {
         ok = true;
       } else {
         pv = SampleState::calc_pA(S.reads[raw], S.rcomp[raw].lambda * double(c.reads), true);
+        if (S.conf->fp32) {  // the map decision near omega_c from the FP64 product
+          S.fp32_evals.fetch_add(1, std::memory_order_relaxed);
+          if (SampleState::near_threshold(pv, S.conf->omega_c)) {
+            pv = SampleState::calc_pA(S.reads[raw], S.lambda64_of(raw) * double(c.reads), true);
+            S.fp32_fallbacks.fetch_add(1, std::memory_order_relaxed);
+          }
+        }
         ok = pv >= S.conf->omega_c;
       }
       S.p[raw] = pv;
@@ -2085,6 +2183,8 @@ static dgpu_result* finish(SampleState& S, const SampleSeqs& in) {
   R->times[3] = st.t_wait;
   R->times[4] = st.t_slot_wait;
   R->times[5] = st.t_job_wait;
+  R->fp32[0] = S.fp32_evals.load();
+  R->fp32[1] = S.fp32_fallbacks.load();
   return R;
 }
 
@@ -2311,7 +2411,8 @@ static int batch_prepare(Batch& B, int device, const dgpu_dada_params* prm, int 
   int ncol2 = ncol;
   std::vector<double> err = qsums ? extend_err(errm, ncol, B.E.qmax, ncol2)
                                   : std::vector<double>(errm, errm + 16 * size_t(ncol));
-  const KParams kp = to_kparams(prm->align, prm->use_quals, prm->greedy, ncol2);
+  KParams kp = to_kparams(prm->align, prm->use_quals, prm->greedy, ncol2);
+  kp.lambda32 = prm->lambda_fp32 ? 1 : 0;
   TRY(B.pool.upload(uint32_t(B.E.off.size()), B.E.seq, B.E.off.data(), B.E.len.data(), B.E.qual, B.E.reads.data(), kp,
                     err.data()));
   B.conf.omega_a = prm->omega_a;
@@ -2321,6 +2422,7 @@ static int batch_prepare(Batch& B, int device, const dgpu_dada_params* prm, int 
   B.conf.kdist_cutoff = prm->align.kdist_cutoff;
   B.conf.detect_singletons = prm->detect_singletons != 0;
   B.conf.greedy = prm->greedy != 0;
+  B.conf.fp32 = prm->lambda_fp32 != 0;
   B.conf.min_hamming = prm->min_hamming;
   B.conf.min_abund = prm->min_abund;
   B.confs.assign(static_cast<size_t>(nsamples), B.conf);
@@ -2658,7 +2760,7 @@ int dgpu_compare_store(dgpu_ctx* ctx, int center, int cluster_i, double kdist_cu
   uint32_t ctr[TC_NCOUNTERS];
   P.task_counters(0, ctr);
   uint32_t k = 0;
-  P.for_each_stored(0, [&](uint32_t idx, double lam, uint32_t ham) {
+  P.for_each_stored(0, [&](uint32_t idx, double lam, uint32_t ham, float) {
     if (comp_index) comp_index[k] = idx;
     if (comp_lambda) comp_lambda[k] = lam;
     if (comp_hamming) comp_hamming[k] = ham;
@@ -2754,6 +2856,13 @@ int dgpu_result_sizes(const dgpu_result* r, int64_t* sizes) {
   sizes[1] = int64_t(r->nraw);
   sizes[2] = int64_t(r->mem_raw.size());
   sizes[3] = int64_t(r->cl_seq.size());
+  return 0;
+}
+
+int dgpu_result_fp32_stats(const dgpu_result* r, uint64_t* out2) {
+  if (!r || !out2) return fail(DGPU_E_INVALID, "null argument");
+  out2[0] = r->fp32[0];
+  out2[1] = r->fp32[1];
   return 0;
 }
 

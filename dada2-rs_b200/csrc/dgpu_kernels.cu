@@ -2187,6 +2187,7 @@ __global__ void __launch_bounds__(kStoreThreads) k_store(CompareLaunch L) {
       L.comp_index[o] = r0 + q;
       L.comp_lambda[o] = lam[q];
       L.comp_ham[o] = (ham[q] == 0xffffffffu) ? 0u : ham[q];
+      if (L.comp_ll32) L.comp_ll32[o] = L.pool.res_loglam32[T.base + r0 + q];
     }
   }
   c_scr = __reduce_add_sync(FULL, c_scr);

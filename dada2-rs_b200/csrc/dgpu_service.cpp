@@ -133,11 +133,11 @@ struct dgpu_service {
         std::unique_lock<std::mutex> lk(mu);
         cv_work.wait(lk, [&] { return (stop && pending.empty()) || take(batch, used); });
         if (batch.empty()) return;  // stop requested and nothing left
+        batches += 1;  // counted when taken: every batch is, before its requests complete
       }
       serve(batch);
       std::lock_guard<std::mutex> g(mu);
       in_flight -= used;
-      batches += 1;
       cv_work.notify_all();
     }
   }

@@ -72,12 +72,15 @@ class DadaParams:
     greedy: bool = True
     host_threads: int = 0
     transitions: bool = False  # also return DadaAux.transitions (src/error.rs:194-249)
+    # decisions from the FP32 compensated log-sum lambda, FP64 within 1e3x of the thresholds
+    lambda_fp32: bool = False
 
     def c(self) -> DadaParamsC:
         return DadaParamsC(self.align.c(), float(self.omega_a), float(self.omega_p), float(self.omega_c),
                            int(bool(self.detect_singletons)), int(self.max_clust), float(self.min_fold),
                            int(self.min_hamming), int(self.min_abund), int(bool(self.use_quals)),
-                           int(bool(self.greedy)), int(self.host_threads), int(bool(self.transitions)))
+                           int(bool(self.greedy)), int(self.host_threads), int(bool(self.transitions)),
+                           int(bool(self.lambda_fp32)))
 
 
 def _counters(c: CountersC) -> dict:
@@ -209,6 +212,9 @@ def _read_result(h) -> dict:
     res["pvals"] = a["pvals"][:nraw]
     res["counters"] = {k: int(v) for k, v in zip(COUNTER_KEYS, a["counters"])}
     res["clusters"] = ClusterList(a, ncl)
+    f32 = np.zeros(2, np.uint64)
+    check(lib().dgpu_result_fp32_stats(h, ptr(f32)))
+    res["fp32"] = {"pvalues": int(f32[0]), "fallbacks": int(f32[1])}
     tncol = lib().dgpu_result_transitions(h, None)
     if tncol > 0:
         tr = np.zeros(16 * tncol, np.uint32)

@@ -44,7 +44,7 @@ class DadaParamsC(C.Structure):
         ("omega_c", C.c_double), ("detect_singletons", C.c_int32), ("max_clust", C.c_int32),
         ("min_fold", C.c_double), ("min_hamming", C.c_uint32), ("min_abund", C.c_uint32),
         ("use_quals", C.c_int32), ("greedy", C.c_int32), ("host_threads", C.c_int32),
-        ("transitions", C.c_int32),
+        ("transitions", C.c_int32), ("lambda_fp32", C.c_int32),
     ]
 
 
@@ -95,6 +95,7 @@ def lib():
         L.dgpu_result_sizes.argtypes = [_P, _P]
         L.dgpu_result_fill.argtypes = [_P, C.POINTER(DadaOutC)]
         L.dgpu_result_transitions.argtypes = [_P, _P]
+        L.dgpu_result_fp32_stats.argtypes = [_P, _P]
         L.dgpu_service_create.argtypes = [C.c_int, C.POINTER(DadaParamsC), _P, C.c_int, C.c_uint64, _P]
         L.dgpu_service_submit.argtypes = [_P, C.c_int, _P, _P, _P, _P, _P, _P, _P]
         L.dgpu_service_wait.argtypes = [_P, C.c_uint64, _P, _P]

@@ -61,6 +61,12 @@ typedef struct {
   int32_t host_threads; /* threads for the host phases of dgpu_dada_batch; 0 = half the cores */
   int32_t transitions;  /* 1: also count transitions by quality after the final-subs pass
                            (DadaAux.transitions, src/dada.rs:609-673, src/error.rs:194-249) */
+  int32_t lambda_fp32;  /* 1: decisions take lambda from its compensated FP32 log-sum,
+                           except that any p-value within 1e3x of omega_a (times the
+                           raws, as the bud tests it), omega_p (prior raws) or omega_c
+                           (the final map) is repriced from the FP64 product; the
+                           store's e_minmax bound stays FP64. Not in the reference:
+                           a precision variant, compared against the FP64 default. */
 } dgpu_dada_params;
 
 /* Counters of one compare call (CompareTiming's denominators, src/cluster.rs:190-231). */
@@ -229,6 +235,10 @@ double dgpu_calc_pA(uint32_t reads, double e_reads, int prior);
  * from submit to completion. Destroying the service serves what is pending.
  * No counterpart in the reference, whose per-sample fan-out is
  * for_each_sample_concurrent (src/main.rs:4648-4697). */
+/* With lambda_fp32: [0] p-values priced from the FP32 lambda, [1] of those
+ * repriced from the FP64 product (the fallback). Zero otherwise. */
+int dgpu_result_fp32_stats(const dgpu_result* res, uint64_t* out2);
+
 typedef struct dgpu_service dgpu_service;
 int dgpu_service_create(int device, const dgpu_dada_params* params, const double* err_mat, int ncol,
                         uint64_t hbm_budget, dgpu_service** out);

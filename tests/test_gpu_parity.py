@@ -545,3 +545,26 @@ def test_service_budget_splits_batches():
         assert svc.stats() == {"batches": 3, "served": 3}
     for s, g in zip(reqs, got):
         assert_same_dada(g, D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, D.DadaParams(), quals=s.quals))
+
+
+@pytest.mark.parametrize("seed", [21, 22, 23, 1000])
+def test_fp32_lambda_decisions_keep_the_partition(seed):
+    """Decisions from the FP32 compensated log-sum lambda (FP64 within 1e3x of
+    the thresholds) give the FP64 drop-in's partition: the same clusters, the
+    same map, member lambdas within 1e-4 relative where the FP64 lambda is
+    normal."""
+    w = synth.config0() if seed == 1000 else synth.small_illumina(seed)
+    s = w.samples[0]
+    a = D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, D.DadaParams(), quals=s.quals)
+    b = D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, D.DadaParams(lambda_fp32=True), quals=s.quals)
+    assert a["fp32"] == {"pvalues": 0, "fallbacks": 0}
+    assert b["fp32"]["pvalues"] > 0
+    assert b["nclust"] == a["nclust"]
+    assert np.array_equal(b["map"], a["map"])
+    for ga, gb in zip(a["clusters"], b["clusters"]):
+        assert np.array_equal(ga["sequence"], gb["sequence"])
+        assert np.array_equal(np.sort(ga["members"]), np.sort(gb["members"]))
+        la = ga["lambdas"][np.argsort(ga["members"])]
+        lb = gb["lambdas"][np.argsort(gb["members"])]
+        normal = la > 1e-300
+        assert np.all(np.abs(lb[normal] - la[normal]) <= 1e-4 * la[normal])
