@@ -690,6 +690,12 @@ def main():
         "host_phases_s_per_step": {"critical_sample": float(max(r["times"][2] for r in res)),
                                    "all_samples": float(sum(r["times"][2] for r in res)),
                                    "note": "shuffle + p-update + bud on the host, last timed step"},
+        "last_sample": (lambda r: {"uniques": int(r["nraw"]), "done_s": float(r["times"][1]),
+                                   "compare_s": float(r["times"][0]), "host_s": float(r["times"][2]),
+                                   "slot_wait_s": float(r["times"][4]), "job_wait_s": float(r["times"][5]),
+                                   "note": "the sample that finished last in the last timed step: its time "
+                                           "in compare calls, host phases, waiting for a launch slot and "
+                                           "waiting for a host thread"})(max(res, key=lambda r: r["times"][1])),
         "final_subs": final_subs,
         "precision": precision,
         "gpu_launches": launches,
