@@ -237,11 +237,13 @@ def screen_roofline(w, params, device, calls=8):
         m = np.concatenate([m, np.repeat(m[:, -1:], qmax + 1 - w.ncol, axis=1)], axis=1)
     with D.CompareContext(params.align, m.ravel().copy(), m.shape[1], device=device) as ctx:
         ctx.upload(codes, reads, quals=quals)
-        ctx.compare(centers[0], params.align.kdist_cutoff)  # warm-up
+        # compare + store, so the library counts the screened pairs (the
+        # algorithmic bytes) from the store's counters
+        ctx.b_compare_parallel(centers[0], 0, params.align.kdist_cutoff)  # warm-up
         D.stats_reset()
         D.stats_timing(1)
-        for c in centers:
-            ctx.compare(c, params.align.kdist_cutoff)
+        for k, c in enumerate(centers):
+            ctx.b_compare_parallel(c, k + 1, params.align.kdist_cutoff)
         D.stats_timing(False)
         st = D.stats_read()
     ms = st["ms"]["screen"]

@@ -990,6 +990,21 @@ struct SampleState {
     clusters[raw_cluster[raw]].info[raw_pos[raw]] = member_info(raw);
   }
 
+  // Frees the per-raw state; batch_run calls it for all samples in parallel
+  // rather than leaving hundreds of thousands of small frees to one thread.
+  void release() {
+    std::vector<std::vector<Cand>>().swap(cand);
+    std::vector<Cluster>().swap(clusters);
+    std::vector<Comp>().swap(rcomp);
+    std::vector<Comp>().swap(compmax);
+    std::vector<double>().swap(emax);
+    std::vector<double>().swap(p);
+    std::vector<uint32_t>().swap(raw_cluster);
+    std::vector<uint32_t>().swap(raw_pos);
+    std::vector<uint32_t>().swap(ncand);
+    std::vector<uint8_t>().swap(fixed_p);
+  }
+
   void touch(size_t ci) {
     if (ci >= touched.size()) touched.resize(std::max(ci + 1, clusters.size()), 0);
     if (!touched[ci]) {
@@ -2522,6 +2537,20 @@ static int final_subs(Batch& B, std::vector<SampleState>& S, dgpu_result** out) 
 // is finished, while others still run; the result then belongs to on_done's
 // owner and out[s] stays null. With transition counts requested every result
 // goes out at the end, after the final-subs pass.
+// fn(s) for every sample s < ns, on up to one thread per core.
+template <class F>
+static void for_samples(size_t ns, F&& fn) {
+  std::atomic<size_t> next{0};
+  auto work = [&] {
+    for (size_t s; (s = next.fetch_add(1)) < ns;) fn(s);
+  };
+  const size_t nt = std::min<size_t>(ns, std::max(1u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> th;
+  for (size_t t = 1; t < nt; ++t) th.emplace_back(work);
+  work();
+  for (auto& t : th) t.join();
+}
+
 static int batch_run(Batch& B, dgpu_result** out, const std::function<void(size_t, dgpu_result*)>& on_done = {}) {
   const size_t ns = B.counts.size();
   Pool& P = B.pool;
@@ -2531,9 +2560,10 @@ static int batch_run(Batch& B, dgpu_result** out, const std::function<void(size_
   CUDA_TRY(cudaMemsetAsync(P.lock.p, 0, P.nraw, P.st));
   CUDA_TRY(cudaStreamSynchronize(P.st));  // the launch slots run on their own streams
   std::vector<SampleState> S(ns);
-  for (size_t s = 0; s < ns; ++s)
+  for_samples(ns, [&](size_t s) {
     S[s].init(B.counts[s], B.bases[s], B.E.reads.data() + B.bases[s], B.E.prior.data() + B.bases[s],
               P.lock_host.h + B.bases[s], &B.confs[s]);
+  });
   const bool early = on_done && !B.transitions;
   std::vector<uint8_t> released(ns, 0);
   std::function<void(size_t)> on_finish;
@@ -2546,18 +2576,13 @@ static int batch_run(Batch& B, dgpu_result** out, const std::function<void(size_
     };
   TRY(run_samples(P, S, B.align, B.host_threads, on_finish));
   // final p-values and result tables, samples in parallel
-  std::atomic<size_t> next{0};
-  auto work = [&] {
-    for (size_t s; (s = next.fetch_add(1)) < ns;)
-      if (!released[s])
-        out[s] = finish(S[s], SampleSeqs{B.E.seq, B.E.off.data() + B.bases[s], B.E.len.data() + B.bases[s]});
-  };
-  const size_t nt = std::min<size_t>(ns, std::max(1u, std::thread::hardware_concurrency()));
-  std::vector<std::thread> th;
-  for (size_t t = 1; t < nt; ++t) th.emplace_back(work);
-  work();
-  for (auto& t : th) t.join();
-  if (B.transitions) TRY(final_subs(B, S, out));
+  for_samples(ns, [&](size_t s) {
+    if (!released[s])
+      out[s] = finish(S[s], SampleSeqs{B.E.seq, B.E.off.data() + B.bases[s], B.E.len.data() + B.bases[s]});
+  });
+  const int rc = B.transitions ? final_subs(B, S, out) : 0;
+  for_samples(ns, [&](size_t s) { S[s].release(); });
+  if (rc) return rc;
   if (on_done && !early)
     for (size_t s = 0; s < ns; ++s) {
       on_done(s, out[s]);
