@@ -730,6 +730,7 @@ def main():
                      "screen_ms_per_step": screen_ms * scale / args.steps,
                      "timed_launches": st["timed_rounds"], "of_launches": st["rounds"]},
         "kernel_ms_per_step": {k: v * scale / args.steps for k, v in st["ms"].items()},
+        "batch_run_ms_per_step": {k: v / args.steps for k, v in st["batch_ms"].items()},
         "pairs_per_step": mix,
         "nw": {"cells_per_step": nw_cells,
                "gcups": (nw_cells / (st["ms"]["align"] * scale / args.steps / 1e3) / 1e9)

@@ -2562,6 +2562,7 @@ static void for_samples(size_t ns, F&& fn) {
 static int batch_run(Batch& B, dgpu_result** out, const std::function<void(size_t, dgpu_result*)>& on_done = {}) {
   const size_t ns = B.counts.size();
   Pool& P = B.pool;
+  const auto tb0 = Clock::now();
   CUDA_TRY(cudaSetDevice(P.device));
   TRY(P.reset_e_minmax());
   std::memset(P.lock_host.h, 0, P.nraw);
@@ -2582,7 +2583,9 @@ static int batch_run(Batch& B, dgpu_result** out, const std::function<void(size_
       released[s] = 1;
       on_done(s, R);
     };
+  const auto tb1 = Clock::now();
   TRY(run_samples(P, S, B.align, B.host_threads, on_finish));
+  const auto tb2 = Clock::now();
   // final p-values and result tables, samples in parallel
   for_samples(ns, [&](size_t s) {
     if (!released[s])
@@ -2590,6 +2593,12 @@ static int batch_run(Batch& B, dgpu_result** out, const std::function<void(size_
   });
   const int rc = B.transitions ? final_subs(B, S, out) : 0;
   for_samples(ns, [&](size_t s) { S[s].release(); });
+  {
+    std::lock_guard<std::mutex> g(g_stats.mu);
+    g_stats.s.batch_ms[0] += 1e3 * secs(tb0, tb1);
+    g_stats.s.batch_ms[1] += 1e3 * secs(tb1, tb2);
+    g_stats.s.batch_ms[2] += 1e3 * secs(tb2, Clock::now());
+  }
   if (rc) return rc;
   if (on_done && !early)
     for (size_t s = 0; s < ns; ++s) {

@@ -128,6 +128,8 @@ typedef struct {
   uint64_t rounds, compares, screened, screen_bytes;
   uint64_t timed_rounds, timed_screen_bytes, timed_compares;
   uint64_t h2d_bytes;  /* host-to-device bytes copied: uploads, lock flags, per-call task tables */
+  double batch_ms[3];  /* wall time of dgpu_batch_run / dgpu_dada_batch runs: before the loop
+                          (resets, sample state), the loop, after it (results, final-subs) */
 } dgpu_kernel_stats;
 
 const char* dgpu_last_error(void);
