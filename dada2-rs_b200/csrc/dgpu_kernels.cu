@@ -2244,7 +2244,16 @@ void launch_compare(const CompareLaunch& L, cudaStream_t st, cudaEvent_t* ev) {
   }
   if (ev) cudaEventRecord(ev[1], st);
   const size_t asm_ = err_smem_bytes(L.kp.ncol) + size_t(kNwWarps) * align_smem_per_warp(L.geom);
-  if (asm_ > 48 * 1024) cudaFuncSetAttribute(k_align, cudaFuncAttributeMaxDynamicSharedMemorySize, int(asm_));
+  if (asm_ > 48 * 1024) {  // raise the dynamic shared-memory limit only when a launch needs more
+    static std::atomic<int> limit[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::atomic<int>& lim = limit[dev & 63];
+    if (int(asm_) > lim.load(std::memory_order_relaxed)) {
+      cudaFuncSetAttribute(k_align, cudaFuncAttributeMaxDynamicSharedMemorySize, int(asm_));
+      lim.store(int(asm_), std::memory_order_relaxed);
+    }
+  }
   {  // ask for the largest shared-memory carveout once per device so that
      // kAlignCtasPerSm CTAs fit beside each other
     static std::atomic<uint64_t> carved{0};
