@@ -2142,9 +2142,19 @@ static dgpu_result* finish(SampleState& S, const SampleSeqs& in) {
   R->pvals.assign(n, 0.0);
   R->map.assign(n, -1);
   std::vector<uint8_t> correct(n, 0);
-  for (size_t ci = 0; ci < S.clusters.size(); ++ci) {
-    const Cluster& c = S.clusters[ci];
-    for (uint32_t raw : c.raws) {
+  // every raw once, with its cluster; priced independently (in parallel
+  // chunks for a large sample)
+  std::vector<uint32_t> mem_ci(n, 0), order;
+  order.reserve(n);
+  for (size_t ci = 0; ci < S.clusters.size(); ++ci)
+    for (uint32_t raw : S.clusters[ci].raws) {
+      mem_ci[raw] = uint32_t(ci);
+      order.push_back(raw);
+    }
+  auto price = [&](size_t lo, size_t hi) {
+    for (size_t k = lo; k < hi; ++k) {
+      const uint32_t raw = order[k];
+      const Cluster& c = S.clusters[mem_ci[raw]];
       double pv;
       bool ok;
       if (int64_t(raw) == c.center) {
@@ -2165,7 +2175,11 @@ static dgpu_result* finish(SampleState& S, const SampleSeqs& in) {
       correct[raw] = ok;
       R->pvals[raw] = pv;
     }
-  }
+  };
+  if (order.size() < kParMin)
+    price(0, order.size());
+  else
+    Helpers::get().parallel_for(order.size(), kParGrain, [&](size_t, size_t lo, size_t hi) { price(lo, hi); });
   for (size_t ci = 0; ci < S.clusters.size(); ++ci)
     for (uint32_t raw : S.clusters[ci].raws)
       if (correct[raw]) R->map[raw] = int32_t(ci);
