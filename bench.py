@@ -671,13 +671,19 @@ def main():
     # ---- plain single-sample path (rank 0 only; one pass) ----
     plain = None
     if rank == 0 and not args.no_plain:
-        t0 = time.perf_counter()
-        pc = 0
-        for s in w.samples:
-            r = D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, params, quals=s.quals, device=local)
-            pc += r["counters"]["cmp_scanned"]
-        pt = time.perf_counter() - t0
-        plain = {"value": pc / pt, "unit": UNIT, "seconds": pt, "batched_over_plain": (comps / dt) / (pc / pt)}
+        # host wall time of a pass varies by up to 2x between passes on a
+        # shared box, so the faster of two passes is reported, both listed
+        passes = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            pc = 0
+            for s in w.samples:
+                r = D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, params, quals=s.quals, device=local)
+                pc += r["counters"]["cmp_scanned"]
+            passes.append(time.perf_counter() - t0)
+        pt = min(passes)
+        plain = {"value": pc / pt, "unit": UNIT, "seconds": pt, "passes_s": passes,
+                 "batched_over_plain": (comps / dt) / (pc / pt)}
 
     # ---- CPU baseline (rank 0, N=1 only, bounded) ----
     cpu = None
