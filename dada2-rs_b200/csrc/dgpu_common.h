@@ -136,6 +136,7 @@ struct CompareLaunch {
   const uint32_t* task_prefix;
   uint32_t ntask;
   uint32_t total_items;
+  uint32_t screen_chunk;    // items a k_screen warp takes at a time (4..32; set by launch_compare)
   uint32_t* queue_pass;     // nraw capacity: items that passed the screen
   uint32_t* queue_counts;   // 8 words; [4] = items pushed to queue_pass
   uint8_t* nw_scratch;      // nwarps * max(vec_scratch, rm_scratch)

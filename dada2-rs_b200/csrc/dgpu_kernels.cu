@@ -308,9 +308,10 @@ __global__ void __launch_bounds__(kScreenWarps * 32, 4) k_screen(CompareLaunch L
     }
     __syncthreads();
   }
-  for (uint32_t chunk = (blockIdx.x * kScreenWarps + wib) * 32u; chunk < L.total_items; chunk += warps_total * 32u) {
+  const uint32_t CH = L.screen_chunk;  // lanes [0, CH) carry an item
+  for (uint32_t chunk = (blockIdx.x * kScreenWarps + wib) * CH; chunk < L.total_items; chunk += warps_total * CH) {
     const uint32_t item = chunk + lane;
-    const bool valid = item < L.total_items;
+    const bool valid = uint32_t(lane) < CH && item < L.total_items;
     uint32_t t = 0, g = 0, c = 0;
     bool skip = false;
     if (valid) {
@@ -2227,11 +2228,19 @@ static int sm_count() {
   return g_sm_count;
 }
 
-void launch_compare(const CompareLaunch& L, cudaStream_t st, cudaEvent_t* ev) {
-  if (L.total_items == 0) return;
+void launch_compare(const CompareLaunch& L0, cudaStream_t st, cudaEvent_t* ev) {
+  if (L0.total_items == 0) return;
   const int sms = sm_count();
-  uint32_t blocks = (L.total_items + kScreenWarps * 32 - 1) / (kScreenWarps * 32);
   const uint32_t cap = uint32_t(sms) * 8u;
+  // A warp screens its items a few at a time, one dependent round of profile
+  // loads each, so a small call spreads its items thin (down to 4 per warp)
+  // over more warps; a large one keeps 32 per warp within the block cap.
+  CompareLaunch L = L0;
+  L.screen_chunk = 32;
+  while (L.screen_chunk > 4 && (L.total_items + kScreenWarps * (L.screen_chunk / 2) - 1) /
+                                       (kScreenWarps * (L.screen_chunk / 2)) <= cap)
+    L.screen_chunk /= 2;
+  uint32_t blocks = (L.total_items + kScreenWarps * L.screen_chunk - 1) / (kScreenWarps * L.screen_chunk);
   if (blocks > cap) blocks = cap;
   if (ev) cudaEventRecord(ev[0], st);
   switch (L.kp.kmer_size) {
