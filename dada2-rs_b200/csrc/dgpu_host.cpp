@@ -817,11 +817,17 @@ struct BudCand {
   uint32_t r;
   uint32_t raw;
 };
+// A raw's candidate cluster (index_add_cluster, src/cluster.rs:731-739). A
+// sample keeps all of them in one pool, each raw's as a list in the order
+// they were added (ascending cluster index), so the loop makes no per-raw
+// allocations.
 struct Cand {
   uint32_t ci;
-  double lambda;
   uint32_t hamming;
+  uint32_t next;  // the raw's next candidate in the pool, or kNoCand
+  double lambda;
 };
+static constexpr uint32_t kNoCand = 0xffffffffu;
 // One bit per member position: set where the member at that position has
 // the property. Updated with the member list, so scans can skip the rest.
 struct PosBits {
@@ -914,7 +920,8 @@ struct SampleState {
   std::vector<uint32_t> raw_cluster;
   std::vector<uint32_t> raw_pos;  // position of each raw in its cluster's member list
   std::vector<Cluster> clusters;
-  std::vector<std::vector<Cand>> cand;
+  std::vector<Cand> cand_pool;
+  std::vector<uint32_t> cand_head, cand_tail;  // per raw: first and last candidate in cand_pool
   std::vector<uint32_t> ncand;   // cand[raw].size(), kept flat for the shuffle scans
   std::vector<uint8_t> fixed_p;  // get_pA answers 1.0 whatever the cluster (src/pval.rs:383)
   uint64_t nalign = 0, nshroud = 0;
@@ -960,7 +967,10 @@ struct SampleState {
         }
     raw_cluster.assign(n, 0);
     raw_pos.resize(n);
-    cand.assign(n, {});
+    cand_pool.clear();
+    cand_pool.reserve(size_t(n) + n / 2);
+    cand_head.assign(n, kNoCand);
+    cand_tail.assign(n, kNoCand);
     ncand.assign(n, 0);
     changed_mark.assign(n, 0);
     clusters.clear();
@@ -1001,7 +1011,9 @@ struct SampleState {
   // Frees the per-raw state; batch_run calls it for all samples in parallel
   // rather than leaving hundreds of thousands of small frees to one thread.
   void release() {
-    std::vector<std::vector<Cand>>().swap(cand);
+    std::vector<Cand>().swap(cand_pool);
+    std::vector<uint32_t>().swap(cand_head);
+    std::vector<uint32_t>().swap(cand_tail);
     std::vector<Cluster>().swap(clusters);
     std::vector<Comp>().swap(rcomp);
     std::vector<Comp>().swap(compmax);
@@ -1011,6 +1023,16 @@ struct SampleState {
     std::vector<uint32_t>().swap(raw_pos);
     std::vector<uint32_t>().swap(ncand);
     std::vector<uint8_t>().swap(fixed_p);
+  }
+
+  void add_cand(uint32_t raw, uint32_t ci, double lambda, uint32_t hamming) {
+    const uint32_t q = uint32_t(cand_pool.size());
+    cand_pool.push_back(Cand{ci, hamming, kNoCand, lambda});
+    if (cand_tail[raw] == kNoCand)
+      cand_head[raw] = q;
+    else
+      cand_pool[cand_tail[raw]].next = q;
+    cand_tail[raw] = q;
   }
 
   void touch(size_t ci) {
@@ -1103,7 +1125,7 @@ struct SampleState {
     });
     for (const Comp& cp : c.comp) {  // index_add_cluster
       const uint32_t raw = cp.index;
-      cand[raw].push_back(Cand{uint32_t(ci), cp.lambda, cp.hamming});
+      add_cand(raw, uint32_t(ci), cp.lambda, cp.hamming);
       // A raw with one candidate keeps its emax implicit (see shuffle_converge);
       // on gaining a second it gets the value the eager updates would hold.
       if (++ncand[raw] == 2) {
@@ -1600,7 +1622,8 @@ struct SampleState {
       const uint32_t raw = affected[k];
       double be = -std::numeric_limits<double>::infinity();
       Comp best;
-      for (const Cand& c : cand[raw]) {
+      for (uint32_t q = cand_head[raw]; q != kNoCand; q = cand_pool[q].next) {
+        const Cand& c = cand_pool[q];
         const double e = c.lambda * double(clusters[c.ci].reads);
         if (e > be) {
           be = e;
