@@ -321,9 +321,11 @@ struct Slot {
     if (st) cudaStreamDestroy(st);
   }
 
-  int init(Pool* pool) {
+  int init(Pool* pool, bool high_priority = false) {
     P = pool;
-    CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    int lo = 0, hi = 0;
+    CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    CUDA_TRY(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, high_priority ? hi : lo));
     for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
     TRY(queue_counts.alloc(8));
     TRY(err_dev.alloc(1));
@@ -535,7 +537,7 @@ struct Pool {
     for (int k = 0; k < nslots; ++k) {
       slots.emplace_back(new Slot);
       Slot& L = *slots.back();
-      TRY(L.init(this));
+      TRY(L.init(this, k == 0 && nslots > 1));  // slot 0 serves the critical sample
       TRY(L.scratch.alloc(per * size_t(geom.nwarps)));
       TRY(L.queue_pass.alloc(nraw));
     }
@@ -2276,10 +2278,31 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
   int rc = 0;
   std::string err_msg;
   std::atomic<int64_t> host_ns{0};
+  // With several slots, the unfinished sample with the most uniques (the
+  // longest chain) has slot 0 and its high-priority stream to itself: it never
+  // waits for a slot and its kernels are scheduled ahead of the others'. The
+  // other slots serve the rest, largest first.
+  const bool dedicate = std::min(P.slots.size(), ns) > 1;
+  std::vector<uint8_t> is_done(ns, 0);
+  size_t critical = SIZE_MAX;
+  auto pick_critical = [&] {  // under mu
+    critical = SIZE_MAX;
+    if (!dedicate) return;
+    for (size_t s = 0; s < ns; ++s)
+      if (!is_done[s] && (critical == SIZE_MAX || S[s].n > S[critical].n)) critical = s;
+  };
+  pick_critical();
   auto t_start = Clock::now();
   {
     JobQueue jobs(host_threads > 1 ? host_threads : 0);
     auto worker = [&](Slot& L) {
+      const bool mine = dedicate && &L == P.slots[0].get();
+      auto has_work = [&] {  // under mu
+        if (mine) return critical != SIZE_MAX && std::find(ready.begin(), ready.end(), critical) != ready.end();
+        for (size_t s : ready)
+          if (s != critical) return true;
+        return false;
+      };
       if (cudaSetDevice(P.device) != cudaSuccess) {
         std::lock_guard<std::mutex> g(mu);
         if (!rc) {
@@ -2295,16 +2318,25 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
         batch.clear();
         {
           std::unique_lock<std::mutex> lk(mu);
-          cv.wait(lk, [&] { return !ready.empty() || finished == ns || rc != 0; });
-          if (ready.empty() || rc != 0) break;
-          if (ready.size() <= batch_max) {
-            batch.swap(ready);
+          cv.wait(lk, [&] { return has_work() || finished == ns || rc != 0; });
+          if (rc != 0 || !has_work()) break;
+          if (mine) {
+            ready.erase(std::find(ready.begin(), ready.end(), critical));
+            batch.push_back(critical);
           } else {
-            // the largest samples (the longest chains) go first
-            std::stable_sort(ready.begin(), ready.end(), [&](size_t x, size_t y) { return S[x].n > S[y].n; });
-            batch.assign(ready.begin(), ready.begin() + batch_max);
-            ready.erase(ready.begin(), ready.begin() + batch_max);
-            if (!ready.empty()) cv.notify_one();
+            const auto it = std::find(ready.begin(), ready.end(), critical);
+            const bool held = it != ready.end();
+            if (held) ready.erase(it);
+            if (ready.size() <= batch_max) {
+              batch.swap(ready);
+            } else {
+              // the largest samples (the longest chains) go first
+              std::stable_sort(ready.begin(), ready.end(), [&](size_t x, size_t y) { return S[x].n > S[y].n; });
+              batch.assign(ready.begin(), ready.begin() + batch_max);
+              ready.erase(ready.begin(), ready.begin() + batch_max);
+              if (!ready.empty()) cv.notify_all();
+            }
+            if (held) ready.push_back(critical);
           }
         }
         std::sort(batch.begin(), batch.end());
@@ -2365,6 +2397,8 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
             } else {
               ++finished;
               if (!on_finish) ss.stats.t_done = secs(t_start, Clock::now());
+              is_done[sidx] = 1;
+              if (sidx == critical) pick_critical();
             }
             cv.notify_all();
           }, int64_t(S[sidx].n));  // larger samples have the longer chains: serve them first
