@@ -2377,7 +2377,7 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
           sa.absorb(size_t(sa.pending), L, a);
           sa.stats.t_compare += tcmp;
           sa.stats.t_mark = Clock::now();
-          jobs.submit([&, sidx] {
+          auto host_phase = [&, sidx] {
             SampleState& ss = S[sidx];
             auto th = Clock::now();
             ss.stats.t_job_wait += secs(ss.stats.t_mark, th);
@@ -2401,7 +2401,13 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
               if (sidx == critical) pick_critical();
             }
             cv.notify_all();
-          }, int64_t(S[sidx].n));  // larger samples have the longer chains: serve them first
+          };
+          // the dedicated slot runs its sample's host phase itself and goes
+          // straight on to the next compare: no hand-off between threads
+          if (mine)
+            host_phase();
+          else
+            jobs.submit(host_phase, int64_t(S[sidx].n));  // larger samples have the longer chains: serve them first
         }
       }
       std::lock_guard<std::mutex> g(mu);
