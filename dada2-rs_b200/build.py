@@ -22,7 +22,7 @@ CUDA_HOME = os.path.dirname(os.path.dirname(os.path.realpath(NVCC)))
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 SOURCES_CU = ["dgpu_kernels.cu"]
-SOURCES_CPP = ["dgpu_host.cpp", "dgpu_service.cpp"]
+SOURCES_CPP = ["dgpu_host.cpp", "dgpu_service.cpp", "dgpu_derep.cpp"]
 HEADERS = ["dgpu_common.h"]
 
 
@@ -60,7 +60,7 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
             _run(["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra",
                   "-I", CSRC, "-I", INCLUDE, "-I", os.path.join(CUDA_HOME, "include"), "-c", s, "-o", o])
     if force or _stale(OUT, objs):
-        _run([NVCC, "-shared", *ARCH, "-cudart", "static", "-o", OUT, *objs, "-lpthread"])
+        _run([NVCC, "-shared", *ARCH, "-cudart", "static", "-o", OUT, *objs, "-lpthread", "-lz"])
     return OUT
 
 

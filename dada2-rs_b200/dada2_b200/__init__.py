@@ -24,7 +24,7 @@ from ._lib import (AlignParamsC, CountersC, DadaOutC, DadaParamsC, DgpuError, In
                    check, device_count, lib, ptr)
 
 __all__ = ["AlignParams", "DadaParams", "CompareContext", "dada_uniques", "dada_uniques_batch",
-           "ResidentBatch", "PackedBatch", "DenoiseService", "pack_sample", "align_pairs", "stats_reset", "stats_timing", "stats_read",
+           "ResidentBatch", "PackedBatch", "DenoiseService", "pack_sample", "Derep", "derep_fastq", "dada_fastq", "align_pairs", "stats_reset", "stats_timing", "stats_read",
            "DgpuError", "InvalidInput", "device_count", "METHOD_NAMES", "KERNEL_NAMES"]
 
 KERNEL_NAMES = ["profiles", "screen", "align", "store"]
@@ -456,6 +456,51 @@ class DenoiseService:
             self.close()
         except Exception:
             pass
+
+
+@dataclass
+class Derep:
+    """Uniques of a FASTQ file (src/derep.rs:43-240): ``seqs`` (str) by read
+    count descending, ties by sequence; ``abund`` their counts; ``quals`` the
+    per-position Phred sums (u32); ``map`` each read's unique."""
+    seqs: list
+    abund: np.ndarray
+    quals: list
+    map: np.ndarray
+
+
+def derep_fastq(path, phred_offset: int = 33, nthreads: int = 0) -> Derep:
+    """Dereplicate a FASTQ file (plain or gzip) on the host."""
+    h = C.c_void_p()
+    check(lib().dgpu_derep_fastq(str(path).encode(), int(phred_offset), int(nthreads), C.byref(h)))
+    try:
+        sz = np.zeros(3, np.int64)
+        check(lib().dgpu_derep_sizes(h, ptr(sz)))
+        nu, nr, nb = (int(x) for x in sz)
+        cat = np.zeros(max(nb, 1), np.uint8)
+        offs = np.zeros(max(nu, 1), np.uint32)
+        lens = np.zeros(max(nu, 1), np.uint32)
+        cnt = np.zeros(max(nu, 1), np.uint64)
+        qs = np.zeros(max(nb, 1), np.uint32)
+        mp = np.zeros(max(nr, 1), np.uint32)
+        check(lib().dgpu_derep_fill(h, ptr(cat), ptr(offs), ptr(lens), ptr(cnt), ptr(qs), ptr(mp)))
+    finally:
+        lib().dgpu_derep_free(h)
+    raw = cat.tobytes()
+    seqs = [raw[o:o + n].decode("ascii", "replace") for o, n in zip(offs[:nu], lens[:nu])]
+    quals = [qs[o:o + n].copy() for o, n in zip(offs[:nu], lens[:nu])]
+    return Derep(seqs, cnt[:nu].copy(), quals, mp[:nr].copy())
+
+
+def dada_fastq(path, err, ncol, params: DadaParams | None = None, phred_offset: int = 33, device: int = 0) -> dict:
+    """FASTQ -> derep -> dada on the GPU: the `dada` subcommand's per-sample
+    path (src/main.rs:1139-1257) up to its result tables."""
+    d = derep_fastq(path, phred_offset)
+    if np.any(d.abund > np.iinfo(np.uint32).max):
+        raise InvalidInput(-1, "a unique has more than 2^32 - 1 reads")
+    res = dada_uniques(d.seqs, d.abund.astype(np.uint32), err, ncol, params, quals=d.quals, device=device)
+    res["derep"] = d
+    return res
 
 
 def calc_pA(reads: int, e_reads: float, prior: bool = False) -> float:

@@ -100,6 +100,11 @@ def lib():
         L.dgpu_service_submit.argtypes = [_P, C.c_int, _P, _P, _P, _P, _P, _P, _P]
         L.dgpu_service_wait.argtypes = [_P, C.c_uint64, _P, _P]
         L.dgpu_service_stats.argtypes = [_P, _P, _P]
+        L.dgpu_derep_fastq.argtypes = [C.c_char_p, C.c_int, C.c_int, _P]
+        L.dgpu_derep_sizes.argtypes = [_P, _P]
+        L.dgpu_derep_fill.argtypes = [_P, _P, _P, _P, _P, _P, _P]
+        L.dgpu_derep_free.argtypes = [_P]
+        L.dgpu_derep_free.restype = None
         L.dgpu_service_hold.argtypes = [_P, C.c_int]
         L.dgpu_service_destroy.argtypes = [_P]
         L.dgpu_service_destroy.restype = None

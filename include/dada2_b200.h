@@ -241,6 +241,25 @@ double dgpu_calc_pA(uint32_t reads, double e_reads, int prior);
  * repriced from the FP64 product (the fallback). Zero otherwise. */
 int dgpu_result_fp32_stats(const dgpu_result* res, uint64_t* out2);
 
+/* ---- ingest: FASTQ -> uniques ----
+ * Dereplicates a FASTQ file (plain or gzip, four-line records) as
+ * dereplicate does (src/derep.rs:43-240, ordering src/derep.rs:179-185):
+ * uniques by read count descending, ties by sequence bytes ascending; per
+ * unique the per-position SUM of (quality byte - phred_offset), stored as u32
+ * (a negative sum becomes 0, one beyond u32 is DGPU_E_UNSUPPORTED); map[r] is
+ * read r's unique. nthreads 0 = one per core. Host only: no device is used.
+ * The outputs feed dgpu_dada / dgpu_dada_batch directly (counts as abund). */
+typedef struct dgpu_derep dgpu_derep;
+int dgpu_derep_fastq(const char* path, int phred_offset, int nthreads, dgpu_derep** out);
+/* sizes[0] uniques, [1] reads, [2] total bytes of unique sequence */
+int dgpu_derep_sizes(const dgpu_derep* d, int64_t* sizes);
+/* Any output may be null. seqs: sizes[2] bytes; offs, lens, counts:
+ * sizes[0] entries; qual_sums: sizes[2] entries (same offsets as seqs); map:
+ * sizes[1] entries. */
+int dgpu_derep_fill(const dgpu_derep* d, char* seqs, uint32_t* offs, uint32_t* lens, uint64_t* counts,
+                    uint32_t* qual_sums, uint32_t* map);
+void dgpu_derep_free(dgpu_derep* d);
+
 typedef struct dgpu_service dgpu_service;
 int dgpu_service_create(int device, const dgpu_dada_params* params, const double* err_mat, int ncol,
                         uint64_t hbm_budget, dgpu_service** out);

@@ -465,3 +465,54 @@ def dada(seqs, abund, err, ncol, params: DadaParams, quals=None, prior=None):
 
 def hardware_threads() -> int:
     return int(lib().orc_c_hardware_threads())
+
+
+# ---------------- derep (pure Python restatement) ----------------
+
+def read_fastq_records(path):
+    """Four-line FASTQ records (plain or gzip) as (sequence bytes, quality bytes)."""
+    import gzip
+
+    with open(path, "rb") as f:
+        head = f.read(2)
+    opener = gzip.open if head == b"\x1f\x8b" else open
+    with opener(path, "rb") as f:
+        lines = f.read().split(b"\n")
+    if lines and lines[-1] == b"":
+        lines.pop()
+    lines = [ln[:-1] if ln.endswith(b"\r") else ln for ln in lines]
+    recs = []
+    for i in range(0, len(lines), 4):
+        h, s, p, q = (lines[i:i + 4] + [b"", b"", b""])[:4]
+        if not h.startswith(b"@") or not p.startswith(b"+") or len(s) != len(q):
+            raise ValueError(f"record {i // 4}: malformed")
+        recs.append((s, q))
+    return recs
+
+
+def derep(records, phred_offset: int = 33):
+    """src/derep.rs:84-240: group identical sequences in first-seen order,
+    count reads and sum (quality - offset) per position, store round(sum) as
+    u32 (negative -> 0), then order by count descending, ties by sequence
+    bytes ascending; map gives each read's unique."""
+    index, seqs, counts, sums, local = {}, [], [], [], []
+    for s, q in records:
+        j = index.get(s)
+        if j is None:
+            j = len(seqs)
+            index[s] = j
+            seqs.append(s)
+            counts.append(0)
+            sums.append([0] * len(q))
+        counts[j] += 1
+        local.append(j)
+        row = sums[j]
+        if len(q) > len(row):
+            row.extend([0] * (len(q) - len(row)))
+        for p, c in enumerate(q):
+            row[p] += c - phred_offset
+    order = sorted(range(len(seqs)), key=lambda t: (-counts[t], seqs[t]))
+    new = {old: k for k, old in enumerate(order)}
+    return ([seqs[t].decode() for t in order], np.array([counts[t] for t in order], np.uint64),
+            [np.array([max(v, 0) for v in sums[t]], np.uint32) for t in order],
+            np.array([new[j] for j in local], np.uint32))

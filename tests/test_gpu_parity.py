@@ -568,3 +568,28 @@ def test_fp32_lambda_decisions_keep_the_partition(seed):
         lb = gb["lambdas"][np.argsort(gb["members"])]
         normal = la > 1e-300
         assert np.all(np.abs(lb[normal] - la[normal]) <= 1e-4 * la[normal])
+
+
+def test_dada_from_fastq_matches_the_oracle(tmp_path):
+    """FASTQ -> derep -> dada: the library's dereplication feeds the GPU loop
+    and the result equals the oracle's on the oracle's own dereplication."""
+    import gzip
+
+    w = synth.small_illumina(31, nvariants=5, nreads=2000, L=150)
+    rng = np.random.default_rng(31)
+    recs = []
+    for s, a, q in zip(w.samples[0].seqs, w.samples[0].abund, w.samples[0].quals):
+        mean = np.rint(np.asarray(q, np.float64) / a).astype(np.int64)
+        for _ in range(int(a)):
+            qq = np.clip(mean + rng.integers(-2, 3, size=len(mean)), 2, 41)
+            recs.append((s.encode(), (qq + 33).astype(np.uint8).tobytes()))
+    order = rng.permutation(len(recs))
+    recs = [recs[i] for i in order]
+    path = tmp_path / "s.fastq.gz"
+    with gzip.open(path, "wb") as f:
+        f.write(b"".join(b"@r%d\n%s\n+\n%s\n" % (i, s, q) for i, (s, q) in enumerate(recs)))
+    got = D.dada_fastq(path, w.err, w.ncol, D.DadaParams())
+    seqs, counts, quals, mp = O.derep(recs)
+    assert got["derep"].seqs == seqs and np.array_equal(got["derep"].map, mp)
+    want = O.dada(seqs, counts.astype(np.uint32), w.err, w.ncol, O.DadaParams(nthreads=4), quals=quals)
+    assert_same_dada(got, want)
