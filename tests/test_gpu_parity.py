@@ -593,3 +593,10 @@ def test_dada_from_fastq_matches_the_oracle(tmp_path):
     assert got["derep"].seqs == seqs and np.array_equal(got["derep"].map, mp)
     want = O.dada(seqs, counts.astype(np.uint32), w.err, w.ncol, O.DadaParams(nthreads=4), quals=quals)
     assert_same_dada(got, want)
+    import json
+
+    from dada2_b200 import output
+    doc = json.loads(output.dada_json(got, D.DadaParams(), path))
+    assert doc["sample"] == "s" and doc["num_asvs"] == want["nclust"]
+    assert doc["total_reads"] == len(recs)
+    assert doc["map"] == [None if m < 0 else int(m) for m in want["map"]]
