@@ -291,6 +291,16 @@ static void recycle_all(B&... b) {
 // ---------------------------------------------------------------------------
 // Device pool: the resident uniques of one or more samples
 // ---------------------------------------------------------------------------
+// Launch slots dedicated to the longest chains: DGPU_DEDICATED_SLOTS (0..7) if
+// set, else 1.
+static size_t dedicated_slots() {
+  if (const char* e = std::getenv("DGPU_DEDICATED_SLOTS")) {
+    const int v = std::atoi(e);
+    if (v >= 0 && v <= 7) return size_t(v);
+  }
+  return 1;
+}
+
 struct Pool;
 
 // One launch context: its own stream, queue, NW scratch, task tables and store
@@ -537,7 +547,7 @@ struct Pool {
     for (int k = 0; k < nslots; ++k) {
       slots.emplace_back(new Slot);
       Slot& L = *slots.back();
-      TRY(L.init(this, k == 0 && nslots > 1));  // slot 0 serves the critical sample
+      TRY(L.init(this, nslots > 1 && size_t(k) < dedicated_slots()));  // the dedicated slots come first
       TRY(L.scratch.alloc(per * size_t(geom.nwarps)));
       TRY(L.queue_pass.alloc(nraw));
     }
@@ -2278,29 +2288,39 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
   int rc = 0;
   std::string err_msg;
   std::atomic<int64_t> host_ns{0};
-  // With several slots, the unfinished sample with the most uniques (the
-  // longest chain) has slot 0 and its high-priority stream to itself: it never
-  // waits for a slot and its kernels are scheduled ahead of the others'. The
-  // other slots serve the rest, largest first.
-  const bool dedicate = std::min(P.slots.size(), ns) > 1;
-  std::vector<uint8_t> is_done(ns, 0);
-  size_t critical = SIZE_MAX;
-  auto pick_critical = [&] {  // under mu
-    critical = SIZE_MAX;
-    if (!dedicate) return;
-    for (size_t s = 0; s < ns; ++s)
-      if (!is_done[s] && (critical == SIZE_MAX || S[s].n > S[critical].n)) critical = s;
+  // With several slots, the kd unfinished samples with the most uniques (the
+  // longest chains) have a slot each, with a high-priority stream, to
+  // themselves: they never wait for a slot and their kernels are scheduled
+  // ahead of the others'. The other slots serve the rest, largest first.
+  const size_t nw_all = std::min(P.slots.size(), ns);
+  const size_t kd = nw_all > 1 ? std::min(dedicated_slots(), nw_all - 1) : 0;
+  std::vector<uint8_t> is_done(ns, 0), is_crit(ns, 0);
+  std::vector<size_t> crit(kd, SIZE_MAX);  // crit[i]: the sample slot i serves
+  auto pick_critical = [&] {  // under mu: the kd largest unfinished samples
+    for (size_t& c : crit) c = SIZE_MAX;
+    std::fill(is_crit.begin(), is_crit.end(), 0);
+    for (size_t i = 0; i < kd; ++i) {
+      size_t best = SIZE_MAX;
+      for (size_t s = 0; s < ns; ++s)
+        if (!is_done[s] && !is_crit[s] && (best == SIZE_MAX || S[s].n > S[best].n)) best = s;
+      if (best == SIZE_MAX) break;
+      crit[i] = best;
+      is_crit[best] = 1;
+    }
   };
   pick_critical();
   auto t_start = Clock::now();
   {
     JobQueue jobs(host_threads > 1 ? host_threads : 0);
     auto worker = [&](Slot& L) {
-      const bool mine = dedicate && &L == P.slots[0].get();
+      size_t my = SIZE_MAX;  // the dedicated position of this slot, if any
+      for (size_t i = 0; i < kd; ++i)
+        if (&L == P.slots[i].get()) my = i;
+      const bool mine = my != SIZE_MAX;
       auto has_work = [&] {  // under mu
-        if (mine) return critical != SIZE_MAX && std::find(ready.begin(), ready.end(), critical) != ready.end();
+        if (mine) return crit[my] != SIZE_MAX && std::find(ready.begin(), ready.end(), crit[my]) != ready.end();
         for (size_t s : ready)
-          if (s != critical) return true;
+          if (!is_crit[s]) return true;
         return false;
       };
       if (cudaSetDevice(P.device) != cudaSuccess) {
@@ -2321,12 +2341,18 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
           cv.wait(lk, [&] { return has_work() || finished == ns || rc != 0; });
           if (rc != 0 || !has_work()) break;
           if (mine) {
-            ready.erase(std::find(ready.begin(), ready.end(), critical));
-            batch.push_back(critical);
+            ready.erase(std::find(ready.begin(), ready.end(), crit[my]));
+            batch.push_back(crit[my]);
           } else {
-            const auto it = std::find(ready.begin(), ready.end(), critical);
-            const bool held = it != ready.end();
-            if (held) ready.erase(it);
+            std::vector<size_t> held;
+            for (size_t k = 0; k < ready.size();) {
+              if (is_crit[ready[k]]) {
+                held.push_back(ready[k]);
+                ready.erase(ready.begin() + long(k));
+              } else {
+                ++k;
+              }
+            }
             if (ready.size() <= batch_max) {
               batch.swap(ready);
             } else {
@@ -2336,7 +2362,7 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
               ready.erase(ready.begin(), ready.begin() + batch_max);
               if (!ready.empty()) cv.notify_all();
             }
-            if (held) ready.push_back(critical);
+            ready.insert(ready.end(), held.begin(), held.end());
           }
         }
         std::sort(batch.begin(), batch.end());
@@ -2398,7 +2424,7 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
               ++finished;
               if (!on_finish) ss.stats.t_done = secs(t_start, Clock::now());
               is_done[sidx] = 1;
-              if (sidx == critical) pick_critical();
+              if (is_crit[sidx]) pick_critical();
             }
             cv.notify_all();
           };
