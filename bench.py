@@ -629,7 +629,8 @@ def main():
             (2 * L + 1) * (w.band + 1)
 
     # ---- timed: end to end through the C ABI with host buffers ----
-    h2d0 = D.stats_read()["h2d_bytes"]
+    st_e0 = D.stats_read()
+    h2d0 = st_e0["h2d_bytes"]
     barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -644,7 +645,12 @@ def main():
     torch.cuda.synchronize()
     barrier()
     e2e_dt, e2e_comps_all = multi.reduce_run(e0.elapsed_time(e1) / 1e3, e2e_comps, device="cuda")
-    h2d = (D.stats_read()["h2d_bytes"] - h2d0) // max(args.steps, 1)
+    st_e1 = D.stats_read()
+    h2d = (st_e1["h2d_bytes"] - h2d0) // max(args.steps, 1)
+    e2e_split = {"encode_ms": (st_e1["prepare_ms"]["encode"] - st_e0["prepare_ms"]["encode"]) / args.steps,
+                 "upload_profiles_ms": (st_e1["prepare_ms"]["upload"] - st_e0["prepare_ms"]["upload"]) / args.steps,
+                 "loop_ms": (st_e1["batch_ms"]["loop"] - st_e0["batch_ms"]["loop"]) / args.steps,
+                 "results_ms": (st_e1["batch_ms"]["after"] - st_e0["batch_ms"]["after"]) / args.steps}
     e2e = e2e_comps_all / e2e_dt
 
     # ---- the final-subs pass (transition counts), measured beside the step ----
@@ -721,7 +727,8 @@ def main():
                    "l2": "k-mer profiles of the 40 samples exceed L2 (126 MB); no flush between steps"},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(d2h),
                 "h2d_note": "counted by the library: encoded u8 codes and qualities, 12 B per unique, the error "
-                            "matrix, lock flags and each compare call's task tables"},
+                            "matrix, lock flags and each compare call's task tables",
+                "split_ms_per_step": e2e_split},
         "roofline": {"bound": "hbm", "kernel": "k_screen", "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                      "traffic": traffic,

@@ -2498,6 +2498,7 @@ struct Batch {
 static int batch_prepare(Batch& B, int device, const dgpu_dada_params* prm, int nsamples, const uint32_t* sample_start,
                          const char* seqs, const uint32_t* offs, const uint32_t* lens, const uint32_t* abund,
                          const uint8_t* prior, const uint32_t* qsums, const double* errm, int ncol) {
+  const auto tp0 = Clock::now();
   if (!prm || !seqs || !offs || !lens || !abund || !errm || nsamples <= 0 || !sample_start)
     return fail(DGPU_E_INVALID, "null argument or no samples");
   if (ncol <= 0) return fail(DGPU_E_INVALID, "Error matrix length does not match 16 x ncol.");
@@ -2540,8 +2541,14 @@ static int batch_prepare(Batch& B, int device, const dgpu_dada_params* prm, int 
                                   : std::vector<double>(errm, errm + 16 * size_t(ncol));
   KParams kp = to_kparams(prm->align, prm->use_quals, prm->greedy, ncol2);
   kp.lambda32 = prm->lambda_fp32 ? 1 : 0;
+  const auto tp1 = Clock::now();
   TRY(B.pool.upload(uint32_t(B.E.off.size()), B.E.seq, B.E.off.data(), B.E.len.data(), B.E.qual, B.E.reads.data(), kp,
                     err.data()));
+  {
+    std::lock_guard<std::mutex> g(g_stats.mu);
+    g_stats.s.prepare_ms[0] += 1e3 * secs(tp0, tp1);
+    g_stats.s.prepare_ms[1] += 1e3 * secs(tp1, Clock::now());
+  }
   B.conf.omega_a = prm->omega_a;
   B.conf.omega_p = prm->omega_p;
   B.conf.omega_c = prm->omega_c;
