@@ -6,6 +6,7 @@
 // compare (screen, alignment, lambda, store) runs on the GPU; the serial phases
 // (shuffle, p-update, bud) run here, one host thread per sample in batch mode.
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -2020,6 +2021,16 @@ static int check_samples(int nsamples, const uint32_t* sample_start, const uint3
   return nsamples;
 }
 
+// nt code of an input character: A/C/G/T/U in either case -> 1..4, else 0
+static const std::array<uint8_t, 256> kNtCode = [] {
+  std::array<uint8_t, 256> t{};
+  t['A'] = t['a'] = 1;
+  t['C'] = t['c'] = 2;
+  t['G'] = t['g'] = 3;
+  t['T'] = t['t'] = t['U'] = t['u'] = 4;
+  return t;
+}();
+
 // Encodes uniques [sample_start[0], sample_start[nsamples]) into E (seq, qual
 // sized by the caller), in parallel chunks of uniques. Bases map A/C/G/T/U
 // (either case) to 1..4; qualities are round(sum / reads) saturated to u8
@@ -2027,6 +2038,7 @@ static int check_samples(int nsamples, const uint32_t* sample_start, const uint3
 // (src/dada.rs:337-346). On a non-ACGT base the first one in input order is
 // reported, as a sequential scan would: *bad_unique / *bad_pos (else
 // bad_unique = UINT32_MAX).
+
 static void encode_uniques(uint32_t t0, uint32_t t1, const char* seqs, const uint32_t* offs, const uint32_t* lens,
                            const uint32_t* abund, const uint8_t* prior, const uint32_t* qsums, EncodedView& E,
                            uint32_t* bad_unique, uint32_t* bad_pos) {
@@ -2058,14 +2070,7 @@ static void encode_uniques(uint32_t t0, uint32_t t1, const char* seqs, const uin
         uint8_t* out = E.seq + E.off[r];
         bool bad = false;
         for (uint32_t p = 0; p < lens[t]; ++p) {
-          uint8_t code;
-          switch (sq[p]) {
-            case 'A': case 'a': code = 1; break;
-            case 'C': case 'c': code = 2; break;
-            case 'G': case 'g': code = 3; break;
-            case 'T': case 't': case 'U': case 'u': code = 4; break;
-            default: code = 0; break;
-          }
+          const uint8_t code = kNtCode[static_cast<unsigned char>(sq[p])];
           if (!code) {
             ch_bad[c] = r;
             ch_pos[c] = p;
@@ -2076,16 +2081,22 @@ static void encode_uniques(uint32_t t0, uint32_t t1, const char* seqs, const uin
         }
         if (bad) break;  // later uniques of this chunk cannot be the first failure
         if (E.qual) {
-          const double cnt = double(abund[t]);
-          const double cq = double(std::max<uint32_t>(abund[t], 1));
+          // quality = round(sum / reads) half away from zero as u8
+          // (src/containers.rs:128-137); uqmax takes the unclamped value with
+          // reads floored at 1. For 0 <= x = sum / reads < 2^32, x + 0.5 is
+          // exact and its truncation is that rounding; and x is never within
+          // 1 / (2 reads) of a half-integer without being one, far above the
+          // division's rounding, so this equals rounding the exact quotient.
+          const uint32_t reads = abund[t];
+          const double cq = double(std::max<uint32_t>(reads, 1));
           const uint32_t* qs = qsums + offs[t];
           uint8_t* qo = E.qual + E.off[r];
           uint32_t qm_u = 0;
           for (uint32_t p = 0; p < lens[t]; ++p) {
-            const double q = std::round(double(qs[p]) / cnt);
-            qo[p] = q >= 255.0 ? 255 : (q > 0.0 ? uint8_t(q) : 0);
-            const double qm = std::round(double(qs[p]) / cq);
-            qm_u = std::max<uint32_t>(qm_u, qm > 0 ? uint32_t(qm) : 0);
+            const uint32_t q = uint32_t(double(qs[p]) / cq + 0.5);
+            qm_u = std::max(qm_u, q);
+            // reads == 0: sum / 0 is +inf (-> 255) for a positive sum, NaN (-> 0) for 0
+            qo[p] = reads ? uint8_t(std::min<uint32_t>(q, 255u)) : (qs[p] ? 255 : 0);
           }
           E.uqmax[r] = qm_u;
           qm_max = std::max(qm_max, qm_u);
