@@ -2038,7 +2038,6 @@ static const std::array<uint8_t, 256> kNtCode = [] {
 // (src/dada.rs:337-346). On a non-ACGT base the first one in input order is
 // reported, as a sequential scan would: *bad_unique / *bad_pos (else
 // bad_unique = UINT32_MAX).
-
 static void encode_uniques(uint32_t t0, uint32_t t1, const char* seqs, const uint32_t* offs, const uint32_t* lens,
                            const uint32_t* abund, const uint8_t* prior, const uint32_t* qsums, EncodedView& E,
                            uint32_t* bad_unique, uint32_t* bad_pos) {
