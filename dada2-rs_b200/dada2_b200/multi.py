@@ -44,3 +44,68 @@ def reduce_run(seconds: float, compares: int, device=None):
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     dist.all_reduce(c, op=dist.ReduceOp.SUM)
     return float(t.item()), int(round(c.item()))
+
+
+class RequestRouter:
+    """Least-loaded routing of service requests over devices: a request goes
+    to the device with the least outstanding work (sum of uniques x length of
+    its requests not yet collected), ties to the lower device index. Requests
+    are independent samples, so nothing is exchanged between devices."""
+
+    def __init__(self, ndevices: int):
+        self.load = [0] * ndevices
+        self.owner = {}
+
+    def assign(self, key, work: int) -> int:
+        d = min(range(len(self.load)), key=lambda q: (self.load[q], q))
+        self.load[d] += int(work)
+        self.owner[key] = (d, int(work))
+        return d
+
+    def release(self, key) -> int:
+        d, work = self.owner.pop(key)
+        self.load[d] -= work
+        return d
+
+
+class MultiDeviceService:
+    """One DenoiseService per device behind one submit/wait interface (the
+    denoising service sharded over the GPUs of one node). ``submit`` returns a
+    ticket of this object; results are each device's, so identical to
+    ``dada_uniques`` on that sample."""
+
+    def __init__(self, err, ncol, params=None, devices=(0,), hbm_budget: int = 0):
+        import dada2_b200 as D
+
+        self.devices = list(devices)
+        self.services = [D.DenoiseService(err, ncol, params, device=d, hbm_budget=hbm_budget) for d in self.devices]
+        self.router = RequestRouter(len(self.devices))
+        self.tickets = {}
+        self.next = 1
+
+    def submit(self, seqs=None, abund=None, quals=None, prior=None, packed=None) -> int:
+        import dada2_b200 as D
+
+        pk = packed if packed is not None else D.pack_sample(seqs, abund, quals, prior)
+        t = self.next
+        self.next += 1
+        d = self.router.assign(t, int(pk[0].size))  # sequence bytes = uniques x length
+        self.tickets[t] = (d, self.services[d].submit(packed=pk))
+        return t
+
+    def wait(self, ticket: int, read_result: bool = True):
+        d, inner = self.tickets.pop(ticket)
+        try:
+            return self.services[d].wait(inner, read_result=read_result)
+        finally:
+            self.router.release(ticket)
+
+    def close(self):
+        for s in self.services:
+            s.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -600,3 +600,18 @@ def test_dada_from_fastq_matches_the_oracle(tmp_path):
     assert doc["sample"] == "s" and doc["num_asvs"] == want["nclust"]
     assert doc["total_reads"] == len(recs)
     assert doc["map"] == [None if m < 0 else int(m) for m in want["map"]]
+
+
+def test_multi_device_service_matches_single_sample_calls():
+    """The service sharded over the node's devices (here, those visible) gives
+    each request the single-sample result."""
+    from dada2_b200.multi import MultiDeviceService
+
+    reqs = _service_reqs()[:3]
+    w = synth.small_illumina(80)
+    devs = list(range(D.device_count()))
+    with MultiDeviceService(w.err, w.ncol, D.DadaParams(), devices=devs) as svc:
+        ts = [svc.submit(s.seqs, s.abund, quals=s.quals) for s in reqs]
+        got = [svc.wait(t)[0] for t in ts]
+    for s, g in zip(reqs, got):
+        assert_same_dada(g, D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, D.DadaParams(), quals=s.quals))

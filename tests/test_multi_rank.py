@@ -65,3 +65,15 @@ def test_single_process_reduce_is_identity():
 
     assert multi.reduce_run(3.5, 7) == (3.5, 7)
     assert multi.shard_samples([3, 1, 2], 0, 1) == [0, 1, 2]
+
+
+def test_request_router_balances_outstanding_work():
+    """Service requests go to the device with the least outstanding work and
+    their work is returned when collected."""
+    from dada2_b200.multi import RequestRouter
+
+    r = RequestRouter(3)
+    assert [r.assign(k, w) for k, w in enumerate([100, 50, 50, 10, 200])] == [0, 1, 2, 1, 2]
+    assert r.load == [100, 60, 250]
+    assert r.release(0) == 0 and r.load == [0, 60, 250]
+    assert r.assign(9, 5) == 0
