@@ -649,6 +649,9 @@ def main():
     h2d = (st_e1["h2d_bytes"] - h2d0) // max(args.steps, 1)
     e2e_split = {"encode_ms": (st_e1["prepare_ms"]["encode"] - st_e0["prepare_ms"]["encode"]) / args.steps,
                  "upload_profiles_ms": (st_e1["prepare_ms"]["upload"] - st_e0["prepare_ms"]["upload"]) / args.steps,
+                 "of_which_slots_ms": (st_e1["prepare_ms"]["slots"] - st_e0["prepare_ms"]["slots"]) / args.steps,
+                 "of_which_copy_wait_ms": (st_e1["prepare_ms"]["copy_wait"] - st_e0["prepare_ms"]["copy_wait"])
+                 / args.steps,
                  "loop_ms": (st_e1["batch_ms"]["loop"] - st_e0["batch_ms"]["loop"]) / args.steps,
                  "results_ms": (st_e1["batch_ms"]["after"] - st_e0["batch_ms"]["after"]) / args.steps}
     e2e = e2e_comps_all / e2e_dt

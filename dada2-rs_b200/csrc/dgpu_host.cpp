@@ -514,8 +514,15 @@ struct Pool {
       g_stats.s.launches[0] += 1;
     }
     CUDA_TRY(cudaGetLastError());
+    const auto tn0 = Clock::now();
     TRY(size_nw());
+    const auto tn1 = Clock::now();
     CUDA_TRY(cudaStreamSynchronize(st));  // the staging vectors go out of scope
+    {
+      std::lock_guard<std::mutex> g(g_stats.mu);
+      g_stats.s.prepare_ms[2] += 1e3 * secs(tn0, tn1);
+      g_stats.s.prepare_ms[3] += 1e3 * secs(tn1, Clock::now());
+    }
     return 0;
   }
 

@@ -544,7 +544,7 @@ def stats_read() -> dict:
             "timed_screen_bytes": int(s.timed_screen_bytes), "timed_compares": int(s.timed_compares),
             "h2d_bytes": int(s.h2d_bytes),
             "batch_ms": {k: float(s.batch_ms[i]) for i, k in enumerate(("before", "loop", "after"))},
-            "prepare_ms": {k: float(s.prepare_ms[i]) for i, k in enumerate(("encode", "upload"))}}
+            "prepare_ms": {k: float(s.prepare_ms[i]) for i, k in enumerate(("encode", "upload", "slots", "copy_wait"))}}
 
 
 ALIGN_VECTORIZED, ALIGN_HOMO, ALIGN_ENDSFREE = 0, 1, 2

@@ -52,7 +52,7 @@ class KernelStatsC(C.Structure):
     _fields_ = [("launches", C.c_uint64 * 4), ("ms", C.c_double * 4), ("rounds", C.c_uint64),
                 ("compares", C.c_uint64), ("screened", C.c_uint64), ("screen_bytes", C.c_uint64),
                 ("timed_rounds", C.c_uint64), ("timed_screen_bytes", C.c_uint64), ("timed_compares", C.c_uint64),
-                ("h2d_bytes", C.c_uint64), ("batch_ms", C.c_double * 3), ("prepare_ms", C.c_double * 2)]
+                ("h2d_bytes", C.c_uint64), ("batch_ms", C.c_double * 3), ("prepare_ms", C.c_double * 4)]
 
 
 class CountersC(C.Structure):

@@ -130,8 +130,10 @@ typedef struct {
   uint64_t h2d_bytes;  /* host-to-device bytes copied: uploads, lock flags, per-call task tables */
   double batch_ms[3];  /* wall time of dgpu_batch_run / dgpu_dada_batch runs: before the loop
                           (resets, sample state), the loop, after it (results, final-subs) */
-  double prepare_ms[2]; /* wall time of dgpu_batch_prepare / dgpu_dada_batch preparation:
-                           validation, encoding and pool set-up; upload and k-mer profiles */
+  double prepare_ms[4]; /* wall time of dgpu_batch_prepare / dgpu_dada_batch preparation:
+                           validation, encoding and pool set-up; upload and k-mer profiles;
+                           of the latter, the launch slots' set-up and the wait for the copies
+                           and the profile kernel */
 } dgpu_kernel_stats;
 
 const char* dgpu_last_error(void);
