@@ -615,3 +615,32 @@ def test_multi_device_service_matches_single_sample_calls():
         got = [svc.wait(t)[0] for t in ts]
     for s, g in zip(reqs, got):
         assert_same_dada(g, D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, D.DadaParams(), quals=s.quals))
+
+
+@pytest.fixture(scope="module")
+def config1_full():
+    return synth.config1(seed=1001)
+
+
+def test_config1_largest_samples_match_the_oracle(config1_full):
+    """The 40-sample workload at full size: its two largest samples (16,124
+    and 15,475 uniques, about 400 clusters each) denoised in one batch equal
+    the oracle's run_dada on each."""
+    w = config1_full
+    big = sorted(w.samples, key=lambda s: -len(s.seqs))[:2]
+    got = D.dada_uniques_batch(big, w.err, w.ncol, D.DadaParams())
+    import os
+
+    nt = max(2, (os.cpu_count() or 2))
+    for s, g in zip(big, got):
+        assert_same_dada(g, O.dada(s.seqs, s.abund, w.err, w.ncol, O.DadaParams(nthreads=nt), quals=s.quals))
+
+
+def test_config1_batched_equals_single_sample_path(config1_full):
+    """All 40 samples batched (six slots, one dedicated, up to four samples a
+    launch) give each sample exactly what the single-sample path gives it."""
+    w = config1_full
+    pb = D.PackedBatch(w.samples)
+    got = D.dada_uniques_batch(w.samples, w.err, w.ncol, D.DadaParams(), packed=pb)
+    for s, g in zip(w.samples, got):
+        assert_same_dada(g, D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, D.DadaParams(), quals=s.quals))
