@@ -2231,16 +2231,33 @@ static int sm_count() {
 void launch_compare(const CompareLaunch& L0, cudaStream_t st, cudaEvent_t* ev) {
   if (L0.total_items == 0) return;
   const int sms = sm_count();
-  const uint32_t cap = uint32_t(sms) * 8u;
-  // A warp screens its items a few at a time, one dependent round of profile
-  // loads each, so a small call spreads its items thin (down to 4 per warp)
-  // over more warps; a large one keeps 32 per warp within the block cap.
+  // One wave: k_screen's 64 registers x 256 threads leave room for 4 blocks
+  // per SM. A warp screens its chunk a few items at a time, one dependent
+  // round of profile loads each. A call that fits the wave at one chunk per
+  // warp takes the smallest chunk that does (its items spread thin over many
+  // warps); a larger one takes the largest chunk that still shares the
+  // chunks evenly over the wave's warps (at least 90 % of them busy in the
+  // last round), so no partial second wave or ragged tail is left; chunks
+  // stay at 16 or more there, since a chunk's per-item bookkeeping runs on
+  // one lane per item.
+  const uint32_t cap = uint32_t(sms) * 4u;
+  const uint64_t warps = uint64_t(cap) * kScreenWarps;
   CompareLaunch L = L0;
-  L.screen_chunk = 32;
-  while (L.screen_chunk > 4 && (L.total_items + kScreenWarps * (L.screen_chunk / 2) - 1) /
-                                       (kScreenWarps * (L.screen_chunk / 2)) <= cap)
-    L.screen_chunk /= 2;
-  uint32_t blocks = (L.total_items + kScreenWarps * L.screen_chunk - 1) / (kScreenWarps * L.screen_chunk);
+  auto nblocks = [&](uint32_t ch) {
+    return uint32_t((uint64_t(L.total_items) + kScreenWarps * ch - 1) / (uint64_t(kScreenWarps) * ch));
+  };
+  L.screen_chunk = 4;
+  if (nblocks(32) <= cap) {
+    while (nblocks(L.screen_chunk) > cap) L.screen_chunk *= 2;
+  } else {
+    for (uint32_t ch = 32; ch >= 16; ch /= 2) {
+      const uint64_t chunks = (uint64_t(L.total_items) + ch - 1) / ch;
+      const uint64_t rounds = (chunks + warps - 1) / warps;
+      L.screen_chunk = ch;
+      if (double(chunks) >= 0.9 * double(rounds * warps)) break;
+    }
+  }
+  uint32_t blocks = nblocks(L.screen_chunk);
   if (blocks > cap) blocks = cap;
   if (ev) cudaEventRecord(ev[0], st);
   switch (L.kp.kmer_size) {
