@@ -19,6 +19,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <string>
 #include <thread>
 #include <vector>
@@ -820,7 +821,7 @@ class Helpers {
 
 static constexpr size_t kParMin = 8192;   // loops shorter than this stay serial
 static constexpr size_t kParGrain = 2048;
-static constexpr size_t kParMinRepriced = 32;  // p-values worth splitting a reprice for
+static constexpr size_t kParMinRepriced = 2048;  // repriced members worth splitting a reprice for
 static constexpr size_t kRepriceGrain = 256;   // members per reprice chunk
 
 // ---------------------------------------------------------------------------
@@ -862,6 +863,21 @@ struct PosBits {
     const uint64_t m = uint64_t(1) << (r & 63);
     w[k] = v ? (w[k] | m) : (w[k] & ~m);
   }
+  // f(r) for every position in [lo, hi) set here and not in ex, ascending
+  template <class F>
+  void each_excluding(const PosBits& ex, size_t lo, size_t hi, F&& f) const {
+    hi = std::min(hi, w.size() * 64);
+    for (size_t k = lo >> 6; k * 64 < hi; ++k) {
+      uint64_t x = w[k] & ~(k < ex.w.size() ? ex.w[k] : uint64_t(0));
+      if (k * 64 < lo) x &= ~uint64_t(0) << (lo & 63);
+      while (x) {
+        const size_t r = k * 64 + size_t(__builtin_ctzll(x));
+        if (r >= hi) return;
+        f(r);
+        x &= x - 1;
+      }
+    }
+  }
   // f(r) for every set position in [lo, hi), ascending
   template <class F>
   void each(size_t lo, size_t hi, F&& f) const {
@@ -897,6 +913,13 @@ struct Cluster {
   std::vector<MemberInfo> info;  // info[r] describes raws[r]
   PosBits var;    // members that are repriced (not fixed_p)
   PosBits multi;  // members with two or more candidate clusters
+  // Members known to price at exactly 0.0 for as long as the cluster's reads
+  // stay at or below z_reads (non-prior bud candidates; see pA_floor), by
+  // reads descending then position: the reprice skips them and takes the
+  // first as its candidate among them. zbits marks their positions.
+  std::set<std::pair<uint32_t, uint32_t>> zset;  // (UINT32_MAX - reads, position)
+  PosBits zbits;
+  uint32_t z_reads = 0;
   uint32_t reads = 0;
   uint32_t nvar = 0;  // members whose p is repriced (not fixed at 1.0)
   bool update_e = true, check_locks = true;
@@ -1025,7 +1048,14 @@ struct SampleState {
   // rcomp[raw] = cp, and the copy beside the raw's place in its cluster
   void set_rcomp(uint32_t raw, const Comp& cp) {
     rcomp[raw] = cp;
-    clusters[raw_cluster[raw]].info[raw_pos[raw]] = member_info(raw);
+    Cluster& c = clusters[raw_cluster[raw]];
+    c.info[raw_pos[raw]] = member_info(raw);
+    zero_drop(c, raw_pos[raw]);  // its comp changed: no longer known to price at zero
+  }
+  void zero_drop(Cluster& c, size_t r) {
+    if (!c.zbits.get(r)) return;
+    c.zset.erase({UINT32_MAX - reads[c.raws[r]], uint32_t(r)});
+    c.zbits.put(r, false);
   }
 
   // Frees the per-raw state; batch_run calls it for all samples in parallel
@@ -1084,6 +1114,16 @@ struct SampleState {
     Cluster& c = clusters[ci];
     uint32_t raw = v[r];
     const size_t last = v.size() - 1;
+    zero_drop(c, r);
+    if (last != r && c.zbits.get(last)) {  // the last member moves to r
+      const uint32_t mv = UINT32_MAX - reads[v[last]];
+      c.zset.erase({mv, uint32_t(last)});
+      c.zbits.put(last, false);
+      if (r != 0) {  // position 0 is never a bud candidate
+        c.zset.insert({mv, uint32_t(r)});
+        c.zbits.put(r, true);
+      }
+    }
     v[r] = v.back();
     v.pop_back();
     c.info[r] = c.info.back();
@@ -1165,6 +1205,7 @@ struct SampleState {
   struct BudAcc {
     bool have = false, havep = false;
     BudCand bm{}, bmp{};
+    std::vector<uint32_t> newz;  // positions found to price at zero for good (see pA_floor)
   };
 
   // get_pA, answering 0.0 at once where calc_pA's log-space tail
@@ -1200,12 +1241,19 @@ struct SampleState {
   // underflowing (the test of get_pA_quick, loosened so it needs no log:
   // ax <= k * ex * ln 2 - e - lnGamma(k) for e = m * 2^ex, m in [0.5, 1);
   // -ln k <= 0; -ln(1 - r) <= 2r for r = e / (k + 1) < 1/2).
-  double pA_floor(uint32_t rd, bool pr, double lambda, uint32_t hamming, uint32_t bi_reads, bool* zero) const {
+  //
+  // *forever is set where that 0.0 holds for every smaller bi_reads too:
+  // lambda == 0, or the underflow test with e added to its left side (as
+  // bi_reads falls, e falls, ex does not grow and -e grows by less than e).
+  double pA_floor(uint32_t rd, bool pr, double lambda, uint32_t hamming, uint32_t bi_reads, bool* zero,
+                  bool* forever) const {
     *zero = false;
+    *forever = false;
     if (rd == 1 && !pr && !conf->detect_singletons) return 1.0;
     if (hamming == 0) return 1.0;
     if (lambda == 0.0) {
       *zero = true;
+      *forever = true;
       return 0.0;
     }
     const double e = lambda * double(bi_reads);
@@ -1223,6 +1271,7 @@ struct SampleState {
     if (ax_hi < -711.0) {  // below gamma_lr's underflow limit: no floor above 0
       const double r = e / (a + 1.0);
       *zero = r < 0.5 && ax_hi + 2.0 * r + 1.0 < -745.2;
+      *forever = r < 0.5 && ax_hi + e + 2.0 * r + 1.0 < -745.2;
       return 0.0;
     }
     const double ax = a * std::log(e) - e - lgamma_of(a);
@@ -1314,7 +1363,7 @@ struct SampleState {
     thread_local std::vector<double> floor_of;
     thread_local std::vector<uint8_t> zero_of;
     pos.clear();
-    bi.var.each(lo, hi, [&](size_t r) { pos.push_back(uint32_t(r)); });
+    bi.var.each_excluding(bi.zbits, lo, hi, [&](size_t r) { pos.push_back(uint32_t(r)); });
     floor_of.resize(pos.size());
     zero_of.resize(pos.size());
     double fmin = std::numeric_limits<double>::infinity(), fminp = fmin;
@@ -1324,10 +1373,11 @@ struct SampleState {
       const size_t r = pos[i];
       if (!eligible(r)) continue;
       const MemberInfo& m = info[r];
-      bool z = false;
-      const double f = pA_floor(m.reads, m.prior(), m.lambda, m.hamming(), bi_reads, &z);
+      bool z = false, fz = false;
+      const double f = pA_floor(m.reads, m.prior(), m.lambda, m.hamming(), bi_reads, &z, &fz);
       floor_of[i] = f;
       zero_of[i] = z;
+      if (fz && !m.prior()) acc.newz.push_back(uint32_t(r));
       if (!zmin && (!any || f < fmin || z)) {
         fmin = f;
         amin = r;
@@ -1380,9 +1430,16 @@ struct SampleState {
       Cluster& bi = clusters[i];
       if (bi.update_e) {
         const size_t nm = bi.raws.size();
+        if (!bi.zset.empty() && bi.reads > bi.z_reads) {  // the zero set holds only while reads do not grow
+          bi.zset.clear();
+          std::fill(bi.zbits.w.begin(), bi.zbits.w.end(), uint64_t(0));
+        }
         BudAcc acc;
         const size_t grain = kRepriceGrain;
-        if (bi.nvar < kParMinRepriced || nm < 2 * grain) {
+        // members the scan prices (the zero set is skipped); a short scan
+        // stays on this thread, since waking the helpers costs more
+        const size_t to_scan = bi.nvar > bi.zset.size() ? bi.nvar - bi.zset.size() : 0;
+        if (to_scan < kParMinRepriced || nm < 2 * grain) {
           reprice_range(bi, 0, nm, acc);
         } else {
           // chunk-local caches folded in chunk order: the same first-of-equals
@@ -1400,6 +1457,26 @@ struct SampleState {
               acc.bmp = a.bmp;
               acc.havep = true;
             }
+            acc.newz.insert(acc.newz.end(), a.newz.begin(), a.newz.end());
+          }
+        }
+        if (!acc.newz.empty()) {
+          for (uint32_t r : acc.newz) {
+            bi.zset.insert({UINT32_MAX - reads[bi.raws[r]], r});
+            bi.zbits.put(r, true);
+          }
+          bi.z_reads = bi.reads;
+        }
+        if (!bi.zset.empty()) {
+          // the zero set's first (most reads, then lowest position) is its
+          // candidate; against the scanned ones p = 0.0 ties break on reads,
+          // then on position (the scan keeps the first of equals)
+          const auto& zf = *bi.zset.begin();
+          const BudCand zc{0.0, UINT32_MAX - zf.first, zf.second, bi.raws[zf.second]};
+          if (!acc.have || zc.p < acc.bm.p ||
+              (zc.p == acc.bm.p && (zc.reads > acc.bm.reads || (zc.reads == acc.bm.reads && zc.r < acc.bm.r)))) {
+            acc.bm = zc;
+            acc.have = true;
           }
         }
         bi.has_bm = acc.have;
