@@ -962,6 +962,8 @@ struct SampleState {
   std::vector<double> p;
   std::vector<uint32_t> raw_cluster;
   std::vector<uint32_t> raw_pos;  // position of each raw in its cluster's member list
+  std::vector<uint32_t> center_raw;  // each cluster's center (compact, for the shuffle's scans)
+  std::vector<std::pair<uint64_t, uint32_t>> mv_buf;  // move_changed's work list
   std::vector<Cluster> clusters;
   std::vector<Cand> cand_pool;
   std::vector<uint32_t> cand_head, cand_tail;  // per raw: first and last candidate in cand_pool
@@ -1017,6 +1019,7 @@ struct SampleState {
     ncand.assign(n, 0);
     changed_mark.assign(n, 0);
     clusters.clear();
+    center_raw.clear();
     Cluster c0;
     c0.birth_e = double(total_reads);
     c0.raws.resize(n);
@@ -1040,6 +1043,8 @@ struct SampleState {
     for (uint32_t r : c.raws)
       if (reads[r] >= reads[best]) best = r;
     c.center = best;
+    if (center_raw.size() <= i) center_raw.resize(i + 1, UINT32_MAX);
+    center_raw[i] = best;
   }
 
   MemberInfo member_info(uint32_t raw) const {
@@ -1762,7 +1767,8 @@ struct SampleState {
   // mover, and appends to later clusters leave their positions alone, so the
   // pops and appends are exactly the full passes'.
   size_t move_changed() {
-    std::vector<std::pair<uint64_t, uint32_t>> mv;  // (cluster << 32 | ~position, raw)
+    std::vector<std::pair<uint64_t, uint32_t>>& mv = mv_buf;  // (cluster << 32 | ~position, raw)
+    mv.clear();
     for (uint32_t raw : changed_raws) {
       if (changed_mark[raw]) continue;
       changed_mark[raw] = 1;
@@ -1874,9 +1880,9 @@ struct SampleState {
       }
       // the centers of other clusters whose best is a cluster that lost reads
       if (!reads_fell_list.empty())
-        for (size_t cj = 0; cj < clusters.size(); ++cj) {
-          if (clusters[cj].center < 0) continue;
-          const uint32_t raw = uint32_t(clusters[cj].center);
+        for (size_t cj = 0; cj < center_raw.size(); ++cj) {
+          const uint32_t raw = center_raw[cj];
+          if (raw == UINT32_MAX) continue;
           const uint32_t bi = compmax[raw].i;
           if (bi != cj && reads_fell[bi] && !in_affected[raw]) {
             in_affected[raw] = 1;
