@@ -930,8 +930,6 @@ struct Cluster {
   Comp birth_comp;
   std::vector<Comp> comp;
   std::vector<double> comp64;  // with DadaConf::fp32: the FP64 lambda of each comp
-  bool has_bm = false, has_bmp = false;
-  BudCand bm{}, bmp{};
 };
 
 struct RunStats {
@@ -963,6 +961,10 @@ struct SampleState {
   std::vector<uint32_t> raw_cluster;
   std::vector<uint32_t> raw_pos;  // position of each raw in its cluster's member list
   std::vector<uint32_t> center_raw;  // each cluster's center (compact, for the shuffle's scans)
+  // each cluster's bud cache (src/pval.rs:91-123), kept compact for the bud
+  // scan: bm_flags bit 0 = a candidate, bit 1 = a prior candidate
+  std::vector<BudCand> bm_c, bmp_c;
+  std::vector<uint8_t> bm_flags;
   std::vector<std::pair<uint64_t, uint32_t>> mv_buf;  // move_changed's work list
   std::vector<Cluster> clusters;
   std::vector<Cand> cand_pool;
@@ -1020,6 +1022,9 @@ struct SampleState {
     changed_mark.assign(n, 0);
     clusters.clear();
     center_raw.clear();
+    bm_c.clear();
+    bmp_c.clear();
+    bm_flags.clear();
     Cluster c0;
     c0.birth_e = double(total_reads);
     c0.raws.resize(n);
@@ -1431,6 +1436,9 @@ struct SampleState {
 
   void p_update() {  // src/pval.rs:45-130
     const DadaConf& C = *conf;
+    bm_c.resize(clusters.size());
+    bmp_c.resize(clusters.size());
+    bm_flags.resize(clusters.size(), 0);
     for (size_t i = 0; i < clusters.size(); ++i) {
       Cluster& bi = clusters[i];
       if (bi.update_e) {
@@ -1484,10 +1492,9 @@ struct SampleState {
             acc.have = true;
           }
         }
-        bi.has_bm = acc.have;
-        bi.bm = acc.bm;
-        bi.has_bmp = acc.havep;
-        bi.bmp = acc.bmp;
+        bm_c[i] = acc.bm;
+        bmp_c[i] = acc.bmp;
+        bm_flags[i] = uint8_t((acc.have ? 1 : 0) | (acc.havep ? 2 : 0));
         bi.update_e = false;
       }
       if (C.greedy && bi.check_locks) {
@@ -1625,21 +1632,24 @@ struct SampleState {
     size_t mci = 0, mpci = 0;
     double min_p = p[ic], min_pp = p[ic];
     uint32_t min_r = reads[ic], min_rp = reads[ic];
-    for (size_t ci = 0; ci < clusters.size(); ++ci) {
-      const Cluster& c = clusters[ci];
-      if (c.has_bm && (c.bm.p < min_p || (c.bm.p == min_p && c.bm.reads > min_r))) {
+    for (size_t ci = 0; ci < bm_flags.size(); ++ci) {
+      const uint8_t fl = bm_flags[ci];
+      if (!fl) continue;
+      const BudCand& bm = bm_c[ci];
+      if ((fl & 1) && (bm.p < min_p || (bm.p == min_p && bm.reads > min_r))) {
         have = true;
-        m = c.bm;
+        m = bm;
         mci = ci;
-        min_p = c.bm.p;
-        min_r = c.bm.reads;
+        min_p = bm.p;
+        min_r = bm.reads;
       }
-      if (c.has_bmp && (c.bmp.p < min_pp || (c.bmp.p == min_pp && c.bmp.reads > min_rp))) {
+      const BudCand& bmp = bmp_c[ci];
+      if ((fl & 2) && (bmp.p < min_pp || (bmp.p == min_pp && bmp.reads > min_rp))) {
         havep = true;
-        mp = c.bmp;
+        mp = bmp;
         mpci = ci;
-        min_pp = c.bmp.p;
-        min_rp = c.bmp.reads;
+        min_pp = bmp.p;
+        min_rp = bmp.reads;
       }
     }
     const double p_a = min_p * double(n);
