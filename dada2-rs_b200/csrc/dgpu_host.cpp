@@ -1038,6 +1038,7 @@ struct SampleState {
     c0.reads = total_reads;
     for (uint32_t t = 0; t < n; ++t) c0.nvar += fixed_p[t] ? 0u : 1u;
     clusters.push_back(std::move(c0));
+    upd_list.assign(1, 0u);
     assign_center(0);
   }
 
@@ -1095,6 +1096,16 @@ struct SampleState {
     cand_tail[raw] = q;
   }
 
+  // clusters whose p-values need repricing: update_e set, listed once
+  std::vector<uint32_t> upd_list;
+  void mark_update(size_t ci) {
+    Cluster& c = clusters[ci];
+    if (!c.update_e) {
+      c.update_e = true;
+      upd_list.push_back(uint32_t(ci));
+    }
+  }
+
   void touch(size_t ci) {
     if (ci >= touched.size()) touched.resize(std::max(ci + 1, clusters.size()), 0);
     if (!touched[ci]) {
@@ -1115,7 +1126,7 @@ struct SampleState {
     clusters[ci].raws.push_back(raw);
     clusters[ci].reads += reads[raw];
     clusters[ci].nvar += fixed_p[raw] ? 0u : 1u;
-    clusters[ci].update_e = true;
+    mark_update(ci);
   }
 
   uint32_t pop_raw(size_t ci, size_t r) {  // src/containers.rs:424-435 (swap_remove)
@@ -1145,7 +1156,7 @@ struct SampleState {
     c.multi.put(last, false);
     clusters[ci].reads -= reads[raw];
     clusters[ci].nvar -= fixed_p[raw] ? 0u : 1u;
-    clusters[ci].update_e = true;
+    mark_update(ci);
     return raw;
   }
 
@@ -1439,7 +1450,9 @@ struct SampleState {
     bm_c.resize(clusters.size());
     bmp_c.resize(clusters.size());
     bm_flags.resize(clusters.size(), 0);
-    for (size_t i = 0; i < clusters.size(); ++i) {
+    // only the listed clusters can have update_e or check_locks set
+    std::sort(upd_list.begin(), upd_list.end());
+    for (const uint32_t i : upd_list) {
       Cluster& bi = clusters[i];
       if (bi.update_e) {
         const size_t nm = bi.raws.size();
@@ -1510,6 +1523,7 @@ struct SampleState {
         bi.check_locks = false;
       }
     }
+    upd_list.clear();
   }
 
   double get_pA(uint32_t rd, bool pr, double lambda, uint32_t hamming, uint32_t bi_reads) const {  // src/pval.rs:376-398
@@ -1672,6 +1686,7 @@ struct SampleState {
     nb.birth_comp = bc;
     clusters.push_back(std::move(nb));
     const size_t nci = clusters.size() - 1;
+    upd_list.push_back(uint32_t(nci));  // born with update_e and check_locks set
     add_raw(nci, raw);
     assign_center(nci);
     return int64_t(nci);
