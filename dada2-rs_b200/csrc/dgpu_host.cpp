@@ -916,9 +916,13 @@ struct Cluster {
   // Members known to price at exactly 0.0 for as long as the cluster's reads
   // stay at or below z_reads (non-prior bud candidates; see pA_floor), by
   // reads descending then position: the reprice skips them and takes the
-  // first as its candidate among them. zbits marks their positions.
-  std::set<std::pair<uint32_t, uint32_t>> zset;  // (UINT32_MAX - reads, position)
+  // first as its candidate among them. zbits marks their positions (and
+  // zcount counts them); zheap is a min-heap on (UINT32_MAX - reads,
+  // position, raw) whose entries count only while that position is marked
+  // and still holds that raw, so a member leaves the set by clearing its bit.
+  std::vector<std::array<uint32_t, 3>> zheap;
   PosBits zbits;
+  uint32_t zcount = 0;
   uint32_t z_reads = 0;
   uint32_t reads = 0;
   uint32_t nvar = 0;  // members whose p is repriced (not fixed at 1.0)
@@ -1063,10 +1067,43 @@ struct SampleState {
     c.info[raw_pos[raw]] = member_info(raw);
     zero_drop(c, raw_pos[raw]);  // its comp changed: no longer known to price at zero
   }
+  static bool zero_valid(const Cluster& c, const std::array<uint32_t, 3>& e) {
+    return c.zbits.get(e[1]) && e[1] < c.raws.size() && c.raws[e[1]] == e[2];
+  }
+  void zero_add(Cluster& c, size_t r, uint32_t raw) {
+    if (!c.zbits.get(r)) ++c.zcount;
+    c.zbits.put(r, true);
+    c.zheap.push_back({UINT32_MAX - reads[raw], uint32_t(r), raw});
+    std::push_heap(c.zheap.begin(), c.zheap.end(), std::greater<>());
+  }
+  // The zero set's first member (most reads, then lowest position), dropping
+  // stale heap entries; false when the set is empty.
+  bool zero_first(Cluster& c, uint32_t* zr, uint32_t* zpos) {
+    if (c.zcount == 0) {
+      c.zheap.clear();
+      return false;
+    }
+    if (c.zheap.size() > 2 * size_t(c.zcount) + 4096) {  // mostly stale: rebuild
+      std::vector<std::array<uint32_t, 3>> keep;
+      keep.reserve(c.zcount);
+      for (const auto& e : c.zheap)
+        if (zero_valid(c, e)) keep.push_back(e);
+      c.zheap.swap(keep);
+      std::make_heap(c.zheap.begin(), c.zheap.end(), std::greater<>());
+    }
+    while (!c.zheap.empty() && !zero_valid(c, c.zheap.front())) {
+      std::pop_heap(c.zheap.begin(), c.zheap.end(), std::greater<>());
+      c.zheap.pop_back();
+    }
+    if (c.zheap.empty()) return false;
+    *zr = UINT32_MAX - c.zheap.front()[0];
+    *zpos = c.zheap.front()[1];
+    return true;
+  }
   void zero_drop(Cluster& c, size_t r) {
     if (!c.zbits.get(r)) return;
-    c.zset.erase({UINT32_MAX - reads[c.raws[r]], uint32_t(r)});
     c.zbits.put(r, false);
+    --c.zcount;
   }
 
   // Frees the per-raw state; batch_run calls it for all samples in parallel
@@ -1137,13 +1174,9 @@ struct SampleState {
     const size_t last = v.size() - 1;
     zero_drop(c, r);
     if (last != r && c.zbits.get(last)) {  // the last member moves to r
-      const uint32_t mv = UINT32_MAX - reads[v[last]];
-      c.zset.erase({mv, uint32_t(last)});
       c.zbits.put(last, false);
-      if (r != 0) {  // position 0 is never a bud candidate
-        c.zset.insert({mv, uint32_t(r)});
-        c.zbits.put(r, true);
-      }
+      --c.zcount;
+      if (r != 0) zero_add(c, r, v[last]);  // position 0 is never a bud candidate
     }
     v[r] = v.back();
     v.pop_back();
@@ -1359,7 +1392,12 @@ struct SampleState {
     });
   }
 
-  void reprice_range(const Cluster& bi, size_t lo, size_t hi, BudAcc& acc) {
+  // With a zero set, zr / zpos are its first member's reads and position (else
+  // zr = 0): a non-prior member with fewer reads, or as many at a later
+  // position, can beat that p = 0.0 candidate neither on p nor on the ties,
+  // so it is not visited.
+  void reprice_range(const Cluster& bi, size_t lo, size_t hi, BudAcc& acc, uint32_t zr = 0,
+                     uint32_t zpos = 0) {
     if (conf->fp32) {
       reprice_range_fp32(bi, lo, hi, acc);
       return;
@@ -1384,7 +1422,14 @@ struct SampleState {
     thread_local std::vector<double> floor_of;
     thread_local std::vector<uint8_t> zero_of;
     pos.clear();
-    bi.var.each_excluding(bi.zbits, lo, hi, [&](size_t r) { pos.push_back(uint32_t(r)); });
+    if (zr == 0) {
+      bi.var.each_excluding(bi.zbits, lo, hi, [&](size_t r) { pos.push_back(uint32_t(r)); });
+    } else {
+      bi.var.each_excluding(bi.zbits, lo, hi, [&](size_t r) {
+        const MemberInfo& m = info[r];
+        if (m.prior() || m.reads > zr || (m.reads == zr && r < zpos)) pos.push_back(uint32_t(r));
+      });
+    }
     floor_of.resize(pos.size());
     zero_of.resize(pos.size());
     double fmin = std::numeric_limits<double>::infinity(), fminp = fmin;
@@ -1456,23 +1501,26 @@ struct SampleState {
       Cluster& bi = clusters[i];
       if (bi.update_e) {
         const size_t nm = bi.raws.size();
-        if (!bi.zset.empty() && bi.reads > bi.z_reads) {  // the zero set holds only while reads do not grow
-          bi.zset.clear();
+        if (bi.zcount && bi.reads > bi.z_reads) {  // the zero set holds only while reads do not grow
+          bi.zheap.clear();
+          bi.zcount = 0;
           std::fill(bi.zbits.w.begin(), bi.zbits.w.end(), uint64_t(0));
         }
         BudAcc acc;
+        uint32_t zr = 0, zpos = 0;  // the zero set's first member, if any
+        zero_first(bi, &zr, &zpos);
         const size_t grain = kRepriceGrain;
         // members the scan prices (the zero set is skipped); a short scan
         // stays on this thread, since waking the helpers costs more
-        const size_t to_scan = bi.nvar > bi.zset.size() ? bi.nvar - bi.zset.size() : 0;
+        const size_t to_scan = bi.nvar > bi.zcount ? bi.nvar - bi.zcount : 0;
         if (to_scan < kParMinRepriced || nm < 2 * grain) {
-          reprice_range(bi, 0, nm, acc);
+          reprice_range(bi, 0, nm, acc, zr, zpos);
         } else {
           // chunk-local caches folded in chunk order: the same first-of-equals
           // winner as one ascending scan
           std::vector<BudAcc> part((nm + grain - 1) / grain);
           Helpers::get().parallel_for(nm, grain, [&](size_t c, size_t lo, size_t hi) {
-            reprice_range(bi, lo, hi, part[c]);
+            reprice_range(bi, lo, hi, part[c], zr, zpos);
           });
           for (const BudAcc& a : part) {
             if (a.have && (!acc.have || better(a.bm, acc.bm))) {
@@ -1487,18 +1535,15 @@ struct SampleState {
           }
         }
         if (!acc.newz.empty()) {
-          for (uint32_t r : acc.newz) {
-            bi.zset.insert({UINT32_MAX - reads[bi.raws[r]], r});
-            bi.zbits.put(r, true);
-          }
+          for (uint32_t r : acc.newz) zero_add(bi, r, bi.raws[r]);
           bi.z_reads = bi.reads;
         }
-        if (!bi.zset.empty()) {
+        uint32_t zr2 = 0, zp2 = 0;
+        if (zero_first(bi, &zr2, &zp2)) {
           // the zero set's first (most reads, then lowest position) is its
           // candidate; against the scanned ones p = 0.0 ties break on reads,
           // then on position (the scan keeps the first of equals)
-          const auto& zf = *bi.zset.begin();
-          const BudCand zc{0.0, UINT32_MAX - zf.first, zf.second, bi.raws[zf.second]};
+          const BudCand zc{0.0, zr2, zp2, bi.raws[zp2]};
           if (!acc.have || zc.p < acc.bm.p ||
               (zc.p == acc.bm.p && (zc.reads > acc.bm.reads || (zc.reads == acc.bm.reads && zc.r < acc.bm.r)))) {
             acc.bm = zc;
