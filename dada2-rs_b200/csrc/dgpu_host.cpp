@@ -821,7 +821,7 @@ class Helpers {
 
 static constexpr size_t kParMin = 8192;   // loops shorter than this stay serial
 static constexpr size_t kParGrain = 2048;
-static constexpr size_t kParMinRepriced = 2048;  // repriced members worth splitting a reprice for
+static constexpr size_t kParMinRepriced = 16384;  // repriced members worth splitting a reprice for
 static constexpr size_t kRepriceGrain = 256;   // members per reprice chunk
 
 // ---------------------------------------------------------------------------
