@@ -853,15 +853,23 @@ static constexpr uint32_t kNoCand = 0xffffffffu;
 // the property. Updated with the member list, so scans can skip the rest.
 struct PosBits {
   std::vector<uint64_t> w;
+  std::vector<uint64_t> sum;  // bit k set iff w[k] != 0, so sparse scans skip empty words
   bool get(size_t r) const { return (r >> 6) < w.size() && ((w[r >> 6] >> (r & 63)) & 1u); }
   void put(size_t r, bool v) {
     const size_t k = r >> 6;
     if (k >= w.size()) {
       if (!v) return;
       w.resize(k + 1, 0);
+      sum.resize((w.size() + 63) >> 6, 0);
     }
     const uint64_t m = uint64_t(1) << (r & 63);
     w[k] = v ? (w[k] | m) : (w[k] & ~m);
+    const uint64_t sm = uint64_t(1) << (k & 63);
+    sum[k >> 6] = w[k] ? (sum[k >> 6] | sm) : (sum[k >> 6] & ~sm);
+  }
+  void clear() {
+    std::fill(w.begin(), w.end(), uint64_t(0));
+    std::fill(sum.begin(), sum.end(), uint64_t(0));
   }
   // f(r) for every position in [lo, hi) set here and not in ex, ascending
   template <class F>
@@ -878,18 +886,27 @@ struct PosBits {
       }
     }
   }
-  // f(r) for every set position in [lo, hi), ascending
+  // f(r) for every set position in [lo, hi), ascending (nonempty words only)
   template <class F>
   void each(size_t lo, size_t hi, F&& f) const {
     hi = std::min(hi, w.size() * 64);
-    for (size_t k = lo >> 6; k * 64 < hi; ++k) {
-      uint64_t x = w[k];
-      if (k * 64 < lo) x &= ~uint64_t(0) << (lo & 63);
-      while (x) {
-        const size_t r = k * 64 + size_t(__builtin_ctzll(x));
-        if (r >= hi) return;
-        f(r);
-        x &= x - 1;
+    if (lo >= hi) return;
+    const size_t k0 = lo >> 6, k1 = (hi - 1) >> 6;
+    for (size_t sk = k0 >> 6; sk <= (k1 >> 6); ++sk) {
+      uint64_t y = sum[sk];
+      if (sk == (k0 >> 6)) y &= ~uint64_t(0) << (k0 & 63);
+      while (y) {
+        const size_t k = sk * 64 + size_t(__builtin_ctzll(y));
+        y &= y - 1;
+        if (k > k1) return;
+        uint64_t x = w[k];
+        if (k == k0) x &= ~uint64_t(0) << (lo & 63);
+        while (x) {
+          const size_t r = k * 64 + size_t(__builtin_ctzll(x));
+          if (r >= hi) return;
+          f(r);
+          x &= x - 1;
+        }
       }
     }
   }
@@ -1504,7 +1521,7 @@ struct SampleState {
         if (bi.zcount && bi.reads > bi.z_reads) {  // the zero set holds only while reads do not grow
           bi.zheap.clear();
           bi.zcount = 0;
-          std::fill(bi.zbits.w.begin(), bi.zbits.w.end(), uint64_t(0));
+          bi.zbits.clear();
         }
         BudAcc acc;
         uint32_t zr = 0, zpos = 0;  // the zero set's first member, if any
