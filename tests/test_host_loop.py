@@ -1,0 +1,89 @@
+"""The product's clustering loop on the CPU: SampleState's absorb, shuffle,
+p-update (floors, zero set), bud and final pass, driven by the oracle's
+compare instead of the GPU kernels (tests/host_loop_driver.cpp), must give
+the oracle's own run_dada result bit for bit. Host only: no GPU."""
+import os
+import shutil
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+from dada2_b200 import synth
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _cuda_home():
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    return os.path.dirname(os.path.dirname(os.path.realpath(nvcc)))
+
+
+@pytest.fixture(scope="module")
+def driver(tmp_path_factory):
+    cuda = _cuda_home()
+    lib = os.path.join(cuda, "lib64")
+    out = str(tmp_path_factory.mktemp("hostloop") / "driver")
+    cmd = ["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-I", os.path.join(ROOT, "dada2-rs_b200", "csrc"),
+           "-I", os.path.join(ROOT, "include"), "-I", os.path.join(cuda, "include"),
+           os.path.join(ROOT, "tests", "host_loop_driver.cpp"), os.path.join(ROOT, "oracle", "dada_oracle.cpp"),
+           os.path.join(ROOT, "oracle", "oracle_capi.cpp"), "-o", out, "-L", lib, f"-Wl,-rpath,{lib}", "-lcudart",
+           "-lpthread"]
+    subprocess.run(cmd, check=True, capture_output=True)
+    return out
+
+
+def _run(driver, tmp_path, s, err, ncol):
+    enc = [x.encode() for x in s.seqs]
+    lens = np.array([len(x) for x in enc], np.uint32)
+    q = np.concatenate([np.asarray(a, np.uint32) for a in s.quals])
+    path = tmp_path / "sample.bin"
+    with open(path, "wb") as f:
+        f.write(struct.pack("<iii", len(enc), int(lens.sum()), ncol))
+        f.write(lens.tobytes())
+        f.write(b"".join(enc))
+        f.write(np.asarray(s.abund, np.uint32).tobytes())
+        f.write(q.tobytes())
+        f.write(np.ascontiguousarray(err, np.float64).tobytes())
+    out = subprocess.run([driver, str(path)], check=True, capture_output=True, text=True).stdout
+    rows = {}
+    for line in out.splitlines():
+        k, *v = line.split()
+        rows[k] = v
+    return rows
+
+
+def _f64(hexes):
+    return np.array([int(h, 16) for h in hexes], np.uint64).view(np.float64)
+
+
+@pytest.mark.parametrize("case", ["small41", "small42", "config0", "pooled4"])
+def test_host_loop_matches_the_oracle(driver, tmp_path, case):
+    if case == "config0":
+        w = synth.config0()
+    elif case == "pooled4":
+        w = synth.config3(nsamples=4, nvariants=300, reads_per_sample=6000, workers=1)
+    else:
+        w = synth.small_illumina(int(case[-2:]), nvariants=7, nreads=4000, L=150)
+    s = w.samples[0]
+    got = _run(driver, tmp_path, s, w.err, w.ncol)
+    want = O.dada(s.seqs, s.abund, w.err, w.ncol, O.DadaParams(nthreads=4), quals=s.quals)
+    assert int(got["nclust"][0]) == want["nclust"]
+    assert np.array_equal(np.array(got["map"], np.int64), want["map"].astype(np.int64))
+    assert _f64(got["pvals"]).tobytes() == want["pvals"].tobytes()
+    assert [int(x) for x in got["cl_reads"]] == [c["reads"] for c in want["clusters"]]
+    assert [int(x) for x in got["cl_birth_type"]] == [c["birth_type"] for c in want["clusters"]]
+    off = [int(x) for x in got["cl_mem_off"]]
+    raws = np.array(got["mem_raw"], np.int64)
+    lam, pv = _f64(got["mem_lambda"]), _f64(got["mem_pval"])
+    bp, bf, be = _f64(got["cl_birth_pval"]), _f64(got["cl_birth_fold"]), _f64(got["cl_birth_e"])
+    for ci, c in enumerate(want["clusters"]):
+        a, b = off[ci], off[ci + 1]
+        assert np.array_equal(raws[a:b], c["members"].astype(np.int64))
+        assert lam[a:b].tobytes() == c["lambdas"].tobytes()
+        assert pv[a:b].tobytes() == c["pvals"].tobytes()
+        assert np.float64(bp[ci]).tobytes() == np.float64(c["birth_pval"]).tobytes()
+        assert np.float64(bf[ci]).tobytes() == np.float64(c["birth_fold"]).tobytes()
+        assert np.float64(be[ci]).tobytes() == np.float64(c["birth_e"]).tobytes()
