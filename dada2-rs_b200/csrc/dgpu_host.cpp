@@ -1353,12 +1353,6 @@ struct SampleState {
     return lb * (1.0 - 1e-9);
   }
 
-  // Members [lo, hi) of cluster bi: reprice and fold into a local cache. Only
-  // the bud candidates (src/pval.rs:91-123) and cluster 0's center (the bud
-  // scan's starting p) read these p-values; the final pass prices every member
-  // again. So a candidate whose floor lies above the exact p of the candidate
-  // with the lowest floor (above both, for a prior raw) can be neither cache
-  // entry and is not priced: the cache is the one a full scan builds.
   // ---- FP32 lambda decisions (DadaConf::fp32) ----
   std::atomic<uint64_t> fp32_evals{0}, fp32_fallbacks{0};
   static bool near_threshold(double pv, double omega) { return pv >= omega * 1e-3 && pv <= omega * 1e3; }
@@ -1409,6 +1403,13 @@ struct SampleState {
     });
   }
 
+  // Members [lo, hi) of cluster bi: reprice and fold into a local cache. Only
+  // the bud candidates (src/pval.rs:91-123) and cluster 0's center (the bud
+  // scan's starting p) read these p-values; the final pass prices every member
+  // again. So a candidate whose floor lies above the exact p of the candidate
+  // with the lowest floor (above both, for a prior raw) can be neither cache
+  // entry and is not priced: the cache is the one a full scan builds.
+  //
   // With a zero set, zr / zpos are its first member's reads and position (else
   // zr = 0): a non-prior member with fewer reads, or as many at a later
   // position, can beat that p = 0.0 candidate neither on p nor on the ties,
