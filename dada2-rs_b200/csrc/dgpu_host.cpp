@@ -1226,6 +1226,15 @@ struct SampleState {
   void absorb(size_t ci, const Slot& P, uint32_t t) {
     uint32_t ctr[TC_NCOUNTERS];
     P.task_counters(t, ctr);
+    absorb_from(ci, ctr, P.task_self.h[t], [&](auto&& f) { P.for_each_stored(t, f); });
+  }
+
+  // absorb for comps from any source: ctr = the call's counters (TC_STORED =
+  // the number of comps), self = the center's own lambda, and each(f) calls
+  // f(index, lambda, hamming, FP32 ln lambda) for every stored comp in
+  // ascending raw order.
+  template <class Each>
+  void absorb_from(size_t ci, const uint32_t* ctr, double self, Each&& each) {
     const uint32_t ns = ctr[TC_STORED];
     nalign += ctr[TC_SCREENED];
     nshroud += ctr[TC_SHROUD];
@@ -1239,13 +1248,13 @@ struct SampleState {
     stats.homo += ctr[TC_HOMO];
     stats.endsfree += ctr[TC_ENDSFREE];
     Cluster& c = clusters[ci];
-    c.self_ = P.task_self.h[t];
+    c.self_ = self;
     c.comp.clear();
     c.comp.reserve(ns);
     const uint32_t center = uint32_t(c.center);
     c.comp64.clear();
     const bool fp32 = conf->fp32;
-    P.for_each_stored(t, [&](uint32_t idx, double lam, uint32_t ham, float ll32) {
+    each([&](uint32_t idx, double lam, uint32_t ham, float ll32) {
       // with fp32 the decisions take exp of the FP32 log-sum; the FP64
       // product is kept beside for the threshold fallback
       const double ld = !fp32 || lam == 0.0 ? lam : std::exp(double(ll32));
@@ -2922,6 +2931,165 @@ int dada_batch_each(int device, const dgpu_dada_params* params, int nsamples, co
   return rc;
 }
 
+// ---------------------------------------------------------------------------
+// One sample sharded over ranks (one process or thread per GPU)
+// ---------------------------------------------------------------------------
+// Every rank holds the whole sample and runs the same clustering loop; a
+// compare call screens and aligns only the rank's contiguous share of the
+// uniques, and the stored comps of all shares are gathered in rank order,
+// which is the ascending raw order of a single-device store
+// (src/cluster.rs:351-397). The host phases are deterministic, so every rank
+// takes the same next center and the same number of exchanges.
+
+// One rank's outcome of one compare call (or of the setup, with err alone).
+struct ShardHead {
+  int32_t err;        // 0, or the rank's DGPU_E_* code
+  uint32_t ns;        // comps stored from the rank's share
+  uint32_t has_self;  // the center lies in the rank's share
+  uint32_t pad;
+  double self;        // the center's own lambda, with has_self
+  uint32_t ctr[TC_NCOUNTERS];
+};
+struct ShardComp {
+  uint32_t index, hamming;
+  double lambda;
+  float ll32;
+  uint32_t pad;
+};
+static_assert(sizeof(ShardHead) == 56 && sizeof(ShardComp) == 24, "exchange records have a fixed layout");
+
+// All-gather of fixed-size blocks: send `bytes` bytes, receive world * bytes
+// with rank r's block at r * bytes; nonzero when the exchange failed.
+using ShardGather = std::function<int(const void* send, uint64_t bytes, void* recv)>;
+
+// Shares of the uniques [0, n), contiguous and balanced by bases (the work of
+// a compare grows with the raw's length); world + 1 bounds.
+static std::vector<uint32_t> shard_bounds(const uint32_t* lens, uint32_t n, int world) {
+  uint64_t tot = 0;
+  for (uint32_t t = 0; t < n; ++t) tot += lens[t];
+  std::vector<uint32_t> b(size_t(world) + 1, n);
+  b[0] = 0;
+  int r = 1;
+  uint64_t acc = 0;
+  for (uint32_t t = 0; t < n && r < world; ++t) {
+    acc += lens[t];
+    while (r < world && acc * uint64_t(world) >= tot * uint64_t(r)) b[size_t(r++)] = t + 1;
+  }
+  return b;
+}
+
+// The heads of every rank; fails on every rank alike when any rank failed.
+static int shard_heads(const ShardHead& mine, int world, const ShardGather& gather, std::vector<ShardHead>& heads) {
+  heads.assign(size_t(world), ShardHead{});
+  if (gather(&mine, sizeof(ShardHead), heads.data())) return fail(DGPU_E_INVALID, "shard exchange failed");
+  if (mine.err) return mine.err;  // this rank's own message stands
+  for (int r = 0; r < world; ++r)
+    if (heads[size_t(r)].err)
+      return fail(heads[size_t(r)].err, "rank " + std::to_string(r) + " of the sharded run failed");
+  return 0;
+}
+
+// One compare call's exchange: gathers every rank's head and comps and folds
+// them into S in rank order. Every rank calls it once per compare call, its
+// own call failed or not, so that the ranks stay in step.
+static int shard_exchange(SampleState& S, size_t ci, const ShardHead& mine, const std::vector<ShardComp>& local,
+                          int world, const ShardGather& gather) {
+  std::vector<ShardHead> heads;
+  TRY(shard_heads(mine, world, gather, heads));
+  uint32_t maxns = 0;
+  for (const ShardHead& h : heads) maxns = std::max(maxns, h.ns);
+  std::vector<ShardComp> all(size_t(world) * maxns);
+  if (maxns) {
+    std::vector<ShardComp> send(maxns, ShardComp{});
+    std::copy(local.begin(), local.end(), send.begin());
+    if (gather(send.data(), uint64_t(maxns) * sizeof(ShardComp), all.data()))
+      return fail(DGPU_E_INVALID, "shard exchange failed");
+  }
+  uint32_t ctr[TC_NCOUNTERS] = {};
+  double self = 0.0;
+  for (const ShardHead& h : heads) {
+    for (int k = 0; k < TC_NCOUNTERS; ++k) ctr[k] += h.ctr[k];
+    if (h.has_self) self = h.self;
+  }
+  S.absorb_from(ci, ctr, self, [&](auto&& f) {
+    for (int r = 0; r < world; ++r)
+      for (uint32_t k = 0; k < heads[size_t(r)].ns; ++k) {
+        const ShardComp& c = all[size_t(r) * maxns + k];
+        f(c.index, c.lambda, c.hamming, c.ll32);
+      }
+  });
+  return 0;
+}
+
+// This rank's compare of cluster ci's center against the uniques [lo, hi).
+static int shard_compare(Pool& P, SampleState& S, size_t ci, double cutoff, uint32_t lo, uint32_t hi, ShardHead& h,
+                         std::vector<ShardComp>& local) {
+  h = ShardHead{};
+  local.clear();
+  Slot& L = P.slot0();
+  if (S.lock_dirty) {
+    TRY(P.push_locks(S.base, S.n, L.st));
+    S.lock_dirty = false;
+  }
+  if (lo == hi) return 0;
+  TRY(L.ensure_tasks(1));
+  TaskDev T = S.task_for(ci, cutoff);
+  T.base = S.base + lo;
+  T.n = hi - lo;
+  L.task_stage.h[0] = T;
+  TRY(L.run_compare(1, true, nullptr));
+  L.task_counters(0, h.ctr);
+  h.ns = h.ctr[TC_STORED];
+  h.has_self = T.center >= T.base && T.center - T.base < T.n ? 1u : 0u;
+  h.self = h.has_self ? L.task_self.h[0] : 0.0;
+  local.reserve(h.ns);
+  L.for_each_stored(0, [&](uint32_t idx, double lam, uint32_t ham, float ll) {
+    local.push_back(ShardComp{lo + idx, ham, lam, ll, 0u});
+  });
+  return 0;
+}
+
+// The clustering loop of the batch's one sample with the compares sharded;
+// prep_rc = this rank's batch_prepare outcome, exchanged first so that a rank
+// that could not prepare stops the others before their first compare.
+static int shard_run(Batch& B, int prep_rc, int rank, int world, const ShardGather& gather, dgpu_result** out) {
+  Pool& P = B.pool;
+  const auto t0 = Clock::now();
+  std::vector<SampleState> S(1);
+  SampleState& s = S[0];
+  ShardHead setup{};
+  setup.err = prep_rc ? prep_rc : [&]() -> int {
+    CUDA_TRY(cudaSetDevice(P.device));
+    TRY(P.reset_e_minmax());
+    std::memset(P.lock_host.h, 0, P.nraw);
+    CUDA_TRY(cudaMemsetAsync(P.lock.p, 0, P.nraw, P.st));
+    CUDA_TRY(cudaStreamSynchronize(P.st));
+    return 0;
+  }();
+  std::vector<ShardHead> heads;
+  TRY(shard_heads(setup, world, gather, heads));
+  s.init(B.counts[0], B.bases[0], B.E.reads.data(), B.E.prior.data(), P.lock_host.h, &B.confs[0]);
+  const std::vector<uint32_t> bounds = shard_bounds(B.E.len.data(), s.n, world);
+  const uint32_t lo = bounds[size_t(rank)], hi = bounds[size_t(rank) + 1];
+  ShardHead h{};
+  std::vector<ShardComp> local;
+  for (int64_t ci = 0; ci >= 0;) {
+    const auto tc = Clock::now();
+    const int rc = shard_compare(P, s, size_t(ci), ci == 0 ? 1.0 : B.align.kdist_cutoff, lo, hi, h, local);
+    if (rc) h = ShardHead{rc, 0, 0, 0, 0.0, {}};
+    TRY(shard_exchange(s, size_t(ci), h, local, world, gather));
+    const auto th = Clock::now();
+    s.stats.t_compare += secs(tc, th);
+    ci = s.advance(size_t(ci));
+    s.stats.t_host += secs(th, Clock::now());
+  }
+  s.stats.t_done = s.stats.t_total = secs(t0, Clock::now());
+  out[0] = finish(s, SampleSeqs{B.E.seq, B.E.off.data(), B.E.len.data()});
+  const int rc = B.transitions ? final_subs(B, S, out) : 0;
+  s.release();
+  return rc;
+}
+
 }  // namespace dgpu
 
 // ---------------------------------------------------------------------------
@@ -3145,6 +3313,35 @@ int dgpu_dada(int device, const dgpu_dada_params* params, int nraw, const char* 
   dgpu_dada_params p1 = *params;
   p1.host_threads = 1;
   return dgpu_dada_batch(device, &p1, 1, ss, seqs, offs, lens, abund, prior, qual_sums, err_mat, ncol, out);
+}
+
+int dgpu_dada_sharded(int device, const dgpu_dada_params* params, int nraw, const char* seqs, const uint32_t* offs,
+                      const uint32_t* lens, const uint32_t* abund, const uint8_t* prior, const uint32_t* qual_sums,
+                      const double* err_mat, int ncol, int rank, int world, dgpu_allgather_fn gather, void* user,
+                      dgpu_result** out) {
+  // argument errors return before the first exchange: they are the caller's on every rank
+  if (!out || !gather) return fail(DGPU_E_INVALID, "null output or gather");
+  if (world < 1 || rank < 0 || rank >= world) return fail(DGPU_E_INVALID, "rank out of range of world");
+  *out = nullptr;
+  const ShardGather g = [&](const void* s, uint64_t bytes, void* r) { return gather(user, s, bytes, r); };
+  Batch b;
+  int prep = 0;
+  if (nraw <= 0) {
+    prep = fail(DGPU_E_INVALID, "Zero input sequences.");
+  } else if (!params) {
+    prep = fail(DGPU_E_INVALID, "null params");
+  } else {
+    const uint32_t ss[2] = {0, uint32_t(nraw)};
+    dgpu_dada_params p1 = *params;
+    p1.host_threads = 1;
+    prep = batch_prepare(b, device, &p1, 1, ss, seqs, offs, lens, abund, prior, qual_sums, err_mat, ncol);
+  }
+  const int rc = shard_run(b, prep, rank, world, g, out);
+  if (rc) {
+    delete *out;
+    *out = nullptr;
+  }
+  return rc;
 }
 
 int dgpu_dada_batch(int device, const dgpu_dada_params* params, int nsamples, const uint32_t* sample_start,

@@ -23,7 +23,7 @@ import numpy as np
 from ._lib import (AlignParamsC, CountersC, DadaOutC, DadaParamsC, DgpuError, InvalidInput, KernelStatsC,
                    check, device_count, lib, ptr)
 
-__all__ = ["AlignParams", "DadaParams", "CompareContext", "dada_uniques", "dada_uniques_batch",
+__all__ = ["AlignParams", "DadaParams", "CompareContext", "dada_uniques", "dada_uniques_batch", "dada_uniques_sharded",
            "ResidentBatch", "PackedBatch", "DenoiseService", "pack_sample", "Derep", "derep_fastq", "dada_fastq", "align_pairs", "stats_reset", "stats_timing", "stats_read",
            "DgpuError", "InvalidInput", "device_count", "METHOD_NAMES", "KERNEL_NAMES"]
 
@@ -280,6 +280,47 @@ def dada_uniques(seqs, abund, err, ncol, params: DadaParams | None = None, quals
                           ptr(qcat), ptr(err), int(ncol), C.byref(h)))
     try:
         return _read_result(h) if read_result else _read_counters(h)
+    finally:
+        lib().dgpu_result_free(h)
+
+
+def _c_gather(gather, world: int):
+    """A dgpu_allgather_fn over the Python callable ``gather`` (uint8 block ->
+    the world's blocks back to back). A raised exception or a wrong size
+    returns nonzero, which fails the sharded run on this rank."""
+    from ._lib import ALLGATHER_FN
+
+    def cb(user, send, nbytes, recv):
+        try:
+            block = np.frombuffer((C.c_uint8 * nbytes).from_address(send), np.uint8).copy()
+            out = np.ascontiguousarray(gather(block), np.uint8).reshape(-1)
+            if out.size != nbytes * world:
+                return 1
+            C.memmove(recv, out.ctypes.data, out.size)
+            return 0
+        except Exception:  # noqa: BLE001 - any failure is reported to the C side as nonzero
+            return 1
+
+    return ALLGATHER_FN(cb)
+
+
+def dada_uniques_sharded(seqs, abund, err, ncol, params: DadaParams | None = None, quals=None, prior=None, *,
+                         rank: int, world: int, gather, device: int = 0, packed=None) -> dict:
+    """``dada_uniques`` with the compare calls split over ``world`` ranks, this
+    one on ``device`` (dgpu_dada_sharded): every rank passes the same sample
+    and parameters and gets the same result, dada_uniques' own. ``gather``
+    all-gathers a uint8 block among the ranks (``multi.torch_gather`` for a
+    process group; all ranks' blocks concatenated in rank order)."""
+    params = params or DadaParams()
+    cat, offs, lens, ab, qcat, pr = packed if packed is not None else _pack(seqs, abund, quals, prior)
+    err = np.ascontiguousarray(err, np.float64)
+    pc = params.c()
+    h = C.c_void_p()
+    fn = _c_gather(gather, int(world))
+    check(lib().dgpu_dada_sharded(device, C.byref(pc), len(lens), ptr(cat), ptr(offs), ptr(lens), ptr(ab), ptr(pr),
+                                  ptr(qcat), ptr(err), int(ncol), int(rank), int(world), fn, None, C.byref(h)))
+    try:
+        return _read_result(h)
     finally:
         lib().dgpu_result_free(h)
 

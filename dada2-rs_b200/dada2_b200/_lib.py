@@ -70,6 +70,10 @@ class DadaOutC(C.Structure):
         "mem_hamming", "mem_lambda", "mem_pval", "map", "pvals", "counters", "times")]
 
 
+# dgpu_allgather_fn: (user, send, bytes, recv) -> 0 or nonzero
+ALLGATHER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p)
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -92,6 +96,8 @@ def lib():
                                 C.c_int, C.POINTER(_P)]
         L.dgpu_dada_batch.argtypes = [C.c_int, C.POINTER(DadaParamsC), C.c_int, _P, _P, _P, _P, _P, _P,
                                       _P, _P, C.c_int, _P]
+        L.dgpu_dada_sharded.argtypes = [C.c_int, C.POINTER(DadaParamsC), C.c_int, _P, _P, _P, _P, _P, _P, _P,
+                                        C.c_int, C.c_int, C.c_int, ALLGATHER_FN, _P, C.POINTER(_P)]
         L.dgpu_result_sizes.argtypes = [_P, _P]
         L.dgpu_result_fill.argtypes = [_P, C.POINTER(DadaOutC)]
         L.dgpu_result_transitions.argtypes = [_P, _P]

@@ -4,6 +4,10 @@ Samples are independent (the reference fans them out with no shared state,
 src/main.rs:4648-4697), so the data path has no collective: each rank denoises
 its own samples on its own GPU. The only cross-rank traffic is the timing and
 counter reduction after a timed region (max of seconds, sum of compares).
+
+One large sample can instead span the ranks (``dada_uniques_sharded``): each
+compare call is split by uniques and its stored comps are all-gathered
+(``torch_gather``), the one exchange step of that path.
 """
 from __future__ import annotations
 
@@ -29,6 +33,29 @@ def shard_samples(sizes, rank: int, world: int):
         owner[i] = r
         load[r] += sizes[i]
     return [i for i in range(len(sizes)) if owner[i] == rank]
+
+
+def torch_gather(group=None, device=None):
+    """The all-gather a sharded run (``dada_uniques_sharded``) exchanges its
+    compare results through: torch.distributed over ``group`` (NCCL with
+    ``device`` a CUDA device, gloo on the CPU). Give the process group a
+    timeout: a rank that has gone then ends the others' exchange with an
+    error instead of a wait."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+
+    def gather(block):
+        t = torch.from_numpy(np.ascontiguousarray(block, np.uint8))
+        if device is not None:
+            t = t.to(device)
+        parts = [torch.empty_like(t) for _ in range(world)]
+        dist.all_gather(parts, t, group=group)
+        return torch.cat(parts).cpu().numpy()
+
+    return gather
 
 
 def reduce_run(seconds: float, compares: int, device=None):

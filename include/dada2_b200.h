@@ -184,6 +184,32 @@ int dgpu_batch_prepare(int device, const dgpu_dada_params* params, int nsamples,
 int dgpu_batch_run(dgpu_batch* batch, dgpu_result** out);
 void dgpu_batch_free(dgpu_batch* batch);
 
+/* ---- one sample over several GPUs ---- */
+/* All-gather of fixed-size blocks among the ranks of a sharded run: every
+ * rank passes `bytes` bytes in send; recv (world * bytes) receives rank r's
+ * block at offset r * bytes. Returns 0, or nonzero when the exchange failed.
+ * The callback must end with an error, not block, when a peer has gone (for
+ * example through a process-group timeout). */
+typedef int (*dgpu_allgather_fn)(void* user, const void* send, uint64_t bytes, void* recv);
+/* dgpu_dada with the compare calls split over `world` ranks (one process or
+ * thread per GPU, `device` being the rank's own). Every rank passes the same
+ * inputs and parameters and runs the same clustering loop; a compare call
+ * screens and aligns only the rank's contiguous share of the uniques
+ * (balanced by bases) and the stored comps of all shares are all-gathered in
+ * rank order, the ascending raw order of the one-device store
+ * (src/cluster.rs:351-397). Two exchanges per compare call: a 56-byte head
+ * (status, counters, the center's own lambda) and, when any share stored
+ * comps, 24 bytes per comp of the largest share. Every rank's result equals
+ * dgpu_dada's on the same inputs. A failure on any rank after the argument
+ * checks fails every rank at the same exchange. Replaces, for one pooled
+ * sample spanning GPUs, the per-raw map of b_compare_parallel
+ * (src/cluster.rs:279-330), which the reference runs on one host's threads. */
+int dgpu_dada_sharded(int device, const dgpu_dada_params* params, int nraw, const char* seqs,
+                      const uint32_t* offs, const uint32_t* lens, const uint32_t* abund,
+                      const uint8_t* prior, const uint32_t* qual_sums, const double* err_mat,
+                      int ncol, int rank, int world, dgpu_allgather_fn gather, void* user,
+                      dgpu_result** out);
+
 /* Device memory reuse. No counterpart in the reference (its compare step holds
  * no device memory). A finished pool (dgpu_dada, dgpu_dada_batch,
  * dgpu_batch_free) keeps its device and pinned host blocks in a per-device

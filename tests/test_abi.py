@@ -61,6 +61,31 @@ def test_gpu_entry_points_fail_loudly_without_a_device():
         D.dada_uniques(["ACGTACGTAC"], [3], np.full(16, 0.01), 1)
 
 
+def test_sharded_run_keeps_its_ranks_in_step_without_a_device():
+    """dgpu_dada_sharded: argument errors return before any exchange; a rank
+    that cannot prepare (no device here) still takes part in the setup
+    exchange, once, reporting its error, so its peers stop there too."""
+    import numpy as np
+
+    import dada2_b200 as D
+
+    if D.device_count() > 0:
+        pytest.skip("a GPU is present; covered by the gpu tests")
+    calls = []
+
+    def gather(block):
+        calls.append(block.size)
+        return np.concatenate([block, block])
+
+    args = (["ACGTACGTAC"], [3], np.full(16, 0.01), 1)
+    with pytest.raises(D.InvalidInput, match="rank out of range"):
+        D.dada_uniques_sharded(*args, rank=2, world=2, gather=gather)
+    assert calls == []
+    with pytest.raises(D.DgpuError):
+        D.dada_uniques_sharded(*args, rank=0, world=2, gather=gather)
+    assert calls == [56]
+
+
 def test_service_lifecycle_without_a_device():
     """Without a GPU the service's worker fails every request with a CUDA
     error instead of hanging, and destroy returns."""

@@ -1,7 +1,11 @@
 """The product's clustering loop on the CPU: SampleState's absorb, shuffle,
 p-update (floors, zero set), bud and final pass, driven by the oracle's
 compare instead of the GPU kernels (tests/host_loop_driver.cpp), must give
-the oracle's own run_dada result bit for bit. Host only: no GPU."""
+the oracle's own run_dada result bit for bit. Host only: no GPU.
+
+The sharded cases run the loop as W ranks (threads) of dgpu_dada_sharded's
+exchange: each rank keeps only its own share's comps, and the product's
+shard_exchange must rebuild the one-device store on every rank."""
 import os
 import shutil
 import struct
@@ -35,7 +39,7 @@ def driver(tmp_path_factory):
     return out
 
 
-def _run(driver, tmp_path, s, err, ncol):
+def _run(driver, tmp_path, s, err, ncol, world=1):
     enc = [x.encode() for x in s.seqs]
     lens = np.array([len(x) for x in enc], np.uint32)
     q = np.concatenate([np.asarray(a, np.uint32) for a in s.quals])
@@ -47,7 +51,7 @@ def _run(driver, tmp_path, s, err, ncol):
         f.write(np.asarray(s.abund, np.uint32).tobytes())
         f.write(q.tobytes())
         f.write(np.ascontiguousarray(err, np.float64).tobytes())
-    out = subprocess.run([driver, str(path)], check=True, capture_output=True, text=True).stdout
+    out = subprocess.run([driver, str(path), str(world)], check=True, capture_output=True, text=True).stdout
     rows = {}
     for line in out.splitlines():
         k, *v = line.split()
@@ -59,8 +63,9 @@ def _f64(hexes):
     return np.array([int(h, 16) for h in hexes], np.uint64).view(np.float64)
 
 
-@pytest.mark.parametrize("case", ["small41", "small42", "config0", "pooled4"])
-def test_host_loop_matches_the_oracle(driver, tmp_path, case):
+@pytest.mark.parametrize("case,world", [("small41", 1), ("small42", 1), ("config0", 1), ("pooled4", 1),
+                                        ("small41", 2), ("config0", 3), ("pooled4", 4)])
+def test_host_loop_matches_the_oracle(driver, tmp_path, case, world):
     if case == "config0":
         w = synth.config0()
     elif case == "pooled4":
@@ -68,7 +73,7 @@ def test_host_loop_matches_the_oracle(driver, tmp_path, case):
     else:
         w = synth.small_illumina(int(case[-2:]), nvariants=7, nreads=4000, L=150)
     s = w.samples[0]
-    got = _run(driver, tmp_path, s, w.err, w.ncol)
+    got = _run(driver, tmp_path, s, w.err, w.ncol, world)
     want = O.dada(s.seqs, s.abund, w.err, w.ncol, O.DadaParams(nthreads=4), quals=s.quals)
     assert int(got["nclust"][0]) == want["nclust"]
     assert np.array_equal(np.array(got["map"], np.int64), want["map"].astype(np.int64))
@@ -87,3 +92,23 @@ def test_host_loop_matches_the_oracle(driver, tmp_path, case):
         assert np.float64(bp[ci]).tobytes() == np.float64(c["birth_pval"]).tobytes()
         assert np.float64(bf[ci]).tobytes() == np.float64(c["birth_fold"]).tobytes()
         assert np.float64(be[ci]).tobytes() == np.float64(c["birth_e"]).tobytes()
+
+
+@pytest.mark.parametrize("world,fail", [(2, "1:0"), (3, "0:5"), (3, "2:3")])
+def test_sharded_failure_stops_every_rank_at_the_same_exchange(driver, tmp_path, world, fail):
+    """A rank whose compare fails reports it in its exchange head; every rank
+    leaves the loop at that exchange with an error (none waits for good)."""
+    w = synth.small_illumina(41, nvariants=7, nreads=4000, L=150)
+    s = w.samples[0]
+    _run(driver, tmp_path, s, w.err, w.ncol, world)  # writes sample.bin
+    res = subprocess.run([driver, str(tmp_path / "sample.bin"), str(world), fail], capture_output=True, text=True,
+                         timeout=120)
+    assert res.returncode == 0, res.stdout + res.stderr
+    call = fail.split(":")[1]
+    lines = res.stdout.splitlines()
+    assert len(lines) == world
+    bad = int(fail.split(":")[0])
+    for r, line in enumerate(lines):
+        assert line.startswith(f"rank {r} rc 6 failed at call {call}:")
+        if r != bad:
+            assert f"rank {bad} of the sharded run failed" in line

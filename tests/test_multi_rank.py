@@ -77,3 +77,65 @@ def test_request_router_balances_outstanding_work():
     assert r.load == [100, 60, 250]
     assert r.release(0) == 0 and r.load == [0, 60, 250]
     assert r.assign(9, 5) == 0
+
+
+def _gather_worker(rank, world, port, out):
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, os.path.join(root, "dada2-rs_b200"))
+    import ctypes as C
+    import datetime
+
+    import numpy as np
+    import torch.distributed as dist
+
+    import dada2_b200
+    from dada2_b200 import multi
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    fn = dada2_b200._c_gather(multi.torch_gather(), world)
+    got = []
+    for nbytes in (56, 24 * 37, 56):  # a head, a comp block, a head: the sharded run's exchange sizes
+        send = (np.arange(nbytes, dtype=np.uint32) * (rank + 3) % 251).astype(np.uint8)
+        recv = np.zeros(world * nbytes, np.uint8)
+        rc = fn(None, C.c_void_p(send.ctypes.data), nbytes, C.c_void_p(recv.ctypes.data))
+        got.append((rc, recv.tobytes()))
+    # a gather that raises, or answers with the wrong size, reports nonzero
+    bad = dada2_b200._c_gather(lambda b: (_ for _ in ()).throw(RuntimeError("peer gone")), world)
+    short = dada2_b200._c_gather(lambda b: b, world)
+    one = np.zeros(8, np.uint8)
+    sink = np.zeros(8 * world, np.uint8)
+    rc_bad = bad(None, C.c_void_p(one.ctypes.data), 8, C.c_void_p(sink.ctypes.data))
+    rc_short = short(None, C.c_void_p(one.ctypes.data), 8, C.c_void_p(sink.ctypes.data))
+    out.put((rank, got, rc_bad, rc_short))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_sharded_exchange_gather():
+    """The all-gather a sharded run calls through its C callback
+    (dgpu_allgather_fn over torch.distributed): every rank receives every
+    rank's block in rank order, at the head and comp-block sizes."""
+    pytest.importorskip("torch")
+    import numpy as np
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gather_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for nb_i, nbytes in enumerate((56, 24 * 37, 56)):
+        want = b"".join((np.arange(nbytes, dtype=np.uint32) * (r + 3) % 251).astype(np.uint8).tobytes()
+                        for r in range(2))
+        for rank, got, _, _ in res:
+            assert got[nb_i] == (0, want)
+    for _, _, rc_bad, rc_short in res:
+        assert rc_bad != 0 and rc_short != 0
