@@ -106,8 +106,9 @@ struct ThreadGather {
 struct Input {
   int n = 0, ncol2 = 0;
   EncodedView in;
-  std::vector<uint8_t> seqb, qualb;
+  std::vector<uint8_t> seqb, qualb, prior;
   std::vector<double> errx;
+  DadaConf conf{};
 };
 
 static std::mutex oracle_mu;  // the oracle sessions are driven one call at a time
@@ -120,13 +121,12 @@ static int run_rank(const Input& I, int rank, int world, ThreadGather& G, std::s
   void* sess;
   {
     std::lock_guard<std::mutex> g(oracle_mu);
-    sess = orc_c_b_new(n, in.seq, in.off.data(), in.len.data(), in.qual, in.reads.data(), nullptr, 5, 1, 1e-40,
-                       1e-4, 1);
+    sess = orc_c_b_new(n, in.seq, in.off.data(), in.len.data(), in.qual, in.reads.data(), I.prior.data(), 5, 1,
+                       I.conf.omega_a, I.conf.omega_p, 1);
   }
-  DadaConf conf{1e-40, 1e-4, 1e-40, 1.0, 0.42, false, true, 1, 1, size_t(n)};
-  std::vector<uint8_t> lock(n, 0), prior(n, 0), pushed(n, 0);
+  std::vector<uint8_t> lock(n, 0), pushed(n, 0);
   SampleState S;
-  S.init(n, 0, in.reads.data(), prior.data(), lock.data(), &conf);
+  S.init(n, 0, in.reads.data(), I.prior.data(), lock.data(), &I.conf);
   const std::vector<uint32_t> bounds = shard_bounds(in.len.data(), uint32_t(n), world);
   const uint32_t lo = bounds[size_t(rank)], hi = bounds[size_t(rank) + 1];
   const ShardGather gather = [&](const void* s, uint64_t b, void* r) { return G.run(rank, s, b, r); };
@@ -148,8 +148,8 @@ static int run_rank(const Input& I, int rank, int world, ThreadGather& G, std::s
       orc_align_params p = ap;
       p.kdist_cutoff = ci == 0 ? 1.0 : 0.42;
       uint64_t cnt[9];
-      ns = orc_c_b_compare(sess, int(ci), I.errx.data(), I.ncol2, &p, 1, 2, ci_.data(), cl.data(), ch.data(),
-                           em.data(), &h.self, cnt);
+      ns = orc_c_b_compare(sess, int(ci), I.errx.data(), I.ncol2, &p, I.conf.greedy ? 1 : 0, 2, ci_.data(),
+                           cl.data(), ch.data(), em.data(), &h.self, cnt);
     }
     // this rank's share of the stored comps, as its device's store gives them
     local.clear();
@@ -192,7 +192,9 @@ static int run_rank(const Input& I, int rank, int world, ThreadGather& G, std::s
 }
 
 // input: n, total bytes, ncol (int32); lens u32[n]; bases char[total];
-// abund u32[n]; Phred sums u32[total]; err f64[16 * ncol]
+// abund u32[n]; Phred sums u32[total]; err f64[16 * ncol]; then, optional,
+// omega_a, omega_p, omega_c, min_fold (f64); detect_singletons, greedy,
+// min_hamming, min_abund, max_clust (int32; max_clust 0 = all); prior u8[n]
 int main(int argc, char** argv) {
   if (argc < 2) return 2;
   const int world = argc > 2 ? std::atoi(argv[2]) : 1;
@@ -210,6 +212,17 @@ int main(int argc, char** argv) {
       std::fread(ab.data(), 4, n, f) != size_t(n) || std::fread(qs.data(), 4, tot, f) != size_t(tot) ||
       std::fread(err.data(), 8, err.size(), f) != err.size())
     return 2;
+  Input I;
+  I.n = n;
+  I.conf = DadaConf{1e-40, 1e-4, 1e-40, 1.0, 0.42, false, true, 1, 1, size_t(n)};
+  I.prior.assign(size_t(n), 0);
+  double dp[4];
+  int32_t ip[5];
+  if (std::fread(dp, 8, 4, f) == 4) {
+    if (std::fread(ip, 4, 5, f) != 5 || std::fread(I.prior.data(), 1, size_t(n), f) != size_t(n)) return 2;
+    I.conf = DadaConf{dp[0], dp[1], dp[2], dp[3], 0.42, ip[0] != 0, ip[1] != 0, uint32_t(ip[2]), uint32_t(ip[3]),
+                      ip[4] > 0 ? size_t(ip[4]) : size_t(n)};
+  }
   std::fclose(f);
   std::vector<uint32_t> offs(n);
   uint32_t w = 0;
@@ -217,8 +230,6 @@ int main(int argc, char** argv) {
     offs[t] = w;
     w += lens[t];
   }
-  Input I;
-  I.n = n;
   I.seqb.resize(tot);
   I.qualb.resize(tot);
   I.in.seq = I.seqb.data();

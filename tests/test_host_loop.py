@@ -39,7 +39,7 @@ def driver(tmp_path_factory):
     return out
 
 
-def _run(driver, tmp_path, s, err, ncol, world=1):
+def _run(driver, tmp_path, s, err, ncol, world=1, params=None, prior=None):
     enc = [x.encode() for x in s.seqs]
     lens = np.array([len(x) for x in enc], np.uint32)
     q = np.concatenate([np.asarray(a, np.uint32) for a in s.quals])
@@ -51,6 +51,12 @@ def _run(driver, tmp_path, s, err, ncol, world=1):
         f.write(np.asarray(s.abund, np.uint32).tobytes())
         f.write(q.tobytes())
         f.write(np.ascontiguousarray(err, np.float64).tobytes())
+        if params is not None:
+            f.write(struct.pack("<dddd", params.omega_a, params.omega_p, params.omega_c, params.min_fold))
+            f.write(struct.pack("<iiiii", int(params.detect_singletons), int(params.greedy), params.min_hamming,
+                                params.min_abund, params.max_clust))
+            pr = np.zeros(len(enc), np.uint8) if prior is None else np.asarray(prior, np.uint8)
+            f.write(pr.tobytes())
     out = subprocess.run([driver, str(path), str(world)], check=True, capture_output=True, text=True).stdout
     rows = {}
     for line in out.splitlines():
@@ -112,3 +118,51 @@ def test_sharded_failure_stops_every_rank_at_the_same_exchange(driver, tmp_path,
         assert line.startswith(f"rank {r} rc 6 failed at call {call}:")
         if r != bad:
             assert f"rank {bad} of the sharded run failed" in line
+
+
+def _check(got, want):
+    assert int(got["nclust"][0]) == want["nclust"]
+    assert np.array_equal(np.array(got["map"], np.int64), want["map"].astype(np.int64))
+    assert _f64(got["pvals"]).tobytes() == want["pvals"].tobytes()
+    assert [int(x) for x in got["cl_reads"]] == [c["reads"] for c in want["clusters"]]
+    assert [int(x) for x in got["cl_birth_type"]] == [c["birth_type"] for c in want["clusters"]]
+    assert [int(x) for x in got["cl_birth_from"]] == [c["birth_from"] for c in want["clusters"]]
+    off = [int(x) for x in got["cl_mem_off"]]
+    raws = np.array(got["mem_raw"], np.int64)
+    lam, pv = _f64(got["mem_lambda"]), _f64(got["mem_pval"])
+    for ci, c in enumerate(want["clusters"]):
+        a, b = off[ci], off[ci + 1]
+        assert np.array_equal(raws[a:b], c["members"].astype(np.int64))
+        assert lam[a:b].tobytes() == c["lambdas"].tobytes()
+        assert pv[a:b].tobytes() == c["pvals"].tobytes()
+
+
+# parameter regimes of the host phases: singleton detection, priors (omega_p,
+# the prior bud), no greedy skip, fold and hamming filters, a cluster cap, an
+# abundance floor; each also as two sharded ranks
+# (on this sample the default run gives 9 clusters; these give 52, 10, 9 with
+# a Prior birth, 13 and 3)
+REGIMES = {
+    "singletons": dict(detect_singletons=True, omega_a=0.5),
+    "min_abund": dict(detect_singletons=True, omega_a=0.5, min_abund=2),
+    "priors": dict(omega_p=1e-2),
+    "nogreedy_fold_ham": dict(detect_singletons=True, omega_a=0.5, greedy=False, min_fold=4.0, min_hamming=3),
+    "max_clust": dict(max_clust=3),
+}
+
+
+@pytest.mark.parametrize("world", [1, 2])
+@pytest.mark.parametrize("regime", sorted(REGIMES))
+def test_host_loop_parameter_regimes_match_the_oracle(driver, tmp_path, regime, world):
+    w = synth.small_illumina(43, nvariants=9, nreads=5000, L=150)
+    s = w.samples[0]
+    params = O.DadaParams(nthreads=4, **REGIMES[regime])
+    prior = None
+    if regime == "priors":
+        rng = np.random.default_rng(7)
+        prior = np.zeros(len(s.seqs), np.uint8)
+        prior[rng.choice(len(s.seqs), size=min(25, len(s.seqs)), replace=False)] = 1
+    got = _run(driver, tmp_path, s, w.err, w.ncol, world, params=params, prior=prior)
+    want = O.dada(s.seqs, s.abund, w.err, w.ncol, params, quals=s.quals,
+                  prior=None if prior is None else prior.astype(bool))
+    _check(got, want)
