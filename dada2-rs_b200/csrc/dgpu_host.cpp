@@ -2995,7 +2995,10 @@ static int shard_heads(const ShardHead& mine, int world, const ShardGather& gath
 static int shard_exchange(SampleState& S, size_t ci, const ShardHead& mine, const std::vector<ShardComp>& local,
                           int world, const ShardGather& gather) {
   std::vector<ShardHead> heads;
-  TRY(shard_heads(mine, world, gather, heads));
+  ShardHead head = mine;
+  if (!head.err && local.size() != head.ns)  // reported in the head, so every rank stops here
+    head.err = fail(DGPU_E_INVALID, "shard comps do not match the head");
+  TRY(shard_heads(head, world, gather, heads));
   uint32_t maxns = 0;
   for (const ShardHead& h : heads) maxns = std::max(maxns, h.ns);
   std::vector<ShardComp> all(size_t(world) * maxns);
@@ -3076,7 +3079,10 @@ static int shard_run(Batch& B, int prep_rc, int rank, int world, const ShardGath
   for (int64_t ci = 0; ci >= 0;) {
     const auto tc = Clock::now();
     const int rc = shard_compare(P, s, size_t(ci), ci == 0 ? 1.0 : B.align.kdist_cutoff, lo, hi, h, local);
-    if (rc) h = ShardHead{rc, 0, 0, 0, 0.0, {}};
+    if (rc) {
+      h = ShardHead{rc, 0, 0, 0, 0.0, {}};
+      local.clear();
+    }
     TRY(shard_exchange(s, size_t(ci), h, local, world, gather));
     const auto th = Clock::now();
     s.stats.t_compare += secs(tc, th);
