@@ -155,7 +155,11 @@ static int run_rank(const Input& I, int rank, int world, ThreadGather& G, std::s
     local.clear();
     for (int k = 0; k < ns; ++k)
       if (ci_[k] >= lo && ci_[k] < hi)
-        local.push_back(ShardComp{ci_[k], ch[k], cl[k], std::numeric_limits<float>::quiet_NaN(), 0u});
+        local.push_back(ShardComp{ci_[k], ch[k], cl[k],
+                                  I.conf.fp32 ? (cl[k] > 0.0 ? float(std::log(cl[k]))
+                                                             : -std::numeric_limits<float>::infinity())
+                                              : std::numeric_limits<float>::quiet_NaN(),
+                                  0u});
     const uint32_t center = uint32_t(S.clusters[size_t(ci)].center);
     h.has_self = center >= lo && center < hi ? 1u : 0u;
     if (!h.has_self) h.self = 0.0;
@@ -187,6 +191,7 @@ static int run_rank(const Input& I, int rank, int world, ThreadGather& G, std::s
   hex_row(out, "cl_birth_pval", R->cl_birth_pval.data(), R->cl_birth_pval.size());
   hex_row(out, "cl_birth_fold", R->cl_birth_fold.data(), R->cl_birth_fold.size());
   hex_row(out, "cl_birth_e", R->cl_birth_e.data(), R->cl_birth_e.size());
+  out += "fp32 " + std::to_string(R->fp32[0]) + " " + std::to_string(R->fp32[1]) + "\n";
   delete R;
   return 0;
 }
@@ -194,7 +199,9 @@ static int run_rank(const Input& I, int rank, int world, ThreadGather& G, std::s
 // input: n, total bytes, ncol (int32); lens u32[n]; bases char[total];
 // abund u32[n]; Phred sums u32[total]; err f64[16 * ncol]; then, optional,
 // omega_a, omega_p, omega_c, min_fold (f64); detect_singletons, greedy,
-// min_hamming, min_abund, max_clust (int32; max_clust 0 = all); prior u8[n]
+// min_hamming, min_abund, max_clust (max_clust 0 = all), fp32 (int32);
+// prior u8[n]. With fp32 the comps carry float(ln lambda) as their FP32
+// log-sum, the stand-in for the kernel's compensated sum.
 int main(int argc, char** argv) {
   if (argc < 2) return 2;
   const int world = argc > 2 ? std::atoi(argv[2]) : 1;
@@ -217,11 +224,12 @@ int main(int argc, char** argv) {
   I.conf = DadaConf{1e-40, 1e-4, 1e-40, 1.0, 0.42, false, true, 1, 1, size_t(n)};
   I.prior.assign(size_t(n), 0);
   double dp[4];
-  int32_t ip[5];
+  int32_t ip[6];
   if (std::fread(dp, 8, 4, f) == 4) {
-    if (std::fread(ip, 4, 5, f) != 5 || std::fread(I.prior.data(), 1, size_t(n), f) != size_t(n)) return 2;
+    if (std::fread(ip, 4, 6, f) != 6 || std::fread(I.prior.data(), 1, size_t(n), f) != size_t(n)) return 2;
     I.conf = DadaConf{dp[0], dp[1], dp[2], dp[3], 0.42, ip[0] != 0, ip[1] != 0, uint32_t(ip[2]), uint32_t(ip[3]),
                       ip[4] > 0 ? size_t(ip[4]) : size_t(n)};
+    I.conf.fp32 = ip[5] != 0;
   }
   std::fclose(f);
   std::vector<uint32_t> offs(n);

@@ -39,7 +39,7 @@ def driver(tmp_path_factory):
     return out
 
 
-def _run(driver, tmp_path, s, err, ncol, world=1, params=None, prior=None):
+def _run(driver, tmp_path, s, err, ncol, world=1, params=None, prior=None, fp32=False):
     enc = [x.encode() for x in s.seqs]
     lens = np.array([len(x) for x in enc], np.uint32)
     q = np.concatenate([np.asarray(a, np.uint32) for a in s.quals])
@@ -53,8 +53,8 @@ def _run(driver, tmp_path, s, err, ncol, world=1, params=None, prior=None):
         f.write(np.ascontiguousarray(err, np.float64).tobytes())
         if params is not None:
             f.write(struct.pack("<dddd", params.omega_a, params.omega_p, params.omega_c, params.min_fold))
-            f.write(struct.pack("<iiiii", int(params.detect_singletons), int(params.greedy), params.min_hamming,
-                                params.min_abund, params.max_clust))
+            f.write(struct.pack("<iiiiii", int(params.detect_singletons), int(params.greedy), params.min_hamming,
+                                params.min_abund, params.max_clust, int(fp32)))
             pr = np.zeros(len(enc), np.uint8) if prior is None else np.asarray(prior, np.uint8)
             f.write(pr.tobytes())
     out = subprocess.run([driver, str(path), str(world)], check=True, capture_output=True, text=True).stdout
@@ -166,3 +166,24 @@ def test_host_loop_parameter_regimes_match_the_oracle(driver, tmp_path, regime, 
     want = O.dada(s.seqs, s.abund, w.err, w.ncol, params, quals=s.quals,
                   prior=None if prior is None else prior.astype(bool))
     _check(got, want)
+
+
+@pytest.mark.parametrize("world", [1, 2])
+@pytest.mark.parametrize("case", ["small41", "singletons"])
+def test_host_loop_fp32_decisions_keep_the_partition(driver, tmp_path, case, world):
+    """FP32-decision mode (exp of the FP32 ln lambda, FP64 within 1e3x of the
+    thresholds): the partition equals the oracle's FP64 run."""
+    w = synth.small_illumina(41 if case == "small41" else 43, nvariants=7 if case == "small41" else 9,
+                             nreads=4000 if case == "small41" else 5000, L=150)
+    s = w.samples[0]
+    params = O.DadaParams(nthreads=4, **({} if case == "small41" else REGIMES["singletons"]))
+    got = _run(driver, tmp_path, s, w.err, w.ncol, world, params=params, fp32=True)
+    want = O.dada(s.seqs, s.abund, w.err, w.ncol, params, quals=s.quals)
+    assert int(got["fp32"][0]) > 0
+    assert int(got["nclust"][0]) == want["nclust"]
+    assert np.array_equal(np.array(got["map"], np.int64), want["map"].astype(np.int64))
+    assert [int(x) for x in got["cl_reads"]] == [c["reads"] for c in want["clusters"]]
+    off = [int(x) for x in got["cl_mem_off"]]
+    raws = np.array(got["mem_raw"], np.int64)
+    for ci, c in enumerate(want["clusters"]):
+        assert np.array_equal(np.sort(raws[off[ci]:off[ci + 1]]), np.sort(c["members"].astype(np.int64)))
