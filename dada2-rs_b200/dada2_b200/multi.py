@@ -37,10 +37,11 @@ def shard_samples(sizes, rank: int, world: int):
 
 def torch_gather(group=None, device=None):
     """The all-gather a sharded run (``dada_uniques_sharded``) exchanges its
-    compare results through: torch.distributed over ``group`` (NCCL with
-    ``device`` a CUDA device, gloo on the CPU). Give the process group a
-    timeout: a rank that has gone then ends the others' exchange with an
-    error instead of a wait."""
+    compare results through: torch.distributed over ``group``. The records
+    are host memory, so a gloo group (``device`` None) needs no device copy;
+    with ``device`` a CUDA device they go through NCCL. Give the process
+    group a timeout: a rank that has gone then ends the others' exchange
+    with an error instead of a wait."""
     import numpy as np
     import torch
     import torch.distributed as dist
