@@ -20,6 +20,8 @@
  *   dgpu_dada            dada_uniques (plain: one sample)   src/dada.rs:225-592
  *   dgpu_dada_batch      many independent samples at once (the per-sample fan-out of
  *                        for_each_sample_concurrent)        src/main.rs:4648-4697
+ *   dgpu_dada_sharded    dada_uniques with each compare call split over ranks
+ *                        (the per-raw map of b_compare_parallel, src/cluster.rs:279-330)
  *   dgpu_align_debug     the aligners alone (test entry)    src/nwalign.rs:336-1140
  *
  * Threading: a context is used by one host thread at a time. Calls that take no
