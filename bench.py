@@ -18,12 +18,22 @@ Multi-GPU (torchrun): samples are independent, so each rank denoises its own
 40-sample batch (seeded by rank) with no collective on the data path
 (weak scaling); timing is the max over ranks.
 
---config 3 denoises the pooled 400,000-unique sample (see pooled_bench);
---config 4 replays the denoising-service request trace (see service_bench).
+  roofline : the kernel with the larger share of the timed step's device
+           spans -- k_align (integer issue: isolated launches, 7 ops per cell
+           of the reference's cell model) or k_screen (HBM: isolated launches,
+           algorithmic profile bytes); both are reported (roofline_dp,
+           roofline_screen)
+  decision_margin : the closest any threshold test came to its omega
+
+At N=1 the default run also reports configs 0 (plain 20-variant sample),
+2 (PacBio 16S), 3 (pooled 400,000 uniques) and 4 (denoising service) under
+other_configs, each with its oracle timing (--no-others skips them).
+--config 3 / --config 4 print only that config's report (pooled_report,
+service_report).
 
 --impl reference times the CPU restatement of the reference (oracle/,
-multithreaded like the reference's per-sample fan-out) on a bounded subset of
-the same workload.
+multithreaded like the reference's per-sample fan-out) on the same 40
+samples per step.
 """
 from __future__ import annotations
 
@@ -57,6 +67,8 @@ def parse():
     ap.add_argument("--config", type=int, default=1)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-others", action="store_true",
+                    help="skip the reports of configs 0, 2, 3 and 4 that the default config-1 run adds")
     ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
                     help="weak: every rank denoises its own 40-sample batch; strong: the 40 samples are sharded")
     return ap.parse_args()
@@ -253,6 +265,100 @@ def screen_roofline(w, params, device, calls=8):
             "compares_per_launch": st["timed_compares"] / max(st["timed_rounds"], 1)}
 
 
+def _encode_pool(samples, w):
+    """Codes, reads and rounded qualities of the samples' uniques as one
+    pool, and the error matrix extended by its last column past qmax
+    (src/dada.rs:337-384)."""
+    lut = np.zeros(256, np.uint8)
+    for ch, c in zip("ACGT", (1, 2, 3, 4)):
+        lut[ord(ch)] = c
+    codes, reads, quals, bases = [], [], [], []
+    for s in samples:
+        bases.append(len(codes))
+        ab = np.asarray(s.abund, np.uint32)
+        codes += [lut[np.frombuffer(x.encode(), np.uint8)] for x in s.seqs]
+        reads.append(ab)
+        quals += [np.floor(np.asarray(q, np.float64) / a + 0.5).astype(np.uint8) for q, a in zip(s.quals, ab)]
+    reads = np.concatenate(reads)
+    m = np.asarray(w.err, np.float64).reshape(16, w.ncol)
+    qmax = max(int(q.max()) for q in quals)
+    if qmax >= w.ncol:
+        m = np.concatenate([m, np.repeat(m[:, -1:], qmax + 1 - w.ncol, axis=1)], axis=1)
+    return codes, reads, quals, bases, m
+
+
+def finite_margins(m):
+    """Decision margins with +inf (no test of that kind ran) as None, so the
+    line stays valid JSON."""
+    return {k: (float(v) if np.isfinite(v) else None) for k, v in m.items()}
+
+
+def issue_peak_tops(sm_mhz):
+    """INT32 lane-op issue peak of the B200: 148 SMs x 4 SM sub-partitions x
+    32 lanes per clock, at the SM clock sampled during the run."""
+    return 148 * 4 * 32 * (sm_mhz or 1965.0) * 1e6 / 1e12
+
+
+def committed_dp_profile():
+    """ncu figures of one isolated k_align launch (issue activity, DRAM bytes)
+    from the committed profile summary, if any."""
+    path = os.path.join(ROOT, "profiles", "k_align_profile.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return None
+
+
+def dp_roofline(samples, w, params, device, calls=4, sm_mhz=None):
+    """k_align alone: every unique of the samples in one pool against the
+    centers of the first `calls` samples with the k-mer screen off (cutoff
+    1.0, like run_dada's first compare, src/dada.rs:835-838), one launch per
+    call on one stream with nothing else running. Cells are the reference's
+    cell model, (len1 + len2 + 1) x (band + 1) per NW pair (the aligner each
+    raw took is read back per call); 7 integer ops per cell (equality test,
+    select, three saturating adds, max with tie rule, strict diagonal test).
+    The launch also aligns the gapless pairs and forms every lambda; their
+    time is inside the figure."""
+    import dada2_b200 as D
+
+    codes, reads, quals, bases, m = _encode_pool(samples, w)
+    lens = np.array([len(c) for c in codes], np.int64)
+    centers = []
+    for s, b in zip(samples[:calls], bases):
+        ab = np.asarray(s.abund, np.uint32)
+        centers.append(b + int(np.flatnonzero(ab == ab.max())[-1]))
+    band = params.align.band
+    with D.CompareContext(params.align, m.ravel().copy(), m.shape[1], device=device) as ctx:
+        ctx.upload(codes, reads, quals=quals)
+        ctx.compare(centers[0], 1.0)  # warm-up
+        cells = pairs = gapless = 0
+        D.stats_reset()
+        D.stats_timing(1)
+        for c in centers:
+            ctx.compare(c, 1.0)
+            meth = ctx.methods()
+            nw = (meth >= 2) & (meth <= 4)
+            pairs += int(nw.sum())
+            gapless += int((meth == 1).sum())
+            cells += int(((lens[nw] + lens[c] + 1) * (band + 1)).sum())
+        D.stats_timing(False)
+        st = D.stats_read()
+    ms = st["ms"]["align"]
+    n = max(st["timed_rounds"], 1)
+    cups = cells / (ms / 1e3) if ms > 0 else None
+    peak = issue_peak_tops(sm_mhz)
+    ops = 7.0 * cups / 1e12 if cups else None
+    return {"bound": "int_issue", "kernel": "k_align", "achieved": ops, "peak": peak,
+            "unit": "Tops/s (INT32 lane ops, 7 per cell)", "frac": ops / peak if ops else None,
+            "gcups": cups / 1e9 if cups else None, "launches": int(st["timed_rounds"]),
+            "ms_per_launch": ms / n, "nw_pairs_per_launch": pairs / n, "gapless_pairs_per_launch": gapless / n,
+            "cells_per_launch": cells / n,
+            "peak_note": "148 SMs x 4 SMSPs x 32 lanes x the sampled SM clock; MEASURED_PEAKS.json has no integer "
+                         "figure",
+            "measured": f"{len(centers)} isolated launches, every unique of the workload against one center with "
+                        f"the screen off, one stream"}
+
+
 def fp32_partition(samples, w, params, device):
     """The samples denoised twice, with FP64 lambda (the drop-in) and with
     decisions from the FP32 compensated log-sum lambda (FP64 within 1e3x of
@@ -313,7 +419,7 @@ def reference_arm(args):
 
     O.build()
     w = load_workload(args.config, 0)
-    sub = cpu_subset(w.samples)
+    sub = w.samples  # the same samples the GPU arm denoises each step
     threads = os.cpu_count() or 1
     for _ in range(max(args.warmup, 0)):
         run_oracle(sub, w, threads)
@@ -328,9 +434,11 @@ def reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": w.name, "samples_per_step": len(sub), "note": "bounded subset of the 40 samples"},
+        "config": {"workload": w.name, "samples": len(sub), "uniques": int(sum(len(x.seqs) for x in sub)),
+                   "compares_per_step": comps // max(args.steps, 1),
+                   "note": "every sample of the workload each step, as the GPU arm"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"first {len(sub)} of {len(w.samples)} samples per step; C++ restatement of the "
+                         "sample": f"all {len(sub)} samples per step; C++ restatement of the "
                                    "reference (oracle/), round(threads/4) samples at a time"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -346,18 +454,15 @@ def _prefix_sample(s, n):
     return synth.Sample(s.seqs[:n], np.asarray(s.abund[:n]), s.quals[:n], 0, name=f"{s.name}[:{n}]")
 
 
-def pooled_bench(args):
+def pooled_report(local, steps, warmup, with_cpu=True):
     """Pooled mode: 200 samples pooled (first-seen order) into one sample of
     about 400,000 uniques from 3,000 variants x 150 nt, denoised by the
     single-sample path. value: inputs resident (ResidentBatch); e2e: dgpu_dada
     from host buffers. Also the FP32 ln(lambda) report on its first compare
-    call and the oracle on a bounded prefix. Rank 0 only."""
-    rank, world, local = dist_env()
-    if rank != 0:
-        return
+    call and the oracle on a bounded prefix."""
     from dada2_b200 import synth
 
-    w = synth.config3(seed=1003)  # generated in a spawn pool before any GPU call
+    w = synth.config3(seed=1003)  # generated in a spawn-started process pool
     import torch
 
     torch.cuda.set_device(local)
@@ -366,7 +471,7 @@ def pooled_bench(args):
     params = dada_params(w)
     s = w.samples[0]
     warm = _prefix_sample(s, 20000)
-    for _ in range(max(args.warmup, 1)):
+    for _ in range(max(warmup, 1)):
         D.dada_uniques(warm.seqs, warm.abund, w.err, w.ncol, params, quals=warm.quals, device=local,
                        read_result=False)
     pb = D.PackedBatch([s])
@@ -379,7 +484,7 @@ def pooled_bench(args):
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record()
         comps = 0
-        for _ in range(args.steps):
+        for _ in range(steps):
             res = rb.run(read_results=False)
             comps += res[0]["counters"]["cmp_scanned"]
         ev1.record()
@@ -393,7 +498,7 @@ def pooled_bench(args):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     e2e_comps = 0
-    for _ in range(args.steps):
+    for _ in range(steps):
         r = D.dada_uniques(None, None, w.err, w.ncol, params, packed=pk, device=local, read_result=False)
         e2e_comps += r["counters"]["cmp_scanned"]
     e1.record()
@@ -403,16 +508,19 @@ def pooled_bench(args):
     precision = precision_report(w, params, local)
     precision["partition"] = fp32_partition([s], w, params, local)
     cpu = None
-    if world == 1 and not args.no_cpu:
+    if with_cpu:
         sub = _prefix_sample(s, 30000)
         c, t, cores = run_oracle([sub], w, os.cpu_count() or 1)
         cpu = {"value": c / t, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"the first 30,000 pooled uniques as one sample ({c} compares), C++ restatement of the "
                          f"reference (oracle/)"}
     r0 = res[0]
+    screen_ms = st["ms"]["screen"]
+    screen_gbs = st["timed_screen_bytes"] / (screen_ms / 1e3) / 1e9 if screen_ms > 0 else None
+    peak, peak_kind = measured_peaks()
     line = {
-        "metric": POOLED_METRIC, "value": comps / dt, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * dt / max(args.steps, 1), "higher_is_better": True,
+        "metric": POOLED_METRIC, "value": comps / dt, "unit": UNIT, "n_gpus": 1, "steps": steps,
+        "warmup": warmup, "ms_per_step": 1e3 * dt / max(steps, 1), "higher_is_better": True,
         "scaling": "replicas only", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": w.name, "uniques": len(s.seqs), "clusters": int(r0["nclust"]),
                    "compares_per_step": int(r0["counters"]["cmp_scanned"]),
@@ -424,29 +532,30 @@ def pooled_bench(args):
         "latency_ms": {"p50": float(np.percentile(lat, 50)) if len(lat) else None,
                        "p99": float(np.percentile(lat, 99)) if len(lat) else None, "unit": "per compare call"},
         "host_phases_s_per_step": float(r0["times"][2]),
-        "kernel_ms_per_step": {k: v * (st["rounds"] / max(st["timed_rounds"], 1)) / max(args.steps, 1)
-                               for k, v in st["ms"].items()},
+        "roofline": {"bound": "hbm", "kernel": "k_screen", "achieved": screen_gbs, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": screen_gbs / peak if screen_gbs else None,
+                     "measured": "screen bytes of the sampled compare calls / their CUDA-event spans (one sample, "
+                                 "one launch at a time)",
+                     "bytes_per_call": st["timed_screen_bytes"] / max(st["timed_rounds"], 1)},
+        "decision_margin": finite_margins(r0["margins"]),
         "precision": precision,
         "gpu_launches": int(sum(st["launches"].values())),
         "clocks": clk,
         "cpu_baseline": cpu,
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 SERVICE_METRIC = "unique x center compares/s (denoising service, Poisson 20/s request trace)"
 
 
-def service_bench(args):
+def service_report(local, steps, warmup, with_cpu=True):
     """The denoising-service workload: a Poisson trace of 48 requests replayed
     in real time against DenoiseService (batched by length class, admitted by
     device-memory footprint) and against one-request-at-a-time dgpu_dada;
     then the same requests all at once (capacity). Latency is host wall time
     from submit to result; compares/s is all requests' compares over the
-    replay's span. Rank 0 only."""
-    rank, world, local = dist_env()
-    if rank != 0:
-        return
+    replay's span."""
     from dada2_b200 import synth
 
     w = synth.config4(seed=1004)  # generated in a spawn pool before any GPU call
@@ -458,7 +567,7 @@ def service_bench(args):
     params = D.DadaParams()
     packs = [D.pack_sample(s.seqs, s.abund, s.quals) for s in w.samples]
     arr = np.asarray(w.notes["arrivals"], np.float64)
-    for i in range(min(max(args.warmup, 1), len(packs))):
+    for i in range(min(max(warmup, 1), len(packs))):
         D.dada_uniques(None, None, w.err, w.ncol, params, packed=packs[i], read_result=False, device=local)
 
     def replay_service(svc, arrivals):
@@ -485,7 +594,7 @@ def service_bench(args):
             comps += r["counters"]["cmp_scanned"]
         return lats, comps, time.perf_counter() - t0
 
-    lens = np.tile(np.asarray(w.notes["lengths"]), max(args.steps, 1))
+    lens = np.tile(np.asarray(w.notes["lengths"]), max(steps, 1))
 
     def summary(lats, comps, span):
         lats = np.asarray(lats)
@@ -504,7 +613,7 @@ def service_bench(args):
     clocks.start()
     svc_l, svc_c, svc_t, batches = [], 0, 0.0, 0
     with D.DenoiseService(w.err, w.ncol, params, device=local) as svc:
-        for _ in range(args.steps):
+        for _ in range(steps):
             lats, c, t = replay_service(svc, arr)
             svc_l += lats
             svc_c += c
@@ -514,7 +623,7 @@ def service_bench(args):
         batches = svc.stats()["batches"]
     launches = int(sum(D.stats_read()["launches"].values()))
     pl_l, pl_c, pl_t = [], 0, 0.0
-    for _ in range(args.steps):
+    for _ in range(steps):
         lats, c, t = replay_plain(arr)
         pl_l += lats
         pl_c += c
@@ -523,7 +632,7 @@ def service_bench(args):
     clk = clocks.stop()
     svc_sum, plain_sum = summary(svc_l, svc_c, svc_t), summary(pl_l, pl_c, pl_t)
     cpu = None
-    if world == 1 and not args.no_cpu:
+    if with_cpu:
         sub = cpu_subset(w.samples, target=6_000_000)
         c, t, cores = run_oracle(sub, w, os.cpu_count() or 1)
         cpu = {"value": c / t, "unit": UNIT, "cores": cores, "kind": "port",
@@ -532,7 +641,7 @@ def service_bench(args):
     u = [len(s.seqs) for s in w.samples]
     line = {
         "metric": SERVICE_METRIC, "value": svc_sum["compares_per_s"], "unit": UNIT, "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * svc_t / max(args.steps, 1),
+        "steps": steps, "warmup": warmup, "ms_per_step": 1e3 * svc_t / max(steps, 1),
         "higher_is_better": True, "scaling": "replicas only", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": w.name, "requests": len(u), "uniques_median": int(np.median(u)),
@@ -553,7 +662,76 @@ def service_bench(args):
         "clocks": clk,
         "cpu_baseline": cpu,
     }
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def single_sample_report(config, local, steps, warmup, with_cpu=True, sm_mhz=None):
+    """One sample denoised by the plain single-sample path (config 0, the
+    20-variant Illumina sample, and config 2, the 5,000-unique PacBio 16S
+    sample): compares/s with the inputs resident and end to end, per-call
+    latency, the isolated k_align roofline, decision margins and the oracle
+    timed on the same sample."""
+    import torch
+
+    import dada2_b200 as D
+
+    w = load_workload(config, 0)
+    params = dada_params(w)
+    s = w.samples[0]
+    pb = D.PackedBatch([s])
+    with D.ResidentBatch([s], w.err, w.ncol, params, device=local, packed=pb) as rb:
+        for _ in range(max(warmup, 1)):
+            rb.run(read_results=False)
+        D.stats_reset()
+        D.stats_timing(TIMING_EVERY)
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        comps = 0
+        for _ in range(steps):
+            res = rb.run(read_results=False)
+            comps += res[0]["counters"]["cmp_scanned"]
+        ev1.record()
+        torch.cuda.synchronize()
+    dt = ev0.elapsed_time(ev1) / 1e3
+    D.stats_timing(False)
+    st = D.stats_read()
+    lat = D.stats_latencies()
+    pk = D.pack_sample(s.seqs, s.abund, s.quals)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    e2e_comps = 0
+    for _ in range(steps):
+        r = D.dada_uniques(None, None, w.err, w.ncol, params, packed=pk, device=local, read_result=False)
+        e2e_comps += r["counters"]["cmp_scanned"]
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_dt = e0.elapsed_time(e1) / 1e3
+    dp = dp_roofline([s], w, params, local, calls=1, sm_mhz=sm_mhz)
+    cpu = None
+    if with_cpu:
+        c, t, cores = run_oracle([s], w, os.cpu_count() or 1)
+        cpu = {"value": c / t, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"the whole sample ({c} compares), C++ restatement of the reference (oracle/)"}
+    r0 = res[0]
+    return {
+        "metric": f"unique x center compares/s (dada compare step, {w.name})", "value": comps / dt, "unit": UNIT,
+        "steps": steps, "ms_per_step": 1e3 * dt / max(steps, 1),
+        "config": {"workload": w.name, "uniques": len(s.seqs), "clusters": int(r0["nclust"]),
+                   "compares_per_step": int(r0["counters"]["cmp_scanned"]), "band": w.band,
+                   "homo_gap_p": w.homo_gap_p, "note": "one sample; a step is one full denoising"},
+        "e2e": {"value": e2e_comps / e2e_dt, "unit": UNIT, "h2d_bytes_per_step": int(pb.h2d_bytes),
+                "d2h_bytes_per_step": None},
+        "pairs_per_step": {k: int(r0["counters"][k]) for k in ("screened", "aligned", "nshroud", "gapless",
+                                                                "vectorized", "homo")},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)) if len(lat) else None,
+                       "p99": float(np.percentile(lat, 99)) if len(lat) else None, "unit": "per compare call"},
+        "roofline": dp,
+        "decision_margin": finite_margins(r0["margins"]),
+        "gpu_launches": int(sum(st["launches"].values())),
+        "cpu_baseline": cpu,
+    }
 
 
 def main():
@@ -561,11 +739,12 @@ def main():
     if args.impl == "reference":
         reference_arm(args)
         return
-    if args.config == 4:
-        service_bench(args)
-        return
-    if args.config == 3:
-        pooled_bench(args)
+    if args.config in (3, 4):
+        rank, world, local = dist_env()
+        if rank != 0:
+            return
+        fn = pooled_report if args.config == 3 else service_report
+        print(json.dumps(fn(local, args.steps, args.warmup, with_cpu=(world == 1 and not args.no_cpu))), flush=True)
         return
     rank, world, local = dist_env()
     import torch
@@ -697,10 +876,9 @@ def main():
     # ---- CPU baseline (rank 0, N=1 only, bounded) ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        sub = cpu_subset(w.samples)
-        c, t, cores = run_oracle(sub, w, os.cpu_count() or 1)
+        c, t, cores = run_oracle(w.samples, w, os.cpu_count() or 1)
         cpu = {"value": c / t, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"first {len(sub)} of {len(w.samples)} samples ({c} compares), C++ restatement of the "
+               "sample": f"all {len(w.samples)} samples once ({c} compares), C++ restatement of the "
                          f"reference (oracle/), round(threads/4) samples at a time"}
 
     if rank != 0:
@@ -708,17 +886,55 @@ def main():
             torch.distributed.destroy_process_group()
         return
     peak, peak_kind = measured_peaks()
-    # kernel times come from the sampled calls; per step they are scaled by
-    # all calls / timed calls
+    # kernel spans come from the sampled calls (every TIMING_EVERY-th); with
+    # six streams launching at once the spans overlap, so only their shares
+    # are reported, not their sum
     screen_ms = st["ms"]["screen"]
     scale = st["rounds"] / max(st["timed_rounds"], 1)
     step_rate = st["timed_screen_bytes"] / (screen_ms / 1e3) / 1e9 if screen_ms > 0 else None
+    span_tot = sum(st["ms"][k] for k in ("screen", "align", "store")) or 1.0
+    span_share = {k: st["ms"][k] / span_tot for k in ("screen", "align", "store")}
     iso = screen_roofline(w, params, local)
     achieved = iso["achieved_gbs"]
     tr = committed_traffic()
     traffic = None
     if tr:
         traffic = tr["dram_bytes_per_compare"] * iso["compares_per_launch"]
+    dp = dp_roofline(w.samples, w, params, local, sm_mhz=clk.get("sm_mhz"))
+    dprof = committed_dp_profile()
+    if dprof:
+        dp["traffic"] = dprof.get("dram_bytes_per_cell", 0.0) * dp["cells_per_launch"]
+        dp["ncu"] = dprof
+    else:
+        dp["traffic"] = None
+    roof_screen = {"bound": "hbm", "kernel": "k_screen", "achieved": achieved, "peak": peak,
+                   "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                   "traffic": traffic,
+                   "measured": f"{iso['launches']} isolated launches of {iso['compares_per_launch']:.0f} compares "
+                               f"(every unique of the workload against one center, "
+                               f"{iso['bytes_per_launch'] / 1e6:.0f} MB of profiles, more than L2), "
+                               f"{iso['ms_per_launch'] * 1e3:.1f} us each",
+                   "timed_step_gbs": step_rate,
+                   "timed_step_note": "bytes / summed CUDA-event spans of the sampled launches in the timed "
+                                      "step, where six streams run at once and the spans overlap",
+                   "algorithmic_bytes": "4^k profile bytes per non-skipped compare + 16 B metadata per compare"}
+    # the headline roofline is the kernel with the larger share of the
+    # timed step's sampled device spans
+    dominant = "align" if span_share["align"] >= span_share["screen"] else "screen"
+    margins = {k: float(min(r["margins"][k] for r in res)) for k in ("omega_a", "omega_p", "omega_c")}
+    others = None
+    if rank == 0 and world == 1 and not args.no_others:
+        others = {}
+        for cfg, fn in ((0, lambda: single_sample_report(0, local, 10, 3, not args.no_cpu, clk.get("sm_mhz"))),
+                        (2, lambda: single_sample_report(2, local, 5, 2, not args.no_cpu, clk.get("sm_mhz"))),
+                        (3, lambda: pooled_report(local, 2, 1, not args.no_cpu)),
+                        (4, lambda: service_report(local, 1, 1, not args.no_cpu))):
+            t0 = time.perf_counter()
+            try:
+                others[str(cfg)] = fn()
+            except Exception as exc:  # a failed side report must not lose the headline line
+                others[str(cfg)] = {"error": f"{type(exc).__name__}: {exc}"}
+            others[str(cfg)]["report_wall_s"] = time.perf_counter() - t0
     launches = int(sum(st["launches"].values()))
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -732,27 +948,20 @@ def main():
                 "h2d_note": "counted by the library: encoded u8 codes and qualities, 12 B per unique, the error "
                             "matrix, lock flags and each compare call's task tables",
                 "split_ms_per_step": e2e_split},
-        "roofline": {"bound": "hbm", "kernel": "k_screen", "achieved": achieved, "peak": peak,
-                     "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                     "traffic": traffic,
-                     "measured": f"{iso['launches']} isolated launches of {iso['compares_per_launch']:.0f} compares "
-                                 f"(every unique of the workload against one center, "
-                                 f"{iso['bytes_per_launch'] / 1e6:.0f} MB of profiles, more than L2), "
-                                 f"{iso['ms_per_launch'] * 1e3:.1f} us each",
-                     "timed_step_gbs": step_rate,
-                     "timed_step_note": "bytes / summed CUDA-event spans of the sampled launches in the timed "
-                                        "step, where six streams run at once and the spans overlap",
-                     "algorithmic_bytes": "4^k profile bytes per non-skipped compare + 16 B metadata per compare",
-                     "screen_ms_per_step": screen_ms * scale / args.steps,
-                     "timed_launches": st["timed_rounds"], "of_launches": st["rounds"]},
-        "kernel_ms_per_step": {k: v * scale / args.steps for k, v in st["ms"].items()},
+        "roofline": dp if dominant == "align" else roof_screen,
+        "roofline_dp": dp,
+        "roofline_screen": roof_screen,
+        "kernel_span_share": {**span_share, "note": "shares of the CUDA-event spans of the sampled compare calls "
+                                                    "in the timed step (spans overlap across six streams, so only "
+                                                    "the shares are meaningful)"},
         "batch_run_ms_per_step": {k: v / args.steps for k, v in st["batch_ms"].items()},
         "pairs_per_step": mix,
         "nw": {"cells_per_step": nw_cells,
-               "gcups": (nw_cells / (st["ms"]["align"] * scale / args.steps / 1e3) / 1e9)
-               if st["ms"]["align"] > 0 else None,
-               "note": "cells = (len1+len2+1) x (band+1) per NW pair; gcups over the align kernel's device time, "
-                       "which also covers the gapless pairs and lambda"},
+               "note": "cells = (len1+len2+1) x (band+1) per NW pair of the last timed step; the aligner's rate is "
+                       "roofline_dp's, from isolated launches"},
+        "decision_margin": {**finite_margins(margins), "note": "smallest |p - omega| / omega over every threshold test of the "
+                                               "40 samples: bud p*nraw vs omega_a, prior p vs omega_p, final map "
+                                               "p vs omega_c (+inf: no such test)"},
         "latency_ms": {"p50": float(np.percentile(lat, 50)) if len(lat) else None,
                        "p99": float(np.percentile(lat, 99)) if len(lat) else None,
                        "unit": "per batched compare call"},
@@ -771,6 +980,7 @@ def main():
         "clocks": clk,
         "plain": plain,
         "cpu_baseline": cpu,
+        "other_configs": others,
     }
     print(json.dumps(line), flush=True)
     if world > 1:

@@ -1,8 +1,11 @@
 // Plain-data structures shared by the CUDA kernels and the C++ host driver.
 #pragma once
 
+#include <chrono>
 #include <cstddef>
 #include <cstdint>
+#include <cstdlib>
+#include <thread>
 
 #include <cuda_runtime.h>
 
@@ -191,5 +194,37 @@ void launch_align_debug(int which, const uint8_t* s1cat, const uint32_t* off1, c
 
 // Records the message dgpu_last_error() returns on this thread.
 void set_last_error(const char* msg);
+
+// Host wait limit for a compare launch, in seconds: DGPU_WAIT_LIMIT_S, else
+// 300. No launch of this library runs anywhere near that long (the largest
+// workloads' launches take milliseconds), so reaching it means the device
+// stopped making progress.
+inline double wait_limit_s() {
+  static const double limit = [] {
+    const char* v = std::getenv("DGPU_WAIT_LIMIT_S");
+    const double x = v ? std::atof(v) : 0.0;
+    return x > 0.0 ? x : 300.0;
+  }();
+  return limit;
+}
+
+// Waits for queued device work by polling `query` (cudaStreamQuery on the
+// stream) and yielding the thread between polls, for at most limit_s
+// seconds. Returns cudaSuccess once the work is done, the first error other
+// than cudaErrorNotReady that query reports, or cudaErrorTimeout when the work
+// is still running at the limit; the work is then left queued, and the
+// caller reports the failure instead of blocking for good.
+template <class Query>
+cudaError_t poll_with_limit(Query query, double limit_s) {
+  const auto t0 = std::chrono::steady_clock::now();
+  for (uint64_t k = 0;; ++k) {
+    const cudaError_t q = query();
+    if (q != cudaErrorNotReady) return q;
+    if ((k & 63) == 63 &&
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > limit_s)
+      return cudaErrorTimeout;
+    std::this_thread::yield();
+  }
+}
 
 }  // namespace dgpu

@@ -686,12 +686,11 @@ int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
   // Poll and yield rather than block in the driver's spin: the launch slots'
   // threads share the cores with the host phases they wait for (on B200 with
   // 16 host cores the 40-sample step went from 79-82 ms to 75-78 ms).
-  for (;;) {
-    const cudaError_t q = cudaStreamQuery(st);
-    if (q == cudaSuccess) break;
-    if (q != cudaErrorNotReady) CUDA_TRY(q);
-    std::this_thread::yield();
-  }
+  const cudaError_t q = poll_with_limit([&] { return cudaStreamQuery(st); }, wait_limit_s());
+  if (q == cudaErrorTimeout)
+    return fail(DGPU_E_CUDA, "compare launch still running after the wait limit (DGPU_WAIT_LIMIT_S, default 300 s); "
+                             "the context must not be reused");
+  CUDA_TRY(q);
   const auto t1 = Clock::now();
   if (wait_s) *wait_s += secs(t0, t1);
   {
@@ -1362,6 +1361,17 @@ struct SampleState {
     return lb * (1.0 - 1e-9);
   }
 
+  // ---- decision margins ----
+  // The smallest relative distance |p - omega| / omega of any p-value that a
+  // threshold test of the loop compared: the bud's p * nraw against omega_a
+  // and the prior raw's p against omega_p (src/cluster.rs:1501-1640), and
+  // the final map's p against omega_c (src/dada.rs:525-533). A margin far
+  // above 1e-12 means that ulp-level differences in the p-values cannot
+  // change a decision. +inf when no test of that kind ran.
+  double margin[3] = {std::numeric_limits<double>::infinity(), std::numeric_limits<double>::infinity(),
+                      std::numeric_limits<double>::infinity()};
+  static double rel_margin(double pv, double omega) { return std::fabs(pv - omega) / omega; }
+
   // ---- FP32 lambda decisions (DadaConf::fp32) ----
   std::atomic<uint64_t> fp32_evals{0}, fp32_fallbacks{0};
   static bool near_threshold(double pv, double omega) { return pv >= omega * 1e-3 && pv <= omega * 1e3; }
@@ -1605,16 +1615,30 @@ struct SampleState {
     return calc_pA(rd, lambda * double(bi_reads), pr || conf->detect_singletons);
   }
 
-  // Regularised lower incomplete gamma, statrs 0.18.0's Poisson::sf kernel,
-  // following the published Cephes igam/igamc method (series when x <= 1 or
-  // x <= a, Legendre continued fraction otherwise).
-  // lnGamma of the integer read counts, filled once; the same lgamma_r call
+  // lnGamma as statrs 0.18.0's ln_gamma computes it (the function behind
+  // Poisson::sf): the Lanczos approximation with G. R. Pugh's parameters
+  // ("An Analysis of the Lanczos Gamma Approximation", 2004, p. 116),
+  // r = 10.900511 and eleven coefficients, for x >= 0.5:
+  //   ln(d_0 + sum_{k=1..10} d_k / ((x + k) - 1)) + ln(2 sqrt(e/pi))
+  //     + (x - 0.5) ln(((x - 0.5) + r) / e),
+  // summed left to right. Read counts are >= 1, so the x < 0.5 reflection
+  // is never needed. It differs from the C library's lgamma by ulps.
+  static double ln_gamma_lanczos(double x) {
+    static const double kD[11] = {
+        2.48574089138753565546e-5,  1.05142378581721974210,     -3.45687097222016235469,
+        4.51227709466894823700,     -2.98285225323576655721,    1.05639711577126713077,
+        -1.95428773191645869583e-1, 1.70970543404441224307e-2,  -5.71926117404305781283e-4,
+        4.63399473359905636708e-6,  -2.71994908488607703910e-9};
+    double s = kD[0];
+    for (int k = 1; k <= 10; ++k) s = s + kD[k] / (x + double(k) - 1.0);
+    return std::log(s) + 0.6207822376352452 + (x - 0.5) * std::log((x - 0.5 + 10.900511) / 2.718281828459045);
+  }
+  // lnGamma of the integer read counts, filled once with the same function
   // on the same argument, so every value is the one computed on demand.
   static const std::vector<double>& lgamma_table() {
     static const std::vector<double> table = [] {
       std::vector<double> t(size_t(1) << 16);
-      int sg = 0;
-      for (size_t k = 1; k < t.size(); ++k) t[k] = lgamma_r(double(k), &sg);
+      for (size_t k = 1; k < t.size(); ++k) t[k] = ln_gamma_lanczos(double(k));
       return t;
     }();
     return table;
@@ -1622,13 +1646,18 @@ struct SampleState {
   static double lgamma_of(double a) {
     const std::vector<double>& table = lgamma_table();
     if (a >= 1.0 && a < double(table.size()) && a == std::floor(a)) return table[size_t(a)];
-    int sg = 0;
-    return lgamma_r(a, &sg);
+    return ln_gamma_lanczos(a);
   }
 
+  // Regularised lower incomplete gamma, statrs 0.18.0's Poisson::sf kernel,
+  // following the published Cephes igam/igamc method (series when x <= 1 or
+  // x <= a, Legendre continued fraction otherwise). Like statrs it first
+  // answers 0.0 for x within 10 * 2^-53 of zero (its default accuracy).
   static double gamma_lr(double a, double x) {
     const double eps = 1e-15, big = 4503599627370496.0, big_inv = 2.22044604925031308085e-16;
     if (std::isnan(a) || std::isnan(x)) return std::numeric_limits<double>::quiet_NaN();
+    if (std::fabs(a) < 1.1102230246251565e-15) return 1.0;
+    if (std::fabs(x) < 1.1102230246251565e-15) return 0.0;
     const double ax = a * std::log(x) - x - lgamma_of(a);
     if (ax < -709.78271289338399) return a < x ? 1.0 : 0.0;
     if (x <= 1.0 || x <= a) {
@@ -1739,7 +1768,9 @@ struct SampleState {
       }
     }
     const double p_a = min_p * double(n);
+    if (have) margin[0] = std::min(margin[0], rel_margin(p_a, C.omega_a));
     if (p_a < C.omega_a && have) return bud_tail(mci, m.r, m.raw, p_a, 1);
+    if (havep) margin[1] = std::min(margin[1], rel_margin(min_pp, C.omega_p));
     if (min_pp < C.omega_p && havep) return bud_tail(mpci, mp.r, mp.raw, min_pp, 2);
     return -1;
   }
@@ -2353,6 +2384,7 @@ struct dgpu_result {
   uint64_t counters[16] = {0};
   double times[6] = {0};
   uint64_t fp32[2] = {0, 0};          // FP32-lambda p-values, FP64 fallbacks among them
+  double margin[3] = {0, 0, 0};       // decision margins against omega_a, omega_p, omega_c
   std::vector<uint32_t> transitions;  // 16 x tncol when requested
   int tncol = 0;
 };
@@ -2383,7 +2415,10 @@ static dgpu_result* finish(SampleState& S, const SampleSeqs& in) {
       mem_ci[raw] = uint32_t(ci);
       order.push_back(raw);
     }
+  std::mutex margin_mu;
+  double margin_c = std::numeric_limits<double>::infinity();
   auto price = [&](size_t lo, size_t hi) {
+    double mc = std::numeric_limits<double>::infinity();
     for (size_t k = lo; k < hi; ++k) {
       const uint32_t raw = order[k];
       const Cluster& c = S.clusters[mem_ci[raw]];
@@ -2402,11 +2437,14 @@ static dgpu_result* finish(SampleState& S, const SampleSeqs& in) {
           }
         }
         ok = pv >= S.conf->omega_c;
+        mc = std::min(mc, SampleState::rel_margin(pv, S.conf->omega_c));
       }
       S.p[raw] = pv;
       correct[raw] = ok;
       R->pvals[raw] = pv;
     }
+    std::lock_guard<std::mutex> lk(margin_mu);
+    margin_c = std::min(margin_c, mc);
   };
   if (order.size() < kParMin)
     price(0, order.size());
@@ -2454,6 +2492,9 @@ static dgpu_result* finish(SampleState& S, const SampleSeqs& in) {
   R->times[5] = st.t_job_wait;
   R->fp32[0] = S.fp32_evals.load();
   R->fp32[1] = S.fp32_fallbacks.load();
+  R->margin[0] = S.margin[0];
+  R->margin[1] = S.margin[1];
+  R->margin[2] = margin_c;
   return R;
 }
 
@@ -3266,6 +3307,15 @@ int dgpu_compare(dgpu_ctx* ctx, int center, double kdist_cutoff, int greedy, dou
   return 0;
 }
 
+int dgpu_get_methods(dgpu_ctx* ctx, uint8_t* out) {
+  if (!ctx || !out) return fail(DGPU_E_INVALID, "null argument");
+  Pool& P = ctx->pool;
+  const uint32_t n = P.nraw;
+  CUDA_TRY(cudaMemcpy(out, P.status.p, n, cudaMemcpyDeviceToHost));
+  for (uint32_t t = 0; t < n; ++t) out[t] = uint8_t(out[t] >> 2);
+  return 0;
+}
+
 int dgpu_compare_store(dgpu_ctx* ctx, int center, int cluster_i, double kdist_cutoff, int greedy,
                        uint32_t* comp_index, double* comp_lambda, uint32_t* comp_hamming, int* nstored,
                        double* self_out, dgpu_counters* cnt) {
@@ -3407,6 +3457,12 @@ int dgpu_result_fp32_stats(const dgpu_result* r, uint64_t* out2) {
   if (!r || !out2) return fail(DGPU_E_INVALID, "null argument");
   out2[0] = r->fp32[0];
   out2[1] = r->fp32[1];
+  return 0;
+}
+
+int dgpu_result_margins(const dgpu_result* r, double* out3) {
+  if (!r || !out3) return fail(DGPU_E_INVALID, "null argument");
+  std::copy(r->margin, r->margin + 3, out3);
   return 0;
 }
 

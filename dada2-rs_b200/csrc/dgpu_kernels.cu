@@ -2344,12 +2344,14 @@ void launch_align_debug(int which, const uint8_t* s1cat, const uint32_t* off1, c
 // ---------------------------------------------------------------------------
 // Allocation-free alignment entry point (dgpu_align_pairs_noalloc).
 //
-// For callers that must not allocate device memory -- code running inside
-// CUDA stream capture, or hosts whose device memory is owned by another
-// allocator -- the pointer-matrix scratch the aligners need lives in this
-// file-scope array instead of a cudaMalloc'd buffer. Every GPU that loads the
-// library holds it until the process exits. Calls share it: two calls whose
-// kernels overlap on one device race on it.
+// For callers that must not allocate device memory -- a host whose device
+// memory is already reserved by its own pool allocator (where cudaMalloc
+// fails or fragments that pool), or a latency-bound pipeline that cannot
+// afford cudaFree's implicit device-wide synchronisation -- the
+// pointer-matrix scratch the aligners need lives in this file-scope array
+// instead of a cudaMalloc'd buffer. Every GPU that loads the library holds it
+// until the process exits. Calls share it: two calls whose kernels overlap on
+// one device race on it.
 // ---------------------------------------------------------------------------
 constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;  // 16 MiB per device
 constexpr size_t kNoAllocHeader = 256;                     // error word, cleared per call
@@ -2372,6 +2374,12 @@ __global__ void __launch_bounds__(kNwWarps * 32) k_align_noalloc(int which, cons
   const int kb = rm_kbound(geom.rm_pairs);
   for (uint32_t pair = gw; pair < npairs; pair += nw) {
     uint32_t ham = 0;
+    // the shared-memory carve and the scratch slot are sized for geom.lmax:
+    // a longer pair is refused before anything is staged
+    if (len1[pair] > uint32_t(geom.lmax) || len2[pair] > uint32_t(geom.lmax)) {
+      if (lane == 0) atomicOr(err_word, DERR_GEOMETRY);
+      continue;
+    }
     const uint8_t* a = s1cat + off1[pair];
     const uint8_t* b = s2cat + off2[pair];
     uint8_t* o0 = al0 + aloff[pair];
@@ -2404,7 +2412,9 @@ __global__ void __launch_bounds__(kNwWarps * 32) k_align_noalloc(int which, cons
 
 // Device address of g_noalloc_scratch, resolved once per device with that
 // device current (cudaGetSymbolAddress); host code must never hand the
-// symbol itself to a kernel.
+// symbol itself to a kernel. The cached address belongs to the device's
+// primary context: after cudaDeviceReset the module may load elsewhere, so
+// this entry point must not be used again in that process.
 static std::mutex g_noalloc_mu;
 static uint8_t* g_noalloc_ptr[64] = {nullptr};
 
@@ -2474,10 +2484,20 @@ extern "C" int dgpu_align_pairs_noalloc(int which, int npairs, int max_len, cons
   g.nwarps = int32_t(warps);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   uint32_t* err_word = reinterpret_cast<uint32_t*>(base);
+  const size_t smem = (which == 0 ? nw_smem_per_warp_vec(g) : nw_smem_per_warp_rm(g)) * kNwWarps;
+  int smem_optin = 0;
+  e = cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  if (e != cudaSuccess) return bad(DGPU_E_CUDA, cudaGetErrorString(e));
+  if (smem > size_t(smem_optin))
+    return bad(DGPU_E_INVALID, "max_len too long: four alignments' shared-memory staging exceeds the device's "
+                               "per-block limit");
+  if (smem > 48 * 1024) {
+    e = cudaFuncSetAttribute(k_align_noalloc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return bad(DGPU_E_CUDA, cudaGetErrorString(e));
+  }
   e = cudaMemsetAsync(err_word, 0, 4, st);
   if (e != cudaSuccess) return bad(DGPU_E_CUDA, cudaGetErrorString(e));
-  const size_t smem = (which == 0 ? nw_smem_per_warp_vec(g) : nw_smem_per_warp_rm(g)) * kNwWarps;
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_align_noalloc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  (void)cudaGetLastError();  // so the check after the launch sees only this launch's error
   k_align_noalloc<<<uint32_t(warps / kNwWarps), kNwWarps * 32, smem, st>>>(which, s1cat, off1, len1, s2cat, off2, len2,
                                                                 uint32_t(npairs), kp, end_gap, g, base + kNoAllocHeader,
                                                                 slot, al0, al1, al_off, al_len, err_word);
@@ -2487,6 +2507,8 @@ extern "C" int dgpu_align_pairs_noalloc(int which, int npairs, int max_len, cons
   e = cudaMemcpyAsync(&flag, err_word, 4, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return bad(DGPU_E_CUDA, cudaGetErrorString(e));
+  if (flag & DERR_GEOMETRY)
+    return bad(DGPU_E_DEVICE, "a pair exceeded the bounds sized for max_len and was refused (its outputs are left unwritten)");
   if (flag) return bad(flag & DERR_UNSUPPORTED ? DGPU_E_UNSUPPORTED : DGPU_E_DEVICE, "device error flag set");
   return 0;
 }

@@ -149,6 +149,12 @@ class CompareContext:
         return {"index": idx[:k].copy(), "lambda": lam[:k].copy(), "hamming": ham[:k].copy(),
                 "self": self_.value, "counters": _counters(cnt)}
 
+    def methods(self) -> np.ndarray:
+        """The aligner each raw took in the latest compare (codes of METHOD_NAMES)."""
+        out = np.zeros(self.n, np.uint8)
+        check(lib().dgpu_get_methods(self.h, ptr(out)))
+        return out
+
     def set_lambda32(self, enable: bool = True):
         """Also form ln(lambda) in compensated FP32 on later compares (precision report)."""
         check(lib().dgpu_ctx_set_lambda32(self.h, int(bool(enable))))
@@ -215,6 +221,9 @@ def _read_result(h) -> dict:
     f32 = np.zeros(2, np.uint64)
     check(lib().dgpu_result_fp32_stats(h, ptr(f32)))
     res["fp32"] = {"pvalues": int(f32[0]), "fallbacks": int(f32[1])}
+    mg = np.zeros(3, np.float64)
+    check(lib().dgpu_result_margins(h, ptr(mg)))
+    res["margins"] = {"omega_a": float(mg[0]), "omega_p": float(mg[1]), "omega_c": float(mg[2])}
     tncol = lib().dgpu_result_transitions(h, None)
     if tncol > 0:
         tr = np.zeros(16 * tncol, np.uint32)
@@ -426,8 +435,11 @@ def _read_counters(h) -> dict:
     check(lib().dgpu_result_fill(h, C.byref(o)))
     sizes = np.zeros(4, np.int64)
     check(lib().dgpu_result_sizes(h, ptr(sizes)))
+    mg = np.zeros(3, np.float64)
+    check(lib().dgpu_result_margins(h, ptr(mg)))
     return {"nclust": int(sizes[0]), "nraw": int(sizes[1]),
-            "counters": {k: int(v) for k, v in zip(COUNTER_KEYS, cnt)}, "times": tm}
+            "counters": {k: int(v) for k, v in zip(COUNTER_KEYS, cnt)}, "times": tm,
+            "margins": {"omega_a": float(mg[0]), "omega_p": float(mg[1]), "omega_c": float(mg[2])}}
 
 
 class DenoiseService:

@@ -102,6 +102,8 @@ def lib():
         L.dgpu_result_fill.argtypes = [_P, C.POINTER(DadaOutC)]
         L.dgpu_result_transitions.argtypes = [_P, _P]
         L.dgpu_result_fp32_stats.argtypes = [_P, _P]
+        L.dgpu_result_margins.argtypes = [_P, _P]
+        L.dgpu_get_methods.argtypes = [_P, _P]
         L.dgpu_service_create.argtypes = [C.c_int, C.POINTER(DadaParamsC), _P, C.c_int, C.c_uint64, _P]
         L.dgpu_service_submit.argtypes = [_P, C.c_int, _P, _P, _P, _P, _P, _P, _P]
         L.dgpu_service_wait.argtypes = [_P, C.c_uint64, _P, _P]

@@ -156,6 +156,10 @@ int dgpu_get_e_minmax(dgpu_ctx* ctx, double* out);
 /* The map: per raw lambda, hamming (UINT32_MAX = shrouded or skipped), skipped flag. */
 int dgpu_compare(dgpu_ctx* ctx, int center, double kdist_cutoff, int greedy, double* lambda_out,
                  uint32_t* hamming_out, uint8_t* skipped_out, dgpu_counters* cnt);
+/* The aligner each raw took in the context's latest compare (raw_align_dp's
+ * method choice, src/nwalign.rs:1315-1414): 0 none (skipped or shrouded),
+ * 1 gapless, 2 vectorized, 3 homopolymer, 4 ends-free; nraw bytes. */
+int dgpu_get_methods(dgpu_ctx* ctx, uint8_t* out);
 /* Map + store: comps with lambda*total_reads > e_minmax, ascending raw index,
  * e_minmax updated on the device; self_out = the center's own lambda. */
 int dgpu_compare_store(dgpu_ctx* ctx, int center, int cluster_i, double kdist_cutoff, int greedy,
@@ -272,6 +276,14 @@ double dgpu_calc_pA(uint32_t reads, double e_reads, int prior);
 /* With lambda_fp32: [0] p-values priced from the FP32 lambda, [1] of those
  * repriced from the FP64 product (the fallback). Zero otherwise. */
 int dgpu_result_fp32_stats(const dgpu_result* res, uint64_t* out2);
+/* Decision margins of the run: out3[0] the smallest |p - omega_a| / omega_a
+ * over the bud's tests of p * nraw against omega_a, out3[1] the same for the
+ * prior raw's p against omega_p (both src/cluster.rs:1501-1640), out3[2] for
+ * the final map's p against omega_c (src/dada.rs:525-533); +inf where no
+ * such test ran. A margin far above 1e-12 shows that p-values differing by a
+ * few ulps could not have changed any decision. No counterpart in the
+ * reference (a diagnostic of this implementation). */
+int dgpu_result_margins(const dgpu_result* res, double* out3);
 
 /* ---- ingest: FASTQ -> uniques ----
  * Dereplicates a FASTQ file (plain or gzip, four-line records) as
@@ -316,17 +328,24 @@ int dgpu_align_debug(int device, int which, int npairs, const uint8_t* s1cat, co
 
 /* ---- aligners without device allocation ----
  * No counterpart in the reference. Same alignments as dgpu_align_debug, for
- * callers that cannot allocate device memory (code running under CUDA stream
- * capture, or hosts whose device memory belongs to another allocator): all
- * pointers are caller-owned and must be readable/writable by the current
- * device (device or managed memory), and the aligners' scratch is a 16 MiB
- * static device array that every GPU loading this library holds until exit.
- * max_len bounds every sequence length (at most 3500 for which = 0); lengths
- * whose scratch for four concurrent alignments exceeds the array are rejected
- * with DGPU_E_INVALID. The first call on a device looks up the array's address
- * (cudaGetSymbolAddress), so make it before any stream capture. Calls share
- * the array: calls whose kernels overlap on one device race. Runs on `stream`
- * (a cudaStream_t; NULL = legacy default stream) and returns after it finishes. */
+ * callers that cannot allocate device memory: a host whose device memory is
+ * already reserved by its own pool allocator (cudaMalloc would fail or
+ * fragment that pool), or a latency-bound pipeline that cannot afford the
+ * device-wide synchronisation cudaFree implies. All pointers are
+ * caller-owned and must be readable/writable by the current device (device
+ * or managed memory); nothing is allocated. The aligners' scratch is a
+ * 16 MiB static device array that every GPU loading this library holds until
+ * exit. max_len bounds every sequence length (at most 3500 for which = 0);
+ * lengths whose scratch for four concurrent alignments exceeds the array, or
+ * whose shared-memory staging exceeds the device's per-block limit, are
+ * rejected with DGPU_E_INVALID. A pair longer than max_len is refused on the
+ * device: its outputs stay unwritten and the call returns DGPU_E_DEVICE (the
+ * other pairs are aligned). The first call on a device looks up the array's
+ * address (cudaGetSymbolAddress) and keeps it, so make that first call before
+ * any stream capture, and do not use this entry point after cudaDeviceReset.
+ * Every call shares the array: calls whose kernels overlap on one device race.
+ * Runs on `stream` (a cudaStream_t; NULL = legacy default stream) and returns
+ * after it finishes. */
 int dgpu_align_pairs_noalloc(int which, int npairs, int max_len, const uint8_t* s1cat,
                              const uint32_t* off1, const uint32_t* len1, const uint8_t* s2cat,
                              const uint32_t* off2, const uint32_t* len2,

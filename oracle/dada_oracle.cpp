@@ -782,20 +782,49 @@ double compute_lambda(const Raw& raw, const Sub* sub, const double* err_mat, siz
   return lambda;
 }
 
+// lnGamma as statrs 0.18.0 documents its `ln_gamma`: the Lanczos
+// approximation with the parameters of G. R. Pugh, "An Analysis of the Lanczos
+// Gamma Approximation" (PhD thesis, UBC 2004, p. 116): r = 10.900511 and the
+// eleven coefficients d_0..d_10 below, evaluated for x >= 0.5 as
+//   ln(d_0 + sum_{k=1..10} d_k / (x + k - 1)) + ln(2 sqrt(e / pi))
+//     + (x - 0.5) ln((x - 0.5 + r) / e),
+// the sum accumulated left to right from d_0, each term's divisor formed as
+// (x + k) - 1, and e the double nearest Euler's number. Calc_pA only needs
+// a >= 1 (a = reads), so the reflection branch for x < 0.5 is not restated.
+// Not the C library's lgamma: the two differ by a few ulps (ln_gamma(1) is
+// -4.4e-16 here, not 0), which moves p-values by ulps.
+double ln_gamma_lanczos(double x) {
+  static const double kR = 10.900511;
+  static const double kD[11] = {
+      2.48574089138753565546e-5,  1.05142378581721974210,     -3.45687097222016235469,
+      4.51227709466894823700,     -2.98285225323576655721,    1.05639711577126713077,
+      -1.95428773191645869583e-1, 1.70970543404441224307e-2,  -5.71926117404305781283e-4,
+      4.63399473359905636708e-6,  -2.71994908488607703910e-9};
+  static const double kLn2SqrtEOverPi = 0.6207822376352452;  // ln(2 sqrt(e / pi))
+  static const double kE = 2.718281828459045;
+  double s = kD[0];
+  for (int k = 1; k <= 10; ++k) s = s + kD[k] / (x + double(k) - 1.0);
+  return std::log(s) + kLn2SqrtEOverPi + (x - 0.5) * std::log((x - 0.5 + kR) / kE);
+}
+
 // Regularised lower incomplete gamma P(a, x). statrs 0.18.0's
 // `Poisson::sf(k) = gamma_lr(k + 1, lambda)` (the call site is src/pval.rs:219-223)
 // follows the published Cephes igam/igamc method (S. Moshier): a power series
 // when x <= 1 or x <= a, otherwise 1 - (Legendre continued fraction for the
 // upper tail), with the exponent prefactor a*ln(x) - x - lnGamma(a) tested for
-// underflow first. This is a restatement of that method, with lnGamma taken
-// from the C library; bit-level agreement with statrs is not pinned (no
-// reference test fixes calc_pA values).
+// underflow first, lnGamma being ln_gamma_lanczos above. Before that, statrs
+// answers 0.0 for an x within its default accuracy (10 * 2^-53) of zero. No
+// reference test fixes calc_pA values, so bit-level agreement with statrs
+// rests on this restatement of its documented method.
 double gamma_lr(double a, double x) {
   const double eps = 1e-15;
   const double big = 4503599627370496.0;            // 2^52
   const double big_inv = 2.22044604925031308085e-16;  // 2^-52
+  const double zero_acc = 1.1102230246251565e-15;     // 10 * 2^-53
   if (std::isnan(a) || std::isnan(x)) return std::numeric_limits<double>::quiet_NaN();
-  double ax = a * std::log(x) - x - std::lgamma(a);
+  if (std::fabs(a) < zero_acc) return 1.0;
+  if (std::fabs(x) < zero_acc) return 0.0;
+  double ax = a * std::log(x) - x - ln_gamma_lanczos(a);
   if (ax < -709.78271289338399) return a < x ? 1.0 : 0.0;
   if (x <= 1.0 || x <= a) {
     double r = a, c = 1.0, ans = 1.0;

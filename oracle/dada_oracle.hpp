@@ -179,6 +179,7 @@ double compute_lambda(const Raw& raw, const Sub* sub, const double* err_mat, siz
                       bool use_quals);
 double calc_pA(uint32_t reads, double e_reads, bool prior);
 double gamma_lr(double a, double x);
+double ln_gamma_lanczos(double x);
 double get_pA(uint32_t reads, bool prior, double lambda, uint32_t hamming, uint32_t bi_reads,
               bool detect_singletons);
 uint64_t b_p_update(B& b, bool greedy, bool detect_singletons, double min_fold,

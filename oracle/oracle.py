@@ -105,6 +105,8 @@ def lib():
         _lib.orc_c_calc_pA.argtypes = [C.c_uint32, d, C.c_int]
         _lib.orc_c_gamma_lr.restype = d
         _lib.orc_c_gamma_lr.argtypes = [d, d]
+        _lib.orc_c_ln_gamma.restype = d
+        _lib.orc_c_ln_gamma.argtypes = [d]
         _lib.orc_c_get_pA.restype = d
         _lib.orc_c_get_pA.argtypes = [C.c_uint32, C.c_int, d, C.c_uint32, C.c_uint32, C.c_int]
         _lib.orc_c_assign_kmer8_sparse.restype = C.c_size_t
@@ -278,6 +280,11 @@ def calc_pA(reads: int, e_reads: float, prior: bool) -> float:
 
 def gamma_lr(a: float, x: float) -> float:
     return lib().orc_c_gamma_lr(a, x)
+
+
+def ln_gamma(x: float) -> float:
+    """lnGamma as statrs 0.18.0 computes it (Lanczos, Pugh's r = 10.900511)."""
+    return lib().orc_c_ln_gamma(x)
 
 
 def get_pA(reads, prior, lam, hamming, bi_reads, detect_singletons=False) -> float:

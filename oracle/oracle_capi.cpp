@@ -197,6 +197,7 @@ int orc_c_al2subs(const uint8_t* al0, const uint8_t* al1, int alen, uint32_t* le
 
 double orc_c_calc_pA(uint32_t reads, double e_reads, int prior) { return calc_pA(reads, e_reads, prior != 0); }
 double orc_c_gamma_lr(double a, double x) { return gamma_lr(a, x); }
+double orc_c_ln_gamma(double x) { return ln_gamma_lanczos(x); }
 double orc_c_get_pA(uint32_t reads, int prior, double lambda, uint32_t hamming, uint32_t bi_reads,
                     int detect_singletons) {
   return get_pA(reads, prior != 0, lambda, hamming, bi_reads, detect_singletons != 0);

@@ -6,7 +6,10 @@ expected values out of the `#[cfg(test)]` modules and writes them, each with
 the file:line it came from, to ``reference_vectors.json`` beside this file.
 The parity tests load that JSON; nothing reads the reference tree at test time.
 
-Usage: python tests/golden/extract_reference_vectors.py [REFERENCE_ROOT]
+Usage: python tests/golden/extract_reference_vectors.py REFERENCE_ROOT
+
+REFERENCE_ROOT is the top of a dada2-rs 0.2.0 source tree (the directory
+holding src/nwalign.rs).
 """
 from __future__ import annotations
 
@@ -208,7 +211,9 @@ def extract(root: str) -> dict:
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: extract_reference_vectors.py REFERENCE_ROOT")
+    root = sys.argv[1]
     data = extract(root)
     path = os.path.join(HERE, "reference_vectors.json")
     with open(path, "w", encoding="utf-8") as f:

@@ -121,7 +121,7 @@ def test_library_calc_pA_matches_the_oracle_bit_for_bit():
     from oracle import oracle as O
 
     for k in (1, 2, 3, 5, 10, 40, 200, 3000):
-        for le in np.linspace(-14, 4, 61):
+        for le in np.linspace(-17, 4, 85):
             e = float(10.0 ** le)
             for prior in (False, True):
                 a, b = D.calc_pA(k, e, prior), O.calc_pA(k, e, prior)

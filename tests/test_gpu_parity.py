@@ -241,6 +241,63 @@ def test_dada_config0_matches_oracle():
     want = O.dada(s.seqs, s.abund, w.err, w.ncol, O.DadaParams(nthreads=8), quals=s.quals)
     got = D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, D.DadaParams(), quals=s.quals)
     assert_same_dada(got, want)
+    # the map's decision margin is the closest final p-value to omega_c
+    # among the non-centers (a center is not tested against omega_c)
+    index = {q: i for i, q in enumerate(s.seqs)}
+    noncenter = np.ones(len(s.seqs), bool)
+    for c in got["clusters"]:
+        noncenter[index["".join("ACGT"[x - 1] for x in np.asarray(c["sequence"]))]] = False
+    omega_c = D.DadaParams().omega_c
+    pv = got["pvals"]
+    assert got["margins"]["omega_c"] == float(np.min(np.abs(pv[noncenter] - omega_c) / omega_c))
+    assert got["margins"]["omega_a"] > 1e-6
+
+
+def test_dada_config2_full_size_matches_oracle():
+    """PacBio 16S at the full configured size: 5,000 uniques of 1,400-1,550 nt
+    from 60 variants, indel-heavy errors, band 32 and homopolymer gap -1 (the
+    row-major i32 homopolymer aligner, src/nwalign.rs:435-528), qualities up
+    to Q93 (the error matrix extends by its last column)."""
+    w = synth.config2(seed=1002)
+    s = w.samples[0]
+    assert len(s.seqs) == 5000
+    import os
+
+    op = O.DadaParams(align=O.AlignParams(band=32, homo_gap_p=-1), nthreads=max(2, os.cpu_count() or 2))
+    dp = D.DadaParams(align=D.AlignParams(band=32, homo_gap_p=-1))
+    want = O.dada(s.seqs, s.abund, w.err, w.ncol, op, quals=s.quals)
+    got = D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, dp, quals=s.quals)
+    assert want["counters"]["homo"] > 10000
+    assert_same_dada(got, want)
+
+
+@pytest.fixture(scope="module")
+def config3_prefix():
+    w = synth.config3(seed=1003)
+    s = w.samples[0]
+    n = 30000
+    return w, synth.Sample(s.seqs[:n], np.asarray(s.abund[:n]), s.quals[:n], 0, name="config3[:30000]")
+
+
+def test_dada_config3_pooled_prefix_matches_oracle(config3_prefix):
+    """The pooled workload (200 samples pooled in first-seen order, 3,000
+    variants x 150 nt): its first 30,000 pooled uniques as one sample --
+    about 2,700 clusters -- equal the oracle's run_dada bit for bit, with
+    FP64 lambda and with decisions from the FP32 log-sum lambda."""
+    import os
+
+    w, s = config3_prefix
+    op = O.DadaParams(align=O.AlignParams(band=w.band, homo_gap_p=w.homo_gap_p, kmer_size=w.kmer_size),
+                      nthreads=max(2, os.cpu_count() or 2))
+    dp = D.DadaParams(align=D.AlignParams(band=w.band, homo_gap_p=w.homo_gap_p, kmer_size=w.kmer_size))
+    want = O.dada(s.seqs, s.abund, w.err, w.ncol, op, quals=s.quals)
+    got = D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, dp, quals=s.quals)
+    assert want["nclust"] > 1000
+    assert_same_dada(got, want)
+    dp32 = D.DadaParams(align=dp.align, lambda_fp32=True)
+    got32 = D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, dp32, quals=s.quals)
+    assert got32["nclust"] == want["nclust"]
+    assert np.array_equal(got32["map"], want["map"])
 
 
 def test_dada_batch_matches_per_sample_oracle():

@@ -160,6 +160,35 @@ def test_calc_pA_matches_incomplete_gamma(reads, lam):
         assert O.calc_pA(reads, lam, False) == pytest.approx(got / norm, rel=1e-15)
 
 
+def test_ln_gamma_is_the_lanczos_form_statrs_documents():
+    """statrs 0.18.0 computes lnGamma by the Lanczos approximation with Pugh's
+    r = 10.900511 and eleven coefficients (accurate to about 16 digits), not
+    by the C library: it agrees with lgamma to ~1e-15 relative but not to the
+    bit (lnGamma(1) is -4.4e-16 there, a known property of that form)."""
+    for x in (0.5, 0.75, 1.0, 1.5, 2.0, 3.0, 7.5, 10.0, 41.0, 100.0, 999.5, 12345.0, 65535.0, 1e6):
+        got, want = O.ln_gamma(x), math.lgamma(x)
+        assert got == pytest.approx(want, rel=2e-14, abs=2e-15), x
+    assert O.ln_gamma(1.0) == -4.440892098500626e-16
+    assert O.ln_gamma(2.0) == 0.0
+    # ln(k!) = lnGamma(k + 1) over the read counts the p-values see
+    acc = 0.0
+    for k in range(1, 3000):
+        acc += math.log(k)
+        assert O.ln_gamma(k + 1.0) == pytest.approx(acc, rel=1e-13, abs=1e-14)
+
+
+def test_gamma_lr_answers_zero_within_statrs_accuracy_of_zero():
+    """statrs' gamma_lr returns 0.0 for x within its default accuracy
+    (10 * 2^-53) of zero, so calc_pA takes the log-space tail
+    (src/pval.rs:219-226) for such tiny expected abundances."""
+    assert O.gamma_lr(3.0, 1e-15) == 0.0
+    assert O.gamma_lr(1.0, 1.2e-15) > 0.0
+    for reads in (1, 2, 4):
+        p = O.calc_pA(reads, 5e-16, True)
+        ln_want = reads * math.log(5e-16) - 5e-16 - math.lgamma(reads + 1)
+        assert math.log(p) == pytest.approx(ln_want, rel=1e-12)
+
+
 def test_calc_pA_tiny_lambda_fallback():
     sp = pytest.importorskip("scipy.special")
     for reads in (2, 5, 40):
