@@ -140,6 +140,8 @@ struct CompareLaunch {
   uint32_t ntask;
   uint32_t total_items;
   uint32_t screen_chunk;    // items a k_screen warp takes at a time (4..32; set by launch_compare)
+  uint32_t screen_chunk_max;  // tuning: the largest chunk launch_compare may pick (16 or 32)
+  uint32_t screen_blocks_per_sm;  // tuning: k_screen blocks per SM in its one wave (1..4)
   uint32_t* queue_pass;     // nraw capacity: items that passed the screen
   uint32_t* queue_counts;   // 8 words; [4] = items pushed to queue_pass
   uint8_t* nw_scratch;      // nwarps * max(vec_scratch, rm_scratch)

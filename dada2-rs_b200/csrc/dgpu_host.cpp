@@ -5,9 +5,12 @@
 // screen off, then bud -> compare -> shuffle -> p-update until nothing buds. The
 // compare (screen, alignment, lambda, store) runs on the GPU; the serial phases
 // (shuffle, p-update, bud) run here, one host thread per sample in batch mode.
+#include <dlfcn.h>
+
 #include <algorithm>
 #include <array>
 #include <atomic>
+#include <cctype>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -293,14 +296,159 @@ static void recycle_all(B&... b) {
 // ---------------------------------------------------------------------------
 // Device pool: the resident uniques of one or more samples
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Tuning table: the launch shape of the compare step per read-length class
+// (class 0: longest unique <= 200 nt, 1: <= 600 nt, 2: longer). Filled by the
+// autotuner (dada2_b200/autotune.py sweeps these knobs on synthetic workloads
+// of each class and saves the fastest), loaded at first use from
+// DGPU_TUNING_FILE or else tuning.txt beside this library, and set or saved
+// through dgpu_tuning_*. The DGPU_LAUNCH_SLOTS / DGPU_BATCH_MAX /
+// DGPU_DEDICATED_SLOTS environment variables still override it. Without a
+// table the built-in values below apply (measured on the 40-sample
+// 250/220-nt batch).
+// ---------------------------------------------------------------------------
+static const dgpu_tuning kTuneDefault = {6, 4, 1, kAlignCtasPerSm, 32, 4};
+static std::mutex g_tune_mu;
+static dgpu_tuning g_tune[3] = {kTuneDefault, kTuneDefault, kTuneDefault};
+static bool g_tune_loaded = false;
+
+static int length_class(uint32_t lmax) { return lmax <= 200 ? 0 : (lmax <= 600 ? 1 : 2); }
+
+static bool tuning_valid(const dgpu_tuning& t) {
+  return t.launch_slots >= 1 && t.launch_slots <= 8 && t.samples_per_launch >= 1 && t.samples_per_launch <= 4096 &&
+         t.dedicated_slots >= 0 && t.dedicated_slots <= 7 && t.align_ctas_per_sm >= 1 &&
+         t.align_ctas_per_sm <= kAlignCtasPerSm && (t.screen_chunk_max == 16 || t.screen_chunk_max == 32) &&
+         t.screen_blocks_per_sm >= 1 && t.screen_blocks_per_sm <= 4;
+}
+
+// Text form: one line per class, "class C launch_slots A samples_per_launch B
+// dedicated_slots D align_ctas_per_sm E screen_chunk_max F
+// screen_blocks_per_sm G"; '#' starts a comment. Unknown keys are an error.
+static int tuning_parse(const std::string& text, dgpu_tuning out[3], std::string* msg) {
+  dgpu_tuning t[3] = {g_tune[0], g_tune[1], g_tune[2]};
+  size_t pos = 0;
+  int lineno = 0;
+  while (pos < text.size()) {
+    size_t e = text.find('\n', pos);
+    if (e == std::string::npos) e = text.size();
+    std::string line = text.substr(pos, e - pos);
+    pos = e + 1;
+    ++lineno;
+    const size_t h = line.find('#');
+    if (h != std::string::npos) line.resize(h);
+    std::vector<std::string> tok;
+    size_t q = 0;
+    while (q < line.size()) {
+      while (q < line.size() && std::isspace(static_cast<unsigned char>(line[q]))) ++q;
+      size_t r = q;
+      while (r < line.size() && !std::isspace(static_cast<unsigned char>(line[r]))) ++r;
+      if (r > q) tok.push_back(line.substr(q, r - q));
+      q = r;
+    }
+    if (tok.empty()) continue;
+    if (tok.size() % 2 != 0 || tok[0] != "class") {
+      *msg = "tuning line " + std::to_string(lineno) + ": expected 'class C key value ...'";
+      return DGPU_E_INVALID;
+    }
+    const int c = std::atoi(tok[1].c_str());
+    if (c < 0 || c > 2 || tok[1].find_first_not_of("0123456789") != std::string::npos) {
+      *msg = "tuning line " + std::to_string(lineno) + ": class must be 0, 1 or 2";
+      return DGPU_E_INVALID;
+    }
+    dgpu_tuning v = t[c];
+    for (size_t k = 2; k + 1 < tok.size(); k += 2) {
+      const int x = std::atoi(tok[k + 1].c_str());
+      if (tok[k] == "launch_slots") v.launch_slots = x;
+      else if (tok[k] == "samples_per_launch") v.samples_per_launch = x;
+      else if (tok[k] == "dedicated_slots") v.dedicated_slots = x;
+      else if (tok[k] == "align_ctas_per_sm") v.align_ctas_per_sm = x;
+      else if (tok[k] == "screen_chunk_max") v.screen_chunk_max = x;
+      else if (tok[k] == "screen_blocks_per_sm") v.screen_blocks_per_sm = x;
+      else {
+        *msg = "tuning line " + std::to_string(lineno) + ": unknown key " + tok[k];
+        return DGPU_E_INVALID;
+      }
+    }
+    if (!tuning_valid(v)) {
+      *msg = "tuning line " + std::to_string(lineno) + ": value out of range";
+      return DGPU_E_INVALID;
+    }
+    t[c] = v;
+  }
+  for (int c = 0; c < 3; ++c) out[c] = t[c];
+  return 0;
+}
+
+static std::string tuning_format(const dgpu_tuning t[3]) {
+  std::string o = "# compare-step launch shape per read-length class (0: <= 200 nt, 1: <= 600 nt, 2: longer)\n";
+  for (int c = 0; c < 3; ++c)
+    o += "class " + std::to_string(c) + " launch_slots " + std::to_string(t[c].launch_slots) +
+         " samples_per_launch " + std::to_string(t[c].samples_per_launch) + " dedicated_slots " +
+         std::to_string(t[c].dedicated_slots) + " align_ctas_per_sm " + std::to_string(t[c].align_ctas_per_sm) +
+         " screen_chunk_max " + std::to_string(t[c].screen_chunk_max) + " screen_blocks_per_sm " +
+         std::to_string(t[c].screen_blocks_per_sm) + "\n";
+  return o;
+}
+
+// Under g_tune_mu.
+static int tuning_load_file(const std::string& path, std::string* msg) {
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) {
+    *msg = "cannot open tuning file " + path;
+    return DGPU_E_INVALID;
+  }
+  std::string text;
+  char buf[4096];
+  size_t n;
+  while ((n = std::fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, n);
+  std::fclose(f);
+  dgpu_tuning t[3];
+  const int rc = tuning_parse(text, t, msg);
+  if (rc) return rc;
+  for (int c = 0; c < 3; ++c) g_tune[c] = t[c];
+  return 0;
+}
+
+// Under g_tune_mu: on first use, the table of DGPU_TUNING_FILE or of
+// tuning.txt beside this library (a missing or malformed file leaves the
+// built-in table).
+static void tuning_first_use() {
+  if (g_tune_loaded) return;
+  g_tune_loaded = true;
+  std::string path;
+  if (const char* e = std::getenv("DGPU_TUNING_FILE")) {
+    path = e;
+  } else {
+    Dl_info info{};
+    if (dladdr(reinterpret_cast<void*>(&tuning_first_use), &info) && info.dli_fname) {
+      path = info.dli_fname;
+      const size_t sl = path.rfind('/');
+      path = (sl == std::string::npos ? std::string(".") : path.substr(0, sl)) + "/tuning.txt";
+    }
+  }
+  if (path.empty()) return;
+  if (FILE* f = std::fopen(path.c_str(), "rb")) {
+    std::fclose(f);
+    std::string msg;
+    (void)tuning_load_file(path, &msg);
+  }
+}
+
+static dgpu_tuning tuning_class(int c) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  tuning_first_use();
+  return g_tune[c];
+}
+static dgpu_tuning tuning_for(uint32_t lmax) { return tuning_class(length_class(lmax)); }
+
 // Launch slots dedicated to the longest chains: DGPU_DEDICATED_SLOTS (0..7) if
-// set, else 1.
-static size_t dedicated_slots() {
+// set, else the tuning table's (1 built in).
+static size_t dedicated_slots(uint32_t lmax) {
   if (const char* e = std::getenv("DGPU_DEDICATED_SLOTS")) {
     const int v = std::atoi(e);
     if (v >= 0 && v <= 7) return size_t(v);
   }
-  return 1;
+  return size_t(tuning_for(lmax).dedicated_slots);
 }
 
 struct Pool;
@@ -550,13 +698,13 @@ struct Pool {
     // (at most 4 groups) for the register form
     geom.vec_scratch = vec_possible ? align16(size_t(geom.vec_nrow) * std::max<size_t>(size_t(geom.vec_ncol), 32)) : 0;
     geom.rm_scratch = rm_possible ? align16(size_t(2 * lmax + 1) * 2 * kb * 4) : 0;
-    geom.nwarps = sms * kAlignCtasPerSm * kNwWarps;
+    geom.nwarps = sms * tuning_for(lmax).align_ctas_per_sm * kNwWarps;
     const size_t per = std::max<size_t>(std::max(geom.vec_scratch, geom.rm_scratch), 16);
     slots.clear();
     for (int k = 0; k < nslots; ++k) {
       slots.emplace_back(new Slot);
       Slot& L = *slots.back();
-      TRY(L.init(this, nslots > 1 && size_t(k) < dedicated_slots()));  // the dedicated slots come first
+      TRY(L.init(this, nslots > 1 && size_t(k) < dedicated_slots(lmax)));  // the dedicated slots come first
       TRY(L.scratch.alloc(per * size_t(geom.nwarps)));
       TRY(L.queue_pass.alloc(nraw));
     }
@@ -674,6 +822,11 @@ int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
   L.nstore_blocks = nblk;
   L.do_store = do_store ? 1 : 0;
   L.err_host = err_host.d;
+  {
+    const dgpu_tuning tu = tuning_for(Q.lmax);
+    L.screen_chunk_max = uint32_t(tu.screen_chunk_max);
+    L.screen_blocks_per_sm = uint32_t(tu.screen_blocks_per_sm);
+  }
   const uint64_t every = g_stats.timing_every.load();
   const bool timing = every != 0 && g_stats.call_seq.fetch_add(1) % every == 0;
   launch_compare(L, st, timing ? ev : nullptr);
@@ -2505,14 +2658,14 @@ static dgpu_result* finish(SampleState& S, const SampleSeqs& in) {
 // queue; with several slots a sample that becomes ready while a launch is in
 // flight goes out at once on another slot. A sample's own sequence of steps is
 // exactly run_dada's.
-static size_t batch_max_samples();
+static size_t batch_max_samples(uint32_t lmax);
 
 // on_finish (may be empty) is called for each sample as soon as its loop ends,
 // from the host thread that ran its last phase.
 static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_params& ap, int host_threads,
                        const std::function<void(size_t)>& on_finish = {}) {
   const size_t ns = S.size();
-  const size_t batch_max = batch_max_samples();
+  const size_t batch_max = batch_max_samples(P.lmax);
   std::mutex mu;
   std::condition_variable cv;
   std::vector<size_t> ready;
@@ -2531,7 +2684,7 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
   // themselves: they never wait for a slot and their kernels are scheduled
   // ahead of the others'. The other slots serve the rest, largest first.
   const size_t nw_all = std::min(P.slots.size(), ns);
-  const size_t kd = nw_all > 1 ? std::min(dedicated_slots(), nw_all - 1) : 0;
+  const size_t kd = nw_all > 1 ? std::min(dedicated_slots(P.lmax), nw_all - 1) : 0;
   std::vector<uint8_t> is_done(ns, 0), is_crit(ns, 0);
   std::vector<size_t> crit(kd, SIZE_MAX);  // crit[i]: the sample slot i serves
   auto pick_critical = [&] {  // under mu: the kd largest unfinished samples
@@ -2693,21 +2846,23 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
 }
 
 // Most samples one compare launch covers: DGPU_BATCH_MAX (1..4096) if set,
-// else 4. Small launches finish sooner, and the largest ready samples (the
-// longest chains of dependent rounds) are served first.
-static size_t batch_max_samples() {
+// else the tuning table's (4 built in). Small launches finish sooner, and the
+// largest ready samples (the longest chains of dependent rounds) are served
+// first.
+static size_t batch_max_samples(uint32_t lmax) {
   if (const char* e = std::getenv("DGPU_BATCH_MAX")) {
     const long v = std::atol(e);
     if (v >= 1 && v <= 4096) return size_t(v);
   }
-  return 4;
+  return size_t(tuning_for(lmax).samples_per_launch);
 }
 
 // Launch slots for a batch of nsamples: DGPU_LAUNCH_SLOTS (1..8) if set, else
-// 6 (on B200 the 40-sample batch steps in 84-86 ms with 6, 87-88 with 4 and
-// 96-101 with 3); never more than there are samples.
-static int launch_slots(int nsamples) {
-  int k = 6;
+// the tuning table's (6 built in: on B200 the 40-sample batch stepped in
+// 84-86 ms with 6, 87-88 with 4 and 96-101 with 3); never more than there are
+// samples.
+static int launch_slots(int nsamples, uint32_t lmax) {
+  int k = tuning_for(lmax).launch_slots;
   if (const char* e = std::getenv("DGPU_LAUNCH_SLOTS")) {
     const int v = std::atoi(e);
     if (v >= 1 && v <= 8) k = v;
@@ -2750,7 +2905,9 @@ static int batch_prepare(Batch& B, int device, const dgpu_dada_params* prm, int 
   std::string smsg;
   const int first_bad = check_samples(nsamples, sample_start, lens, k, &total, &src, &smsg);
   if (total >= 0xffffffffull) return fail(DGPU_E_UNSUPPORTED, "more than 4 GiB of sequence in one pool");
-  TRY(B.pool.init(device, launch_slots(nsamples)));
+  uint32_t lmax_all = 0;
+  for (uint32_t t = sample_start[0]; t < sample_start[nsamples]; ++t) lmax_all = std::max(lmax_all, lens[t]);
+  TRY(B.pool.init(device, launch_slots(nsamples, lmax_all)));
   const int ns_ok = first_bad;  // samples [0, ns_ok) passed the structural checks
   uint64_t ok_bytes = 0;
   for (uint32_t t = sample_start[0]; t < sample_start[ns_ok]; ++t) ok_bytes += lens[t];
@@ -3457,6 +3614,48 @@ int dgpu_result_fp32_stats(const dgpu_result* r, uint64_t* out2) {
   if (!r || !out2) return fail(DGPU_E_INVALID, "null argument");
   out2[0] = r->fp32[0];
   out2[1] = r->fp32[1];
+  return 0;
+}
+
+int dgpu_tuning_get(int max_len, dgpu_tuning* out) {
+  if (!out || max_len < 0) return fail(DGPU_E_INVALID, "bad argument");
+  *out = tuning_for(uint32_t(max_len));
+  return 0;
+}
+
+int dgpu_tuning_set(int length_class, const dgpu_tuning* t) {
+  if (!t || length_class < 0 || length_class > 2) return fail(DGPU_E_INVALID, "bad argument");
+  if (!tuning_valid(*t)) return fail(DGPU_E_INVALID, "tuning value out of range");
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  tuning_first_use();  // the default file must not overwrite this later
+  g_tune[length_class] = *t;
+  return 0;
+}
+
+int dgpu_tuning_load(const char* path) {
+  if (!path) return fail(DGPU_E_INVALID, "null path");
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  tuning_first_use();
+  std::string msg;
+  const int rc = tuning_load_file(path, &msg);
+  return rc ? fail(rc, msg) : 0;
+}
+
+int dgpu_tuning_save(const char* path) {
+  if (!path) return fail(DGPU_E_INVALID, "null path");
+  const dgpu_tuning t[3] = {tuning_class(0), tuning_class(1), tuning_class(2)};
+  const std::string text = tuning_format(t);
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return fail(DGPU_E_INVALID, std::string("cannot write ") + path);
+  const bool ok = std::fwrite(text.data(), 1, text.size(), f) == text.size();
+  std::fclose(f);
+  return ok ? 0 : fail(DGPU_E_INVALID, std::string("short write to ") + path);
+}
+
+int dgpu_tuning_reset(void) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  g_tune_loaded = true;  // the built-in table; no file is read afterwards
+  for (int c = 0; c < 3; ++c) g_tune[c] = kTuneDefault;
   return 0;
 }
 

@@ -2240,17 +2240,21 @@ void launch_compare(const CompareLaunch& L0, cudaStream_t st, cudaEvent_t* ev) {
   // last round), so no partial second wave or ragged tail is left; chunks
   // stay at 16 or more there, since a chunk's per-item bookkeeping runs on
   // one lane per item.
-  const uint32_t cap = uint32_t(sms) * 4u;
+  // The wave's blocks per SM (at most 4) and the largest chunk (16 or 32)
+  // come from the tuning table.
+  const uint32_t bps = (L0.screen_blocks_per_sm >= 1 && L0.screen_blocks_per_sm <= 4) ? L0.screen_blocks_per_sm : 4u;
+  const uint32_t chmax = L0.screen_chunk_max == 16 ? 16u : 32u;
+  const uint32_t cap = uint32_t(sms) * bps;
   const uint64_t warps = uint64_t(cap) * kScreenWarps;
   CompareLaunch L = L0;
   auto nblocks = [&](uint32_t ch) {
     return uint32_t((uint64_t(L.total_items) + kScreenWarps * ch - 1) / (uint64_t(kScreenWarps) * ch));
   };
   L.screen_chunk = 4;
-  if (nblocks(32) <= cap) {
+  if (nblocks(chmax) <= cap) {
     while (nblocks(L.screen_chunk) > cap) L.screen_chunk *= 2;
   } else {
-    for (uint32_t ch = 32; ch >= 16; ch /= 2) {
+    for (uint32_t ch = chmax; ch >= 16; ch /= 2) {
       const uint64_t chunks = (uint64_t(L.total_items) + ch - 1) / ch;
       const uint64_t rounds = (chunks + warps - 1) / warps;
       L.screen_chunk = ch;

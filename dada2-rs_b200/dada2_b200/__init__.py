@@ -21,11 +21,12 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from ._lib import (AlignParamsC, CountersC, DadaOutC, DadaParamsC, DgpuError, InvalidInput, KernelStatsC,
-                   check, device_count, lib, ptr)
+                   TuningC, check, device_count, lib, ptr)
 
 __all__ = ["AlignParams", "DadaParams", "CompareContext", "dada_uniques", "dada_uniques_batch", "dada_uniques_sharded",
            "ResidentBatch", "PackedBatch", "DenoiseService", "pack_sample", "Derep", "derep_fastq", "dada_fastq", "align_pairs", "stats_reset", "stats_timing", "stats_read",
-           "DgpuError", "InvalidInput", "device_count", "METHOD_NAMES", "KERNEL_NAMES"]
+           "DgpuError", "InvalidInput", "device_count", "METHOD_NAMES", "KERNEL_NAMES", "TUNING_KEYS",
+           "tuning_get", "tuning_set", "tuning_load", "tuning_save", "tuning_reset", "length_class"]
 
 KERNEL_NAMES = ["profiles", "screen", "align", "store"]
 
@@ -567,6 +568,40 @@ def cache_release(device: int = -1) -> int:
     n = C.c_uint64(0)
     check(lib().dgpu_cache_release(int(device), C.byref(n)))
     return int(n.value)
+
+
+TUNING_KEYS = [n for n, _ in TuningC._fields_]
+
+
+def length_class(max_len: int) -> int:
+    """The tuning table's read-length class: 0 up to 200 nt, 1 up to 600, 2 longer."""
+    return 0 if max_len <= 200 else (1 if max_len <= 600 else 2)
+
+
+def tuning_get(max_len: int) -> dict:
+    """The launch shape a pool whose longest unique has ``max_len`` bases uses."""
+    t = TuningC()
+    check(lib().dgpu_tuning_get(int(max_len), C.byref(t)))
+    return {k: int(getattr(t, k)) for k in TUNING_KEYS}
+
+
+def tuning_set(cls: int, setting: dict):
+    """Sets read-length class ``cls``'s launch shape (pools created later use it)."""
+    t = TuningC(*[int(setting[k]) for k in TUNING_KEYS])
+    check(lib().dgpu_tuning_set(int(cls), C.byref(t)))
+
+
+def tuning_load(path: str):
+    check(lib().dgpu_tuning_load(str(path).encode()))
+
+
+def tuning_save(path: str):
+    check(lib().dgpu_tuning_save(str(path).encode()))
+
+
+def tuning_reset():
+    """Back to the built-in table (no tuning file is read afterwards)."""
+    check(lib().dgpu_tuning_reset())
 
 
 def stats_reset():

@@ -55,6 +55,11 @@ class KernelStatsC(C.Structure):
                 ("h2d_bytes", C.c_uint64), ("batch_ms", C.c_double * 3), ("prepare_ms", C.c_double * 4)]
 
 
+class TuningC(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("launch_slots", "samples_per_launch", "dedicated_slots",
+                                         "align_ctas_per_sm", "screen_chunk_max", "screen_blocks_per_sm")]
+
+
 class CountersC(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("screened", "aligned", "shrouded", "stored", "gapless",
                                           "vectorized", "homo", "endsfree")]
@@ -103,6 +108,11 @@ def lib():
         L.dgpu_result_transitions.argtypes = [_P, _P]
         L.dgpu_result_fp32_stats.argtypes = [_P, _P]
         L.dgpu_result_margins.argtypes = [_P, _P]
+        L.dgpu_tuning_get.argtypes = [C.c_int, C.POINTER(TuningC)]
+        L.dgpu_tuning_set.argtypes = [C.c_int, C.POINTER(TuningC)]
+        L.dgpu_tuning_load.argtypes = [C.c_char_p]
+        L.dgpu_tuning_save.argtypes = [C.c_char_p]
+        L.dgpu_tuning_reset.argtypes = []
         L.dgpu_get_methods.argtypes = [_P, _P]
         L.dgpu_service_create.argtypes = [C.c_int, C.POINTER(DadaParamsC), _P, C.c_int, C.c_uint64, _P]
         L.dgpu_service_submit.argtypes = [_P, C.c_int, _P, _P, _P, _P, _P, _P, _P]

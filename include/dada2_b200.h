@@ -224,6 +224,33 @@ int dgpu_dada_sharded(int device, const dgpu_dada_params* params, int nraw, cons
  * writes the bytes given back to *freed (may be NULL). */
 int dgpu_cache_release(int device, uint64_t* freed);
 
+/* ---- tuning table ----
+ * The launch shape of the compare step per read-length class of a pool
+ * (class 0: longest unique <= 200 nt, 1: <= 600 nt, 2: longer):
+ * launch_slots         concurrent compare launches (streams) of a batch, 1..8
+ * samples_per_launch   most samples one compare launch serves, 1..4096
+ * dedicated_slots      slots reserved for the samples with the longest chains, 0..7
+ * align_ctas_per_sm    resident CTAs of the alignment kernel per SM (4 pairs each), 1..4
+ * screen_chunk_max     largest run of (center, unique) items one screen warp takes, 16 or 32
+ * screen_blocks_per_sm screen blocks per SM in its single wave, 1..4
+ * The library loads DGPU_TUNING_FILE, else tuning.txt beside itself, at first
+ * use (the autotuner, dada2_b200/autotune.py, writes that file); the
+ * DGPU_LAUNCH_SLOTS, DGPU_BATCH_MAX and DGPU_DEDICATED_SLOTS environment
+ * variables override it. A setting applies to pools created after it.
+ * Results never depend on it. Replaces the reference's only scheduling knob,
+ * the rayon grain DADA2_RS_PAR_GRAIN (src/cluster.rs:19-28). */
+typedef struct {
+  int32_t launch_slots, samples_per_launch, dedicated_slots, align_ctas_per_sm, screen_chunk_max,
+      screen_blocks_per_sm;
+} dgpu_tuning;
+/* the setting a pool whose longest unique has max_len bases would use */
+int dgpu_tuning_get(int max_len, dgpu_tuning* out);
+int dgpu_tuning_set(int length_class, const dgpu_tuning* t);
+int dgpu_tuning_load(const char* path);
+int dgpu_tuning_save(const char* path);
+/* back to the built-in table; no file is loaded afterwards */
+int dgpu_tuning_reset(void);
+
 int dgpu_stats_reset(void);
 /* every = 0 stops the per-kernel timing; every = N >= 1 times every N-th
  * compare call (events cost a few microseconds per call). */
