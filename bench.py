@@ -310,53 +310,55 @@ def committed_dp_profile():
 
 
 def dp_roofline(samples, w, params, device, calls=4, sm_mhz=None):
-    """k_align alone: every unique of the samples in one pool against the
-    centers of the first `calls` samples with the k-mer screen off (cutoff
-    1.0, like run_dada's first compare, src/dada.rs:835-838), one launch per
-    call on one stream with nothing else running. Cells are the reference's
-    cell model, (len1 + len2 + 1) x (band + 1) per NW pair (the aligner each
-    raw took is read back per call); 7 integer ops per cell (equality test,
-    select, three saturating adds, max with tie rule, strict diagonal test).
-    The launch also aligns the gapless pairs and forms every lambda; their
-    time is inside the figure."""
+    """k_align alone, on run_dada's first compare call (src/dada.rs:835-838):
+    each of the `calls` largest samples in its own context, every unique
+    against the sample's cluster-0 center with the k-mer screen off (cutoff
+    1.0), one launch per sample on one stream with nothing else running.
+    Cells are the reference's cell model, (len1 + len2 + 1) x (band + 1) per
+    NW pair (the aligner each raw took is read back per call); 7 integer ops
+    per cell (equality test, select, three saturating adds, max with tie
+    rule, strict diagonal test). The launch also aligns the gapless pairs and
+    forms every lambda; their time is inside the figure."""
     import dada2_b200 as D
 
-    codes, reads, quals, bases, m = _encode_pool(samples, w)
-    lens = np.array([len(c) for c in codes], np.int64)
-    centers = []
-    for s, b in zip(samples[:calls], bases):
-        ab = np.asarray(s.abund, np.uint32)
-        centers.append(b + int(np.flatnonzero(ab == ab.max())[-1]))
+    big = sorted(samples, key=lambda x: -len(x.seqs))[:max(calls, 1)]
     band = params.align.band
-    with D.CompareContext(params.align, m.ravel().copy(), m.shape[1], device=device) as ctx:
-        ctx.upload(codes, reads, quals=quals)
-        ctx.compare(centers[0], 1.0)  # warm-up
-        cells = pairs = gapless = 0
-        D.stats_reset()
-        D.stats_timing(1)
-        for c in centers:
-            ctx.compare(c, 1.0)
+    cells = pairs = gapless = 0
+    ms = 0.0
+    n = 0
+    for s in big:
+        codes, reads, quals, bases, m = _encode_pool([s], w)
+        lens = np.array([len(c) for c in codes], np.int64)
+        center = int(np.flatnonzero(reads == reads.max())[-1])  # B::new's center (src/containers.rs:450-458)
+        with D.CompareContext(params.align, m.ravel().copy(), m.shape[1], device=device) as ctx:
+            ctx.upload(codes, reads, quals=quals)
+            ctx.compare(center, 1.0)  # warm-up
+            D.stats_reset()
+            D.stats_timing(1)
+            ctx.compare(center, 1.0)
+            D.stats_timing(False)
+            st = D.stats_read()
             meth = ctx.methods()
-            nw = (meth >= 2) & (meth <= 4)
-            pairs += int(nw.sum())
-            gapless += int((meth == 1).sum())
-            cells += int(((lens[nw] + lens[c] + 1) * (band + 1)).sum())
-        D.stats_timing(False)
-        st = D.stats_read()
-    ms = st["ms"]["align"]
-    n = max(st["timed_rounds"], 1)
+        nw = (meth >= 2) & (meth <= 4)
+        pairs += int(nw.sum())
+        gapless += int((meth == 1).sum())
+        cells += int(((lens[nw] + lens[center] + 1) * (band + 1)).sum())
+        ms += st["ms"]["align"]
+        n += int(st["timed_rounds"])
+    n = max(n, 1)
     cups = cells / (ms / 1e3) if ms > 0 else None
     peak = issue_peak_tops(sm_mhz)
     ops = 7.0 * cups / 1e12 if cups else None
     return {"bound": "int_issue", "kernel": "k_align", "achieved": ops, "peak": peak,
             "unit": "Tops/s (INT32 lane ops, 7 per cell)", "frac": ops / peak if ops else None,
-            "gcups": cups / 1e9 if cups else None, "launches": int(st["timed_rounds"]),
+            "gcups": cups / 1e9 if cups else None, "launches": n,
             "ms_per_launch": ms / n, "nw_pairs_per_launch": pairs / n, "gapless_pairs_per_launch": gapless / n,
             "cells_per_launch": cells / n,
             "peak_note": "148 SMs x 4 SMSPs x 32 lanes x the sampled SM clock; MEASURED_PEAKS.json has no integer "
                          "figure",
-            "measured": f"{len(centers)} isolated launches, every unique of the workload against one center with "
-                        f"the screen off, one stream"}
+            "measured": f"the first compare call of the {len(big)} largest samples ({', '.join(str(len(x.seqs)) for x in big)} "
+                        f"uniques), each alone on one stream: every unique against its sample's first center, "
+                        f"screen off"}
 
 
 def fp32_partition(samples, w, params, device):
@@ -538,6 +540,7 @@ def pooled_report(local, steps, warmup, with_cpu=True):
                                  "one launch at a time)",
                      "bytes_per_call": st["timed_screen_bytes"] / max(st["timed_rounds"], 1)},
         "decision_margin": finite_margins(r0["margins"]),
+        "tuning": D.tuning_get(max(len(q) for q in s.seqs)),
         "precision": precision,
         "gpu_launches": int(sum(st["launches"].values())),
         "clocks": clk,
@@ -659,6 +662,7 @@ def service_report(local, steps, warmup, with_cpu=True):
                 "d2h_bytes_per_step": None, "note": "requests from host buffers through the service, results "
                                                     "read back as sizes and counters"},
         "gpu_launches": launches,
+        "tuning": {str(L): D.tuning_get(L) for L in (150, 250, 1450)},
         "clocks": clk,
         "cpu_baseline": cpu,
     }
@@ -729,6 +733,7 @@ def single_sample_report(config, local, steps, warmup, with_cpu=True, sm_mhz=Non
                        "p99": float(np.percentile(lat, 99)) if len(lat) else None, "unit": "per compare call"},
         "roofline": dp,
         "decision_margin": finite_margins(r0["margins"]),
+        "tuning": D.tuning_get(max(len(q) for q in s.seqs)),
         "gpu_launches": int(sum(st["launches"].values())),
         "cpu_baseline": cpu,
     }
@@ -959,7 +964,7 @@ def main():
         "nw": {"cells_per_step": nw_cells,
                "note": "cells = (len1+len2+1) x (band+1) per NW pair of the last timed step; the aligner's rate is "
                        "roofline_dp's, from isolated launches"},
-        "decision_margin": {**finite_margins(margins), "note": "smallest |p - omega| / omega over every threshold test of the "
+        "decision_margin": {**finite_margins(margins), "note": "smallest |p - omega| / min(p, omega) over every threshold test of the "
                                                "40 samples: bud p*nraw vs omega_a, prior p vs omega_p, final map "
                                                "p vs omega_c (+inf: no such test)"},
         "latency_ms": {"p50": float(np.percentile(lat, 50)) if len(lat) else None,
@@ -980,6 +985,9 @@ def main():
         "clocks": clk,
         "plain": plain,
         "cpu_baseline": cpu,
+        "tuning": {**D.tuning_get(max(len(q) for x in w.samples for q in x.seqs)),
+                   "note": "launch shape in force (tuning.txt beside the library, written by "
+                           "dada2_b200.autotune on a B200; built-in values without it)"},
         "other_configs": others,
     }
     print(json.dumps(line), flush=True)

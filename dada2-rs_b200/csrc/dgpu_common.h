@@ -43,6 +43,14 @@ struct PoolDev {
   uint32_t* res_ham;
   uint8_t* res_status;
   float* res_loglam32;  // with KParams::lambda32: FP32 ln(lambda) of aligned pairs, -inf otherwise
+  // Pivot bound of the screen (k <= 7, the clustering loop only): per raw the
+  // largest u8 k-mer dot with any center so far (piv_dot) and that center's
+  // cluster (piv_cl, kNoPivot when none); per sample, cl_center[base + i] =
+  // cluster i's center and cdot[base + i] = the current center's dot with it.
+  uint32_t* piv_dot;
+  uint32_t* piv_cl;
+  uint32_t* cl_center;
+  uint32_t* cdot;
   uint32_t nraw;
   uint32_t maxlen;
 };
@@ -93,6 +101,8 @@ constexpr int kScreenSmemTasks = 128; // tasks whose table the screen keeps in s
 constexpr int kNwWarps = 4;       // warps per NW CTA
 constexpr int kAlignCtasPerSm = 4; // resident align CTAs per SM (128 registers per thread)
 constexpr int kStageBytes = 4096; // traceback staging per warp
+constexpr uint32_t kNoPivot = 0xffffffffu;
+constexpr int kRmStageRows = 128; // anti-diagonals of pointer planes the row-major traceback stages at once
 constexpr int kStoreSpan = 2048;  // raws per store CTA (its own output segment)
 constexpr int kStoreThreads = 256; // threads per store CTA
 constexpr int kSeqPad = 160;      // guard bytes on each side of the aligners' shared-memory sequences
@@ -113,7 +123,7 @@ __host__ __device__ inline size_t nw_smem_per_warp_vec(const NwGeom& g) {
          align16(g.lmax);
 }
 __host__ __device__ inline size_t nw_smem_per_warp_rm(const NwGeom& g) {
-  return align16(g.lmax) * 4 + align16(size_t(32) * 2 * rm_kbound(g.rm_pairs) * 4) + align16(g.lmax) +
+  return align16(g.lmax) * 4 + align16(size_t(kRmStageRows) * 2 * rm_kbound(g.rm_pairs) * 4) + align16(g.lmax) +
          align16(size_t(g.lmax) * 2);
 }
 // The align kernel carves either layout from the same per-warp region.
@@ -142,6 +152,14 @@ struct CompareLaunch {
   uint32_t screen_chunk;    // items a k_screen warp takes at a time (4..32; set by launch_compare)
   uint32_t screen_chunk_max;  // tuning: the largest chunk launch_compare may pick (16 or 32)
   uint32_t screen_blocks_per_sm;  // tuning: k_screen blocks per SM in its one wave (1..4)
+  // Pivot bound: with `pivot` the screen keeps each raw's pivot and records
+  // each task's center as cl_center[base + cluster]; with `cdot_ready`
+  // k_pivot_dots has filled cdot for clusters [0, cluster) of every task
+  // (task_cl_prefix: prefix sums of the tasks' cluster indices) and the
+  // screen excludes raws by the bound.
+  uint32_t pivot, cdot_ready;
+  const uint32_t* task_cl_prefix;
+  uint32_t total_cl;
   uint32_t* queue_pass;     // nraw capacity: items that passed the screen
   uint32_t* queue_counts;   // 8 words; [4] = items pushed to queue_pass
   uint8_t* nw_scratch;      // nwarps * max(vec_scratch, rm_scratch)

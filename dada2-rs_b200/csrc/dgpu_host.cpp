@@ -307,7 +307,7 @@ static void recycle_all(B&... b) {
 // table the built-in values below apply (measured on the 40-sample
 // 250/220-nt batch).
 // ---------------------------------------------------------------------------
-static const dgpu_tuning kTuneDefault = {6, 4, 1, kAlignCtasPerSm, 32, 4};
+static const dgpu_tuning kTuneDefault = {6, 4, 1, kAlignCtasPerSm, 32, 4, 32768};
 static std::mutex g_tune_mu;
 static dgpu_tuning g_tune[3] = {kTuneDefault, kTuneDefault, kTuneDefault};
 static bool g_tune_loaded = false;
@@ -318,7 +318,7 @@ static bool tuning_valid(const dgpu_tuning& t) {
   return t.launch_slots >= 1 && t.launch_slots <= 8 && t.samples_per_launch >= 1 && t.samples_per_launch <= 4096 &&
          t.dedicated_slots >= 0 && t.dedicated_slots <= 7 && t.align_ctas_per_sm >= 1 &&
          t.align_ctas_per_sm <= kAlignCtasPerSm && (t.screen_chunk_max == 16 || t.screen_chunk_max == 32) &&
-         t.screen_blocks_per_sm >= 1 && t.screen_blocks_per_sm <= 4;
+         t.screen_blocks_per_sm >= 1 && t.screen_blocks_per_sm <= 4 && t.pivot_min_items >= 0;
 }
 
 // Text form: one line per class, "class C launch_slots A samples_per_launch B
@@ -364,6 +364,7 @@ static int tuning_parse(const std::string& text, dgpu_tuning out[3], std::string
       else if (tok[k] == "align_ctas_per_sm") v.align_ctas_per_sm = x;
       else if (tok[k] == "screen_chunk_max") v.screen_chunk_max = x;
       else if (tok[k] == "screen_blocks_per_sm") v.screen_blocks_per_sm = x;
+      else if (tok[k] == "pivot_min_items") v.pivot_min_items = x;
       else {
         *msg = "tuning line " + std::to_string(lineno) + ": unknown key " + tok[k];
         return DGPU_E_INVALID;
@@ -386,7 +387,8 @@ static std::string tuning_format(const dgpu_tuning t[3]) {
          " samples_per_launch " + std::to_string(t[c].samples_per_launch) + " dedicated_slots " +
          std::to_string(t[c].dedicated_slots) + " align_ctas_per_sm " + std::to_string(t[c].align_ctas_per_sm) +
          " screen_chunk_max " + std::to_string(t[c].screen_chunk_max) + " screen_blocks_per_sm " +
-         std::to_string(t[c].screen_blocks_per_sm) + "\n";
+         std::to_string(t[c].screen_blocks_per_sm) + " pivot_min_items " + std::to_string(t[c].pivot_min_items) +
+         "\n";
   return o;
 }
 
@@ -489,8 +491,9 @@ struct Slot {
     for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
     TRY(queue_counts.alloc(8));
     TRY(err_dev.alloc(1));
-    TRY(err_host.alloc(1));
+    TRY(err_host.alloc(2));  // [0] error flags, [1] profiles the screen read
     err_host.h[0] = 0;
+    err_host.h[1] = 0;
     // both start at zero; every call leaves them at zero again
     CUDA_TRY(cudaMemsetAsync(queue_counts.p, 0, 32, st));
     CUDA_TRY(cudaMemsetAsync(err_dev.p, 0, 4, st));
@@ -545,6 +548,8 @@ struct Pool {
   DBuf<uint8_t> kcnt;
   DBuf<double> e_minmax, err, lambda;
   DBuf<float> loglam32;
+  DBuf<uint32_t> piv_dot, piv_cl, cl_center, cdot;  // the screen's pivot bound (PoolDev)
+  bool pivot_on = false;  // the clustering loop runs here: keep pivots and use the bound
   // stored comps of each task, at the task's first raw (its sample's base)
   HBuf<uint32_t> comp_index, comp_ham;
   HBuf<double> comp_lambda;
@@ -557,7 +562,7 @@ struct Pool {
     slots.clear();  // each slot drains its own stream first
     if (st && cudaStreamSynchronize(st) == cudaSuccess)
       recycle_all(seq, qual, kmer8, sat, lock, status, off, len, reads, ham, knum, kidx, kcnt, e_minmax, err, lambda, loglam32,
-                  comp_index, comp_ham, comp_lambda, comp_ll32, lock_host);
+                  comp_index, comp_ham, comp_lambda, comp_ll32, lock_host, piv_dot, piv_cl, cl_center, cdot);
     if (st) cudaStreamDestroy(st);
   }
 
@@ -636,6 +641,13 @@ struct Pool {
     TRY(kcnt.alloc(sparse ? seq_bytes : 1));
     TRY(knum.alloc(sparse ? n : 1));
     TRY(sat.alloc(n));
+    {
+      const size_t pn = kp.use_kmers && !sparse ? size_t(n) : 1;
+      TRY(piv_dot.alloc(pn));
+      TRY(piv_cl.alloc(pn));
+      TRY(cl_center.alloc(pn));
+      TRY(cdot.alloc(pn));
+    }
     TRY(comp_index.alloc(n));
     TRY(comp_ham.alloc(n));
     TRY(comp_lambda.alloc(n));
@@ -675,9 +687,13 @@ struct Pool {
     return 0;
   }
 
+  // Per-run device state: every e_minmax back to -999 (B::new,
+  // src/containers.rs:342) and no raw with a pivot yet.
   int reset_e_minmax() {
-    launch_fill_f64(e_minmax.p, nraw, -999.0, st);  // B::new (src/containers.rs:342)
+    launch_fill_f64(e_minmax.p, nraw, -999.0, st);
     CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemsetAsync(piv_cl.p, 0xff, piv_cl.n * 4, st));
+    CUDA_TRY(cudaMemsetAsync(piv_dot.p, 0, piv_dot.n * 4, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     return 0;
   }
@@ -730,6 +746,10 @@ struct Pool {
     v.res_ham = ham.p;
     v.res_status = status.p;
     v.res_loglam32 = loglam32.p;
+    v.piv_dot = piv_dot.p;
+    v.piv_cl = piv_cl.p;
+    v.cl_center = cl_center.p;
+    v.cdot = cdot.p;
     v.nraw = nraw;
     v.maxlen = lmax;
     return v;
@@ -781,7 +801,8 @@ int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
   }
   TRY(ensure_blocks(nblk));
   const size_t o_pref = align16(sizeof(TaskDev) * ntask);
-  const size_t o_map = o_pref + align16(size_t(4) * (ntask + 1));
+  const size_t o_clp = o_pref + align16(size_t(4) * (ntask + 1));
+  const size_t o_map = o_clp + align16(size_t(4) * (ntask + 1));
   const size_t pack_bytes = o_map + align16(size_t(8) * std::max<uint32_t>(nblk, 1));
   TRY(ensure_pack(pack_bytes));
   std::memcpy(hpack.h, task_stage.h, sizeof(TaskDev) * ntask);
@@ -797,6 +818,18 @@ int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
     }
   }
   pref[ntask] = total;
+  // the pivot bound: clusters [0, cluster) of each task get a center dot
+  uint32_t* clp = reinterpret_cast<uint32_t*>(hpack.h + o_clp);
+  uint32_t total_cl = 0;
+  const bool pivot = Q.pivot_on && Q.kp.use_kmers && Q.kp.kmer_size <= 7;
+  for (uint32_t t = 0; t < ntask; ++t) {
+    clp[t] = total_cl;
+    const TaskDev& T = task_stage.h[t];
+    if (pivot && T.cluster < T.n) total_cl += T.cluster;
+  }
+  clp[ntask] = total_cl;
+  const uint32_t min_items = uint32_t(tuning_for(Q.lmax).pivot_min_items);
+  const bool cdot_ready = pivot && total_cl > 0 && min_items > 0 && total >= min_items;
   CUDA_TRY(cudaMemcpyAsync(dpack.p, hpack.h, pack_bytes, cudaMemcpyHostToDevice, st));
   count_h2d(pack_bytes);
   CompareLaunch L{};
@@ -827,13 +860,18 @@ int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
     L.screen_chunk_max = uint32_t(tu.screen_chunk_max);
     L.screen_blocks_per_sm = uint32_t(tu.screen_blocks_per_sm);
   }
+  L.pivot = pivot ? 1u : 0u;
+  L.cdot_ready = cdot_ready ? 1u : 0u;
+  L.task_cl_prefix = reinterpret_cast<const uint32_t*>(dpack.p + o_clp);
+  L.total_cl = cdot_ready ? total_cl : 0u;
   const uint64_t every = g_stats.timing_every.load();
   const bool timing = every != 0 && g_stats.call_seq.fetch_add(1) % every == 0;
   launch_compare(L, st, timing ? ev : nullptr);
   CUDA_TRY(cudaGetLastError());
   if (!do_store) {  // no store kernel to rearm the queue or report the flags
-    CUDA_TRY(cudaMemsetAsync(queue_counts.p, 0, 32, st));
     CUDA_TRY(cudaMemcpyAsync(err_host.h, err_dev.p, 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(err_host.h + 1, queue_counts.p + 5, 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemsetAsync(queue_counts.p, 0, 32, st));
   }
   auto t0 = Clock::now();
   // Poll and yield rather than block in the driver's spin: the launch slots'
@@ -862,11 +900,16 @@ int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
     S.rounds += 1;
     S.compares += total;
     S.screened += screened;
-    // algorithmic screen bytes: the raw's 4^k profile, or for k = 8 its sparse
-    // list (3 bytes per present k-mer, at most L - k + 1), plus 16 B of metadata
+    // algorithmic screen bytes: the 4^k profile of every raw whose profile the
+    // screen read (screened raws less those the pivot bound excluded), or
+    // for k = 8 the sparse list of every screened raw (3 bytes per present
+    // k-mer, at most L - k + 1); 16 B of metadata per compare, 8 more for the
+    // pivot when the loop keeps pivots; and both profiles of each center dot
     const uint64_t prof = Q.kp.kmer_size >= 8 ? uint64_t(3) * (Q.lmax - uint32_t(Q.kp.kmer_size) + 1)
                                               : (uint64_t(1) << (2 * Q.kp.kmer_size));
-    const uint64_t sb = screened * prof + uint64_t(total) * 16u;
+    const uint64_t nread = Q.kp.kmer_size >= 8 ? screened : uint64_t(err_host.h[1]);
+    const uint64_t sb = nread * prof + uint64_t(total) * (pivot ? 24u : 16u) +
+                        (cdot_ready ? uint64_t(total_cl) * 2u * prof : 0u);
     S.screen_bytes += sb;
     if (timing) {
       S.timed_rounds += 1;
@@ -884,6 +927,7 @@ int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
     if (ew & DERR_UNSUPPORTED) what += " band wider than 1024 offsets on the row-major aligner;";
     if (ew & DERR_LAMBDA) what += " non-ACGT code or quality beyond the error matrix in lambda;";
     err_host.h[0] = 0;
+    err_host.h[1] = 0;
     CUDA_TRY(cudaMemsetAsync(err_dev.p, 0, 4, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     return fail(ew & DERR_UNSUPPORTED ? DGPU_E_UNSUPPORTED : DGPU_E_DEVICE, "device error:" + what);
@@ -1515,15 +1559,20 @@ struct SampleState {
   }
 
   // ---- decision margins ----
-  // The smallest relative distance |p - omega| / omega of any p-value that a
-  // threshold test of the loop compared: the bud's p * nraw against omega_a
-  // and the prior raw's p against omega_p (src/cluster.rs:1501-1640), and
-  // the final map's p against omega_c (src/dada.rs:525-533). A margin far
-  // above 1e-12 means that ulp-level differences in the p-values cannot
-  // change a decision. +inf when no test of that kind ran.
+  // The smallest relative distance |p - omega| / min(p, omega) of any
+  // p-value that a threshold test of the loop compared: the bud's p * nraw
+  // against omega_a and the prior raw's p against omega_p
+  // (src/cluster.rs:1501-1640), and the final map's p against omega_c
+  // (src/dada.rs:525-533). It is symmetric (p = omega / 2 and p = 2 omega
+  // both give 1) and +inf for p = 0. A margin far above 1e-12 means that
+  // ulp-level differences in the p-values cannot change a decision. +inf when
+  // no test of that kind ran.
   double margin[3] = {std::numeric_limits<double>::infinity(), std::numeric_limits<double>::infinity(),
                       std::numeric_limits<double>::infinity()};
-  static double rel_margin(double pv, double omega) { return std::fabs(pv - omega) / omega; }
+  static double rel_margin(double pv, double omega) {
+    const double lo = std::min(pv, omega);
+    return lo > 0.0 ? std::fabs(pv - omega) / lo : std::numeric_limits<double>::infinity();
+  }
 
   // ---- FP32 lambda decisions (DadaConf::fp32) ----
   std::atomic<uint64_t> fp32_evals{0}, fp32_fallbacks{0};
@@ -3069,6 +3118,7 @@ static int batch_run(Batch& B, dgpu_result** out, const std::function<void(size_
   Pool& P = B.pool;
   const auto tb0 = Clock::now();
   CUDA_TRY(cudaSetDevice(P.device));
+  P.pivot_on = true;  // cluster indices are the loop's own: the screen may keep pivots
   TRY(P.reset_e_minmax());
   std::memset(P.lock_host.h, 0, P.nraw);
   CUDA_TRY(cudaMemsetAsync(P.lock.p, 0, P.nraw, P.st));
@@ -3261,6 +3311,7 @@ static int shard_run(Batch& B, int prep_rc, int rank, int world, const ShardGath
   ShardHead setup{};
   setup.err = prep_rc ? prep_rc : [&]() -> int {
     CUDA_TRY(cudaSetDevice(P.device));
+    P.pivot_on = false;  // a share's task base is not its sample's: no pivots
     TRY(P.reset_e_minmax());
     std::memset(P.lock_host.h, 0, P.nraw);
     CUDA_TRY(cudaMemsetAsync(P.lock.p, 0, P.nraw, P.st));

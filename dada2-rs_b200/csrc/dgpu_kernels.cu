@@ -275,6 +275,35 @@ __device__ __forceinline__ uint32_t mismatch_word(const uint8_t* a, const uint8_
 
 // Lean streaming screen: greedy skip, profile dot product, strict cutoff
 // (src/cluster.rs:295-298, src/kmers.rs:254-269, src/nwalign.rs:1299).
+// Pivot dots: for every task of the launch and every earlier cluster i of its
+// sample, cdot[base + i] = the u8 k-mer dot of the task's center with cluster
+// i's center (cl_center[base + i]); the screen's pivot bound reads them. One
+// warp per (task, cluster) item, 16-byte vector loads of both profiles.
+template <int K>
+__global__ void __launch_bounds__(256) k_pivot_dots(CompareLaunch L) {
+  constexpr int NK16 = (1 << (2 * K)) / 16;
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps_total = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t item = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); item < L.total_cl; item += warps_total) {
+    const uint32_t t = find_task(L.task_cl_prefix, L.ntask, item);
+    const TaskDev T = L.tasks[t];
+    const uint32_t ci = item - L.task_cl_prefix[t];
+    const uint32_t p = L.pool.cl_center[T.base + ci];
+    const uint4* pc = reinterpret_cast<const uint4*>(L.pool.kmer8 + size_t(T.center) * size_t(NK16) * 16);
+    const uint4* pp = reinterpret_cast<const uint4*>(L.pool.kmer8 + size_t(p) * size_t(NK16) * 16);
+    uint32_t dot = 0;
+    for (int v = lane; v < NK16; v += 32) {
+      const uint4 a = __ldg(pc + v), b = __ldg(pp + v);
+      dot = __dp4a(__vminu4(a.x, b.x), 0x01010101u, dot);
+      dot = __dp4a(__vminu4(a.y, b.y), 0x01010101u, dot);
+      dot = __dp4a(__vminu4(a.z, b.z), 0x01010101u, dot);
+      dot = __dp4a(__vminu4(a.w, b.w), 0x01010101u, dot);
+    }
+    dot = __reduce_add_sync(FULL, dot);
+    if (lane == 0) L.pool.cdot[T.base + ci] = dot;
+  }
+}
+
 // A warp takes 32 consecutive items: lane l resolves item l's task and raw
 // metadata, then the warp streams the raw profiles four at a time against the
 // center profile held in registers. Survivors go to the align queue with their
@@ -294,6 +323,7 @@ __global__ void __launch_bounds__(kScreenWarps * 32, 4) k_screen(CompareLaunch L
   __shared__ uint32_t s_prefix[kScreenSmemTasks + 1];
   __shared__ uint32_t s_base[kScreenSmemTasks], s_center[kScreenSmemTasks], s_creads[kScreenSmemTasks];
   __shared__ double s_cutoff[kScreenSmemTasks];
+  __shared__ uint32_t s_cluster[kScreenSmemTasks];
   const bool tasks_smem = L.ntask <= uint32_t(kScreenSmemTasks);
   if (tasks_smem) {
     for (uint32_t t = threadIdx.x; t <= L.ntask; t += blockDim.x) {
@@ -304,32 +334,72 @@ __global__ void __launch_bounds__(kScreenWarps * 32, 4) k_screen(CompareLaunch L
         s_center[t] = T.center;
         s_creads[t] = T.center_reads;
         s_cutoff[t] = T.cutoff;
+        s_cluster[t] = T.cluster;
       }
     }
     __syncthreads();
   }
+  // the pivot bound (k <= 7 only): every task's center becomes a pivot
+  // candidate for the sample's later calls
+  const bool pivot = K < 8 && L.pivot != 0 && kp.use_kmers;
+  if (pivot && blockIdx.x == 0)
+    for (uint32_t t = threadIdx.x; t < L.ntask; t += blockDim.x) {
+      const TaskDev T = L.tasks[t];
+      if (T.cluster < T.n) L.pool.cl_center[T.base + T.cluster] = T.center;
+    }
   const uint32_t CH = L.screen_chunk;  // lanes [0, CH) carry an item
   for (uint32_t chunk = (blockIdx.x * kScreenWarps + wib) * CH; chunk < L.total_items; chunk += warps_total * CH) {
     const uint32_t item = chunk + lane;
     const bool valid = uint32_t(lane) < CH && item < L.total_items;
-    uint32_t t = 0, g = 0, c = 0;
-    bool skip = false;
+    uint32_t t = 0, g = 0, c = 0, ccl = 0, tbase = 0;
+    bool skip = false, bounded = false, pivot_raw = false, cl_fits = false;
     if (valid) {
       uint32_t creads;
       if (tasks_smem) {
         t = find_task(s_prefix, L.ntask, item);
-        g = s_base[t] + (item - s_prefix[t]);
+        tbase = s_base[t];
         c = s_center[t];
         creads = s_creads[t];
+        ccl = s_cluster[t];
       } else {
         t = find_task(L.task_prefix, L.ntask, item);
-        g = L.tasks[t].base + (item - L.task_prefix[t]);
+        tbase = L.tasks[t].base;
         c = L.tasks[t].center;
         creads = L.tasks[t].center_reads;
+        ccl = L.tasks[t].cluster;
       }
+      const uint32_t t0 = tasks_smem ? s_prefix[t] : L.task_prefix[t];
+      const uint32_t tn = (tasks_smem ? s_prefix[t + 1] : L.task_prefix[t + 1]) - t0;
+      g = tbase + (item - t0);
+      cl_fits = ccl < tn;  // cluster indices of a whole sample stay below its raw count
       skip = kp.greedy && (L.pool.reads[g] > creads || L.pool.lock[g]);
+      if (pivot && !skip) {
+        // Exact exclusion without reading the raw's profile. For non-negative
+        // count vectors min(c, r) <= min(c, p) + r - min(r, p) elementwise, so
+        // dot(c, r) <= dot(c, p) + |r| - dot(r, p) for the raw's pivot center
+        // p (|r| = len - K + 1 windows while no count saturates). kdist =
+        // 1 - dot / (minlen - K + 1) falls as the dot rises, in floating point
+        // too, so a bound kdist above the cutoff means the exact one is above
+        // it as well: the raw is shrouded (src/nwalign.rs:1295-1301). Raws or
+        // centers with a saturated count take the exact path and never this.
+        const int lc = int(L.pool.len[c]), lg = int(L.pool.len[g]);
+        pivot_raw = cl_fits && !L.pool.sat[g] && !L.pool.sat[c] && lc >= K && lg >= K;
+        if (pivot_raw && L.cdot_ready) {
+          const uint32_t pc = L.pool.piv_cl[g];
+          if (pc < ccl) {
+            const int minl = lc < lg ? lc : lg;
+            const uint32_t ub = L.pool.cdot[tbase + pc] + uint32_t(lg - K + 1) - L.pool.piv_dot[g];
+            const double kd_lb = 1.0 - double(ub) / double(minl - K + 1);
+            bounded = kd_lb > (tasks_smem ? s_cutoff[t] : L.tasks[t].cutoff);
+          }
+        }
+      }
     }
-    const bool need = valid && !skip && kp.use_kmers;
+    const bool need = valid && !skip && kp.use_kmers && !bounded;
+    {
+      const uint32_t needm = __ballot_sync(FULL, need);  // profiles this chunk reads
+      if (lane == 0 && needm) atomicAdd(&L.queue_counts[5], uint32_t(__popc(needm)));
+    }
     uint32_t mydot = 0, myovf = 0;
     uint32_t todo = __ballot_sync(FULL, need);
     if constexpr (K >= 8) {
@@ -464,10 +534,22 @@ __global__ void __launch_bounds__(kScreenWarps * 32, 4) k_screen(CompareLaunch L
       exact = __reduce_add_sync(FULL, exact);
       if (lane == j) mydot = exact;
     }
+    // the dot becomes the raw's pivot when it beats the one it has
+    if (pivot && need && pivot_raw) {
+      const uint32_t pc = L.pool.piv_cl[g];
+      if (pc == kNoPivot || mydot > L.pool.piv_dot[g]) {
+        L.pool.piv_dot[g] = mydot;
+        L.pool.piv_cl[g] = ccl;
+      }
+    }
     bool pass = false;
     if (valid) {
       if (kp.lambda32) L.pool.res_loglam32[g] = -INFINITY;
-      if (skip) {
+      if (bounded) {
+        L.pool.res_lambda[g] = 0.0;
+        L.pool.res_ham[g] = 0xffffffffu;
+        L.pool.res_status[g] = ST_SHROUDED;
+      } else if (skip) {
         L.pool.res_lambda[g] = 0.0;
         L.pool.res_ham[g] = 0xffffffffu;
         L.pool.res_status[g] = ST_SKIPPED;
@@ -1684,22 +1766,33 @@ struct RmSmem {
   uint8_t* s2;
   uint8_t* h1;
   uint8_t* h2;
-  uint32_t* stage;  // 32 diagonals x 2K words
+  uint32_t* stage;  // kRmStageRows diagonals x 2K words
   uint8_t* tcode;
   uint16_t* fidx;
 };
 
-__device__ void homo_mask_warp(int lane, const uint8_t* s, int n, uint8_t* m) {
-  // p lies in a run of >= 3 equal bases (src/nwalign.rs:211-227)
+// m[p] = the base code s[p] (1..4) with bit 4 set when p lies in a run of
+// >= 3 equal bases (src/nwalign.rs:211-227) and `homo` is on, so the aligner
+// reads a position's base and its gap class with one load.
+__device__ void code_mask_warp(int lane, const uint8_t* s, int n, uint8_t* m, bool homo) {
   for (int p = lane; p < n; p += 32) {
     bool in = false;
-    if (p >= 2 && s[p - 2] == s[p] && s[p - 1] == s[p]) in = true;
-    if (p >= 1 && p + 1 < n && s[p - 1] == s[p] && s[p + 1] == s[p]) in = true;
-    if (p + 2 < n && s[p + 1] == s[p] && s[p + 2] == s[p]) in = true;
-    m[p] = in ? 1 : 0;
+    if (homo) {
+      if (p >= 2 && s[p - 2] == s[p] && s[p - 1] == s[p]) in = true;
+      if (p >= 1 && p + 1 < n && s[p - 1] == s[p] && s[p + 1] == s[p]) in = true;
+      if (p + 2 < n && s[p + 1] == s[p] && s[p + 2] == s[p]) in = true;
+    }
+    m[p] = uint8_t(s[p] | (in ? 16u : 0u));
   }
 }
 
+// Row-major ends-free aligner (src/nwalign.rs:336-528) evaluated as an
+// anti-diagonal wavefront: cell (i, j) sits on anti-diagonal t = i + j at
+// offset o = j - i; lane q of group m owns offsets o_lo + 2(q + 32 m) + par,
+// par = (t - o_lo) & 1, so every anti-diagonal's band cells are spread over
+// the lanes and each needs only its own lane's and one neighbour's previous
+// values (one shuffle). Gaps inside homopolymer runs cost homo_gap; the last
+// row and column are free; ties prefer up, then left, then diagonal.
 template <int K>
 __device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8_t* g2, int len2, int match,
                               int mismatch, int gap, int homo_gap, int band, bool homo, const RmSmem& S,
@@ -1708,10 +1801,8 @@ __device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8
   for (int p = lane; p < len1; p += 32) S.s1[p] = g1[p];
   for (int p = lane; p < len2; p += 32) S.s2[p] = g2[p];
   __syncwarp();
-  if (homo) {
-    homo_mask_warp(lane, S.s1, len1, S.h1);
-    homo_mask_warp(lane, S.s2, len2, S.h2);
-  }
+  code_mask_warp(lane, S.s1, len1, S.h1, homo);
+  code_mask_warp(lane, S.s2, len2, S.h2, homo);
   int lband, rband, o_lo, o_hi;
   if (band >= 0) {
     if (len2 > len1) { lband = band; rband = band + (len2 - len1); }
@@ -1732,54 +1823,83 @@ __device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8
     return false;
   }
   __syncwarp();
+  const int hgap = homo ? homo_gap : gap;
+  // What a cell needs besides its neighbours' values depends only on its
+  // position: the up and left gap costs (free on the last row / column,
+  // homo_gap inside a homopolymer run), the diagonal score and whether it is
+  // a band cell, row 0 / column 0 or outside. Those of anti-diagonal t + 1
+  // are loaded and formed while anti-diagonal t's values are computed, so
+  // the shared-memory loads stay off the dependency chain.
+  struct Cost {
+    int gu, gl, sd;
+    uint32_t kind;  // 1 cell, 2 row 0 / column 0 inside the band, 0 outside
+  };
+  auto cost_at = [&](int t, int m) {
+    const int q = lane + 32 * m;
+    const int o = o_lo + 2 * q + ((t - o_lo) & 1);
+    const int i = (t - o) >> 1, j = (t + o) >> 1;
+    const bool inband = q < P && o <= o_hi;
+    const bool cell = inband && i >= 1 && j >= 1 && i <= len1 && j <= len2;
+    const bool edge = inband && !cell && i >= 0 && j >= 0 && i <= len1 && j <= len2;
+    // clamped reads: a lane outside the matrix reads a valid byte it ignores
+    const uint32_t x = S.h1[max(0, min(i - 1, len1 - 1))], y = S.h2[max(0, min(j - 1, len2 - 1))];
+    Cost c;
+    c.gu = (j == len2) ? 0 : ((x & 16u) ? hgap : gap);
+    c.gl = (i == len1) ? 0 : ((y & 16u) ? hgap : gap);
+    c.sd = ((x ^ y) & 15u) == 0u ? match : mismatch;
+    c.kind = cell ? 1u : (edge ? 2u : 0u);
+    return c;
+  };
   int ve[K], vo[K];
+  Cost cur[K];
 #pragma unroll
-  for (int m = 0; m < K; ++m) { ve[m] = kNegSentinel; vo[m] = kNegSentinel; }
+  for (int m = 0; m < K; ++m) {
+    ve[m] = kNegSentinel;
+    vo[m] = kNegSentinel;
+    cur[m] = cost_at(0, m);
+  }
   uint32_t pw[2 * K];
 #pragma unroll
   for (int m = 0; m < 2 * K; ++m) pw[m] = 0;
   const int tmax = len1 + len2;
   for (int t = 0; t <= tmax; ++t) {
+    Cost nxt[K];
+#pragma unroll
+    for (int m = 0; m < K; ++m) nxt[m] = cost_at(t + 1, m);  // past tmax: unused
     const int par = (t - o_lo) & 1;
 #pragma unroll
     for (int m = 0; m < K; ++m) {
       const int q = lane + 32 * m;
-      const int o = o_lo + 2 * q + par;
-      int own = par ? vo[m] : ve[m];
+      const int own = par ? vo[m] : ve[m];
       int left_nb, up_nb;
       if (par == 0) {
-        int a = __shfl_up_sync(FULL, vo[m], 1);
-        int a31 = (m > 0) ? __shfl_sync(FULL, vo[m > 0 ? m - 1 : 0], 31) : kNegSentinel;
+        const int a = __shfl_up_sync(FULL, vo[m], 1);
+        const int a31 = (m > 0) ? __shfl_sync(FULL, vo[m > 0 ? m - 1 : 0], 31) : kNegSentinel;
         left_nb = (lane == 0) ? a31 : a;
         if (q == 0) left_nb = kNegSentinel;
         up_nb = vo[m];
       } else {
-        int b = __shfl_down_sync(FULL, ve[m], 1);
-        int b0 = (m + 1 < K) ? __shfl_sync(FULL, ve[m + 1 < K ? m + 1 : m], 0) : kNegSentinel;
+        const int b = __shfl_down_sync(FULL, ve[m], 1);
+        const int b0 = (m + 1 < K) ? __shfl_sync(FULL, ve[m + 1 < K ? m + 1 : m], 0) : kNegSentinel;
         up_nb = (lane == 31) ? b0 : b;
         if (q + 1 >= P) up_nb = kNegSentinel;
         left_nb = ve[m];
       }
-      const int i = (t - o) >> 1, j = (t + o) >> 1;
-      int val, code = 0;
-      if (q >= P || o > o_hi) {
-        val = kNegSentinel;
-      } else if (i >= 1 && i <= len1 && j >= 1 && j <= len2) {
-        const int up = up_nb + ((j == len2) ? 0 : ((homo && S.h1[i - 1]) ? homo_gap : gap));
-        const int left = left_nb + ((i == len1) ? 0 : ((homo && S.h2[j - 1]) ? homo_gap : gap));
-        const int dg = own + (S.s1[i - 1] == S.s2[j - 1] ? match : mismatch);
-        if (up >= dg && up >= left) { val = up; code = 3; }
-        else if (left >= dg) { val = left; code = 2; }
-        else { val = dg; code = 1; }
-      } else if (i >= 0 && j >= 0 && i <= len1 && j <= len2) {
-        val = 0;  // row 0 / column 0 inside the band
-      } else {
-        val = kNegSentinel;
+      const int up = up_nb + cur[m].gu;
+      const int left = left_nb + cur[m].gl;
+      const int dg = own + cur[m].sd;
+      const bool upw = up >= dg && up >= left;
+      const bool lw = !upw && left >= dg;
+      int val = upw ? up : (lw ? left : dg);
+      uint32_t code = upw ? 3u : (lw ? 2u : 1u);
+      if (cur[m].kind != 1u) {
+        val = cur[m].kind == 2u ? 0 : kNegSentinel;
+        code = 0u;
       }
       if (par) vo[m] = val;
       else ve[m] = val;
-      const uint32_t b0w = __ballot_sync(FULL, code & 1);
-      const uint32_t b1w = __ballot_sync(FULL, (code >> 1) & 1);
+      const uint32_t b0w = __ballot_sync(FULL, code & 1u);
+      const uint32_t b1w = __ballot_sync(FULL, code & 2u);
       if (lane == (t & 31)) {
         pw[2 * m] = b0w;
         pw[2 * m + 1] = b1w;
@@ -1793,9 +1913,15 @@ __device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8
         for (int m = 0; m < 2 * K; ++m) dst[m] = pw[m];
       }
     }
+#pragma unroll
+    for (int m = 0; m < K; ++m) cur[m] = nxt[m];
   }
   __syncwarp();
   // Traceback (src/nwalign.rs:234-273): row 0 moves left, column 0 moves up.
+  // A window of kRmStageRows anti-diagonals of pointer planes is staged in
+  // shared memory; lane k tests whether the k-th next step is diagonal (cell
+  // (i-k, j-k): anti-diagonal t-2k, same offset), so a run of f diagonal
+  // steps is taken at once, one per lane. Other steps are taken singly.
   for (int p = lane; p < len2; p += 32) S.tcode[p] = uint8_t(kUnaligned | ((unsigned(S.s2[p]) - 1u) * 5u));
   int i = len1, j = len2, slo = 0x7fffffff;
   uint32_t ham = 0, alen = 0;
@@ -1808,8 +1934,8 @@ __device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8
     else {
       const int o = j - i, t = i + j;
       if (o < o_lo || o > o_hi) { ok = false; break; }
-      if (t < slo) {
-        const int nlo = max(0, t - 31);
+      if (t < slo || (t - slo < kRmStageRows / 2 && slo > 0)) {  // keep half a window below t
+        const int nlo = max(0, t - (kRmStageRows - 1));
         __syncwarp();
         const int nw = (t - nlo + 1) * 2 * K;
         const uint32_t* src = pscr + size_t(nlo) * (2 * K);
@@ -1818,17 +1944,35 @@ __device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8
         slo = nlo;
       }
       const int q = (o - o_lo) >> 1, L = q & 31, m = q >> 5;
+      const int tk = t - 2 * lane;
+      bool diag = false;
+      if (tk >= slo && i - lane >= 1 && j - lane >= 1) {
+        const uint32_t* wk = S.stage + (tk - slo) * (2 * K) + 2 * m;
+        diag = (((wk[0] >> L) & 1u) | (((wk[1] >> L) & 1u) << 1)) == 1u;
+      }
+      const uint32_t nd = __ballot_sync(FULL, !diag);
+      const int f = nd ? __ffs(nd) - 1 : 32;
+      if (f > 0) {
+        bool mm = false;
+        if (lane < f) {
+          const uint8_t a = S.s1[i - 1 - lane], b = S.s2[j - 1 - lane];
+          S.tcode[j - 1 - lane] = uint8_t((unsigned(a) - 1u) * 4u + (unsigned(b) - 1u));
+          mm = a != b;
+          if (dbg0) {
+            dbg0[alen + lane] = a;
+            dbg1[alen + lane] = b;
+          }
+        }
+        ham += __popc(__ballot_sync(FULL, mm));
+        i -= f;
+        j -= f;
+        alen += uint32_t(f);
+        continue;
+      }
       const uint32_t* w = S.stage + (t - slo) * (2 * K) + 2 * m;
       v = int((w[0] >> L) & 1u) | (int((w[1] >> L) & 1u) << 1);
     }
-    if (v == 1) {
-      const uint8_t a = S.s1[i - 1], b = S.s2[j - 1];
-      if (lane == 0) S.tcode[j - 1] = uint8_t((unsigned(a) - 1u) * 4u + (unsigned(b) - 1u));
-      ham += (a != b) ? 1u : 0u;
-      if (dbg0 && lane == 0) { dbg0[alen] = a; dbg1[alen] = b; }
-      --i;
-      --j;
-    } else if (v == 2) {
+    if (v == 2) {
       if (dbg0 && lane == 0) { dbg0[alen] = '-'; dbg1[alen] = S.s2[j - 1]; }
       --j;
     } else if (v == 3) {
@@ -1858,7 +2002,7 @@ __device__ RmSmem carve_rm(unsigned char* base, int lmax, int kbound) {
   S.s2 = take(lmax);
   S.h1 = take(lmax);
   S.h2 = take(lmax);
-  S.stage = reinterpret_cast<uint32_t*>(take(size_t(32) * 2 * kbound * 4));
+  S.stage = reinterpret_cast<uint32_t*>(take(size_t(kRmStageRows) * 2 * kbound * 4));
   S.tcode = take(lmax);
   S.fidx = reinterpret_cast<uint16_t*>(take(size_t(lmax) * 2));
   return S;
@@ -2212,7 +2356,11 @@ __global__ void __launch_bounds__(kStoreThreads) k_store(CompareLaunch L) {
   if (blk == 0) {
     // the screen and align kernels have finished: hand their error flags to
     // the host through mapped memory and rearm the queue for the next call
-    if (threadIdx.x == 0) *reinterpret_cast<volatile uint32_t*>(L.err_host) = *L.err_word;
+    if (threadIdx.x == 0) {
+      reinterpret_cast<volatile uint32_t*>(L.err_host)[0] = *L.err_word;
+      reinterpret_cast<volatile uint32_t*>(L.err_host)[1] = L.queue_counts[5];  // profiles the screen read
+    }
+    __syncthreads();
     if (threadIdx.x < 8) L.queue_counts[threadIdx.x] = 0;
   }
 }
@@ -2264,6 +2412,16 @@ void launch_compare(const CompareLaunch& L0, cudaStream_t st, cudaEvent_t* ev) {
   uint32_t blocks = nblocks(L.screen_chunk);
   if (blocks > cap) blocks = cap;
   if (ev) cudaEventRecord(ev[0], st);
+  if (L.cdot_ready && L.total_cl > 0 && L.kp.kmer_size <= 7) {
+    const uint32_t pb = std::min<uint32_t>((L.total_cl + 7) / 8, uint32_t(sms) * 8u);
+    switch (L.kp.kmer_size) {
+      case 3: k_pivot_dots<3><<<pb, 256, 0, st>>>(L); break;
+      case 4: k_pivot_dots<4><<<pb, 256, 0, st>>>(L); break;
+      case 5: k_pivot_dots<5><<<pb, 256, 0, st>>>(L); break;
+      case 6: k_pivot_dots<6><<<pb, 256, 0, st>>>(L); break;
+      default: k_pivot_dots<7><<<pb, 256, 0, st>>>(L); break;
+    }
+  }
   switch (L.kp.kmer_size) {
     case 3: k_screen<3><<<blocks, kScreenWarps * 32, 0, st>>>(L); break;
     case 4: k_screen<4><<<blocks, kScreenWarps * 32, 0, st>>>(L); break;

@@ -1,10 +1,11 @@
 """Autotuner of the compare step's launch shape, per read-length class.
 
 The reference schedules its compare map on rayon with one knob, the grain
-DADA2_RS_PAR_GRAIN (src/cluster.rs:19-28). Here the launch shape has six
+DADA2_RS_PAR_GRAIN (src/cluster.rs:19-28). Here the launch shape has seven
 knobs (include/dada2_b200.h, dgpu_tuning): concurrent launch slots, samples
 per launch, slots dedicated to the longest chains, resident alignment CTAs
-per SM (pairs in flight), the screen's largest chunk and its blocks per SM.
+per SM (pairs in flight), the screen's largest chunk and its blocks per SM,
+and the launch size from which the screen's pivot bound runs.
 Their best values depend on read length: short reads give many cheap
 compare calls, long reads few expensive alignments.
 
@@ -39,6 +40,7 @@ SPACE = {
     "align_ctas_per_sm": [2, 3, 4],
     "screen_chunk_max": [16, 32],
     "screen_blocks_per_sm": [2, 3, 4],
+    "pivot_min_items": [0, 8192, 32768, 131072],
 }
 
 # representative read length of each class

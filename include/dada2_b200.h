@@ -233,6 +233,9 @@ int dgpu_cache_release(int device, uint64_t* freed);
  * align_ctas_per_sm    resident CTAs of the alignment kernel per SM (4 pairs each), 1..4
  * screen_chunk_max     largest run of (center, unique) items one screen warp takes, 16 or 32
  * screen_blocks_per_sm screen blocks per SM in its single wave, 1..4
+ * pivot_min_items      compare launches of at least this many (center, unique) items
+ *                      exclude far uniques by the exact pivot bound without reading
+ *                      their k-mer profiles (one extra small kernel); 0 = never
  * The library loads DGPU_TUNING_FILE, else tuning.txt beside itself, at first
  * use (the autotuner, dada2_b200/autotune.py, writes that file); the
  * DGPU_LAUNCH_SLOTS, DGPU_BATCH_MAX and DGPU_DEDICATED_SLOTS environment
@@ -241,7 +244,7 @@ int dgpu_cache_release(int device, uint64_t* freed);
  * the rayon grain DADA2_RS_PAR_GRAIN (src/cluster.rs:19-28). */
 typedef struct {
   int32_t launch_slots, samples_per_launch, dedicated_slots, align_ctas_per_sm, screen_chunk_max,
-      screen_blocks_per_sm;
+      screen_blocks_per_sm, pivot_min_items;
 } dgpu_tuning;
 /* the setting a pool whose longest unique has max_len bases would use */
 int dgpu_tuning_get(int max_len, dgpu_tuning* out);
@@ -303,8 +306,9 @@ double dgpu_calc_pA(uint32_t reads, double e_reads, int prior);
 /* With lambda_fp32: [0] p-values priced from the FP32 lambda, [1] of those
  * repriced from the FP64 product (the fallback). Zero otherwise. */
 int dgpu_result_fp32_stats(const dgpu_result* res, uint64_t* out2);
-/* Decision margins of the run: out3[0] the smallest |p - omega_a| / omega_a
- * over the bud's tests of p * nraw against omega_a, out3[1] the same for the
+/* Decision margins of the run: out3[0] the smallest |p - omega_a| /
+ * min(p, omega_a) over the bud's tests of p * nraw against omega_a (+inf for
+ * p = 0), out3[1] the same for the
  * prior raw's p against omega_p (both src/cluster.rs:1501-1640), out3[2] for
  * the final map's p against omega_c (src/dada.rs:525-533); +inf where no
  * such test ran. A margin far above 1e-12 shows that p-values differing by a
