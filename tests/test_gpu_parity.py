@@ -275,10 +275,16 @@ def test_dada_config2_full_size_matches_oracle():
 
 @pytest.fixture(scope="module")
 def config3_prefix():
+    import os
+
     w = synth.config3(seed=1003)
     s = w.samples[0]
     n = 30000
-    return w, synth.Sample(s.seqs[:n], np.asarray(s.abund[:n]), s.quals[:n], 0, name="config3[:30000]")
+    sub = synth.Sample(s.seqs[:n], np.asarray(s.abund[:n]), s.quals[:n], 0, name="config3[:30000]")
+    op = O.DadaParams(align=O.AlignParams(band=w.band, homo_gap_p=w.homo_gap_p, kmer_size=w.kmer_size),
+                      nthreads=max(2, os.cpu_count() or 2))
+    want = O.dada(sub.seqs, sub.abund, w.err, w.ncol, op, quals=sub.quals)
+    return w, sub, want
 
 
 def test_dada_config3_pooled_prefix_matches_oracle(config3_prefix):
@@ -286,13 +292,8 @@ def test_dada_config3_pooled_prefix_matches_oracle(config3_prefix):
     variants x 150 nt): its first 30,000 pooled uniques as one sample --
     about 2,700 clusters -- equal the oracle's run_dada bit for bit, with
     FP64 lambda and with decisions from the FP32 log-sum lambda."""
-    import os
-
-    w, s = config3_prefix
-    op = O.DadaParams(align=O.AlignParams(band=w.band, homo_gap_p=w.homo_gap_p, kmer_size=w.kmer_size),
-                      nthreads=max(2, os.cpu_count() or 2))
+    w, s, want = config3_prefix
     dp = D.DadaParams(align=D.AlignParams(band=w.band, homo_gap_p=w.homo_gap_p, kmer_size=w.kmer_size))
-    want = O.dada(s.seqs, s.abund, w.err, w.ncol, op, quals=s.quals)
     got = D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, dp, quals=s.quals)
     assert want["nclust"] > 1000
     assert_same_dada(got, want)
@@ -300,6 +301,30 @@ def test_dada_config3_pooled_prefix_matches_oracle(config3_prefix):
     got32 = D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, dp32, quals=s.quals)
     assert got32["nclust"] == want["nclust"]
     assert np.array_equal(got32["map"], want["map"])
+
+
+def test_pivot_bound_excludes_profiles_and_keeps_results(config3_prefix):
+    """The screen's pivot bound (a far unique is shrouded from its best dot
+    with an earlier center, without reading its profile) forced on for every
+    compare launch: the run still equals the oracle's bit for bit, counters
+    included, and it read fewer profile bytes than the run without it."""
+    w, s, want = config3_prefix
+    dp = D.DadaParams(align=D.AlignParams(band=w.band, homo_gap_p=w.homo_gap_p, kmer_size=w.kmer_size))
+    keep = D.tuning_get(150)
+    try:
+        D.tuning_set(0, {**keep, "pivot_min_items": 0})
+        D.stats_reset()
+        off = D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, dp, quals=s.quals)
+        bytes_off = D.stats_read()["screen_bytes"]
+        D.tuning_set(0, {**keep, "pivot_min_items": 1})
+        D.stats_reset()
+        on = D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, dp, quals=s.quals)
+        bytes_on = D.stats_read()["screen_bytes"]
+    finally:
+        D.tuning_set(0, keep)
+    assert_same_dada(off, want)
+    assert_same_dada(on, want)
+    assert bytes_on < 0.5 * bytes_off, (bytes_on, bytes_off)
 
 
 def test_dada_batch_matches_per_sample_oracle():
