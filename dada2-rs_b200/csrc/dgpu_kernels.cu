@@ -15,6 +15,7 @@
 // exactly like the reference's separately-rounded operations.
 #include <atomic>
 #include <algorithm>
+#include <type_traits>
 #include <cfloat>
 #include <cstdio>
 #include <mutex>
@@ -1398,7 +1399,22 @@ __device__ bool vec_align_fast(int lane, int len1, int len2, int match, int mism
         sc1[m] = x == y ? match : (((x | y) & 0x30u) ? fill : mismatch);
       }
       int r0 = row0;
-      for (;;) {
+      // The pairs stay in the middle regime while r0 + 1 <= last,
+      // A - cmE + band_mod2 < len1 - 1, (r0 + 1) / 2 + cxE - start_col < len2
+      // and (r0 + 2) / 2 + cxO - start_col < len2. With r0 (even) rising by 2
+      // and A by 1 per pair each test is linear in the pair count, so the
+      // count is fixed here and the loop carries no data-dependent exit.
+      int npairs;
+      {
+        auto fdiv2 = [](int x) { return x >= 0 ? x / 2 : -((1 - x) / 2); };  // floor(x / 2)
+        const int h = r0 / 2;
+        int k = fdiv2(last - 1 - r0);
+        k = min(k, len1 - 2 - A + cmE - band_mod2);
+        k = min(k, len2 - cxE + start_col - 1 - h);
+        k = min(k, len2 - cxO + start_col - 2 - h);
+        npairs = 1 + max(k, 0);
+      }
+      for (int pr = 0; pr < npairs; ++pr) {
         // Scores two rows ahead: over a pair A and B each rise by one, so the
         // loads for rows r0+2 / r0+3 go out while rows r0 / r0+1 are computed.
         int sc2[M], sc3[M];
@@ -1482,10 +1498,6 @@ __device__ bool vec_align_fast(int lane, int len1, int len2, int match, int mism
           sc[m] = sc2[m];
           sc1[m] = sc3[m];
         }
-        // the next pair stays in the middle regime (same tests as above)
-        if (!(r0 + 1 <= last && A - cmE + band_mod2 < len1 - 1 && (r0 + 1) / 2 + cxE - start_col < len2 &&
-              (r0 + 2) / 2 + cxO - start_col < len2))
-          break;
       }
       col_min = cmE;
       col_max = cxE;
@@ -1862,17 +1874,19 @@ __device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8
 #pragma unroll
   for (int m = 0; m < 2 * K; ++m) pw[m] = 0;
   const int tmax = len1 + len2;
-  for (int t = 0; t <= tmax; ++t) {
+  // One anti-diagonal; PAR = (t - o_lo) & 1 is a template argument, so the
+  // loop below runs two anti-diagonals per iteration with no branch on it.
+  auto diag = [&](int t, auto par_tag) {
+    constexpr int PAR = decltype(par_tag)::value;
     Cost nxt[K];
 #pragma unroll
     for (int m = 0; m < K; ++m) nxt[m] = cost_at(t + 1, m);  // past tmax: unused
-    const int par = (t - o_lo) & 1;
 #pragma unroll
     for (int m = 0; m < K; ++m) {
       const int q = lane + 32 * m;
-      const int own = par ? vo[m] : ve[m];
+      const int own = PAR ? vo[m] : ve[m];
       int left_nb, up_nb;
-      if (par == 0) {
+      if (PAR == 0) {
         const int a = __shfl_up_sync(FULL, vo[m], 1);
         const int a31 = (m > 0) ? __shfl_sync(FULL, vo[m > 0 ? m - 1 : 0], 31) : kNegSentinel;
         left_nb = (lane == 0) ? a31 : a;
@@ -1896,7 +1910,7 @@ __device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8
         val = cur[m].kind == 2u ? 0 : kNegSentinel;
         code = 0u;
       }
-      if (par) vo[m] = val;
+      if (PAR) vo[m] = val;
       else ve[m] = val;
       const uint32_t b0w = __ballot_sync(FULL, code & 1u);
       const uint32_t b1w = __ballot_sync(FULL, code & 2u);
@@ -1915,6 +1929,19 @@ __device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8
     }
 #pragma unroll
     for (int m = 0; m < K; ++m) cur[m] = nxt[m];
+  };
+  using Even = std::integral_constant<int, 0>;
+  using Odd = std::integral_constant<int, 1>;
+  if ((o_lo & 1) == 0) {  // t = 0 has parity 0
+    for (int t = 0; t <= tmax; t += 2) {
+      diag(t, Even{});
+      if (t + 1 <= tmax) diag(t + 1, Odd{});
+    }
+  } else {
+    for (int t = 0; t <= tmax; t += 2) {
+      diag(t, Odd{});
+      if (t + 1 <= tmax) diag(t + 1, Even{});
+    }
   }
   __syncwarp();
   // Traceback (src/nwalign.rs:234-273): row 0 moves left, column 0 moves up.
