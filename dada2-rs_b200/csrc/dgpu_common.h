@@ -201,6 +201,7 @@ struct FinalSubsLaunch {
   int tncol;      // columns counted (the error matrix's, or 1 without qualities)
   int has_quals;  // count at the raw's quality (else column 0)
   uint32_t* out;
+  unsigned long long* out64;  // non-null: counts go here (64-bit) instead of out
   uint32_t* err_word;
 };
 void launch_final_subs(const FinalSubsLaunch& F, cudaStream_t st);

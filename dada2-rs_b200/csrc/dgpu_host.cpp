@@ -2930,6 +2930,7 @@ struct Batch {
   dgpu_align_params align{};
   int host_threads = 1;
   bool transitions = false;  // run the final-subs pass after the loop
+  int learn_nq = 0;          // > 0: that pass counts build_trans_mat's matrix (learn-errors)
   int ncol_in = 0;           // the caller's error-matrix width (before extension)
   ~Batch() {  // Pool::upload waited for its copies, so the staging blocks are idle
     seq_h.recycle();
@@ -3041,19 +3042,28 @@ static int final_subs(Batch& B, std::vector<SampleState>& S, dgpu_result** out) 
     }
   }
   const bool has_q = B.E.qual != nullptr;
-  const int tncol = has_q ? P.kp.ncol : 1;
+  // learn-errors (build_trans_mat, src/learn_errors.rs:618-738) counts every
+  // sample at one width nq = the largest rounded quality + 1, so no quality
+  // is clamped, and saturates each sample's counts at u32; without qualities
+  // it counts nothing
+  const bool learn = B.learn_nq > 0;
+  if (learn && !has_q) raw.clear();
+  const int tncol = learn ? B.learn_nq : (has_q ? P.kp.ncol : 1);
   const size_t nbins = size_t(16) * size_t(tncol);
   const uint32_t nitems = uint32_t(raw.size());
   DBuf<uint32_t> items, counts, err;
+  DBuf<unsigned long long> counts64;
   TRY(items.alloc(size_t(3) * std::max<uint32_t>(nitems, 1)));
-  TRY(counts.alloc(ns * nbins));
+  TRY(counts.alloc(learn ? 1 : ns * nbins));
+  if (learn) TRY(counts64.alloc(ns * nbins));
   TRY(err.alloc(1));
   CUDA_TRY(cudaMemcpyAsync(items.p, raw.data(), size_t(4) * nitems, cudaMemcpyHostToDevice, P.st));
   CUDA_TRY(cudaMemcpyAsync(items.p + nitems, center.data(), size_t(4) * nitems, cudaMemcpyHostToDevice, P.st));
   CUDA_TRY(cudaMemcpyAsync(items.p + 2 * size_t(nitems), sample.data(), size_t(4) * nitems, cudaMemcpyHostToDevice,
                            P.st));
   count_h2d(uint64_t(12) * nitems);
-  CUDA_TRY(cudaMemsetAsync(counts.p, 0, ns * nbins * 4, P.st));
+  if (learn) CUDA_TRY(cudaMemsetAsync(counts64.p, 0, ns * nbins * 8, P.st));
+  else CUDA_TRY(cudaMemsetAsync(counts.p, 0, ns * nbins * 4, P.st));
   CUDA_TRY(cudaMemsetAsync(err.p, 0, 4, P.st));
   FinalSubsLaunch F{};
   F.pool = P.view();
@@ -3068,16 +3078,31 @@ static int final_subs(Batch& B, std::vector<SampleState>& S, dgpu_result** out) 
   F.tncol = tncol;
   F.has_quals = has_q ? 1 : 0;
   F.out = counts.p;
+  F.out64 = learn ? counts64.p : nullptr;
   F.err_word = err.p;
   launch_final_subs(F, P.st);
   CUDA_TRY(cudaGetLastError());
   std::vector<uint32_t> host(ns * nbins);
+  std::vector<unsigned long long> host64(learn ? ns * nbins : 0);
   uint32_t ew = 0;
-  CUDA_TRY(cudaMemcpyAsync(host.data(), counts.p, host.size() * 4, cudaMemcpyDeviceToHost, P.st));
+  if (learn)
+    CUDA_TRY(cudaMemcpyAsync(host64.data(), counts64.p, host64.size() * 8, cudaMemcpyDeviceToHost, P.st));
+  else
+    CUDA_TRY(cudaMemcpyAsync(host.data(), counts.p, host.size() * 4, cudaMemcpyDeviceToHost, P.st));
   CUDA_TRY(cudaMemcpyAsync(&ew, err.p, 4, cudaMemcpyDeviceToHost, P.st));
   CUDA_TRY(cudaStreamSynchronize(P.st));
-  recycle_all(items, counts, err);
+  recycle_all(items, counts, counts64, err);
   if (ew) return fail(ew & DERR_UNSUPPORTED ? DGPU_E_UNSUPPORTED : DGPU_E_DEVICE, "device error in the final-subs pass");
+  if (learn) {
+    for (size_t s = 0; s < ns; ++s) {
+      dgpu_result* R = out[s];
+      R->tncol = tncol;
+      R->transitions.resize(nbins);
+      for (size_t b = 0; b < nbins; ++b)
+        R->transitions[b] = uint32_t(std::min<unsigned long long>(host64[s * nbins + b], 0xffffffffull));
+    }
+    return 0;
+  }
   for (size_t s = 0; s < ns; ++s) {
     int nc = 1;
     if (has_q) {
@@ -3364,6 +3389,45 @@ struct dgpu_ctx {
 
 using namespace dgpu;
 
+struct dgpu_learn {
+  int32_t nq = 0, passes = 0, converged = 0;
+  std::vector<uint32_t> trans;
+  std::vector<double> err_in, err_out;
+};
+
+namespace dgpu {
+int errfun_apply(const dgpu_errfun& ef, const uint32_t* trans, int nq, double* err, std::string* msg);
+
+// One learn-errors pass over the prepared samples: denoise them all with
+// `err` (16 x nq) and at most max_clust clusters each (0: the parameters'
+// own), count each sample's transitions as build_trans_mat does and sum them
+// (accumulate_trans, src/error_models.rs:495-515, wrapping u32 additions).
+static int learn_pass(Batch& B, const std::vector<double>& err, size_t max_clust, int nq,
+                      std::vector<uint32_t>& acc) {
+  Pool& P = B.pool;
+  CUDA_TRY(cudaSetDevice(P.device));
+  CUDA_TRY(cudaMemcpy(P.err.p, err.data(), err.size() * 8, cudaMemcpyHostToDevice));
+  count_h2d(err.size() * 8);
+  const size_t ns = B.counts.size();
+  std::vector<size_t> keep(ns);
+  for (size_t s = 0; s < ns; ++s) {
+    keep[s] = B.confs[s].max_clust;
+    if (max_clust) B.confs[s].max_clust = max_clust;
+  }
+  std::vector<dgpu_result*> res(ns, nullptr);
+  const int rc = batch_run(B, res.data());
+  for (size_t s = 0; s < ns; ++s) B.confs[s].max_clust = keep[s];
+  acc.assign(size_t(16) * nq, 0u);
+  for (dgpu_result* R : res) {
+    if (!R) continue;
+    if (!rc && R->transitions.size() == acc.size())
+      for (size_t b = 0; b < acc.size(); ++b) acc[b] += R->transitions[b];
+    dgpu_result_free(R);
+  }
+  return rc;
+}
+}  // namespace dgpu
+
 extern "C" {
 
 const char* dgpu_last_error(void) { return g_err.c_str(); }
@@ -3618,6 +3682,86 @@ int dgpu_dada_batch(int device, const dgpu_dada_params* params, int nsamples, co
                     ncol));
   return batch_run(b.b, out);
 }
+
+int dgpu_learn_errors(int device, const dgpu_dada_params* params, const dgpu_errfun* errfun, int max_consist,
+                      int nsamples, const uint32_t* sample_start, const char* seqs, const uint32_t* offs,
+                      const uint32_t* lens, const uint32_t* abund, const uint32_t* qual_sums, dgpu_learn** out) {
+  using namespace dgpu;
+  if (!out || !params || !errfun || max_consist < 0 || nsamples <= 0 || !sample_start || !lens || !abund)
+    return fail(DGPU_E_INVALID, "bad argument");
+  if (!qual_sums) return fail(DGPU_E_INVALID, "learn-errors needs quality sums: without them no transition is counted");
+  *out = nullptr;
+  // nq: the largest round(sum / reads) over every position of every sample,
+  // plus one (src/learn_errors.rs:494-506)
+  uint32_t qmax = 0;
+  for (uint32_t t = sample_start[0]; t < sample_start[nsamples]; ++t) {
+    const double ab = double(abund[t]);
+    for (uint32_t p = 0; p < lens[t]; ++p) {
+      const double q = std::round(double(qual_sums[size_t(offs[t]) + p]) / ab);
+      if (q > double(qmax)) qmax = uint32_t(std::min(q, 1e9));
+    }
+  }
+  const int nq = int(qmax) + 1;
+  std::vector<double> err(size_t(16) * nq, 1.0);  // the init pass: every entry 1 (src/learn_errors.rs:536-540)
+  dgpu_dada_params prm = *params;
+  prm.transitions = 1;
+  prm.lambda_fp32 = 0;
+  dgpu_batch b;
+  TRY(batch_prepare(b.b, device, &prm, nsamples, sample_start, seqs, offs, lens, abund, nullptr, qual_sums, err.data(),
+                    nq));
+  Batch& B = b.b;
+  B.learn_nq = nq;
+  std::unique_ptr<dgpu_learn> L(new dgpu_learn());
+  L->nq = nq;
+  std::vector<uint32_t> acc;
+  std::string msg;
+  // init pass: one cluster per sample, fit, diagonals forced to 1
+  TRY(learn_pass(B, err, 1, nq, acc));
+  std::vector<double> fit(size_t(16) * nq);
+  if (int rc = errfun_apply(*errfun, acc.data(), nq, fit.data(), &msg)) return fail(rc, "init-pass errfun failed: " + msg);
+  for (int r : {0, 5, 10, 15})
+    for (int q = 0; q < nq; ++q) fit[size_t(r) * nq + q] = 1.0;
+  err = fit;
+  L->trans.assign(size_t(16) * nq, 0u);
+  L->err_in = err;
+  L->err_out = err;
+  std::vector<std::vector<double>> history;
+  for (int it = 0; it < max_consist; ++it) {
+    L->passes = it + 1;
+    history.push_back(err);
+    TRY(learn_pass(B, err, 0, nq, acc));
+    if (int rc = errfun_apply(*errfun, acc.data(), nq, fit.data(), &msg)) return fail(rc, "errfun failed: " + msg);
+    // converged when the fit equals (as f64 values) a matrix already used
+    // as input (src/learn_errors.rs:962-967)
+    bool conv = false;
+    for (const auto& h : history) conv |= h == fit;
+    L->err_in = err;
+    L->trans = acc;
+    L->err_out = fit;
+    if (conv) {
+      L->converged = 1;
+      break;
+    }
+    err = fit;
+  }
+  *out = L.release();
+  return 0;
+}
+
+int dgpu_learn_read(const dgpu_learn* l, int32_t* info, uint32_t* trans, double* err_in, double* err_out) {
+  if (!l) return dgpu::fail(DGPU_E_INVALID, "null argument");
+  if (info) {
+    info[0] = l->nq;
+    info[1] = l->passes;
+    info[2] = l->converged;
+  }
+  if (trans) std::copy(l->trans.begin(), l->trans.end(), trans);
+  if (err_in) std::copy(l->err_in.begin(), l->err_in.end(), err_in);
+  if (err_out) std::copy(l->err_out.begin(), l->err_out.end(), err_out);
+  return 0;
+}
+
+void dgpu_learn_free(dgpu_learn* l) { delete l; }
 
 int dgpu_cache_release(int device, uint64_t* freed) {
   const size_t n = cache_release(device);

@@ -2244,30 +2244,43 @@ __global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_final_subs(F
   auto flush = [&]() {
     __syncwarp();
     if (cur_s != 0xffffffffu) {
-      uint32_t* dst = F.out + size_t(cur_s) * nbins;
       for (int b = lane; b < nbins; b += 32) {
         const uint32_t v = hist[b];
-        if (v) atomicAdd(dst + b, v);
+        if (v) {
+          if (F.out64) atomicAdd(F.out64 + size_t(cur_s) * nbins + b, static_cast<unsigned long long>(v));
+          else atomicAdd(F.out + size_t(cur_s) * nbins + b, v);
+        }
         hist[b] = 0;
       }
     }
     __syncwarp();
   };
+  uint64_t bound = 0;  // what the shared bins may hold since the last flush
   for (uint32_t i = i0; i < i1; ++i) {
     const uint32_t g = F.raw[i], c = F.center[i], smp = F.sample[i];
-    if (smp != cur_s) {
+    // a raw adds at most reads x length to one bin: flush before a 32-bit
+    // shared bin could wrap (a raw that could wrap one alone counts in global
+    // memory directly)
+    const uint64_t add = uint64_t(F.pool.reads[g]) * F.pool.len[g];
+    if (smp != cur_s || bound + add > 0xffffffffull) {
       flush();
       cur_s = smp;
+      bound = 0;
     }
+    bound += add;
     const PairResult R = align_pair(lane, kp, F.pool, F.geom, g, c, 0.0, F.has_quals != 0, VS, RS, kb, scratch,
                                     F.err_word);
     if (!R.ok) continue;  // the error word reports it
     const uint32_t reads = F.pool.reads[g];
+    const bool direct = add > 0xffffffffull;  // alone it could wrap a 32-bit bin: count in global memory
     for (int p = lane; p < R.lg; p += 32) {
       const unsigned t = R.tcode[p];
       if (t > 15u) continue;  // an insertion in the raw (or an invalid code)
       const unsigned q = (F.has_quals && R.qual) ? R.qual[p] : 0u;
-      if (q < unsigned(F.tncol)) atomicAdd(&hist[t * F.tncol + q], reads);
+      if (q >= unsigned(F.tncol)) continue;
+      if (!direct) atomicAdd(&hist[t * F.tncol + q], reads);
+      else if (F.out64) atomicAdd(F.out64 + size_t(smp) * nbins + t * F.tncol + q, static_cast<unsigned long long>(reads));
+      else atomicAdd(F.out + size_t(smp) * nbins + t * F.tncol + q, reads);
     }
     __syncwarp();
   }

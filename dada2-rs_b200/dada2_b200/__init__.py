@@ -20,13 +20,14 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from ._lib import (AlignParamsC, CountersC, DadaOutC, DadaParamsC, DgpuError, InvalidInput, KernelStatsC,
+from ._lib import (AlignParamsC, CountersC, DadaOutC, DadaParamsC, DgpuError, ErrFunC, InvalidInput, KernelStatsC,
                    TuningC, check, device_count, lib, ptr)
 
 __all__ = ["AlignParams", "DadaParams", "CompareContext", "dada_uniques", "dada_uniques_batch", "dada_uniques_sharded",
            "ResidentBatch", "PackedBatch", "DenoiseService", "pack_sample", "Derep", "derep_fastq", "dada_fastq", "align_pairs", "stats_reset", "stats_timing", "stats_read",
            "DgpuError", "InvalidInput", "device_count", "METHOD_NAMES", "KERNEL_NAMES", "TUNING_KEYS",
-           "tuning_get", "tuning_set", "tuning_load", "tuning_save", "tuning_reset", "length_class"]
+           "tuning_get", "tuning_set", "tuning_load", "tuning_save", "tuning_reset", "length_class",
+           "ErrFun", "errfun_apply", "learn_errors"]
 
 KERNEL_NAMES = ["profiles", "screen", "align", "store"]
 
@@ -568,6 +569,67 @@ def cache_release(device: int = -1) -> int:
     n = C.c_uint64(0)
     check(lib().dgpu_cache_release(int(device), C.byref(n)))
     return int(n.value)
+
+
+@dataclass
+class ErrFun:
+    """The error-model fit of learn-errors (src/learn_errors.rs:67-100):
+    kind "loess" (surface "direct", the dada2-rs default, or "interpolate"
+    with ``cell``, R's default) or "noqual" (``pseudocount``); off-diagonal
+    rates clamped to [min_error_rate, max_error_rate]."""
+    kind: str = "loess"
+    surface: str = "direct"
+    cell: float = 0.2
+    max_error_rate: float = 0.25
+    min_error_rate: float = 1e-7
+    pseudocount: float = 1.0
+
+    def c(self) -> ErrFunC:
+        kinds = {"loess": 0, "noqual": 1}
+        surfaces = {"direct": 0, "interpolate": 1}
+        return ErrFunC(kinds[self.kind], surfaces[self.surface], float(self.cell), float(self.max_error_rate),
+                       float(self.min_error_rate), float(self.pseudocount))
+
+
+def errfun_apply(trans, nq: int, errfun: ErrFun | None = None) -> np.ndarray:
+    """The 16 x nq error-rate matrix fitted to a 16 x nq transition matrix (host)."""
+    t = np.ascontiguousarray(trans, np.uint32).reshape(-1)
+    out = np.zeros(16 * nq, np.float64)
+    ef = (errfun or ErrFun()).c()
+    check(lib().dgpu_errfun_apply(C.byref(ef), ptr(t), int(nq), ptr(out)))
+    return out.reshape(16, nq)
+
+
+def learn_errors(samples, params: DadaParams | None = None, errfun: ErrFun | None = None, max_consist: int = 10,
+                 device: int = 0) -> dict:
+    """learn_errors (src/learn_errors.rs:739-1020): the self-consistent error
+    model of the samples (objects with .seqs, .abund and .quals as Phred
+    sums). Every pass denoises all samples together on the device and counts
+    their transitions there. Returns nq, passes, converged and the last pass's
+    trans, err_in and err_out (16 x nq)."""
+    params = params or DadaParams()
+    seqs = [q for s in samples for q in s.seqs]
+    abund = np.concatenate([np.asarray(s.abund, np.uint32) for s in samples])
+    quals = [q for s in samples for q in s.quals]
+    cat, offs, lens, ab, qcat, _ = _pack(seqs, abund, quals, None)
+    start = np.concatenate([[0], np.cumsum([len(s.seqs) for s in samples])]).astype(np.uint32)
+    pc = params.c()
+    ef = (errfun or ErrFun()).c()
+    h = C.c_void_p()
+    check(lib().dgpu_learn_errors(int(device), C.byref(pc), C.byref(ef), int(max_consist), len(samples), ptr(start),
+                                  ptr(cat), ptr(offs), ptr(lens), ptr(ab), ptr(qcat), C.byref(h)))
+    try:
+        info = np.zeros(3, np.int32)
+        check(lib().dgpu_learn_read(h, ptr(info), None, None, None))
+        nq = int(info[0])
+        tr = np.zeros(16 * nq, np.uint32)
+        ei = np.zeros(16 * nq, np.float64)
+        eo = np.zeros(16 * nq, np.float64)
+        check(lib().dgpu_learn_read(h, ptr(info), ptr(tr), ptr(ei), ptr(eo)))
+        return {"nq": nq, "passes": int(info[1]), "converged": bool(info[2]), "trans": tr.reshape(16, nq),
+                "err_in": ei.reshape(16, nq), "err_out": eo.reshape(16, nq)}
+    finally:
+        lib().dgpu_learn_free(h)
 
 
 TUNING_KEYS = [n for n, _ in TuningC._fields_]

@@ -61,6 +61,11 @@ class TuningC(C.Structure):
                                          "pivot_min_items")]
 
 
+class ErrFunC(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("surface", C.c_int32), ("cell", C.c_double),
+                ("max_error_rate", C.c_double), ("min_error_rate", C.c_double), ("pseudocount", C.c_double)]
+
+
 class CountersC(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("screened", "aligned", "shrouded", "stored", "gapless",
                                           "vectorized", "homo", "endsfree")]
@@ -109,6 +114,12 @@ def lib():
         L.dgpu_result_transitions.argtypes = [_P, _P]
         L.dgpu_result_fp32_stats.argtypes = [_P, _P]
         L.dgpu_result_margins.argtypes = [_P, _P]
+        L.dgpu_errfun_apply.argtypes = [C.POINTER(ErrFunC), _P, C.c_int, _P]
+        L.dgpu_learn_errors.argtypes = [C.c_int, C.POINTER(DadaParamsC), C.POINTER(ErrFunC), C.c_int, C.c_int, _P, _P,
+                                        _P, _P, _P, _P, C.POINTER(_P)]
+        L.dgpu_learn_read.argtypes = [_P, _P, _P, _P, _P]
+        L.dgpu_learn_free.argtypes = [_P]
+        L.dgpu_learn_free.restype = None
         L.dgpu_tuning_get.argtypes = [C.c_int, C.POINTER(TuningC)]
         L.dgpu_tuning_set.argtypes = [C.c_int, C.POINTER(TuningC)]
         L.dgpu_tuning_load.argtypes = [C.c_char_p]

@@ -316,6 +316,55 @@ int dgpu_result_fp32_stats(const dgpu_result* res, uint64_t* out2);
  * reference (a diagnostic of this implementation). */
 int dgpu_result_margins(const dgpu_result* res, double* out3);
 
+/* ---- learn-errors ----
+ * The error-model fit applied to an accumulated 16 x nq transition matrix
+ * (row 4 * ref nt + query nt, column = quality score):
+ *   DGPU_ERRFUN_LOESS   loess_errfun (src/error_models.rs:119-210): per
+ *                       off-diagonal transition, LOESS (span 0.75, degree 2)
+ *                       of log10((count + 1) / total of the source nucleotide)
+ *                       on the quality score weighted by that total, surface
+ *                       0 direct (the dada2-rs default) or 1 kd-tree
+ *                       interpolation with `cell` (R's default, 0.2), flat
+ *                       extrapolation, rates clamped to [min, max]
+ *   DGPU_ERRFUN_NOQUAL  noqual_errfun (src/error_models.rs:212-261): one
+ *                       rate per transition from counts summed over
+ *                       qualities plus `pseudocount`
+ * The diagonal of each nucleotide is 1 minus its three off-diagonals. */
+#define DGPU_ERRFUN_LOESS 0
+#define DGPU_ERRFUN_NOQUAL 1
+typedef struct {
+  int32_t kind;
+  int32_t surface;  /* LOESS: 0 direct, 1 interpolate */
+  double cell;      /* LOESS interpolate: kd-tree cell fraction (0.2) */
+  double max_error_rate, min_error_rate;  /* clamp of the off-diagonal rates (0.25, 1e-7) */
+  double pseudocount;                     /* NOQUAL (1.0) */
+} dgpu_errfun;
+/* err_out (16 x nq) = the fit of trans (16 x nq). Host only. */
+int dgpu_errfun_apply(const dgpu_errfun* ef, const uint32_t* trans, int nq, double* err_out);
+
+/* learn_errors (src/learn_errors.rs:739-1010): the self-consistent loop that
+ * estimates the error model from samples. nq = the largest rounded mean
+ * quality + 1 (src/learn_errors.rs:494-506). An init pass denoises every
+ * sample with an all-ones error matrix and at most one cluster, counts
+ * transitions, fits and forces the diagonal to 1 (src/learn_errors.rs:525-616);
+ * then up to max_consist passes denoise all samples with the current matrix
+ * (the batched GPU path), count each sample's transitions by realigning every
+ * corrected unique to its center (build_trans_mat, src/learn_errors.rs:618-738;
+ * counted on the device), sum them, fit, and stop once the fit equals bit for
+ * bit any matrix used as input so far. Samples as in dgpu_dada_batch;
+ * qual_sums are required (without qualities no transition is counted). The
+ * dada parameters' error matrix is the loop's own. */
+typedef struct dgpu_learn dgpu_learn;
+int dgpu_learn_errors(int device, const dgpu_dada_params* params, const dgpu_errfun* errfun, int max_consist,
+                      int nsamples, const uint32_t* sample_start, const char* seqs, const uint32_t* offs,
+                      const uint32_t* lens, const uint32_t* abund, const uint32_t* qual_sums, dgpu_learn** out);
+/* info[0] nq, [1] passes run (init pass excluded), [2] converged (0/1);
+ * trans (16 x nq, may be NULL): the last pass's summed transitions; err_in /
+ * err_out (16 x nq doubles, may be NULL): the matrix that pass used and the
+ * fit of its transitions. */
+int dgpu_learn_read(const dgpu_learn* l, int32_t* info, uint32_t* trans, double* err_in, double* err_out);
+void dgpu_learn_free(dgpu_learn* l);
+
 /* ---- ingest: FASTQ -> uniques ----
  * Dereplicates a FASTQ file (plain or gzip, four-line records) as
  * dereplicate does (src/derep.rs:43-240, ordering src/derep.rs:179-185):

@@ -299,4 +299,25 @@ struct DadaResult {
 std::string dada_uniques(const std::vector<RawInput>& inputs, const DadaParams& params,
                          DadaResult& out);
 
+// ---- learn_errors.rs / error_models.rs / loess.rs (oracle_learn.cpp) ----
+struct ErrFunSpec {
+  int kind = 0;     // 0 loess, 1 noqual
+  int surface = 0;  // loess: 0 direct, 1 interpolate
+  double cell = 0.2;
+  double max_error_rate = 0.25, min_error_rate = 1e-7;
+  double pseudocount = 1.0;
+};
+struct LearnResult {
+  size_t nq = 0, passes = 0;
+  bool converged = false;
+  std::vector<uint32_t> trans;
+  std::vector<double> err_in, err_out;
+};
+std::string errfun_apply(const ErrFunSpec& e, const std::vector<uint32_t>& trans, size_t nq,
+                         std::vector<double>& err);
+std::vector<uint32_t> build_trans_mat(const std::vector<RawInput>& inputs, const DadaResult& res,
+                                      const AlignParams& ap, size_t nq);
+std::string learn_errors(const std::vector<std::vector<RawInput>>& samples, DadaParams params,
+                         const ErrFunSpec& ef, size_t max_consist, LearnResult& out);
+
 }  // namespace orc

@@ -22,8 +22,13 @@ METHOD_NAMES = {0: "none", 1: "gapless", 2: "vectorized", 3: "homo", 4: "endsfre
 
 
 def build(force: bool = False) -> str:
-    """Compile liboracle_dada.so with the committed Makefile."""
-    if force or not os.path.exists(_LIB_PATH):
+    """Compile liboracle_dada.so with the committed Makefile (make rebuilds it
+    only when a source is newer)."""
+    if force and os.path.exists(_LIB_PATH):
+        os.unlink(_LIB_PATH)
+    if force or not os.path.exists(_LIB_PATH) or any(
+            os.path.getmtime(os.path.join(_HERE, f)) > os.path.getmtime(_LIB_PATH)
+            for f in os.listdir(_HERE) if f.endswith((".cpp", ".hpp"))):
         subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return _LIB_PATH
 
@@ -45,6 +50,11 @@ class DadaParamsC(C.Structure):
         ("use_quals", C.c_int32), ("greedy", C.c_int32), ("nthreads", C.c_int32),
         ("transitions", C.c_int32),
     ]
+
+
+class ErrFunC(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("surface", C.c_int32), ("cell", C.c_double),
+                ("max_error_rate", C.c_double), ("min_error_rate", C.c_double), ("pseudocount", C.c_double)]
 
 
 _P = C.c_void_p
@@ -121,6 +131,12 @@ def lib():
                                            C.c_int, C.c_int, _P, _P, _P, _P]
         _lib.orc_c_b_compare.argtypes = [C.c_void_p, C.c_int, _P, C.c_int, C.POINTER(AlignParamsC),
                                          C.c_int, C.c_int, _P, _P, _P, _P, _P, _P]
+        _lib.orc_c_errfun_apply.restype = C.c_int
+        _lib.orc_c_errfun_apply.argtypes = [C.POINTER(ErrFunC), _P, C.c_int, _P, C.c_char_p, C.c_int]
+        _lib.orc_c_learn_errors.restype = C.c_int
+        _lib.orc_c_learn_errors.argtypes = [C.c_int, _P, _P, _P, _P, _P, _P, C.POINTER(DadaParamsC),
+                                            C.POINTER(ErrFunC), C.c_int, C.c_int, _P, _P, _P, _P, C.c_char_p,
+                                            C.c_int]
         _lib.orc_c_dada.restype = C.c_void_p
         _lib.orc_c_dada.argtypes = [C.c_int, _P, _P, _P, _P, _P, _P, C.POINTER(DadaParamsC), _P,
                                     C.c_int, C.c_char_p, C.c_int]
@@ -468,6 +484,52 @@ def dada(seqs, abund, err, ncol, params: DadaParams, quals=None, prior=None):
         return res
     finally:
         lib().orc_c_dada_free(h)
+
+
+ERRFUN_LOESS, ERRFUN_NOQUAL = 0, 1
+
+
+def errfun_c(kind=ERRFUN_LOESS, surface=0, cell=0.2, max_error_rate=0.25, min_error_rate=1e-7, pseudocount=1.0):
+    return ErrFunC(int(kind), int(surface), float(cell), float(max_error_rate), float(min_error_rate),
+                   float(pseudocount))
+
+
+def errfun_apply(trans, nq, **kw) -> np.ndarray:
+    """The error-model fit (loess_errfun / noqual_errfun) of a 16 x nq
+    transition matrix; raises ValueError when LOESS fails everywhere."""
+    t = np.ascontiguousarray(trans, np.uint32).reshape(-1)
+    out = np.zeros(16 * nq, np.float64)
+    eb = C.create_string_buffer(256)
+    ef = errfun_c(**kw)
+    if lib().orc_c_errfun_apply(C.byref(ef), _ptr(t), int(nq), _ptr(out), eb, 256) != 0:
+        raise ValueError(eb.value.decode())
+    return out.reshape(16, nq)
+
+
+def learn_errors(samples, params: DadaParams, max_consist=10, **errfun_kw) -> dict:
+    """learn_errors (src/learn_errors.rs:739-1020) over samples (objects with
+    .seqs, .abund, .quals as Phred sums)."""
+    seqs = [q for s in samples for q in s.seqs]
+    abund = np.concatenate([np.asarray(s.abund, np.uint32) for s in samples])
+    quals = [q for s in samples for q in s.quals]
+    cat, offs, lens, ab, qcat, _ = pack_inputs(seqs, abund, quals, None)
+    start = np.concatenate([[0], np.cumsum([len(s.seqs) for s in samples])]).astype(np.uint32)
+    pc = dada_params_c(params)
+    ef = errfun_c(**errfun_kw)
+    cap = 256
+    info = np.zeros(3, np.int32)
+    tr = np.zeros(16 * cap, np.uint32)
+    ei = np.zeros(16 * cap, np.float64)
+    eo = np.zeros(16 * cap, np.float64)
+    eb = C.create_string_buffer(512)
+    nq = lib().orc_c_learn_errors(len(samples), _ptr(start), _ptr(cat), _ptr(offs), _ptr(lens), _ptr(ab), _ptr(qcat),
+                                  C.byref(pc), C.byref(ef), int(max_consist), cap, _ptr(info), _ptr(tr), _ptr(ei),
+                                  _ptr(eo), eb, 512)
+    if nq < 0:
+        raise ValueError(eb.value.decode())
+    return {"nq": int(info[0]), "passes": int(info[1]), "converged": bool(info[2]),
+            "trans": tr[:16 * nq].reshape(16, nq).copy(), "err_in": ei[:16 * nq].reshape(16, nq).copy(),
+            "err_out": eo[:16 * nq].reshape(16, nq).copy()}
 
 
 def hardware_threads() -> int:

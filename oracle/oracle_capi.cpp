@@ -329,6 +329,86 @@ void* orc_c_dada(int nraw, const char* seqcat, const uint32_t* off, const uint32
 
 void orc_c_dada_free(void* h) { delete static_cast<OrcDada*>(h); }
 
+// ---------------- learn-errors (oracle_learn.cpp) ----------------
+struct orc_errfun {
+  int32_t kind, surface;
+  double cell, max_error_rate, min_error_rate, pseudocount;
+};
+static ErrFunSpec to_errfun(const orc_errfun* e) {
+  ErrFunSpec s;
+  s.kind = e->kind;
+  s.surface = e->surface;
+  s.cell = e->cell;
+  s.max_error_rate = e->max_error_rate;
+  s.min_error_rate = e->min_error_rate;
+  s.pseudocount = e->pseudocount;
+  return s;
+}
+int orc_c_errfun_apply(const orc_errfun* e, const uint32_t* trans, int nq, double* out, char* errbuf, int errcap) {
+  std::vector<uint32_t> t(trans, trans + 16 * size_t(nq));
+  std::vector<double> err;
+  const std::string m = errfun_apply(to_errfun(e), t, size_t(nq), err);
+  if (!m.empty()) {
+    if (errbuf && errcap > 0) {
+      std::strncpy(errbuf, m.c_str(), size_t(errcap - 1));
+      errbuf[errcap - 1] = 0;
+    }
+    return -1;
+  }
+  std::copy(err.begin(), err.end(), out);
+  return 0;
+}
+// Samples as in orc_c_dada, sample s owning uniques [start[s], start[s+1]).
+// info: [0] nq, [1] passes, [2] converged. trans/err_in/err_out need 16 x
+// nq_cap slots; returns nq, or -1 with the message in errbuf.
+int orc_c_learn_errors(int nsamples, const uint32_t* start, const char* seqcat, const uint32_t* off,
+                       const uint32_t* len, const uint32_t* abund, const uint32_t* qualcat, const orc_dada_params* pp,
+                       const orc_errfun* ef, int max_consist, int nq_cap, int32_t* info, uint32_t* trans,
+                       double* err_in, double* err_out, char* errbuf, int errcap) {
+  std::vector<std::vector<RawInput>> samples(static_cast<size_t>(nsamples));
+  for (int s = 0; s < nsamples; ++s)
+    for (uint32_t t = start[s]; t < start[s + 1]; ++t) {
+      RawInput r;
+      r.seq.assign(seqcat + off[t], seqcat + off[t] + len[t]);
+      r.abundance = abund[t];
+      if (qualcat) {
+        r.has_quals = true;
+        r.quals.assign(qualcat + off[t], qualcat + off[t] + len[t]);
+      }
+      samples[size_t(s)].push_back(std::move(r));
+    }
+  DadaParams dp;
+  dp.align = to_params(&pp->align);
+  dp.omega_a = pp->omega_a;
+  dp.omega_p = pp->omega_p;
+  dp.omega_c = pp->omega_c;
+  dp.detect_singletons = pp->detect_singletons != 0;
+  dp.max_clust = size_t(pp->max_clust);
+  dp.min_fold = pp->min_fold;
+  dp.min_hamming = pp->min_hamming;
+  dp.min_abund = pp->min_abund;
+  dp.use_quals = pp->use_quals != 0;
+  dp.greedy = pp->greedy != 0;
+  dp.nthreads = pp->nthreads;
+  LearnResult lr;
+  const std::string m = learn_errors(samples, dp, to_errfun(ef), size_t(max_consist), lr);
+  if (!m.empty() || int(lr.nq) > nq_cap) {
+    const std::string msg = m.empty() ? std::string("nq beyond nq_cap") : m;
+    if (errbuf && errcap > 0) {
+      std::strncpy(errbuf, msg.c_str(), size_t(errcap - 1));
+      errbuf[errcap - 1] = 0;
+    }
+    return -1;
+  }
+  info[0] = int32_t(lr.nq);
+  info[1] = int32_t(lr.passes);
+  info[2] = lr.converged ? 1 : 0;
+  std::copy(lr.trans.begin(), lr.trans.end(), trans);
+  std::copy(lr.err_in.begin(), lr.err_in.end(), err_in);
+  std::copy(lr.err_out.begin(), lr.err_out.end(), err_out);
+  return int(lr.nq);
+}
+
 // Transition counts of a run made with transitions set: returns the column
 // count and copies 16 x ncol values to out (when non-null); 0 if none.
 int orc_c_dada_transitions(void* h, uint32_t* out) {

@@ -701,6 +701,27 @@ def test_multi_device_service_matches_single_sample_calls():
         assert_same_dada(g, D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, D.DadaParams(), quals=s.quals))
 
 
+@pytest.mark.parametrize("kind,surface", [("loess", "direct"), ("loess", "interpolate"), ("noqual", "direct")])
+def test_learn_errors_matches_the_oracle(kind, surface):
+    """learn_errors (src/learn_errors.rs:739-1020) on three Illumina-style
+    samples: the init pass, every self-consistency pass (all samples denoised
+    together on the device, transitions counted there) and the fits give the
+    oracle's nq, pass count, convergence, summed transitions and input/output
+    error matrices bit for bit."""
+    ws = [synth.small_illumina(60 + i, nvariants=6 + 2 * i, nreads=3000 + 500 * i, L=150) for i in range(3)]
+    samples = [w.samples[0] for w in ws]
+    ef = D.ErrFun(kind=kind, surface=surface)
+    got = D.learn_errors(samples, D.DadaParams(), ef, max_consist=6)
+    want = O.learn_errors(samples, O.DadaParams(nthreads=8), max_consist=6, kind=0 if kind == "loess" else 1,
+                          surface=0 if surface == "direct" else 1)
+    assert (got["nq"], got["passes"], got["converged"]) == (want["nq"], want["passes"], want["converged"])
+    assert got["passes"] >= 1
+    assert np.array_equal(got["trans"], want["trans"])
+    assert got["trans"].sum() > 0
+    assert got["err_in"].tobytes() == want["err_in"].tobytes()
+    assert got["err_out"].tobytes() == want["err_out"].tobytes()
+
+
 @pytest.fixture(scope="module")
 def config1_full():
     return synth.config1(seed=1001)

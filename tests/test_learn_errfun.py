@@ -1,0 +1,107 @@
+"""Error-model fits of learn-errors (CPU only).
+
+The product's fit (dgpu_errfun_apply, host code in the library) and the
+oracle's restatement are each held to the reference's own errfun tests
+(src/error_models.rs tests: an empty matrix is an error, one populated
+quality column fits a constant (11 / 10,030), binned-quality schemes fit,
+the diagonal is 1 minus the off-diagonals), and to each other bit for bit on
+random transition matrices, for LOESS on both surfaces and for noqual.
+"""
+import numpy as np
+import pytest
+
+import dada2_b200 as D
+from oracle import oracle as O
+
+KINDS = [({}, D.ErrFun()), ({"surface": 1}, D.ErrFun(surface="interpolate")), ({"kind": 1}, D.ErrFun(kind="noqual"))]
+
+
+def both(trans, nq, okw, ef):
+    return O.errfun_apply(trans, nq, **okw), D.errfun_apply(trans, nq, ef)
+
+
+def test_empty_matrix_is_an_error():
+    """src/error_models.rs: loess_errfun_errors_on_an_empty_transition_matrix."""
+    nq = 40
+    t = np.zeros((16, nq), np.uint32)
+    with pytest.raises(ValueError, match="all 12 transitions"):
+        O.errfun_apply(t, nq)
+    with pytest.raises(D.DgpuError, match="all 12 transitions"):
+        D.errfun_apply(t, nq)
+
+
+def test_single_populated_column_fits_a_constant():
+    """src/error_models.rs: loess_errfun_single_populated_column_fits_a_constant."""
+    nq = 40
+    t = np.zeros((16, nq), np.uint32)
+    for i in range(4):
+        for j in range(4):
+            t[i * 4 + j, 30] = 10_000 if i == j else 10
+    for okw, ef in KINDS[:2]:
+        a, b = both(t, nq, okw, ef)
+        assert a.tobytes() == b.tobytes()
+        assert np.all(np.abs(a[1] - 11.0 / 10_030.0) < 1e-12)
+
+
+@pytest.mark.parametrize("bins", [[12, 24, 38], [2, 12, 23, 37]])
+def test_binned_quality_schemes_fit(bins):
+    """src/error_models.rs: loess_errfun_fits_binned_quality_schemes."""
+    nq = 40
+    t = np.zeros((16, nq), np.uint32)
+    for rank, q in enumerate(bins):
+        for i in range(4):
+            for j in range(4):
+                t[i * 4 + j, q] = 10_000 * (rank + 1) if i == j else 100 // (rank + 1) + 1
+    for okw, ef in KINDS[:2]:
+        a, b = both(t, nq, okw, ef)
+        assert a.tobytes() == b.tobytes()
+        off = np.array([a[i * 4 + j] for i in range(4) for j in range(4) if i != j])
+        assert np.any(off > 1e-7)
+        assert np.all((a >= 0.0) & (a <= 1.0))
+
+
+def test_diagonal_is_one_minus_the_off_diagonals():
+    """src/error_models.rs: test_expand_err_matrix_diagonal, through a flat
+    noqual fit: every off-diagonal equal gives diagonal 1 - 3 x rate."""
+    nq = 3
+    t = np.full((16, nq), 1000, np.uint32)
+    a, b = both(t, nq, {"kind": 1}, D.ErrFun(kind="noqual"))
+    assert a.tobytes() == b.tobytes()
+    rate = (3000 + 1.0) / (4 * 3001.0)
+    for i in range(4):
+        assert np.allclose(a[i * 5], 1.0 - 3 * rate, atol=1e-12)
+
+
+def test_rates_are_clamped():
+    nq = 20
+    t = np.zeros((16, nq), np.uint32)
+    t[0] = 1_000_000  # A: no errors at all
+    t[1] = 1_000_000  # C from A as often as A itself
+    t[5] = 1000
+    t[10] = 1000
+    t[15] = 1000
+    for okw, ef in KINDS:
+        a, b = both(t, nq, okw, ef)
+        assert a.tobytes() == b.tobytes()
+        off = np.array([a[i * 4 + j] for i in range(4) for j in range(4) if i != j])
+        assert off.min() >= 1e-7 and off.max() <= 0.25
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_product_fit_equals_the_oracle_bit_for_bit(seed):
+    rng = np.random.default_rng(seed)
+    for _ in range(40):
+        nq = int(rng.integers(3, 60))
+        t = rng.integers(0, int(10 ** rng.uniform(0, 5)), size=(16, nq)).astype(np.uint32)
+        for i in range(4):
+            t[i * 5] *= int(rng.integers(1, 2000))
+        t[:, rng.random(nq) < 0.2] = 0
+        for okw, ef in KINDS:
+            try:
+                a = O.errfun_apply(t, nq, **okw)
+            except ValueError:
+                with pytest.raises(D.DgpuError):
+                    D.errfun_apply(t, nq, ef)
+                continue
+            b = D.errfun_apply(t, nq, ef)
+            assert a.tobytes() == b.tobytes(), (nq, okw)
