@@ -739,6 +739,33 @@ def single_sample_report(config, local, steps, warmup, with_cpu=True, sm_mhz=Non
     }
 
 
+def learn_report(local, with_cpu=True, nsamples=6):
+    """learn_errors (src/learn_errors.rs:739-1020) on the first `nsamples`
+    samples of the 40-sample workload, LOESS fit (direct surface): wall time
+    of the GPU loop (every pass denoises the samples together on the device
+    and counts transitions there) beside the oracle's restatement on the
+    host cores, and whether both gave the same matrices."""
+    import dada2_b200 as D
+    from oracle import oracle as O
+
+    w = load_workload(1, 0)
+    samples = w.samples[:nsamples]
+    D.learn_errors(samples[:1], D.DadaParams(), max_consist=1, device=local)  # warm-up
+    t0 = time.perf_counter()
+    got = D.learn_errors(samples, D.DadaParams(), max_consist=10, device=local)
+    t_gpu = time.perf_counter() - t0
+    out = {"samples": nsamples, "uniques": int(sum(len(s.seqs) for s in samples)), "nq": got["nq"],
+           "passes": got["passes"], "converged": got["converged"], "gpu_s": t_gpu}
+    if with_cpu:
+        t0 = time.perf_counter()
+        want = O.learn_errors(samples, O.DadaParams(nthreads=os.cpu_count() or 1), max_consist=10)
+        out["oracle_s"] = time.perf_counter() - t0
+        out["oracle_cores"] = os.cpu_count()
+        out["identical"] = bool(got["passes"] == want["passes"] and np.array_equal(got["trans"], want["trans"]) and
+                                got["err_out"].tobytes() == want["err_out"].tobytes())
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -933,7 +960,8 @@ def main():
         for cfg, fn in ((0, lambda: single_sample_report(0, local, 10, 3, not args.no_cpu, clk.get("sm_mhz"))),
                         (2, lambda: single_sample_report(2, local, 5, 2, not args.no_cpu, clk.get("sm_mhz"))),
                         (3, lambda: pooled_report(local, 2, 1, not args.no_cpu)),
-                        (4, lambda: service_report(local, 1, 1, not args.no_cpu))):
+                        (4, lambda: service_report(local, 1, 1, not args.no_cpu)),
+                        ("learn_errors", lambda: learn_report(local, not args.no_cpu))):
             t0 = time.perf_counter()
             try:
                 others[str(cfg)] = fn()
