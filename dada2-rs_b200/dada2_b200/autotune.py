@@ -10,7 +10,7 @@ Their best values depend on read length: short reads give many cheap
 compare calls, long reads few expensive alignments.
 
 For each class (150, 250/220 and 1,450 nt) the tuner denoises a seeded
-synthetic workload of that class with inputs resident on the device
+production-sized synthetic workload of that class with inputs resident on the device
 (ResidentBatch) and descends one knob at a time: every value of a knob is
 timed with the others fixed, and a value is kept only when it is at least
 2 % faster than the best so far; two passes over the knobs. Each timing is
@@ -48,25 +48,29 @@ CLASS_LENGTH = {0: 150, 1: 250, 2: 1450}
 
 
 def class_workload(cls: int, seed: int = 4242):
-    """A seeded synthetic workload of read-length class ``cls``: Illumina-style
-    samples (uniques log-uniform in [500, 8,000], 50-200 variants) at 150 nt
-    or alternating 250/220 nt, or three PacBio-style 16S samples of 1,000
-    uniques at 1,400-1,550 nt (band 32, homopolymer gap -1)."""
+    """A seeded synthetic workload of read-length class ``cls``, sized like
+    production batches: for 250/220 nt the 40-sample shape (uniques
+    log-uniform in [500, 30,000], 50-400 variants, alternating lengths), for
+    150 nt 24 such samples of up to 15,000 uniques, for long reads three
+    PacBio-style 16S samples of 1,000 uniques at 1,400-1,550 nt (band 32,
+    homopolymer gap -1). The seeds differ from the benchmark's."""
     rng = np.random.default_rng(seed + cls)
     if cls == 2:
         errm = synth.error_matrix(94, floor=1e-3)
         samples = [synth.pacbio_sample(rng, 30, 1000, 1400, 1550, errm, 94) for _ in range(3)]
         return synth.Workload(2, "tuning: PacBio-style 16S x3", samples, errm, 94, band=32, homo_gap_p=-1)
+    if cls == 1:
+        w = synth.config1(seed=seed + 1)
+        w.name = "tuning: 40 Illumina-style samples at 250/220 nt"
+        return w
     errm = synth.error_matrix(41)
     samples = []
-    for si in range(12):
-        target = int(np.exp(rng.uniform(np.log(500), np.log(8000))))
-        nvar = int(rng.integers(50, 201))
-        L = 150 if cls == 0 else (250 if si % 2 == 0 else 220)
-        frac = 0.076 if L == 150 else 0.155
-        nreads = max(int((target - nvar) / frac), 2 * nvar)
-        samples.append(synth.illumina_sample(rng, nvar, nreads, L, errm, 41))
-    return synth.Workload(cls, f"tuning: 12 Illumina-style samples, class {cls}", samples, errm, 41)
+    for si in range(24):
+        target = int(np.exp(rng.uniform(np.log(500), np.log(15000))))
+        nvar = int(rng.integers(50, 401))
+        nreads = max(int((target - nvar) / 0.076), 2 * nvar)
+        samples.append(synth.illumina_sample(rng, nvar, nreads, 150, errm, 41))
+    return synth.Workload(0, "tuning: 24 Illumina-style samples at 150 nt", samples, errm, 41)
 
 
 def time_setting(w, params, packed, device: int, reps: int) -> float:
