@@ -311,6 +311,9 @@ __global__ void __launch_bounds__(256) k_pivot_dots(CompareLaunch L) {
 // kdist parked in res_lambda.
 template <int K>
 __global__ void __launch_bounds__(kScreenWarps * 32, 4) k_screen(CompareLaunch L) {
+  // every screen block is running: the alignment kernel may start launching
+  // (its blocks wait for this grid's results in cudaGridDependencySynchronize)
+  cudaTriggerProgrammaticLaunchCompletion();
   constexpr int NK16 = (1 << (2 * K)) / 16;            // 16-byte vectors per profile
   constexpr int VPL = NK16 >= 32 ? NK16 / 32 : 1;      // vectors per lane
   constexpr bool CENTER_REGS = VPL <= 2;               // k <= 5: center stays in registers
@@ -2166,12 +2169,15 @@ __device__ __forceinline__ PairResult align_pair(int lane, const KParams& kp, co
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_align(CompareLaunch L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const uint32_t count = *(volatile uint32_t*)&L.queue_counts[4];
-  if (blockIdx.x * kNwWarps >= count) return;  // nothing queued for this block
+  cudaTriggerProgrammaticLaunchCompletion();  // the store kernel may start launching
   const KParams& kp = L.kp;
+  // the error matrix does not depend on the screen: staged while it finishes
   double* err_s = reinterpret_cast<double*>(smem_raw);
   const int nerr = 16 * kp.ncol;
   for (int t = threadIdx.x; t < nerr; t += blockDim.x) err_s[t] = L.pool.err[t];
+  cudaGridDependencySynchronize();  // the screen's pass queue and results are complete
+  const uint32_t count = *(volatile uint32_t*)&L.queue_counts[4];
+  if (blockIdx.x * kNwWarps >= count) return;  // nothing queued for this block
   const size_t err_bytes = err_smem_bytes(kp.ncol);
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int gw = blockIdx.x * kNwWarps + wib;
@@ -2304,6 +2310,7 @@ __global__ void __launch_bounds__(kStoreThreads) k_store(CompareLaunch L) {
   constexpr int IPT = kStoreSpan / kStoreThreads;
   __shared__ uint32_t warp_off[32];
   __shared__ uint32_t ctr[TC_NCOUNTERS];
+  cudaGridDependencySynchronize();  // the alignment kernel's results are complete
   const uint32_t blk = blockIdx.x;
   const uint32_t t = L.store_task[blk];
   const uint32_t span0 = L.store_chunk[blk] * uint32_t(kStoreSpan);
@@ -2493,9 +2500,27 @@ void launch_compare(const CompareLaunch& L0, cudaStream_t st, cudaEvent_t* ev) {
       carved.fetch_or(bit);
     }
   }
-  k_align<<<L.geom.nwarps / kNwWarps, kNwWarps * 32, asm_, st>>>(L);
+  // Programmatic dependent launch: the alignment and store kernels are
+  // scheduled while their predecessor drains and wait for its results in
+  // cudaGridDependencySynchronize, so the launch gaps overlap with work.
+  cudaLaunchAttribute pdl[1];
+  pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  pdl[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.stream = st;
+  cfg.attrs = pdl;
+  cfg.numAttrs = 1;
+  cfg.gridDim = dim3(L.geom.nwarps / kNwWarps);
+  cfg.blockDim = dim3(kNwWarps * 32);
+  cfg.dynamicSmemBytes = asm_;
+  cudaLaunchKernelEx(&cfg, k_align, L);
   if (ev) cudaEventRecord(ev[2], st);
-  if (L.do_store) k_store<<<L.nstore_blocks, kStoreThreads, 0, st>>>(L);
+  if (L.do_store) {
+    cfg.gridDim = dim3(L.nstore_blocks);
+    cfg.blockDim = dim3(kStoreThreads);
+    cfg.dynamicSmemBytes = 0;
+    cudaLaunchKernelEx(&cfg, k_store, L);
+  }
   if (ev) cudaEventRecord(ev[3], st);
 }
 
