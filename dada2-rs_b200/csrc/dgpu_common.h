@@ -158,6 +158,7 @@ struct CompareLaunch {
   // (task_cl_prefix: prefix sums of the tasks' cluster indices) and the
   // screen excludes raws by the bound.
   uint32_t pivot, cdot_ready;
+  uint32_t pdl;  // tuning: launch the align and store kernels as programmatic dependents
   const uint32_t* task_cl_prefix;
   uint32_t total_cl;
   uint32_t* queue_pass;     // nraw capacity: items that passed the screen

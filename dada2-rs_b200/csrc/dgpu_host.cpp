@@ -307,7 +307,7 @@ static void recycle_all(B&... b) {
 // table the built-in values below apply (measured on the 40-sample
 // 250/220-nt batch).
 // ---------------------------------------------------------------------------
-static const dgpu_tuning kTuneDefault = {6, 4, 1, kAlignCtasPerSm, 32, 4, 32768};
+static const dgpu_tuning kTuneDefault = {6, 4, 1, kAlignCtasPerSm, 32, 4, 32768, 1};
 static std::mutex g_tune_mu;
 static dgpu_tuning g_tune[3] = {kTuneDefault, kTuneDefault, kTuneDefault};
 static bool g_tune_loaded = false;
@@ -318,7 +318,8 @@ static bool tuning_valid(const dgpu_tuning& t) {
   return t.launch_slots >= 1 && t.launch_slots <= 8 && t.samples_per_launch >= 1 && t.samples_per_launch <= 4096 &&
          t.dedicated_slots >= 0 && t.dedicated_slots <= 7 && t.align_ctas_per_sm >= 1 &&
          t.align_ctas_per_sm <= kAlignCtasPerSm && (t.screen_chunk_max == 16 || t.screen_chunk_max == 32) &&
-         t.screen_blocks_per_sm >= 1 && t.screen_blocks_per_sm <= 4 && t.pivot_min_items >= 0;
+         t.screen_blocks_per_sm >= 1 && t.screen_blocks_per_sm <= 4 && t.pivot_min_items >= 0 &&
+         (t.programmatic_launch == 0 || t.programmatic_launch == 1);
 }
 
 // Text form: one line per class, "class C launch_slots A samples_per_launch B
@@ -365,6 +366,7 @@ static int tuning_parse(const std::string& text, dgpu_tuning out[3], std::string
       else if (tok[k] == "screen_chunk_max") v.screen_chunk_max = x;
       else if (tok[k] == "screen_blocks_per_sm") v.screen_blocks_per_sm = x;
       else if (tok[k] == "pivot_min_items") v.pivot_min_items = x;
+      else if (tok[k] == "programmatic_launch") v.programmatic_launch = x;
       else {
         *msg = "tuning line " + std::to_string(lineno) + ": unknown key " + tok[k];
         return DGPU_E_INVALID;
@@ -388,7 +390,7 @@ static std::string tuning_format(const dgpu_tuning t[3]) {
          std::to_string(t[c].dedicated_slots) + " align_ctas_per_sm " + std::to_string(t[c].align_ctas_per_sm) +
          " screen_chunk_max " + std::to_string(t[c].screen_chunk_max) + " screen_blocks_per_sm " +
          std::to_string(t[c].screen_blocks_per_sm) + " pivot_min_items " + std::to_string(t[c].pivot_min_items) +
-         "\n";
+         " programmatic_launch " + std::to_string(t[c].programmatic_launch) + "\n";
   return o;
 }
 
@@ -859,6 +861,7 @@ int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
     const dgpu_tuning tu = tuning_for(Q.lmax);
     L.screen_chunk_max = uint32_t(tu.screen_chunk_max);
     L.screen_blocks_per_sm = uint32_t(tu.screen_blocks_per_sm);
+    L.pdl = uint32_t(tu.programmatic_launch);
   }
   L.pivot = pivot ? 1u : 0u;
   L.cdot_ready = cdot_ready ? 1u : 0u;

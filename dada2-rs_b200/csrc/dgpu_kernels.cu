@@ -2509,7 +2509,7 @@ void launch_compare(const CompareLaunch& L0, cudaStream_t st, cudaEvent_t* ev) {
   cudaLaunchConfig_t cfg = {};
   cfg.stream = st;
   cfg.attrs = pdl;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = L.pdl ? 1 : 0;
   cfg.gridDim = dim3(L.geom.nwarps / kNwWarps);
   cfg.blockDim = dim3(kNwWarps * 32);
   cfg.dynamicSmemBytes = asm_;

@@ -58,7 +58,7 @@ class KernelStatsC(C.Structure):
 class TuningC(C.Structure):
     _fields_ = [(n, C.c_int32) for n in ("launch_slots", "samples_per_launch", "dedicated_slots",
                                          "align_ctas_per_sm", "screen_chunk_max", "screen_blocks_per_sm",
-                                         "pivot_min_items")]
+                                         "pivot_min_items", "programmatic_launch")]
 
 
 class ErrFunC(C.Structure):

@@ -1,11 +1,12 @@
 """Autotuner of the compare step's launch shape, per read-length class.
 
 The reference schedules its compare map on rayon with one knob, the grain
-DADA2_RS_PAR_GRAIN (src/cluster.rs:19-28). Here the launch shape has seven
+DADA2_RS_PAR_GRAIN (src/cluster.rs:19-28). Here the launch shape has eight
 knobs (include/dada2_b200.h, dgpu_tuning): concurrent launch slots, samples
 per launch, slots dedicated to the longest chains, resident alignment CTAs
 per SM (pairs in flight), the screen's largest chunk and its blocks per SM,
-and the launch size from which the screen's pivot bound runs.
+the launch size from which the screen's pivot bound runs, and whether the
+alignment and store kernels launch as programmatic dependents.
 Their best values depend on read length: short reads give many cheap
 compare calls, long reads few expensive alignments.
 
@@ -41,6 +42,7 @@ SPACE = {
     "screen_chunk_max": [16, 32],
     "screen_blocks_per_sm": [2, 3, 4],
     "pivot_min_items": [0, 8192, 32768, 131072],
+    "programmatic_launch": [0, 1],
 }
 
 # representative read length of each class
@@ -51,14 +53,14 @@ def class_workload(cls: int, seed: int = 4242):
     """A seeded synthetic workload of read-length class ``cls``, sized like
     production batches: for 250/220 nt the 40-sample shape (uniques
     log-uniform in [500, 30,000], 50-400 variants, alternating lengths), for
-    150 nt 24 such samples of up to 15,000 uniques, for long reads three
-    PacBio-style 16S samples of 1,000 uniques at 1,400-1,550 nt (band 32,
-    homopolymer gap -1). The seeds differ from the benchmark's."""
+    150 nt 24 such samples of up to 15,000 uniques, for long reads eight
+    PacBio-style 16S samples of 800 uniques at 1,400-1,550 nt (band 32,
+    homopolymer gap -1), enough samples that the slot knobs matter. The seeds differ from the benchmark's."""
     rng = np.random.default_rng(seed + cls)
     if cls == 2:
         errm = synth.error_matrix(94, floor=1e-3)
-        samples = [synth.pacbio_sample(rng, 30, 1000, 1400, 1550, errm, 94) for _ in range(3)]
-        return synth.Workload(2, "tuning: PacBio-style 16S x3", samples, errm, 94, band=32, homo_gap_p=-1)
+        samples = [synth.pacbio_sample(rng, 30, 800, 1400, 1550, errm, 94) for _ in range(8)]
+        return synth.Workload(2, "tuning: PacBio-style 16S x8", samples, errm, 94, band=32, homo_gap_p=-1)
     if cls == 1:
         w = synth.config1(seed=seed + 1)
         w.name = "tuning: 40 Illumina-style samples at 250/220 nt"

@@ -236,6 +236,9 @@ int dgpu_cache_release(int device, uint64_t* freed);
  * pivot_min_items      compare launches of at least this many (center, unique) items
  *                      exclude far uniques by the exact pivot bound without reading
  *                      their k-mer profiles (one extra small kernel); 0 = never
+ * programmatic_launch  1: the alignment and store kernels are launched as programmatic
+ *                      dependents of the kernel before them (scheduled while it drains);
+ *                      0: ordinary stream order
  * The library loads DGPU_TUNING_FILE, else tuning.txt beside itself, at first
  * use (the autotuner, dada2_b200/autotune.py, writes that file); the
  * DGPU_LAUNCH_SLOTS, DGPU_BATCH_MAX and DGPU_DEDICATED_SLOTS environment
@@ -244,7 +247,7 @@ int dgpu_cache_release(int device, uint64_t* freed);
  * the rayon grain DADA2_RS_PAR_GRAIN (src/cluster.rs:19-28). */
 typedef struct {
   int32_t launch_slots, samples_per_launch, dedicated_slots, align_ctas_per_sm, screen_chunk_max,
-      screen_blocks_per_sm, pivot_min_items;
+      screen_blocks_per_sm, pivot_min_items, programmatic_launch;
 } dgpu_tuning;
 /* the setting a pool whose longest unique has max_len bases would use */
 int dgpu_tuning_get(int max_len, dgpu_tuning* out);

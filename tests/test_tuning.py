@@ -27,7 +27,8 @@ def test_classes_follow_read_length(saved_table):
 def test_save_and_load_round_trip(saved_table):
     path = saved_table / "t.txt"
     a = {"launch_slots": 8, "samples_per_launch": 2, "dedicated_slots": 0, "align_ctas_per_sm": 3,
-         "screen_chunk_max": 16, "screen_blocks_per_sm": 2, "pivot_min_items": 4096}
+         "screen_chunk_max": 16, "screen_blocks_per_sm": 2, "pivot_min_items": 4096,
+         "programmatic_launch": 0}
     b = {**a, "launch_slots": 4, "samples_per_launch": 16, "dedicated_slots": 2}
     D.tuning_set(1, a)
     D.tuning_set(2, b)
@@ -55,6 +56,7 @@ def test_partial_lines_keep_other_keys(saved_table):
     ("class 0 screen_chunk_max 24\n", "out of range"),
     ("class 0 align_ctas_per_sm 0\n", "out of range"),
     ("class 0 pivot_min_items -1\n", "out of range"),
+    ("class 0 programmatic_launch 2\n", "out of range"),
     ("class 0 warp_size 16\n", "unknown key"),
     ("launch_slots 2\n", "expected"),
 ])
