@@ -69,7 +69,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--only", default=None, choices=["dp", "screen"],
                     help="run only the isolated k_align (dp) or k_screen launches of the roofline on config 1 "
-                         "(small, for ncu captures) and print their figures")
+                         "(or 2 with --config 2; small, for ncu captures) and print their figures")
     ap.add_argument("--no-others", action="store_true",
                     help="skip the reports of configs 0, 2, 3 and 4 that the default config-1 run adds")
     ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
@@ -786,7 +786,7 @@ def main():
 
     torch.cuda.set_device(local)
     if args.only:
-        w = load_workload(1, 0)
+        w = load_workload(args.config if args.config in (1, 2) else 1, 0)
         params = dada_params(w)
         if args.only == "dp":
             print(json.dumps(dp_roofline(w.samples, w, params, local, calls=1)), flush=True)
