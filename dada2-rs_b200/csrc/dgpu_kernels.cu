@@ -2310,6 +2310,9 @@ __global__ void __launch_bounds__(kStoreThreads) k_store(CompareLaunch L) {
   constexpr int IPT = kStoreSpan / kStoreThreads;
   __shared__ uint32_t warp_off[32];
   __shared__ uint32_t ctr[TC_NCOUNTERS];
+  __shared__ uint32_t s_idx[kStoreSpan], s_ham[kStoreSpan];
+  __shared__ double s_lam[kStoreSpan];
+  __shared__ float s_ll[kStoreSpan];
   cudaGridDependencySynchronize();  // the alignment kernel's results are complete
   const uint32_t blk = blockIdx.x;
   const uint32_t t = L.store_task[blk];
@@ -2371,15 +2374,30 @@ __global__ void __launch_bounds__(kStoreThreads) k_store(CompareLaunch L) {
     if (lane == 31) ctr[TC_STORED] = wi;
   }
   __syncthreads();
+  // The CTA's stored comps are staged in shared memory in ascending raw order
+  // and then written out contiguously, so each warp's stores to the mapped
+  // host arrays cover consecutive addresses (few, full PCIe writes instead of
+  // one small write per comp).
   uint32_t pos = warp_off[w] + (incl - cnt);
 #pragma unroll
   for (int q = 0; q < IPT; ++q) {
     if (flags & (1u << q)) {
-      const uint32_t o = T.out_off + span0 + pos++;
-      L.comp_index[o] = r0 + q;
-      L.comp_lambda[o] = lam[q];
-      L.comp_ham[o] = (ham[q] == 0xffffffffu) ? 0u : ham[q];
-      if (L.comp_ll32) L.comp_ll32[o] = L.pool.res_loglam32[T.base + r0 + q];
+      s_idx[pos] = r0 + q;
+      s_lam[pos] = lam[q];
+      s_ham[pos] = (ham[q] == 0xffffffffu) ? 0u : ham[q];
+      if (L.comp_ll32) s_ll[pos] = L.pool.res_loglam32[T.base + r0 + q];
+      ++pos;
+    }
+  }
+  __syncthreads();
+  {
+    const uint32_t nst = ctr[TC_STORED];
+    const uint32_t o0 = T.out_off + span0;
+    for (uint32_t k = threadIdx.x; k < nst; k += blockDim.x) {
+      L.comp_index[o0 + k] = s_idx[k];
+      L.comp_lambda[o0 + k] = s_lam[k];
+      L.comp_ham[o0 + k] = s_ham[k];
+      if (L.comp_ll32) L.comp_ll32[o0 + k] = s_ll[k];
     }
   }
   c_scr = __reduce_add_sync(FULL, c_scr);
