@@ -122,14 +122,26 @@ __host__ __device__ inline size_t nw_smem_per_warp_vec(const NwGeom& g) {
          align16(g.vec_ncol) + align16(kStageBytes) + align16(g.lmax) + align16(size_t(g.lmax) * 2) +
          align16(g.lmax);
 }
-__host__ __device__ inline size_t nw_smem_per_warp_rm(const NwGeom& g) {
-  return align16(g.lmax) * 4 + align16(size_t(kRmStageRows) * 2 * rm_kbound(g.rm_pairs) * 4) + align16(g.lmax) +
-         align16(size_t(g.lmax) * 2);
+__host__ __device__ inline size_t rm_stage_bytes(int kbound) { return align16(size_t(kRmStageRows) * 2 * kbound * 4); }
+// The lambda indices (2 bytes per raw position) are built after the traceback
+// is done with the staged window, so they share its bytes when they fit.
+__host__ __device__ inline bool rm_fidx_in_stage(int lmax, int kbound) {
+  return size_t(lmax) * 2 <= rm_stage_bytes(kbound);
 }
-// The align kernel carves either layout from the same per-warp region.
+__host__ __device__ inline size_t nw_smem_per_warp_rm(const NwGeom& g) {
+  const int kb = rm_kbound(g.rm_pairs);
+  return align16(g.lmax) * 2 + rm_stage_bytes(kb) + align16(g.lmax) +
+         (rm_fidx_in_stage(g.lmax, kb) ? 0 : align16(size_t(g.lmax) * 2));
+}
+// The align kernel carves either layout from the same per-warp region, sized
+// for the forms the geometry lets a pair take (a zero scratch size marks a
+// form no pair of the launch can reach: the register form needs a vectorized
+// launch without homopolymer gaps and both lengths <= 3500; every other pair
+// is row-major).
 __host__ __device__ inline size_t align_smem_per_warp(const NwGeom& g) {
-  const size_t a = nw_smem_per_warp_vec(g), b = nw_smem_per_warp_rm(g);
-  return a > b ? a : b;
+  const size_t a = g.vec_scratch ? nw_smem_per_warp_vec(g) : 0, b = g.rm_scratch ? nw_smem_per_warp_rm(g) : 0;
+  const size_t m = a > b ? a : b;
+  return m > 16 ? m : 16;
 }
 
 // ---- launchers (dgpu_kernels.cu) ----
@@ -162,7 +174,8 @@ struct CompareLaunch {
   const uint32_t* task_cl_prefix;
   uint32_t total_cl;
   uint32_t* queue_pass;     // nraw capacity: items that passed the screen
-  uint32_t* queue_counts;   // 8 words; [4] = items pushed to queue_pass
+  uint32_t* queue_counts;   // 8 words; [4] = items pushed to queue_pass, [5] = profiles the
+                            // screen read, [6] = the align warps' slot cursor
   uint8_t* nw_scratch;      // nwarps * max(vec_scratch, rm_scratch)
   NwGeom geom;
   uint32_t* err_word;

@@ -1777,13 +1777,11 @@ __device__ bool vec_align_any(int lane, const uint8_t* g1, int l1, const uint8_t
 // K5: row-major ends-free / homopolymer aligner as an anti-diagonal wavefront
 // ---------------------------------------------------------------------------
 struct RmSmem {
-  uint8_t* s1;
-  uint8_t* s2;
-  uint8_t* h1;
+  uint8_t* h1;      // base code (bits 0-3) | homopolymer bit 16, per position
   uint8_t* h2;
   uint32_t* stage;  // kRmStageRows diagonals x 2K words
   uint8_t* tcode;
-  uint16_t* fidx;
+  uint16_t* fidx;   // inside stage when it fits there (built after the traceback)
 };
 
 // m[p] = the base code s[p] (1..4) with bit 4 set when p lies in a run of
@@ -1813,11 +1811,8 @@ __device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8
                               int mismatch, int gap, int homo_gap, int band, bool homo, const RmSmem& S,
                               uint32_t* pscr, uint32_t* ham_out, uint32_t* err_word, uint8_t* dbg0, uint8_t* dbg1,
                               uint32_t* dbg_len) {
-  for (int p = lane; p < len1; p += 32) S.s1[p] = g1[p];
-  for (int p = lane; p < len2; p += 32) S.s2[p] = g2[p];
-  __syncwarp();
-  code_mask_warp(lane, S.s1, len1, S.h1, homo);
-  code_mask_warp(lane, S.s2, len2, S.h2, homo);
+  code_mask_warp(lane, g1, len1, S.h1, homo);
+  code_mask_warp(lane, g2, len2, S.h2, homo);
   int lband, rband, o_lo, o_hi;
   if (band >= 0) {
     if (len2 > len1) { lband = band; rband = band + (len2 - len1); }
@@ -1952,7 +1947,7 @@ __device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8
   // shared memory; lane k tests whether the k-th next step is diagonal (cell
   // (i-k, j-k): anti-diagonal t-2k, same offset), so a run of f diagonal
   // steps is taken at once, one per lane. Other steps are taken singly.
-  for (int p = lane; p < len2; p += 32) S.tcode[p] = uint8_t(kUnaligned | ((unsigned(S.s2[p]) - 1u) * 5u));
+  for (int p = lane; p < len2; p += 32) S.tcode[p] = uint8_t(kUnaligned | (((S.h2[p] & 15u) - 1u) * 5u));
   int i = len1, j = len2, slo = 0x7fffffff;
   uint32_t ham = 0, alen = 0;
   bool ok = true;
@@ -1985,7 +1980,7 @@ __device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8
       if (f > 0) {
         bool mm = false;
         if (lane < f) {
-          const uint8_t a = S.s1[i - 1 - lane], b = S.s2[j - 1 - lane];
+          const uint8_t a = S.h1[i - 1 - lane] & 15u, b = S.h2[j - 1 - lane] & 15u;
           S.tcode[j - 1 - lane] = uint8_t((unsigned(a) - 1u) * 4u + (unsigned(b) - 1u));
           mm = a != b;
           if (dbg0) {
@@ -2003,10 +1998,10 @@ __device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8
       v = int((w[0] >> L) & 1u) | (int((w[1] >> L) & 1u) << 1);
     }
     if (v == 2) {
-      if (dbg0 && lane == 0) { dbg0[alen] = '-'; dbg1[alen] = S.s2[j - 1]; }
+      if (dbg0 && lane == 0) { dbg0[alen] = '-'; dbg1[alen] = S.h2[j - 1] & 15u; }
       --j;
     } else if (v == 3) {
-      if (dbg0 && lane == 0) { dbg0[alen] = S.s1[i - 1]; dbg1[alen] = '-'; }
+      if (dbg0 && lane == 0) { dbg0[alen] = S.h1[i - 1] & 15u; dbg1[alen] = '-'; }
       --i;
     } else {
       ok = false;
@@ -2028,13 +2023,12 @@ __device__ RmSmem carve_rm(unsigned char* base, int lmax, int kbound) {
   RmSmem S;
   size_t o = 0;
   auto take = [&](size_t bytes) { unsigned char* p = base + o; o += (bytes + 15) & ~size_t(15); return p; };
-  S.s1 = take(lmax);
-  S.s2 = take(lmax);
   S.h1 = take(lmax);
   S.h2 = take(lmax);
-  S.stage = reinterpret_cast<uint32_t*>(take(size_t(kRmStageRows) * 2 * kbound * 4));
+  S.stage = reinterpret_cast<uint32_t*>(take(rm_stage_bytes(kbound)));
   S.tcode = take(lmax);
-  S.fidx = reinterpret_cast<uint16_t*>(take(size_t(lmax) * 2));
+  S.fidx = rm_fidx_in_stage(lmax, kbound) ? reinterpret_cast<uint16_t*>(S.stage)
+                                          : reinterpret_cast<uint16_t*>(take(size_t(lmax) * 2));
   return S;
 }
 
@@ -2114,7 +2108,10 @@ __device__ __forceinline__ PairResult align_pair(int lane, const KParams& kp, co
   double kodist = -1.0;
   const int minl = lc < lg ? lc : lg;
   const bool want_kod = kp.use_kmers && kp.gapless && lc == lg;
-  PairResult R{true, AM_NONE, 0u, lg, VS.tcode, VS.fidx, qg};
+  // the raw's transition codes and lambda indices live in the layout of the
+  // form this pair takes (the per-warp region holds only the forms the
+  // launch can reach)
+  PairResult R{true, AM_NONE, 0u, lg, rm ? RS.tcode : VS.tcode, rm ? RS.fidx : VS.fidx, qg};
   uint32_t ham = 0;
   if (want_kod || kp.band == 0) {
     const int klen = lc - (k - 1);
@@ -2137,7 +2134,7 @@ __device__ __forceinline__ PairResult align_pair(int lane, const KParams& kp, co
   const bool gapless = kp.band == 0 || (kp.gapless && fabs(kodist - kdist) < DBL_EPSILON);
   if (gapless) {
     // raw position p aligns to center position p while p < len(center)
-    uint8_t* tcode = VS.tcode;
+    uint8_t* tcode = rm ? RS.tcode : VS.tcode;
     for (int p = lane; p < lg; p += 32) {
       const unsigned r = sg[p];
       const unsigned code = (p < lc) ? (unsigned(sc[p]) - 1u) * 4u + (r - 1u) : (kUnaligned | ((r - 1u) * 5u));
@@ -2188,8 +2185,16 @@ __global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_align(Compar
   const size_t scr_stride = L.geom.vec_scratch > L.geom.rm_scratch ? L.geom.vec_scratch : L.geom.rm_scratch;
   uint8_t* scratch = L.nw_scratch + size_t(gw) * scr_stride;
   __syncthreads();
-  const uint32_t warps_total = gridDim.x * kNwWarps;
-  for (uint32_t slot = uint32_t(gw); slot < count; slot += warps_total) {
+  // Warps claim queue slots one at a time from a shared cursor (cleared with
+  // the other counters after each call), so pairs of unequal cost -- gapless
+  // against NW, short against long -- and CTAs that become resident late
+  // (when shared memory admits fewer CTAs per SM than the grid assumes) even
+  // out. Results go to each raw's own entries, so the order is free.
+  for (;;) {
+    uint32_t slot = 0;
+    if (lane == 0) slot = atomicAdd(&L.queue_counts[6], 1u);
+    slot = __shfl_sync(FULL, slot, 0);
+    if (slot >= count) break;
     const uint32_t item = L.queue_pass[slot];
     const uint32_t t = find_task(L.task_prefix, L.ntask, item);
     const TaskDev T = L.tasks[t];
