@@ -1840,33 +1840,61 @@ __device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8
   // a band cell, row 0 / column 0 or outside. Those of anti-diagonal t + 1
   // are loaded and formed while anti-diagonal t's values are computed, so
   // the shared-memory loads stay off the dependency chain.
+  //
+  // On anti-diagonal t of relative parity p = (t - o_lo) & 1, lane q = lane +
+  // 32 m holds cell (i, j) = (E - q, E + q + o_lo + p) with E = (t - o_lo - p)
+  // / 2. From one anti-diagonal to the next i steps up when the parity turns
+  // even and j when it turns odd, so a lane keeps its two sequence bytes in
+  // registers and loads one new byte per group per anti-diagonal.
   struct Cost {
     int gu, gl, sd;
-    uint32_t kind;  // 1 cell, 2 row 0 / column 0 inside the band, 0 outside
+    bool cell, edge;  // band cell; row 0 / column 0 inside the band
   };
-  auto cost_at = [&](int t, int m) {
+  uint32_t inb = 0;  // bit 2m + p: q < P and o_lo + 2q + p <= o_hi
+#pragma unroll
+  for (int m = 0; m < K; ++m) {
     const int q = lane + 32 * m;
-    const int o = o_lo + 2 * q + ((t - o_lo) & 1);
-    const int i = (t - o) >> 1, j = (t + o) >> 1;
-    const bool inband = q < P && o <= o_hi;
-    const bool cell = inband && i >= 1 && j >= 1 && i <= len1 && j <= len2;
-    const bool edge = inband && !cell && i >= 0 && j >= 0 && i <= len1 && j <= len2;
-    // clamped reads: a lane outside the matrix reads a valid byte it ignores
-    const uint32_t x = S.h1[max(0, min(i - 1, len1 - 1))], y = S.h2[max(0, min(j - 1, len2 - 1))];
+#pragma unroll
+    for (int p = 0; p < 2; ++p)
+      if (q < P && o_lo + 2 * q + p <= o_hi) inb |= 1u << (2 * m + p);
+  }
+  // clamped reads: a lane outside the matrix reads a valid byte it ignores
+  const unsigned cl1 = unsigned(len1 > 0 ? len1 - 1 : 0), cl2 = unsigned(len2 > 0 ? len2 - 1 : 0);
+  uint32_t xb[K], yb[K];
+  // LD: 1 loads the h1 byte (i moved), 2 the h2 byte (j moved), 3 both
+  auto cost_of = [&](int E, int m, auto par_tag, auto ld_tag) {
+    constexpr int PN = decltype(par_tag)::value;
+    constexpr int LD = decltype(ld_tag)::value;
+    const int q = lane + 32 * m;
+    const int i = E - q, j = E + q + o_lo + PN;
+    if (LD & 1) xb[m] = S.h1[min(unsigned(i - 1), cl1)];
+    if (LD & 2) yb[m] = S.h2[min(unsigned(j - 1), cl2)];
+    const uint32_t x = xb[m], y = yb[m];
+    const bool inband = (inb >> (2 * m + PN)) & 1u;
     Cost c;
+    c.cell = inband && unsigned(i - 1) < unsigned(len1) && unsigned(j - 1) < unsigned(len2);
+    c.edge = inband && !c.cell && unsigned(i) <= unsigned(len1) && unsigned(j) <= unsigned(len2);
     c.gu = (j == len2) ? 0 : ((x & 16u) ? hgap : gap);
     c.gl = (i == len1) ? 0 : ((y & 16u) ? hgap : gap);
     c.sd = ((x ^ y) & 15u) == 0u ? match : mismatch;
-    c.kind = cell ? 1u : (edge ? 2u : 0u);
     return c;
   };
+  using Even = std::integral_constant<int, 0>;
+  using Odd = std::integral_constant<int, 1>;
+  using LoadX = std::integral_constant<int, 1>;
+  using LoadY = std::integral_constant<int, 2>;
+  using LoadXY = std::integral_constant<int, 3>;
   int ve[K], vo[K];
   Cost cur[K];
+  {
+    const int p0 = o_lo & 1;  // parity of t = 0
+    const int E0 = (0 - o_lo - p0) >> 1;
 #pragma unroll
-  for (int m = 0; m < K; ++m) {
-    ve[m] = kNegSentinel;
-    vo[m] = kNegSentinel;
-    cur[m] = cost_at(0, m);
+    for (int m = 0; m < K; ++m) {
+      ve[m] = kNegSentinel;
+      vo[m] = kNegSentinel;
+      cur[m] = p0 ? cost_of(E0, m, Odd{}, LoadXY{}) : cost_of(E0, m, Even{}, LoadXY{});
+    }
   }
   uint32_t pw[2 * K];
 #pragma unroll
@@ -1877,8 +1905,12 @@ __device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8
   auto diag = [&](int t, auto par_tag) {
     constexpr int PAR = decltype(par_tag)::value;
     Cost nxt[K];
+    const int En = (t - o_lo + PAR) >> 1;  // E of anti-diagonal t + 1 (parity 1 - PAR)
 #pragma unroll
-    for (int m = 0; m < K; ++m) nxt[m] = cost_at(t + 1, m);  // past tmax: unused
+    for (int m = 0; m < K; ++m) {  // past tmax: unused
+      if (PAR) nxt[m] = cost_of(En, m, Even{}, LoadX{});
+      else nxt[m] = cost_of(En, m, Odd{}, LoadY{});
+    }
 #pragma unroll
     for (int m = 0; m < K; ++m) {
       const int q = lane + 32 * m;
@@ -1904,8 +1936,8 @@ __device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8
       const bool lw = !upw && left >= dg;
       int val = upw ? up : (lw ? left : dg);
       uint32_t code = upw ? 3u : (lw ? 2u : 1u);
-      if (cur[m].kind != 1u) {
-        val = cur[m].kind == 2u ? 0 : kNegSentinel;
+      if (!cur[m].cell) {
+        val = cur[m].edge ? 0 : kNegSentinel;
         code = 0u;
       }
       if (PAR) vo[m] = val;
@@ -1928,8 +1960,6 @@ __device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8
 #pragma unroll
     for (int m = 0; m < K; ++m) cur[m] = nxt[m];
   };
-  using Even = std::integral_constant<int, 0>;
-  using Odd = std::integral_constant<int, 1>;
   if ((o_lo & 1) == 0) {  // t = 0 has parity 0
     for (int t = 0; t <= tmax; t += 2) {
       diag(t, Even{});
