@@ -1806,6 +1806,89 @@ __device__ void code_mask_warp(int lane, const uint8_t* s, int n, uint8_t* m, bo
 // the lanes and each needs only its own lane's and one neighbour's previous
 // values (one shuffle). Gaps inside homopolymer runs cost homo_gap; the last
 // row and column are free; ties prefer up, then left, then diagonal.
+// Traceback of the row-major aligner (src/nwalign.rs:234-273) over the
+// pointer planes the DP left in pscr (rows t = 0 .. len1 + len2 of 2K words).
+template <int K>
+__device__ __forceinline__ bool rm_traceback(int lane, int len1, int len2, int o_lo, int o_hi, const RmSmem& S,
+                                             const uint32_t* pscr, uint32_t* ham_out, uint32_t* err_word,
+                                             uint8_t* dbg0, uint8_t* dbg1, uint32_t* dbg_len) {
+  // Row 0 moves left, column 0 moves up.
+  // A window of kRmStageRows anti-diagonals of pointer planes is staged in
+  // shared memory; lane k tests whether the k-th next step is diagonal (cell
+  // (i-k, j-k): anti-diagonal t-2k, same offset), so a run of f diagonal
+  // steps is taken at once, one per lane. Other steps are taken singly.
+  for (int p = lane; p < len2; p += 32) S.tcode[p] = uint8_t(kUnaligned | (((S.h2[p] & 15u) - 1u) * 5u));
+  int i = len1, j = len2, slo = 0x7fffffff;
+  uint32_t ham = 0, alen = 0;
+  bool ok = true;
+  __syncwarp();
+  while (i > 0 || j > 0) {
+    int v;
+    if (i == 0) v = 2;
+    else if (j == 0) v = 3;
+    else {
+      const int o = j - i, t = i + j;
+      if (o < o_lo || o > o_hi) { ok = false; break; }
+      if (t < slo || (t - slo < kRmStageRows / 2 && slo > 0)) {  // keep half a window below t
+        const int nlo = max(0, t - (kRmStageRows - 1));
+        __syncwarp();
+        const int nw = (t - nlo + 1) * 2 * K;
+        const uint32_t* src = pscr + size_t(nlo) * (2 * K);
+        for (int x = lane; x < nw; x += 32) S.stage[x] = src[x];
+        __syncwarp();
+        slo = nlo;
+      }
+      const int q = (o - o_lo) >> 1, L = q & 31, m = q >> 5;
+      const int tk = t - 2 * lane;
+      bool diag = false;
+      if (tk >= slo && i - lane >= 1 && j - lane >= 1) {
+        const uint32_t* wk = S.stage + (tk - slo) * (2 * K) + 2 * m;
+        diag = (((wk[0] >> L) & 1u) | (((wk[1] >> L) & 1u) << 1)) == 1u;
+      }
+      const uint32_t nd = __ballot_sync(FULL, !diag);
+      const int f = nd ? __ffs(nd) - 1 : 32;
+      if (f > 0) {
+        bool mm = false;
+        if (lane < f) {
+          const uint8_t a = S.h1[i - 1 - lane] & 15u, b = S.h2[j - 1 - lane] & 15u;
+          S.tcode[j - 1 - lane] = uint8_t((unsigned(a) - 1u) * 4u + (unsigned(b) - 1u));
+          mm = a != b;
+          if (dbg0) {
+            dbg0[alen + lane] = a;
+            dbg1[alen + lane] = b;
+          }
+        }
+        ham += __popc(__ballot_sync(FULL, mm));
+        i -= f;
+        j -= f;
+        alen += uint32_t(f);
+        continue;
+      }
+      const uint32_t* w = S.stage + (t - slo) * (2 * K) + 2 * m;
+      v = int((w[0] >> L) & 1u) | (int((w[1] >> L) & 1u) << 1);
+    }
+    if (v == 2) {
+      if (dbg0 && lane == 0) { dbg0[alen] = '-'; dbg1[alen] = S.h2[j - 1] & 15u; }
+      --j;
+    } else if (v == 3) {
+      if (dbg0 && lane == 0) { dbg0[alen] = S.h1[i - 1] & 15u; dbg1[alen] = '-'; }
+      --i;
+    } else {
+      ok = false;
+      break;
+    }
+    ++alen;
+  }
+  __syncwarp();
+  if (!ok) {
+    if (lane == 0) atomicOr(err_word, DERR_TRACEBACK);
+    return false;
+  }
+  if (dbg_len && lane == 0) *dbg_len = alen;
+  *ham_out = ham;
+  return true;
+}
+
 template <int K>
 __device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8_t* g2, int len2, int match,
                               int mismatch, int gap, int homo_gap, int band, bool homo, const RmSmem& S,
@@ -1972,81 +2055,225 @@ __device__ bool rm_align_warp(int lane, const uint8_t* g1, int len1, const uint8
     }
   }
   __syncwarp();
-  // Traceback (src/nwalign.rs:234-273): row 0 moves left, column 0 moves up.
-  // A window of kRmStageRows anti-diagonals of pointer planes is staged in
-  // shared memory; lane k tests whether the k-th next step is diagonal (cell
-  // (i-k, j-k): anti-diagonal t-2k, same offset), so a run of f diagonal
-  // steps is taken at once, one per lane. Other steps are taken singly.
-  for (int p = lane; p < len2; p += 32) S.tcode[p] = uint8_t(kUnaligned | (((S.h2[p] & 15u) - 1u) * 5u));
-  int i = len1, j = len2, slo = 0x7fffffff;
-  uint32_t ham = 0, alen = 0;
-  bool ok = true;
-  __syncwarp();
-  while (i > 0 || j > 0) {
-    int v;
-    if (i == 0) v = 2;
-    else if (j == 0) v = 3;
-    else {
-      const int o = j - i, t = i + j;
-      if (o < o_lo || o > o_hi) { ok = false; break; }
-      if (t < slo || (t - slo < kRmStageRows / 2 && slo > 0)) {  // keep half a window below t
-        const int nlo = max(0, t - (kRmStageRows - 1));
-        __syncwarp();
-        const int nw = (t - nlo + 1) * 2 * K;
-        const uint32_t* src = pscr + size_t(nlo) * (2 * K);
-        for (int x = lane; x < nw; x += 32) S.stage[x] = src[x];
-        __syncwarp();
-        slo = nlo;
-      }
-      const int q = (o - o_lo) >> 1, L = q & 31, m = q >> 5;
-      const int tk = t - 2 * lane;
-      bool diag = false;
-      if (tk >= slo && i - lane >= 1 && j - lane >= 1) {
-        const uint32_t* wk = S.stage + (tk - slo) * (2 * K) + 2 * m;
-        diag = (((wk[0] >> L) & 1u) | (((wk[1] >> L) & 1u) << 1)) == 1u;
-      }
-      const uint32_t nd = __ballot_sync(FULL, !diag);
-      const int f = nd ? __ffs(nd) - 1 : 32;
-      if (f > 0) {
-        bool mm = false;
-        if (lane < f) {
-          const uint8_t a = S.h1[i - 1 - lane] & 15u, b = S.h2[j - 1 - lane] & 15u;
-          S.tcode[j - 1 - lane] = uint8_t((unsigned(a) - 1u) * 4u + (unsigned(b) - 1u));
-          mm = a != b;
-          if (dbg0) {
-            dbg0[alen + lane] = a;
-            dbg1[alen + lane] = b;
-          }
-        }
-        ham += __popc(__ballot_sync(FULL, mm));
-        i -= f;
-        j -= f;
-        alen += uint32_t(f);
-        continue;
-      }
-      const uint32_t* w = S.stage + (t - slo) * (2 * K) + 2 * m;
-      v = int((w[0] >> L) & 1u) | (int((w[1] >> L) & 1u) << 1);
-    }
-    if (v == 2) {
-      if (dbg0 && lane == 0) { dbg0[alen] = '-'; dbg1[alen] = S.h2[j - 1] & 15u; }
-      --j;
-    } else if (v == 3) {
-      if (dbg0 && lane == 0) { dbg0[alen] = S.h1[i - 1] & 15u; dbg1[alen] = '-'; }
-      --i;
-    } else {
-      ok = false;
-      break;
-    }
-    ++alen;
+  return rm_traceback<K>(lane, len1, len2, o_lo, o_hi, S, pscr, ham_out, err_word, dbg0, dbg1, dbg_len);
+}
+
+// Cooperative form of rm_align_warp for calls that carry few pairs: the
+// kNwWarps warps of a CTA share one pair. Warp w owns lane groups
+// [w G, (w + 1) G) of the K (G = K / NW, NW = min(K, kNwWarps) warps; the
+// others only keep the barriers), so each warp computes G groups per
+// anti-diagonal instead of K. The values at a warp boundary -- lane 31 of a
+// warp's last group and lane 0 of its first -- pass through shared memory
+// (xch[(side * 2 + (t & 1)) * kNwWarps + warp]) with one __syncthreads per
+// anti-diagonal. Every warp of the CTA calls this with the same pair, and
+// every branch depends on the pair alone, so the barriers line up. S and
+// pscr are warp 0's; warp 0 takes the traceback and returns the result, the
+// other warps return false.
+template <int K>
+__device__ bool rm_align_coop(int lane, int wib, const uint8_t* g1, int len1, const uint8_t* g2, int len2, int match,
+                              int mismatch, int gap, int homo_gap, int band, bool homo, const RmSmem& S,
+                              uint32_t* pscr, uint32_t* ham_out, uint32_t* err_word, int* xch) {
+  constexpr int NW = K < kNwWarps ? K : kNwWarps;
+  constexpr int G = K / NW;
+  if (wib == 0) {
+    code_mask_warp(lane, g1, len1, S.h1, homo);
+    code_mask_warp(lane, g2, len2, S.h2, homo);
   }
-  __syncwarp();
-  if (!ok) {
-    if (lane == 0) atomicOr(err_word, DERR_TRACEBACK);
+  int o_lo, o_hi;
+  if (band >= 0) {
+    const int lband = band + (len1 > len2 ? len1 - len2 : 0);
+    const int rband = band + (len2 > len1 ? len2 - len1 : 0);
+    o_lo = max(-lband, -len1);
+    o_hi = min(rband, len2);
+  } else {
+    o_lo = -len1;
+    o_hi = len2;
+  }
+  const int P = (o_hi - o_lo + 2) / 2;
+  if (P > 32 * K) {
+    if (wib == 0 && lane == 0) atomicOr(err_word, DERR_UNSUPPORTED);
     return false;
   }
-  if (dbg_len && lane == 0) *dbg_len = alen;
-  *ham_out = ham;
-  return true;
+  // before the first anti-diagonal every neighbour holds the sentinel
+  if (threadIdx.x < 4 * kNwWarps) xch[threadIdx.x] = kNegSentinel;
+  __syncthreads();  // the code bytes and the exchange slots are ready
+  const bool act = wib < NW;
+  const int m0 = wib * G;
+  const int hgap = homo ? homo_gap : gap;
+  struct Cost {
+    int gu, gl, sd;
+    bool cell, edge;
+  };
+  uint32_t inb = 0;  // bit 2g + p: q < P and o_lo + 2q + p <= o_hi, q = lane + 32 (m0 + g)
+#pragma unroll
+  for (int g = 0; g < G; ++g) {
+    const int q = lane + 32 * (m0 + g);
+#pragma unroll
+    for (int p = 0; p < 2; ++p)
+      if (q < P && o_lo + 2 * q + p <= o_hi) inb |= 1u << (2 * g + p);
+  }
+  const unsigned cl1 = unsigned(len1 > 0 ? len1 - 1 : 0), cl2 = unsigned(len2 > 0 ? len2 - 1 : 0);
+  uint32_t xb[G], yb[G];
+  auto cost_of = [&](int E, int g, auto par_tag, auto ld_tag) {
+    constexpr int PN = decltype(par_tag)::value;
+    constexpr int LD = decltype(ld_tag)::value;
+    const int q = lane + 32 * (m0 + g);
+    const int i = E - q, j = E + q + o_lo + PN;
+    if (LD & 1) xb[g] = S.h1[min(unsigned(i - 1), cl1)];
+    if (LD & 2) yb[g] = S.h2[min(unsigned(j - 1), cl2)];
+    const uint32_t x = xb[g], y = yb[g];
+    const bool inband = (inb >> (2 * g + PN)) & 1u;
+    Cost c;
+    c.cell = inband && unsigned(i - 1) < unsigned(len1) && unsigned(j - 1) < unsigned(len2);
+    c.edge = inband && !c.cell && unsigned(i) <= unsigned(len1) && unsigned(j) <= unsigned(len2);
+    c.gu = (j == len2) ? 0 : ((x & 16u) ? hgap : gap);
+    c.gl = (i == len1) ? 0 : ((y & 16u) ? hgap : gap);
+    c.sd = ((x ^ y) & 15u) == 0u ? match : mismatch;
+    return c;
+  };
+  using Even = std::integral_constant<int, 0>;
+  using Odd = std::integral_constant<int, 1>;
+  using LoadX = std::integral_constant<int, 1>;
+  using LoadY = std::integral_constant<int, 2>;
+  using LoadXY = std::integral_constant<int, 3>;
+  auto X = [&](int side, int par, int w) -> int& { return xch[(side * 2 + par) * kNwWarps + w]; };
+  int ve[G], vo[G];
+  Cost cur[G];
+  {
+    const int p0 = o_lo & 1;  // parity of t = 0
+    const int E0 = (0 - o_lo - p0) >> 1;
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      ve[g] = kNegSentinel;
+      vo[g] = kNegSentinel;
+      cur[g] = p0 ? cost_of(E0, g, Odd{}, LoadXY{}) : cost_of(E0, g, Even{}, LoadXY{});
+    }
+  }
+  uint32_t pw[2 * G];
+#pragma unroll
+  for (int g = 0; g < 2 * G; ++g) pw[g] = 0;
+  const int tmax = len1 + len2;
+  auto diag = [&](int t, auto par_tag) {
+    constexpr int PAR = decltype(par_tag)::value;
+    if (act) {
+      Cost nxt[G];
+      const int En = (t - o_lo + PAR) >> 1;  // E of anti-diagonal t + 1 (parity 1 - PAR)
+#pragma unroll
+      for (int g = 0; g < G; ++g) {  // past tmax: unused
+        if (PAR) nxt[g] = cost_of(En, g, Even{}, LoadX{});
+        else nxt[g] = cost_of(En, g, Odd{}, LoadY{});
+      }
+      const int pt = (t - 1) & 1;  // the exchange slot of anti-diagonal t - 1
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        const int q = lane + 32 * (m0 + g);
+        const int own = PAR ? vo[g] : ve[g];
+        int left_nb, up_nb;
+        if (PAR == 0) {
+          const int a = __shfl_up_sync(FULL, vo[g], 1);
+          int a31;
+          if (g > 0) a31 = __shfl_sync(FULL, vo[g > 0 ? g - 1 : 0], 31);
+          else a31 = wib > 0 ? X(0, pt, wib > 0 ? wib - 1 : 0) : kNegSentinel;
+          left_nb = (lane == 0) ? a31 : a;
+          if (q == 0) left_nb = kNegSentinel;
+          up_nb = vo[g];
+        } else {
+          const int b = __shfl_down_sync(FULL, ve[g], 1);
+          int b0;
+          if (g + 1 < G) b0 = __shfl_sync(FULL, ve[g + 1 < G ? g + 1 : g], 0);
+          else b0 = wib + 1 < NW ? X(1, pt, wib + 1 < NW ? wib + 1 : wib) : kNegSentinel;
+          up_nb = (lane == 31) ? b0 : b;
+          if (q + 1 >= P) up_nb = kNegSentinel;
+          left_nb = ve[g];
+        }
+        const int up = up_nb + cur[g].gu;
+        const int left = left_nb + cur[g].gl;
+        const int dg = own + cur[g].sd;
+        const bool upw = up >= dg && up >= left;
+        const bool lw = !upw && left >= dg;
+        int val = upw ? up : (lw ? left : dg);
+        uint32_t code = upw ? 3u : (lw ? 2u : 1u);
+        if (!cur[g].cell) {
+          val = cur[g].edge ? 0 : kNegSentinel;
+          code = 0u;
+        }
+        if (PAR) vo[g] = val;
+        else ve[g] = val;
+        const uint32_t b0w = __ballot_sync(FULL, code & 1u);
+        const uint32_t b1w = __ballot_sync(FULL, code & 2u);
+        if (lane == (t & 31)) {
+          pw[2 * g] = b0w;
+          pw[2 * g + 1] = b1w;
+        }
+      }
+      // this anti-diagonal's boundary values for the neighbouring warps
+      if (lane == 31) X(0, t & 1, wib) = PAR ? vo[G - 1] : ve[G - 1];
+      if (lane == 0) X(1, t & 1, wib) = PAR ? vo[0] : ve[0];
+      if ((t & 31) == 31 || t == tmax) {
+        const int base = t & ~31;
+        if (base + lane <= t) {
+          uint32_t* dst = pscr + size_t(base + lane) * (2 * K) + 2 * m0;
+#pragma unroll
+          for (int g = 0; g < 2 * G; ++g) dst[g] = pw[g];
+        }
+      }
+#pragma unroll
+      for (int g = 0; g < G; ++g) cur[g] = nxt[g];
+    }
+    __syncthreads();
+  };
+  if ((o_lo & 1) == 0) {  // t = 0 has parity 0
+    for (int t = 0; t <= tmax; t += 2) {
+      diag(t, Even{});
+      if (t + 1 <= tmax) diag(t + 1, Odd{});
+    }
+  } else {
+    for (int t = 0; t <= tmax; t += 2) {
+      diag(t, Odd{});
+      if (t + 1 <= tmax) diag(t + 1, Even{});
+    }
+  }
+  // the last __syncthreads made every warp's pointer planes visible
+  if (wib != 0) return false;
+  return rm_traceback<K>(lane, len1, len2, o_lo, o_hi, S, pscr, ham_out, err_word, nullptr, nullptr, nullptr);
+}
+
+// rm_dispatch for the cooperative form: every warp of the CTA calls it with
+// the same pair; a pair that needs one lane group runs on warp 0 alone.
+__device__ bool rm_dispatch_coop(int lane, int wib, const uint8_t* g1, int len1, const uint8_t* g2, int len2,
+                                 const KParams& kp, bool homo, int kbound, const RmSmem& S, uint32_t* pscr,
+                                 uint32_t* ham, uint32_t* err_word, int* xch) {
+  int o_lo, o_hi;
+  if (kp.band >= 0) {
+    const int lband = kp.band + (len1 > len2 ? len1 - len2 : 0);
+    const int rband = kp.band + (len2 > len1 ? len2 - len1 : 0);
+    o_lo = max(-lband, -len1);
+    o_hi = min(rband, len2);
+  } else {
+    o_lo = -len1;
+    o_hi = len2;
+  }
+  const int P = (o_hi - o_lo + 2) / 2;
+  const int need = (P + 31) / 32;
+  if (need > kbound) {
+    if (wib == 0 && lane == 0) atomicOr(err_word, DERR_UNSUPPORTED);
+    return false;
+  }
+  if (need <= 1) {
+    if (wib != 0) return false;
+    return rm_align_warp<1>(lane, g1, len1, g2, len2, kp.match, kp.mismatch, kp.gap, kp.homo_gap, kp.band, homo, S,
+                            pscr, ham, err_word, nullptr, nullptr, nullptr);
+  }
+#define RM_COOP_CASE(KK)                                                                                            \
+  if (need <= KK)                                                                                                   \
+    return rm_align_coop<KK>(lane, wib, g1, len1, g2, len2, kp.match, kp.mismatch, kp.gap, kp.homo_gap, kp.band,    \
+                             homo, S, pscr, ham, err_word, xch);
+  RM_COOP_CASE(2)
+  RM_COOP_CASE(4)
+  RM_COOP_CASE(8)
+  RM_COOP_CASE(16)
+#undef RM_COOP_CASE
+  return false;
 }
 
 __device__ RmSmem carve_rm(unsigned char* base, int lmax, int kbound) {
@@ -2112,10 +2339,16 @@ struct PairResult {
   const uint8_t* qual;
 };
 
+// COOP: every warp of the CTA calls this with the same pair and warp 0's
+// buffers (VS, RS, scratch); the row-major DP is shared (rm_dispatch_coop),
+// everything else is warp 0's, and only warp 0's result is meaningful. It is
+// used only in launches whose geometry rules out the register form, so every
+// NW pair of such a launch is row-major.
+template <bool COOP>
 __device__ __forceinline__ PairResult align_pair(int lane, const KParams& kp, const PoolDev& pool, const NwGeom& geom,
                                                  uint32_t g, uint32_t c, double kdist, bool want_qual,
                                                  const VecSmem& VS, const RmSmem& RS, int kb, uint8_t* scratch,
-                                                 uint32_t* err_word) {
+                                                 uint32_t* err_word, int wib = 0, int* xch = nullptr) {
   const int k = kp.kmer_size;
   const int lc = int(pool.len[c]), lg = int(pool.len[g]);
   const uint8_t* sc = pool.seq + pool.off[c];
@@ -2123,7 +2356,7 @@ __device__ __forceinline__ PairResult align_pair(int lane, const KParams& kp, co
   const uint8_t* qg = pool.qual ? pool.qual + pool.off[g] : nullptr;
   const bool use_homo = kp.homo_gap != kp.gap && kp.homo_gap <= 0;
   const bool rm = use_homo || !kp.vectorized || lc > 3500 || lg > 3500;
-  if (!rm) {
+  if (!COOP && !rm) {
     const bool swap = lc > lg;
     uint8_t* dc = swap ? VS.s2 : VS.s1;
     uint8_t* dg = swap ? VS.s1 : VS.s2;
@@ -2165,20 +2398,24 @@ __device__ __forceinline__ PairResult align_pair(int lane, const KParams& kp, co
   if (gapless) {
     // raw position p aligns to center position p while p < len(center)
     uint8_t* tcode = rm ? RS.tcode : VS.tcode;
-    for (int p = lane; p < lg; p += 32) {
+    for (int p = (!COOP || wib == 0) ? lane : lg; p < lg; p += 32) {
       const unsigned r = sg[p];
       const unsigned code = (p < lc) ? (unsigned(sc[p]) - 1u) * 4u + (r - 1u) : (kUnaligned | ((r - 1u) * 5u));
       const bool valid = r >= 1u && r <= 4u && (p >= lc || (sc[p] >= 1 && sc[p] <= 4));
       tcode[p] = uint8_t(valid ? code : 255u);
     }
     R.method = AM_GAPLESS;
-  } else if (!rm) {
+  } else if (!COOP && !rm) {
     R.ok = vec_align_any(lane, sc, lc, sg, lg, int16_t(kp.match), int16_t(kp.mismatch), int16_t(kp.gap), 0, kp.band,
                          VS, scratch, geom.vec_ncol, geom.vec_nrow, &ham, err_word, nullptr, nullptr, nullptr, true);
     R.method = AM_VECTORIZED;
   } else {
-    R.ok = rm_dispatch(lane, sc, lc, sg, lg, kp, use_homo, kb, RS, reinterpret_cast<uint32_t*>(scratch), &ham,
-                       err_word, nullptr, nullptr, nullptr);
+    if (COOP)
+      R.ok = rm_dispatch_coop(lane, wib, sc, lc, sg, lg, kp, use_homo, kb, RS, reinterpret_cast<uint32_t*>(scratch),
+                              &ham, err_word, xch);
+    else
+      R.ok = rm_dispatch(lane, sc, lc, sg, lg, kp, use_homo, kb, RS, reinterpret_cast<uint32_t*>(scratch), &ham,
+                         err_word, nullptr, nullptr, nullptr);
     R.tcode = RS.tcode;
     R.fidx = RS.fidx;
     R.method = use_homo ? AM_HOMO : AM_ENDSFREE;
@@ -2204,33 +2441,23 @@ __global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_align(Compar
   for (int t = threadIdx.x; t < nerr; t += blockDim.x) err_s[t] = L.pool.err[t];
   cudaGridDependencySynchronize();  // the screen's pass queue and results are complete
   const uint32_t count = *(volatile uint32_t*)&L.queue_counts[4];
-  if (blockIdx.x * kNwWarps >= count) return;  // nothing queued for this block
+  const int kb = rm_kbound(L.geom.rm_pairs);
+  // Few pairs of a launch whose NW pairs are all row-major and span two or
+  // more lane groups: the CTA's warps share each pair (rm_align_coop), which
+  // cuts a long pair's latency, the bound of such calls.
+  const bool coop = L.geom.vec_scratch == 0 && kb >= 2 && count <= 2u * gridDim.x;
+  if (blockIdx.x * (coop ? 1u : uint32_t(kNwWarps)) >= count) return;  // nothing queued for this block
   const size_t err_bytes = err_smem_bytes(kp.ncol);
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int gw = blockIdx.x * kNwWarps + wib;
-  const int kb = rm_kbound(L.geom.rm_pairs);
   unsigned char* wbase = smem_raw + err_bytes + size_t(wib) * align_smem_per_warp(L.geom);
   const VecSmem VS = carve_vec(wbase, L.geom.lmax, L.geom.vec_ncol);
   const RmSmem RS = carve_rm(wbase, L.geom.lmax, kb);
   const size_t scr_stride = L.geom.vec_scratch > L.geom.rm_scratch ? L.geom.vec_scratch : L.geom.rm_scratch;
   uint8_t* scratch = L.nw_scratch + size_t(gw) * scr_stride;
   __syncthreads();
-  // Warps claim queue slots one at a time from a shared cursor (cleared with
-  // the other counters after each call), so pairs of unequal cost -- gapless
-  // against NW, short against long -- and CTAs that become resident late
-  // (when shared memory admits fewer CTAs per SM than the grid assumes) even
-  // out. Results go to each raw's own entries, so the order is free.
-  for (;;) {
-    uint32_t slot = 0;
-    if (lane == 0) slot = atomicAdd(&L.queue_counts[6], 1u);
-    slot = __shfl_sync(FULL, slot, 0);
-    if (slot >= count) break;
-    const uint32_t item = L.queue_pass[slot];
-    const uint32_t t = find_task(L.task_prefix, L.ntask, item);
-    const TaskDev T = L.tasks[t];
-    const uint32_t g = T.base + (item - L.task_prefix[t]);
-    const PairResult R = align_pair(lane, kp, L.pool, L.geom, g, T.center, L.pool.res_lambda[g], kp.use_quals != 0, VS,
-                                    RS, kb, scratch, L.err_word);
+  // lambda and the raw's result entries, by the warp that holds the alignment
+  auto finish = [&](const PairResult& R, uint32_t g) {
     double lam = 0.0;
     float ll32 = -INFINITY;
     if (R.ok) {
@@ -2250,6 +2477,65 @@ __global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_align(Compar
       L.pool.res_status[g] = uint8_t(ST_ALIGNED | (R.method << 2));
     }
     __syncwarp();
+  };
+  if (coop) {
+    // Thread 0 claims a slot for the CTA and reads the raw's screen distance
+    // (which warp 0 overwrites with lambda when the pair is done) into shared
+    // memory, so every warp takes the same branches through the pair and the
+    // barriers inside the shared DP line up. Warp 0's buffers hold the pair.
+    __shared__ uint32_t s_slot;
+    __shared__ double s_kdist;
+    __shared__ int s_xch[4 * kNwWarps];
+    unsigned char* w0 = smem_raw + err_bytes;
+    const VecSmem VS0 = carve_vec(w0, L.geom.lmax, L.geom.vec_ncol);
+    const RmSmem RS0 = carve_rm(w0, L.geom.lmax, kb);
+    uint8_t* scratch0 = L.nw_scratch + size_t(blockIdx.x) * kNwWarps * scr_stride;
+    auto raw_of = [&](uint32_t slot, uint32_t* center) {
+      const uint32_t item = L.queue_pass[slot];
+      const uint32_t t = find_task(L.task_prefix, L.ntask, item);
+      const TaskDev T = L.tasks[t];
+      *center = T.center;
+      return T.base + (item - L.task_prefix[t]);
+    };
+    for (;;) {
+      if (threadIdx.x == 0) {
+        const uint32_t sl = atomicAdd(&L.queue_counts[6], 1u);
+        s_slot = sl;
+        if (sl < count) {
+          uint32_t c0;
+          s_kdist = L.pool.res_lambda[raw_of(sl, &c0)];
+        }
+      }
+      __syncthreads();
+      const uint32_t slot = s_slot;
+      const double kdist = slot < count ? s_kdist : 0.0;
+      __syncthreads();  // every thread has read the slot before thread 0 claims again
+      if (slot >= count) break;
+      uint32_t center;
+      const uint32_t g = raw_of(slot, &center);
+      const PairResult R = align_pair<true>(lane, kp, L.pool, L.geom, g, center, kdist, kp.use_quals != 0, VS0, RS0,
+                                            kb, scratch0, L.err_word, wib, s_xch);
+      if (wib == 0) finish(R, g);
+    }
+    return;
+  }
+  // Warps claim queue slots one at a time from a shared cursor (cleared with
+  // the other counters after each call), so pairs of unequal cost -- gapless
+  // against NW, short against long -- and CTAs that become resident late
+  // (when shared memory admits fewer CTAs per SM than the grid assumes) even
+  // out. Results go to each raw's own entries, so the order is free.
+  for (;;) {
+    uint32_t slot = 0;
+    if (lane == 0) slot = atomicAdd(&L.queue_counts[6], 1u);
+    slot = __shfl_sync(FULL, slot, 0);
+    if (slot >= count) break;
+    const uint32_t item = L.queue_pass[slot];
+    const uint32_t t = find_task(L.task_prefix, L.ntask, item);
+    const TaskDev T = L.tasks[t];
+    const uint32_t g = T.base + (item - L.task_prefix[t]);
+    const PairResult R = align_pair<false>(lane, kp, L.pool, L.geom, g, T.center, L.pool.res_lambda[g],
+                                           kp.use_quals != 0, VS, RS, kb, scratch, L.err_word);
+    finish(R, g);
   }
 }
 
@@ -2309,7 +2595,7 @@ __global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_final_subs(F
       bound = 0;
     }
     bound += add;
-    const PairResult R = align_pair(lane, kp, F.pool, F.geom, g, c, 0.0, F.has_quals != 0, VS, RS, kb, scratch,
+    const PairResult R = align_pair<false>(lane, kp, F.pool, F.geom, g, c, 0.0, F.has_quals != 0, VS, RS, kb, scratch,
                                     F.err_word);
     if (!R.ok) continue;  // the error word reports it
     const uint32_t reads = F.pool.reads[g];
