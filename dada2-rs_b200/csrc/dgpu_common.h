@@ -93,7 +93,15 @@ struct NwGeom {
   int32_t nwarps;      // resident warps of the persistent NW kernels
   size_t vec_scratch;  // bytes per warp (pointer matrix)
   size_t rm_scratch;   // bytes per warp (pointer bit planes)
+  int32_t forms;       // the aligner forms a compare launch can reach (kForms*)
 };
+// Aligner forms a compare launch can reach, fixed by the pool's geometry and
+// parameters; k_align is compiled once per set, so a launch runs only the code
+// it can use (a smaller kernel: fewer instruction-cache misses in the
+// latency-bound late calls, and no register pressure from unused forms).
+constexpr int32_t kFormsAll = 0;   // every form
+constexpr int32_t kFormsVec1 = 1;  // gapless and the fast register form with one lane group
+constexpr int32_t kFormsRm = 2;    // gapless and the row-major forms
 
 // ---- shared-memory carving, used by kernels and by the host sizing code ----
 constexpr int kScreenWarps = 8;   // warps per screen CTA

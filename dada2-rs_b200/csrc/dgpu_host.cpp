@@ -717,6 +717,16 @@ struct Pool {
     geom.vec_scratch = vec_possible ? align16(size_t(geom.vec_nrow) * std::max<size_t>(size_t(geom.vec_ncol), 32)) : 0;
     geom.rm_scratch = rm_possible ? align16(size_t(2 * lmax + 1) * 2 * kb * 4) : 0;
     geom.nwarps = sms * tuning_for(lmax).align_ctas_per_sm * kNwWarps;
+    // the forms k_align can reach (vec_align_any takes the fast register form
+    // with one lane group for every pair when the compressed width is <= 32,
+    // gaps are not positive and no sum can saturate i16)
+    geom.forms = kFormsAll;
+    if (rm_possible && !vec_possible) {
+      geom.forms = kFormsRm;
+    } else if (vec_possible && !rm_possible) {
+      const int64_t pmax = std::max<int64_t>({int64_t(kp.match), int64_t(kp.mismatch), 0});
+      if (geom.vec_ncol <= 32 && kp.gap <= 0 && pmax * (int64_t(lmax) + 1) <= 32767) geom.forms = kFormsVec1;
+    }
     const size_t per = std::max<size_t>(std::max(geom.vec_scratch, geom.rm_scratch), 16);
     slots.clear();
     for (int k = 0; k < nslots; ++k) {

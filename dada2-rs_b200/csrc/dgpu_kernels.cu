@@ -1711,6 +1711,10 @@ __device__ bool vec_align_fast(int lane, int len1, int len2, int match, int mism
 // Picks the register form when the pair's compressed width fits 128 columns.
 // With `staged` the caller has already put the shorter sequence (the first on
 // ties) in S.s1 and the other in S.s2, and g1/g2 point at those copies.
+// ONLY_M1: the caller has shown that every pair takes the fast form with one
+// lane group (kFormsVec1); the other forms are not compiled in, and a pair
+// outside it is refused.
+template <bool ONLY_M1 = false>
 __device__ bool vec_align_any(int lane, const uint8_t* g1, int l1, const uint8_t* g2, int l2, int16_t match,
                               int16_t mismatch, int16_t gap, int16_t egp, int band_in, const VecSmem& S,
                               uint8_t* scratch, int ncol_bound, int nrow_bound, uint32_t* ham_out, uint32_t* err_word,
@@ -1724,6 +1728,10 @@ __device__ bool vec_align_any(int lane, const uint8_t* g1, int l1, const uint8_t
   const int pmax = max(max(int(match), int(mismatch)), 0);
   const bool fast = ncol >= 4 && ncol <= 128 && len1 >= 1 && nrow <= nrow_bound && gap <= 0 && egp <= 0 &&
                     pmax * ((len1 + len2) / 2 + 1) <= 32767;
+  if (ONLY_M1 && !(fast && ncol <= 32)) {
+    if (lane == 0) atomicOr(err_word, DERR_UNSUPPORTED);
+    return false;
+  }
   if (fast) {
     const bool swap = l1 > l2;
     {
@@ -1752,14 +1760,17 @@ __device__ bool vec_align_any(int lane, const uint8_t* g1, int l1, const uint8_t
       if (swap) VEC_FAST(1, true);
       VEC_FAST(1, false);
     }
-    if (mw == 2) {
-      if (swap) VEC_FAST(2, true);
-      VEC_FAST(2, false);
+    if constexpr (!ONLY_M1) {
+      if (mw == 2) {
+        if (swap) VEC_FAST(2, true);
+        VEC_FAST(2, false);
+      }
+      if (swap) VEC_FAST(4, true);
+      VEC_FAST(4, false);
     }
-    if (swap) VEC_FAST(4, true);
-    VEC_FAST(4, false);
 #undef VEC_FAST
   }
+  if constexpr (ONLY_M1) return false;  // not reached: refused above
   if (ncol <= 32)
     return vec_align_reg<1>(lane, g1, l1, g2, l2, match, mismatch, gap, egp, band_in, S, w, nrow_bound, ham_out,
                             err_word, dbg0, dbg1, dbg_len);
@@ -2344,7 +2355,9 @@ struct PairResult {
 // everything else is warp 0's, and only warp 0's result is meaningful. It is
 // used only in launches whose geometry rules out the register form, so every
 // NW pair of such a launch is row-major.
-template <bool COOP>
+// FORMS (kForms*): the forms this launch can reach; the others are not
+// compiled in, and a pair that would need one is refused.
+template <bool COOP, int FORMS = kFormsAll>
 __device__ __forceinline__ PairResult align_pair(int lane, const KParams& kp, const PoolDev& pool, const NwGeom& geom,
                                                  uint32_t g, uint32_t c, double kdist, bool want_qual,
                                                  const VecSmem& VS, const RmSmem& RS, int kb, uint8_t* scratch,
@@ -2355,7 +2368,12 @@ __device__ __forceinline__ PairResult align_pair(int lane, const KParams& kp, co
   const uint8_t* sg = pool.seq + pool.off[g];
   const uint8_t* qg = pool.qual ? pool.qual + pool.off[g] : nullptr;
   const bool use_homo = kp.homo_gap != kp.gap && kp.homo_gap <= 0;
-  const bool rm = use_homo || !kp.vectorized || lc > 3500 || lg > 3500;
+  const bool rm_pair = use_homo || !kp.vectorized || lc > 3500 || lg > 3500;
+  const bool rm = FORMS == kFormsRm ? true : (FORMS == kFormsVec1 ? false : rm_pair);
+  if (rm != rm_pair) {
+    if (lane == 0) atomicOr(err_word, DERR_UNSUPPORTED);
+    return PairResult{false, AM_NONE, 0u, lg, VS.tcode, VS.fidx, qg};
+  }
   if (!COOP && !rm) {
     const bool swap = lc > lg;
     uint8_t* dc = swap ? VS.s2 : VS.s1;
@@ -2406,16 +2424,19 @@ __device__ __forceinline__ PairResult align_pair(int lane, const KParams& kp, co
     }
     R.method = AM_GAPLESS;
   } else if (!COOP && !rm) {
-    R.ok = vec_align_any(lane, sc, lc, sg, lg, int16_t(kp.match), int16_t(kp.mismatch), int16_t(kp.gap), 0, kp.band,
+    R.ok = vec_align_any<FORMS == kFormsVec1>(lane, sc, lc, sg, lg, int16_t(kp.match), int16_t(kp.mismatch),
+                                              int16_t(kp.gap), 0, kp.band,
                          VS, scratch, geom.vec_ncol, geom.vec_nrow, &ham, err_word, nullptr, nullptr, nullptr, true);
     R.method = AM_VECTORIZED;
   } else {
-    if (COOP)
-      R.ok = rm_dispatch_coop(lane, wib, sc, lc, sg, lg, kp, use_homo, kb, RS, reinterpret_cast<uint32_t*>(scratch),
-                              &ham, err_word, xch);
-    else
-      R.ok = rm_dispatch(lane, sc, lc, sg, lg, kp, use_homo, kb, RS, reinterpret_cast<uint32_t*>(scratch), &ham,
-                         err_word, nullptr, nullptr, nullptr);
+    if constexpr (FORMS != kFormsVec1) {
+      if (COOP)
+        R.ok = rm_dispatch_coop(lane, wib, sc, lc, sg, lg, kp, use_homo, kb, RS, reinterpret_cast<uint32_t*>(scratch),
+                                &ham, err_word, xch);
+      else
+        R.ok = rm_dispatch(lane, sc, lc, sg, lg, kp, use_homo, kb, RS, reinterpret_cast<uint32_t*>(scratch), &ham,
+                           err_word, nullptr, nullptr, nullptr);
+    }
     R.tcode = RS.tcode;
     R.fidx = RS.fidx;
     R.method = use_homo ? AM_HOMO : AM_ENDSFREE;
@@ -2431,6 +2452,7 @@ __device__ __forceinline__ PairResult align_pair(int lane, const KParams& kp, co
 // codes for ACGT input), method choice (src/nwalign.rs:1324-1403), then the
 // gapless alignment or the vectorized / row-major aligner, then lambda.
 // ---------------------------------------------------------------------------
+template <int FORMS>
 __global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_align(CompareLaunch L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cudaTriggerProgrammaticLaunchCompletion();  // the store kernel may start launching
@@ -2445,7 +2467,7 @@ __global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_align(Compar
   // Few pairs of a launch whose NW pairs are all row-major and span two or
   // more lane groups: the CTA's warps share each pair (rm_align_coop), which
   // cuts a long pair's latency, the bound of such calls.
-  const bool coop = L.geom.vec_scratch == 0 && kb >= 2 && count <= 2u * gridDim.x;
+  const bool coop = FORMS != kFormsVec1 && L.geom.vec_scratch == 0 && kb >= 2 && count <= 2u * gridDim.x;
   if (blockIdx.x * (coop ? 1u : uint32_t(kNwWarps)) >= count) return;  // nothing queued for this block
   const size_t err_bytes = err_smem_bytes(kp.ncol);
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -2478,7 +2500,7 @@ __global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_align(Compar
     }
     __syncwarp();
   };
-  if (coop) {
+  if constexpr (FORMS != kFormsVec1) if (coop) {
     // Thread 0 claims a slot for the CTA and reads the raw's screen distance
     // (which warp 0 overwrites with lambda when the pair is done) into shared
     // memory, so every warp takes the same branches through the pair and the
@@ -2513,7 +2535,7 @@ __global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_align(Compar
       if (slot >= count) break;
       uint32_t center;
       const uint32_t g = raw_of(slot, &center);
-      const PairResult R = align_pair<true>(lane, kp, L.pool, L.geom, g, center, kdist, kp.use_quals != 0, VS0, RS0,
+      const PairResult R = align_pair<true, FORMS>(lane, kp, L.pool, L.geom, g, center, kdist, kp.use_quals != 0, VS0, RS0,
                                             kb, scratch0, L.err_word, wib, s_xch);
       if (wib == 0) finish(R, g);
     }
@@ -2533,7 +2555,7 @@ __global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_align(Compar
     const uint32_t t = find_task(L.task_prefix, L.ntask, item);
     const TaskDev T = L.tasks[t];
     const uint32_t g = T.base + (item - L.task_prefix[t]);
-    const PairResult R = align_pair<false>(lane, kp, L.pool, L.geom, g, T.center, L.pool.res_lambda[g],
+    const PairResult R = align_pair<false, FORMS>(lane, kp, L.pool, L.geom, g, T.center, L.pool.res_lambda[g],
                                            kp.use_quals != 0, VS, RS, kb, scratch, L.err_word);
     finish(R, g);
   }
@@ -2818,25 +2840,27 @@ void launch_compare(const CompareLaunch& L0, cudaStream_t st, cudaEvent_t* ev) {
   }
   if (ev) cudaEventRecord(ev[1], st);
   const size_t asm_ = err_smem_bytes(L.kp.ncol) + size_t(kNwWarps) * align_smem_per_warp(L.geom);
-  if (asm_ > 48 * 1024) {  // raise the dynamic shared-memory limit only when a launch needs more
-    static std::atomic<int> limit[64];
+  // the k_align instance for the forms this launch can reach, with its
+  // attributes set once per device (dynamic shared memory above 48 KB, the
+  // largest carveout so that kAlignCtasPerSm CTAs fit beside each other)
+  void (*kalign)(CompareLaunch) = L.geom.forms == kFormsVec1 ? k_align<kFormsVec1>
+                                  : L.geom.forms == kFormsRm ? k_align<kFormsRm>
+                                                             : k_align<kFormsAll>;
+  {
+    const int fi = L.geom.forms == kFormsVec1 ? 1 : (L.geom.forms == kFormsRm ? 2 : 0);
+    static std::atomic<int> limit[3][64];
+    static std::atomic<uint64_t> carved[3];
     int dev = 0;
     cudaGetDevice(&dev);
-    std::atomic<int>& lim = limit[dev & 63];
-    if (int(asm_) > lim.load(std::memory_order_relaxed)) {
-      cudaFuncSetAttribute(k_align, cudaFuncAttributeMaxDynamicSharedMemorySize, int(asm_));
+    std::atomic<int>& lim = limit[fi][dev & 63];
+    if (asm_ > 48 * 1024 && int(asm_) > lim.load(std::memory_order_relaxed)) {
+      cudaFuncSetAttribute(kalign, cudaFuncAttributeMaxDynamicSharedMemorySize, int(asm_));
       lim.store(int(asm_), std::memory_order_relaxed);
     }
-  }
-  {  // ask for the largest shared-memory carveout once per device so that
-     // kAlignCtasPerSm CTAs fit beside each other
-    static std::atomic<uint64_t> carved{0};
-    int dev = 0;
-    cudaGetDevice(&dev);
     const uint64_t bit = uint64_t(1) << (dev & 63);
-    if (!(carved.load(std::memory_order_relaxed) & bit)) {
-      cudaFuncSetAttribute(k_align, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-      carved.fetch_or(bit);
+    if (!(carved[fi].load(std::memory_order_relaxed) & bit)) {
+      cudaFuncSetAttribute(kalign, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+      carved[fi].fetch_or(bit);
     }
   }
   // Programmatic dependent launch: the alignment and store kernels are
@@ -2852,7 +2876,7 @@ void launch_compare(const CompareLaunch& L0, cudaStream_t st, cudaEvent_t* ev) {
   cfg.gridDim = dim3(L.geom.nwarps / kNwWarps);
   cfg.blockDim = dim3(kNwWarps * 32);
   cfg.dynamicSmemBytes = asm_;
-  cudaLaunchKernelEx(&cfg, k_align, L);
+  cudaLaunchKernelEx(&cfg, kalign, L);
   if (ev) cudaEventRecord(ev[2], st);
   if (L.do_store) {
     cfg.gridDim = dim3(L.nstore_blocks);
