@@ -1023,7 +1023,9 @@ def main():
                                    "all_samples": float(sum(r["times"][2] for r in res)),
                                    "note": "shuffle + p-update + bud on the host, last timed step"},
         "last_sample": (lambda r: {"uniques": int(r["nraw"]), "done_s": float(r["times"][1]),
-                                   "compare_s": float(r["times"][0]), "host_s": float(r["times"][2]),
+                                   "compare_s": float(r["times"][0]), "gpu_wait_s": float(r["times"][3]),
+                                   "compare_calls": int(r["counters"]["compare_calls"]),
+                                   "host_s": float(r["times"][2]),
                                    "slot_wait_s": float(r["times"][4]), "job_wait_s": float(r["times"][5]),
                                    "note": "the sample that finished last in the last timed step: its time "
                                            "in compare calls, host phases, waiting for a launch slot and "

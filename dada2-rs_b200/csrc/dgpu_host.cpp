@@ -2737,7 +2737,6 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
     S[s].stats.t_mark = Clock::now();
     ready.push_back(s);
   }
-  double wait = 0.0;
   int rc = 0;
   std::string err_msg;
   std::atomic<int64_t> host_ns{0};
@@ -2834,6 +2833,7 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
           }
         }
         const auto tc = Clock::now();
+        const double w0 = my_wait;
         if (!r) r = L.run_compare(uint32_t(batch.size()), true, &my_wait);
         if (r) {
           std::lock_guard<std::mutex> g(mu);
@@ -2855,6 +2855,7 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
           SampleState& sa = S[sidx];
           sa.absorb(size_t(sa.pending), L, a);
           sa.stats.t_compare += tcmp;
+          sa.stats.t_wait += my_wait - w0;  // the device wait of the calls that carried this sample
           sa.stats.t_mark = Clock::now();
           auto host_phase = [&, sidx] {
             SampleState& ss = S[sidx];
@@ -2889,8 +2890,6 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
             jobs.submit(host_phase, int64_t(S[sidx].n));  // larger samples have the longer chains: serve them first
         }
       }
-      std::lock_guard<std::mutex> g(mu);
-      wait += my_wait;
     };
     const size_t nw = std::min(P.slots.size(), ns);
     std::vector<std::thread> th;
@@ -2901,7 +2900,6 @@ static int run_samples(Pool& P, std::vector<SampleState>& S, const dgpu_align_pa
   const double total = secs(t_start, Clock::now());
   for (auto& ss : S) {
     ss.stats.t_total = ss.stats.t_done >= 0 ? ss.stats.t_done : total;
-    ss.stats.t_wait = wait;
   }
   if (rc) return fail(rc, err_msg);
   return 0;
@@ -3172,7 +3170,6 @@ static int batch_run(Batch& B, dgpu_result** out, const std::function<void(size_
   if (early)
     on_finish = [&](size_t s) {
       dgpu_result* R = finish(S[s], SampleSeqs{B.E.seq, B.E.off.data() + B.bases[s], B.E.len.data() + B.bases[s]});
-      R->times[3] = 0.0;  // the batch's slot wait is not known yet
       released[s] = 1;
       on_done(s, R);
     };

@@ -88,7 +88,8 @@ typedef struct {
  * host spent in shuffle, p-update and bud. times (6 slots, seconds): this
  * sample's compare calls (launch to results), the time from the start of the
  * clustering loop until this sample finished, this sample's host phases
- * (shuffle, p-update, bud), time the host waited on the device, time this
+ * (shuffle, p-update, bud), time the host waited on the device for this
+ * sample's compare calls (a batched call counts for every sample it carries), time this
  * sample waited for a launch slot (ready to launched) and for a host thread
  * (results absorbed to host phase started). */
 typedef struct {
