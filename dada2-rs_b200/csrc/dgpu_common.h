@@ -67,6 +67,17 @@ struct TaskDev {
   uint32_t cluster;       // cluster index i (for the store's update_raw rule)
 };
 
+// The per-call values of a compare launch, at the head of the launch's table
+// upload. A launch replayed from a captured CUDA graph keeps its kernel
+// parameters fixed and takes these from device memory instead (CompareLaunch::
+// hdr); the offsets are from the header's own address.
+struct CallHeader {
+  uint32_t ntask, total_items, screen_chunk, nstore_blocks;
+  uint32_t pivot, cdot_ready, total_cl, pad;
+  uint32_t o_tasks, o_pref, o_clp, o_map;
+};
+static_assert(sizeof(CallHeader) == 48, "the call header has a fixed layout");
+
 // res_status layout: low 2 bits = outcome, next 3 bits = aligner.
 enum : uint8_t { ST_ALIGNED = 0, ST_SKIPPED = 1, ST_SHROUDED = 2 };
 enum : uint8_t { AM_NONE = 0, AM_GAPLESS = 1, AM_VECTORIZED = 2, AM_HOMO = 3, AM_ENDSFREE = 4 };
@@ -203,10 +214,22 @@ struct CompareLaunch {
   // with do_store: the store's first CTA copies *err_word to err_host (mapped
   // host memory) and clears queue_counts for the launch context's next call
   uint32_t* err_host;
+  // null: the fields above are this call's; else the launch is a graph
+  // replay and ntask, total_items, screen_chunk, nstore_blocks, pivot,
+  // cdot_ready, total_cl and the table pointers come from *hdr
+  const CallHeader* hdr;
 };
 // ev (optional): 4 events recorded before the screen and after screen, align
 // and store, for per-kernel device times.
 void launch_compare(const CompareLaunch& L, cudaStream_t st, cudaEvent_t* ev = nullptr);
+// The screen's chunk size for a call of `total` items (launch_compare's rule).
+uint32_t compare_screen_chunk(uint32_t total, uint32_t screen_blocks_per_sm, uint32_t screen_chunk_max);
+// Captures the compare sequence on `st` as a graph for replay with L.hdr set:
+// the screen's full wave, k_pivot_dots when `pivot_dots`, k_align and
+// `store_grid` store CTAs (those past the call's count return at once).
+// Returns 0 and sets *out, or a CUDA error code (nothing is captured then).
+int capture_compare_graph(const CompareLaunch& L, cudaStream_t st, bool pivot_dots, uint32_t store_grid,
+                          cudaGraphExec_t* out);
 
 // Final-subs pass (src/dada.rs:609-673) feeding the transition counts
 // (src/error.rs:194-249): item i realigns raw[i] against center[i]; counts go

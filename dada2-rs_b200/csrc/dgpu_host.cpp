@@ -445,6 +445,15 @@ static dgpu_tuning tuning_class(int c) {
 }
 static dgpu_tuning tuning_for(uint32_t lmax) { return tuning_class(length_class(lmax)); }
 
+// Compare calls replay captured CUDA graphs unless DGPU_COMPARE_GRAPHS=0.
+static bool compare_graphs_on() {
+  static const bool on = [] {
+    const char* e = std::getenv("DGPU_COMPARE_GRAPHS");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 // Launch slots dedicated to the longest chains: DGPU_DEDICATED_SLOTS (0..7) if
 // set, else the tuning table's (1 built in).
 static size_t dedicated_slots(uint32_t lmax) {
@@ -475,8 +484,20 @@ struct Slot {
   std::vector<uint32_t> task_blk0;  // first store CTA of each task in the latest launch
   uint32_t ntask_cap = 0, nblk_cap = 0;
   size_t pack_cap = 0;
+  // Captured compare graphs (k_pivot_dots or not, x store grid), all for the
+  // fixed launch parameters in graph_key; a change there drops them.
+  std::map<uint32_t, cudaGraphExec_t> graphs;
+  CompareLaunch graph_key;
+  bool graphs_failed = false;
+
+  void drop_graphs() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    graphs.clear();
+  }
 
   ~Slot() {
+    if (st) (void)cudaStreamSynchronize(st);
+    drop_graphs();
     if (st && cudaStreamSynchronize(st) == cudaSuccess)  // every block is idle now
       recycle_all(queue_pass, queue_counts, err_dev, scratch, dpack, hpack, blk_counters, err_host, task_self,
                   task_stage);
@@ -812,12 +833,14 @@ int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
     nblk += (task_stage.h[t].n + kStoreSpan - 1) / kStoreSpan;
   }
   TRY(ensure_blocks(nblk));
-  const size_t o_pref = align16(sizeof(TaskDev) * ntask);
+  // header | tasks | task prefix | cluster prefix | store map
+  const size_t o_tasks = align16(sizeof(CallHeader));
+  const size_t o_pref = o_tasks + align16(sizeof(TaskDev) * ntask);
   const size_t o_clp = o_pref + align16(size_t(4) * (ntask + 1));
   const size_t o_map = o_clp + align16(size_t(4) * (ntask + 1));
   const size_t pack_bytes = o_map + align16(size_t(8) * std::max<uint32_t>(nblk, 1));
   TRY(ensure_pack(pack_bytes));
-  std::memcpy(hpack.h, task_stage.h, sizeof(TaskDev) * ntask);
+  std::memcpy(hpack.h + o_tasks, task_stage.h, sizeof(TaskDev) * ntask);
   uint32_t* pref = reinterpret_cast<uint32_t*>(hpack.h + o_pref);
   uint32_t* smap = reinterpret_cast<uint32_t*>(hpack.h + o_map);
   for (uint32_t t = 0; t < ntask; ++t) {
@@ -842,12 +865,29 @@ int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
   clp[ntask] = total_cl;
   const uint32_t min_items = uint32_t(tuning_for(Q.lmax).pivot_min_items);
   const bool cdot_ready = pivot && total_cl > 0 && min_items > 0 && total >= min_items;
+  const dgpu_tuning tu = tuning_for(Q.lmax);
+  {
+    CallHeader& H = *reinterpret_cast<CallHeader*>(hpack.h);
+    H = CallHeader{};
+    H.ntask = ntask;
+    H.total_items = total;
+    H.screen_chunk = compare_screen_chunk(total, uint32_t(tu.screen_blocks_per_sm), uint32_t(tu.screen_chunk_max));
+    H.nstore_blocks = nblk;
+    H.pivot = pivot ? 1u : 0u;
+    H.cdot_ready = cdot_ready ? 1u : 0u;
+    H.total_cl = cdot_ready ? total_cl : 0u;
+    H.o_tasks = uint32_t(o_tasks);
+    H.o_pref = uint32_t(o_pref);
+    H.o_clp = uint32_t(o_clp);
+    H.o_map = uint32_t(o_map);
+  }
   CUDA_TRY(cudaMemcpyAsync(dpack.p, hpack.h, pack_bytes, cudaMemcpyHostToDevice, st));
   count_h2d(pack_bytes);
-  CompareLaunch L{};
+  CompareLaunch L;
+  std::memset(&L, 0, sizeof L);  // padding too: graph_key compares the bytes
   L.pool = Q.view();
   L.kp = Q.kp;
-  L.tasks = reinterpret_cast<const TaskDev*>(dpack.p);
+  L.tasks = reinterpret_cast<const TaskDev*>(dpack.p + o_tasks);
   L.task_prefix = reinterpret_cast<const uint32_t*>(dpack.p + o_pref);
   L.ntask = ntask;
   L.total_items = total;
@@ -868,7 +908,6 @@ int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
   L.do_store = do_store ? 1 : 0;
   L.err_host = err_host.d;
   {
-    const dgpu_tuning tu = tuning_for(Q.lmax);
     L.screen_chunk_max = uint32_t(tu.screen_chunk_max);
     L.screen_blocks_per_sm = uint32_t(tu.screen_blocks_per_sm);
     L.pdl = uint32_t(tu.programmatic_launch);
@@ -879,7 +918,41 @@ int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
   L.total_cl = cdot_ready ? total_cl : 0u;
   const uint64_t every = g_stats.timing_every.load();
   const bool timing = every != 0 && g_stats.call_seq.fetch_add(1) % every == 0;
-  launch_compare(L, st, timing ? ev : nullptr);
+  bool launched = false;
+  if (do_store && !timing && total > 0 && compare_graphs_on() && !graphs_failed) {
+    // Replay a captured graph of the launch sequence: one submission instead
+    // of three or four, which the launch slots' threads otherwise contend
+    // for in the driver. Its kernels take this call's values from the
+    // header just uploaded; the store grid is rounded up (spare CTAs return).
+    CompareLaunch K = L;
+    K.ntask = K.total_items = K.screen_chunk = K.nstore_blocks = 0;
+    K.pivot = K.cdot_ready = K.total_cl = 0;
+    K.tasks = nullptr;
+    K.task_prefix = K.task_cl_prefix = K.store_task = K.store_chunk = nullptr;
+    K.hdr = reinterpret_cast<const CallHeader*>(dpack.p);
+    if (graphs.empty() || std::memcmp(&K, &graph_key, sizeof K) != 0) {
+      drop_graphs();
+      graph_key = K;
+    }
+    uint32_t grid = 8;
+    while (grid < nblk) grid *= 4;
+    const uint32_t key = (grid << 1) | (cdot_ready ? 1u : 0u);
+    auto it = graphs.find(key);
+    if (it == graphs.end()) {
+      cudaGraphExec_t ge = nullptr;
+      if (capture_compare_graph(K, st, cdot_ready, grid, &ge) == 0 && ge) {
+        it = graphs.emplace(key, ge).first;
+      } else {
+        (void)cudaGetLastError();
+        graphs_failed = true;  // direct launches from here on
+      }
+    }
+    if (it != graphs.end()) {
+      CUDA_TRY(cudaGraphLaunch(it->second, st));
+      launched = true;
+    }
+  }
+  if (!launched) launch_compare(L, st, timing ? ev : nullptr);
   CUDA_TRY(cudaGetLastError());
   if (!do_store) {  // no store kernel to rearm the queue or report the flags
     CUDA_TRY(cudaMemcpyAsync(err_host.h, err_dev.p, 4, cudaMemcpyDeviceToHost, st));

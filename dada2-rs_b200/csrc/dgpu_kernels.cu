@@ -276,12 +276,35 @@ __device__ __forceinline__ uint32_t mismatch_word(const uint8_t* a, const uint8_
 
 // Lean streaming screen: greedy skip, profile dot product, strict cutoff
 // (src/cluster.rs:295-298, src/kmers.rs:254-269, src/nwalign.rs:1299).
+// A graph replay's per-call values (CompareLaunch::hdr) into the kernel's
+// own copy of the launch parameters.
+__device__ __forceinline__ void load_call(CompareLaunch& L) {
+  if (!L.hdr) return;
+  const CallHeader H = *L.hdr;
+  const uint8_t* base = reinterpret_cast<const uint8_t*>(L.hdr);
+  L.ntask = H.ntask;
+  L.total_items = H.total_items;
+  L.screen_chunk = H.screen_chunk;
+  L.nstore_blocks = H.nstore_blocks;
+  L.pivot = H.pivot;
+  L.cdot_ready = H.cdot_ready;
+  L.total_cl = H.total_cl;
+  L.tasks = reinterpret_cast<const TaskDev*>(base + H.o_tasks);
+  L.task_prefix = reinterpret_cast<const uint32_t*>(base + H.o_pref);
+  L.task_cl_prefix = reinterpret_cast<const uint32_t*>(base + H.o_clp);
+  L.store_task = reinterpret_cast<const uint32_t*>(base + H.o_map);
+  L.store_chunk = L.store_task + H.nstore_blocks;
+}
+
 // Pivot dots: for every task of the launch and every earlier cluster i of its
 // sample, cdot[base + i] = the u8 k-mer dot of the task's center with cluster
 // i's center (cl_center[base + i]); the screen's pivot bound reads them. One
 // warp per (task, cluster) item, 16-byte vector loads of both profiles.
 template <int K>
-__global__ void __launch_bounds__(256) k_pivot_dots(CompareLaunch L) {
+__global__ void __launch_bounds__(256) k_pivot_dots(CompareLaunch Lp) {
+  CompareLaunch L = Lp;
+  load_call(L);
+  if (!L.cdot_ready) return;
   constexpr int NK16 = (1 << (2 * K)) / 16;
   const int lane = threadIdx.x & 31;
   const uint32_t warps_total = gridDim.x * (blockDim.x >> 5);
@@ -310,7 +333,9 @@ __global__ void __launch_bounds__(256) k_pivot_dots(CompareLaunch L) {
 // center profile held in registers. Survivors go to the align queue with their
 // kdist parked in res_lambda.
 template <int K>
-__global__ void __launch_bounds__(kScreenWarps * 32, 4) k_screen(CompareLaunch L) {
+__global__ void __launch_bounds__(kScreenWarps * 32, 4) k_screen(CompareLaunch Lp) {
+  CompareLaunch L = Lp;
+  load_call(L);
   // every screen block is running: the alignment kernel may start launching
   // (its blocks wait for this grid's results in cudaGridDependencySynchronize)
   cudaTriggerProgrammaticLaunchCompletion();
@@ -2453,7 +2478,9 @@ __device__ __forceinline__ PairResult align_pair(int lane, const KParams& kp, co
 // gapless alignment or the vectorized / row-major aligner, then lambda.
 // ---------------------------------------------------------------------------
 template <int FORMS>
-__global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_align(CompareLaunch L) {
+__global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_align(CompareLaunch Lp) {
+  CompareLaunch L = Lp;
+  load_call(L);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cudaTriggerProgrammaticLaunchCompletion();  // the store kernel may start launching
   const KParams& kp = L.kp;
@@ -2649,7 +2676,10 @@ void launch_final_subs(const FinalSubsLaunch& F, cudaStream_t st) {
 // Each CTA owns kStoreSpan consecutive raws of one task; its stored comps go
 // to that span's own segment of the task's output (so concatenating segments
 // in order gives ascending raw order) with a per-CTA count and counters.
-__global__ void __launch_bounds__(kStoreThreads) k_store(CompareLaunch L) {
+__global__ void __launch_bounds__(kStoreThreads) k_store(CompareLaunch Lp) {
+  CompareLaunch L = Lp;
+  load_call(L);
+  if (blockIdx.x >= L.nstore_blocks) return;  // a replayed graph's spare CTAs
   constexpr int IPT = kStoreSpan / kStoreThreads;
   __shared__ uint32_t warp_off[32];
   __shared__ uint32_t ctr[TC_NCOUNTERS];
@@ -2784,85 +2814,90 @@ static int sm_count() {
   return g_sm_count;
 }
 
-void launch_compare(const CompareLaunch& L0, cudaStream_t st, cudaEvent_t* ev) {
-  if (L0.total_items == 0) return;
+// The screen's chunk for a call of `total` items.
+// One wave: k_screen's 64 registers x 256 threads leave room for 4 blocks
+// per SM. A warp screens its chunk a few items at a time, one dependent
+// round of profile loads each. A call that fits the wave at one chunk per
+// warp takes the smallest chunk that does (its items spread thin over many
+// warps); a larger one takes the largest chunk that still shares the
+// chunks evenly over the wave's warps (at least 90 % of them busy in the
+// last round), so no partial second wave or ragged tail is left; chunks
+// stay at 16 or more there, since a chunk's per-item bookkeeping runs on
+// one lane per item.
+// The wave's blocks per SM (at most 4) and the largest chunk (16 or 32)
+// come from the tuning table.
+uint32_t compare_screen_chunk(uint32_t total, uint32_t screen_blocks_per_sm, uint32_t screen_chunk_max) {
   const int sms = sm_count();
-  // One wave: k_screen's 64 registers x 256 threads leave room for 4 blocks
-  // per SM. A warp screens its chunk a few items at a time, one dependent
-  // round of profile loads each. A call that fits the wave at one chunk per
-  // warp takes the smallest chunk that does (its items spread thin over many
-  // warps); a larger one takes the largest chunk that still shares the
-  // chunks evenly over the wave's warps (at least 90 % of them busy in the
-  // last round), so no partial second wave or ragged tail is left; chunks
-  // stay at 16 or more there, since a chunk's per-item bookkeeping runs on
-  // one lane per item.
-  // The wave's blocks per SM (at most 4) and the largest chunk (16 or 32)
-  // come from the tuning table.
-  const uint32_t bps = (L0.screen_blocks_per_sm >= 1 && L0.screen_blocks_per_sm <= 4) ? L0.screen_blocks_per_sm : 4u;
-  const uint32_t chmax = L0.screen_chunk_max == 16 ? 16u : 32u;
+  const uint32_t bps = (screen_blocks_per_sm >= 1 && screen_blocks_per_sm <= 4) ? screen_blocks_per_sm : 4u;
+  const uint32_t chmax = screen_chunk_max == 16 ? 16u : 32u;
   const uint32_t cap = uint32_t(sms) * bps;
   const uint64_t warps = uint64_t(cap) * kScreenWarps;
-  CompareLaunch L = L0;
   auto nblocks = [&](uint32_t ch) {
-    return uint32_t((uint64_t(L.total_items) + kScreenWarps * ch - 1) / (uint64_t(kScreenWarps) * ch));
+    return uint32_t((uint64_t(total) + kScreenWarps * ch - 1) / (uint64_t(kScreenWarps) * ch));
   };
-  L.screen_chunk = 4;
+  uint32_t chunk = 4;
   if (nblocks(chmax) <= cap) {
-    while (nblocks(L.screen_chunk) > cap) L.screen_chunk *= 2;
+    while (nblocks(chunk) > cap) chunk *= 2;
   } else {
     for (uint32_t ch = chmax; ch >= 16; ch /= 2) {
-      const uint64_t chunks = (uint64_t(L.total_items) + ch - 1) / ch;
+      const uint64_t chunks = (uint64_t(total) + ch - 1) / ch;
       const uint64_t rounds = (chunks + warps - 1) / warps;
-      L.screen_chunk = ch;
+      chunk = ch;
       if (double(chunks) >= 0.9 * double(rounds * warps)) break;
     }
   }
-  uint32_t blocks = nblocks(L.screen_chunk);
-  if (blocks > cap) blocks = cap;
-  if (ev) cudaEventRecord(ev[0], st);
-  if (L.cdot_ready && L.total_cl > 0 && L.kp.kmer_size <= 7) {
-    const uint32_t pb = std::min<uint32_t>((L.total_cl + 7) / 8, uint32_t(sms) * 8u);
-    switch (L.kp.kmer_size) {
-      case 3: k_pivot_dots<3><<<pb, 256, 0, st>>>(L); break;
-      case 4: k_pivot_dots<4><<<pb, 256, 0, st>>>(L); break;
-      case 5: k_pivot_dots<5><<<pb, 256, 0, st>>>(L); break;
-      case 6: k_pivot_dots<6><<<pb, 256, 0, st>>>(L); break;
-      default: k_pivot_dots<7><<<pb, 256, 0, st>>>(L); break;
-    }
-  }
-  switch (L.kp.kmer_size) {
-    case 3: k_screen<3><<<blocks, kScreenWarps * 32, 0, st>>>(L); break;
-    case 4: k_screen<4><<<blocks, kScreenWarps * 32, 0, st>>>(L); break;
-    case 5: k_screen<5><<<blocks, kScreenWarps * 32, 0, st>>>(L); break;
-    case 6: k_screen<6><<<blocks, kScreenWarps * 32, 0, st>>>(L); break;
-    case 7: k_screen<7><<<blocks, kScreenWarps * 32, 0, st>>>(L); break;
-    default: k_screen<8><<<blocks, kScreenWarps * 32, 0, st>>>(L); break;
-  }
-  if (ev) cudaEventRecord(ev[1], st);
-  const size_t asm_ = err_smem_bytes(L.kp.ncol) + size_t(kNwWarps) * align_smem_per_warp(L.geom);
-  // the k_align instance for the forms this launch can reach, with its
-  // attributes set once per device (dynamic shared memory above 48 KB, the
-  // largest carveout so that kAlignCtasPerSm CTAs fit beside each other)
+  return chunk;
+}
+
+// The k_align instance for the forms a launch can reach, with its attributes
+// set once per device (dynamic shared memory above 48 KB, the largest
+// carveout so that kAlignCtasPerSm CTAs fit beside each other).
+static void (*align_kernel(const CompareLaunch& L, size_t smem))(CompareLaunch) {
   void (*kalign)(CompareLaunch) = L.geom.forms == kFormsVec1 ? k_align<kFormsVec1>
                                   : L.geom.forms == kFormsRm ? k_align<kFormsRm>
                                                              : k_align<kFormsAll>;
-  {
-    const int fi = L.geom.forms == kFormsVec1 ? 1 : (L.geom.forms == kFormsRm ? 2 : 0);
-    static std::atomic<int> limit[3][64];
-    static std::atomic<uint64_t> carved[3];
-    int dev = 0;
-    cudaGetDevice(&dev);
-    std::atomic<int>& lim = limit[fi][dev & 63];
-    if (asm_ > 48 * 1024 && int(asm_) > lim.load(std::memory_order_relaxed)) {
-      cudaFuncSetAttribute(kalign, cudaFuncAttributeMaxDynamicSharedMemorySize, int(asm_));
-      lim.store(int(asm_), std::memory_order_relaxed);
-    }
-    const uint64_t bit = uint64_t(1) << (dev & 63);
-    if (!(carved[fi].load(std::memory_order_relaxed) & bit)) {
-      cudaFuncSetAttribute(kalign, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-      carved[fi].fetch_or(bit);
+  const int fi = L.geom.forms == kFormsVec1 ? 1 : (L.geom.forms == kFormsRm ? 2 : 0);
+  static std::atomic<int> limit[3][64];
+  static std::atomic<uint64_t> carved[3];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::atomic<int>& lim = limit[fi][dev & 63];
+  if (smem > 48 * 1024 && int(smem) > lim.load(std::memory_order_relaxed)) {
+    cudaFuncSetAttribute(kalign, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    lim.store(int(smem), std::memory_order_relaxed);
+  }
+  const uint64_t bit = uint64_t(1) << (dev & 63);
+  if (!(carved[fi].load(std::memory_order_relaxed) & bit)) {
+    cudaFuncSetAttribute(kalign, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    carved[fi].fetch_or(bit);
+  }
+  return kalign;
+}
+
+// The launch sequence of one compare: k_pivot_dots (pivot_blocks > 0), the
+// screen, k_align and the store (store_grid > 0), chained by programmatic
+// dependent launch when the tuning asks for it.
+static void launch_chain(const CompareLaunch& L, cudaStream_t st, cudaEvent_t* ev, uint32_t screen_blocks,
+                         uint32_t pivot_blocks, uint32_t store_grid, void (*kalign)(CompareLaunch), size_t asmem) {
+  if (ev) cudaEventRecord(ev[0], st);
+  if (pivot_blocks > 0) {
+    switch (L.kp.kmer_size) {
+      case 3: k_pivot_dots<3><<<pivot_blocks, 256, 0, st>>>(L); break;
+      case 4: k_pivot_dots<4><<<pivot_blocks, 256, 0, st>>>(L); break;
+      case 5: k_pivot_dots<5><<<pivot_blocks, 256, 0, st>>>(L); break;
+      case 6: k_pivot_dots<6><<<pivot_blocks, 256, 0, st>>>(L); break;
+      default: k_pivot_dots<7><<<pivot_blocks, 256, 0, st>>>(L); break;
     }
   }
+  switch (L.kp.kmer_size) {
+    case 3: k_screen<3><<<screen_blocks, kScreenWarps * 32, 0, st>>>(L); break;
+    case 4: k_screen<4><<<screen_blocks, kScreenWarps * 32, 0, st>>>(L); break;
+    case 5: k_screen<5><<<screen_blocks, kScreenWarps * 32, 0, st>>>(L); break;
+    case 6: k_screen<6><<<screen_blocks, kScreenWarps * 32, 0, st>>>(L); break;
+    case 7: k_screen<7><<<screen_blocks, kScreenWarps * 32, 0, st>>>(L); break;
+    default: k_screen<8><<<screen_blocks, kScreenWarps * 32, 0, st>>>(L); break;
+  }
+  if (ev) cudaEventRecord(ev[1], st);
   // Programmatic dependent launch: the alignment and store kernels are
   // scheduled while their predecessor drains and wait for its results in
   // cudaGridDependencySynchronize, so the launch gaps overlap with work.
@@ -2875,16 +2910,55 @@ void launch_compare(const CompareLaunch& L0, cudaStream_t st, cudaEvent_t* ev) {
   cfg.numAttrs = L.pdl ? 1 : 0;
   cfg.gridDim = dim3(L.geom.nwarps / kNwWarps);
   cfg.blockDim = dim3(kNwWarps * 32);
-  cfg.dynamicSmemBytes = asm_;
+  cfg.dynamicSmemBytes = asmem;
   cudaLaunchKernelEx(&cfg, kalign, L);
   if (ev) cudaEventRecord(ev[2], st);
-  if (L.do_store) {
-    cfg.gridDim = dim3(L.nstore_blocks);
+  if (store_grid > 0) {
+    cfg.gridDim = dim3(store_grid);
     cfg.blockDim = dim3(kStoreThreads);
     cfg.dynamicSmemBytes = 0;
     cudaLaunchKernelEx(&cfg, k_store, L);
   }
   if (ev) cudaEventRecord(ev[3], st);
+}
+
+void launch_compare(const CompareLaunch& L0, cudaStream_t st, cudaEvent_t* ev) {
+  if (L0.total_items == 0) return;
+  const int sms = sm_count();
+  const uint32_t bps = (L0.screen_blocks_per_sm >= 1 && L0.screen_blocks_per_sm <= 4) ? L0.screen_blocks_per_sm : 4u;
+  const uint32_t cap = uint32_t(sms) * bps;
+  CompareLaunch L = L0;
+  L.hdr = nullptr;
+  L.screen_chunk = compare_screen_chunk(L.total_items, L0.screen_blocks_per_sm, L0.screen_chunk_max);
+  uint32_t blocks = uint32_t((uint64_t(L.total_items) + kScreenWarps * L.screen_chunk - 1) /
+                             (uint64_t(kScreenWarps) * L.screen_chunk));
+  if (blocks > cap) blocks = cap;
+  const uint32_t pb = (L.cdot_ready && L.total_cl > 0 && L.kp.kmer_size <= 7)
+                          ? std::min<uint32_t>((L.total_cl + 7) / 8, uint32_t(sms) * 8u)
+                          : 0u;
+  const size_t asm_ = err_smem_bytes(L.kp.ncol) + size_t(kNwWarps) * align_smem_per_warp(L.geom);
+  launch_chain(L, st, ev, blocks, pb, L.do_store ? L.nstore_blocks : 0u, align_kernel(L, asm_), asm_);
+}
+
+int capture_compare_graph(const CompareLaunch& L, cudaStream_t st, bool pivot_dots, uint32_t store_grid,
+                          cudaGraphExec_t* out) {
+  const int sms = sm_count();
+  const uint32_t bps = (L.screen_blocks_per_sm >= 1 && L.screen_blocks_per_sm <= 4) ? L.screen_blocks_per_sm : 4u;
+  const size_t asm_ = err_smem_bytes(L.kp.ncol) + size_t(kNwWarps) * align_smem_per_warp(L.geom);
+  void (*kalign)(CompareLaunch) = align_kernel(L, asm_);  // attributes before the capture
+  cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return int(e);
+  launch_chain(L, st, nullptr, uint32_t(sms) * bps, pivot_dots && L.kp.kmer_size <= 7 ? uint32_t(sms) * 8u : 0u,
+               store_grid, kalign, asm_);
+  cudaGraph_t g = nullptr;
+  e = cudaStreamEndCapture(st, &g);
+  if (e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return int(e);
+  }
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  return int(e);
 }
 
 // ---------------------------------------------------------------------------
