@@ -225,11 +225,12 @@ void launch_compare(const CompareLaunch& L, cudaStream_t st, cudaEvent_t* ev = n
 // The screen's chunk size for a call of `total` items (launch_compare's rule).
 uint32_t compare_screen_chunk(uint32_t total, uint32_t screen_blocks_per_sm, uint32_t screen_chunk_max);
 // Captures the compare sequence on `st` as a graph for replay with L.hdr set:
-// the screen's full wave, k_pivot_dots when `pivot_dots`, k_align and
-// `store_grid` store CTAs (those past the call's count return at once).
-// Returns 0 and sets *out, or a CUDA error code (nothing is captured then).
-int capture_compare_graph(const CompareLaunch& L, cudaStream_t st, bool pivot_dots, uint32_t store_grid,
-                          cudaGraphExec_t* out);
+// `screen_grid` screen CTAs, k_pivot_dots when `pivot_dots`, k_align and
+// `store_grid` store CTAs (spare screen warps find no chunk, spare store CTAs
+// return at once). Returns 0 and sets *out (the caller instantiates it or
+// updates an instantiated one and destroys it), or a CUDA error code.
+int capture_compare_graph(const CompareLaunch& L, cudaStream_t st, uint32_t screen_grid, bool pivot_dots,
+                          uint32_t store_grid, cudaGraph_t* out);
 
 // Final-subs pass (src/dada.rs:609-673) feeding the transition counts
 // (src/error.rs:194-249): item i realigns raw[i] against center[i]; counts go

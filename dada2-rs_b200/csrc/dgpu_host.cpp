@@ -470,6 +470,30 @@ struct Pool;
 // bookkeeping, so that compares of different samples can be in flight at once.
 // Results land in the pool's raw-indexed arrays, which concurrent launches
 // never share: a sample has at most one compare pending.
+// Compare graphs by variant (screen grid, store grid, k_pivot_dots), each
+// with the fixed launch parameters it was captured for.
+struct GraphSet {
+  struct Entry {
+    cudaGraphExec_t exec = nullptr;
+    CompareLaunch key;
+  };
+  std::map<uint32_t, Entry> by_variant;
+};
+static std::mutex g_graph_mu;
+static std::vector<GraphSet*> g_graph_free[64];  // per device; never freed (the execs outlive pools)
+static GraphSet* graph_set_take(int dev) {
+  std::lock_guard<std::mutex> g(g_graph_mu);
+  std::vector<GraphSet*>& f = g_graph_free[dev & 63];
+  if (f.empty()) return new GraphSet();
+  GraphSet* s = f.back();
+  f.pop_back();
+  return s;
+}
+static void graph_set_return(int dev, GraphSet* s) {
+  std::lock_guard<std::mutex> g(g_graph_mu);
+  g_graph_free[dev & 63].push_back(s);
+}
+
 struct Slot {
   Pool* P = nullptr;
   cudaStream_t st = nullptr;
@@ -484,20 +508,15 @@ struct Slot {
   std::vector<uint32_t> task_blk0;  // first store CTA of each task in the latest launch
   uint32_t ntask_cap = 0, nblk_cap = 0;
   size_t pack_cap = 0;
-  // Captured compare graphs (k_pivot_dots or not, x store grid), all for the
-  // fixed launch parameters in graph_key; a change there drops them.
-  std::map<uint32_t, cudaGraphExec_t> graphs;
-  CompareLaunch graph_key;
+  // Instantiated compare graphs, checked out of a per-device free list for
+  // the slot's lifetime and handed back after it (a new pool's slots update
+  // them in place instead of instantiating again).
+  GraphSet* gs = nullptr;
   bool graphs_failed = false;
-
-  void drop_graphs() {
-    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
-    graphs.clear();
-  }
+  int dev = 0;  // the slot's device
 
   ~Slot() {
-    if (st) (void)cudaStreamSynchronize(st);
-    drop_graphs();
+    if (st && cudaStreamSynchronize(st) == cudaSuccess && gs) graph_set_return(dev, gs);
     if (st && cudaStreamSynchronize(st) == cudaSuccess)  // every block is idle now
       recycle_all(queue_pass, queue_counts, err_dev, scratch, dpack, hpack, blk_counters, err_host, task_self,
                   task_stage);
@@ -508,6 +527,7 @@ struct Slot {
 
   int init(Pool* pool, bool high_priority = false) {
     P = pool;
+    CUDA_TRY(cudaGetDevice(&dev));
     int lo = 0, hi = 0;
     CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
     CUDA_TRY(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, high_priority ? hi : lo));
@@ -564,6 +584,11 @@ struct Pool {
   KParams kp{};
   NwGeom geom{};
   int sms = 148;
+  // Compare calls replay captured graphs (Slot::run_compare): on for pools
+  // that serve many batch runs (resident batches, learn-errors, compare
+  // contexts), where the graphs' set-up is paid once; a one-shot denoising
+  // launches directly.
+  bool replay_graphs = false;
   int nslots = 1;
   DBuf<uint8_t> seq, qual, kmer8, sat, lock, status;
   DBuf<uint32_t> off, len, reads, ham, knum;
@@ -919,7 +944,7 @@ int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
   const uint64_t every = g_stats.timing_every.load();
   const bool timing = every != 0 && g_stats.call_seq.fetch_add(1) % every == 0;
   bool launched = false;
-  if (do_store && !timing && total > 0 && compare_graphs_on() && !graphs_failed) {
+  if (do_store && !timing && total > 0 && Q.replay_graphs && compare_graphs_on() && !graphs_failed) {
     // Replay a captured graph of the launch sequence: one submission instead
     // of three or four, which the launch slots' threads otherwise contend
     // for in the driver. Its kernels take this call's values from the
@@ -930,25 +955,45 @@ int Slot::run_compare(uint32_t ntask, bool do_store, double* wait_s) {
     K.tasks = nullptr;
     K.task_prefix = K.task_cl_prefix = K.store_task = K.store_chunk = nullptr;
     K.hdr = reinterpret_cast<const CallHeader*>(dpack.p);
-    if (graphs.empty() || std::memcmp(&K, &graph_key, sizeof K) != 0) {
-      drop_graphs();
-      graph_key = K;
-    }
+    if (!gs) gs = graph_set_take(dev);
+    // the screen's grid as launch_compare sizes it, rounded up to a power of
+    // two (at least 64, at most the one wave); the store grid to 8 x 4^j
+    const CallHeader& H = *reinterpret_cast<const CallHeader*>(hpack.h);
+    const uint32_t bps = (tu.screen_blocks_per_sm >= 1 && tu.screen_blocks_per_sm <= 4) ? uint32_t(tu.screen_blocks_per_sm) : 4u;
+    const uint32_t wave = uint32_t(Q.sms) * bps;
+    const uint32_t need = uint32_t((uint64_t(total) + uint64_t(kScreenWarps) * H.screen_chunk - 1) /
+                                   (uint64_t(kScreenWarps) * H.screen_chunk));
+    uint32_t sgrid = 64;
+    while (sgrid < need && sgrid < wave) sgrid *= 2;
+    sgrid = std::min(sgrid, wave);
     uint32_t grid = 8;
     while (grid < nblk) grid *= 4;
-    const uint32_t key = (grid << 1) | (cdot_ready ? 1u : 0u);
-    auto it = graphs.find(key);
-    if (it == graphs.end()) {
-      cudaGraphExec_t ge = nullptr;
-      if (capture_compare_graph(K, st, cdot_ready, grid, &ge) == 0 && ge) {
-        it = graphs.emplace(key, ge).first;
+    const uint32_t key = (sgrid << 20) ^ (grid << 1) ^ (cdot_ready ? 1u : 0u);
+    GraphSet::Entry& E = gs->by_variant[key];
+    if (!E.exec || std::memcmp(&E.key, &K, sizeof K) != 0) {
+      cudaGraph_t g = nullptr;
+      bool ok = capture_compare_graph(K, st, sgrid, cdot_ready, grid, &g) == 0 && g;
+      if (ok && E.exec) {  // same shape, new parameters: update in place
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(E.exec, g, &info) != cudaSuccess) {
+          (void)cudaGetLastError();
+          cudaGraphExecDestroy(E.exec);
+          E.exec = nullptr;
+        }
+      }
+      if (ok && !E.exec) ok = cudaGraphInstantiate(&E.exec, g, 0) == cudaSuccess;
+      if (g) cudaGraphDestroy(g);
+      if (ok) {
+        E.key = K;
       } else {
         (void)cudaGetLastError();
+        if (E.exec) cudaGraphExecDestroy(E.exec);
+        gs->by_variant.erase(key);
         graphs_failed = true;  // direct launches from here on
       }
     }
-    if (it != graphs.end()) {
-      CUDA_TRY(cudaGraphLaunch(it->second, st));
+    if (!graphs_failed) {
+      CUDA_TRY(cudaGraphLaunch(gs->by_variant[key].exec, st));
       launched = true;
     }
   }
@@ -3539,6 +3584,7 @@ int dgpu_ctx_create(int device, const dgpu_align_params* params, const double* e
     delete c;
     return rc;
   }
+  c->pool.replay_graphs = true;  // a compare context serves many calls
   c->kp = to_kparams(*params, use_quals, 1, ncol);
   c->err.assign(err_mat, err_mat + 16 * size_t(ncol));
   *out = c;
@@ -3704,6 +3750,7 @@ int dgpu_batch_prepare(int device, const dgpu_dada_params* params, int nsamples,
     delete b;
     return rc;
   }
+  b->b.pool.replay_graphs = true;  // a resident batch runs many times
   *out = b;
   return 0;
 }
@@ -3794,6 +3841,7 @@ int dgpu_learn_errors(int device, const dgpu_dada_params* params, const dgpu_err
                     nq));
   Batch& B = b.b;
   B.learn_nq = nq;
+  B.pool.replay_graphs = true;  // several passes over the same pool
   std::unique_ptr<dgpu_learn> L(new dgpu_learn());
   L->nq = nq;
   std::vector<uint32_t> acc;

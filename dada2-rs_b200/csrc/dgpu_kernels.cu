@@ -2940,15 +2940,14 @@ void launch_compare(const CompareLaunch& L0, cudaStream_t st, cudaEvent_t* ev) {
   launch_chain(L, st, ev, blocks, pb, L.do_store ? L.nstore_blocks : 0u, align_kernel(L, asm_), asm_);
 }
 
-int capture_compare_graph(const CompareLaunch& L, cudaStream_t st, bool pivot_dots, uint32_t store_grid,
-                          cudaGraphExec_t* out) {
+int capture_compare_graph(const CompareLaunch& L, cudaStream_t st, uint32_t screen_grid, bool pivot_dots,
+                          uint32_t store_grid, cudaGraph_t* out) {
   const int sms = sm_count();
-  const uint32_t bps = (L.screen_blocks_per_sm >= 1 && L.screen_blocks_per_sm <= 4) ? L.screen_blocks_per_sm : 4u;
   const size_t asm_ = err_smem_bytes(L.kp.ncol) + size_t(kNwWarps) * align_smem_per_warp(L.geom);
   void (*kalign)(CompareLaunch) = align_kernel(L, asm_);  // attributes before the capture
   cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return int(e);
-  launch_chain(L, st, nullptr, uint32_t(sms) * bps, pivot_dots && L.kp.kmer_size <= 7 ? uint32_t(sms) * 8u : 0u,
+  launch_chain(L, st, nullptr, screen_grid, pivot_dots && L.kp.kmer_size <= 7 ? uint32_t(sms) * 8u : 0u,
                store_grid, kalign, asm_);
   cudaGraph_t g = nullptr;
   e = cudaStreamEndCapture(st, &g);
@@ -2956,9 +2955,8 @@ int capture_compare_graph(const CompareLaunch& L, cudaStream_t st, bool pivot_do
     if (g) cudaGraphDestroy(g);
     return int(e);
   }
-  e = cudaGraphInstantiate(out, g, 0);
-  cudaGraphDestroy(g);
-  return int(e);
+  *out = g;
+  return 0;
 }
 
 // ---------------------------------------------------------------------------

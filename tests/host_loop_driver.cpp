@@ -27,7 +27,7 @@ void launch_profiles_sparse(const uint8_t*, const uint32_t*, const uint32_t*, ui
 void launch_compare(const CompareLaunch&, cudaStream_t, cudaEvent_t*) {}
 uint32_t compare_screen_chunk(uint32_t, uint32_t, uint32_t) { return 4; }
 // no graphs on the CPU: the host takes its direct-launch path
-int capture_compare_graph(const CompareLaunch&, cudaStream_t, bool, uint32_t, cudaGraphExec_t*) { return 1; }
+int capture_compare_graph(const CompareLaunch&, cudaStream_t, uint32_t, bool, uint32_t, cudaGraph_t*) { return 1; }
 void launch_fill_f64(double*, size_t, double, cudaStream_t) {}
 void launch_final_subs(const FinalSubsLaunch&, cudaStream_t) {}
 void launch_align_debug(int, const uint8_t*, const uint32_t*, const uint32_t*, const uint8_t*, const uint32_t*,
