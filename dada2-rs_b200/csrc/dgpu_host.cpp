@@ -589,6 +589,10 @@ struct Pool {
   // contexts), where the graphs' set-up is paid once; a one-shot denoising
   // launches directly.
   bool replay_graphs = false;
+  // The largest length difference of two uniques that are ever compared (a
+  // batch compares only within a sample); -1: any two uniques of the pool.
+  // It bounds the aligners' band geometry.
+  int64_t pair_spread = -1;
   int nslots = 1;
   DBuf<uint8_t> seq, qual, kmer8, sat, lock, status;
   DBuf<uint32_t> off, len, reads, ham, knum;
@@ -752,7 +756,8 @@ struct Pool {
     const bool rm_possible = use_homo || !kp.vectorized || lmax > 3500;
     geom.lmax = int32_t(lmax);
     const int64_t bb = kp.band < 0 ? int64_t(lmax) : int64_t(kp.band);
-    const int64_t diff = int64_t(lmax) - int64_t(lmin);
+    int64_t diff = int64_t(lmax) - int64_t(lmin);
+    if (pair_spread >= 0 && pair_spread < diff) diff = pair_spread;
     geom.vec_ncol = int32_t(4 + (std::min<int64_t>(bb, lmax) + 1) / 2 + std::min<int64_t>(bb + diff, lmax) / 2);
     geom.vec_nrow = int32_t(2 * lmax + 1);
     int64_t W = kp.band < 0 ? int64_t(2 * lmax + 1) : std::min<int64_t>(2 * bb + diff + 1, 2 * int64_t(lmax) + 1);
@@ -3116,6 +3121,18 @@ static int batch_prepare(Batch& B, int device, const dgpu_dada_params* prm, int 
   KParams kp = to_kparams(prm->align, prm->use_quals, prm->greedy, ncol2);
   kp.lambda32 = prm->lambda_fp32 ? 1 : 0;
   const auto tp1 = Clock::now();
+  {  // uniques are compared only within their sample
+    int64_t spread = 0;
+    for (int s = 0; s < nsamples; ++s) {
+      uint32_t lo = 0xffffffffu, hi = 0;
+      for (uint32_t t = B.bases[size_t(s)]; t < B.bases[size_t(s)] + B.counts[size_t(s)]; ++t) {
+        lo = std::min(lo, B.E.len[t]);
+        hi = std::max(hi, B.E.len[t]);
+      }
+      if (hi >= lo) spread = std::max<int64_t>(spread, int64_t(hi) - int64_t(lo));
+    }
+    B.pool.pair_spread = spread;
+  }
   TRY(B.pool.upload(uint32_t(B.E.off.size()), B.E.seq, B.E.off.data(), B.E.len.data(), B.E.qual, B.E.reads.data(), kp,
                     err.data()));
   {
