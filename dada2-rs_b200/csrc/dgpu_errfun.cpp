@@ -279,38 +279,11 @@ void expand(const std::vector<double>& off, int nq, double* err) {
     }
 }
 
-}  // namespace
-
-// The fit the learn-errors loop applies to its accumulated transition matrix.
-// Returns 0, or DGPU_E_INVALID with *msg when LOESS fails for all twelve
-// transitions (the reference's error, src/error_models.rs:186-201).
-int errfun_apply(const dgpu_errfun& ef, const uint32_t* trans, int nq, double* err, std::string* msg) {
+// LOESS per off-diagonal transition over the nq columns of trans (row 4i+j,
+// column q) into err. Returns 0, or DGPU_E_INVALID with *msg when the fit
+// fails for all twelve transitions (src/error_models.rs:186-201).
+int loess_fit(const dgpu_errfun& ef, const uint32_t* trans, int nq, double* err, std::string* msg) {
   std::vector<double> off(size_t(12) * nq, 0.0);
-  if (ef.kind == DGPU_ERRFUN_NOQUAL) {
-    double obs[16];
-    for (int r = 0; r < 16; ++r) {
-      double s = 0.0;
-      for (int q = 0; q < nq; ++q) s += double(trans[size_t(r) * nq + q]);
-      obs[r] = s + ef.pseudocount;
-    }
-    int orow = 0;
-    for (int i = 0; i < 4; ++i) {
-      double tot = 0.0;
-      for (int j = 0; j < 4; ++j) tot += obs[i * 4 + j];
-      for (int j = 0; j < 4; ++j) {
-        if (i == j) continue;
-        const double rate = tot > 0.0 ? clamp_rate(obs[i * 4 + j] / tot, ef) : ef.min_error_rate;
-        for (int q = 0; q < nq; ++q) off[size_t(orow) * nq + q] = rate;
-        ++orow;
-      }
-    }
-    expand(off, nq, err);
-    return 0;
-  }
-  if (ef.kind != DGPU_ERRFUN_LOESS) {
-    *msg = "unknown error function kind";
-    return DGPU_E_INVALID;
-  }
   std::vector<double> xs(nq), tot(nq), rlogp(nq);
   for (int q = 0; q < nq; ++q) xs[q] = double(q);
   int orow = 0, failed = 0;
@@ -344,6 +317,144 @@ int errfun_apply(const dgpu_errfun& ef, const uint32_t* trans, int nq, double* e
   }
   expand(off, nq, err);
   return 0;
+}
+
+// An anchor quality as an index: what Rust's `f64 as usize` gives (NaN and
+// negatives 0, truncation, saturation).
+size_t anchor_col(double v) {
+  if (!(v > 0.0)) return 0;
+  if (v >= 18446744073709551615.0) return std::numeric_limits<size_t>::max();
+  return size_t(v);
+}
+
+// An f64 as Rust's `{}` prints it, for the messages the reference returns.
+std::string f64_text(double v) {
+  if (std::isnan(v)) return "NaN";
+  if (std::isinf(v)) return v < 0 ? "-inf" : "inf";
+  char b[64];
+  if (std::fabs(v) < 1e15 && v == std::floor(v)) std::snprintf(b, sizeof b, "%.0f", v);
+  else std::snprintf(b, sizeof b, "%.17g", v);
+  return b;
+}
+
+// Piecewise-linear rates between anchor qualities (quality scores 0..nq-1).
+int binned_fit(const dgpu_errfun& ef, const uint32_t* trans, int nq, double* err, std::string* msg) {
+  const double inf = std::numeric_limits<double>::infinity();
+  double lo_obs = inf, hi_obs = -inf;
+  for (int q = 0; q < nq; ++q) {
+    uint64_t c = 0;
+    for (int r = 0; r < 16; ++r) c += trans[size_t(r) * nq + q];
+    if (c) {
+      lo_obs = std::min(lo_obs, double(q));
+      hi_obs = std::max(hi_obs, double(q));
+    }
+  }
+  if (hi_obs < lo_obs) {
+    *msg = "No observed transitions";
+    return DGPU_E_INVALID;
+  }
+  const int nb = ef.bins ? ef.nbins : 0;
+  double bmin = inf, bmax = -inf;
+  for (int k = 0; k < nb; ++k) {
+    bmin = std::min(bmin, ef.bins[k]);
+    bmax = std::max(bmax, ef.bins[k]);
+  }
+  if (hi_obs > bmax) {
+    *msg = "Input data contains quality score " + f64_text(hi_obs) + " higher than max binned value " + f64_text(bmax);
+    return DGPU_E_INVALID;
+  }
+  if (lo_obs < bmin) {
+    *msg = "Input data contains quality score " + f64_text(lo_obs) + " lower than min binned value " + f64_text(bmin);
+    return DGPU_E_INVALID;
+  }
+  const double nan = std::numeric_limits<double>::quiet_NaN();
+  std::vector<double> off(size_t(12) * nq, 0.0), rate(nq), line(nq);
+  int orow = 0;
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) {
+      if (i == j) continue;
+      for (int q = 0; q < nq; ++q) {
+        double t = 0.0;
+        for (int k = 0; k < 4; ++k) t += double(trans[size_t(i * 4 + k) * nq + q]);
+        rate[q] = t > 0.0 ? double(trans[size_t(i * 4 + j) * nq + q]) / t : nan;
+      }
+      std::fill(line.begin(), line.end(), nan);
+      for (int k = 0; k + 1 < nb; ++k) {
+        const size_t a = anchor_col(ef.bins[k]), b = anchor_col(ef.bins[k + 1]);
+        if (a >= size_t(nq) || b >= size_t(nq)) continue;
+        if (b < a) {
+          *msg = "binned quality scores must be ascending";
+          return DGPU_E_INVALID;
+        }
+        if (!std::isfinite(rate[a]) || !std::isfinite(rate[b])) continue;
+        const size_t n = b - a + 1;
+        for (size_t s = 0; s < n; ++s) {
+          const double f = n > 1 ? double(s) / double(n - 1) : 0.0;
+          line[a + s] = rate[a] * (1.0 - f) + rate[b] * f;
+        }
+      }
+      extrapolate_flat(line);
+      for (int q = 0; q < nq; ++q)
+        off[size_t(orow) * nq + q] = std::isfinite(line[q]) ? clamp_rate(line[q], ef) : ef.min_error_rate;
+      ++orow;
+    }
+  expand(off, nq, err);
+  return 0;
+}
+
+// PacBio: LOESS below Q93 and a pseudocount estimate in the Q93 column.
+int pacbio_fit(const dgpu_errfun& ef, const uint32_t* trans, int nq, double* err, std::string* msg) {
+  if (nq != 94) return loess_fit(ef, trans, nq, err, msg);
+  const int lo = 93;
+  std::vector<uint32_t> below(size_t(16) * lo);
+  for (int r = 0; r < 16; ++r)
+    std::copy(trans + size_t(r) * nq, trans + size_t(r) * nq + lo, below.begin() + size_t(r) * lo);
+  std::vector<double> fit(size_t(16) * lo);
+  const int rc = loess_fit(ef, below.data(), lo, fit.data(), msg);
+  if (rc) return rc;
+  for (int r = 0; r < 16; ++r) std::copy(fit.begin() + size_t(r) * lo, fit.begin() + size_t(r + 1) * lo, err + size_t(r) * nq);
+  for (int i = 0; i < 4; ++i) {
+    double t = 0.0;
+    for (int j = 0; j < 4; ++j) t += double(trans[size_t(i * 4 + j) * nq + lo]);
+    for (int j = 0; j < 4; ++j)
+      err[size_t(i * 4 + j) * nq + lo] = (double(trans[size_t(i * 4 + j) * nq + lo]) + 1.0) / (t + 4.0);
+  }
+  return 0;
+}
+
+}  // namespace
+
+// The fit the learn-errors loop applies to its accumulated transition matrix
+// (quality scores 0..nq-1, src/learn_errors.rs:84-100). Returns 0, or
+// DGPU_E_INVALID with *msg where the reference's fit returns an error.
+int errfun_apply(const dgpu_errfun& ef, const uint32_t* trans, int nq, double* err, std::string* msg) {
+  if (ef.kind == DGPU_ERRFUN_NOQUAL) {
+    std::vector<double> off(size_t(12) * nq, 0.0);
+    double obs[16];
+    for (int r = 0; r < 16; ++r) {
+      double s = 0.0;
+      for (int q = 0; q < nq; ++q) s += double(trans[size_t(r) * nq + q]);
+      obs[r] = s + ef.pseudocount;
+    }
+    int orow = 0;
+    for (int i = 0; i < 4; ++i) {
+      double tot = 0.0;
+      for (int j = 0; j < 4; ++j) tot += obs[i * 4 + j];
+      for (int j = 0; j < 4; ++j) {
+        if (i == j) continue;
+        const double rate = tot > 0.0 ? clamp_rate(obs[i * 4 + j] / tot, ef) : ef.min_error_rate;
+        for (int q = 0; q < nq; ++q) off[size_t(orow) * nq + q] = rate;
+        ++orow;
+      }
+    }
+    expand(off, nq, err);
+    return 0;
+  }
+  if (ef.kind == DGPU_ERRFUN_LOESS) return loess_fit(ef, trans, nq, err, msg);
+  if (ef.kind == DGPU_ERRFUN_BINNED) return binned_fit(ef, trans, nq, err, msg);
+  if (ef.kind == DGPU_ERRFUN_PACBIO) return pacbio_fit(ef, trans, nq, err, msg);
+  *msg = "unknown error function kind";
+  return DGPU_E_INVALID;
 }
 
 }  // namespace dgpu

@@ -575,20 +575,27 @@ def cache_release(device: int = -1) -> int:
 class ErrFun:
     """The error-model fit of learn-errors (src/learn_errors.rs:67-100):
     kind "loess" (surface "direct", the dada2-rs default, or "interpolate"
-    with ``cell``, R's default) or "noqual" (``pseudocount``); off-diagonal
-    rates clamped to [min_error_rate, max_error_rate]."""
+    with ``cell``, R's default), "noqual" (``pseudocount``), "binned"
+    (piecewise linear between the anchor qualities ``bins``) or "pacbio"
+    (LOESS, with a maximum-likelihood Q93 column); off-diagonal rates clamped
+    to [min_error_rate, max_error_rate]."""
     kind: str = "loess"
     surface: str = "direct"
     cell: float = 0.2
     max_error_rate: float = 0.25
     min_error_rate: float = 1e-7
     pseudocount: float = 1.0
+    bins: tuple = ()
 
     def c(self) -> ErrFunC:
-        kinds = {"loess": 0, "noqual": 1}
+        kinds = {"loess": 0, "noqual": 1, "binned": 2, "pacbio": 3}
         surfaces = {"direct": 0, "interpolate": 1}
-        return ErrFunC(kinds[self.kind], surfaces[self.surface], float(self.cell), float(self.max_error_rate),
-                       float(self.min_error_rate), float(self.pseudocount))
+        b = np.ascontiguousarray(self.bins, np.float64)
+        ef = ErrFunC(kinds[self.kind], surfaces[self.surface], float(self.cell), float(self.max_error_rate),
+                     float(self.min_error_rate), float(self.pseudocount), b.ctypes.data if len(b) else None,
+                     int(len(b)))
+        ef._bins = b  # the anchors stay alive with the structure
+        return ef
 
 
 def errfun_apply(trans, nq: int, errfun: ErrFun | None = None) -> np.ndarray:

@@ -63,7 +63,8 @@ class TuningC(C.Structure):
 
 class ErrFunC(C.Structure):
     _fields_ = [("kind", C.c_int32), ("surface", C.c_int32), ("cell", C.c_double),
-                ("max_error_rate", C.c_double), ("min_error_rate", C.c_double), ("pseudocount", C.c_double)]
+                ("max_error_rate", C.c_double), ("min_error_rate", C.c_double), ("pseudocount", C.c_double),
+                ("bins", C.c_void_p), ("nbins", C.c_int32)]
 
 
 class CountersC(C.Structure):

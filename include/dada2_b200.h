@@ -333,15 +333,30 @@ int dgpu_result_margins(const dgpu_result* res, double* out3);
  *   DGPU_ERRFUN_NOQUAL  noqual_errfun (src/error_models.rs:212-261): one
  *                       rate per transition from counts summed over
  *                       qualities plus `pseudocount`
- * The diagonal of each nucleotide is 1 minus its three off-diagonals. */
+ *   DGPU_ERRFUN_BINNED  binned_qual_errfun (src/error_models.rs:263-396):
+ *                       the observed rate at each of the `nbins` anchor
+ *                       qualities `bins` (ascending), linear between
+ *                       adjacent anchors, flat beyond the outer ones;
+ *                       DGPU_E_INVALID when no column has an observation or
+ *                       an observed quality lies outside the anchors
+ *   DGPU_ERRFUN_PACBIO  pacbio_errfun (src/error_models.rs:408-462): with
+ *                       nq = 94 (a Q93 column), LOESS over columns 0..92 and
+ *                       (count + 1) / (source total + 4) for column 93;
+ *                       otherwise LOESS
+ * The diagonal of each nucleotide is 1 minus its three off-diagonals
+ * (PacBio's column 93 excepted). */
 #define DGPU_ERRFUN_LOESS 0
 #define DGPU_ERRFUN_NOQUAL 1
+#define DGPU_ERRFUN_BINNED 2
+#define DGPU_ERRFUN_PACBIO 3
 typedef struct {
   int32_t kind;
   int32_t surface;  /* LOESS: 0 direct, 1 interpolate */
   double cell;      /* LOESS interpolate: kd-tree cell fraction (0.2) */
   double max_error_rate, min_error_rate;  /* clamp of the off-diagonal rates (0.25, 1e-7) */
   double pseudocount;                     /* NOQUAL (1.0) */
+  const double* bins;                     /* BINNED: anchor qualities (NULL otherwise) */
+  int32_t nbins;
 } dgpu_errfun;
 /* err_out (16 x nq) = the fit of trans (16 x nq). Host only. */
 int dgpu_errfun_apply(const dgpu_errfun* ef, const uint32_t* trans, int nq, double* err_out);

@@ -301,11 +301,12 @@ std::string dada_uniques(const std::vector<RawInput>& inputs, const DadaParams& 
 
 // ---- learn_errors.rs / error_models.rs / loess.rs (oracle_learn.cpp) ----
 struct ErrFunSpec {
-  int kind = 0;     // 0 loess, 1 noqual
+  int kind = 0;     // 0 loess, 1 noqual, 2 binned quality, 3 PacBio
   int surface = 0;  // loess: 0 direct, 1 interpolate
   double cell = 0.2;
   double max_error_rate = 0.25, min_error_rate = 1e-7;
   double pseudocount = 1.0;
+  std::vector<double> bins;  // binned quality: the anchor quality scores, ascending
 };
 struct LearnResult {
   size_t nq = 0, passes = 0;

@@ -54,7 +54,8 @@ class DadaParamsC(C.Structure):
 
 class ErrFunC(C.Structure):
     _fields_ = [("kind", C.c_int32), ("surface", C.c_int32), ("cell", C.c_double),
-                ("max_error_rate", C.c_double), ("min_error_rate", C.c_double), ("pseudocount", C.c_double)]
+                ("max_error_rate", C.c_double), ("min_error_rate", C.c_double), ("pseudocount", C.c_double),
+                ("bins", C.c_void_p), ("nbins", C.c_int32)]
 
 
 _P = C.c_void_p
@@ -486,12 +487,18 @@ def dada(seqs, abund, err, ncol, params: DadaParams, quals=None, prior=None):
         lib().orc_c_dada_free(h)
 
 
-ERRFUN_LOESS, ERRFUN_NOQUAL = 0, 1
+ERRFUN_LOESS, ERRFUN_NOQUAL, ERRFUN_BINNED, ERRFUN_PACBIO = 0, 1, 2, 3
 
 
-def errfun_c(kind=ERRFUN_LOESS, surface=0, cell=0.2, max_error_rate=0.25, min_error_rate=1e-7, pseudocount=1.0):
-    return ErrFunC(int(kind), int(surface), float(cell), float(max_error_rate), float(min_error_rate),
-                   float(pseudocount))
+def errfun_c(kind=ERRFUN_LOESS, surface=0, cell=0.2, max_error_rate=0.25, min_error_rate=1e-7, pseudocount=1.0,
+             bins=None):
+    """kind 0 LOESS, 1 noqual, 2 binned quality (anchors `bins`), 3 PacBio. The
+    returned structure keeps the anchors' array alive as `_bins`."""
+    b = np.ascontiguousarray(bins if bins is not None else [], np.float64)
+    ef = ErrFunC(int(kind), int(surface), float(cell), float(max_error_rate), float(min_error_rate),
+                 float(pseudocount), b.ctypes.data if len(b) else None, int(len(b)))
+    ef._bins = b
+    return ef
 
 
 def errfun_apply(trans, nq, **kw) -> np.ndarray:

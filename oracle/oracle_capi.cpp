@@ -333,6 +333,8 @@ void orc_c_dada_free(void* h) { delete static_cast<OrcDada*>(h); }
 struct orc_errfun {
   int32_t kind, surface;
   double cell, max_error_rate, min_error_rate, pseudocount;
+  const double* bins;
+  int32_t nbins;
 };
 static ErrFunSpec to_errfun(const orc_errfun* e) {
   ErrFunSpec s;
@@ -342,6 +344,7 @@ static ErrFunSpec to_errfun(const orc_errfun* e) {
   s.max_error_rate = e->max_error_rate;
   s.min_error_rate = e->min_error_rate;
   s.pseudocount = e->pseudocount;
+  if (e->bins && e->nbins > 0) s.bins.assign(e->bins, e->bins + e->nbins);
   return s;
 }
 int orc_c_errfun_apply(const orc_errfun* e, const uint32_t* trans, int nq, double* out, char* errbuf, int errcap) {

@@ -225,28 +225,10 @@ void expand12(const std::vector<double>& off, size_t nq, std::vector<double>& er
 
 }  // namespace
 
-std::string errfun_apply(const ErrFunSpec& e, const std::vector<uint32_t>& trans, size_t nq, std::vector<double>& err) {
+// loess_errfun (src/error_models.rs:119-210) over the nq columns of trans.
+static std::string loess_fit(const ErrFunSpec& e, const std::vector<uint32_t>& trans, size_t nq,
+                             std::vector<double>& err) {
   std::vector<double> off(12 * nq, 0.0);
-  if (e.kind == 1) {  // noqual
-    double obs[16];
-    for (size_t r = 0; r < 16; ++r) {
-      double s = 0.0;
-      for (size_t q = 0; q < nq; ++q) s += double(trans[r * nq + q]);
-      obs[r] = s + e.pseudocount;
-    }
-    size_t o = 0;
-    for (size_t i = 0; i < 4; ++i) {
-      const double tot = obs[i * 4] + obs[i * 4 + 1] + obs[i * 4 + 2] + obs[i * 4 + 3];
-      for (size_t j = 0; j < 4; ++j) {
-        if (i == j) continue;
-        const double rate = tot > 0.0 ? clampr(obs[i * 4 + j] / tot, e) : e.min_error_rate;
-        for (size_t q = 0; q < nq; ++q) off[o * nq + q] = rate;
-        ++o;
-      }
-    }
-    expand12(off, nq, err);
-    return std::string();
-  }
   std::vector<double> x(nq), tot(nq), yl(nq);
   for (size_t q = 0; q < nq; ++q) x[q] = double(q);
   size_t o = 0, failed = 0;
@@ -272,6 +254,135 @@ std::string errfun_apply(const ErrFunSpec& e, const std::vector<uint32_t>& trans
   if (failed == 12) return "LOESS fit failed for all 12 transitions";
   expand12(off, nq, err);
   return std::string();
+}
+
+// A quality anchor as Rust's `f64 as usize` gives it: NaN and negatives to 0,
+// truncation toward zero otherwise (saturating).
+static size_t anchor_index(double v) {
+  if (!(v > 0.0)) return 0;
+  if (v >= 18446744073709551615.0) return std::numeric_limits<size_t>::max();
+  return size_t(v);
+}
+
+// Rust's `{}` of an f64 for the messages: integral values without a point.
+static std::string rust_f64(double v) {
+  if (std::isinf(v)) return v > 0 ? "inf" : "-inf";
+  if (std::isnan(v)) return "NaN";
+  char b[64];
+  if (v == std::floor(v) && std::fabs(v) < 1e15) std::snprintf(b, sizeof b, "%.0f", v);
+  else std::snprintf(b, sizeof b, "%.17g", v);
+  return b;
+}
+
+// binned_qual_errfun (src/error_models.rs:263-396): per off-diagonal
+// transition, the observed rate at each anchor quality, linear between
+// adjacent anchors, flat beyond the outer ones; quality scores are 0..nq-1
+// (src/learn_errors.rs:87). Unsorted anchors, on which the reference's
+// unsigned step count underflows, are refused.
+static std::string binned_fit(const ErrFunSpec& e, const std::vector<uint32_t>& trans, size_t nq,
+                              std::vector<double>& err) {
+  double qmin = std::numeric_limits<double>::infinity(), qmax = -qmin;
+  bool observed = false;
+  for (size_t q = 0; q < nq; ++q) {
+    double t = 0.0;
+    for (size_t r = 0; r < 16; ++r) t += double(trans[r * nq + q]);
+    if (t > 0.0) {
+      observed = true;
+      qmin = std::min(qmin, double(q));
+      qmax = std::max(qmax, double(q));
+    }
+  }
+  if (!observed) return "No observed transitions";
+  double bmin = std::numeric_limits<double>::infinity(), bmax = -bmin;
+  for (double b : e.bins) {
+    bmax = std::max(bmax, b);
+    bmin = std::min(bmin, b);
+  }
+  if (qmax > bmax)
+    return "Input data contains quality score " + rust_f64(qmax) + " higher than max binned value " + rust_f64(bmax);
+  if (qmin < bmin)
+    return "Input data contains quality score " + rust_f64(qmin) + " lower than min binned value " + rust_f64(bmin);
+  std::vector<double> off(12 * nq, 0.0);
+  size_t o = 0;
+  for (size_t i = 0; i < 4; ++i) {
+    std::vector<double> tot(nq, 0.0);
+    for (size_t q = 0; q < nq; ++q)
+      for (size_t j = 0; j < 4; ++j) tot[q] += double(trans[(i * 4 + j) * nq + q]);
+    for (size_t j = 0; j < 4; ++j) {
+      if (i == j) continue;
+      std::vector<double> p(nq), pred(nq, std::numeric_limits<double>::quiet_NaN());
+      for (size_t q = 0; q < nq; ++q)
+        p[q] = tot[q] > 0.0 ? double(trans[(i * 4 + j) * nq + q]) / tot[q] : std::numeric_limits<double>::quiet_NaN();
+      for (size_t k = 0; k + 1 < e.bins.size(); ++k) {
+        const size_t lo = anchor_index(e.bins[k]), hi = anchor_index(e.bins[k + 1]);
+        if (lo >= nq || hi >= nq) continue;
+        if (hi < lo) return "binned quality scores must be ascending";
+        const double lp = p[lo], hp = p[hi];
+        if (!std::isfinite(lp) || !std::isfinite(hp)) continue;
+        const size_t steps = hi - lo + 1;
+        for (size_t s = 0; s < steps; ++s) {
+          const double t = steps > 1 ? double(s) / double(steps - 1) : 0.0;
+          pred[lo + s] = lp * (1.0 - t) + hp * t;
+        }
+      }
+      fill_ends(pred);
+      for (size_t q = 0; q < nq; ++q) off[o * nq + q] = std::isfinite(pred[q]) ? clampr(pred[q], e) : e.min_error_rate;
+      ++o;
+    }
+  }
+  expand12(off, nq, err);
+  return std::string();
+}
+
+// pacbio_errfun (src/error_models.rs:408-462): with a Q93 column (quality
+// scores 0..nq-1, so nq = 94), LOESS over columns 0..92 and (count + 1) /
+// (source total + 4) for every entry of column 93; otherwise LOESS.
+static std::string pacbio_fit(const ErrFunSpec& e, const std::vector<uint32_t>& trans, size_t nq,
+                              std::vector<double>& err) {
+  if (nq != 94) return loess_fit(e, trans, nq, err);
+  const size_t sub = nq - 1;
+  std::vector<uint32_t> ts(16 * sub);
+  for (size_t r = 0; r < 16; ++r)
+    for (size_t q = 0; q < sub; ++q) ts[r * sub + q] = trans[r * nq + q];
+  std::vector<double> es;
+  const std::string m = loess_fit(e, ts, sub, es);
+  if (!m.empty()) return m;
+  err.assign(16 * nq, 0.0);
+  for (size_t r = 0; r < 16; ++r)
+    for (size_t q = 0; q < sub; ++q) err[r * nq + q] = es[r * sub + q];
+  for (size_t i = 0; i < 4; ++i) {
+    double t93 = 0.0;
+    for (size_t j = 0; j < 4; ++j) t93 += double(trans[(i * 4 + j) * nq + sub]);
+    for (size_t j = 0; j < 4; ++j) err[(i * 4 + j) * nq + sub] = (double(trans[(i * 4 + j) * nq + sub]) + 1.0) / (t93 + 4.0);
+  }
+  return std::string();
+}
+
+std::string errfun_apply(const ErrFunSpec& e, const std::vector<uint32_t>& trans, size_t nq, std::vector<double>& err) {
+  std::vector<double> off(12 * nq, 0.0);
+  if (e.kind == 1) {  // noqual
+    double obs[16];
+    for (size_t r = 0; r < 16; ++r) {
+      double s = 0.0;
+      for (size_t q = 0; q < nq; ++q) s += double(trans[r * nq + q]);
+      obs[r] = s + e.pseudocount;
+    }
+    size_t o = 0;
+    for (size_t i = 0; i < 4; ++i) {
+      const double tot = obs[i * 4] + obs[i * 4 + 1] + obs[i * 4 + 2] + obs[i * 4 + 3];
+      for (size_t j = 0; j < 4; ++j) {
+        if (i == j) continue;
+        const double rate = tot > 0.0 ? clampr(obs[i * 4 + j] / tot, e) : e.min_error_rate;
+        for (size_t q = 0; q < nq; ++q) off[o * nq + q] = rate;
+        ++o;
+      }
+    }
+    expand12(off, nq, err);
+    return std::string();
+  }
+  if (e.kind == 2) return binned_fit(e, trans, nq, err);
+  if (e.kind == 3) return pacbio_fit(e, trans, nq, err);
+  return loess_fit(e, trans, nq, err);
 }
 
 // src/learn_errors.rs:618-738

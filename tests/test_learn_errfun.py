@@ -7,6 +7,8 @@ quality column fits a constant (11 / 10,030), binned-quality schemes fit,
 the diagonal is 1 minus the off-diagonals), and to each other bit for bit on
 random transition matrices, for LOESS on both surfaces and for noqual.
 """
+import re
+
 import numpy as np
 import pytest
 
@@ -105,3 +107,100 @@ def test_product_fit_equals_the_oracle_bit_for_bit(seed):
                 continue
             b = D.errfun_apply(t, nq, ef)
             assert a.tobytes() == b.tobytes(), (nq, okw)
+
+
+def _binned_case(rng, nq):
+    bins = np.sort(rng.choice(np.arange(nq), size=int(rng.integers(2, min(6, nq + 1))), replace=False)).astype(np.float64)
+    t = np.zeros((16, nq), np.uint32)
+    lo, hi = int(bins[0]), int(bins[-1])
+    cols = rng.integers(lo, hi + 1, size=int(rng.integers(1, 8)))
+    for q in cols:
+        t[:, q] = rng.integers(0, 2000, size=16)
+        for i in range(4):
+            t[i * 5, q] += int(rng.integers(1000, 50000))
+    return t, bins
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_binned_fit_equals_the_oracle_bit_for_bit(seed):
+    """binned_qual_errfun (src/error_models.rs:263-396), product against oracle."""
+    rng = np.random.default_rng(100 + seed)
+    for _ in range(30):
+        nq = int(rng.integers(4, 50))
+        t, bins = _binned_case(rng, nq)
+        try:
+            a = O.errfun_apply(t, nq, kind=2, bins=bins)
+        except ValueError as e:
+            with pytest.raises(D.DgpuError, match=re.escape(str(e))):
+                D.errfun_apply(t, nq, D.ErrFun(kind="binned", bins=tuple(bins)))
+            continue
+        b = D.errfun_apply(t, nq, D.ErrFun(kind="binned", bins=tuple(bins)))
+        assert a.tobytes() == b.tobytes(), (nq, bins)
+
+
+def test_binned_fit_interpolates_between_anchors():
+    """The observed rate at each anchor, linear between them, flat outside."""
+    nq = 41
+    bins = (10.0, 20.0, 40.0)
+    t = np.zeros((16, nq), np.uint32)
+    for q, e in ((10, 100), (20, 300), (40, 50)):
+        for i in range(4):
+            for j in range(4):
+                t[i * 4 + j, q] = 100_000 if i == j else e
+    got = D.errfun_apply(t, nq, D.ErrFun(kind="binned", bins=bins))
+    r = {q: e / (100_000 + 3 * e) for q, e in ((10, 100), (20, 300), (40, 50))}
+    assert got[1, 10] == r[10] and got[1, 20] == r[20] and got[1, 40] == r[40]
+    assert got[1, 0] == r[10]  # flat below the first anchor
+    assert abs(got[1, 15] - (r[10] * 0.5 + r[20] * 0.5)) < 1e-18
+    assert abs(got[1, 30] - (r[20] * 0.5 + r[40] * 0.5)) < 1e-18
+    assert np.allclose(got[0], 1.0 - got[1] - got[2] - got[3])
+
+
+def test_binned_fit_errors():
+    """No observations, and observed qualities outside the anchors, are errors."""
+    nq = 30
+    t = np.zeros((16, nq), np.uint32)
+    for ef, kw in ((D.ErrFun(kind="binned", bins=(5.0, 20.0)), {"kind": 2, "bins": [5.0, 20.0]}),):
+        with pytest.raises(ValueError, match="No observed transitions"):
+            O.errfun_apply(t, nq, **kw)
+        with pytest.raises(D.DgpuError, match="No observed transitions"):
+            D.errfun_apply(t, nq, ef)
+        t2 = t.copy()
+        t2[0, 25] = 10
+        with pytest.raises(ValueError, match="quality score 25 higher than max binned value 20"):
+            O.errfun_apply(t2, nq, **kw)
+        with pytest.raises(D.DgpuError, match="quality score 25 higher than max binned value 20"):
+            D.errfun_apply(t2, nq, ef)
+        t3 = t.copy()
+        t3[0, 2] = 10
+        with pytest.raises(D.DgpuError, match="quality score 2 lower than min binned value 5"):
+            D.errfun_apply(t3, nq, ef)
+
+
+def _pacbio_trans(rng, nq):
+    t = rng.integers(0, 300, size=(16, nq)).astype(np.uint32)
+    for i in range(4):
+        t[i * 5] += rng.integers(5_000, 90_000, size=nq).astype(np.uint32)
+    t[:, rng.random(nq) < 0.15] = 0
+    return t
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_pacbio_fit(seed):
+    """pacbio_errfun (src/error_models.rs:408-462): with a Q93 column (nq = 94)
+    LOESS below it and (count + 1) / (total + 4) in it; otherwise LOESS."""
+    rng = np.random.default_rng(200 + seed)
+    nq = 94
+    t = _pacbio_trans(rng, nq)
+    a = O.errfun_apply(t, nq, kind=3)
+    b = D.errfun_apply(t, nq, D.ErrFun(kind="pacbio"))
+    assert a.tobytes() == b.tobytes()
+    below = D.errfun_apply(np.ascontiguousarray(t[:, :93]), 93, D.ErrFun())
+    assert b[:, :93].tobytes() == below.tobytes()
+    for i in range(4):
+        tot = float(t[i * 4:i * 4 + 4, 93].sum())
+        for j in range(4):
+            assert b[i * 4 + j, 93] == (float(t[i * 4 + j, 93]) + 1.0) / (tot + 4.0)
+    t2 = _pacbio_trans(rng, 60)
+    assert D.errfun_apply(t2, 60, D.ErrFun(kind="pacbio")).tobytes() == D.errfun_apply(t2, 60, D.ErrFun()).tobytes()
+    assert O.errfun_apply(t2, 60, kind=3).tobytes() == D.errfun_apply(t2, 60, D.ErrFun(kind="pacbio")).tobytes()
