@@ -22,7 +22,7 @@ CUDA_HOME = os.path.dirname(os.path.dirname(os.path.realpath(NVCC)))
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 SOURCES_CU = ["dgpu_kernels.cu"]
-SOURCES_CPP = ["dgpu_host.cpp", "dgpu_service.cpp", "dgpu_derep.cpp", "dgpu_errfun.cpp"]
+SOURCES_CPP = ["dgpu_host.cpp", "dgpu_service.cpp", "dgpu_derep.cpp", "dgpu_errfun.cpp", "dgpu_errfun_external.cpp"]
 HEADERS = ["dgpu_common.h"]
 
 

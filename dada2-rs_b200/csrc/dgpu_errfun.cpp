@@ -31,6 +31,7 @@
 namespace dgpu {
 
 void set_last_error(const char* msg);
+int external_errfun_fit(const char* cmd, const uint32_t* trans, int nq, double* err, std::string* msg);
 
 namespace {
 
@@ -453,6 +454,7 @@ int errfun_apply(const dgpu_errfun& ef, const uint32_t* trans, int nq, double* e
   if (ef.kind == DGPU_ERRFUN_LOESS) return loess_fit(ef, trans, nq, err, msg);
   if (ef.kind == DGPU_ERRFUN_BINNED) return binned_fit(ef, trans, nq, err, msg);
   if (ef.kind == DGPU_ERRFUN_PACBIO) return pacbio_fit(ef, trans, nq, err, msg);
+  if (ef.kind == DGPU_ERRFUN_EXTERNAL) return external_errfun_fit(ef.cmd, trans, nq, err, msg);
   *msg = "unknown error function kind";
   return DGPU_E_INVALID;
 }

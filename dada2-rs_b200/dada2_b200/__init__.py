@@ -576,9 +576,10 @@ class ErrFun:
     """The error-model fit of learn-errors (src/learn_errors.rs:67-100):
     kind "loess" (surface "direct", the dada2-rs default, or "interpolate"
     with ``cell``, R's default), "noqual" (``pseudocount``), "binned"
-    (piecewise linear between the anchor qualities ``bins``) or "pacbio"
-    (LOESS, with a maximum-likelihood Q93 column); off-diagonal rates clamped
-    to [min_error_rate, max_error_rate]."""
+    (piecewise linear between the anchor qualities ``bins``), "pacbio"
+    (LOESS, with a maximum-likelihood Q93 column) or "external" (the command
+    ``cmd`` fits the matrix from TSV files); off-diagonal rates clamped to
+    [min_error_rate, max_error_rate]."""
     kind: str = "loess"
     surface: str = "direct"
     cell: float = 0.2
@@ -586,14 +587,15 @@ class ErrFun:
     min_error_rate: float = 1e-7
     pseudocount: float = 1.0
     bins: tuple = ()
+    cmd: str = ""
 
     def c(self) -> ErrFunC:
-        kinds = {"loess": 0, "noqual": 1, "binned": 2, "pacbio": 3}
+        kinds = {"loess": 0, "noqual": 1, "binned": 2, "pacbio": 3, "external": 4}
         surfaces = {"direct": 0, "interpolate": 1}
         b = np.ascontiguousarray(self.bins, np.float64)
         ef = ErrFunC(kinds[self.kind], surfaces[self.surface], float(self.cell), float(self.max_error_rate),
                      float(self.min_error_rate), float(self.pseudocount), b.ctypes.data if len(b) else None,
-                     int(len(b)))
+                     int(len(b)), self.cmd.encode() if self.cmd else None)
         ef._bins = b  # the anchors stay alive with the structure
         return ef
 

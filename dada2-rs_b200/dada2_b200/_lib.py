@@ -64,7 +64,7 @@ class TuningC(C.Structure):
 class ErrFunC(C.Structure):
     _fields_ = [("kind", C.c_int32), ("surface", C.c_int32), ("cell", C.c_double),
                 ("max_error_rate", C.c_double), ("min_error_rate", C.c_double), ("pseudocount", C.c_double),
-                ("bins", C.c_void_p), ("nbins", C.c_int32)]
+                ("bins", C.c_void_p), ("nbins", C.c_int32), ("cmd", C.c_char_p)]
 
 
 class CountersC(C.Structure):

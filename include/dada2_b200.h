@@ -343,12 +343,21 @@ int dgpu_result_margins(const dgpu_result* res, double* out3);
  *                       nq = 94 (a Q93 column), LOESS over columns 0..92 and
  *                       (count + 1) / (source total + 4) for column 93;
  *                       otherwise LOESS
+ *   DGPU_ERRFUN_EXTERNAL external_errfun (src/error_models.rs:650-780): the
+ *                       command `cmd` (split on whitespace, no shell) runs
+ *                       with two paths appended, a TSV of the transitions
+ *                       to read and a TSV of the error matrix to write (R's
+ *                       read.table layout: a header of a tab and 0..nq-1,
+ *                       then rows A2A .. T2T); every value must be finite
+ *                       and in [0, 1]; a failed command's standard error
+ *                       is in the message
  * The diagonal of each nucleotide is 1 minus its three off-diagonals
- * (PacBio's column 93 excepted). */
+ * (PacBio's column 93 and the external fit excepted). */
 #define DGPU_ERRFUN_LOESS 0
 #define DGPU_ERRFUN_NOQUAL 1
 #define DGPU_ERRFUN_BINNED 2
 #define DGPU_ERRFUN_PACBIO 3
+#define DGPU_ERRFUN_EXTERNAL 4
 typedef struct {
   int32_t kind;
   int32_t surface;  /* LOESS: 0 direct, 1 interpolate */
@@ -357,6 +366,7 @@ typedef struct {
   double pseudocount;                     /* NOQUAL (1.0) */
   const double* bins;                     /* BINNED: anchor qualities (NULL otherwise) */
   int32_t nbins;
+  const char* cmd;                        /* EXTERNAL: the command line */
 } dgpu_errfun;
 /* err_out (16 x nq) = the fit of trans (16 x nq). Host only. */
 int dgpu_errfun_apply(const dgpu_errfun* ef, const uint32_t* trans, int nq, double* err_out);

@@ -380,6 +380,7 @@ std::string errfun_apply(const ErrFunSpec& e, const std::vector<uint32_t>& trans
     expand12(off, nq, err);
     return std::string();
   }
+  if (e.kind == 4) return "external_errfun runs a user command: not restated here";
   if (e.kind == 2) return binned_fit(e, trans, nq, err);
   if (e.kind == 3) return pacbio_fit(e, trans, nq, err);
   return loess_fit(e, trans, nq, err);

@@ -34,7 +34,8 @@ def driver(tmp_path_factory):
            "-I", os.path.join(ROOT, "include"), "-I", os.path.join(cuda, "include"),
            os.path.join(ROOT, "tests", "host_loop_driver.cpp"), os.path.join(ROOT, "oracle", "dada_oracle.cpp"),
            os.path.join(ROOT, "oracle", "oracle_capi.cpp"), os.path.join(ROOT, "oracle", "oracle_learn.cpp"),
-           os.path.join(ROOT, "dada2-rs_b200", "csrc", "dgpu_errfun.cpp"), "-o", out, "-L", lib,
+           os.path.join(ROOT, "dada2-rs_b200", "csrc", "dgpu_errfun.cpp"),
+           os.path.join(ROOT, "dada2-rs_b200", "csrc", "dgpu_errfun_external.cpp"), "-o", out, "-L", lib,
            f"-Wl,-rpath,{lib}", "-lcudart", "-lpthread"]
     subprocess.run(cmd, check=True, capture_output=True)
     return out

@@ -8,6 +8,7 @@ the diagonal is 1 minus the off-diagonals), and to each other bit for bit on
 random transition matrices, for LOESS on both surfaces and for noqual.
 """
 import re
+import sys
 
 import numpy as np
 import pytest
@@ -204,3 +205,83 @@ def test_pacbio_fit(seed):
     t2 = _pacbio_trans(rng, 60)
     assert D.errfun_apply(t2, 60, D.ErrFun(kind="pacbio")).tobytes() == D.errfun_apply(t2, 60, D.ErrFun()).tobytes()
     assert O.errfun_apply(t2, 60, kind=3).tobytes() == D.errfun_apply(t2, 60, D.ErrFun(kind="pacbio")).tobytes()
+
+
+def _script(tmp_path, name, body):
+    p = tmp_path / name
+    p.write_text("#!/bin/sh\n" + body)
+    return f"/bin/sh {p}"
+
+
+def _ext(cmd):
+    return D.ErrFun(kind="external", cmd=cmd)
+
+
+def test_external_fit_round_trip(tmp_path, monkeypatch):
+    """external_errfun (src/error_models.rs:650-705): the command reads the
+    transitions' TSV and writes the error matrix's (the reference's
+    test_external_errfun_roundtrip: a constant 0.01 comes back)."""
+    monkeypatch.setenv("TMPDIR", str(tmp_path))
+    cmd = _script(tmp_path, "const.sh", "awk -F'\\t' 'NR==1{print; n=NF-1; next} "
+                  "{s=$1; for(i=1;i<=n;i++) s=s \"\\t0.01\"; print s}' \"$1\" > \"$2\"\n")
+    nq = 4
+    t = np.arange(16 * nq, dtype=np.uint32).reshape(16, nq)
+    got = D.errfun_apply(t, nq, _ext(cmd))
+    assert np.all(got == 0.01)
+    assert [p.name for p in tmp_path.iterdir() if p.name.startswith("dada2-rs-errfun")] == []  # folder removed
+
+
+def test_external_fit_reads_the_transitions(tmp_path, monkeypatch):
+    """The command sees the layout of R's read.table (header of a tab and
+    0..nq-1, rows A2A..T2T) and its numbers come back exactly."""
+    monkeypatch.setenv("TMPDIR", str(tmp_path))
+    prog = tmp_path / "fit.py"
+    prog.write_text(
+        "import sys\n"
+        "rows = open(sys.argv[1]).read().split('\\n')\n"
+        "out = [rows[0]]\n"
+        "for r in rows[1:17]:\n"
+        "    f = r.split('\\t')\n"
+        "    out.append('\\t'.join([f[0]] + [repr((int(x) + 1) / 1000.0) for x in f[1:]]))\n"
+        "open(sys.argv[2], 'w').write('\\n'.join(out) + '\\n')\n")
+    nq = 7
+    rng = np.random.default_rng(3)
+    t = rng.integers(0, 999, size=(16, nq)).astype(np.uint32)
+    got = D.errfun_apply(t, nq, _ext(f"{sys.executable} {prog}"))
+    assert got.tobytes() == ((t.astype(np.float64) + 1.0) / 1000.0).tobytes()
+    head = "\t" + "\t".join(str(q) for q in range(nq))
+    labels = [a + "2" + b for a in "ACGT" for b in "ACGT"]
+    echo = _script(tmp_path, "echo.sh", "cp \"$1\" \"$TMPDIR/seen.tsv\"; awk -F'\\t' 'NR==1{print; n=NF-1; next} "
+                   "{s=$1; for(i=1;i<=n;i++) s=s \"\\t0\"; print s}' \"$1\" > \"$2\"\n")
+    D.errfun_apply(t, nq, _ext(echo))
+    lines = (tmp_path / "seen.tsv").read_text().split("\n")
+    assert lines[0] == head and [ln.split("\t")[0] for ln in lines[1:17]] == labels
+    assert [[int(x) for x in ln.split("\t")[1:]] for ln in lines[1:17]] == t.tolist()
+
+
+def test_external_fit_errors(tmp_path, monkeypatch):
+    """A failing command's status and standard error, an invalid probability
+    (the reference's test_external_errfun_propagates_nonzero_exit and
+    test_external_errfun_rejects_invalid_probability), an empty command and a
+    malformed table are errors."""
+    monkeypatch.setenv("TMPDIR", str(tmp_path))
+    t = np.zeros((16, 4), np.uint32)
+    fail = _script(tmp_path, "fail.sh", "echo 'oops' >&2\nexit 7\n")
+    with pytest.raises(D.DgpuError, match=r"exited with exit status: 7\n--- stderr ---\noops"):
+        D.errfun_apply(t, 4, _ext(fail))
+    bad = _script(tmp_path, "bad.sh", "awk -F'\\t' 'NR==1{print; n=NF-1; next} "
+                  "{s=$1 \"\\t1.5\"; for(i=2;i<=n;i++) s=s \"\\t0.01\"; print s}' \"$1\" > \"$2\"\n")
+    with pytest.raises(D.DgpuError, match=re.escape("err[A2A][0] = 1.5 is not a valid probability in [0, 1]")):
+        D.errfun_apply(t, 4, _ext(bad))
+    with pytest.raises(D.DgpuError, match="--errfun-cmd is empty"):
+        D.errfun_apply(t, 4, _ext("   "))
+    word = _script(tmp_path, "word.sh", "awk -F'\\t' 'NR==1{print; n=NF-1; next} "
+                   "{s=$1 \"\\tabc\"; for(i=2;i<=n;i++) s=s \"\\t0\"; print s}' \"$1\" > \"$2\"\n")
+    with pytest.raises(D.DgpuError, match=re.escape('row 1 column 0 ("abc"): invalid float literal')):
+        D.errfun_apply(t, 4, _ext(word))
+    short = _script(tmp_path, "short.sh", "head -n 5 \"$1\" > \"$2\"\n")
+    with pytest.raises(D.DgpuError, match="err TSV has 4 data rows, expected 16"):
+        D.errfun_apply(t, 4, _ext(short))
+    with pytest.raises(D.DgpuError, match="failed to spawn"):
+        D.errfun_apply(t, 4, _ext(str(tmp_path / "no-such-program")))
+    assert [p.name for p in tmp_path.iterdir() if p.name.startswith("dada2-rs-errfun")] == []
