@@ -701,7 +701,8 @@ def test_multi_device_service_matches_single_sample_calls():
         assert_same_dada(g, D.dada_uniques(s.seqs, s.abund, w.err, w.ncol, D.DadaParams(), quals=s.quals))
 
 
-@pytest.mark.parametrize("kind,surface", [("loess", "direct"), ("loess", "interpolate"), ("noqual", "direct")])
+@pytest.mark.parametrize("kind,surface", [("loess", "direct"), ("loess", "interpolate"), ("noqual", "direct"),
+                                          ("binned", "direct"), ("pacbio", "direct")])
 def test_learn_errors_matches_the_oracle(kind, surface):
     """learn_errors (src/learn_errors.rs:739-1020) on three Illumina-style
     samples: the init pass, every self-consistency pass (all samples denoised
@@ -710,10 +711,12 @@ def test_learn_errors_matches_the_oracle(kind, surface):
     error matrices bit for bit."""
     ws = [synth.small_illumina(60 + i, nvariants=6 + 2 * i, nreads=3000 + 500 * i, L=150) for i in range(3)]
     samples = [w.samples[0] for w in ws]
-    ef = D.ErrFun(kind=kind, surface=surface)
+    bins = (0.0, 10.0, 20.0, 30.0, 40.0, 93.0) if kind == "binned" else ()
+    ef = D.ErrFun(kind=kind, surface=surface, bins=bins)
     got = D.learn_errors(samples, D.DadaParams(), ef, max_consist=6)
-    want = O.learn_errors(samples, O.DadaParams(nthreads=8), max_consist=6, kind=0 if kind == "loess" else 1,
-                          surface=0 if surface == "direct" else 1)
+    want = O.learn_errors(samples, O.DadaParams(nthreads=8), max_consist=6,
+                          kind={"loess": 0, "noqual": 1, "binned": 2, "pacbio": 3}[kind],
+                          surface=0 if surface == "direct" else 1, bins=list(bins) or None)
     assert (got["nq"], got["passes"], got["converged"]) == (want["nq"], want["passes"], want["converged"])
     assert got["passes"] >= 1
     assert np.array_equal(got["trans"], want["trans"])
