@@ -2491,10 +2491,12 @@ __global__ void __launch_bounds__(kNwWarps * 32, kAlignCtasPerSm) k_align(Compar
   cudaGridDependencySynchronize();  // the screen's pass queue and results are complete
   const uint32_t count = *(volatile uint32_t*)&L.queue_counts[4];
   const int kb = rm_kbound(L.geom.rm_pairs);
-  // Few pairs of a launch whose NW pairs are all row-major and span two or
-  // more lane groups: the CTA's warps share each pair (rm_align_coop), which
-  // cuts a long pair's latency, the bound of such calls.
-  const bool coop = FORMS != kFormsVec1 && L.geom.vec_scratch == 0 && kb >= 2 && count <= 2u * gridDim.x;
+  // Few pairs of a launch whose NW pairs are all row-major and span two to
+  // four lane groups: the CTA's warps share each pair (rm_align_coop), which
+  // cuts a long pair's latency, the bound of such calls. Wider bands (eight
+  // or sixteen groups, G > 1 per warp) keep one warp per pair.
+  const bool coop = FORMS != kFormsVec1 && L.geom.vec_scratch == 0 && kb >= 2 && kb <= kNwWarps &&
+                    count <= 2u * gridDim.x;
   if (blockIdx.x * (coop ? 1u : uint32_t(kNwWarps)) >= count) return;  // nothing queued for this block
   const size_t err_bytes = err_smem_bytes(kp.ncol);
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
