@@ -259,15 +259,25 @@ int external_errfun_fit(const char* cmd_c, const uint32_t* trans, int nq, double
   }
   TempFolder tmp;
   {
+    // a folder this call creates itself (an existing one, which another user
+    // could have planted, is never written into)
     const char* t = std::getenv("TMPDIR");
     const std::string base = (t && *t) ? t : "/tmp";
-    const std::string path = base + "/dada2-rs-errfun-" + std::to_string(getpid()) + "-" +
-                             std::to_string(g_folder_seq.fetch_add(1));
-    if (mkdir(path.c_str(), 0700) != 0 && errno != EEXIST) {
-      *msg = "external_errfun: failed to create temp dir: " + os_error(errno);
+    int e = EEXIST;
+    for (int tries = 0; tries < 100 && e == EEXIST; ++tries) {
+      const std::string path = base + "/dada2-rs-errfun-" + std::to_string(getpid()) + "-" +
+                               std::to_string(g_folder_seq.fetch_add(1));
+      if (mkdir(path.c_str(), 0700) == 0) {
+        tmp.path = path;
+        e = 0;
+      } else {
+        e = errno;
+      }
+    }
+    if (e != 0) {
+      *msg = "external_errfun: failed to create temp dir: " + os_error(e);
       return DGPU_E_INVALID;
     }
-    tmp.path = path;
   }
   const std::string trans_path = tmp.path + "/trans.tsv", err_path = tmp.path + "/err.tsv";
   {
